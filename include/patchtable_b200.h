@@ -1,0 +1,153 @@
+/* patchtable_b200 -- C ABI of the B200 PatchTable build + query path.
+
+   Plain pointers and sizes only; no CUDA or torch types cross this boundary (streams are passed
+   as void *).  Every entry point returns a pt_status; pt_last_error() gives the message of the
+   last failure on the calling thread.  Host buffers are never retained: the library copies
+   what it needs to device memory.
+
+   Each declaration names the reference interface it replaces (paths relative to the
+   reference project root, uva-graphics/patchtable). */
+#ifndef PATCHTABLE_B200_H
+#define PATCHTABLE_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PT_OK = 0,
+    PT_BAD_ARG = 1,       /* invalid size, pointer or parameter */
+    PT_OOM = 2,           /* device or host allocation failed */
+    PT_CUDA_ERR = 3,      /* a CUDA call failed; see pt_last_error() */
+    PT_TIMEOUT = 4,       /* a bounded device wait gave up */
+    PT_UNSUPPORTED = 5,   /* parameter combination not implemented on the GPU path */
+    PT_IO = 6             /* table file could not be read or written */
+} pt_status;
+
+#define PT_MAX_DIMS 16
+#define PT_PATH_MAX 256
+
+/* Numeric fields of PatchTableParams (patchtable/patchtable_params.h:23-161) read by the
+   build/query path, with the reference's names and meanings. */
+typedef struct pt_params {
+    double limit;                 /* max table cells (switch value x 1e6), patchtable.cpp:171 */
+    int ndims, nchroma, grid_ndims;
+    int nslices[PT_MAX_DIMS];     /* explicit -nslices (n_nslices > 0) */
+    int n_nslices;
+    int partition_step;
+    int populate_random, populate_nearest;
+    int run_dt, dt_algo, dt_iters;        /* dt_algo: 0 raster 1 prop 2 brute 3 kdtree 4 downsample 5 hybrid 6 euclidean */
+    int kcoherence, kcoherence_min_dist, kcoherence_step, kcoherence_iter;
+    int flann_reset_step, flann_build_step;
+    double triangle_factor;
+    int prop_iters, query_step, do_prop, prop_dist;
+    double coherence_spatial, coherence_temporal;
+    int do_table_lookup, do_rs, spatial;
+    int allowed_index;
+    int recalc_dist_temporal, sanitize_input, init_random;
+    int convert_colorspace, colorspace;   /* colorspace: 0 yuv, 1 lab */
+    int is_descriptor, descriptor_padded;
+    int patch_w;
+    int threads, verbose, query_iters, ntables;
+    double table_ratio;
+    int lookup_algo, kcoherence_algo, dim_algo;
+    int incoherence, randomize_dt, parallel_dt, populate_exptime, dt_mode;
+    char load_filename[PT_PATH_MAX];
+    char save_filename[PT_PATH_MAX];
+    /* GPU query schedule (no reference counterpart): number of parallel propagation passes
+       that replace the reference's sequential scanline sweeps; 0 picks the default. */
+    int gpu_prop_passes;
+} pt_params;
+
+typedef struct pt_table pt_table;
+
+/* PatchTableParams::PatchTableParams() = set_defaults() + set_speed(3),
+   patchtable.cpp:26-136, 380-382. */
+void pt_params_default(pt_params *p);
+
+/* PatchTableParams::set_speed(i), patchtable.cpp:138-150.  PT_BAD_ARG unless 0 <= i <= 9. */
+pt_status pt_params_set_speed(pt_params *p, int speed);
+
+/* PatchTableParams::set_from_switches(string), patchtable.cpp:152-373: "-name value" pairs with
+   the reference's switch names, "-speed" applied first, "-limit" in millions. */
+pt_status pt_params_from_switches(pt_params *p, const char *switches);
+
+/* PatchTable<float,float,int32_t>(PatchTableParams *p, const Array<float> &b,
+   Array<int32_t> *allowed_patches = NULL), patchtable.h:4397-4424 -> PatchTableFixedN ctor
+   patchtable.h:2584-3373.  b is h x w x 3 float RGB (row-major, channels interleaved);
+   allowed is (h-7) x (w-7) int32 or NULL.  In descriptor mode (p->is_descriptor) b is
+   h x w x channels descriptors. */
+pt_status pt_table_create(const pt_params *p, const float *b, int h, int w, int channels,
+                          const int32_t *allowed, pt_table **out);
+
+/* PatchTableFixedN(p, b, allowed, b0_no_copy, wh0_no_copy), patchtable.h:2584: build from a
+   precomputed padded descriptor wh0 of (h+7) x (w+7) x ndims floats instead of computing it. */
+pt_status pt_table_create_with_descriptor(const pt_params *p, const float *b, int h, int w,
+                                          const float *wh0, const int32_t *allowed, pt_table **out);
+
+/* PatchTableFixedN(PatchTableParams *, string filename) / load(), patchtable.h:1574-1622. */
+pt_status pt_table_load(const pt_params *p, const char *filename, pt_table **out);
+
+/* PatchTable<>::save(string), patchtable.h:4470-4490 / PatchTableFixedN::save, :1574-1605. */
+pt_status pt_table_save(const pt_table *t, const char *filename);
+
+void pt_table_free(pt_table *t);
+
+/* double PatchTable<>::lookup(const Array<float> &a, Array<double> &ann,
+   Array<double> *ann_prev = NULL, Array<float> *coherence_temporal_sv = NULL),
+   patchtable.h:4448-4468 -> lookup_templated, :3468-4217.
+   a: h x w x 3 host floats.  ann_out: (h-7) x (w-7) x 3 host doubles [NNF_X, NNF_Y, NNF_DIST]
+   (patchtable.h:175-177).  ann_prev: same layout or NULL.  coh_sv: (h-7) x (w-7) floats or NULL.
+   *seconds (may be NULL) receives the wall time of the call including a's descriptor, like the
+   reference's return value (patchtable.h:3477, 4211). */
+pt_status pt_table_lookup(pt_table *t, const float *a, int h, int w, double *ann_out,
+                          const double *ann_prev, const float *coh_sv, double *seconds);
+
+/* Device-resident form of pt_table_lookup (no reference counterpart; the reference has no
+   device memory): d_a and d_ann are device pointers with the host layouts above; the call is
+   asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream). */
+pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int h, int w, double *d_ann,
+                                 void *stream);
+
+/* Batched query (no reference counterpart; the reference matches one image per lookup() call,
+   patchtable.h:4448): n query images of individual sizes against one table, in one persistent
+   launch over the flattened patch index.  a[i] / ann_out[i] are host buffers with the
+   pt_table_lookup layouts. */
+pt_status pt_table_lookup_batch(pt_table *t, int n, const float *const *a, const int *h,
+                                const int *w, double *const *ann_out);
+
+/* ---- introspection (parity tests); shapes as in the reference members patchtable.h:1487-1549 ---- */
+
+/* Grid dimension count; nslices receives PT_MAX_DIMS entries; *ncells the table size. */
+int pt_table_shape(const pt_table *t, int *nslices, int64_t *ncells);
+/* table (ncells int32, row-major over nslices, values XY_TO_INT(x+7, y+7)). */
+pt_status pt_table_get_cells(const pt_table *t, int32_t *out);
+/* Descriptor of every b patch, (h-7) x (w-7) x ndims, i.e. wh0 without its padding. */
+pt_status pt_table_get_descriptor(const pt_table *t, float *out);
+/* Partition of dimension dim: centers/lsizes/rsizes (nslices[dim] floats each),
+   to_bin (16384 int32), mmr = {min_val, max_val, range} (patchtable.h:1131-1145). */
+pt_status pt_table_get_partition(const pt_table *t, int dim, float *centers, float *lsizes,
+                                 float *rsizes, int32_t *to_bin, float *mmr);
+/* k-coherence set (patchtable.h:1520): (h-7) x (w-7) x kcoherence packed positions and dists. */
+pt_status pt_table_get_kcoherence(const pt_table *t, int32_t *pos, float *dist);
+/* Number of cells seeded by populate (table_add_count, patchtable.h:1539). */
+int64_t pt_table_add_count(const pt_table *t);
+
+/* Descriptor of an RGB image as the query computes it: (h-7) x (w-7) x ndims floats. */
+pt_status pt_descriptor(const pt_params *p, const float *rgb, int h, int w, float *out);
+
+/* Device kernel launches issued by this thread since the last reset (evidence counter). */
+int64_t pt_kernel_launch_count(void);
+void pt_kernel_launch_count_reset(void);
+
+const char *pt_last_error(void);
+const char *pt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PATCHTABLE_B200_H */

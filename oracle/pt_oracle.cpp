@@ -1,0 +1,808 @@
+/* CPU restatement of the reference PatchTable build + query path.
+
+   TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
+   leg load this library, and only as the checker.  It restates, step by step and in the same
+   floating-point order, the reference functions cited beside each routine (paths are relative
+   to the reference project root).  Its results are pinned against the reference's own sources
+   compiled in oracle/_ref (tests/test_oracle_vs_ref.py).
+
+   Deliberate stand-in: the k-coherence nearest-neighbour search uses the exact search of
+   oracle/knn_exact.h in place of FLANN (FLANN is neither vendored nor version-pinned).
+
+   All arithmetic is float unless the reference uses double; the file is compiled with
+   -ffp-contract=off so no multiply-add is fused. */
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include "knn_exact.h"
+#include "gck_steps.h"
+
+using std::vector;
+
+namespace {
+
+const int PW = 8;                 /* patch width: TABLE_PATCH_W, patchtable.h:48 */
+const int NMAP = 16384;           /* PATCH_PARTITION_NMAP, patchtable.h:216 */
+const int UNUSED = (1 << 30) - 1; /* TABLE_UNUSED, patchtable.h:109-112 */
+const double DIST_INF = 100000;   /* DIST_INFINITY, patchtable.h:173 */
+
+inline int xy_to_int(int x, int y) { return x | (y << 16); }   /* patchtable.h:163-165 */
+inline int int_to_x(int v) { return v & 65535; }
+inline int int_to_y(int v) { return v >> 16; }
+
+}  // namespace
+
+extern "C" {
+
+/* The subset of PatchTableParams (patchtable_params.h:23-161) that the build/query path reads. */
+typedef struct {
+    int ndims, nchroma, grid_ndims;
+    double limit;
+    int nslices[16], n_nslices;       /* explicit -nslices, n_nslices == 0 means automatic */
+    int partition_step;
+    int populate_random;
+    int run_dt, dt_algo, dt_iters;    /* dt_algo: 1 = prop (the only one restated here) */
+    int kcoherence, kcoherence_min_dist, kcoherence_step, kcoherence_iter;
+    int flann_reset_step, flann_build_step;
+    double triangle_factor;
+    int prop_iters, query_step, do_prop, prop_dist;
+    double coherence_spatial, coherence_temporal;
+    int do_table_lookup, do_rs, spatial;
+    int allowed_index;
+    int recalc_dist_temporal, sanitize_input, init_random;
+    int convert_colorspace;
+} orc_params;
+
+}
+
+namespace {
+
+/* ------------------------------------------------------------------------------------------
+   Colour conversion: ARRAY_RGB2YUV, solver/array.h:1116-1127.  The constants are double, the
+   pixel is float, the sum is evaluated left to right in double and stored as float.
+   ------------------------------------------------------------------------------------------ */
+void rgb2yuv(const float *in, int n, float *out) {
+    for (int i = 0; i < n; i++) {
+        float R = in[3 * i], G = in[3 * i + 1], B = in[3 * i + 2];
+        out[3 * i + 0] = (float) (0.299 * R + 0.587 * G + 0.114 * B);
+        out[3 * i + 1] = (float) (-0.14713 * R + -0.28886 * G + 0.436 * B);
+        out[3 * i + 2] = (float) (0.615 * R + -0.51499 * G + -0.10001 * B);
+    }
+}
+
+/* ------------------------------------------------------------------------------------------
+   Gray-code kernels: gck_8<float,float,n,nchroma>, patchtable/gck.h:29-1950 (generated by
+   gck.py:84-517).  Output is (h+7) x (w+7) x (n + 2*nchroma) "full" convolution.
+   ------------------------------------------------------------------------------------------ */
+void gck8(const float *in, int h, int w, int n, int nchroma, float *out) {
+    const int rpad = PW / 2, lpad = rpad - 1, lread = rpad, rread = lpad, pad = lpad + rpad;
+    const int OH = h + pad, OW = w + pad, OC = n + nchroma * 2;
+    vector<float> temp((size_t) OH * OW * 3);
+    auto in_zero = [&](int y, int x, int c) -> float {
+        if (y < 0 || y >= h || x < 0 || x >= w) return 0.0f;
+        return in[((size_t) y * w + x) * 3 + c];
+    };
+    auto T = [&](int y, int x, int c) -> float & { return temp[((size_t) y * OW + x) * 3 + c]; };
+    auto T_zero = [&](int y, int x, int c) -> float {
+        if (y < 0 || y >= OH || x < 0 || x >= OW) return 0.0f;
+        return temp[((size_t) y * OW + x) * 3 + c];
+    };
+    auto O = [&](int y, int x, int c) -> float & { return out[((size_t) y * OW + x) * OC + c]; };
+    auto O_zero = [&](int y, int x, int c) -> float {
+        if (y < 0 || y >= OH || x < 0 || x >= OW) return 0.0f;
+        return out[((size_t) y * OW + x) * OC + c];
+    };
+    /* Horizontal running box sum (gck.h:52-152): temp(y,x) = temp(y,x-1) + in(y-3, x) - in(y-3, x-8). */
+    for (int y = 0; y < OH; y++) {
+        int ysrc = y - lpad;
+        for (int c = 0; c < 3; c++) T(y, 0, c) = in_zero(ysrc, 0, c);
+        for (int x = 1; x < OW; x++) {
+            int xsrc = x - lpad;
+            for (int c = 0; c < 3; c++)
+                T(y, x, c) = T(y, x - 1, c) + in_zero(ysrc, xsrc + rread, c) - in_zero(ysrc, xsrc - lread - 1, c);
+        }
+    }
+    /* Vertical running box sum (gck.h:160-205). */
+    for (int x = 0; x < OW; x++)
+        for (int c = 0; c < 3; c++) O(0, x, c) = T(rread, x, c);
+    for (int y = 1; y < OH; y++)
+        for (int x = 0; x < OW; x++)
+            for (int c = 0; c < 3; c++)
+                O(y, x, c) = O(y - 1, x, c) + T_zero(y + rread, x, c) - T_zero(y - lread - 1, x, c);
+    /* Snake-order recurrences for kernels 1..n-1 (gck.h:215-1950, gck.py:364-420):
+       out_i(p) = s*out_i(p-d) + out_{i-1}(p) + s*out_{i-1}(p-d), evaluated left to right. */
+    auto c0 = [&](int k) { return k < nchroma ? k * 3 : nchroma * 3 + (k - nchroma); };
+    for (int y = 0; y < OH; y++) {
+        for (int x = 0; x < OW; x++) {
+            for (int i = 1; i < n; i++) {
+                int horiz = ORC_GCK_STEPS[i - 1][0], d = ORC_GCK_STEPS[i - 1][1];
+                float s = (float) ORC_GCK_STEPS[i - 1][2];
+                int yp = horiz ? y : y - d, xp = horiz ? x - d : x;
+                int nc = i < nchroma ? 3 : 1;
+                for (int c = 0; c < nc; c++) {
+                    float a = s * O_zero(yp, xp, c0(i) + c);
+                    float b = O(y, x, c0(i - 1) + c);
+                    float e = s * O_zero(yp, xp, c0(i - 1) + c);
+                    O(y, x, c0(i) + c) = a + b + e;
+                }
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------------------------
+   Exact patch distance: patch_dist_exact<float,8,3>, patchtable.h:330-373 (SSE path).  Four
+   lane sums over 8 rows x 6 chunks of 4 floats, lanes added 0+1+2+3 at the end.
+   ------------------------------------------------------------------------------------------ */
+float patch_dist_exact(const float *a, int a_w, int ax, int ay, const float *b, int b_w, int bx, int by) {
+    float lane[4] = {0, 0, 0, 0};
+    for (int dy = 0; dy < PW; dy++) {
+        const float *arow = a + ((size_t) (ay + dy) * a_w + ax) * 3;
+        const float *brow = b + ((size_t) (by + dy) * b_w + bx) * 3;
+        float d[6][4];
+        for (int nn = 0; nn < 6; nn++)
+            for (int q = 0; q < 4; q++) {
+                float t = arow[nn * 4 + q] - brow[nn * 4 + q];
+                d[nn][q] = t * t;
+            }
+        for (int q = 0; q < 4; q++)
+            lane[q] = lane[q] + d[0][q] + d[1][q] + d[2][q] + d[3][q] + d[4][q] + d[5][q];
+    }
+    return lane[0] + lane[1] + lane[2] + lane[3];
+}
+
+/* ------------------------------------------------------------------------------------------
+   One-dimensional partition: PatchPartition1D, patchtable.h:1131-1326 (non-regular grid,
+   randomize = false).
+   ------------------------------------------------------------------------------------------ */
+struct Partition1D {
+    vector<int> to_bin;
+    vector<float> centers, lsizes, rsizes;
+    float min_val, max_val, range;
+    int nslices;
+
+    /* get_bin, patchtable.h:1298-1325. */
+    int get_bin(float v) const {
+        int idx = (int) ((v - min_val) * (float) (NMAP - 1) / range);
+        if (idx < 0) idx = 0;
+        else if (idx >= NMAP) idx = NMAP - 1;
+        return to_bin[idx];
+    }
+};
+
+struct Table {
+    orc_params p;
+    int h, w;                   /* b size */
+    int nd;                     /* descriptor dims */
+    int gnd;                    /* grid dims */
+    vector<float> b0;           /* h x w x 3 RGB */
+    vector<float> wh0;          /* (h+7) x (w+7) x nd */
+    vector<int> allowed;        /* (h-7) x (w-7), empty if none */
+    vector<int> nslices;
+    vector<int64_t> stride;
+    int64_t ncells = 0;
+    vector<int32_t> table;
+    vector<Partition1D> part;
+    int table_add_count = 0;
+    int kc_h = 0, kc_w = 0;
+    vector<int32_t> kc_pos;     /* kc_h x kc_w x kcoherence */
+    vector<float> kc_dist;
+    vector<float> min_val, max_val, range;
+    /* Scratch reused across lookups, like lookup_buffer/lookup_wh (patchtable.h:1507-1509). */
+    vector<float> lookup_wh;
+
+    int WW() const { return w + 7; }
+    float whv(int y, int x, int i) const { return wh0[((size_t) y * WW() + x) * nd + i]; }
+    bool is_allowed(int py, int px) const {
+        return allowed.empty() || allowed[(size_t) py * (w - 7) + px] == p.allowed_index;
+    }
+};
+
+/* get_padded_descriptor for RGB input (patchtable.h:2492-2546): YUV then gck. */
+void padded_descriptor(const orc_params &p, const float *rgb, int h, int w, vector<float> &wh) {
+    vector<float> yuv((size_t) h * w * 3);
+    if (p.convert_colorspace) rgb2yuv(rgb, h * w, yuv.data());
+    else memcpy(yuv.data(), rgb, sizeof(float) * yuv.size());
+    wh.assign((size_t) (h + 7) * (w + 7) * p.ndims, 0.0f);
+    gck8(yuv.data(), h, w, p.ndims - p.nchroma * 2, p.nchroma, wh.data());
+}
+
+/* scale_slices_to_limit, patchtable.cpp:611-642 (product and multiply: solver/util.cpp:186-205). */
+vector<int> scale_slices_to_limit(vector<int> nslices, double limit) {
+    auto product = [](const vector<int> &L) { double a = 1.0; for (int v : L) a *= v; return a; };
+    if (limit > 0) {
+        vector<int> nslices0(nslices);
+        double factor = 1.0;
+        for (auto &v : nslices) v = std::max(v, 1);
+        while (product(nslices) > limit) {
+            factor *= 0.995;
+            for (size_t i = 0; i < nslices.size(); i++) nslices[i] = (int) (nslices0[i] * factor + 0.5);
+            for (auto &v : nslices) v = std::max(v, 1);
+        }
+        for (;;) {
+            nslices0 = nslices;
+            bool success = false;
+            for (size_t i = 0; i < nslices.size(); i++) {
+                nslices[i]++;
+                if (product(nslices) > limit) nslices = nslices0;
+                else { success = true; nslices0 = nslices; }
+            }
+            if (!success) break;
+        }
+    }
+    return nslices;
+}
+
+void build_kcoherence(Table &t);
+void dt_prop(Table &t);
+
+/* PatchTableFixedN constructor, patchtable.h:2584-3373, default path (no product quantisation,
+   no k-means, populate_nearest with TABLE_POPULATE_FAST, single table). */
+Table *build(const orc_params &p, const float *b, int h, int w, const int32_t *allowed, const float *wh0_in) {
+    Table *t = new Table();
+    t->p = p;
+    t->h = h; t->w = w;
+    t->nd = p.ndims;
+    t->gnd = p.grid_ndims < 0 ? p.ndims : p.grid_ndims;
+    t->b0.assign(b, b + (size_t) h * w * 3);
+    if (wh0_in) t->wh0.assign(wh0_in, wh0_in + (size_t) (h + 7) * (w + 7) * p.ndims);
+    else padded_descriptor(p, b, h, w, t->wh0);
+    if (allowed) t->allowed.assign(allowed, allowed + (size_t) (h - 7) * (w - 7));
+    const int xmin = 7, ymin = 7, xmax = w, ymax = h;   /* gck_xmin/xmax, patchtable_params.h:14-17 */
+
+    if (p.kcoherence) build_kcoherence(*t);
+
+    /* set_min_max, patchtable.h:1758-1778. */
+    int G = t->gnd;
+    t->min_val.assign(G, 1e20f);
+    t->max_val.assign(G, -1e20f);
+    for (int y = ymin; y < ymax; y++)
+        for (int x = xmin; x < xmax; x++) {
+            if (!t->is_allowed(y - ymin, x - xmin)) continue;
+            for (int i = 0; i < G; i++) {
+                float v = t->whv(y, x, i);
+                t->min_val[i] = std::min(t->min_val[i], v);
+                t->max_val[i] = std::max(t->max_val[i], v);
+            }
+        }
+    t->range.resize(G);
+    for (int i = 0; i < G; i++) t->range[i] = t->max_val[i] - t->min_val[i];
+
+    /* set_default_nslices, patchtable.h:1780-1810 (TABLE_SIZE_STDDEV == 0). */
+    vector<int> ns(G);
+    if (p.n_nslices == 0) {
+        float max_range = t->range[0];
+        for (int i = 1; i < G; i++) if (t->range[i] > max_range) max_range = t->range[i];
+        double scale = 200.0 / max_range;
+        for (int i = 0; i < G; i++) ns[i] = (int) (t->range[i] * scale);
+    } else {
+        for (int i = 0; i < G; i++) ns[i] = p.nslices[i];
+    }
+    t->nslices = scale_slices_to_limit(ns, p.limit);
+
+    /* PatchPartition, patchtable.h:1355-1396: patches sampled every partition_step. */
+    vector<int> patches;
+    for (int y = ymin; y < ymax; y += p.partition_step)
+        for (int x = xmin; x < xmax; x += p.partition_step)
+            if (t->is_allowed(y - ymin, x - xmin)) patches.push_back(xy_to_int(x, y));
+    t->part.resize(G);
+    for (int c = 0; c < G; c++) {
+        Partition1D &P = t->part[c];
+        int ncs = t->nslices[c];
+        P.nslices = ncs;
+        /* Sorting by channel value; only values at quantile positions are read, so the
+           (unstable) order of equal values does not matter (patchtable.h:1172-1176). */
+        vector<float> vals(patches.size());
+        for (size_t i = 0; i < patches.size(); i++) vals[i] = t->whv(int_to_y(patches[i]), int_to_x(patches[i]), c);
+        std::sort(vals.begin(), vals.end());
+        P.min_val = t->min_val[c];
+        P.max_val = t->max_val[c];
+        P.range = P.max_val - P.min_val;
+        P.centers.resize(ncs); P.lsizes.resize(ncs); P.rsizes.resize(ncs);
+        int N = (int) vals.size();
+        for (int i = 0; i < ncs; i++) {            /* patchtable.h:1193-1201 */
+            int idx1 = (N - 1) * i / ncs;
+            int idx2 = (N - 1) * (i + 1) / ncs;
+            float cell_max = vals[idx2], cell_min = vals[idx1];
+            P.centers[i] = (cell_min + cell_max) / 2;
+        }
+        for (int i = 0; i < ncs; i++) {            /* patchtable.h:1203-1215 */
+            float prev_center = (i - 1 >= 0) ? P.centers[i - 1] : P.min_val;
+            float next_center = (i + 1 < ncs) ? P.centers[i + 1] : P.max_val;
+            P.lsizes[i] = P.centers[i] - prev_center;
+            if (i - 1 >= 0) P.lsizes[i] /= 2;
+            P.rsizes[i] = next_center - P.centers[i];
+            if (i + 1 < ncs) P.rsizes[i] /= 2;
+        }
+        P.to_bin.resize(NMAP);                      /* patchtable.h:1219-1256 */
+        int icenter = 0;
+        for (int i = 0; i < NMAP; i++) {
+            double coord = P.min_val + (i + 0.5) * P.range / NMAP;
+            while (coord > P.centers[icenter]) {
+                if (icenter + 1 < ncs) icenter++;
+                else break;
+            }
+            int prev_c = icenter - 1;
+            if (prev_c < 0) prev_c = 0;
+            int next_c = icenter;
+            if (next_c == 0) next_c++;
+            if (ncs == 1) next_c = prev_c = 0;
+            double mid = (P.centers[prev_c] + P.centers[next_c]) / 2.0;
+            P.to_bin[i] = (coord < mid) ? prev_c : next_c;
+        }
+    }
+
+    /* Table shape and strides: Array<itype>::resize(nslices), row-major (solver/array.h:262-294). */
+    t->stride.assign(G, 1);
+    t->ncells = 1;
+    for (int i = G - 1; i >= 0; i--) { t->stride[i] = t->ncells; t->ncells *= t->nslices[i]; }
+    t->table.assign((size_t) t->ncells, UNUSED);
+
+    /* Populate, TABLE_POPULATE_INNER_BLOCK with populate_random (patchtable.h:3121-3159):
+       std::random_shuffle of the allowed patch list, first visitor of a cell wins. */
+    vector<int> order;
+    for (int y = ymin; y < ymax; y++)
+        for (int x = xmin; x < xmax; x++)
+            if (t->is_allowed(y - ymin, x - xmin)) order.push_back(xy_to_int(x, y));
+    if (p.populate_random) {
+        /* libstdc++ random_shuffle(first, last): for i in 1..n-1, j = rand() % (i + 1), swap. */
+        for (size_t i = 1; i < order.size(); i++) {
+            size_t j = (size_t) (rand() % (int) (i + 1));
+            if (i != j) std::swap(order[i], order[j]);
+        }
+    }
+    for (int pos : order) {
+        int x = int_to_x(pos), y = int_to_y(pos);
+        int64_t cell = 0;
+        for (int i = 0; i < G; i++) cell += (int64_t) t->part[i].get_bin(t->whv(y, x, i)) * t->stride[i];
+        if (t->table[cell] == UNUSED) { t->table[cell] = xy_to_int(x, y); t->table_add_count++; }
+    }
+
+    /* Distance transform (patchtable.h:3254-3298). */
+    bool zeros_filled = false;
+    if (p.run_dt) {
+        if (p.dt_algo == 1) { dt_prop(*t); zeros_filled = (p.dt_iters <= 0); }
+        else { fprintf(stderr, "oracle: only dt_algo prop is restated\n"); abort(); }
+    }
+    if (!zeros_filled) {                            /* fill_zeros, patchtable.h:2063-2079 */
+        int vfill = xy_to_int(PW - 1, PW - 1);
+        if (!t->allowed.empty()) {
+            bool found = false;
+            for (int y = ymin; y < ymax && !found; y++)
+                for (int x = xmin; x < xmax; x++)
+                    if (t->is_allowed(y - ymin, x - xmin)) { vfill = xy_to_int(x, y); found = true; break; }
+        }
+        for (auto &v : t->table) if (v == UNUSED) v = vfill;
+    }
+    return t;
+}
+
+/* do_dt_prop, patchtable.h:2081-2165, with PropEdge labels (patchtable.h:1435-1468). */
+void dt_prop(Table &t) {
+    int G = t.gnd;
+    struct Elem { int64_t grid_index; int32_t table_value; uint8_t label; };
+    vector<Elem> cur, nxt;
+    for (int64_t j = 0; j < t.ncells; j++)
+        if (t.table[j] != UNUSED) cur.push_back(Elem{j, t.table[j], 0});
+    int nlabels = 1 + G * 2;
+    struct Edge { int dim, dir, label; };
+    auto mk = [&](int dim, int dir) { return Edge{dim, dir, 2 * dim + 1 + (dir + 1) / 2}; };
+    vector<vector<Edge>> next_label;
+    vector<Edge> next0;
+    for (int i = 0; i < G; i++) { next0.push_back(mk(i, -1)); next0.push_back(mk(i, 1)); }
+    next_label.push_back(next0);
+    for (int i = 0; i < G; i++)
+        for (int dir = -1; dir <= 1; dir += 2) {
+            vector<Edge> nx;
+            nx.push_back(mk(i, dir));
+            for (int j = i + 1; j < G; j++) { nx.push_back(mk(j, -1)); nx.push_back(mk(j, 1)); }
+            next_label.push_back(nx);
+        }
+    (void) nlabels;
+    for (int iter = 0;; iter++) {
+        if (t.p.dt_iters > 0 && iter > t.p.dt_iters) break;
+        if (cur.empty()) break;
+        nxt.clear();
+        for (const Elem &e : cur) {
+            for (const Edge &E : next_label[e.label]) {
+                int64_t gp = e.grid_index + E.dir * t.stride[E.dim];
+                if (gp >= 0 && gp < t.ncells && t.table[gp] == UNUSED) {
+                    int64_t dp = (e.grid_index / t.stride[E.dim]) % t.nslices[E.dim] + E.dir;
+                    if (dp >= 0 && dp < t.nslices[E.dim]) {
+                        t.table[gp] = e.table_value;
+                        nxt.push_back(Elem{gp, e.table_value, (uint8_t) E.label});
+                    }
+                }
+            }
+        }
+        cur.swap(nxt);
+    }
+}
+
+/* k-coherence with the FLANN path, patchtable.h:2653-2869 (TABLE_KCOHERENCE_TRIANGLE,
+   kcoherence_algo flann, incoherence off).  The vectors is_valid / matched_* live across the
+   patch loop exactly as in the reference, so entries past the early break keep the values the
+   previous patch left in them (patchtable.h:2675-2677, 2793-2796). */
+void build_kcoherence(Table &t) {
+    const orc_params &p = t.p;
+    const int xmin = 7, ymin = 7, xmax = t.w, ymax = t.h;
+    int bew = xmax - xmin, beh = ymax - ymin;
+    int K = p.kcoherence, nd = t.nd;
+    t.kc_h = beh; t.kc_w = bew;
+    t.kc_pos.assign((size_t) beh * bew * K, 0);
+    t.kc_dist.assign((size_t) beh * bew * K, 0.0f);
+    /* build_flann_index_func, patchtable.h:822-861. */
+    vector<float> train;
+    vector<int> index_to_pos;
+    for (int y = ymin; y < ymax; y += p.flann_build_step)
+        for (int x = xmin; x < xmax; x += p.flann_build_step) {
+            if (!t.is_allowed(y - ymin, x - xmin)) continue;
+            for (int i = 0; i < nd; i++) train.push_back(t.whv(y, x, i));
+            index_to_pos.push_back(xy_to_int(x - xmin, y - ymin));
+        }
+    ptoracle::ExactKnn index(train.data(), (int) index_to_pos.size(), nd);
+    int knn0 = K + 1;
+    vector<float> q(nd);
+    vector<bool> is_valid(knn0);
+    vector<int> matched_indices(knn0);
+    vector<float> matched_dists(knn0);
+    vector<ptoracle::KnnResult> res;
+    int prev_knn = knn0;
+    int min_dist2 = p.kcoherence_min_dist * p.kcoherence_min_dist;
+    vector<std::pair<float, std::pair<int, int>>> triples;
+    for (int y = ymin; y < ymax; y += p.kcoherence_step) {
+        for (int x = xmin; x < xmax; x += p.kcoherence_step) {
+            if (!t.is_allowed(y - ymin, x - xmin)) continue;
+            int yk = (y - ymin) / p.kcoherence_step, xk = (x - xmin) / p.kcoherence_step;
+            for (int i = 0; i < nd; i++) q[i] = t.whv(y, x, i);
+            int knn = (x / p.kcoherence_step) % p.flann_reset_step == 0 ? knn0 : prev_knn;
+            while (1) {
+                is_valid.resize(knn);
+                matched_indices.resize(knn);
+                matched_dists.resize(knn);
+                index.query(q.data(), knn, res);
+                if ((int) res.size() < knn) { fprintf(stderr, "oracle: k-coherence needs more points\n"); abort(); }
+                for (int i = 0; i < knn; i++) { matched_indices[i] = index_to_pos[res[i].idx]; matched_dists[i] = res[i].dist; }
+                int nvalid = 0;
+                for (int i = 0; i < knn; i++) {
+                    int bx = int_to_x(matched_indices[i]), by = int_to_y(matched_indices[i]);
+                    int dx = bx + xmin - x, dy = by + ymin - y;
+                    is_valid[i] = dx * dx + dy * dy >= min_dist2;
+                    if (is_valid[i]) { nvalid++; if (nvalid >= K) break; }
+                }
+                if (nvalid < K) { knn *= 2; continue; }
+                /* Exact distance of each match to this patch, then sort (dist, pos, valid). */
+                for (int i = 0; i < knn; i++) {
+                    int v = matched_indices[i];
+                    matched_dists[i] = patch_dist_exact(t.b0.data(), t.w, x - xmin, y - ymin, t.b0.data(), t.w, int_to_x(v), int_to_y(v));
+                }
+                triples.resize(knn);
+                for (int i = 0; i < knn; i++) triples[i] = std::make_pair(matched_dists[i], std::make_pair(matched_indices[i], (int) is_valid[i]));
+                std::sort(triples.begin(), triples.end());
+                for (int i = 0; i < knn; i++) {
+                    matched_dists[i] = triples[i].first;
+                    matched_indices[i] = triples[i].second.first;
+                    is_valid[i] = triples[i].second.second;
+                }
+                int cv = 0;
+                for (int i = 0; i < knn; i++) {
+                    if (is_valid[i]) {
+                        size_t o = ((size_t) yk * t.kc_w + xk) * K + cv;
+                        t.kc_pos[o] = xy_to_int(int_to_x(matched_indices[i]), int_to_y(matched_indices[i]));
+                        t.kc_dist[o] = matched_dists[i];
+                        cv++;
+                        if (cv >= K) break;
+                    }
+                }
+                break;
+            }
+            prev_knn = knn;
+        }
+    }
+}
+
+/* lookup_templated<is_descriptor=0, use_allowed_patches>, patchtable.h:3468-4217. */
+double lookup(Table &t, const float *a, int ah, int aw, double *ann, const double *ann_prev,
+              const float *coh_sv) {
+    const orc_params &p = t.p;
+    vector<float> &a_wh = t.lookup_wh;
+    padded_descriptor(p, a, ah, aw, a_wh);
+    const int nd = t.nd, G = t.gnd;
+    const int awhw = aw + 7;
+    double prop_scale = 1.0 / (1 + p.coherence_spatial);
+    double temporal_scale = 1.0 / (1 + p.coherence_temporal);
+    int ann_h = ah - PW + 1, ann_w = aw - PW + 1;
+    int b0_ew = t.w - PW + 1, b0_eh = t.h - PW + 1;
+    int a_w = aw, a_h = ah, b_w = t.w, b_h = t.h;
+    bool use_allowed = !t.allowed.empty();
+    auto ANN = [&](int y, int x, int c) -> double & { return ann[((size_t) y * ann_w + x) * 3 + c]; };
+    auto dist = [&](int ax, int ay, int bx, int by) {
+        return patch_dist_exact(a, aw, ax, ay, t.b0.data(), t.w, bx, by);
+    };
+    vector<float> lookup_dist_orig;
+    if (p.init_random) {                                  /* patchtable.h:3522-3537 */
+        for (int y = 0; y < ann_h; y++)
+            for (int x = 0; x < ann_w; x++) {
+                int xs = rand() % b0_ew, ys = rand() % b0_eh;
+                ANN(y, x, 0) = xs; ANN(y, x, 1) = ys; ANN(y, x, 2) = dist(x, y, xs, ys);
+            }
+    } else if (!ann_prev) {                               /* patchtable.h:3538-3547 */
+        for (int y = 0; y < ann_h; y++)
+            for (int x = 0; x < ann_w; x++) {
+                ANN(y, x, 0) = b0_ew + 1;
+                ANN(y, x, 1) = 0;        /* left uninitialised by the reference; never read when do_table_lookup */
+                ANN(y, x, 2) = DIST_INF;
+            }
+    } else {                                              /* patchtable.h:3548-3585 */
+        lookup_dist_orig.assign((size_t) ann_h * ann_w, 0.0f);
+        for (int y = 0; y < ann_h; y++)
+            for (int x = 0; x < ann_w; x++) {
+                const double *pp = &ann_prev[((size_t) y * ann_w + x) * 3];
+                int xs = (int) pp[0], ys = (int) pp[1];
+                if (p.sanitize_input) {
+                    if (xs < 0) xs = 0; else if (xs >= b0_ew) xs = b0_ew - 1;
+                    if (ys < 0) ys = 0; else if (ys >= b0_eh) ys = b0_eh - 1;
+                }
+                ANN(y, x, 0) = xs; ANN(y, x, 1) = ys;
+                if (p.recalc_dist_temporal) {
+                    float dc = dist(x, y, xs, ys);
+                    double ts = coh_sv ? (double) coh_sv[(size_t) y * ann_w + x] : temporal_scale;
+                    float v = (float) (dc * ts);
+                    lookup_dist_orig[(size_t) y * ann_w + x] = v;
+                    ANN(y, x, 2) = v;
+                } else {
+                    ANN(y, x, 2) = pp[2] * temporal_scale;
+                }
+            }
+    }
+    const int dx_table[8] = {-1, 0, 1, -1, 1, -1, 0, 1};
+    const int dy_table[8] = {-1, -1, -1, 0, 0, 1, 1, 1};
+    bool do_rs_or_spatial = p.do_rs || p.spatial;
+    int prop_w = (p.query_step + p.prop_dist) * 2 + 1;
+    int sat_w = PW + prop_w + 1 - 1;
+    int sat_w_nopad = sat_w - 1;
+    const int pw1 = PW - 1;
+    for (int prop_iter = 0; prop_iter < p.prop_iters; prop_iter++) {
+        bool reverse = prop_iter % 2;
+        bool do_lookup = prop_iter == 0 && p.do_table_lookup;
+        bool do_kcoh = p.kcoherence > 0 && (p.kcoherence_iter < 0 || p.kcoherence_iter == prop_iter);
+        for (int y0 = 0; y0 < ann_h; y0 += p.query_step) {
+            int y = reverse ? (ann_h - 1 - y0) : y0;
+            vector<float> sat((size_t) sat_w * sat_w, 0.0f);
+            for (int x0 = 0; x0 < ann_w; x0 += p.query_step) {
+                int x = reverse ? (ann_w - 1 - x0) : x0;
+                int xbest = (int) ANN(y, x, 0);
+                int ybest = (int) ANN(y, x, 1);
+                float dbest = (float) (ANN(y, x, 2) * prop_scale);
+                if (do_lookup) {                          /* patchtable.h:3641-3709 */
+                    const float *wh_p = &a_wh[((size_t) (y + pw1) * awhw + (x + pw1)) * nd];
+                    int64_t idx = 0;
+                    for (int i = 0; i < G; i++) idx += (int64_t) t.part[i].get_bin(wh_p[i]) * t.stride[i];
+                    int v = t.table[idx];
+                    int xs = int_to_x(v) - pw1, ys = int_to_y(v) - pw1;
+                    if (xs != xbest || ys != ybest) {
+                        float dc = dist(x, y, xs, ys);
+                        if (dc < dbest) { dbest = dc; xbest = xs; ybest = ys; }
+                    }
+                }
+                if (do_kcoh) {                            /* patchtable.h:3750-3851 */
+                    int ks = p.kcoherence_step;
+                    const int32_t *kp = &t.kc_pos[((size_t) (ybest / ks) * t.kc_w + (xbest / ks)) * p.kcoherence];
+                    const float *kd = &t.kc_dist[((size_t) (ybest / ks) * t.kc_w + (xbest / ks)) * p.kcoherence];
+                    int kdx = 0, kdy = 0;
+                    if (ks > 1) { kdx = xbest % ks; kdy = ybest % ks; }
+                    for (int k = 0; k < p.kcoherence; k++) {
+                        float k_dist = kd[k];
+                        if (k_dist >= p.triangle_factor * dbest) break;
+                        int v = kp[k];
+                        int xs = int_to_x(v), ys = int_to_y(v);
+                        if (ks > 1) {
+                            xs += kdx; ys += kdy;
+                            if (xs >= b0_ew) xs = b0_ew - 1;
+                            if (ys >= b0_eh) ys = b0_eh - 1;
+                        }
+                        float dc = dist(x, y, xs, ys);
+                        if (dc < dbest) { dbest = dc; xbest = xs; ybest = ys; }
+                    }
+                }
+                if (do_rs_or_spatial) {                   /* patchtable.h:3854-3905 */
+                    if (p.spatial) {
+                        int symin = ybest - p.spatial, symax = ybest + p.spatial + 1;
+                        int sxmin = xbest - p.spatial, sxmax = xbest + p.spatial + 1;
+                        int xb0 = xbest, yb0 = ybest;
+                        if (symin < 0) symin = 0; else if (symax > b0_eh) symax = b0_eh;
+                        if (sxmin < 0) sxmin = 0; else if (sxmax > b0_ew) sxmax = b0_ew;
+                        for (int ys = symin; ys < symax; ys++)
+                            for (int xs = sxmin; xs < sxmax; xs++)
+                                if ((xs != xb0 || ys != yb0) && (!use_allowed || t.is_allowed(ys, xs))) {
+                                    float dc = dist(x, y, xs, ys);
+                                    if (dc < dbest) { dbest = dc; xbest = xs; ybest = ys; }
+                                }
+                    } else {
+                        int r = rand() & 7;
+                        int xs = xbest + dx_table[r], ys = ybest + dy_table[r];
+                        if (xs >= 0 && xs < b0_ew && ys >= 0 && ys < b0_eh && (!use_allowed || t.is_allowed(ys, xs))) {
+                            float dc = dist(x, y, xs, ys);
+                            if (dc < dbest) { dbest = dc; xbest = xs; ybest = ys; }
+                        }
+                    }
+                }
+                if (p.do_prop) {                          /* patchtable.h:3908-4145 */
+                    int ax_shift = x - p.query_step, ay_shift = y - p.query_step;
+                    int bx_shift = xbest - p.query_step, by_shift = ybest - p.query_step;
+                    int dy_min = 0, dy_max = sat_w_nopad, dx_min = 0, dx_max = sat_w_nopad;
+                    if (ax_shift + dx_min < 0) dx_min = -ax_shift;
+                    else if (ax_shift + dx_max > a_w) dx_max = a_w - ax_shift;
+                    if (ay_shift + dy_min < 0) dy_min = -ay_shift;
+                    else if (ay_shift + dy_max > a_h) dy_max = a_h - ay_shift;
+                    if (bx_shift + dx_min < 0) dx_min = -bx_shift;
+                    else if (bx_shift + dx_max > b_w) dx_max = b_w - bx_shift;
+                    if (by_shift + dy_min < 0) dy_min = -by_shift;
+                    else if (by_shift + dy_max > b_h) dy_max = b_h - by_shift;
+                    if (dx_min > 0 || dy_min > 0) {
+                        if (dx_min > 0)
+                            for (int dy = dy_min > 0 ? dy_min - 1 : dy_min; dy < dy_max; dy++) sat[(size_t) (dy + 1) * sat_w + dx_min] = 0;
+                        if (dy_min > 0)
+                            for (int dx = dx_min; dx < dx_max; dx++) sat[(size_t) dy_min * sat_w + dx + 1] = 0;
+                    }
+                    for (int dy = dy_min; dy < dy_max; dy++) {
+                        const float *a_row = a + ((size_t) (ay_shift + dy) * aw + ax_shift) * 3;
+                        const float *b_row = t.b0.data() + ((size_t) (by_shift + dy) * t.w + bx_shift) * 3;
+                        float *sat_row = &sat[(size_t) (dy + 1) * sat_w + 1];
+                        float *sat_row_prev = &sat[(size_t) dy * sat_w + 1];
+                        float row_sum = 0;
+                        for (int dx = dx_min; dx < dx_max; dx++) {
+                            const float *ap = a_row + dx * 3, *bp = b_row + dx * 3;
+                            float d0 = ap[0] - bp[0], d1 = ap[1] - bp[1], d2 = ap[2] - bp[2];
+                            row_sum += d0 * d0 + d1 * d1 + d2 * d2;
+                            sat_row[dx] = row_sum + sat_row_prev[dx];
+                        }
+                    }
+                    int dy_max_patch = dy_max - PW + 1, dx_max_patch = dx_max - PW + 1;
+                    bool missing = false;
+                    for (int dy = dy_min; dy < dy_max_patch; dy++) {
+                        const float *s1 = &sat[(size_t) dy * sat_w];
+                        const float *s2 = &sat[(size_t) (dy + PW) * sat_w];
+                        int ys = dy + by_shift;
+                        for (int dx = dx_min; dx < dx_max_patch; dx++) {
+                            int xs = dx + bx_shift;
+                            if (use_allowed && !t.is_allowed(ys, xs)) { missing = true; continue; }
+                            int dx2 = dx + PW;
+                            float dc = s1[dx] - s1[dx2] - s2[dx] + s2[dx2];
+                            double *ap = &ANN(ay_shift + dy, ax_shift + dx, 0);
+                            if (dc < ap[2]) { ap[0] = xs; ap[1] = ys; ap[2] = dc; }
+                        }
+                    }
+                    if (dx_max < sat_w_nopad || dy_max < sat_w_nopad || missing) {   /* patchtable.h:4086-4145 */
+                        int dy_start, dy_end, dx_start, dx_end;
+                        if (missing) {
+                            dx_start = 0; dx_end = p.query_step * 2;
+                            dy_start = 0; dy_end = p.query_step * 2;
+                            if (ax_shift + dx_start < 0) dx_start = -ax_shift;
+                            if (ay_shift + dy_start < 0) dy_start = -ay_shift;
+                            if (ax_shift + dx_end > ann_w) dx_end = ann_w - ax_shift;
+                            if (ay_shift + dy_end > ann_h) dy_end = ann_h - ay_shift;
+                        } else if (reverse) {
+                            dx_start = 0; dx_end = p.query_step;
+                            dy_start = 0; dy_end = p.query_step;
+                            if (ax_shift + dx_start < 0) dx_start = -ax_shift;
+                            if (ay_shift + dy_start < 0) dy_start = -ay_shift;
+                        } else {
+                            dx_start = p.query_step; dx_end = p.query_step * 2;
+                            dy_start = p.query_step; dy_end = p.query_step * 2;
+                            if (ax_shift + dx_end > ann_w) dx_end = ann_w - ax_shift;
+                            if (ay_shift + dy_end > ann_h) dy_end = ann_h - ay_shift;
+                        }
+                        for (int dy = dy_start; dy < dy_end; dy++) {
+                            int ys = ybest + (ay_shift + dy) - y;
+                            if (ys < 0) ys = 0; else if (ys >= b0_eh) ys = b0_eh - 1;
+                            for (int dx = dx_start; dx < dx_end; dx++) {
+                                double *ap = &ANN(ay_shift + dy, ax_shift + dx, 0);
+                                if (ap[2] == DIST_INF) {
+                                    int xs = xbest + (ax_shift + dx) - x;
+                                    if (xs < 0) xs = 0; else if (xs >= b0_ew) xs = b0_ew - 1;
+                                    if (use_allowed)
+                                        while (!t.is_allowed(ys, xs)) { xs = rand() % b0_ew; ys = rand() % b0_eh; }
+                                    float dc = dist(ax_shift + dx, ay_shift + dy, xs, ys);
+                                    ap[2] = dc; ap[0] = xs; ap[1] = ys;
+                                }
+                            }
+                        }
+                    }
+                } else {
+                    ANN(y, x, 0) = xbest; ANN(y, x, 1) = ybest; ANN(y, x, 2) = dbest;
+                }
+            }
+        }
+    }
+    if (ann_prev && p.coherence_temporal != 0.0) {       /* patchtable.h:4178-4193 */
+        for (int y = 0; y < ann_h; y++)
+            for (int x = 0; x < ann_w; x++) {
+                double *ap = &ANN(y, x, 0);
+                const double *pp = &ann_prev[((size_t) y * ann_w + x) * 3];
+                if (ap[0] == pp[0] && ap[1] == pp[1]) {
+                    if ((p.recalc_dist_temporal && ap[2] == lookup_dist_orig[(size_t) y * ann_w + x]) ||
+                        (!p.recalc_dist_temporal && ap[2] == pp[2] * temporal_scale))
+                        ap[2] /= temporal_scale;
+                }
+            }
+    }
+    return 0.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_srand(unsigned s) { srand(s); }
+
+void orc_rgb2yuv(const float *in, int h, int w, float *out) { rgb2yuv(in, h * w, out); }
+
+void orc_gck(const float *yuv, int h, int w, int n, int nchroma, float *out) { gck8(yuv, h, w, n, nchroma, out); }
+
+/* Padded descriptor of an RGB image: (h+7) x (w+7) x ndims. */
+void orc_descriptor(const orc_params *p, const float *rgb, int h, int w, float *out) {
+    vector<float> wh;
+    padded_descriptor(*p, rgb, h, w, wh);
+    memcpy(out, wh.data(), sizeof(float) * wh.size());
+}
+
+float orc_patch_dist(const float *a, int aw, int ax, int ay, const float *b, int bw, int bx, int by) {
+    return patch_dist_exact(a, aw, ax, ay, b, bw, bx, by);
+}
+
+void orc_scale_slices(const int *in, int n, double limit, int *out) {
+    vector<int> r = scale_slices_to_limit(vector<int>(in, in + n), limit);
+    for (int i = 0; i < n; i++) out[i] = r[i];
+}
+
+/* wh0 may be NULL (computed from b) or a (h+7) x (w+7) x ndims descriptor to build from. */
+void *orc_build(const orc_params *p, const float *b, int h, int w, const int32_t *allowed, const float *wh0) {
+    return build(*p, b, h, w, allowed, wh0);
+}
+
+void orc_free(void *t) { delete (Table *) t; }
+
+int orc_table_shape(void *tv, int *nslices, long long *ncells) {
+    Table *t = (Table *) tv;
+    for (int i = 0; i < t->gnd; i++) nslices[i] = t->nslices[i];
+    *ncells = t->ncells;
+    return t->gnd;
+}
+
+int orc_table_add_count(void *tv) { return ((Table *) tv)->table_add_count; }
+
+void orc_get_table(void *tv, int32_t *out) {
+    Table *t = (Table *) tv;
+    memcpy(out, t->table.data(), sizeof(int32_t) * t->table.size());
+}
+
+void orc_get_wh0(void *tv, float *out) {
+    Table *t = (Table *) tv;
+    memcpy(out, t->wh0.data(), sizeof(float) * t->wh0.size());
+}
+
+void orc_get_partition(void *tv, int dim, float *centers, float *lsizes, float *rsizes, int32_t *to_bin, float *mmr) {
+    Table *t = (Table *) tv;
+    const Partition1D &P = t->part[dim];
+    for (int i = 0; i < P.nslices; i++) { centers[i] = P.centers[i]; lsizes[i] = P.lsizes[i]; rsizes[i] = P.rsizes[i]; }
+    for (int i = 0; i < NMAP; i++) to_bin[i] = P.to_bin[i];
+    mmr[0] = P.min_val; mmr[1] = P.max_val; mmr[2] = P.range;
+}
+
+void orc_get_kcoherence(void *tv, int32_t *pos, float *dist) {
+    Table *t = (Table *) tv;
+    memcpy(pos, t->kc_pos.data(), sizeof(int32_t) * t->kc_pos.size());
+    memcpy(dist, t->kc_dist.data(), sizeof(float) * t->kc_dist.size());
+}
+
+/* ann_out: (ah-7) x (aw-7) x 3 doubles [x, y, dist]. ann_prev / coh_sv may be NULL. */
+void orc_lookup(void *tv, const float *a, int ah, int aw, double *ann_out, const double *ann_prev, const float *coh_sv) {
+    lookup(*(Table *) tv, a, ah, aw, ann_out, ann_prev, coh_sv);
+}
+
+}  // extern "C"

@@ -1,0 +1,1 @@
+#include "ptstub_mpl.hpp"
