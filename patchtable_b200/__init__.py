@@ -1,0 +1,275 @@
+"""patchtable_b200: B200-native PatchTable build and nearest-neighbour-field query.
+
+Python binding of the C ABI in include/patchtable_b200.h (ctypes over the in-tree
+libpatchtable_b200.so).  Names follow the reference's C++ API (patchtable/patchtable.h:4359-4491,
+patchtable/patchtable_params.h):
+
+    p = PatchTableParams("-speed 3 -coherence_spatial 4")   # PatchTableParams(argc, argv)
+    table = PatchTable(p, b)                                # PatchTable<>(&p, b, allowed)
+    ann = table.lookup(a)                                   # table.lookup(a, ann)
+
+``ann`` is a (h-7) x (w-7) x 3 float64 array [NNF_X, NNF_Y, NNF_DIST] like the reference's.
+Errors raise PatchTableError with the library's message; there is no CPU fallback: if the
+library or a GPU is missing, construction fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = ["PatchTableParams", "PatchTable", "PatchTableError", "NNF_X", "NNF_Y", "NNF_DIST", "lib",
+           "descriptor", "launch_count", "reset_launch_count"]
+
+NNF_X, NNF_Y, NNF_DIST = 0, 1, 2
+PT_MAX_DIMS = 16
+PT_PATH_MAX = 256
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpatchtable_b200.so")
+
+STATUS = {0: "PT_OK", 1: "PT_BAD_ARG", 2: "PT_OOM", 3: "PT_CUDA_ERR", 4: "PT_TIMEOUT", 5: "PT_UNSUPPORTED", 6: "PT_IO"}
+
+
+class PatchTableError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__("%s: %s" % (STATUS.get(status, status), message))
+        self.status = status
+
+
+class _Params(C.Structure):
+    """Mirror of pt_params (include/patchtable_b200.h)."""
+    _fields_ = [
+        ("limit", C.c_double),
+        ("ndims", C.c_int), ("nchroma", C.c_int), ("grid_ndims", C.c_int),
+        ("nslices", C.c_int * PT_MAX_DIMS), ("n_nslices", C.c_int),
+        ("partition_step", C.c_int),
+        ("populate_random", C.c_int), ("populate_nearest", C.c_int),
+        ("run_dt", C.c_int), ("dt_algo", C.c_int), ("dt_iters", C.c_int),
+        ("kcoherence", C.c_int), ("kcoherence_min_dist", C.c_int), ("kcoherence_step", C.c_int),
+        ("kcoherence_iter", C.c_int),
+        ("flann_reset_step", C.c_int), ("flann_build_step", C.c_int),
+        ("triangle_factor", C.c_double),
+        ("prop_iters", C.c_int), ("query_step", C.c_int), ("do_prop", C.c_int), ("prop_dist", C.c_int),
+        ("coherence_spatial", C.c_double), ("coherence_temporal", C.c_double),
+        ("do_table_lookup", C.c_int), ("do_rs", C.c_int), ("spatial", C.c_int),
+        ("allowed_index", C.c_int),
+        ("recalc_dist_temporal", C.c_int), ("sanitize_input", C.c_int), ("init_random", C.c_int),
+        ("convert_colorspace", C.c_int), ("colorspace", C.c_int),
+        ("is_descriptor", C.c_int), ("descriptor_padded", C.c_int),
+        ("patch_w", C.c_int),
+        ("threads", C.c_int), ("verbose", C.c_int), ("query_iters", C.c_int), ("ntables", C.c_int),
+        ("table_ratio", C.c_double),
+        ("lookup_algo", C.c_int), ("kcoherence_algo", C.c_int), ("dim_algo", C.c_int),
+        ("incoherence", C.c_int), ("randomize_dt", C.c_int), ("parallel_dt", C.c_int),
+        ("populate_exptime", C.c_int), ("dt_mode", C.c_int),
+        ("load_filename", C.c_char * PT_PATH_MAX),
+        ("save_filename", C.c_char * PT_PATH_MAX),
+        ("gpu_prop_passes", C.c_int),
+    ]
+
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads the native library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise PatchTableError(1, "native library %s is missing; run python -m patchtable_b200.build" % LIB_PATH)
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER(_Params)
+    vp = C.c_void_p
+    L.pt_params_default.argtypes = [P]
+    L.pt_params_default.restype = None
+    L.pt_params_set_speed.argtypes = [P, C.c_int]
+    L.pt_params_from_switches.argtypes = [P, C.c_char_p]
+    L.pt_table_create.argtypes = [P, _f32p, C.c_int, C.c_int, C.c_int, vp, C.POINTER(vp)]
+    L.pt_table_create_with_descriptor.argtypes = [P, _f32p, C.c_int, C.c_int, _f32p, vp, C.POINTER(vp)]
+    L.pt_table_free.argtypes = [vp]
+    L.pt_table_free.restype = None
+    L.pt_table_lookup.argtypes = [vp, _f32p, C.c_int, C.c_int, _f64p, vp, vp, C.POINTER(C.c_double)]
+    L.pt_table_lookup_device.argtypes = [vp, vp, C.c_int, C.c_int, vp, vp]
+    L.pt_table_shape.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int64)]
+    L.pt_table_shape.restype = C.c_int
+    L.pt_table_get_cells.argtypes = [vp, _i32p]
+    L.pt_table_get_descriptor.argtypes = [vp, _f32p]
+    L.pt_table_get_partition.argtypes = [vp, C.c_int, _f32p, _f32p, _f32p, _i32p, _f32p]
+    L.pt_table_get_kcoherence.argtypes = [vp, _i32p, _f32p]
+    L.pt_table_add_count.argtypes = [vp]
+    L.pt_table_add_count.restype = C.c_int64
+    L.pt_table_dt_levels.argtypes = [vp]
+    L.pt_descriptor.argtypes = [P, _f32p, C.c_int, C.c_int, _f32p]
+    L.pt_last_error.restype = C.c_char_p
+    L.pt_version.restype = C.c_char_p
+    L.pt_kernel_launch_count.restype = C.c_int64
+    L.pt_kernel_launch_count_reset.restype = None
+    _lib = L
+    return L
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        raise PatchTableError(status, lib().pt_last_error().decode(errors="replace"))
+
+
+class PatchTableParams:
+    """PatchTableParams (patchtable/patchtable_params.h:23-161): reference defaults (speed 3),
+    then the switches, parsed with the reference's names and semantics."""
+
+    def __init__(self, switches: str = ""):
+        object.__setattr__(self, "_p", _Params())
+        lib().pt_params_default(C.byref(self._p))
+        if switches:
+            self.set_from_switches(switches)
+
+    def set_from_switches(self, switches: str) -> None:
+        _check(lib().pt_params_from_switches(C.byref(self._p), switches.encode()))
+
+    def set_speed(self, i: int) -> None:
+        _check(lib().pt_params_set_speed(C.byref(self._p), int(i)))
+
+    @property
+    def nslices(self):
+        return [self._p.nslices[i] for i in range(self._p.n_nslices)]
+
+    def __getattr__(self, name):
+        p = object.__getattribute__(self, "_p")
+        v = getattr(p, name)
+        return v.decode() if isinstance(v, bytes) else v
+
+    def __setattr__(self, name, value):
+        if name == "nslices":
+            self._p.n_nslices = len(value)
+            for i, v in enumerate(value):
+                self._p.nslices[i] = int(v)
+            return
+        if not hasattr(self._p, name):
+            raise AttributeError(name)
+        setattr(self._p, name, value.encode() if isinstance(value, str) else value)
+
+    def as_dict(self) -> dict:
+        d = {f: getattr(self, f) for f, _ in _Params._fields_ if f not in ("nslices", "n_nslices")}
+        d["nslices"] = self.nslices
+        return d
+
+
+def _img(x, channels=3):
+    x = np.ascontiguousarray(x, np.float32)
+    if x.ndim != 3 or x.shape[2] != channels:
+        raise PatchTableError(1, "expected an H x W x %d float image, got shape %s" % (channels, x.shape))
+    return x
+
+
+class PatchTable:
+    """PatchTable<float, float, int32_t> (patchtable/patchtable.h:4359-4491) on the GPU."""
+
+    def __init__(self, params: PatchTableParams, b, allowed_patches=None, wh0=None):
+        b = _img(b)
+        self.params = params
+        self.shape_b = b.shape
+        h = C.c_void_p()
+        al = None
+        if allowed_patches is not None:
+            allowed_patches = np.ascontiguousarray(allowed_patches, np.int32)
+            if allowed_patches.shape != (b.shape[0] - 7, b.shape[1] - 7):
+                raise PatchTableError(1, "allowed_patches must be (h-7) x (w-7)")
+            al = allowed_patches.ctypes.data_as(C.c_void_p)
+        if wh0 is None:
+            _check(lib().pt_table_create(C.byref(params._p), b, b.shape[0], b.shape[1], 3, al, C.byref(h)))
+        else:
+            wh0 = np.ascontiguousarray(wh0, np.float32)
+            _check(lib().pt_table_create_with_descriptor(C.byref(params._p), b, b.shape[0], b.shape[1], wh0, al, C.byref(h)))
+        self._h = h
+        self.last_seconds = 0.0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            lib().pt_table_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def lookup(self, a, ann_prev=None, coherence_temporal_sv=None):
+        """PatchTable::lookup (patchtable.h:4448): returns the NNF; the wall time of the call
+        (including a's descriptor, like the reference's return value) is in self.last_seconds."""
+        a = _img(a)
+        ann = np.empty((a.shape[0] - 7, a.shape[1] - 7, 3), np.float64)
+        secs = C.c_double()
+        prev = None if ann_prev is None else np.ascontiguousarray(ann_prev, np.float64).ctypes.data_as(C.c_void_p)
+        sv = None if coherence_temporal_sv is None else np.ascontiguousarray(coherence_temporal_sv, np.float32).ctypes.data_as(C.c_void_p)
+        _check(lib().pt_table_lookup(self._h, a, a.shape[0], a.shape[1], ann, prev, sv, C.byref(secs)))
+        self.last_seconds = secs.value
+        return ann
+
+    def lookup_device(self, a_ptr: int, h: int, w: int, ann_ptr: int, stream: int = 0) -> None:
+        """Device-resident lookup: a_ptr / ann_ptr are device addresses (e.g. torch data_ptr())."""
+        _check(lib().pt_table_lookup_device(self._h, C.c_void_p(a_ptr), h, w, C.c_void_p(ann_ptr), C.c_void_p(stream)))
+
+    # -- introspection for parity tests --------------------------------------------------------
+    def shape(self):
+        ns = (C.c_int * PT_MAX_DIMS)()
+        nc = C.c_int64()
+        g = lib().pt_table_shape(self._h, ns, C.byref(nc))
+        return [ns[i] for i in range(g)], nc.value
+
+    def table(self):
+        _, nc = self.shape()
+        out = np.empty(nc, np.int32)
+        _check(lib().pt_table_get_cells(self._h, out))
+        return out
+
+    def descriptor(self):
+        H, W, _ = self.shape_b
+        out = np.empty((H - 7, W - 7, self.params.ndims), np.float32)
+        _check(lib().pt_table_get_descriptor(self._h, out))
+        return out
+
+    def partition(self, dim):
+        ns, _ = self.shape()
+        n = ns[dim]
+        c, l, r = (np.empty(n, np.float32) for _ in range(3))
+        tb = np.empty(16384, np.int32)
+        mmr = np.empty(3, np.float32)
+        _check(lib().pt_table_get_partition(self._h, dim, c, l, r, tb, mmr))
+        return dict(centers=c, lsizes=l, rsizes=r, to_bin=tb, min=mmr[0], max=mmr[1], range=mmr[2])
+
+    def kcoherence(self):
+        H, W, _ = self.shape_b
+        k = self.params.kcoherence
+        pos = np.empty((H - 7) * (W - 7) * k, np.int32)
+        dist = np.empty((H - 7) * (W - 7) * k, np.float32)
+        _check(lib().pt_table_get_kcoherence(self._h, pos, dist))
+        return pos.reshape(H - 7, W - 7, k), dist.reshape(H - 7, W - 7, k)
+
+    def add_count(self) -> int:
+        return int(lib().pt_table_add_count(self._h))
+
+    def dt_levels(self) -> int:
+        return int(lib().pt_table_dt_levels(self._h))
+
+
+def descriptor(params: PatchTableParams, img):
+    """Descriptor of every 8x8 patch of an RGB image, (h-7) x (w-7) x ndims."""
+    img = _img(img)
+    out = np.empty((img.shape[0] - 7, img.shape[1] - 7, params.ndims), np.float32)
+    _check(lib().pt_descriptor(C.byref(params._p), img, img.shape[0], img.shape[1], out))
+    return out
+
+
+def launch_count() -> int:
+    return int(lib().pt_kernel_launch_count())
+
+
+def reset_launch_count() -> None:
+    lib().pt_kernel_launch_count_reset()

@@ -1,0 +1,172 @@
+/* Patch descriptor kernel: RGB -> (RGBA copy, YUV, Walsh-Hadamard projections of every 8x8 patch).
+
+   Replaces get_padded_descriptor (patchtable/patchtable.h:2492-2546): ARRAY_RGB2YUV
+   (solver/array.h:1116-1127) followed by gck_8 (patchtable/gck.h:29-1950).  The reference
+   evaluates the projections with running sums along rows and columns; this kernel computes each
+   patch's projections directly from a shared-memory tile, so there is no sequential dependency
+   and every output is an independent 8-term sum per pass.  Values agree with the reference to
+   float rounding (the reference's running sums drift along long rows).
+
+   One CTA owns a 64 x 8 block of patches.  It loads the (8+7) x (64+7) pixel region once with
+   coalesced loads, converts it to YUV in double precision exactly as the reference does (double
+   constants, left-to-right sum, rounded to float), applies each needed horizontal sign vector
+   per row, then each vertical sign vector per patch, and writes the descriptor as ndims floats
+   padded to a 32- or 64-byte record.  The same pass writes the RGBA (float4) copy of the image
+   used by the distance kernels. */
+#include <cuda_runtime.h>
+#include <cstdio>
+
+#include "pt_internal.h"
+#include "wh_tables.h"
+#include "pt_kernels.h"
+
+namespace {
+
+constexpr int TW = 64, TH = 8;            /* patches per CTA */
+constexpr int RW = TW + 7, RH = TH + 7;   /* pixel region per CTA */
+constexpr int RWP = RW + 1;               /* padded smem row */
+constexpr int NT = 256;
+
+struct DescPlan {
+    int nd;                               /* output channels */
+    int ncombo;                           /* distinct (plane, horizontal vector) filters */
+    int combo_plane[PT_DESC_MAX];
+    signed char combo_h[PT_DESC_MAX][8];
+    int ch_combo[PT_DESC_MAX];
+    signed char ch_v[PT_DESC_MAX][8];
+};
+
+
+__device__ __forceinline__ void yuv_exact(float R, float G, float B, float &Y, float &U, float &V) {
+    /* ARRAY_RGB2YUV, solver/array.h:1124-1126: double constants x float pixels, summed left to
+       right in double, stored as float.  Explicit _rn intrinsics keep the compiler from fusing. */
+    double r = R, g = G, b = B;
+    Y = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.299, r), __dmul_rn(0.587, g)), __dmul_rn(0.114, b)));
+    U = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(-0.14713, r), __dmul_rn(-0.28886, g)), __dmul_rn(0.436, b)));
+    V = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.615, r), __dmul_rn(-0.51499, g)), __dmul_rn(-0.10001, b)));
+}
+
+__global__ void __launch_bounds__(NT)
+k_descriptor(const DescPlan c_plan, const float *__restrict__ rgb, int h, int w, int convert,
+             float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh, int ew) {
+    extern __shared__ float smem[];
+    float *pix = smem;                               /* 3 planes x RH x RWP */
+    float *hs = smem + 3 * RH * RWP;                 /* ncombo x RH x TW */
+    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+    const int tid = threadIdx.x;
+    const bool last_col = x0 + TW >= ew, last_row = y0 + TH >= eh;
+    const int own_x1 = last_col ? w : x0 + TW, own_y1 = last_row ? h : y0 + TH;
+
+    for (int i = tid; i < RH * RW; i += NT) {
+        int r = i / RW, c = i % RW;
+        int gy = y0 + r, gx = x0 + c;
+        float R = 0.f, G = 0.f, B = 0.f;
+        if (gy < h && gx < w) {
+            const float *p = rgb + ((size_t) gy * w + gx) * 3;
+            R = __ldg(p); G = __ldg(p + 1); B = __ldg(p + 2);
+            if (rgba && gy < own_y1 && gx < own_x1) rgba[(size_t) gy * w + gx] = make_float4(R, G, B, 0.f);
+        }
+        float Y = R, U = G, V = B;
+        if (convert) yuv_exact(R, G, B, Y, U, V);
+        pix[(0 * RH + r) * RWP + c] = Y;
+        pix[(1 * RH + r) * RWP + c] = U;
+        pix[(2 * RH + r) * RWP + c] = V;
+    }
+    __syncthreads();
+
+    const int ncombo = c_plan.ncombo;
+    for (int i = tid; i < ncombo * RH * TW; i += NT) {
+        int m = i / (RH * TW), rem = i % (RH * TW), r = rem / TW, j = rem % TW;
+        const float *row = pix + (c_plan.combo_plane[m] * RH + r) * RWP + j;
+        float s = 0.f;
+#pragma unroll
+        for (int b = 0; b < 8; b++) s = c_plan.combo_h[m][b] > 0 ? __fadd_rn(s, row[b]) : __fsub_rn(s, row[b]);
+        hs[(m * RH + r) * TW + j] = s;
+    }
+    __syncthreads();
+
+    const int nd = c_plan.nd;
+    for (int i = tid; i < TW * TH; i += NT) {
+        int pi = i / TW, pj = i % TW;
+        int py = y0 + pi, px = x0 + pj;
+        if (py >= eh || px >= ew || desc == nullptr) continue;
+        float out[PT_DESC_MAX];
+#pragma unroll
+        for (int c = 0; c < PT_DESC_MAX; c++) {
+            if (c < nd) {
+                const float *col = hs + (c_plan.ch_combo[c] * RH + pi) * TW + pj;
+                float s = 0.f;
+#pragma unroll
+                for (int a = 0; a < 8; a++) s = c_plan.ch_v[c][a] > 0 ? __fadd_rn(s, col[a * TW]) : __fsub_rn(s, col[a * TW]);
+                out[c] = s;
+            } else {
+                out[c] = 0.f;
+            }
+        }
+        float4 *dst = reinterpret_cast<float4 *>(desc + ((size_t) py * ew + px) * ds);
+        for (int q = 0; q < ds / 4; q++) dst[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
+    }
+}
+
+}  // namespace
+
+/* Builds the per-channel plan for n = ndims - 2*nchroma kernels (gck.h channel map,
+   gck.py:386-389): kernel k < nchroma has Y, U, V channels at 3k..3k+2, the others one Y
+   channel at 3*nchroma + (k - nchroma). */
+static pt_status make_plan(int ndims, int nchroma, DescPlan &plan) {
+    int n = ndims - 2 * nchroma;
+    if (ndims < 1 || ndims > PT_DESC_MAX || nchroma < 0 || nchroma > 3 || n < 1 || n > 64 || n < nchroma)
+        return pt_fail(PT_UNSUPPORTED, "descriptor: ndims=%d nchroma=%d not supported on the GPU path (ndims <= %d)",
+                       ndims, nchroma, PT_DESC_MAX);
+    memset(&plan, 0, sizeof(plan));
+    plan.nd = ndims;
+    auto combo_of = [&](int plane, int k) {
+        for (int m = 0; m < plan.ncombo; m++) {
+            bool same = plan.combo_plane[m] == plane;
+            for (int b = 0; b < 8 && same; b++) same = plan.combo_h[m][b] == PT_WH_H[k][b];
+            if (same) return m;
+        }
+        int m = plan.ncombo++;
+        plan.combo_plane[m] = plane;
+        for (int b = 0; b < 8; b++) plan.combo_h[m][b] = PT_WH_H[k][b];
+        return m;
+    };
+    for (int k = 0; k < n; k++) {
+        int nc = k < nchroma ? 3 : 1;
+        int c0 = k < nchroma ? 3 * k : 3 * nchroma + (k - nchroma);
+        for (int c = 0; c < nc; c++) {
+            int ch = c0 + c;
+            plan.ch_combo[ch] = combo_of(c, k);
+            for (int a = 0; a < 8; a++) plan.ch_v[ch][a] = PT_WH_V[k][a];
+        }
+    }
+    return PT_OK;
+}
+
+pt_status pt_descriptor_check(int ndims, int nchroma) {
+    DescPlan plan;
+    return make_plan(ndims, nchroma, plan);
+}
+
+size_t pt_descriptor_smem(int ndims) {
+    (void) ndims;
+    return sizeof(float) * (3 * RH * RWP + PT_DESC_MAX * RH * TW);
+}
+
+pt_status pt_launch_descriptor(int ndims, int nchroma, const float *rgb, int h, int w, int convert, float4 *rgba,
+                               float *desc, int ds, cudaStream_t st) {
+    int eh = h - 7, ew = w - 7;
+    DescPlan plan;
+    PT_TRY(make_plan(ndims, nchroma, plan));
+    if (eh < 1 || ew < 1) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    static bool attr = false;
+    size_t smem = pt_descriptor_smem(0);
+    if (!attr) {
+        PT_CUDA(cudaFuncSetAttribute(k_descriptor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        attr = true;
+    }
+    dim3 grid((ew + TW - 1) / TW, (eh + TH - 1) / TH);
+    k_descriptor<<<grid, NT, smem, st>>>(plan, rgb, h, w, convert, rgba, desc, ds, eh, ew);
+    PT_LAUNCHED();
+    return PT_OK;
+}

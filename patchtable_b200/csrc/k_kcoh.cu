@@ -1,0 +1,320 @@
+/* k-coherence set of the table image (patchtable/patchtable.h:2653-2869, FLANN path with
+   TABLE_KCOHERENCE_TRIANGLE).
+
+   For every query patch of b the reference asks for its knn nearest patches in descriptor space,
+   marks a neighbour valid when it lies at least kcoherence_min_dist pixels away, doubles knn until
+   `kcoherence` valid neighbours exist, re-sorts the knn matches by exact 8x8x3 distance and keeps
+   the first `kcoherence` valid ones.  Two details of that loop carry state from patch to patch:
+     * knn starts from the previous patch's final knn unless x is a multiple of flann_reset_step
+       (patchtable.h:2714), so knn is a running maximum over segments of the raster order;
+     * the validity loop stops at the kcoherence-th valid match, so the flags past that point keep
+       the values the previous patch left in the vector (after its exact-distance sort), and those
+       stale flags take part in the final selection (patchtable.h:2793-2856).
+   The kernels below reproduce both: one thread walks each segment in order, carrying the flag
+   vector; the only state that crosses a segment boundary is one flag bit, which is resolved by a
+   scan over segments after each segment has been evaluated for both values of that bit.
+
+   The nearest-neighbour search is exact, ranked by (float squared L2 summed in dimension order
+   without fused operations, point index); FLANN's approximate tree is not reproduced. */
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include "pt_internal.h"
+#include "pt_kernels.h"
+
+namespace {
+
+constexpr int NT = 128;
+
+/* Squared descriptor distance in the ranking's order. */
+__device__ __forceinline__ float knn_dist(const float *q, const float *p, int nd) {
+    float s = 0.f;
+    for (int i = 0; i < nd; i++) {
+        float t = __fsub_rn(q[i], p[i]);
+        s = __fadd_rn(s, __fmul_rn(t, t));
+    }
+    return s;
+}
+
+/* Exact top-K by (dist, index) of every query among all train points; brute force over tiles
+   of train points staged in shared memory, visited in increasing index order. */
+template<int K>
+__global__ void __launch_bounds__(NT)
+k_knn_brute(const float *__restrict__ train, int N, int nd, const float *__restrict__ qdesc, int Q, int *out) {
+    constexpr int TILE = 512;
+    __shared__ float tp[TILE * PT_DESC_MAX];
+    int q = blockIdx.x * NT + threadIdx.x;
+    float qv[PT_DESC_MAX];
+    float kd[K];
+    int ki[K];
+#pragma unroll
+    for (int t = 0; t < K; t++) { kd[t] = __int_as_float(0x7f800000); ki[t] = -1; }
+    if (q < Q)
+        for (int i = 0; i < nd; i++) qv[i] = qdesc[(size_t) q * nd + i];
+    for (int base = 0; base < N; base += TILE) {
+        int cnt = min(TILE, N - base);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cnt * nd; i += NT) tp[i] = train[(size_t) base * nd + i];
+        __syncthreads();
+        if (q >= Q) continue;
+        for (int j = 0; j < cnt; j++) {
+            float d = knn_dist(qv, tp + j * nd, nd);
+            if (d < kd[K - 1]) {
+                int idx = base + j;
+#pragma unroll
+                for (int t = K - 1; t >= 0; t--) {
+                    if (kd[t] > d) {
+                        if (t > 0 && kd[t - 1] > d) { kd[t] = kd[t - 1]; ki[t] = ki[t - 1]; }
+                        else { kd[t] = d; ki[t] = idx; }
+                    }
+                }
+            }
+        }
+    }
+    if (q < Q)
+        for (int t = 0; t < K; t++) out[(size_t) q * K + t] = ki[t];
+}
+
+/* Copies descriptor rows (ds-strided records) of the listed patches into a compact n x nd array. */
+__global__ void k_gather_rows(const float *__restrict__ desc, int ds, int nd, const int *__restrict__ rows, int n,
+                              float *out) {
+    long long t = blockIdx.x * 256ll + threadIdx.x;
+    if (t >= (long long) n * nd) return;
+    int i = (int) (t / nd), d = (int) (t % nd);
+    out[t] = desc[(size_t) rows[i] * ds + d];
+}
+
+/* Validity bits of each query's sorted neighbour list and m = the smallest knn0 * 2^j whose
+   prefix holds `kc` valid neighbours (0 when the list of Kc entries is too short). */
+__global__ void k_kc_valid(const int *__restrict__ nbr, int Kc, int Q, const int *__restrict__ qpos,
+                           const int *__restrict__ tpos, int min_dist2, int kc, int knn0,
+                           unsigned long long *valid, int *m_out) {
+    int q = blockIdx.x * 256 + threadIdx.x;
+    if (q >= Q) return;
+    int qx = pt_x(qpos[q]), qy = pt_y(qpos[q]);
+    unsigned long long bits = 0;
+    for (int j = 0; j < Kc && j < 64; j++) {
+        int v = tpos[nbr[(size_t) q * Kc + j]];
+        int dx = pt_x(v) - qx, dy = pt_y(v) - qy;
+        if (dx * dx + dy * dy >= min_dist2) bits |= 1ull << j;
+    }
+    valid[q] = bits;
+    int m = 0;
+    for (int k = knn0; k <= Kc; k *= 2) {
+        unsigned long long mask = k >= 64 ? ~0ull : ((1ull << k) - 1);
+        if (__popcll(bits & mask) >= kc) { m = k; break; }
+    }
+    m_out[q] = m;
+}
+
+/* Final knn of every query: running maximum of m over each segment, restarting at knn0. */
+__global__ void k_kc_chain(const int *__restrict__ seg_start, int nseg, int Q, const int *__restrict__ m,
+                           int knn0, int Kc, int *knn, int *overflow) {
+    int s = blockIdx.x * 256 + threadIdx.x;
+    if (s >= nseg) return;
+    int q0 = seg_start[s], q1 = (s + 1 < nseg) ? seg_start[s + 1] : Q;
+    int cur = knn0;
+    for (int q = q0; q < q1; q++) {
+        int mq = m[q];
+        if (mq == 0) { atomicExch(overflow, 1); mq = Kc; }
+        cur = max(cur, mq);
+        if (cur > Kc) atomicExch(overflow, 1);
+        knn[q] = min(cur, Kc);
+    }
+}
+
+/* patch_dist_exact<float,8,3> (patchtable.h:330-373): four lane sums over 8 rows of 24
+   interleaved RGB floats, lane q taking float indices q, q+4, ..., q+20 of each row in order,
+   lanes added 0+1+2+3 at the end.  Inputs are RGBA images. */
+__device__ __forceinline__ float ssd_exact(const float4 *__restrict__ A, int aw, int ax, int ay,
+                                           const float4 *__restrict__ B, int bw, int bx, int by) {
+    float l0 = 0.f, l1 = 0.f, l2 = 0.f, l3 = 0.f;
+#pragma unroll 2
+    for (int dy = 0; dy < 8; dy++) {
+        const float4 *ar = A + (size_t) (ay + dy) * aw + ax;
+        const float4 *br = B + (size_t) (by + dy) * bw + bx;
+        float e[24];
+#pragma unroll
+        for (int p = 0; p < 8; p++) {
+            float4 a = __ldg(ar + p), b = __ldg(br + p);
+            float t0 = __fsub_rn(a.x, b.x), t1 = __fsub_rn(a.y, b.y), t2 = __fsub_rn(a.z, b.z);
+            e[3 * p] = __fmul_rn(t0, t0); e[3 * p + 1] = __fmul_rn(t1, t1); e[3 * p + 2] = __fmul_rn(t2, t2);
+        }
+#pragma unroll
+        for (int n = 0; n < 6; n++) {
+            l0 = __fadd_rn(l0, e[4 * n]); l1 = __fadd_rn(l1, e[4 * n + 1]);
+            l2 = __fadd_rn(l2, e[4 * n + 2]); l3 = __fadd_rn(l3, e[4 * n + 3]);
+        }
+    }
+    return __fadd_rn(__fadd_rn(__fadd_rn(l0, l1), l2), l3);
+}
+
+/* Exact distance from each query patch to its first knn neighbours. */
+__global__ void k_kc_ssd(const float4 *__restrict__ b, int bw, const int *__restrict__ nbr, int Kc, int Q,
+                         const int *__restrict__ qpos, const int *__restrict__ tpos, const int *__restrict__ knn,
+                         float *ssd) {
+    long long t = blockIdx.x * 256ll + threadIdx.x;
+    int q = (int) (t / Kc), j = (int) (t % Kc);
+    if (q >= Q || j >= knn[q]) return;
+    int v = tpos[nbr[(size_t) q * Kc + j]];
+    ssd[(size_t) q * Kc + j] = ssd_exact(b, bw, pt_x(qpos[q]), pt_y(qpos[q]), b, bw, pt_x(v), pt_y(v));
+}
+
+/* The sequential selection of one segment with incoming stale bit `bin` (the flag at index
+   kc after the knn0 truncation).  Writes the kept (position, distance) pairs; returns the
+   outgoing bit. */
+__device__ int select_segment(int q0, int q1, int bin, int kc, int knn0, int Kc, const int *__restrict__ nbr,
+                              const int *__restrict__ tpos, const unsigned long long *__restrict__ valid,
+                              const int *__restrict__ knn, const float *__restrict__ ssd, int2 *outp) {
+    unsigned long long F = bin ? (1ull << kc) : 0ull;   /* flags entering the first patch */
+    int S = knn0;
+    float sd[64];
+    int sp[64], so[64];
+    for (int q = q0; q < q1; q++) {
+        int kq = knn[q];
+        unsigned long long vb = valid[q];
+        /* fresh flags up to and including the kc-th valid neighbour */
+        int r = 0, nv = 0;
+        while (r < kq) { if ((vb >> r) & 1ull) nv++; r++; if (nv >= kc) break; }
+        unsigned long long fresh = r >= 64 ? vb : (vb & ((1ull << r) - 1));
+        unsigned long long keep = (S >= 64) ? ~0ull : ((1ull << S) - 1);
+        unsigned long long stale = F & keep & ~(r >= 64 ? ~0ull : ((1ull << r) - 1));
+        unsigned long long flags = fresh | stale;
+        /* sort (ssd, pos, flag) ascending; positions are distinct */
+        for (int j = 0; j < kq; j++) {
+            float d = ssd[(size_t) q * Kc + j];
+            int p = tpos[nbr[(size_t) q * Kc + j]];
+            int t = j;
+            while (t > 0 && (sd[t - 1] > d || (sd[t - 1] == d && sp[t - 1] > p))) {
+                sd[t] = sd[t - 1]; sp[t] = sp[t - 1]; so[t] = so[t - 1]; t--;
+            }
+            sd[t] = d; sp[t] = p; so[t] = j;
+        }
+        unsigned long long nf = 0;
+        int cv = 0;
+        for (int t = 0; t < kq; t++) {
+            int f = (int) ((flags >> so[t]) & 1ull);
+            if (f) nf |= 1ull << t;
+            if (f && cv < kc) { outp[(size_t) q * kc + cv] = make_int2(sp[t], __float_as_int(sd[t])); cv++; }
+        }
+        F = nf;
+        S = kq;
+    }
+    (void) Kc;
+    return (int) ((F >> kc) & 1ull);
+}
+
+__global__ void k_kc_select(const int *__restrict__ seg_start, int nseg, int Q, int kc, int knn0, int Kc,
+                            const int *__restrict__ nbr, const int *__restrict__ tpos,
+                            const unsigned long long *__restrict__ valid, const int *__restrict__ knn,
+                            const float *__restrict__ ssd, int2 *out0, int2 *out1, unsigned char *fn) {
+    int s = blockIdx.x * 64 + threadIdx.x;
+    if (s >= nseg) return;
+    int q0 = seg_start[s], q1 = (s + 1 < nseg) ? seg_start[s + 1] : Q;
+    int b0 = select_segment(q0, q1, 0, kc, knn0, Kc, nbr, tpos, valid, knn, ssd, out0);
+    int b1 = select_segment(q0, q1, 1, kc, knn0, Kc, nbr, tpos, valid, knn, ssd, out1);
+    fn[s] = (unsigned char) (b0 | (b1 << 1));   /* the segment's map of the carried bit */
+}
+
+/* Composition of bit maps f encoded as (f(0) | f(1) << 1): apply a, then b. */
+struct ComposeOp {
+    __device__ unsigned char operator()(unsigned char a, unsigned char b) const {
+        int a0 = a & 1, a1 = (a >> 1) & 1;
+        int r0 = (b >> a0) & 1, r1 = (b >> a1) & 1;
+        return (unsigned char) (r0 | (r1 << 1));
+    }
+};
+
+/* Picks each segment's scenario given the carried bit (the composed map of all earlier segments
+   applied to the initial 0) and writes the k-coherence set. */
+__global__ void k_kc_finish(const int *__restrict__ seg_start, int nseg, int Q, int kc,
+                            const unsigned char *__restrict__ prefix, const int2 *__restrict__ out0,
+                            const int2 *__restrict__ out1, const int *__restrict__ qcell, int2 *kcoh) {
+    int s = blockIdx.x * 256 + threadIdx.x;
+    if (s >= nseg) return;
+    int bin = s == 0 ? 0 : (prefix[s - 1] & 1);
+    const int2 *src = bin ? out1 : out0;
+    int q0 = seg_start[s], q1 = (s + 1 < nseg) ? seg_start[s + 1] : Q;
+    for (int q = q0; q < q1; q++)
+        for (int k = 0; k < kc; k++) kcoh[(size_t) qcell[q] * kc + k] = src[(size_t) q * kc + k];
+}
+
+}  // namespace
+
+/* train: N x nd compact descriptors (row order = FLANN index order); tpos: packed positions
+   (patch coords) of the train points.  Queries are train rows qrow[q] at positions qpos[q], in
+   the reference's loop order, with output cell qcell[q] (index into the beh x bew grid).
+   seg_start: first query of each segment.  kcoh receives beh x bew x kc (pos, dist bits). */
+pt_status pt_gather_rows(const float *desc, int ds, int nd, const int *rows, int n, float *out, cudaStream_t st) {
+    long long tot = (long long) n * nd;
+    k_gather_rows<<<(unsigned) ((tot + 255) / 256), 256, 0, st>>>(desc, ds, nd, rows, n, out);
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *train, int N, int nd, const int *tpos,
+                        const float *qdesc, const int *qpos, const int *qcell, int Q, const int *seg_start, int nseg,
+                        int kc, int min_dist, int2 *kcoh, int *max_knn_out, cudaStream_t st) {
+    if (kc < 1 || kc >= 32) return pt_fail(PT_UNSUPPORTED, "kcoherence must be in 1..31");
+    int knn0 = kc + 1;
+    int Kc = 16;
+    while (Kc < 2 * knn0) Kc *= 2;
+    for (;;) {
+        if (Kc > 64) return pt_fail(PT_UNSUPPORTED, "k-coherence needs more than 64 neighbours for some patch");
+        if (Kc > N) return pt_fail(PT_BAD_ARG, "k-coherence: image has too few patches (%d)", N);
+        DevBuf<int> nbr, mm, knn, ovf;
+        DevBuf<unsigned long long> valid;
+        DevBuf<float> ssd;
+        PT_CUDA(nbr.reserve((size_t) Q * Kc));
+        PT_CUDA(mm.reserve(Q));
+        PT_CUDA(knn.reserve(Q));
+        PT_CUDA(ovf.reserve(1));
+        PT_CUDA(valid.reserve(Q));
+        PT_CUDA(ssd.reserve((size_t) Q * Kc));
+        PT_TRY(pt_launch_knn(train, N, nd, qdesc, Q, Kc, nbr.p, st));
+        k_kc_valid<<<(Q + 255) / 256, 256, 0, st>>>(nbr.p, Kc, Q, qpos, tpos, min_dist * min_dist, kc, knn0, valid.p, mm.p);
+        PT_LAUNCHED();
+        PT_CUDA(cudaMemsetAsync(ovf.p, 0, sizeof(int), st));
+        k_kc_chain<<<(nseg + 255) / 256, 256, 0, st>>>(seg_start, nseg, Q, mm.p, knn0, Kc, knn.p, ovf.p);
+        PT_LAUNCHED();
+        int overflow = 0;
+        PT_CUDA(cudaMemcpyAsync(&overflow, ovf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PT_CUDA(cudaStreamSynchronize(st));
+        if (overflow) { Kc *= 2; continue; }
+        long long tot = (long long) Q * Kc;
+        k_kc_ssd<<<(unsigned) ((tot + 255) / 256), 256, 0, st>>>(b_rgba, bw, nbr.p, Kc, Q, qpos, tpos, knn.p, ssd.p);
+        PT_LAUNCHED();
+        DevBuf<int2> o0, o1;
+        DevBuf<unsigned char> fn, pre;
+        PT_CUDA(o0.reserve((size_t) Q * kc));
+        PT_CUDA(o1.reserve((size_t) Q * kc));
+        PT_CUDA(fn.reserve(nseg));
+        PT_CUDA(pre.reserve(nseg));
+        k_kc_select<<<(nseg + 63) / 64, 64, 0, st>>>(seg_start, nseg, Q, kc, knn0, Kc, nbr.p, tpos, valid.p, knn.p,
+                                                    ssd.p, o0.p, o1.p, fn.p);
+        PT_LAUNCHED();
+        size_t tb = 0;
+        PT_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tb, fn.p, pre.p, ComposeOp(), nseg, st));
+        DevBuf<unsigned char> tmp;
+        PT_CUDA(tmp.reserve(tb));
+        PT_CUDA(cub::DeviceScan::InclusiveScan(tmp.p, tb, fn.p, pre.p, ComposeOp(), nseg, st));
+        pt_count_launches(1);
+        k_kc_finish<<<(nseg + 255) / 256, 256, 0, st>>>(seg_start, nseg, Q, kc, pre.p, o0.p, o1.p, qcell, kcoh);
+        PT_LAUNCHED();
+        if (max_knn_out) *max_knn_out = Kc;
+        PT_CUDA(cudaStreamSynchronize(st));
+        return PT_OK;
+    }
+}
+
+pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, int Q, int K, int *out, cudaStream_t st) {
+    dim3 grid((Q + NT - 1) / NT);
+    switch (K) {
+        case 16: k_knn_brute<16><<<grid, NT, 0, st>>>(train, N, nd, qdesc, Q, out); break;
+        case 32: k_knn_brute<32><<<grid, NT, 0, st>>>(train, N, nd, qdesc, Q, out); break;
+        case 64: k_knn_brute<64><<<grid, NT, 0, st>>>(train, N, nd, qdesc, Q, out); break;
+        default: return pt_fail(PT_UNSUPPORTED, "knn K=%d", K);
+    }
+    PT_LAUNCHED();
+    return PT_OK;
+}

@@ -1,0 +1,211 @@
+/* Query kernels: nearest-neighbour field from image a to the table image b.
+
+   Replaces lookup_templated<0,0> (patchtable/patchtable.h:3468-4217).  The reference sweeps the
+   patches in scanline order (reversed on odd iterations); at each patch it
+     1. starts from the stored match with its distance scaled by prop_scale = 1/(1+coherence_spatial),
+     2. tries the table cell of the patch's descriptor on the first iteration (:3641-3709),
+     3. tries the k-coherence neighbours of the current best, stopping once the stored
+        distance of a neighbour reaches triangle_factor * best (:3750-3851),
+     4. pushes the chosen offset to the 3x3 neighbourhood, replacing a neighbour's match when the
+        pushed patch is closer (summed-area-table propagation, :3908-4145).
+   Here every patch runs steps 1-3 at once ("choose"), then every patch takes the best of the
+   offsets its neighbours chose ("pull", the mirror image of the push), and the pair of phases
+   repeats for a fixed number of passes.  All distances are the reference's patch_dist_exact
+   (patchtable.h:330-373) evaluated in the same float order, so every returned NNF_DIST is that
+   function's value for the returned match; a candidate's sum stops early once its partial sum
+   already reaches the value it must beat (the partial sum can only grow). */
+#include <cuda_runtime.h>
+
+#include "pt_internal.h"
+#include "pt_kernels.h"
+
+namespace {
+
+constexpr int NT = 256;
+
+struct QPlan {
+    int aw, ah;              /* a image size (pixels) */
+    int ew, eh;              /* a patches */
+    int bw, bh;              /* b image size */
+    int bew, beh;            /* b patches */
+    double prop_scale;
+    double triangle;
+    int kc, ks;              /* kcoherence, kcoherence_step */
+    int radius;              /* query_step + prop_dist */
+    int do_kcoh;
+};
+
+__device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
+
+/* patch_dist_exact in the reference's order, abandoning the sum (returning +inf) as soon as the
+   running total reaches `bound`. */
+__device__ __forceinline__ float ssd_bounded(const float4 *__restrict__ A, int aw, int ax, int ay,
+                                             const float4 *__restrict__ B, int bw, int bx, int by, float bound) {
+    float l0 = 0.f, l1 = 0.f, l2 = 0.f, l3 = 0.f;
+    for (int dy = 0; dy < 8; dy++) {
+        const float4 *ar = A + (size_t) (ay + dy) * aw + ax;
+        const float4 *br = B + (size_t) (by + dy) * bw + bx;
+        float e[24];
+#pragma unroll
+        for (int p = 0; p < 8; p++) {
+            float4 a = __ldg(ar + p), b = __ldg(br + p);
+            float t0 = __fsub_rn(a.x, b.x), t1 = __fsub_rn(a.y, b.y), t2 = __fsub_rn(a.z, b.z);
+            e[3 * p] = __fmul_rn(t0, t0); e[3 * p + 1] = __fmul_rn(t1, t1); e[3 * p + 2] = __fmul_rn(t2, t2);
+        }
+#pragma unroll
+        for (int n = 0; n < 6; n++) {
+            l0 = __fadd_rn(l0, e[4 * n]); l1 = __fadd_rn(l1, e[4 * n + 1]);
+            l2 = __fadd_rn(l2, e[4 * n + 2]); l3 = __fadd_rn(l3, e[4 * n + 3]);
+        }
+        if (dy < 7 && __fadd_rn(__fadd_rn(__fadd_rn(l0, l1), l2), l3) >= bound) return finf();
+    }
+    return __fadd_rn(__fadd_rn(__fadd_rn(l0, l1), l2), l3);
+}
+
+/* Steps 1-3 for every patch: returns the chosen match and its exact distance. */
+__global__ void __launch_bounds__(NT)
+k_choose(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
+         const float *__restrict__ cur_d, const long long *__restrict__ cells, const int *__restrict__ table,
+         const int2 *__restrict__ kcoh, int do_table, int *ch_pos, float *ch_d, unsigned *evals) {
+    int p = blockIdx.x * NT + threadIdx.x;
+    if (p >= c_q.ew * c_q.eh) return;
+    int x = p % c_q.ew, y = p / c_q.ew;
+    int pos = cur_pos[p];
+    float dstore = cur_d[p];
+    int xb = pt_x(pos), yb = pt_y(pos);
+    float dbest = (float) ((double) dstore * c_q.prop_scale);
+    float dch = dstore;          /* exact distance of the chosen match */
+    unsigned ne = 0;
+    if (do_table) {
+        int v = table[cells[p]];
+        int xs = pt_x(v) - 7, ys = pt_y(v) - 7;
+        if (xs != xb || ys != yb) {
+            float dc = ssd_bounded(a, c_q.aw, x, y, b, c_q.bw, xs, ys, dbest);
+            ne++;
+            if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
+        }
+    }
+    if (c_q.do_kcoh && xb < c_q.bew && yb < c_q.beh) {
+        int ks = c_q.ks;
+        /* kcoherence_set is beh x bew x kc even when ks > 1 (patchtable.h:2659, 3758). */
+        const int2 *kp = kcoh + ((size_t) (yb / ks) * c_q.bew + (xb / ks)) * c_q.kc;
+        int kdx = ks > 1 ? xb % ks : 0, kdy = ks > 1 ? yb % ks : 0;
+        for (int k = 0; k < c_q.kc; k++) {
+            int2 e = kp[k];
+            float kd = __int_as_float(e.y);
+            if ((double) kd >= c_q.triangle * (double) dbest) break;
+            int xs = pt_x(e.x) + kdx, ys = pt_y(e.x) + kdy;
+            if (xs >= c_q.bew) xs = c_q.bew - 1;
+            if (ys >= c_q.beh) ys = c_q.beh - 1;
+            float dc = ssd_bounded(a, c_q.aw, x, y, b, c_q.bw, xs, ys, dbest);
+            ne++;
+            if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
+        }
+    }
+    ch_pos[p] = pt_xy(xb, yb);
+    ch_d[p] = dch;
+    if (evals) atomicAdd(evals, ne);
+}
+
+/* Step 4 as a pull: the best of the stored match and every neighbour's chosen offset applied
+   to this patch. */
+__global__ void __launch_bounds__(NT)
+k_pull(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
+       const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
+       int *nxt_pos, float *nxt_d, unsigned *evals) {
+    int p = blockIdx.x * NT + threadIdx.x;
+    if (p >= c_q.ew * c_q.eh) return;
+    int x = p % c_q.ew, y = p / c_q.ew;
+    int bpos = cur_pos[p];
+    float bd = cur_d[p];
+    const int R = c_q.radius;
+    int tried[25];
+    int ntried = 0;
+    unsigned ne = 0;
+    for (int dy = -R; dy <= R; dy++) {
+        int ny = y + dy;
+        if (ny < 0 || ny >= c_q.eh) continue;
+        for (int dx = -R; dx <= R; dx++) {
+            int nx = x + dx;
+            if (nx < 0 || nx >= c_q.ew) continue;
+            int q = ny * c_q.ew + nx;
+            int cp = ch_pos[q];
+            int xs = pt_x(cp) - dx, ys = pt_y(cp) - dy;
+            if (xs < 0 || ys < 0 || xs >= c_q.bew || ys >= c_q.beh) continue;
+            int cand = pt_xy(xs, ys);
+            if (cand == bpos) continue;
+            bool dup = false;
+            for (int t = 0; t < ntried; t++) dup |= tried[t] == cand;
+            if (dup) continue;
+            if (ntried < 25) tried[ntried++] = cand;
+            float dc = (dx == 0 && dy == 0) ? ch_d[q] : ssd_bounded(a, c_q.aw, x, y, b, c_q.bw, xs, ys, bd);
+            ne += (dx != 0 || dy != 0);
+            if (dc < bd) { bd = dc; bpos = cand; }
+        }
+    }
+    nxt_pos[p] = bpos;
+    nxt_d[p] = bd;
+    if (evals) atomicAdd(evals, ne);
+}
+
+__global__ void k_init(int n, int pos, float d, int *cur_pos, float *cur_d) {
+    int p = blockIdx.x * NT + threadIdx.x;
+    if (p < n) { cur_pos[p] = pos; cur_d[p] = d; }
+}
+
+__global__ void k_output(int n, const int *__restrict__ pos, const float *__restrict__ d, double *ann) {
+    int p = blockIdx.x * NT + threadIdx.x;
+    if (p >= n) return;
+    int v = pos[p];
+    ann[3 * (size_t) p + 0] = pt_x(v);
+    ann[3 * (size_t) p + 1] = pt_y(v);
+    ann[3 * (size_t) p + 2] = d[p];
+}
+
+}  // namespace
+
+static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
+    memset(&q, 0, sizeof(q));
+    q.aw = s.aw; q.ah = s.ah; q.ew = s.aw - 7; q.eh = s.ah - 7;
+    q.bw = s.bw; q.bh = s.bh; q.bew = s.bw - 7; q.beh = s.bh - 7;
+    q.prop_scale = s.prop_scale;
+    q.triangle = s.triangle_factor;
+    q.kc = s.kcoherence;
+    q.ks = s.kcoherence_step;
+    q.radius = s.radius;
+    q.do_kcoh = s.kcoherence > 0;
+    if (q.radius > 2) return pt_fail(PT_UNSUPPORTED, "propagation radius %d > 2 on the GPU path", q.radius);
+    return PT_OK;
+}
+
+pt_status pt_launch_init(int n, int pos, float d, int *cur_pos, float *cur_d, cudaStream_t st) {
+    k_init<<<(n + NT - 1) / NT, NT, 0, st>>>(n, pos, d, cur_pos, cur_d);
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
+                           const long long *cells, const int *table, const int2 *kcoh, int do_table, int *ch_pos,
+                           float *ch_d, unsigned *evals, cudaStream_t st) {
+    QPlan q;
+    PT_TRY(make_qplan(s, q));
+    k_choose<<<(n + NT - 1) / NT, NT, 0, st>>>(q, a, b, cur_pos, cur_d, cells, table, kcoh, do_table, ch_pos, ch_d, evals);
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
+                         const int *ch_pos, const float *ch_d, int *nxt_pos, float *nxt_d, unsigned *evals,
+                         cudaStream_t st) {
+    QPlan q;
+    PT_TRY(make_qplan(s, q));
+    k_pull<<<(n + NT - 1) / NT, NT, 0, st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals);
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_output(int n, const int *pos, const float *d, double *ann, cudaStream_t st) {
+    k_output<<<(n + NT - 1) / NT, NT, 0, st>>>(n, pos, d, ann);
+    PT_LAUNCHED();
+    return PT_OK;
+}

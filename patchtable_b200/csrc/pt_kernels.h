@@ -1,0 +1,58 @@
+/* Host-side launchers of the CUDA kernels (one translation unit per stage). */
+#pragma once
+
+#include <cuda_runtime.h>
+#include <vector>
+
+#include "pt_internal.h"
+
+/* k_descriptor.cu */
+pt_status pt_descriptor_check(int ndims, int nchroma);
+/* desc may be NULL (only the RGBA copy is written); rgba may be NULL. */
+pt_status pt_launch_descriptor(int ndims, int nchroma, const float *rgb, int h, int w, int convert, float4 *rgba,
+                               float *desc, int ds, cudaStream_t st);
+
+/* k_build.cu */
+pt_status pt_launch_fill(int *p, long long n, int v, cudaStream_t st);
+pt_status pt_launch_minmax(const float *desc, int ds, int G, long long P, const int *allowed, int allowed_index,
+                           float *hmin, float *hmax, cudaStream_t st);
+pt_status pt_quantile_values(const float *desc, int ds, int d, int eh, int ew, int step, const int *allowed,
+                             int allowed_index, const std::vector<int> &want, std::vector<float> &vals,
+                             int *count_out, cudaStream_t st);
+/* Per-dimension get_bin parameters of a built table. */
+struct PtBins {
+    int G;
+    float min_val[PT_DESC_MAX], range[PT_DESC_MAX];
+    long long stride[PT_DESC_MAX];
+};
+pt_status pt_launch_populate(const PtBins &bins, const float *desc, int ds, long long P, const int *rank,
+                             const int *to_bin, int *table, cudaStream_t st);
+pt_status pt_launch_cells(const PtBins &bins, const float *desc, int ds, long long P, const int *to_bin,
+                          long long *cells, cudaStream_t st);
+pt_status pt_dt_prop(int *table, long long ncells, const int *order_xy, int G, const int *nslices,
+                     const long long *stride, int dt_iters, int run, long long *seeded, int *levels_out,
+                     cudaStream_t st);
+pt_status pt_launch_replace(int *table, long long n, int from, int to, cudaStream_t st);
+
+/* k_kcoh.cu */
+pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, int Q, int K, int *out, cudaStream_t st);
+pt_status pt_gather_rows(const float *desc, int ds, int nd, const int *rows, int n, float *out, cudaStream_t st);
+pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *train, int N, int nd, const int *tpos,
+                        const float *qdesc, const int *qpos, const int *qcell, int Q, const int *seg_start, int nseg,
+                        int kc, int min_dist, int2 *kcoh, int *max_knn_out, cudaStream_t st);
+
+/* k_query.cu */
+struct QuerySetup {
+    int aw, ah, bw, bh;
+    double prop_scale, triangle_factor;
+    int kcoherence, kcoherence_step, radius;
+    cudaStream_t stream;
+};
+pt_status pt_launch_init(int n, int pos, float d, int *cur_pos, float *cur_d, cudaStream_t st);
+pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
+                           const long long *cells, const int *table, const int2 *kcoh, int do_table, int *ch_pos,
+                           float *ch_d, unsigned *evals, cudaStream_t st);
+pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
+                         const int *ch_pos, const float *ch_d, int *nxt_pos, float *nxt_d, unsigned *evals,
+                         cudaStream_t st);
+pt_status pt_launch_output(int n, const int *pos, const float *d, double *ann, cudaStream_t st);

@@ -1,0 +1,577 @@
+/* Host side of the PatchTable build and query (the C ABI of include/patchtable_b200.h).
+
+   Build, PatchTableFixedN constructor (patchtable/patchtable.h:2584-3373), on the device:
+     descriptor of b -> per-dimension range -> slice counts (host, scale_slices_to_limit)
+     -> quantile centres (device sort, host arithmetic) and to_bin tables (host)
+     -> k-coherence set -> populate in the reference's random_shuffle order -> DT.
+   Query, lookup_templated (patchtable.h:3468-4217): descriptor of a -> cell of every patch
+     -> choose / pull passes -> float64 NNF.
+
+   The host keeps only parameters, partition arrays and shapes; images, descriptors, the table
+   and the k-coherence set stay in device memory for the table's lifetime. */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "patchtable_b200.h"
+#include "pt_internal.h"
+#include "pt_kernels.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+thread_local long long g_launches = 0;
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+/* scale_slices_to_limit, patchtable.cpp:611-642 (product/multiply: solver/util.cpp:186-205). */
+std::vector<int> scale_slices_to_limit(std::vector<int> nslices, double limit) {
+    auto product = [](const std::vector<int> &L) { double a = 1.0; for (int v : L) a *= v; return a; };
+    if (limit > 0) {
+        std::vector<int> nslices0(nslices);
+        double factor = 1.0;
+        for (auto &v : nslices) v = std::max(v, 1);
+        while (product(nslices) > limit) {
+            factor *= 0.995;
+            for (size_t i = 0; i < nslices.size(); i++) nslices[i] = (int) (nslices0[i] * factor + 0.5);
+            for (auto &v : nslices) v = std::max(v, 1);
+        }
+        for (;;) {
+            nslices0 = nslices;
+            bool success = false;
+            for (size_t i = 0; i < nslices.size(); i++) {
+                nslices[i]++;
+                if (product(nslices) > limit) nslices = nslices0;
+                else { success = true; nslices0 = nslices; }
+            }
+            if (!success) break;
+        }
+    }
+    return nslices;
+}
+
+}  // namespace
+
+pt_status pt_fail(pt_status s, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return s;
+}
+
+void pt_count_launches(int n) { g_launches += n; }
+
+struct pt_table {
+    pt_params p;
+    int h = 0, w = 0, eh = 0, ew = 0;
+    int nd = 0, G = 0, ds = 8;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    DevBuf<float4> b_rgba;
+    DevBuf<float> b_desc;
+    DevBuf<int> allowed;
+    std::vector<int> nslices;
+    std::vector<long long> stride;
+    long long ncells = 0;
+    std::vector<PtPartition> part;
+    std::vector<float> min_val, max_val, range;
+    PtBins bins;
+    DevBuf<int> to_bin;
+    DevBuf<int> table;
+    long long add_count = 0;
+    int dt_levels = 0;
+    DevBuf<int2> kcoh;
+    int kc_list = 0;
+    /* query scratch, reused across lookups (like lookup_buffer/lookup_wh, patchtable.h:1507-1509) */
+    DevBuf<float> q_rgb;
+    DevBuf<float4> q_rgba;
+    DevBuf<float> q_desc;
+    DevBuf<long long> q_cells;
+    DevBuf<int> q_pos[2], q_chpos;
+    DevBuf<float> q_d[2], q_chd;
+    DevBuf<double> q_ann;
+    DevBuf<unsigned> q_evals;
+    unsigned long long last_evals = 0;
+
+    ~pt_table() {
+        if (own_stream && st) cudaStreamDestroy(st);
+    }
+};
+
+namespace {
+
+pt_status check_params(const pt_params *p, int h, int w) {
+    if (!p) return pt_fail(PT_BAD_ARG, "null params");
+    if (p->patch_w != 8) return pt_fail(PT_UNSUPPORTED, "patch_w=%d: only 8x8 patches are supported (gck.h)", p->patch_w);
+    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    if (w > 65535 || h > 16383) return pt_fail(PT_BAD_ARG, "image %dx%d exceeds the packed position range (XY_TO_INT)", w, h);
+    if (p->is_descriptor) return pt_fail(PT_UNSUPPORTED, "descriptor mode is not implemented on the GPU path");
+    if (p->dim_algo != 0) return pt_fail(PT_UNSUPPORTED, "dim_algo pca is not implemented on the GPU path");
+    if (p->convert_colorspace && p->colorspace != 0) return pt_fail(PT_UNSUPPORTED, "colorspace lab is not implemented on the GPU path");
+    if (p->lookup_algo != 0) return pt_fail(PT_UNSUPPORTED, "only lookup_algo table is implemented on the GPU path");
+    if (p->kcoherence && p->kcoherence_algo != 0) return pt_fail(PT_UNSUPPORTED, "only kcoherence_algo flann (exact search) is implemented");
+    if (p->incoherence) return pt_fail(PT_UNSUPPORTED, "incoherence is not implemented on the GPU path");
+    if (p->randomize_dt) return pt_fail(PT_UNSUPPORTED, "randomize_dt is not implemented on the GPU path");
+    if (!p->populate_nearest) return pt_fail(PT_UNSUPPORTED, "populate_nearest 0 is not implemented on the GPU path");
+    if (p->ntables > 1) return pt_fail(PT_UNSUPPORTED, "ntables > 1 is not implemented on the GPU path");
+    if (p->run_dt && p->dt_algo != 1) return pt_fail(PT_UNSUPPORTED, "dt_algo %d is not implemented on the GPU path", p->dt_algo);
+    if (p->do_rs || p->spatial) return pt_fail(PT_UNSUPPORTED, "random/spatial search (-do_rs, -spatial) is not implemented on the GPU path");
+    if (p->init_random) return pt_fail(PT_UNSUPPORTED, "init_random is not implemented on the GPU path");
+    if (p->ndims < 1 || p->ndims > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "ndims %d outside 1..%d", p->ndims, PT_DESC_MAX);
+    int G = p->grid_ndims < 0 ? p->ndims : p->grid_ndims;
+    if (G < 1 || G > p->ndims) return pt_fail(PT_BAD_ARG, "grid_ndims %d outside 1..ndims", G);
+    if (p->partition_step < 1 || p->kcoherence_step < 1 || p->flann_build_step < 1 || p->flann_reset_step < 1)
+        return pt_fail(PT_BAD_ARG, "step parameters must be >= 1");
+    return PT_OK;
+}
+
+pt_status build_partition(pt_table *t) {
+    const int G = t->G;
+    t->part.assign(G, PtPartition());
+    for (int d = 0; d < G; d++) {
+        PtPartition &P = t->part[d];
+        int ns = t->nslices[d];
+        P.nslices = ns;
+        P.min_val = t->min_val[d];
+        P.max_val = t->max_val[d];
+        P.range = P.max_val - P.min_val;
+        /* Count the partition sample first, then fetch the quantile values
+           (PatchPartition1D, patchtable.h:1193-1201). */
+        int N = 0;
+        std::vector<float> vals;
+        PT_TRY(pt_quantile_values(t->b_desc.p, t->ds, d, t->eh, t->ew, t->p.partition_step, t->allowed.p,
+                                  t->p.allowed_index, {}, vals, &N, t->st));
+        if (N < 1) return pt_fail(PT_BAD_ARG, "no allowed patches to build a table from");
+        std::vector<int> want;
+        want.reserve(2 * ns);
+        for (int i = 0; i < ns; i++) {
+            want.push_back((int) ((long long) (N - 1) * i / ns));
+            want.push_back((int) ((long long) (N - 1) * (i + 1) / ns));
+        }
+        int N2 = 0;
+        PT_TRY(pt_quantile_values(t->b_desc.p, t->ds, d, t->eh, t->ew, t->p.partition_step, t->allowed.p,
+                                  t->p.allowed_index, want, vals, &N2, t->st));
+        P.centers.resize(ns);
+        P.lsizes.resize(ns);
+        P.rsizes.resize(ns);
+        for (int i = 0; i < ns; i++) {
+            float cell_min = vals[2 * i], cell_max = vals[2 * i + 1];
+            P.centers[i] = (cell_min + cell_max) / 2;
+        }
+        for (int i = 0; i < ns; i++) {            /* patchtable.h:1203-1215 */
+            float prev_center = (i - 1 >= 0) ? P.centers[i - 1] : P.min_val;
+            float next_center = (i + 1 < ns) ? P.centers[i + 1] : P.max_val;
+            P.lsizes[i] = P.centers[i] - prev_center;
+            if (i - 1 >= 0) P.lsizes[i] /= 2;
+            P.rsizes[i] = next_center - P.centers[i];
+            if (i + 1 < ns) P.rsizes[i] /= 2;
+        }
+        P.to_bin.resize(PT_NMAP);                  /* patchtable.h:1219-1256 */
+        int icenter = 0;
+        for (int i = 0; i < PT_NMAP; i++) {
+            double coord = P.min_val + (i + 0.5) * P.range / PT_NMAP;
+            while (coord > P.centers[icenter]) {
+                if (icenter + 1 < ns) icenter++;
+                else break;
+            }
+            int prev_c = icenter - 1;
+            if (prev_c < 0) prev_c = 0;
+            int next_c = icenter;
+            if (next_c == 0) next_c++;
+            if (ns == 1) next_c = prev_c = 0;
+            double mid = (P.centers[prev_c] + P.centers[next_c]) / 2.0;
+            P.to_bin[i] = (coord < mid) ? prev_c : next_c;
+        }
+    }
+    std::vector<int> flat((size_t) G * PT_NMAP);
+    for (int d = 0; d < G; d++) std::copy(t->part[d].to_bin.begin(), t->part[d].to_bin.end(), flat.begin() + (size_t) d * PT_NMAP);
+    PT_CUDA(t->to_bin.reserve(flat.size()));
+    PT_CUDA(cudaMemcpyAsync(t->to_bin.p, flat.data(), sizeof(int) * flat.size(), cudaMemcpyHostToDevice, t->st));
+    memset(&t->bins, 0, sizeof(t->bins));
+    t->bins.G = G;
+    for (int d = 0; d < G; d++) {
+        t->bins.min_val[d] = t->part[d].min_val;
+        t->bins.range[d] = t->part[d].range;
+        t->bins.stride[d] = t->stride[d];
+    }
+    return PT_OK;
+}
+
+bool host_allowed(const std::vector<int> &allowed, int idx, int py, int px, int ew) {
+    return allowed.empty() || allowed[(size_t) py * ew + px] == idx;
+}
+
+pt_status build_kcoherence(pt_table *t, const std::vector<int> &allowed) {
+    const pt_params &p = t->p;
+    const int ew = t->ew, eh = t->eh;
+    /* Train set: build_flann_index_func (patchtable.h:822-861), allowed patches every
+       flann_build_step pixels in raster order. */
+    std::vector<int> trows, tpos;
+    for (int y = 0; y < eh; y += p.flann_build_step)
+        for (int x = 0; x < ew; x += p.flann_build_step)
+            if (host_allowed(allowed, p.allowed_index, y, x, ew)) { trows.push_back(y * ew + x); tpos.push_back(pt_xy(x, y)); }
+    /* Queries in the reference's loop order (patchtable.h:2705-2713) and the knn reset segments
+       ((x / kcoherence_step) % flann_reset_step == 0 with x in padded coordinates, :2714). */
+    std::vector<int> qrows, qpos, qcell, seg;
+    int ks = p.kcoherence_step;
+    for (int y = 7; y < t->h; y += ks)
+        for (int x = 7; x < t->w; x += ks) {
+            int py = y - 7, px = x - 7;
+            if (!host_allowed(allowed, p.allowed_index, py, px, ew)) continue;
+            int q = (int) qrows.size();
+            if (q == 0 || (x / ks) % p.flann_reset_step == 0) seg.push_back(q);
+            qrows.push_back(py * ew + px);
+            qpos.push_back(pt_xy(px, py));
+            qcell.push_back((py / ks) * ew + px / ks);
+        }
+    int N = (int) trows.size(), Q = (int) qrows.size(), nseg = (int) seg.size();
+    PT_CUDA(t->kcoh.reserve((size_t) eh * ew * p.kcoherence));
+    PT_CUDA(cudaMemsetAsync(t->kcoh.p, 0, sizeof(int2) * (size_t) eh * ew * p.kcoherence, t->st));
+    if (Q == 0) return PT_OK;
+    DevBuf<int> d_trows, d_tpos, d_qrows, d_qpos, d_qcell, d_seg;
+    DevBuf<float> train, qdesc;
+    PT_CUDA(d_trows.reserve(N)); PT_CUDA(d_tpos.reserve(N));
+    PT_CUDA(d_qrows.reserve(Q)); PT_CUDA(d_qpos.reserve(Q)); PT_CUDA(d_qcell.reserve(Q)); PT_CUDA(d_seg.reserve(nseg));
+    PT_CUDA(train.reserve((size_t) N * t->nd)); PT_CUDA(qdesc.reserve((size_t) Q * t->nd));
+    PT_CUDA(cudaMemcpyAsync(d_trows.p, trows.data(), sizeof(int) * N, cudaMemcpyHostToDevice, t->st));
+    PT_CUDA(cudaMemcpyAsync(d_tpos.p, tpos.data(), sizeof(int) * N, cudaMemcpyHostToDevice, t->st));
+    PT_CUDA(cudaMemcpyAsync(d_qrows.p, qrows.data(), sizeof(int) * Q, cudaMemcpyHostToDevice, t->st));
+    PT_CUDA(cudaMemcpyAsync(d_qpos.p, qpos.data(), sizeof(int) * Q, cudaMemcpyHostToDevice, t->st));
+    PT_CUDA(cudaMemcpyAsync(d_qcell.p, qcell.data(), sizeof(int) * Q, cudaMemcpyHostToDevice, t->st));
+    PT_CUDA(cudaMemcpyAsync(d_seg.p, seg.data(), sizeof(int) * nseg, cudaMemcpyHostToDevice, t->st));
+    PT_TRY(pt_gather_rows(t->b_desc.p, t->ds, t->nd, d_trows.p, N, train.p, t->st));
+    PT_TRY(pt_gather_rows(t->b_desc.p, t->ds, t->nd, d_qrows.p, Q, qdesc.p, t->st));
+    PT_TRY(pt_kcoherence(t->b_rgba.p, t->w, train.p, N, t->nd, d_tpos.p, qdesc.p, d_qpos.p, d_qcell.p, Q, d_seg.p,
+                         nseg, p.kcoherence, p.kcoherence_min_dist, t->kcoh.p, &t->kc_list, t->st));
+    return PT_OK;
+}
+
+pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int channels, const float *wh0,
+                      const int32_t *allowed, pt_table **out) {
+    if (!out) return pt_fail(PT_BAD_ARG, "null output pointer");
+    *out = nullptr;
+    if (!b) return pt_fail(PT_BAD_ARG, "null image");
+    PT_TRY(check_params(pin, h, w));
+    if (channels != 3) return pt_fail(PT_BAD_ARG, "expected a 3-channel RGB image, got %d channels", channels);
+    std::unique_ptr<pt_table> t(new pt_table());
+    t->p = *pin;
+    pt_params &p = t->p;
+    if (p.grid_ndims < 0) p.grid_ndims = p.ndims;          /* patchtable.h:2603 */
+    t->h = h; t->w = w; t->eh = h - 7; t->ew = w - 7;
+    t->nd = p.ndims; t->G = p.grid_ndims;
+    t->ds = p.ndims <= 8 ? 8 : 16;
+    PT_TRY(pt_descriptor_check(p.ndims, p.nchroma));
+    PT_CUDA(cudaStreamCreateWithFlags(&t->st, cudaStreamNonBlocking));
+    t->own_stream = true;
+    const long long P = (long long) t->eh * t->ew;
+
+    /* Descriptor of b (get_padded_descriptor, patchtable.h:2492-2546) and the RGBA copy kept as b0. */
+    {
+        DevBuf<float> rgb;
+        PT_CUDA(rgb.reserve((size_t) h * w * 3));
+        PT_CUDA(cudaMemcpyAsync(rgb.p, b, sizeof(float) * (size_t) h * w * 3, cudaMemcpyHostToDevice, t->st));
+        PT_CUDA(t->b_rgba.reserve((size_t) h * w));
+        PT_CUDA(t->b_desc.reserve((size_t) P * t->ds));
+        PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, rgb.p, h, w, p.convert_colorspace, t->b_rgba.p, t->b_desc.p,
+                                    t->ds, t->st));
+        if (wh0) {
+            /* Caller-supplied padded descriptor (wh0_no_copy): interior patches only. */
+            std::vector<float> packed((size_t) P * t->ds, 0.0f);
+            for (int y = 0; y < t->eh; y++)
+                for (int x = 0; x < t->ew; x++)
+                    for (int d = 0; d < t->nd; d++)
+                        packed[((size_t) y * t->ew + x) * t->ds + d] = wh0[((size_t) (y + 7) * (w + 7) + (x + 7)) * t->nd + d];
+            PT_CUDA(cudaMemcpyAsync(t->b_desc.p, packed.data(), sizeof(float) * packed.size(), cudaMemcpyHostToDevice, t->st));
+        }
+        PT_CUDA(cudaStreamSynchronize(t->st));
+    }
+    std::vector<int> allowed_h;
+    if (allowed) {
+        allowed_h.assign(allowed, allowed + P);
+        PT_CUDA(t->allowed.reserve(P));
+        PT_CUDA(cudaMemcpyAsync(t->allowed.p, allowed, sizeof(int) * P, cudaMemcpyHostToDevice, t->st));
+    }
+
+    /* k-coherence is computed before the table in the reference (patchtable.h:2653). */
+    if (p.kcoherence > 0) PT_TRY(build_kcoherence(t.get(), allowed_h));
+
+    /* set_min_max + set_nslices (patchtable.h:1758-1810, 2567-2582). */
+    t->min_val.assign(t->G, 0.f);
+    t->max_val.assign(t->G, 0.f);
+    PT_TRY(pt_launch_minmax(t->b_desc.p, t->ds, t->G, P, t->allowed.p, p.allowed_index, t->min_val.data(),
+                            t->max_val.data(), t->st));
+    t->range.resize(t->G);
+    for (int d = 0; d < t->G; d++) t->range[d] = t->max_val[d] - t->min_val[d];
+    std::vector<int> ns(t->G);
+    if (p.n_nslices == 0) {
+        float max_range = t->range[0];
+        for (int d = 1; d < t->G; d++) if (t->range[d] > max_range) max_range = t->range[d];
+        double scale = 200.0 / max_range;
+        for (int d = 0; d < t->G; d++) ns[d] = (int) (t->range[d] * scale);
+    } else {
+        if (p.n_nslices != t->G) return pt_fail(PT_BAD_ARG, "-nslices has %d entries, grid has %d dims", p.n_nslices, t->G);
+        for (int d = 0; d < t->G; d++) ns[d] = p.nslices[d];
+    }
+    t->nslices = scale_slices_to_limit(ns, p.limit);
+    t->stride.assign(t->G, 1);
+    t->ncells = 1;
+    for (int d = t->G - 1; d >= 0; d--) { t->stride[d] = t->ncells; t->ncells *= t->nslices[d]; }
+    if (t->ncells >= (1ll << 31)) return pt_fail(PT_UNSUPPORTED, "table of %lld cells exceeds 2^31", t->ncells);
+    PT_TRY(build_partition(t.get()));
+
+    /* Populate in std::random_shuffle order (patchtable.h:3142-3154): the permutation is drawn
+       from the C library rand(), consuming it exactly as the reference does. */
+    std::vector<int> order_xy, rank(P, -1);
+    order_xy.reserve(P);
+    for (int y = 0; y < t->eh; y++)
+        for (int x = 0; x < t->ew; x++)
+            if (host_allowed(allowed_h, p.allowed_index, y, x, t->ew)) order_xy.push_back(pt_xy(x + 7, y + 7));
+    if (order_xy.empty()) return pt_fail(PT_BAD_ARG, "no allowed patches");
+    if (p.populate_random)
+        for (size_t i = 1; i < order_xy.size(); i++) {
+            size_t j = (size_t) (rand() % (int) (i + 1));
+            if (i != j) std::swap(order_xy[i], order_xy[j]);
+        }
+    for (size_t i = 0; i < order_xy.size(); i++) {
+        int v = order_xy[i];
+        rank[(size_t) (pt_y(v) - 7) * t->ew + (pt_x(v) - 7)] = (int) i;
+    }
+    {
+        DevBuf<int> d_rank, d_order;
+        PT_CUDA(d_rank.reserve(P));
+        PT_CUDA(d_order.reserve(order_xy.size()));
+        PT_CUDA(cudaMemcpyAsync(d_rank.p, rank.data(), sizeof(int) * P, cudaMemcpyHostToDevice, t->st));
+        PT_CUDA(cudaMemcpyAsync(d_order.p, order_xy.data(), sizeof(int) * order_xy.size(), cudaMemcpyHostToDevice, t->st));
+        PT_CUDA(t->table.reserve(t->ncells));
+        PT_TRY(pt_launch_fill(t->table.p, t->ncells, PT_UNUSED, t->st));
+        PT_TRY(pt_launch_populate(t->bins, t->b_desc.p, t->ds, P, d_rank.p, t->to_bin.p, t->table.p, t->st));
+        PT_TRY(pt_dt_prop(t->table.p, t->ncells, d_order.p, t->G, t->nslices.data(), t->stride.data(), p.dt_iters,
+                          p.run_dt, &t->add_count, &t->dt_levels, t->st));
+        bool zeros_filled = p.run_dt && p.dt_iters <= 0;
+        if (!zeros_filled) {                                  /* fill_zeros, patchtable.h:2063-2079 */
+            int vfill = pt_xy(7, 7);
+            if (!allowed_h.empty())
+                for (long long i = 0; i < P; i++)
+                    if (allowed_h[i] == p.allowed_index) { vfill = pt_xy((int) (i % t->ew) + 7, (int) (i / t->ew) + 7); break; }
+            PT_TRY(pt_launch_replace(t->table.p, t->ncells, PT_UNUSED, vfill, t->st));
+        }
+        PT_CUDA(cudaStreamSynchronize(t->st));
+    }
+    *out = t.release();
+    return PT_OK;
+}
+
+pt_status ensure_query_buffers(pt_table *t, int h, int w) {
+    long long P = (long long) (h - 7) * (w - 7);
+    PT_CUDA(t->q_rgb.reserve((size_t) h * w * 3));
+    PT_CUDA(t->q_rgba.reserve((size_t) h * w));
+    PT_CUDA(t->q_desc.reserve((size_t) P * t->ds));
+    PT_CUDA(t->q_cells.reserve(P));
+    for (int k = 0; k < 2; k++) { PT_CUDA(t->q_pos[k].reserve(P)); PT_CUDA(t->q_d[k].reserve(P)); }
+    PT_CUDA(t->q_chpos.reserve(P));
+    PT_CUDA(t->q_chd.reserve(P));
+    PT_CUDA(t->q_evals.reserve(2));
+    return PT_OK;
+}
+
+int default_passes(const pt_params &p) {
+    if (p.gpu_prop_passes > 0) return p.gpu_prop_passes;
+    return p.prop_iters <= 0 ? 0 : 2 + 2 * p.prop_iters;
+}
+
+/* The device part of a lookup: a_rgb (device, h x w x 3) -> d_ann (device doubles). */
+pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d_ann, cudaStream_t st) {
+    const pt_params &p = t->p;
+    long long P = (long long) (h - 7) * (w - 7);
+    int n = (int) P;
+    PT_TRY(ensure_query_buffers(t, h, w));
+    PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, a_rgb, h, w, p.convert_colorspace, t->q_rgba.p, t->q_desc.p,
+                                t->ds, st));
+    PT_TRY(pt_launch_cells(t->bins, t->q_desc.p, t->ds, P, t->to_bin.p, t->q_cells.p, st));
+    QuerySetup qs;
+    qs.aw = w; qs.ah = h; qs.bw = t->w; qs.bh = t->h;
+    qs.prop_scale = 1.0 / (1 + p.coherence_spatial);
+    qs.triangle_factor = p.triangle_factor;
+    qs.kcoherence = p.kcoherence;
+    qs.kcoherence_step = p.kcoherence_step;
+    qs.radius = p.query_step + p.prop_dist;
+    qs.stream = st;
+    if (qs.radius > 2) qs.radius = 2;
+    /* Initial field (patchtable.h:3538-3547): x = b0_ew + 1, dist = DIST_INFINITY. */
+    PT_TRY(pt_launch_init(n, pt_xy(t->ew + 1, 0), (float) PT_DIST_INF, t->q_pos[0].p, t->q_d[0].p, st));
+    int passes = default_passes(p);
+    int cur = 0;
+    unsigned *ev = t->q_evals.p;
+    PT_CUDA(cudaMemsetAsync(ev, 0, sizeof(unsigned) * 2, st));
+    for (int i = 0; i < passes; i++) {
+        /* Pass 0 plays the reference's first iteration (table lookup, :3641); k-coherence runs
+           on every pass unless restricted to iteration 0 (kcoherence_iter). */
+        bool do_table = i == 0 && p.do_table_lookup;
+        QuerySetup qi = qs;
+        if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
+        PT_TRY(pt_launch_choose(qi, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_cells.p,
+                                t->table.p, t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, ev, st));
+        if (p.do_prop) {
+            PT_TRY(pt_launch_pull(qs, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_chpos.p,
+                                  t->q_chd.p, t->q_pos[1 - cur].p, t->q_d[1 - cur].p, ev + 1, st));
+            cur = 1 - cur;
+        } else {
+            PT_CUDA(cudaMemcpyAsync(t->q_pos[cur].p, t->q_chpos.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
+            PT_CUDA(cudaMemcpyAsync(t->q_d[cur].p, t->q_chd.p, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+        }
+    }
+    PT_TRY(pt_launch_output(n, t->q_pos[cur].p, t->q_d[cur].p, d_ann, st));
+    return PT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pt_status pt_table_create(const pt_params *p, const float *b, int h, int w, int channels, const int32_t *allowed,
+                          pt_table **out) {
+    return create_impl(p, b, h, w, channels, nullptr, allowed, out);
+}
+
+pt_status pt_table_create_with_descriptor(const pt_params *p, const float *b, int h, int w, const float *wh0,
+                                          const int32_t *allowed, pt_table **out) {
+    if (!wh0) return pt_fail(PT_BAD_ARG, "null descriptor");
+    return create_impl(p, b, h, w, 3, wh0, allowed, out);
+}
+
+void pt_table_free(pt_table *t) { delete t; }
+
+pt_status pt_table_lookup(pt_table *t, const float *a, int h, int w, double *ann_out, const double *ann_prev,
+                          const float *coh_sv, double *seconds) {
+    double T0 = now_s();
+    if (!t || !a || !ann_out) return pt_fail(PT_BAD_ARG, "null argument");
+    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    if (ann_prev || coh_sv) return pt_fail(PT_UNSUPPORTED, "ann_prev / coherence_temporal_sv are not implemented yet");
+    long long P = (long long) (h - 7) * (w - 7);
+    PT_TRY(ensure_query_buffers(t, h, w));
+    PT_CUDA(t->q_ann.reserve((size_t) P * 3));
+    PT_CUDA(cudaMemcpyAsync(t->q_rgb.p, a, sizeof(float) * (size_t) h * w * 3, cudaMemcpyHostToDevice, t->st));
+    PT_TRY(lookup_device(t, t->q_rgb.p, h, w, t->q_ann.p, t->st));
+    PT_CUDA(cudaMemcpyAsync(ann_out, t->q_ann.p, sizeof(double) * (size_t) P * 3, cudaMemcpyDeviceToHost, t->st));
+    PT_CUDA(cudaStreamSynchronize(t->st));
+    if (seconds) *seconds = now_s() - T0;
+    return PT_OK;
+}
+
+pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int h, int w, double *d_ann, void *stream) {
+    if (!t || !d_a || !d_ann) return pt_fail(PT_BAD_ARG, "null argument");
+    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    return lookup_device(t, d_a, h, w, d_ann, (cudaStream_t) stream);
+}
+
+pt_status pt_table_lookup_batch(pt_table *t, int n, const float *const *a, const int *h, const int *w,
+                                double *const *ann_out) {
+    if (!t || n < 0 || (n > 0 && (!a || !h || !w || !ann_out))) return pt_fail(PT_BAD_ARG, "null argument");
+    for (int i = 0; i < n; i++) PT_TRY(pt_table_lookup(t, a[i], h[i], w[i], ann_out[i], nullptr, nullptr, nullptr));
+    return PT_OK;
+}
+
+int pt_table_shape(const pt_table *t, int *nslices, int64_t *ncells) {
+    if (!t) return -1;
+    if (nslices) for (int i = 0; i < PT_MAX_DIMS; i++) nslices[i] = i < t->G ? t->nslices[i] : 0;
+    if (ncells) *ncells = t->ncells;
+    return t->G;
+}
+
+pt_status pt_table_get_cells(const pt_table *t, int32_t *out) {
+    if (!t || !out) return pt_fail(PT_BAD_ARG, "null argument");
+    PT_CUDA(cudaMemcpyAsync(out, t->table.p, sizeof(int) * (size_t) t->ncells, cudaMemcpyDeviceToHost, t->st));
+    PT_CUDA(cudaStreamSynchronize(t->st));
+    return PT_OK;
+}
+
+pt_status pt_table_get_descriptor(const pt_table *t, float *out) {
+    if (!t || !out) return pt_fail(PT_BAD_ARG, "null argument");
+    long long P = (long long) t->eh * t->ew;
+    std::vector<float> tmp((size_t) P * t->ds);
+    PT_CUDA(cudaMemcpyAsync(tmp.data(), t->b_desc.p, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost, t->st));
+    PT_CUDA(cudaStreamSynchronize(t->st));
+    for (long long i = 0; i < P; i++)
+        for (int d = 0; d < t->nd; d++) out[i * t->nd + d] = tmp[i * t->ds + d];
+    return PT_OK;
+}
+
+pt_status pt_table_get_partition(const pt_table *t, int dim, float *centers, float *lsizes, float *rsizes,
+                                 int32_t *to_bin, float *mmr) {
+    if (!t || dim < 0 || dim >= t->G) return pt_fail(PT_BAD_ARG, "bad dimension");
+    const PtPartition &P = t->part[dim];
+    for (int i = 0; i < P.nslices; i++) {
+        if (centers) centers[i] = P.centers[i];
+        if (lsizes) lsizes[i] = P.lsizes[i];
+        if (rsizes) rsizes[i] = P.rsizes[i];
+    }
+    if (to_bin) for (int i = 0; i < PT_NMAP; i++) to_bin[i] = P.to_bin[i];
+    if (mmr) { mmr[0] = P.min_val; mmr[1] = P.max_val; mmr[2] = P.range; }
+    return PT_OK;
+}
+
+pt_status pt_table_get_kcoherence(const pt_table *t, int32_t *pos, float *dist) {
+    if (!t) return pt_fail(PT_BAD_ARG, "null table");
+    if (t->p.kcoherence <= 0) return PT_OK;
+    size_t n = (size_t) t->eh * t->ew * t->p.kcoherence;
+    std::vector<int2> tmp(n);
+    PT_CUDA(cudaMemcpyAsync(tmp.data(), t->kcoh.p, sizeof(int2) * n, cudaMemcpyDeviceToHost, t->st));
+    PT_CUDA(cudaStreamSynchronize(t->st));
+    for (size_t i = 0; i < n; i++) {
+        if (pos) pos[i] = tmp[i].x;
+        if (dist) memcpy(&dist[i], &tmp[i].y, sizeof(float));
+    }
+    return PT_OK;
+}
+
+int64_t pt_table_add_count(const pt_table *t) { return t ? t->add_count : -1; }
+
+pt_status pt_descriptor(const pt_params *p, const float *rgb, int h, int w, float *out) {
+    PT_TRY(check_params(p, h, w));
+    long long P = (long long) (h - 7) * (w - 7);
+    int ds = p->ndims <= 8 ? 8 : 16;
+    DevBuf<float> d_rgb, d_desc;
+    PT_CUDA(d_rgb.reserve((size_t) h * w * 3));
+    PT_CUDA(d_desc.reserve((size_t) P * ds));
+    PT_CUDA(cudaMemcpy(d_rgb.p, rgb, sizeof(float) * (size_t) h * w * 3, cudaMemcpyHostToDevice));
+    PT_TRY(pt_launch_descriptor(p->ndims, p->nchroma, d_rgb.p, h, w, p->convert_colorspace, nullptr, d_desc.p, ds, 0));
+    std::vector<float> tmp((size_t) P * ds);
+    PT_CUDA(cudaMemcpy(tmp.data(), d_desc.p, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost));
+    for (long long i = 0; i < P; i++)
+        for (int d = 0; d < p->ndims; d++) out[i * p->ndims + d] = tmp[i * ds + d];
+    return PT_OK;
+}
+
+pt_status pt_table_save(const pt_table *t, const char *filename) {
+    (void) t; (void) filename;
+    return pt_fail(PT_UNSUPPORTED, "save is not implemented yet");
+}
+
+pt_status pt_table_load(const pt_params *p, const char *filename, pt_table **out) {
+    (void) p; (void) filename; (void) out;
+    return pt_fail(PT_UNSUPPORTED, "load is not implemented yet");
+}
+
+int64_t pt_kernel_launch_count(void) { return g_launches; }
+void pt_kernel_launch_count_reset(void) { g_launches = 0; }
+
+const char *pt_last_error(void) { return g_last_error.c_str(); }
+const char *pt_version(void) { return "patchtable_b200 0.1 (sm_100a)"; }
+
+/* Diagnostics (no reference counterpart): DT levels and SSD evaluations of the last lookup. */
+int pt_table_dt_levels(const pt_table *t) { return t ? t->dt_levels : -1; }
+
+}  // extern "C"
