@@ -1,0 +1,308 @@
+#!/usr/bin/env python
+"""PatchTable query throughput on B200.
+
+Workload (default): the 1920x1080 synthetic match -- image a = 4 octaves of value noise + 20
+rectangles, b = a warped by a smooth random flow (max 16 px) + N(0, 0.02) noise (seed 2) -- with
+the reference's default parameters plus -speed 3 -coherence_spatial 4.  One step = one full query
+(descriptor of a, table lookup, k-coherence, propagation passes, float64 NNF) against a table of b
+built once before warm-up.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is query patches per second of device time with a already
+in device memory (L2 flushed between steps); `e2e` is the same metric through the public host API
+(pt_table_lookup) with pinned host buffers, copies included.  --impl reference times the
+reference's own implementation (oracle/_ref, compiled from its sources) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(name="synthetic 1920x1080 match, -speed 3 -coherence_spatial 4", h=1080, w=1920, seed=2,
+                switches="-speed 3 -coherence_spatial 4")
+METRIC = "query patches/s at matched mean NNF dist (learned vs plain, 1 B200); build s"
+UNIT = "patches/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (read-only query)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_inputs():
+    from patchtable_b200 import synth
+    return synth.pair(WORKLOAD["h"], WORKLOAD["w"], WORKLOAD["seed"])
+
+
+def cpu_baseline(a, b):
+    """The reference's own lookup (oracle/_ref) on a bounded crop of the workload, host cores."""
+    from oracle.oracle import REF_SO, Reference
+    if not os.path.exists(REF_SO):
+        return None
+    cores = os.cpu_count() or 1
+    h, w = 540, 960
+    ac, bc = np.ascontiguousarray(a[:h, :w]), np.ascontiguousarray(b[:h, :w])
+    ref = Reference()
+    ref.srand(1)
+    t = ref.build(WORKLOAD["switches"] + " -threads %d" % cores, bc)
+    secs = []
+    for _ in range(3):
+        _, s = t.lookup(ac)
+        secs.append(s)
+    P = (h - 7) * (w - 7)
+    return {"value": P / min(secs[1:]), "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": "reference lookup (oracle/_ref, -threads %d) on the top-left %dx%d crop of the workload pair, "
+                      "best of 2 timed lookups after 1 warm-up; table build %.1f s" % (cores, w, h, t.build_seconds)}
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference implementation on the host cores, full workload."""
+    if rank != 0:
+        return
+    from oracle.oracle import REF_SO, Reference, mean_dist
+    if not os.path.exists(REF_SO):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libptref.so was not built (needs the reference sources)"}))
+        return
+    a, b = make_inputs()
+    cores = os.cpu_count() or 1
+    ref = Reference()
+    ref.srand(1)
+    t = ref.build(WORKLOAD["switches"] + " -threads %d" % cores, b)
+    P = (a.shape[0] - 7) * (a.shape[1] - 7)
+    for _ in range(args.warmup):
+        t.lookup(a)
+    secs = []
+    md = None
+    for _ in range(args.steps):
+        ann, s = t.lookup(a)
+        secs.append(s)
+        md = mean_dist(ann)
+    tot = sum(secs)
+    val = P * args.steps / tot
+    out = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32", "data": "synthetic", "impl": "reference",
+           "config": {"workload": WORKLOAD["name"], "patches_per_step": P, "threads": cores, "build_s": t.build_seconds,
+                      "mean_nnf_dist": md},
+           "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "reference",
+                            "sample": "full workload, one reference lookup per step (PatchTable::lookup timer)"},
+           "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    import patchtable_b200 as ptb
+    from oracle.oracle import mean_dist
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    a, b = make_inputs()
+    H, W = a.shape[:2]
+    P = (H - 7) * (W - 7)
+    params = ptb.PatchTableParams(WORKLOAD["switches"])
+    ctypes.CDLL(None).srand(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    table = ptb.PatchTable(params, b)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    da = torch.from_numpy(a).to(dev)
+    dann = torch.empty((H - 7, W - 7, 3), dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    for _ in range(max(args.warmup, 3)):
+        table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
+    torch.cuda.synchronize()
+    md = mean_dist(dann.cpu().numpy())
+
+    clocks = Clocks(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ptb.reset_launch_count()
+    step_ms, stages, ctrs = [], {k: 0.0 for k in ptb.PatchTable.STAGES}, {}
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    tw0 = time.perf_counter()
+    for i in range(args.steps):
+        flush.zero_()                       # evict L2 between steps (outside the timed events)
+        ev[i][0].record(stream)
+        st, c = table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
+        ev[i][1].record(stream)
+        for k, v in st.items():
+            stages[k] += v
+        for k, v in c.items():
+            ctrs[k] = ctrs.get(k, 0) + v
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - tw0
+    launches = ptb.launch_count()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    # device time per step: the sum of the stage times (CUDA events around every kernel on the
+    # launching stream); the outer events also include the library's host-side launch gaps.
+    outer = [e0.elapsed_time(e1) for e0, e1 in ev]
+    tot_ms = sum(stages.values())
+    tot_t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tot_t, op=dist.ReduceOp.MAX)
+    tot_ms = float(tot_t.item())
+    value = world * P * args.steps / (tot_ms / 1000.0)
+
+    # end-to-end through the public host API with pinned buffers
+    a_pin = torch.from_numpy(a).pin_memory()
+    ann_pin = torch.empty((H - 7, W - 7, 3), dtype=torch.float64).pin_memory()
+    a_np, ann_np = a_pin.numpy(), ann_pin.numpy()
+    table.lookup(a_np, out=ann_np)
+    e2e_s = []
+    for _ in range(max(3, args.steps // 2)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        table.lookup(a_np, out=ann_np)
+        e2e_s.append(time.perf_counter() - t1)
+    e2e_t = torch.tensor([sum(e2e_s) / len(e2e_s)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e = world * P / float(e2e_t.item())
+    md_e2e = mean_dist(ann_np)
+
+    # roofline of the dominant kernel (HBM-bound accounting)
+    hbm, peak_kind = peaks()
+    passes = table.params.gpu_prop_passes or (2 + 2 * table.params.prop_iters)
+    dom = max(("choose", "pull"), key=lambda k: stages[k])
+    per_launch_ms = stages[dom] / (args.steps * passes)
+    alg_bytes = {"pull": 56, "choose": 60}[dom] * P
+    achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "query_%s_c2.md" % dom)) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    traffic = float(line.split(":")[1])
+    except OSError:
+        pass
+    rows = ctrs.get(dom + "_rows", 0)
+    fp32_tflops = rows * 72 / (stages[dom] / 1000.0) / 1e12
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(a, b)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded generator, patchtable_b200/synth.py)",
+        "config": {"workload": WORKLOAD["name"], "patches_per_step": P, "image": [H, W], "table_image": list(b.shape[:2]),
+                   "build_s": build_s, "mean_nnf_dist": md, "mean_nnf_dist_e2e": md_e2e,
+                   "prop_passes": passes, "l2": "flushed between steps (256 MiB write)", "parallelism": "replicas" if world > 1 else "single",
+                   "stage_ms_per_step": {k: v / args.steps for k, v in stages.items()},
+                   "outer_event_ms_per_step": sum(outer) / len(outer), "wall_ms_per_step": 1000 * wall / args.steps,
+                   "ssd_candidates_per_patch": {k: ctrs.get(k + "_cand", 0) / (args.steps * P) for k in ("choose", "pull")}},
+        "roofline": {"bound": "hbm", "kernel": "k_" + dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "fp32": {"achieved_tflops": fp32_tflops, "flop_per_ssd_row": 72,
+                              "ssd_rows_per_launch": rows / (args.steps * passes)}},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(a.nbytes), "d2h_bytes_per_step": int(ann_np.nbytes)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

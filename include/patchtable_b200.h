@@ -68,11 +68,14 @@ typedef struct pt_table pt_table;
    patchtable.cpp:26-136, 380-382. */
 void pt_params_default(pt_params *p);
 
-/* PatchTableParams::set_speed(i), patchtable.cpp:138-150.  PT_BAD_ARG unless 0 <= i <= 9. */
+/* PatchTableParams::set_speed(i), patchtable.cpp:138-150.  PT_BAD_ARG unless 0 <= i <= 9.
+   As in the reference, the preset string's first switch (-ndims) is not applied. */
 pt_status pt_params_set_speed(pt_params *p, int speed);
 
 /* PatchTableParams::set_from_switches(string), patchtable.cpp:152-373: "-name value" pairs with
-   the reference's switch names, "-speed" applied first, "-limit" in millions. */
+   the reference's switch names, "-speed" applied first, "-limit" in millions.  Exactly like the
+   reference, the first token of the string is ignored (it fills argv[0]); pass a command line
+   such as "patchtable -speed 3 -coherence_spatial 4" to have every switch applied. */
 pt_status pt_params_from_switches(pt_params *p, const char *switches);
 
 /* PatchTable<float,float,int32_t>(PatchTableParams *p, const Array<float> &b,
@@ -118,6 +121,16 @@ pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int h, int w, do
    pt_table_lookup layouts. */
 pt_status pt_table_lookup_batch(pt_table *t, int n, const float *const *a, const int *h,
                                 const int *w, double *const *ann_out);
+
+/* Diagnostics (no reference counterpart): pt_table_lookup_device with a CUDA event after every
+   stage.  stage_ms[6] receives the summed device time of {descriptor, cells, init, choose, pull,
+   output}; counters[4] = {choose candidates, choose SSD rows, pull candidates, pull SSD rows}
+   (one SSD row = 24 subtractions, multiplications and additions).  Synchronizes the stream. */
+pt_status pt_table_lookup_profile(pt_table *t, const float *d_a, int h, int w, double *d_ann,
+                                  void *stream, double *stage_ms, uint64_t *counters);
+
+/* Diagnostics: number of breadth-first levels the last DT build ran. */
+int pt_table_dt_levels(const pt_table *t);
 
 /* ---- introspection (parity tests); shapes as in the reference members patchtable.h:1487-1549 ---- */
 

@@ -75,11 +75,17 @@ int ptref_rand() { return rand(); }
 
 void ptref_set_threads(int n) { omp_set_num_threads(n); }
 
-/* Parses switches exactly like the reference CLI (patchtable.cpp:167-373, 384-387). */
+/* Parses switches exactly like the reference CLI: PatchTableParams(argc, argv) with argv[0] the
+   program name (patchtable.cpp:167-373, 384-387). */
 void *ptref_params_new(const char *switches) {
-    PatchTableParams *p = new PatchTableParams();
-    if (switches && switches[0]) p->set_from_switches(std::string(switches));
-    return p;
+    std::vector<std::string> toks;
+    std::istringstream in(switches ? switches : "");
+    std::string tok;
+    while (in >> tok) toks.push_back(tok);
+    std::vector<const char *> argv;
+    argv.push_back("patchtable");
+    for (auto &t : toks) argv.push_back(t.c_str());
+    return new PatchTableParams((int) argv.size(), argv.data());
 }
 
 void ptref_params_free(void *p) { delete (PatchTableParams *) p; }

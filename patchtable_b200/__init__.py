@@ -105,6 +105,7 @@ def lib() -> C.CDLL:
     L.pt_table_add_count.argtypes = [vp]
     L.pt_table_add_count.restype = C.c_int64
     L.pt_table_dt_levels.argtypes = [vp]
+    L.pt_table_lookup_profile.argtypes = [vp, vp, C.c_int, C.c_int, vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
     L.pt_descriptor.argtypes = [P, _f32p, C.c_int, C.c_int, _f32p]
     L.pt_last_error.restype = C.c_char_p
     L.pt_version.restype = C.c_char_p
@@ -121,7 +122,7 @@ def _check(status: int) -> None:
 
 class PatchTableParams:
     """PatchTableParams (patchtable/patchtable_params.h:23-161): reference defaults (speed 3),
-    then the switches, parsed with the reference's names and semantics."""
+    then command-line switches, as PatchTableParams(argc, argv) parses them."""
 
     def __init__(self, switches: str = ""):
         object.__setattr__(self, "_p", _Params())
@@ -130,7 +131,9 @@ class PatchTableParams:
             self.set_from_switches(switches)
 
     def set_from_switches(self, switches: str) -> None:
-        _check(lib().pt_params_from_switches(C.byref(self._p), switches.encode()))
+        """Applies command-line switches ("-speed 3 -coherence_spatial 4"); every switch counts,
+        as with PatchTableParams(argc, argv) whose argv[0] is the program name."""
+        _check(lib().pt_params_from_switches(C.byref(self._p), ("patchtable " + switches).encode()))
 
     def set_speed(self, i: int) -> None:
         _check(lib().pt_params_set_speed(C.byref(self._p), int(i)))
@@ -200,11 +203,18 @@ class PatchTable:
         except Exception:
             pass
 
-    def lookup(self, a, ann_prev=None, coherence_temporal_sv=None):
-        """PatchTable::lookup (patchtable.h:4448): returns the NNF; the wall time of the call
-        (including a's descriptor, like the reference's return value) is in self.last_seconds."""
+    def lookup(self, a, ann_prev=None, coherence_temporal_sv=None, out=None):
+        """PatchTable::lookup (patchtable.h:4448): returns the NNF (written into `out` when given,
+        e.g. a pinned buffer); the wall time of the call (including a's descriptor, like the
+        reference's return value) is in self.last_seconds."""
         a = _img(a)
-        ann = np.empty((a.shape[0] - 7, a.shape[1] - 7, 3), np.float64)
+        shape = (a.shape[0] - 7, a.shape[1] - 7, 3)
+        if out is not None:
+            if out.shape != shape or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
+                raise PatchTableError(1, "out must be a C-contiguous float64 array of shape %s" % (shape,))
+            ann = out
+        else:
+            ann = np.empty(shape, np.float64)
         secs = C.c_double()
         prev = None if ann_prev is None else np.ascontiguousarray(ann_prev, np.float64).ctypes.data_as(C.c_void_p)
         sv = None if coherence_temporal_sv is None else np.ascontiguousarray(coherence_temporal_sv, np.float32).ctypes.data_as(C.c_void_p)
@@ -215,6 +225,17 @@ class PatchTable:
     def lookup_device(self, a_ptr: int, h: int, w: int, ann_ptr: int, stream: int = 0) -> None:
         """Device-resident lookup: a_ptr / ann_ptr are device addresses (e.g. torch data_ptr())."""
         _check(lib().pt_table_lookup_device(self._h, C.c_void_p(a_ptr), h, w, C.c_void_p(ann_ptr), C.c_void_p(stream)))
+
+    STAGES = ("descriptor", "cells", "init", "choose", "pull", "output")
+
+    def lookup_profile(self, a_ptr: int, h: int, w: int, ann_ptr: int, stream: int = 0):
+        """Device lookup with per-stage device times (ms) and SSD work counters."""
+        ms = (C.c_double * 6)()
+        ctr = (C.c_uint64 * 4)()
+        _check(lib().pt_table_lookup_profile(self._h, C.c_void_p(a_ptr), h, w, C.c_void_p(ann_ptr),
+                                             C.c_void_p(stream), ms, ctr))
+        return dict(zip(self.STAGES, list(ms))), dict(choose_cand=ctr[0], choose_rows=ctr[1],
+                                                     pull_cand=ctr[2], pull_rows=ctr[3])
 
     # -- introspection for parity tests --------------------------------------------------------
     def shape(self):

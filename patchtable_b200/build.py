@@ -49,7 +49,7 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
         if s.endswith(".cu"):
             cmd = [nvcc, ARCH, "-lineinfo", "--expt-relaxed-constexpr", "-c", s, "-o", o] + common
         else:
-            cmd = [nvcc, "-x", "c++", "-c", s, "-o", o] + common
+            cmd = [nvcc, ARCH, "-x", "c++", "-c", s, "-o", o] + common
         cmds.append(cmd)
     procs = []
     for cmd in cmds:

@@ -40,9 +40,11 @@ __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
 /* patch_dist_exact in the reference's order, abandoning the sum (returning +inf) as soon as the
    running total reaches `bound`. */
 __device__ __forceinline__ float ssd_bounded(const float4 *__restrict__ A, int aw, int ax, int ay,
-                                             const float4 *__restrict__ B, int bw, int bx, int by, float bound) {
+                                             const float4 *__restrict__ B, int bw, int bx, int by, float bound,
+                                             unsigned &rows) {
     float l0 = 0.f, l1 = 0.f, l2 = 0.f, l3 = 0.f;
     for (int dy = 0; dy < 8; dy++) {
+        rows++;
         const float4 *ar = A + (size_t) (ay + dy) * aw + ax;
         const float4 *br = B + (size_t) (by + dy) * bw + bx;
         float e[24];
@@ -62,25 +64,33 @@ __device__ __forceinline__ float ssd_bounded(const float4 *__restrict__ A, int a
     return __fadd_rn(__fadd_rn(__fadd_rn(l0, l1), l2), l3);
 }
 
+/* Adds per-thread counts to counters[0..1] with one atomic per warp (profiling only). */
+__device__ __forceinline__ void count_work(unsigned long long *counters, unsigned cand, unsigned rows) {
+    if (!counters) return;
+    unsigned c = __reduce_add_sync(0xffffffffu, cand), r = __reduce_add_sync(0xffffffffu, rows);
+    if ((threadIdx.x & 31) == 0) { atomicAdd(counters, (unsigned long long) c); atomicAdd(counters + 1, (unsigned long long) r); }
+}
+
 /* Steps 1-3 for every patch: returns the chosen match and its exact distance. */
 __global__ void __launch_bounds__(NT)
 k_choose(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
          const float *__restrict__ cur_d, const long long *__restrict__ cells, const int *__restrict__ table,
-         const int2 *__restrict__ kcoh, int do_table, int *ch_pos, float *ch_d, unsigned *evals) {
+         const int2 *__restrict__ kcoh, int do_table, int *ch_pos, float *ch_d, unsigned long long *counters) {
     int p = blockIdx.x * NT + threadIdx.x;
-    if (p >= c_q.ew * c_q.eh) return;
+    const bool live = p < c_q.ew * c_q.eh;
+    unsigned ne = 0, rows = 0;
+    if (live) {
     int x = p % c_q.ew, y = p / c_q.ew;
     int pos = cur_pos[p];
     float dstore = cur_d[p];
     int xb = pt_x(pos), yb = pt_y(pos);
     float dbest = (float) ((double) dstore * c_q.prop_scale);
     float dch = dstore;          /* exact distance of the chosen match */
-    unsigned ne = 0;
     if (do_table) {
         int v = table[cells[p]];
         int xs = pt_x(v) - 7, ys = pt_y(v) - 7;
         if (xs != xb || ys != yb) {
-            float dc = ssd_bounded(a, c_q.aw, x, y, b, c_q.bw, xs, ys, dbest);
+            float dc = ssd_bounded(a, c_q.aw, x, y, b, c_q.bw, xs, ys, dbest, rows);
             ne++;
             if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
         }
@@ -97,14 +107,15 @@ k_choose(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict
             int xs = pt_x(e.x) + kdx, ys = pt_y(e.x) + kdy;
             if (xs >= c_q.bew) xs = c_q.bew - 1;
             if (ys >= c_q.beh) ys = c_q.beh - 1;
-            float dc = ssd_bounded(a, c_q.aw, x, y, b, c_q.bw, xs, ys, dbest);
+            float dc = ssd_bounded(a, c_q.aw, x, y, b, c_q.bw, xs, ys, dbest, rows);
             ne++;
             if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
         }
     }
     ch_pos[p] = pt_xy(xb, yb);
     ch_d[p] = dch;
-    if (evals) atomicAdd(evals, ne);
+    }
+    count_work(counters, ne, rows);
 }
 
 /* Step 4 as a pull: the best of the stored match and every neighbour's chosen offset applied
@@ -112,16 +123,17 @@ k_choose(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict
 __global__ void __launch_bounds__(NT)
 k_pull(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
        const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
-       int *nxt_pos, float *nxt_d, unsigned *evals) {
+       int *nxt_pos, float *nxt_d, unsigned long long *counters) {
     int p = blockIdx.x * NT + threadIdx.x;
-    if (p >= c_q.ew * c_q.eh) return;
+    const bool live = p < c_q.ew * c_q.eh;
+    unsigned ne = 0, rows = 0;
+    if (live) {
     int x = p % c_q.ew, y = p / c_q.ew;
     int bpos = cur_pos[p];
     float bd = cur_d[p];
     const int R = c_q.radius;
     int tried[25];
     int ntried = 0;
-    unsigned ne = 0;
     for (int dy = -R; dy <= R; dy++) {
         int ny = y + dy;
         if (ny < 0 || ny >= c_q.eh) continue;
@@ -138,14 +150,15 @@ k_pull(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__
             for (int t = 0; t < ntried; t++) dup |= tried[t] == cand;
             if (dup) continue;
             if (ntried < 25) tried[ntried++] = cand;
-            float dc = (dx == 0 && dy == 0) ? ch_d[q] : ssd_bounded(a, c_q.aw, x, y, b, c_q.bw, xs, ys, bd);
+            float dc = (dx == 0 && dy == 0) ? ch_d[q] : ssd_bounded(a, c_q.aw, x, y, b, c_q.bw, xs, ys, bd, rows);
             ne += (dx != 0 || dy != 0);
             if (dc < bd) { bd = dc; bpos = cand; }
         }
     }
     nxt_pos[p] = bpos;
     nxt_d[p] = bd;
-    if (evals) atomicAdd(evals, ne);
+    }
+    count_work(counters, ne, rows);
 }
 
 __global__ void k_init(int n, int pos, float d, int *cur_pos, float *cur_d) {
@@ -186,7 +199,7 @@ pt_status pt_launch_init(int n, int pos, float d, int *cur_pos, float *cur_d, cu
 
 pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
                            const long long *cells, const int *table, const int2 *kcoh, int do_table, int *ch_pos,
-                           float *ch_d, unsigned *evals, cudaStream_t st) {
+                           float *ch_d, unsigned long long *evals, cudaStream_t st) {
     QPlan q;
     PT_TRY(make_qplan(s, q));
     k_choose<<<(n + NT - 1) / NT, NT, 0, st>>>(q, a, b, cur_pos, cur_d, cells, table, kcoh, do_table, ch_pos, ch_d, evals);
@@ -195,8 +208,8 @@ pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const fl
 }
 
 pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
-                         const int *ch_pos, const float *ch_d, int *nxt_pos, float *nxt_d, unsigned *evals,
-                         cudaStream_t st) {
+                         const int *ch_pos, const float *ch_d, int *nxt_pos, float *nxt_d,
+                         unsigned long long *evals, cudaStream_t st) {
     QPlan q;
     PT_TRY(make_qplan(s, q));
     k_pull<<<(n + NT - 1) / NT, NT, 0, st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals);

@@ -51,8 +51,8 @@ struct QuerySetup {
 pt_status pt_launch_init(int n, int pos, float d, int *cur_pos, float *cur_d, cudaStream_t st);
 pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
                            const long long *cells, const int *table, const int2 *kcoh, int do_table, int *ch_pos,
-                           float *ch_d, unsigned *evals, cudaStream_t st);
+                           float *ch_d, unsigned long long *evals, cudaStream_t st);
 pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
-                         const int *ch_pos, const float *ch_d, int *nxt_pos, float *nxt_d, unsigned *evals,
-                         cudaStream_t st);
+                         const int *ch_pos, const float *ch_d, int *nxt_pos, float *nxt_d,
+                         unsigned long long *evals, cudaStream_t st);
 pt_status pt_launch_output(int n, const int *pos, const float *d, double *ann, cudaStream_t st);

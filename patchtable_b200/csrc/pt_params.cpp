@@ -28,10 +28,11 @@ std::vector<std::string> split(const std::string &s, char c) {
     return out;
 }
 
-/* parse_switches, patchtable.cpp:9-19: "-name value" pairs; a later pair overrides. */
+/* parse_switches, patchtable.cpp:9-19: "-name value" pairs; a later pair overrides.  Like the
+   reference, argv[0] is never examined (it is the program name on a command line). */
 std::map<std::string, std::string> parse_switches(const std::vector<std::string> &argv) {
     std::map<std::string, std::string> ans;
-    for (size_t i = 0; i < argv.size(); i++) {
+    for (size_t i = 1; i < argv.size(); i++) {
         if (!argv[i].empty() && argv[i][0] == '-' && i + 1 < argv.size()) {
             ans[argv[i]] = argv[i + 1];
             i += 1;
@@ -56,6 +57,9 @@ const char *SPEED_PRESETS[10] = {
 
 pt_status apply_switches(pt_params *p, const std::vector<std::string> &argv);
 
+/* set_from_switches(string), patchtable.cpp:152-160: the string is split on spaces and handed
+   over as an argv, so its first token takes the program-name slot and is ignored.  The speed
+   presets start with -ndims, which is therefore never applied by set_speed. */
 pt_status apply_string(pt_params *p, const std::string &s) {
     std::vector<std::string> L = split(s, ' '), argv;
     for (auto &t : L)

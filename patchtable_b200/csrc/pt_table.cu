@@ -103,10 +103,11 @@ struct pt_table {
     DevBuf<int> q_pos[2], q_chpos;
     DevBuf<float> q_d[2], q_chd;
     DevBuf<double> q_ann;
-    DevBuf<unsigned> q_evals;
-    unsigned long long last_evals = 0;
+    DevBuf<unsigned long long> q_counters;
+    std::vector<cudaEvent_t> events;
 
     ~pt_table() {
+        for (auto e : events) cudaEventDestroy(e);
         if (own_stream && st) cudaStreamDestroy(st);
     }
 };
@@ -383,7 +384,27 @@ pt_status ensure_query_buffers(pt_table *t, int h, int w) {
     for (int k = 0; k < 2; k++) { PT_CUDA(t->q_pos[k].reserve(P)); PT_CUDA(t->q_d[k].reserve(P)); }
     PT_CUDA(t->q_chpos.reserve(P));
     PT_CUDA(t->q_chd.reserve(P));
-    PT_CUDA(t->q_evals.reserve(2));
+    PT_CUDA(t->q_counters.reserve(4));
+    return PT_OK;
+}
+
+/* Stage timing of one lookup (pt_table_lookup_profile). */
+struct LookupProfile {
+    enum { DESC, CELLS, INIT, CHOOSE, PULL, OUTPUT, NSTAGES };
+    std::vector<std::pair<int, int>> marks;   /* (stage, event index) */
+    int next = 0;
+};
+
+pt_status mark(pt_table *t, LookupProfile *prof, int stage, cudaStream_t st) {
+    if (!prof) return PT_OK;
+    if (prof->next >= (int) t->events.size()) {
+        cudaEvent_t e;
+        PT_CUDA(cudaEventCreate(&e));
+        t->events.push_back(e);
+    }
+    PT_CUDA(cudaEventRecord(t->events[prof->next], st));
+    prof->marks.push_back({stage, prof->next});
+    prof->next++;
     return PT_OK;
 }
 
@@ -392,15 +413,23 @@ int default_passes(const pt_params &p) {
     return p.prop_iters <= 0 ? 0 : 2 + 2 * p.prop_iters;
 }
 
-/* The device part of a lookup: a_rgb (device, h x w x 3) -> d_ann (device doubles). */
-pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d_ann, cudaStream_t st) {
+/* The device part of a lookup: a_rgb (device, h x w x 3) -> d_ann (device doubles).  With prof,
+   an event is recorded after every stage and SSD work is counted. */
+pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d_ann, cudaStream_t st,
+                        LookupProfile *prof = nullptr) {
     const pt_params &p = t->p;
     long long P = (long long) (h - 7) * (w - 7);
+    if (P >= (1ll << 31)) return pt_fail(PT_BAD_ARG, "query image too large");
     int n = (int) P;
     PT_TRY(ensure_query_buffers(t, h, w));
+    unsigned long long *ctr = prof ? t->q_counters.p : nullptr;
+    if (ctr) PT_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * 4, st));
+    PT_TRY(mark(t, prof, -1, st));
     PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, a_rgb, h, w, p.convert_colorspace, t->q_rgba.p, t->q_desc.p,
                                 t->ds, st));
+    PT_TRY(mark(t, prof, LookupProfile::DESC, st));
     PT_TRY(pt_launch_cells(t->bins, t->q_desc.p, t->ds, P, t->to_bin.p, t->q_cells.p, st));
+    PT_TRY(mark(t, prof, LookupProfile::CELLS, st));
     QuerySetup qs;
     qs.aw = w; qs.ah = h; qs.bw = t->w; qs.bh = t->h;
     qs.prop_scale = 1.0 / (1 + p.coherence_spatial);
@@ -412,10 +441,9 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     if (qs.radius > 2) qs.radius = 2;
     /* Initial field (patchtable.h:3538-3547): x = b0_ew + 1, dist = DIST_INFINITY. */
     PT_TRY(pt_launch_init(n, pt_xy(t->ew + 1, 0), (float) PT_DIST_INF, t->q_pos[0].p, t->q_d[0].p, st));
+    PT_TRY(mark(t, prof, LookupProfile::INIT, st));
     int passes = default_passes(p);
     int cur = 0;
-    unsigned *ev = t->q_evals.p;
-    PT_CUDA(cudaMemsetAsync(ev, 0, sizeof(unsigned) * 2, st));
     for (int i = 0; i < passes; i++) {
         /* Pass 0 plays the reference's first iteration (table lookup, :3641); k-coherence runs
            on every pass unless restricted to iteration 0 (kcoherence_iter). */
@@ -423,10 +451,12 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
         QuerySetup qi = qs;
         if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
         PT_TRY(pt_launch_choose(qi, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_cells.p,
-                                t->table.p, t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, ev, st));
+                                t->table.p, t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, ctr, st));
+        PT_TRY(mark(t, prof, LookupProfile::CHOOSE, st));
         if (p.do_prop) {
             PT_TRY(pt_launch_pull(qs, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_chpos.p,
-                                  t->q_chd.p, t->q_pos[1 - cur].p, t->q_d[1 - cur].p, ev + 1, st));
+                                  t->q_chd.p, t->q_pos[1 - cur].p, t->q_d[1 - cur].p, ctr ? ctr + 2 : nullptr, st));
+            PT_TRY(mark(t, prof, LookupProfile::PULL, st));
             cur = 1 - cur;
         } else {
             PT_CUDA(cudaMemcpyAsync(t->q_pos[cur].p, t->q_chpos.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
@@ -434,6 +464,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
         }
     }
     PT_TRY(pt_launch_output(n, t->q_pos[cur].p, t->q_d[cur].p, d_ann, st));
+    PT_TRY(mark(t, prof, LookupProfile::OUTPUT, st));
     return PT_OK;
 }
 
@@ -475,6 +506,32 @@ pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int h, int w, do
     if (!t || !d_a || !d_ann) return pt_fail(PT_BAD_ARG, "null argument");
     if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
     return lookup_device(t, d_a, h, w, d_ann, (cudaStream_t) stream);
+}
+
+/* Diagnostics (no reference counterpart): pt_table_lookup_device with a CUDA event after every
+   stage.  stage_ms[6] receives the summed device time of {descriptor, cells, init, choose, pull,
+   output}; counters[4] = {choose candidates, choose SSD rows, pull candidates, pull SSD rows}
+   (one SSD row = 24 subtractions, multiplications and additions).  Synchronizes the stream. */
+pt_status pt_table_lookup_profile(pt_table *t, const float *d_a, int h, int w, double *d_ann, void *stream,
+                                  double *stage_ms, uint64_t *counters) {
+    if (!t || !d_a || !d_ann) return pt_fail(PT_BAD_ARG, "null argument");
+    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    cudaStream_t st = (cudaStream_t) stream;
+    LookupProfile prof;
+    PT_TRY(lookup_device(t, d_a, h, w, d_ann, st, &prof));
+    PT_CUDA(cudaStreamSynchronize(st));
+    if (stage_ms) for (int i = 0; i < LookupProfile::NSTAGES; i++) stage_ms[i] = 0;
+    for (size_t k = 1; k < prof.marks.size(); k++) {
+        float ms = 0;
+        PT_CUDA(cudaEventElapsedTime(&ms, t->events[prof.marks[k - 1].second], t->events[prof.marks[k].second]));
+        if (stage_ms) stage_ms[prof.marks[k].first] += ms;
+    }
+    if (counters) {
+        unsigned long long c[4];
+        PT_CUDA(cudaMemcpy(c, t->q_counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < 4; i++) counters[i] = c[i];
+    }
+    return PT_OK;
 }
 
 pt_status pt_table_lookup_batch(pt_table *t, int n, const float *const *a, const int *h, const int *w,

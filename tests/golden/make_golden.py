@@ -1,0 +1,95 @@
+"""Generates tests/golden/oracle_golden.json from the reference's own implementation.
+
+Runs the reference sources compiled in place (oracle/_ref/libptref.so) on seeded synthetic pairs
+and records digests of every intermediate the parity tests compare (descriptor, partition, table
+after the DT, k-coherence set, NNF) plus mean NNF distances.  The CPU tests recompute the same
+quantities with the restatement (oracle/pt_oracle.cpp) and require identical digests, which pins
+the restatement to the reference on machines where the reference cannot be built.
+
+Also records the reference's result on the repository's sample pair patchtable/vidpair0 (the pair
+of patchtable/match_ours_full.txt:4, mean_dist 0.130757 at -speed 3 with the original FLANN).
+
+Run here (needs /root/reference and a built oracle/_ref):  python tests/golden/make_golden.py
+"""
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle.oracle import Reference, mean_dist  # noqa: E402
+from patchtable_b200 import synth  # noqa: E402
+
+CASES = [
+    dict(name="tiny_64x48", h=48, w=64, seed=11, switches="-limit 1"),
+    dict(name="small_96x80_coh4", h=80, w=96, seed=12, switches="-limit 1 -coherence_spatial 4"),
+    dict(name="small_120x90_k4", h=90, w=120, seed=13, switches="-limit 1 -kcoherence 4 -prop_iters 3"),
+    dict(name="small_100x70_speed6", h=70, w=100, seed=15, switches="-speed 6 -limit 0.5"),
+    dict(name="c1_320x240", h=240, w=320, seed=1, switches=""),
+    dict(name="c1_320x240_coh4", h=240, w=320, seed=1, switches="-coherence_spatial 4"),
+]
+C2 = dict(name="c2_1920x1080_coh4", h=1080, w=1920, seed=2, switches="-speed 3 -coherence_spatial 4")
+
+
+def digest(arr) -> str:
+    return hashlib.sha256(np.ascontiguousarray(arr).tobytes()).hexdigest()
+
+
+def run_case(ref: Reference, case: dict, full: bool = True) -> dict:
+    a, b = synth.pair(case["h"], case["w"], case["seed"])
+    ref.srand(1)
+    t = ref.build(case["switches"], b)
+    ann, _ = t.lookup(a)
+    out = dict(case)
+    out["mean_dist"] = mean_dist(ann)
+    out["ann"] = digest(ann)
+    if full:
+        ns, _ = t.shape()
+        out["nslices"] = ns
+        out["add_count"] = t.add_count()
+        out["wh0"] = digest(t.wh0())
+        out["table"] = digest(t.table())
+        parts = [t.partition(d) for d in range(len(ns))]
+        out["partition"] = digest(np.concatenate([np.concatenate([p["centers"], p["lsizes"], p["rsizes"],
+                                                                  p["to_bin"].view(np.float32), [p["min"], p["max"], p["range"]]])
+                                                  for p in parts]))
+        if t.params["kcoherence"] > 0:
+            kp, kd = t.kcoherence()
+            out["kcoh_pos"] = digest(kp)
+            out["kcoh_dist"] = digest(kd)
+    return out
+
+
+def vidpair0(ref: Reference) -> dict:
+    from PIL import Image
+    base = "/root/reference/patchtable/vidpair0"
+
+    def load(fn):
+        # load_color_image for PNG: (real)(px * (1/255.0)), solver/array.h:1676-1680
+        px = np.asarray(Image.open(os.path.join(base, fn)).convert("RGB"), dtype=np.float64)
+        return (px * (1.0 / 255.0)).astype(np.float32)
+    a, b = load("a.png"), load("b.png")
+    ref.srand(1)
+    t = ref.build("-speed 3", b)
+    ann, _ = t.lookup(a)
+    return dict(name="vidpair0_speed3", h=a.shape[0], w=a.shape[1], switches="-speed 3",
+                mean_dist=mean_dist(ann), published_mean_dist=0.130757)
+
+
+def main():
+    ref = Reference()
+    res = {"cases": [run_case(ref, c) for c in CASES]}
+    res["c2"] = run_case(ref, C2, full=False)
+    res["vidpair0"] = vidpair0(ref)
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle_golden.json")
+    with open(path, "w") as f:
+        json.dump(res, f, indent=1)
+    print(json.dumps({c["name"]: c["mean_dist"] for c in res["cases"] + [res["c2"], res["vidpair0"]]}, indent=1))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,202 @@
+"""GPU path vs the CPU oracle (run with -m gpu on a B200).
+
+Bars, per the path's contract:
+  * descriptors: within 2e-6 of the channel scale of exact (float64) arithmetic, and never
+    farther from the oracle than the oracle's own float running sums are from exact arithmetic
+    (plus the same 2e-6 of scale);
+  * partition, table after the DT, k-coherence set: bit-exact given the oracle's descriptors;
+  * every NNF_DIST: bit-exact with the reference's patch_dist_exact for the returned match, and
+    within 1e-5 relative of a float64 recompute;
+  * mean NNF distance: at most 1% above the oracle's (propagation order legitimately differs).
+"""
+import importlib.util
+import json
+import os
+
+import numpy as np
+import pytest
+
+import patchtable_b200 as ptb
+from oracle.oracle import mean_dist, recompute_dists
+from patchtable_b200 import synth
+from tests.conftest import ROOT, srand_all
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.load(open(os.path.join(ROOT, "tests", "golden", "oracle_golden.json")))
+DESC_TOL = 2e-6        # of the channel's max |value|
+DIST_RTOL = 1e-5       # NNF_DIST vs float64 recompute
+MEAN_DIST_SLACK = 1.01
+
+
+def _masks():
+    spec = importlib.util.spec_from_file_location("gen", os.path.join(ROOT, "patchtable_b200", "csrc", "gen_wh_tables.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    return gen.masks(16)
+
+
+def exact_descriptor(oracle, img, ndims, nchroma, convert=True):
+    """float64 descriptor of every full patch, from the oracle's (bit-exact) YUV image."""
+    from numpy.lib.stride_tricks import sliding_window_view
+    yuv = (oracle.rgb2yuv(img) if convert else img).astype(np.float64)
+    H, W, _ = yuv.shape
+    win = sliding_window_view(yuv, (8, 8), axis=(0, 1))[:H - 7, :W - 7]
+    ms = _masks()
+    n = ndims - 2 * nchroma
+    out = np.zeros((H - 7, W - 7, ndims))
+    for k in range(n):
+        M = np.outer(*ms[k])
+        planes = range(3) if k < nchroma else [0]
+        c0 = 3 * k if k < nchroma else 3 * nchroma + (k - nchroma)
+        for j, c in enumerate(planes):
+            out[..., c0 + j] = (win[:, :, c] * M).sum(axis=(-1, -2))
+    return out
+
+
+@pytest.mark.parametrize("h,w,sw", [(240, 320, ""), (53, 37, "-ndims 8"), (8, 8, "-ndims 7"), (9, 200, "-colorspace rgb"),
+                                    (71, 66, "-ndims 4 -nchroma 0"), (130, 90, "-ndims 12 -nchroma 1")])
+def test_descriptor_accuracy(gpu, oracle, h, w, sw):
+    _, b = synth.pair(h, w, 3)
+    p = ptb.PatchTableParams(sw)
+    got = ptb.descriptor(p, b).astype(np.float64)
+    ex = exact_descriptor(oracle, b, p.ndims, p.nchroma, convert=p.convert_colorspace)
+    orc = oracle.descriptor(p.as_dict(), b)[7:h, 7:w].astype(np.float64)
+    scale = np.maximum(np.abs(ex).reshape(-1, p.ndims).max(0), 1e-30)
+    assert (np.abs(got - ex) <= DESC_TOL * scale).all()
+    assert (np.abs(got - orc) <= np.abs(orc - ex) + DESC_TOL * scale).all()
+
+
+BUILD_CASES = [c for c in GOLDEN["cases"]]
+
+
+@pytest.mark.parametrize("case", BUILD_CASES, ids=[c["name"] for c in BUILD_CASES])
+def test_build_bit_exact_given_descriptors(gpu, oracle, libc, case):
+    a, b = synth.pair(case["h"], case["w"], case["seed"])
+    p = ptb.PatchTableParams(case["switches"])
+    srand_all(libc, 1)
+    ot = oracle.build(p.as_dict(), b)
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b, wh0=ot.wh0())
+    ns, nc = gt.shape()
+    assert ns == ot.shape()[0] == case["nslices"]
+    assert gt.add_count() == ot.add_count() == case["add_count"]
+    for d in range(len(ns)):
+        po, pg = ot.partition(d), gt.partition(d)
+        for k in po:
+            assert np.array_equal(po[k], pg[k]), (d, k)
+    tg = gt.table()
+    assert np.array_equal(tg, ot.table())
+    assert (tg != (1 << 30) - 1).all()
+    if p.kcoherence > 0:
+        kg, ko = gt.kcoherence(), ot.kcoherence()
+        assert np.array_equal(kg[0], ko[0])
+        assert np.array_equal(kg[1], ko[1])
+
+
+def check_nnf(oracle, a, b, ann, sample=4000):
+    eh, ew = a.shape[0] - 7, a.shape[1] - 7
+    beh, bew = b.shape[0] - 7, b.shape[1] - 7
+    assert ann.shape == (eh, ew, 3)
+    bx, by = ann[..., 0], ann[..., 1]
+    assert (bx == np.round(bx)).all() and (by == np.round(by)).all()
+    assert (bx >= 0).all() and (bx < bew).all() and (by >= 0).all() and (by < beh).all()
+    rd = recompute_dists(a, b, ann)
+    rel = np.abs(ann[..., 2] - rd) / np.maximum(rd, 1e-12)
+    assert rel.max() <= DIST_RTOL
+    rng = np.random.default_rng(0)
+    ys = rng.integers(0, eh, sample)
+    xs = rng.integers(0, ew, sample)
+    for y, x in zip(ys, xs):
+        d = oracle.patch_dist(a, x, y, b, int(bx[y, x]), int(by[y, x]))
+        assert np.float32(ann[y, x, 2]) == np.float32(d)
+
+
+@pytest.mark.parametrize("seed,sw", [(1, ""), (2, ""), (3, "-coherence_spatial 4"), (1, "-coherence_spatial 4"),
+                                     (4, "-kcoherence 4 -prop_iters 3"), (5, "-speed 6")])
+def test_nnf_quality_and_distances(gpu, oracle, libc, seed, sw):
+    a, b = synth.pair(240, 320, seed)
+    p = ptb.PatchTableParams(sw + " -limit 10")
+    srand_all(libc, 1)
+    ot = oracle.build(p.as_dict(), b)
+    mo = mean_dist(ot.lookup(a))
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b)
+    ann = gt.lookup(a)
+    check_nnf(oracle, a, b, ann)
+    mg = mean_dist(ann)
+    assert mg <= MEAN_DIST_SLACK * mo, (mg, mo)
+
+
+def test_query_of_another_size_and_reuse(gpu, oracle, libc):
+    _, b = synth.pair(150, 170, 7)
+    p = ptb.PatchTableParams("-limit 2")
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b)
+    for (h, w, s) in [(90, 260, 8), (150, 170, 9), (33, 41, 10), (90, 260, 8)]:
+        a = synth.image_a(h, w, s)
+        ann1 = gt.lookup(a)
+        ann2 = gt.lookup(a)
+        assert np.array_equal(ann1, ann2)
+        check_nnf(oracle, a, b, ann1, sample=500)
+
+
+def test_device_lookup_matches_host(gpu, libc):
+    import torch
+    a, b = synth.pair(120, 160, 12)
+    p = ptb.PatchTableParams("-limit 2")
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b)
+    host = gt.lookup(a)
+    da = torch.from_numpy(a).to(gpu)
+    dann = torch.empty((113, 153, 3), dtype=torch.float64, device=gpu)
+    gt.lookup_device(da.data_ptr(), 120, 160, dann.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(dann.cpu().numpy(), host)
+
+
+def test_small_and_degenerate_images(gpu, libc):
+    srand_all(libc, 1)
+    for (h, w) in [(8, 8), (9, 13), (15, 200), (200, 9)]:
+        _, b = synth.pair(h, w, 31)
+        a = synth.image_a(h + 3, w + 5, 32)
+        p = ptb.PatchTableParams("-limit 0.01 -kcoherence 0")
+        gt = ptb.PatchTable(p, b)
+        ann = gt.lookup(a)
+        assert ann.shape == (h + 3 - 7, w + 5 - 7, 3)
+        assert (ann[..., 0] < w - 7).all() and (ann[..., 1] < h - 7).all()
+    with pytest.raises(ptb.PatchTableError):
+        ptb.PatchTable(ptb.PatchTableParams("-limit 0.01"), synth.pair(8, 8, 1)[1])   # k-coherence needs neighbours
+
+
+def test_constant_image(gpu, libc):
+    """Zero range in every dimension (get_bin divides 0 by 0) must still build and match."""
+    b = np.full((40, 50, 3), 0.25, np.float32)
+    a = np.full((30, 30, 3), 0.5, np.float32)
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(ptb.PatchTableParams("-limit 0.1"), b)
+    ann = gt.lookup(a)
+    assert np.allclose(ann[..., 2], 64 * 3 * 0.0625)
+
+
+@pytest.mark.parametrize("sw", ["-do_rs 1", "-spatial 1", "-dt_algo raster", "-ntables 2", "-dim_algo pca"])
+def test_unsupported_options_fail_loudly(gpu, sw):
+    _, b = synth.pair(40, 40, 1)
+    with pytest.raises(ptb.PatchTableError) as e:
+        ptb.PatchTable(ptb.PatchTableParams(sw), b)
+    assert e.value.status == 5
+
+
+def test_full_size_1920x1080(gpu, oracle, libc):
+    """The headline workload, checked through size-independent properties and the reference's
+    mean distance recorded in the golden file."""
+    g = GOLDEN["c2"]
+    a, b = synth.pair(g["h"], g["w"], g["seed"])
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(ptb.PatchTableParams(g["switches"]), b)
+    tab = gt.table()
+    assert (tab != (1 << 30) - 1).all()
+    assert ((tab & 0xFFFF) >= 7).all() and ((tab & 0xFFFF) < g["w"]).all()
+    ann = gt.lookup(a)
+    check_nnf(oracle, a, b, ann, sample=2000)
+    assert mean_dist(ann) <= MEAN_DIST_SLACK * g["mean_dist"]
