@@ -172,7 +172,7 @@ def main():
     import torch
     import torch.distributed as dist
     import patchtable_b200 as ptb
-    from oracle.oracle import mean_dist
+    from patchtable_b200.metrics import get_mean_dist as mean_dist
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
