@@ -256,7 +256,7 @@ def main():
 
     # roofline of the dominant kernel (HBM-bound accounting)
     hbm, peak_kind = peaks()
-    passes = table.params.gpu_prop_passes or (2 + 2 * table.params.prop_iters)
+    passes = table.params.gpu_prop_passes or table.params.prop_iters
     dom = max(("choose", "pull"), key=lambda k: stages[k])
     per_launch_ms = stages[dom] / (args.steps * passes)
     alg_bytes = {"pull": 56, "choose": 60}[dom] * P

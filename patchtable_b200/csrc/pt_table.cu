@@ -408,9 +408,10 @@ pt_status mark(pt_table *t, LookupProfile *prof, int stage, cudaStream_t st) {
     return PT_OK;
 }
 
+/* One choose + pull pass per reference sweep (prop_iters, patchtable.h:3608) unless overridden. */
 int default_passes(const pt_params &p) {
     if (p.gpu_prop_passes > 0) return p.gpu_prop_passes;
-    return p.prop_iters <= 0 ? 0 : 2 + 2 * p.prop_iters;
+    return p.prop_iters <= 0 ? 0 : p.prop_iters;
 }
 
 /* The device part of a lookup: a_rgb (device, h x w x 3) -> d_ann (device doubles).  With prof,
