@@ -58,8 +58,11 @@ typedef struct pt_params {
     char load_filename[PT_PATH_MAX];
     char save_filename[PT_PATH_MAX];
     /* GPU query schedule (no reference counterpart): number of parallel propagation passes
-       that replace the reference's sequential scanline sweeps; 0 picks the default. */
+       that replace the reference's sequential scanline sweeps (0 picks the default), and the
+       neighbour spacing of the first pass, halved on each later pass down to 1 (jump
+       flooding; 0 or 1 = plain neighbours). */
     int gpu_prop_passes;
+    int gpu_jump;
 } pt_params;
 
 typedef struct pt_table pt_table;
@@ -98,6 +101,13 @@ pt_status pt_table_load(const pt_params *p, const char *filename, pt_table **out
 pt_status pt_table_save(const pt_table *t, const char *filename);
 
 void pt_table_free(pt_table *t);
+
+/* The reference's table keeps a pointer to the caller's PatchTableParams (patchtable.h:1546) and
+   lookup() reads the query fields from it on every call (prop_iters, query_step, prop_dist,
+   do_prop, do_table_lookup, coherence_spatial/temporal, recalc_dist_temporal, sanitize_input,
+   triangle_factor, kcoherence_iter).  This copies those fields (and the GPU schedule fields) into
+   the table; fields that shaped the build are left unchanged. */
+pt_status pt_table_set_params(pt_table *t, const pt_params *p);
 
 /* double PatchTable<>::lookup(const Array<float> &a, Array<double> &ann,
    Array<double> *ann_prev = NULL, Array<float> *coherence_temporal_sv = NULL),

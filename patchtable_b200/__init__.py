@@ -66,6 +66,7 @@ class _Params(C.Structure):
         ("load_filename", C.c_char * PT_PATH_MAX),
         ("save_filename", C.c_char * PT_PATH_MAX),
         ("gpu_prop_passes", C.c_int),
+        ("gpu_jump", C.c_int),
     ]
 
 
@@ -94,6 +95,7 @@ def lib() -> C.CDLL:
     L.pt_table_create_with_descriptor.argtypes = [P, _f32p, C.c_int, C.c_int, _f32p, vp, C.POINTER(vp)]
     L.pt_table_free.argtypes = [vp]
     L.pt_table_free.restype = None
+    L.pt_table_set_params.argtypes = [vp, P]
     L.pt_table_lookup.argtypes = [vp, _f32p, C.c_int, C.c_int, _f64p, vp, vp, C.POINTER(C.c_double)]
     L.pt_table_lookup_device.argtypes = [vp, vp, C.c_int, C.c_int, vp, vp]
     L.pt_table_shape.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int64)]
@@ -216,14 +218,20 @@ class PatchTable:
         else:
             ann = np.empty(shape, np.float64)
         secs = C.c_double()
+        self._sync_params()
         prev = None if ann_prev is None else np.ascontiguousarray(ann_prev, np.float64).ctypes.data_as(C.c_void_p)
         sv = None if coherence_temporal_sv is None else np.ascontiguousarray(coherence_temporal_sv, np.float32).ctypes.data_as(C.c_void_p)
         _check(lib().pt_table_lookup(self._h, a, a.shape[0], a.shape[1], ann, prev, sv, C.byref(secs)))
         self.last_seconds = secs.value
         return ann
 
+    def _sync_params(self) -> None:
+        # the reference's table reads the query fields of the caller's params on every lookup
+        _check(lib().pt_table_set_params(self._h, C.byref(self.params._p)))
+
     def lookup_device(self, a_ptr: int, h: int, w: int, ann_ptr: int, stream: int = 0) -> None:
         """Device-resident lookup: a_ptr / ann_ptr are device addresses (e.g. torch data_ptr())."""
+        self._sync_params()
         _check(lib().pt_table_lookup_device(self._h, C.c_void_p(a_ptr), h, w, C.c_void_p(ann_ptr), C.c_void_p(stream)))
 
     STAGES = ("descriptor", "cells", "init", "choose", "pull", "output")
@@ -232,6 +240,7 @@ class PatchTable:
         """Device lookup with per-stage device times (ms) and SSD work counters."""
         ms = (C.c_double * 6)()
         ctr = (C.c_uint64 * 4)()
+        self._sync_params()
         _check(lib().pt_table_lookup_profile(self._h, C.c_void_p(a_ptr), h, w, C.c_void_p(ann_ptr),
                                              C.c_void_p(stream), ms, ctr))
         return dict(zip(self.STAGES, list(ms))), dict(choose_cand=ctr[0], choose_rows=ctr[1],

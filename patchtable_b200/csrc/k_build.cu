@@ -131,6 +131,17 @@ __global__ void k_cells(const BinPlan c_bins, const float *__restrict__ desc, in
     cells[p] = cell;
 }
 
+/* Table candidate of every query patch: the cell's stored patch (patchtable.h:3675-3686). */
+__global__ void k_table_cand(const BinPlan c_bins, const float *__restrict__ desc, int ds, long long P,
+                             const int *__restrict__ to_bin, const int *__restrict__ table, int *tcand) {
+    long long p = blockIdx.x * (long long) NT + threadIdx.x;
+    if (p >= P) return;
+    const float *v = desc + p * ds;
+    long long cell = 0;
+    for (int d = 0; d < c_bins.G; d++) cell += (long long) get_bin(c_bins, to_bin, d, v[d]) * c_bins.stride[d];
+    tcand[p] = __ldg(table + cell);
+}
+
 constexpr int SEG = 4096;   /* cells per block in the ordered compaction */
 
 /* Converts winning shuffle ranks to packed positions and counts seeded cells per block. */
@@ -334,6 +345,13 @@ pt_status pt_launch_populate(const PtBins &bins, const float *desc, int ds, long
 pt_status pt_launch_cells(const PtBins &bins, const float *desc, int ds, long long P, const int *to_bin,
                           long long *cells, cudaStream_t st) {
     k_cells<<<blocks_for(P), NT, 0, st>>>(bin_plan(bins), desc, ds, P, to_bin, cells);
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_table_candidates(const PtBins &bins, const float *desc, int ds, long long P, const int *to_bin,
+                                     const int *table, int *tcand, cudaStream_t st) {
+    k_table_cand<<<blocks_for(P), NT, 0, st>>>(bin_plan(bins), desc, ds, P, to_bin, table, tcand);
     PT_LAUNCHED();
     return PT_OK;
 }

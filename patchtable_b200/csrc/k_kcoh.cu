@@ -14,8 +14,9 @@
    vector; the only state that crosses a segment boundary is one flag bit, which is resolved by a
    scan over segments after each segment has been evaluated for both values of that bit.
 
-   The nearest-neighbour search is exact, ranked by (float squared L2 summed in dimension order
-   without fused operations, point index); FLANN's approximate tree is not reproduced. */
+   The nearest-neighbour search (k_knn.cu) is exact, ranked by (float squared L2 summed in
+   dimension order without fused operations, point index); FLANN's approximate tree is not
+   reproduced. */
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
@@ -23,57 +24,6 @@
 #include "pt_kernels.h"
 
 namespace {
-
-constexpr int NT = 128;
-
-/* Squared descriptor distance in the ranking's order. */
-__device__ __forceinline__ float knn_dist(const float *q, const float *p, int nd) {
-    float s = 0.f;
-    for (int i = 0; i < nd; i++) {
-        float t = __fsub_rn(q[i], p[i]);
-        s = __fadd_rn(s, __fmul_rn(t, t));
-    }
-    return s;
-}
-
-/* Exact top-K by (dist, index) of every query among all train points; brute force over tiles
-   of train points staged in shared memory, visited in increasing index order. */
-template<int K>
-__global__ void __launch_bounds__(NT)
-k_knn_brute(const float *__restrict__ train, int N, int nd, const float *__restrict__ qdesc, int Q, int *out) {
-    constexpr int TILE = 512;
-    __shared__ float tp[TILE * PT_DESC_MAX];
-    int q = blockIdx.x * NT + threadIdx.x;
-    float qv[PT_DESC_MAX];
-    float kd[K];
-    int ki[K];
-#pragma unroll
-    for (int t = 0; t < K; t++) { kd[t] = __int_as_float(0x7f800000); ki[t] = -1; }
-    if (q < Q)
-        for (int i = 0; i < nd; i++) qv[i] = qdesc[(size_t) q * nd + i];
-    for (int base = 0; base < N; base += TILE) {
-        int cnt = min(TILE, N - base);
-        __syncthreads();
-        for (int i = threadIdx.x; i < cnt * nd; i += NT) tp[i] = train[(size_t) base * nd + i];
-        __syncthreads();
-        if (q >= Q) continue;
-        for (int j = 0; j < cnt; j++) {
-            float d = knn_dist(qv, tp + j * nd, nd);
-            if (d < kd[K - 1]) {
-                int idx = base + j;
-#pragma unroll
-                for (int t = K - 1; t >= 0; t--) {
-                    if (kd[t] > d) {
-                        if (t > 0 && kd[t - 1] > d) { kd[t] = kd[t - 1]; ki[t] = ki[t - 1]; }
-                        else { kd[t] = d; ki[t] = idx; }
-                    }
-                }
-            }
-        }
-    }
-    if (q < Q)
-        for (int t = 0; t < K; t++) out[(size_t) q * K + t] = ki[t];
-}
 
 /* Copies descriptor rows (ds-strided records) of the listed patches into a compact n x nd array. */
 __global__ void k_gather_rows(const float *__restrict__ desc, int ds, int nd, const int *__restrict__ rows, int n,
@@ -305,16 +255,4 @@ pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *train, int N,
         PT_CUDA(cudaStreamSynchronize(st));
         return PT_OK;
     }
-}
-
-pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, int Q, int K, int *out, cudaStream_t st) {
-    dim3 grid((Q + NT - 1) / NT);
-    switch (K) {
-        case 16: k_knn_brute<16><<<grid, NT, 0, st>>>(train, N, nd, qdesc, Q, out); break;
-        case 32: k_knn_brute<32><<<grid, NT, 0, st>>>(train, N, nd, qdesc, Q, out); break;
-        case 64: k_knn_brute<64><<<grid, NT, 0, st>>>(train, N, nd, qdesc, Q, out); break;
-        default: return pt_fail(PT_UNSUPPORTED, "knn K=%d", K);
-    }
-    PT_LAUNCHED();
-    return PT_OK;
 }

@@ -1,0 +1,235 @@
+/* Exact k-nearest-neighbour search in descriptor space for the k-coherence step.
+
+   Ranking (shared with the CPU oracle): squared L2 in float, dimensions summed in index order,
+   each product and sum rounded (no fused operations); ties by the smaller point index.
+
+   Structure: train points are sorted by a Morton code of their quantised descriptor, cut into
+   buckets of 32 consecutive points, and a complete binary tree of axis-aligned bounding boxes is
+   built over the buckets (implicit heap layout, one launch per level).  Each query thread
+   descends the tree depth first, nearer child first, and skips a subtree only when the box's
+   lower bound exceeds the current k-th distance by more than the float rounding of a distance
+   could account for -- so the result equals an exhaustive search.  Queries are processed in
+   Morton order so the threads of a warp walk similar paths. */
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include "pt_internal.h"
+#include "pt_kernels.h"
+
+namespace {
+
+constexpr int NT = 128;
+constexpr int BUCKET = 32;
+
+__device__ __forceinline__ float knn_dist(const float *q, const float *p, int nd) {
+    float s = 0.f;
+    for (int i = 0; i < nd; i++) {
+        float t = __fsub_rn(q[i], p[i]);
+        s = __fadd_rn(s, __fmul_rn(t, t));
+    }
+    return s;
+}
+
+__global__ void k_range(const float *__restrict__ pts, int N, int nd, float *mn, float *mx) {
+    __shared__ float smin[PT_DESC_MAX][NT], smax[PT_DESC_MAX][NT];
+    float a[PT_DESC_MAX], b[PT_DESC_MAX];
+    for (int d = 0; d < nd; d++) { a[d] = __int_as_float(0x7f800000); b[d] = -__int_as_float(0x7f800000); }
+    for (int i = blockIdx.x * NT + threadIdx.x; i < N; i += gridDim.x * NT)
+        for (int d = 0; d < nd; d++) { float v = pts[(size_t) i * nd + d]; a[d] = fminf(a[d], v); b[d] = fmaxf(b[d], v); }
+    for (int d = 0; d < nd; d++) { smin[d][threadIdx.x] = a[d]; smax[d][threadIdx.x] = b[d]; }
+    __syncthreads();
+    if (threadIdx.x < nd) {
+        int d = threadIdx.x;
+        float u = smin[d][0], v = smax[d][0];
+        for (int i = 1; i < NT; i++) { u = fminf(u, smin[d][i]); v = fmaxf(v, smax[d][i]); }
+        mn[blockIdx.x * PT_DESC_MAX + d] = u;
+        mx[blockIdx.x * PT_DESC_MAX + d] = v;
+    }
+}
+
+struct Quant {
+    int nd, bits;
+    float mn[PT_DESC_MAX], scale[PT_DESC_MAX];
+};
+
+__global__ void k_morton(const Quant qz, const float *__restrict__ pts, int N, unsigned long long *codes, int *idx) {
+    int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= N) return;
+    unsigned q[PT_DESC_MAX];
+    const unsigned top = (1u << qz.bits) - 1;
+    for (int d = 0; d < qz.nd; d++) {
+        float t = (pts[(size_t) i * qz.nd + d] - qz.mn[d]) * qz.scale[d];
+        t = fminf(fmaxf(t, 0.f), (float) top);
+        q[d] = (unsigned) t;
+    }
+    unsigned long long c = 0;
+    for (int b = qz.bits - 1; b >= 0; b--)
+        for (int d = 0; d < qz.nd; d++) c = (c << 1) | ((q[d] >> b) & 1u);
+    codes[i] = c;
+    idx[i] = i;
+}
+
+__global__ void k_reorder(const float *__restrict__ pts, int N, int nd, const int *__restrict__ perm, float *sp) {
+    long long t = blockIdx.x * 256ll + threadIdx.x;
+    if (t >= (long long) N * nd) return;
+    int i = (int) (t / nd), d = (int) (t % nd);
+    sp[t] = pts[(size_t) perm[i] * nd + d];
+}
+
+/* Leaf boxes (heap nodes L .. 2L-1); empty leaves get an inverted box. */
+__global__ void k_leaf_box(const float *__restrict__ sp, int N, int nd, int L, float *lo, float *hi) {
+    int j = blockIdx.x * 256 + threadIdx.x;
+    if (j >= L) return;
+    int node = L + j;
+    for (int d = 0; d < nd; d++) {
+        float a = __int_as_float(0x7f800000), b = -__int_as_float(0x7f800000);
+        for (int i = j * BUCKET; i < min(N, (j + 1) * BUCKET); i++) { float v = sp[(size_t) i * nd + d]; a = fminf(a, v); b = fmaxf(b, v); }
+        lo[(size_t) node * nd + d] = a;
+        hi[(size_t) node * nd + d] = b;
+    }
+}
+
+__global__ void k_inner_box(int first, int count, int nd, float *lo, float *hi) {
+    int j = blockIdx.x * 256 + threadIdx.x;
+    if (j >= count) return;
+    int node = first + j;
+    for (int d = 0; d < nd; d++) {
+        lo[(size_t) node * nd + d] = fminf(lo[(size_t) (2 * node) * nd + d], lo[(size_t) (2 * node + 1) * nd + d]);
+        hi[(size_t) node * nd + d] = fmaxf(hi[(size_t) (2 * node) * nd + d], hi[(size_t) (2 * node + 1) * nd + d]);
+    }
+}
+
+/* Squared distance from q to a box, rounded down enough to be a lower bound of knn_dist. */
+__device__ __forceinline__ float box_lb(const float *q, const float *lo, const float *hi, int nd) {
+    float s = 0.f;
+    for (int d = 0; d < nd; d++) {
+        float e = fmaxf(fmaxf(lo[d] - q[d], q[d] - hi[d]), 0.f);
+        s += e * e;
+    }
+    return s * (1.0f - 1e-5f);
+}
+
+__device__ __forceinline__ bool before(float d, int i, float d2, int i2) { return d < d2 || (d == d2 && i < i2); }
+
+template<int K>
+__global__ void __launch_bounds__(NT)
+k_knn_tree(const float *__restrict__ sp, const int *__restrict__ sidx, int N, int nd, int L,
+           const float *__restrict__ lo, const float *__restrict__ hi, const float *__restrict__ qdesc,
+           const int *__restrict__ qorder, int Q, int *out) {
+    int t = blockIdx.x * NT + threadIdx.x;
+    if (t >= Q) return;
+    int q = qorder[t];
+    float qv[PT_DESC_MAX];
+    for (int d = 0; d < nd; d++) qv[d] = qdesc[(size_t) q * nd + d];
+    float kd[K];
+    int ki[K];
+#pragma unroll
+    for (int j = 0; j < K; j++) { kd[j] = __int_as_float(0x7f800000); ki[j] = 0x7fffffff; }
+    int stack[48];
+    int sp_top = 0;
+    stack[sp_top++] = 1;
+    while (sp_top > 0) {
+        int node = stack[--sp_top];
+        if (box_lb(qv, lo + (size_t) node * nd, hi + (size_t) node * nd, nd) > kd[K - 1]) continue;
+        if (node >= L) {
+            int j = node - L;
+            int i1 = min(N, (j + 1) * BUCKET);
+            for (int i = j * BUCKET; i < i1; i++) {
+                float d = knn_dist(qv, sp + (size_t) i * nd, nd);
+                int id = sidx[i];
+                if (!before(d, id, kd[K - 1], ki[K - 1])) continue;
+#pragma unroll
+                for (int s = K - 1; s >= 0; s--) {
+                    if (before(d, id, kd[s], ki[s])) {
+                        if (s > 0 && before(d, id, kd[s - 1], ki[s - 1])) { kd[s] = kd[s - 1]; ki[s] = ki[s - 1]; }
+                        else { kd[s] = d; ki[s] = id; }
+                    }
+                }
+            }
+            continue;
+        }
+        int c0 = 2 * node, c1 = 2 * node + 1;
+        float l0 = box_lb(qv, lo + (size_t) c0 * nd, hi + (size_t) c0 * nd, nd);
+        float l1 = box_lb(qv, lo + (size_t) c1 * nd, hi + (size_t) c1 * nd, nd);
+        if (sp_top + 2 > 48) continue;           /* cannot happen: depth <= 31 */
+        if (l0 <= l1) { stack[sp_top++] = c1; stack[sp_top++] = c0; }
+        else { stack[sp_top++] = c0; stack[sp_top++] = c1; }
+    }
+    for (int j = 0; j < K; j++) out[(size_t) q * K + j] = ki[j] == 0x7fffffff ? -1 : ki[j];
+}
+
+}  // namespace
+
+/* Exact top-K (K in {16, 32, 64}) train indices of every query, ascending (dist, index). */
+pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, int Q, int K, int *out, cudaStream_t st) {
+    if (N < 1 || Q < 1) return PT_OK;
+    if (nd < 1 || nd > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "knn: %d dims", nd);
+    /* range of the train points */
+    const int NB = 148;
+    DevBuf<float> pmn, pmx;
+    PT_CUDA(pmn.reserve(NB * PT_DESC_MAX));
+    PT_CUDA(pmx.reserve(NB * PT_DESC_MAX));
+    k_range<<<NB, NT, 0, st>>>(train, N, nd, pmn.p, pmx.p);
+    PT_LAUNCHED();
+    std::vector<float> a(NB * PT_DESC_MAX), b(NB * PT_DESC_MAX);
+    PT_CUDA(cudaMemcpyAsync(a.data(), pmn.p, sizeof(float) * a.size(), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaMemcpyAsync(b.data(), pmx.p, sizeof(float) * b.size(), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaStreamSynchronize(st));
+    Quant qz;
+    memset(&qz, 0, sizeof(qz));
+    qz.nd = nd;
+    qz.bits = std::min(10, 63 / nd);
+    for (int d = 0; d < nd; d++) {
+        float mn = a[d], mx = b[d];
+        for (int i = 1; i < NB; i++) { mn = std::min(mn, a[i * PT_DESC_MAX + d]); mx = std::max(mx, b[i * PT_DESC_MAX + d]); }
+        qz.mn[d] = mn;
+        qz.scale[d] = mx > mn ? (float) ((1u << qz.bits) - 1) / (mx - mn) : 0.f;
+    }
+    /* sort train points and queries by Morton code */
+    DevBuf<unsigned long long> codes, codes2;
+    DevBuf<int> idx, perm, qidx, qorder, sidx;
+    DevBuf<float> sp;
+    PT_CUDA(codes.reserve(std::max(N, Q)));
+    PT_CUDA(codes2.reserve(std::max(N, Q)));
+    PT_CUDA(idx.reserve(std::max(N, Q)));
+    PT_CUDA(perm.reserve(N));
+    PT_CUDA(qorder.reserve(Q));
+    PT_CUDA(sp.reserve((size_t) N * nd));
+    size_t tb = 0;
+    PT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, codes.p, codes2.p, idx.p, perm.p, std::max(N, Q), 0, 64, st));
+    DevBuf<unsigned char> tmp;
+    PT_CUDA(tmp.reserve(tb));
+    k_morton<<<(N + 255) / 256, 256, 0, st>>>(qz, train, N, codes.p, idx.p);
+    PT_LAUNCHED();
+    PT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, codes.p, codes2.p, idx.p, perm.p, N, 0, 64, st));
+    pt_count_launches(4);
+    k_morton<<<(Q + 255) / 256, 256, 0, st>>>(qz, qdesc, Q, codes.p, idx.p);
+    PT_LAUNCHED();
+    PT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, codes.p, codes2.p, idx.p, qorder.p, Q, 0, 64, st));
+    pt_count_launches(4);
+    k_reorder<<<(unsigned) (((long long) N * nd + 255) / 256), 256, 0, st>>>(train, N, nd, perm.p, sp.p);
+    PT_LAUNCHED();
+    /* bucket boxes and the tree above them */
+    int nbk = (N + BUCKET - 1) / BUCKET;
+    int L = 1;
+    while (L < nbk) L <<= 1;
+    DevBuf<float> lo, hi;
+    PT_CUDA(lo.reserve((size_t) 2 * L * nd));
+    PT_CUDA(hi.reserve((size_t) 2 * L * nd));
+    k_leaf_box<<<(L + 255) / 256, 256, 0, st>>>(sp.p, N, nd, L, lo.p, hi.p);
+    PT_LAUNCHED();
+    for (int first = L / 2; first >= 1; first /= 2) {
+        k_inner_box<<<(first + 255) / 256, 256, 0, st>>>(first, first, nd, lo.p, hi.p);
+        PT_LAUNCHED();
+    }
+    dim3 grid((Q + NT - 1) / NT);
+    switch (K) {
+        case 16: k_knn_tree<16><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
+        case 32: k_knn_tree<32><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
+        case 64: k_knn_tree<64><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
+        default: return pt_fail(PT_UNSUPPORTED, "knn K=%d", K);
+    }
+    PT_LAUNCHED();
+    PT_CUDA(cudaStreamSynchronize(st));
+    return PT_OK;
+}

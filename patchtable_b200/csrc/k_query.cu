@@ -33,6 +33,7 @@ struct QPlan {
     int kc, ks;              /* kcoherence, kcoherence_step */
     int radius;              /* query_step + prop_dist */
     int do_kcoh;
+    int step;                /* neighbour spacing of this pull pass (jump flooding) */
 };
 
 __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
@@ -74,8 +75,8 @@ __device__ __forceinline__ void count_work(unsigned long long *counters, unsigne
 /* Steps 1-3 for every patch: returns the chosen match and its exact distance. */
 __global__ void __launch_bounds__(NT)
 k_choose(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
-         const float *__restrict__ cur_d, const long long *__restrict__ cells, const int *__restrict__ table,
-         const int2 *__restrict__ kcoh, int do_table, int *ch_pos, float *ch_d, unsigned long long *counters) {
+         const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
+         int *ch_pos, float *ch_d, unsigned long long *counters) {
     int p = blockIdx.x * NT + threadIdx.x;
     const bool live = p < c_q.ew * c_q.eh;
     unsigned ne = 0, rows = 0;
@@ -87,7 +88,7 @@ k_choose(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict
     float dbest = (float) ((double) dstore * c_q.prop_scale);
     float dch = dstore;          /* exact distance of the chosen match */
     if (do_table) {
-        int v = table[cells[p]];
+        int v = tcand[p];
         int xs = pt_x(v) - 7, ys = pt_y(v) - 7;
         if (xs != xb || ys != yb) {
             float dc = ssd_bounded(a, c_q.aw, x, y, b, c_q.bw, xs, ys, dbest, rows);
@@ -119,7 +120,83 @@ k_choose(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict
 }
 
 /* Step 4 as a pull: the best of the stored match and every neighbour's chosen offset applied
-   to this patch. */
+   to this patch.  Neighbours sit `step` patches apart; passes with decreasing steps (jump
+   flooding) carry an offset across a region in a logarithmic number of passes, where the
+   reference's sequential sweep carries it along a whole row in one sweep.  The patch's own choice is taken first (its exact distance is known), then the
+   distinct neighbour candidates are evaluated row by row together, so each row of the query
+   patch is loaded once for all of them.  Every candidate's sum keeps the reference's order, and
+   candidates are accepted in neighbour order with a strict comparison, as a sequential loop
+   would; a candidate stops as soon as its partial sum reaches the best distance known before
+   the rows start. */
+template<int R>
+__device__ __forceinline__ void pull_patch(const QPlan &c_q, const float4 *__restrict__ a, const float4 *__restrict__ b,
+                                           int x, int y, int &bpos, float &bd, const int *__restrict__ ch_pos,
+                                           const float *__restrict__ ch_d, unsigned &ne, unsigned &rows) {
+    constexpr int MAXC = (2 * R + 1) * (2 * R + 1) - 1;
+    const int S = c_q.step;
+    {
+        int q = y * c_q.ew + x;
+        int cp = ch_pos[q];
+        if (pt_x(cp) < c_q.bew && pt_y(cp) < c_q.beh && cp != bpos && ch_d[q] < bd) { bd = ch_d[q]; bpos = cp; }
+    }
+    int cand[MAXC];
+    int nc = 0;
+#pragma unroll
+    for (int dy = -R; dy <= R; dy++) {
+#pragma unroll
+        for (int dx = -R; dx <= R; dx++) {
+            if (dx == 0 && dy == 0) continue;
+            int ny = y + S * dy, nx = x + S * dx;
+            if (ny < 0 || ny >= c_q.eh || nx < 0 || nx >= c_q.ew) continue;
+            int cp = ch_pos[ny * c_q.ew + nx];
+            int xs = pt_x(cp) - S * dx, ys = pt_y(cp) - S * dy;
+            if (xs < 0 || ys < 0 || xs >= c_q.bew || ys >= c_q.beh) continue;
+            int c = pt_xy(xs, ys);
+            bool dup = c == bpos;
+            for (int t = 0; t < nc; t++) dup |= cand[t] == c;
+            if (!dup) cand[nc++] = c;
+        }
+    }
+    if (nc == 0) return;
+    ne += nc;
+    float l[MAXC][4];
+#pragma unroll
+    for (int c = 0; c < MAXC; c++) { l[c][0] = l[c][1] = l[c][2] = l[c][3] = 0.f; }
+    unsigned active = (1u << nc) - 1u;
+    const float bound = bd;
+    for (int dy = 0; dy < 8 && active; dy++) {
+        const float4 *ar = a + (size_t) (y + dy) * c_q.aw + x;
+        float4 av[8];
+#pragma unroll
+        for (int p = 0; p < 8; p++) av[p] = __ldg(ar + p);
+#pragma unroll
+        for (int c = 0; c < MAXC; c++) {
+            if (!((active >> c) & 1u)) continue;
+            rows++;
+            const float4 *br = b + (size_t) (pt_y(cand[c]) + dy) * c_q.bw + pt_x(cand[c]);
+            float e[24];
+#pragma unroll
+            for (int p = 0; p < 8; p++) {
+                float4 bv = __ldg(br + p);
+                float t0 = __fsub_rn(av[p].x, bv.x), t1 = __fsub_rn(av[p].y, bv.y), t2 = __fsub_rn(av[p].z, bv.z);
+                e[3 * p] = __fmul_rn(t0, t0); e[3 * p + 1] = __fmul_rn(t1, t1); e[3 * p + 2] = __fmul_rn(t2, t2);
+            }
+#pragma unroll
+            for (int n = 0; n < 6; n++) {
+                l[c][0] = __fadd_rn(l[c][0], e[4 * n]); l[c][1] = __fadd_rn(l[c][1], e[4 * n + 1]);
+                l[c][2] = __fadd_rn(l[c][2], e[4 * n + 2]); l[c][3] = __fadd_rn(l[c][3], e[4 * n + 3]);
+            }
+            if (dy < 7 && __fadd_rn(__fadd_rn(__fadd_rn(l[c][0], l[c][1]), l[c][2]), l[c][3]) >= bound) active &= ~(1u << c);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < MAXC; c++) {
+        if (!((active >> c) & 1u)) continue;
+        float d = __fadd_rn(__fadd_rn(__fadd_rn(l[c][0], l[c][1]), l[c][2]), l[c][3]);
+        if (d < bd) { bd = d; bpos = cand[c]; }
+    }
+}
+
 __global__ void __launch_bounds__(NT)
 k_pull(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
        const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
@@ -128,35 +205,13 @@ k_pull(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__
     const bool live = p < c_q.ew * c_q.eh;
     unsigned ne = 0, rows = 0;
     if (live) {
-    int x = p % c_q.ew, y = p / c_q.ew;
-    int bpos = cur_pos[p];
-    float bd = cur_d[p];
-    const int R = c_q.radius;
-    int tried[25];
-    int ntried = 0;
-    for (int dy = -R; dy <= R; dy++) {
-        int ny = y + dy;
-        if (ny < 0 || ny >= c_q.eh) continue;
-        for (int dx = -R; dx <= R; dx++) {
-            int nx = x + dx;
-            if (nx < 0 || nx >= c_q.ew) continue;
-            int q = ny * c_q.ew + nx;
-            int cp = ch_pos[q];
-            int xs = pt_x(cp) - dx, ys = pt_y(cp) - dy;
-            if (xs < 0 || ys < 0 || xs >= c_q.bew || ys >= c_q.beh) continue;
-            int cand = pt_xy(xs, ys);
-            if (cand == bpos) continue;
-            bool dup = false;
-            for (int t = 0; t < ntried; t++) dup |= tried[t] == cand;
-            if (dup) continue;
-            if (ntried < 25) tried[ntried++] = cand;
-            float dc = (dx == 0 && dy == 0) ? ch_d[q] : ssd_bounded(a, c_q.aw, x, y, b, c_q.bw, xs, ys, bd, rows);
-            ne += (dx != 0 || dy != 0);
-            if (dc < bd) { bd = dc; bpos = cand; }
-        }
-    }
-    nxt_pos[p] = bpos;
-    nxt_d[p] = bd;
+        int x = p % c_q.ew, y = p / c_q.ew;
+        int bpos = cur_pos[p];
+        float bd = cur_d[p];
+        if (c_q.radius <= 1) pull_patch<1>(c_q, a, b, x, y, bpos, bd, ch_pos, ch_d, ne, rows);
+        else pull_patch<2>(c_q, a, b, x, y, bpos, bd, ch_pos, ch_d, ne, rows);
+        nxt_pos[p] = bpos;
+        nxt_d[p] = bd;
     }
     count_work(counters, ne, rows);
 }
@@ -187,6 +242,7 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     q.ks = s.kcoherence_step;
     q.radius = s.radius;
     q.do_kcoh = s.kcoherence > 0;
+    q.step = s.step < 1 ? 1 : s.step;
     if (q.radius > 2) return pt_fail(PT_UNSUPPORTED, "propagation radius %d > 2 on the GPU path", q.radius);
     return PT_OK;
 }
@@ -198,11 +254,11 @@ pt_status pt_launch_init(int n, int pos, float d, int *cur_pos, float *cur_d, cu
 }
 
 pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
-                           const long long *cells, const int *table, const int2 *kcoh, int do_table, int *ch_pos,
+                           const int *tcand, const int2 *kcoh, int do_table, int *ch_pos,
                            float *ch_d, unsigned long long *evals, cudaStream_t st) {
     QPlan q;
     PT_TRY(make_qplan(s, q));
-    k_choose<<<(n + NT - 1) / NT, NT, 0, st>>>(q, a, b, cur_pos, cur_d, cells, table, kcoh, do_table, ch_pos, ch_d, evals);
+    k_choose<<<(n + NT - 1) / NT, NT, 0, st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, evals);
     PT_LAUNCHED();
     return PT_OK;
 }

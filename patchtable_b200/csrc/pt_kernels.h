@@ -29,6 +29,9 @@ pt_status pt_launch_populate(const PtBins &bins, const float *desc, int ds, long
                              const int *to_bin, int *table, cudaStream_t st);
 pt_status pt_launch_cells(const PtBins &bins, const float *desc, int ds, long long P, const int *to_bin,
                           long long *cells, cudaStream_t st);
+/* Table entry of every query patch's cell (patchtable.h:3675-3686): tcand[p] = table[cell(p)]. */
+pt_status pt_launch_table_candidates(const PtBins &bins, const float *desc, int ds, long long P, const int *to_bin,
+                                     const int *table, int *tcand, cudaStream_t st);
 pt_status pt_dt_prop(int *table, long long ncells, const int *order_xy, int G, const int *nslices,
                      const long long *stride, int dt_iters, int run, long long *seeded, int *levels_out,
                      cudaStream_t st);
@@ -46,13 +49,33 @@ struct QuerySetup {
     int aw, ah, bw, bh;
     double prop_scale, triangle_factor;
     int kcoherence, kcoherence_step, radius;
+    int step = 1;            /* neighbour spacing of a pull pass */
     cudaStream_t stream;
 };
+/* Neighbour spacing of pull pass i of n: halving from `jump` down to 1, then 1. */
+inline int pt_pass_step(int i, int n, int jump) {
+    (void) n;
+    int s = jump > 1 ? jump : 1;
+    for (int k = 0; k < i && s > 1; k++) s /= 2;
+    return s;
+}
 pt_status pt_launch_init(int n, int pos, float d, int *cur_pos, float *cur_d, cudaStream_t st);
 pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
-                           const long long *cells, const int *table, const int2 *kcoh, int do_table, int *ch_pos,
+                           const int *tcand, const int2 *kcoh, int do_table, int *ch_pos,
                            float *ch_d, unsigned long long *evals, cudaStream_t st);
 pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
                          const int *ch_pos, const float *ch_d, int *nxt_pos, float *nxt_d,
                          unsigned long long *evals, cudaStream_t st);
 pt_status pt_launch_output(int n, const int *pos, const float *d, double *ann, cudaStream_t st);
+
+/* Read-only view of a built table, for entry points outside pt_table.cu. */
+struct PtTableView {
+    pt_params p;
+    int h, w, ds;
+    const float4 *b_rgba;
+    const int *table;
+    const int *to_bin;
+    const int2 *kcoh;
+    PtBins bins;
+};
+pt_status pt_table_view(const pt_table *t, PtTableView *v);

@@ -99,7 +99,7 @@ struct pt_table {
     DevBuf<float> q_rgb;
     DevBuf<float4> q_rgba;
     DevBuf<float> q_desc;
-    DevBuf<long long> q_cells;
+    DevBuf<int> q_tcand;
     DevBuf<int> q_pos[2], q_chpos;
     DevBuf<float> q_d[2], q_chd;
     DevBuf<double> q_ann;
@@ -380,7 +380,7 @@ pt_status ensure_query_buffers(pt_table *t, int h, int w) {
     PT_CUDA(t->q_rgb.reserve((size_t) h * w * 3));
     PT_CUDA(t->q_rgba.reserve((size_t) h * w));
     PT_CUDA(t->q_desc.reserve((size_t) P * t->ds));
-    PT_CUDA(t->q_cells.reserve(P));
+    PT_CUDA(t->q_tcand.reserve(P));
     for (int k = 0; k < 2; k++) { PT_CUDA(t->q_pos[k].reserve(P)); PT_CUDA(t->q_d[k].reserve(P)); }
     PT_CUDA(t->q_chpos.reserve(P));
     PT_CUDA(t->q_chd.reserve(P));
@@ -429,7 +429,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, a_rgb, h, w, p.convert_colorspace, t->q_rgba.p, t->q_desc.p,
                                 t->ds, st));
     PT_TRY(mark(t, prof, LookupProfile::DESC, st));
-    PT_TRY(pt_launch_cells(t->bins, t->q_desc.p, t->ds, P, t->to_bin.p, t->q_cells.p, st));
+    PT_TRY(pt_launch_table_candidates(t->bins, t->q_desc.p, t->ds, P, t->to_bin.p, t->table.p, t->q_tcand.p, st));
     PT_TRY(mark(t, prof, LookupProfile::CELLS, st));
     QuerySetup qs;
     qs.aw = w; qs.ah = h; qs.bw = t->w; qs.bh = t->h;
@@ -451,11 +451,13 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
         bool do_table = i == 0 && p.do_table_lookup;
         QuerySetup qi = qs;
         if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
-        PT_TRY(pt_launch_choose(qi, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_cells.p,
-                                t->table.p, t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, ctr, st));
+        PT_TRY(pt_launch_choose(qi, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_tcand.p,
+                                t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, ctr, st));
         PT_TRY(mark(t, prof, LookupProfile::CHOOSE, st));
         if (p.do_prop) {
-            PT_TRY(pt_launch_pull(qs, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_chpos.p,
+            QuerySetup qp = qs;
+            qp.step = pt_pass_step(i, passes, p.gpu_jump);
+            PT_TRY(pt_launch_pull(qp, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_chpos.p,
                                   t->q_chd.p, t->q_pos[1 - cur].p, t->q_d[1 - cur].p, ctr ? ctr + 2 : nullptr, st));
             PT_TRY(mark(t, prof, LookupProfile::PULL, st));
             cur = 1 - cur;
@@ -597,6 +599,27 @@ pt_status pt_table_get_kcoherence(const pt_table *t, int32_t *pos, float *dist) 
 
 int64_t pt_table_add_count(const pt_table *t) { return t ? t->add_count : -1; }
 
+pt_status pt_table_set_params(pt_table *t, const pt_params *p) {
+    if (!t || !p) return pt_fail(PT_BAD_ARG, "null argument");
+    pt_params &q = t->p;
+    q.prop_iters = p->prop_iters;
+    q.query_step = p->query_step;
+    q.prop_dist = p->prop_dist;
+    q.do_prop = p->do_prop;
+    q.do_table_lookup = p->do_table_lookup;
+    q.coherence_spatial = p->coherence_spatial;
+    q.coherence_temporal = p->coherence_temporal;
+    q.recalc_dist_temporal = p->recalc_dist_temporal;
+    q.sanitize_input = p->sanitize_input;
+    q.triangle_factor = p->triangle_factor;
+    q.kcoherence_iter = p->kcoherence_iter;
+    q.gpu_prop_passes = p->gpu_prop_passes;
+    q.gpu_jump = p->gpu_jump;
+    if (p->do_rs || p->spatial || p->init_random)
+        return pt_fail(PT_UNSUPPORTED, "random/spatial search and init_random are not implemented on the GPU path");
+    return PT_OK;
+}
+
 pt_status pt_descriptor(const pt_params *p, const float *rgb, int h, int w, float *out) {
     PT_TRY(check_params(p, h, w));
     long long P = (long long) (h - 7) * (w - 7);
@@ -624,6 +647,23 @@ pt_status pt_table_load(const pt_params *p, const char *filename, pt_table **out
 }
 
 int64_t pt_kernel_launch_count(void) { return g_launches; }
+
+}  // extern "C"
+
+pt_status pt_table_view(const pt_table *t, PtTableView *v) {
+    if (!t || !v) return pt_fail(PT_BAD_ARG, "null argument");
+    v->p = t->p;
+    v->h = t->h; v->w = t->w; v->ds = t->ds;
+    v->b_rgba = t->b_rgba.p;
+    v->table = t->table.p;
+    v->to_bin = t->to_bin.p;
+    v->kcoh = t->kcoh.p;
+    v->bins = t->bins;
+    return PT_OK;
+}
+
+extern "C" {
+
 void pt_kernel_launch_count_reset(void) { g_launches = 0; }
 
 const char *pt_last_error(void) { return g_last_error.c_str(); }
