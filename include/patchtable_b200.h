@@ -125,6 +125,18 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int h, int w, double *ann
 pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int h, int w, double *d_ann,
                                  void *stream);
 
+/* Zero-allocation form of pt_table_lookup_device (no counterpart in the reference).  For
+   callers that may not allocate device memory during queries -- a frame loop with a fixed
+   latency budget (cudaMalloc/cudaFree synchronise the device), or an application whose own
+   allocator owns the GPU's memory -- every intermediate buffer comes from one 19 MiB file-scope
+   device array instead of cudaMalloc.  Limits: at most PT_NOALLOC_MAX_PIXELS query pixels and
+   ndims <= 8 (PT_BAD_ARG / PT_UNSUPPORTED otherwise).  All calls share that array, so calls
+   that overlap on the GPU race and must be serialised.  The first call on a device resolves the
+   array's address (cudaGetSymbolAddress) and should come before any stream capture. */
+#define PT_NOALLOC_MAX_PIXELS (1 << 18)
+pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_a, int h, int w, double *d_ann,
+                                         void *stream);
+
 /* Batched query (no reference counterpart; the reference matches one image per lookup() call,
    patchtable.h:4448): n query images of individual sizes against one table, in one persistent
    launch over the flattened patch index.  a[i] / ann_out[i] are host buffers with the
