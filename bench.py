@@ -36,6 +36,18 @@ WORKLOAD = dict(name="synthetic 1920x1080 match, -speed 3 -coherence_spatial 4",
 METRIC = "query patches/s at matched mean NNF dist (learned vs plain, 1 B200); build s"
 UNIT = "patches/s"
 L2_FLUSH_BYTES = 256 << 20
+# query schedules (passes, first jump) in increasing cost; the bench times the first whose mean NNF
+# distance is within 1% of the reference's on this workload ("matched mean NNF dist")
+SCHEDULES = [(1, 1), (2, 2), (3, 4), (4, 8), (6, 8)]
+
+
+def reference_mean_dist():
+    """Mean NNF distance of the reference (oracle/_ref, 1 thread) on this workload, recorded by
+    tests/golden/make_golden.py."""
+    with open(os.path.join(ROOT, "tests", "golden", "oracle_golden.json")) as f:
+        g = json.load(f)["c2"]
+    assert (g["h"], g["w"], g["seed"], g["switches"]) == (WORKLOAD["h"], WORKLOAD["w"], WORKLOAD["seed"], WORKLOAD["switches"])
+    return g["mean_dist"]
 
 
 def parse():
@@ -197,6 +209,19 @@ def main():
     dann = torch.empty((H - 7, W - 7, 3), dtype=torch.float64, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
+    ref_md = reference_mean_dist()
+    sched_md = {}
+    chosen = None
+    for (passes, jump) in SCHEDULES:
+        params.gpu_prop_passes, params.gpu_jump = passes, jump
+        table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
+        sched_md["%d/%d" % (passes, jump)] = m = mean_dist(dann.cpu().numpy())
+        if m <= 1.01 * ref_md:
+            chosen = (passes, jump)
+            break
+    if chosen is None:
+        chosen = SCHEDULES[-1]
+    params.gpu_prop_passes, params.gpu_jump = chosen
     for _ in range(max(args.warmup, 3)):
         table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
     torch.cuda.synchronize()
@@ -254,9 +279,20 @@ def main():
     e2e = world * P / float(e2e_t.item())
     md_e2e = mean_dist(ann_np)
 
+    # the library's default schedule on the same workload, for reference
+    params.gpu_prop_passes, params.gpu_jump = 0, 0
+    dflt_ms = []
+    for i in range(max(3, args.steps // 2)):
+        flush.zero_()
+        st, _ = table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
+        dflt_ms.append(sum(st.values()))
+    default_sched = {"patches_per_s": P / (statistics.mean(dflt_ms[1:] or dflt_ms) / 1000.0),
+                     "mean_nnf_dist": mean_dist(dann.cpu().numpy())}
+    params.gpu_prop_passes, params.gpu_jump = chosen
+
     # roofline of the dominant kernel (HBM-bound accounting)
     hbm, peak_kind = peaks()
-    passes = table.params.gpu_prop_passes or table.params.prop_iters
+    passes = chosen[0]
     dom = max(("choose", "pull"), key=lambda k: stages[k])
     per_launch_ms = stages[dom] / (args.steps * passes)
     alg_bytes = {"pull": 56, "choose": 60}[dom] * P
@@ -287,7 +323,10 @@ def main():
         "dtype": "f32", "data": "synthetic (seeded generator, patchtable_b200/synth.py)",
         "config": {"workload": WORKLOAD["name"], "patches_per_step": P, "image": [H, W], "table_image": list(b.shape[:2]),
                    "build_s": build_s, "mean_nnf_dist": md, "mean_nnf_dist_e2e": md_e2e,
-                   "prop_passes": passes, "l2": "flushed between steps (256 MiB write)", "parallelism": "replicas" if world > 1 else "single",
+                   "reference_mean_nnf_dist": ref_md,
+                   "schedule": {"passes": chosen[0], "first_jump": chosen[1], "tried": sched_md,
+                                "rule": "fastest schedule with mean NNF dist <= 1.01 x the reference's on this workload"},
+                   "library_default_schedule": default_sched, "l2": "flushed between steps (256 MiB write)", "parallelism": "replicas" if world > 1 else "single",
                    "stage_ms_per_step": {k: v / args.steps for k, v in stages.items()},
                    "outer_event_ms_per_step": sum(outer) / len(outer), "wall_ms_per_step": 1000 * wall / args.steps,
                    "ssd_candidates_per_patch": {k: ctrs.get(k + "_cand", 0) / (args.steps * P) for k in ("choose", "pull")}},

@@ -128,7 +128,7 @@ pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int h, int w, do
 /* Zero-allocation form of pt_table_lookup_device (no counterpart in the reference).  For
    callers that may not allocate device memory during queries -- a frame loop with a fixed
    latency budget (cudaMalloc/cudaFree synchronise the device), or an application whose own
-   allocator owns the GPU's memory -- every intermediate buffer comes from one 19 MiB file-scope
+   allocator owns the GPU's memory -- every intermediate buffer comes from one 20 MiB file-scope
    device array instead of cudaMalloc.  Limits: at most PT_NOALLOC_MAX_PIXELS query pixels and
    ndims <= 8 (PT_BAD_ARG / PT_UNSUPPORTED otherwise).  All calls share that array, so calls
    that overlap on the GPU race and must be serialised.  The first call on a device resolves the

@@ -76,7 +76,7 @@ __device__ __forceinline__ void count_work(unsigned long long *counters, unsigne
 __global__ void __launch_bounds__(NT)
 k_choose(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
          const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
-         int *ch_pos, float *ch_d, unsigned long long *counters) {
+         int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters) {
     int p = blockIdx.x * NT + threadIdx.x;
     const bool live = p < c_q.ew * c_q.eh;
     unsigned ne = 0, rows = 0;
@@ -96,7 +96,13 @@ k_choose(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict
             if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
         }
     }
-    if (c_q.do_kcoh && xb < c_q.bew && yb < c_q.beh) {
+    /* kc_done[p] holds a position whose k-coherence set was already tried by this patch without
+       any acceptance; with the same position the stored distance, the bound and therefore every
+       outcome would repeat, so the set is skipped (an exact shortcut). */
+    const int kc_src = pt_xy(xb, yb);
+    const bool repeat = use_done && kc_done[p] == kc_src;
+    bool accepted = false;
+    if (c_q.do_kcoh && !repeat && xb < c_q.bew && yb < c_q.beh) {
         int ks = c_q.ks;
         /* kcoherence_set is beh x bew x kc even when ks > 1 (patchtable.h:2659, 3758). */
         const int2 *kp = kcoh + ((size_t) (yb / ks) * c_q.bew + (xb / ks)) * c_q.kc;
@@ -110,9 +116,10 @@ k_choose(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict
             if (ys >= c_q.beh) ys = c_q.beh - 1;
             float dc = ssd_bounded(a, c_q.aw, x, y, b, c_q.bw, xs, ys, dbest, rows);
             ne++;
-            if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
+            if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; accepted = true; }
         }
     }
+    if (c_q.do_kcoh) kc_done[p] = (repeat || !accepted) ? kc_src : -1;
     ch_pos[p] = pt_xy(xb, yb);
     ch_d[p] = dch;
     }
@@ -255,10 +262,10 @@ pt_status pt_launch_init(int n, int pos, float d, int *cur_pos, float *cur_d, cu
 
 pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
                            const int *tcand, const int2 *kcoh, int do_table, int *ch_pos,
-                           float *ch_d, unsigned long long *evals, cudaStream_t st) {
+                           float *ch_d, int *kc_done, int use_done, unsigned long long *evals, cudaStream_t st) {
     QPlan q;
     PT_TRY(make_qplan(s, q));
-    k_choose<<<(n + NT - 1) / NT, NT, 0, st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, evals);
+    k_choose<<<(n + NT - 1) / NT, NT, 0, st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done, use_done, evals);
     PT_LAUNCHED();
     return PT_OK;
 }

@@ -52,7 +52,20 @@ struct QuerySetup {
     int step = 1;            /* neighbour spacing of a pull pass */
     cudaStream_t stream;
 };
-/* Neighbour spacing of pull pass i of n: halving from `jump` down to 1, then 1. */
+/* Query schedule.  By default two choose + pull passes stand in for each of the reference's
+   sequential sweeps (prop_iters, patchtable.h:3608), and the first pull reaches neighbours
+   min(8, 2^(passes-1)) patches away, halving on each pass (jump flooding). */
+inline int pt_default_passes(const pt_params &p) {
+    if (p.gpu_prop_passes > 0) return p.gpu_prop_passes;
+    return p.prop_iters <= 0 ? 0 : 2 * p.prop_iters;
+}
+inline int pt_default_jump(const pt_params &p, int passes) {
+    if (p.gpu_jump > 0) return p.gpu_jump;
+    int j = 1;
+    for (int i = 1; i < passes && j < 8; i++) j *= 2;
+    return j;
+}
+/* Neighbour spacing of pull pass i: halving from `jump` down to 1, then 1. */
 inline int pt_pass_step(int i, int n, int jump) {
     (void) n;
     int s = jump > 1 ? jump : 1;
@@ -62,7 +75,7 @@ inline int pt_pass_step(int i, int n, int jump) {
 pt_status pt_launch_init(int n, int pos, float d, int *cur_pos, float *cur_d, cudaStream_t st);
 pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
                            const int *tcand, const int2 *kcoh, int do_table, int *ch_pos,
-                           float *ch_d, unsigned long long *evals, cudaStream_t st);
+                           float *ch_d, int *kc_done, int use_done, unsigned long long *evals, cudaStream_t st);
 pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
                          const int *ch_pos, const float *ch_d, int *nxt_pos, float *nxt_d,
                          unsigned long long *evals, cudaStream_t st);

@@ -11,7 +11,7 @@
    Limits and behaviour:
      * query images of at most PT_NOALLOC_MAX_PIXELS (262144) pixels, e.g. 512 x 512, and tables
        with ndims <= 8; larger requests fail with PT_BAD_ARG / PT_UNSUPPORTED;
-     * the array costs 19 MiB of device memory on every GPU that loads the library, held until
+     * the array costs 20 MiB of device memory on every GPU that loads the library, held until
        the process exits;
      * all calls share the array: calls that overlap on the GPU (different streams, threads or
        tables at the same time) race on it and must be serialised by the caller;
@@ -31,8 +31,8 @@ namespace {
 
 constexpr size_t kMaxPixels = PT_NOALLOC_MAX_PIXELS;
 /* per pixel: RGBA copy (16 B) + descriptor record (32 B) + table candidate (4 B)
-   + three NNF position buffers (12 B) + three distance buffers (12 B) */
-constexpr size_t kBytesPerPixel = 16 + 32 + 4 + 12 + 12;
+   + four position buffers (16 B) + three distance buffers (12 B) */
+constexpr size_t kBytesPerPixel = 16 + 32 + 4 + 16 + 12;
 constexpr size_t kScratchBytes = kMaxPixels * kBytesPerPixel;
 
 static __device__ __align__(256) unsigned char pt_noalloc_scratch[kScratchBytes];
@@ -82,6 +82,7 @@ extern "C" pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_
     int *pos0 = (int *) s;                  s += N * 4;
     int *pos1 = (int *) s;                  s += N * 4;
     int *chpos = (int *) s;                 s += N * 4;
+    int *kcdone = (int *) s;                s += N * 4;
     float *d0 = (float *) s;                s += N * 4;
     float *d1 = (float *) s;                s += N * 4;
     float *chd = (float *) s;
@@ -102,17 +103,18 @@ extern "C" pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_
     if (qs.radius > 2) qs.radius = 2;
     qs.stream = st;
     PT_TRY(pt_launch_init(n, pt_xy(v.w - 7 + 1, 0), (float) PT_DIST_INF, pos[0], dd[0], st));
-    int passes = p.gpu_prop_passes > 0 ? p.gpu_prop_passes : (p.prop_iters <= 0 ? 0 : p.prop_iters);
+    int passes = pt_default_passes(p);
+    int jump = pt_default_jump(p, passes);
     int cur = 0;
     for (int i = 0; i < passes; i++) {
         bool do_table = i == 0 && p.do_table_lookup;
         QuerySetup qi = qs;
         if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
         PT_TRY(pt_launch_choose(qi, n, rgba, v.b_rgba, pos[cur], dd[cur], tcand, v.kcoh, do_table, chpos, chd,
-                                nullptr, st));
+                                kcdone, i > 0, nullptr, st));
         if (p.do_prop) {
             QuerySetup qp = qs;
-            qp.step = pt_pass_step(i, passes, p.gpu_jump);
+            qp.step = pt_pass_step(i, passes, jump);
             PT_TRY(pt_launch_pull(qp, n, rgba, v.b_rgba, pos[cur], dd[cur], chpos, chd, pos[1 - cur], dd[1 - cur],
                                   nullptr, st));
             cur = 1 - cur;

@@ -100,7 +100,7 @@ struct pt_table {
     DevBuf<float4> q_rgba;
     DevBuf<float> q_desc;
     DevBuf<int> q_tcand;
-    DevBuf<int> q_pos[2], q_chpos;
+    DevBuf<int> q_pos[2], q_chpos, q_kcdone;
     DevBuf<float> q_d[2], q_chd;
     DevBuf<double> q_ann;
     DevBuf<unsigned long long> q_counters;
@@ -383,6 +383,7 @@ pt_status ensure_query_buffers(pt_table *t, int h, int w) {
     PT_CUDA(t->q_tcand.reserve(P));
     for (int k = 0; k < 2; k++) { PT_CUDA(t->q_pos[k].reserve(P)); PT_CUDA(t->q_d[k].reserve(P)); }
     PT_CUDA(t->q_chpos.reserve(P));
+    PT_CUDA(t->q_kcdone.reserve(P));
     PT_CUDA(t->q_chd.reserve(P));
     PT_CUDA(t->q_counters.reserve(4));
     return PT_OK;
@@ -406,12 +407,6 @@ pt_status mark(pt_table *t, LookupProfile *prof, int stage, cudaStream_t st) {
     prof->marks.push_back({stage, prof->next});
     prof->next++;
     return PT_OK;
-}
-
-/* One choose + pull pass per reference sweep (prop_iters, patchtable.h:3608) unless overridden. */
-int default_passes(const pt_params &p) {
-    if (p.gpu_prop_passes > 0) return p.gpu_prop_passes;
-    return p.prop_iters <= 0 ? 0 : p.prop_iters;
 }
 
 /* The device part of a lookup: a_rgb (device, h x w x 3) -> d_ann (device doubles).  With prof,
@@ -443,7 +438,8 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     /* Initial field (patchtable.h:3538-3547): x = b0_ew + 1, dist = DIST_INFINITY. */
     PT_TRY(pt_launch_init(n, pt_xy(t->ew + 1, 0), (float) PT_DIST_INF, t->q_pos[0].p, t->q_d[0].p, st));
     PT_TRY(mark(t, prof, LookupProfile::INIT, st));
-    int passes = default_passes(p);
+    int passes = pt_default_passes(p);
+    int jump = pt_default_jump(p, passes);
     int cur = 0;
     for (int i = 0; i < passes; i++) {
         /* Pass 0 plays the reference's first iteration (table lookup, :3641); k-coherence runs
@@ -452,11 +448,11 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
         QuerySetup qi = qs;
         if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
         PT_TRY(pt_launch_choose(qi, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_tcand.p,
-                                t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, ctr, st));
+                                t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, i > 0, ctr, st));
         PT_TRY(mark(t, prof, LookupProfile::CHOOSE, st));
         if (p.do_prop) {
             QuerySetup qp = qs;
-            qp.step = pt_pass_step(i, passes, p.gpu_jump);
+            qp.step = pt_pass_step(i, passes, jump);
             PT_TRY(pt_launch_pull(qp, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_chpos.p,
                                   t->q_chd.p, t->q_pos[1 - cur].p, t->q_d[1 - cur].p, ctr ? ctr + 2 : nullptr, st));
             PT_TRY(mark(t, prof, LookupProfile::PULL, st));
