@@ -151,6 +151,13 @@ pt_status pt_table_lookup_batch(pt_table *t, int n, const float *const *a, const
 pt_status pt_table_lookup_profile(pt_table *t, const float *d_a, int h, int w, double *d_ann,
                                   void *stream, double *stage_ms, uint64_t *counters);
 
+/* Diagnostics (no reference counterpart): C = A * B^T in FP32 through the hand-written tcgen05
+   BF16 GEMM of the proposal network.  A [M x K], B [N x K] row-major BF16 device arrays (lda, ldb
+   multiples of 8; K a multiple of 16; N in {16, 32, 64, 128, 256}); C [M x N] FP32, ldc.
+   *err_flag (device int, may be NULL) becomes 1 if a bounded wait inside the kernel gave up. */
+pt_status pt_tc_gemm_f32(const void *A, int lda, const void *B, int ldb, float *C, int ldc, int M, int N,
+                         int K, int *err_flag, void *stream);
+
 /* Diagnostics: number of breadth-first levels the last DT build ran. */
 int pt_table_dt_levels(const pt_table *t);
 

@@ -109,6 +109,7 @@ def lib() -> C.CDLL:
     L.pt_table_dt_levels.argtypes = [vp]
     L.pt_table_lookup_profile.argtypes = [vp, vp, C.c_int, C.c_int, vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
     L.pt_descriptor.argtypes = [P, _f32p, C.c_int, C.c_int, _f32p]
+    L.pt_tc_gemm_f32.argtypes = [vp, C.c_int, vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp]
     L.pt_last_error.restype = C.c_char_p
     L.pt_version.restype = C.c_char_p
     L.pt_kernel_launch_count.restype = C.c_int64

@@ -139,11 +139,56 @@ k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__res
     count_work(counters, ne, rows);
 }
 
+/* Up to G candidates' sums advanced together row by row, so each query row is read from shared
+   memory once per group; each candidate's sum keeps the reference's lane order and stops once its
+   partial total reaches `bound`.  Returns the candidates' full sums (+inf when stopped). */
+template<int G>
+__device__ __forceinline__ void ssd_group(const float4 *atile, int tx, const float4 *__restrict__ B, int bw,
+                                          const int *cand, int nc, float bound, float *out, unsigned &rows) {
+    float l[G][4];
+    bool live[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) { l[g][0] = l[g][1] = l[g][2] = l[g][3] = 0.f; live[g] = g < nc; }
+#pragma unroll 1
+    for (int dy = 0; dy < 8; dy++) {
+        bool any = false;
+#pragma unroll
+        for (int g = 0; g < G; g++) any |= live[g];
+        if (!any) break;
+        float4 av[8];
+#pragma unroll
+        for (int p = 0; p < 8; p++) av[p] = atile[dy * ATW + tx + p];
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            if (!live[g]) continue;
+            rows++;
+            const float4 *br = B + (size_t) (pt_y(cand[g]) + dy) * bw + pt_x(cand[g]);
+#pragma unroll
+            for (int p = 0; p < 8; p++) {
+                float4 bv = __ldg(br + p);
+                float t0 = __fsub_rn(av[p].x, bv.x), t1 = __fsub_rn(av[p].y, bv.y), t2 = __fsub_rn(av[p].z, bv.z);
+                float q[3] = {__fmul_rn(t0, t0), __fmul_rn(t1, t1), __fmul_rn(t2, t2)};
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const int e = (3 * p + c) & 3;   /* SSE lane of interleaved float 3p + c */
+                    l[g][e] = __fadd_rn(l[g][e], q[c]);
+                }
+            }
+            if (dy < 7 && __fadd_rn(__fadd_rn(__fadd_rn(l[g][0], l[g][1]), l[g][2]), l[g][3]) >= bound) live[g] = false;
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < G; g++)
+        out[g] = live[g] ? __fadd_rn(__fadd_rn(__fadd_rn(l[g][0], l[g][1]), l[g][2]), l[g][3]) : finf();
+}
+
 /* Step 4 as a pull: the best of the stored match and every neighbour's chosen offset applied to
-   this patch -- the patch's own choice first, then each distinct neighbour candidate in neighbour
-   order, each sum stopping at the running best.  Neighbours sit `step` patches apart; passes with
-   decreasing steps (jump flooding) carry an offset across a region in a logarithmic number of
-   passes, where the reference's sequential sweep carries it along a whole row in one sweep. */
+   this patch.  The patch's own choice comes first; the distinct neighbour candidates follow in
+   increasing order of the distance their neighbour achieved with them (the likeliest good ones
+   first, so the running best -- the early-exit bound -- tightens soonest), three at a time.
+   Neighbours sit `step` patches apart; passes with decreasing steps (jump flooding) carry an
+   offset across a region in a logarithmic number of passes, where the reference's sequential
+   sweep carries it along a whole row in one sweep. */
 template<int R>
 __global__ void __launch_bounds__(TW)
 k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
@@ -166,6 +211,7 @@ k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restr
         }
         constexpr int MAXC = (2 * R + 1) * (2 * R + 1) - 1;
         int cand[MAXC];
+        float key[MAXC];
         int nc = 0;
         const int S = c_q.step;
 #pragma unroll
@@ -175,18 +221,29 @@ k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restr
                 if (dx == 0 && dy == 0) continue;
                 int ny = y + S * dy, nx = x + S * dx;
                 if (ny < 0 || ny >= c_q.eh || nx < 0 || nx >= c_q.ew) continue;
-                int cp = ch_pos[ny * c_q.ew + nx];
+                int q = ny * c_q.ew + nx;
+                int cp = ch_pos[q];
                 int xs = pt_x(cp) - S * dx, ys = pt_y(cp) - S * dy;
                 if (xs < 0 || ys < 0 || xs >= c_q.bew || ys >= c_q.beh) continue;
                 int c = pt_xy(xs, ys);
                 bool dup = c == bpos;
                 for (int t = 0; t < nc; t++) dup |= cand[t] == c;
-                if (!dup) cand[nc++] = c;
+                if (dup) continue;
+                /* insertion by the neighbour's own distance (ties keep neighbour order) */
+                float k = ch_d[q];
+                int t = nc++;
+                while (t > 0 && key[t - 1] > k) { key[t] = key[t - 1]; cand[t] = cand[t - 1]; t--; }
+                key[t] = k;
+                cand[t] = c;
             }
         }
-        for (int c = 0; c < nc; c++) {
-            float d = ssd_tile(atile, threadIdx.x, b, c_q.bw, pt_x(cand[c]), pt_y(cand[c]), bd, rows);
-            if (d < bd) { bd = d; bpos = cand[c]; }
+        constexpr int G = 3;
+        for (int c0 = 0; c0 < nc; c0 += G) {
+            float d[G];
+            ssd_group<G>(atile, threadIdx.x, b, c_q.bw, cand + c0, nc - c0, bd, d, rows);
+#pragma unroll
+            for (int g = 0; g < G; g++)
+                if (c0 + g < nc && d[g] < bd) { bd = d[g]; bpos = cand[c0 + g]; }
         }
         ne += nc;
         nxt_pos[p] = bpos;
