@@ -158,6 +158,72 @@ pt_status pt_table_lookup_profile(pt_table *t, const float *d_a, int h, int w, d
 pt_status pt_tc_gemm_f32(const void *A, int lda, const void *B, int ldb, float *C, int ldc, int M, int N,
                          int K, int *err_flag, void *stream);
 
+/* ---- learned proposal (no reference counterpart) ----
+
+   A small network proposes, for every query patch, the PT_PROP_TOPK table cells most likely to
+   hold its match; their stored patches are scored by the same exact SSD as every other candidate.
+   The network (16 -> 128 -> ReLU -> 128 -> ReLU -> 32) works on tables of at most PT_PROP_DIMS
+   grid dimensions: for each dimension it scores the match's bin offset -2..+2 from the query
+   patch's own bin (PT_PROP_CLASSES logits); a cell's probability is the product over dimensions.
+   BF16 weights and activations, FP32 accumulation, FP32 master weights; every kernel is the
+   library's own tcgen05 code.  Device pointers throughout; `stream` is a cudaStream_t (NULL: the
+   CUDA default stream), and the calls are asynchronous on it unless stated otherwise.  Calls on
+   different streams must be ordered by the caller. */
+#define PT_PROP_IN 16
+#define PT_PROP_HIDDEN 128
+#define PT_PROP_OUT 32
+#define PT_PROP_DIMS 6
+#define PT_PROP_CLASSES 5
+#define PT_PROP_TOPK 8
+
+typedef struct pt_proposal pt_proposal;
+
+/* New network with He-initialised weights drawn from seed; threshold 0.5. */
+pt_status pt_proposal_create(uint32_t seed, pt_proposal **out);
+void pt_proposal_free(pt_proposal *net);
+/* Length of the FP32 parameter vector: W1 [128 x 16], b1, W2 [128 x 128], b2, W3 [32 x 128], b3. */
+int pt_proposal_num_params(void);
+pt_status pt_proposal_get_params(pt_proposal *net, float *host);
+/* Replaces the parameters (host FP32) and resets the optimiser state. */
+pt_status pt_proposal_set_params(pt_proposal *net, const float *host);
+/* Patches whose most probable cell has probability below threshold keep the plain candidates
+   (table cell + k-coherence); with kcoh_confident the confident ones also try k-coherence. */
+pt_status pt_proposal_configure(pt_proposal *net, float threshold, int kcoh_confident);
+/* Training batch: X [B x 16] BF16 features and labels [B x 8] bytes from pt_table_proposal_samples;
+   B a positive multiple of 64.  One AdamW step (lr, decoupled weight decay wd); *loss (may be
+   NULL; if given, the call synchronises) receives the batch's mean cross-entropy summed over the
+   grid dimensions. */
+pt_status pt_proposal_train_step(pt_proposal *net, const void *X, const uint8_t *labels, int B, float lr,
+                                 float wd, float *loss, void *stream);
+/* Mean loss and the FP32 gradient (host, pt_proposal_num_params floats) of a batch, no update. */
+pt_status pt_proposal_gradient(pt_proposal *net, const void *X, const uint8_t *labels, int B, float *loss,
+                               float *grad_host, void *stream);
+/* logits [B x 32] FP32 of X [B x 16] BF16 (three GEMM launches); synchronises. */
+pt_status pt_proposal_forward(pt_proposal *net, const void *X, int B, float *logits, void *stream);
+/* Waits for the stream and reports a tensor-core wait that gave up (PT_TIMEOUT). */
+pt_status pt_proposal_sync(pt_proposal *net, void *stream);
+
+/* Training samples from a query image d_a (device h x w x 3) and an NNF d_ann of it against this
+   table (device doubles, pt_table_lookup layout): X [(h-7)(w-7) x 16] BF16 features and labels
+   [(h-7)(w-7) x 8] bytes (per grid dimension: offset class | valid-below << 3 | valid-above << 5,
+   0xFF when unused; byte 6 = 1 when the match's bin lies within the 5 x ... x 5 window). */
+pt_status pt_table_proposal_samples(pt_table *t, const float *d_a, int h, int w, const double *d_ann,
+                                    void *X, uint8_t *labels, void *stream);
+/* Fused inference only: cand [(h-7)(w-7) x 8] table entries of the proposed cells (-1 where fewer
+   are valid), conf [(h-7)(w-7)] probability of the best cell, logits (may be NULL) [.. x 32]. */
+pt_status pt_table_proposal_infer(pt_table *t, pt_proposal *net, const float *d_a, int h, int w,
+                                  int32_t *cand, float *conf, float *logits, void *stream);
+/* pt_table_lookup with the network's proposals in place of the table candidate (and, unless
+   configured otherwise, of k-coherence) for confident patches; same buffers and result layout. */
+pt_status pt_table_lookup_learned(pt_table *t, pt_proposal *net, const float *a, int h, int w,
+                                  double *ann_out, double *seconds);
+pt_status pt_table_lookup_learned_device(pt_table *t, pt_proposal *net, const float *d_a, int h, int w,
+                                         double *d_ann, void *stream);
+/* Diagnostics: as pt_table_lookup_profile, with stage_ms[7] (the 7th stage is the network) and
+   counters[6] (the 5th counts confident patches, the 6th their proposals). */
+pt_status pt_table_lookup_learned_profile(pt_table *t, pt_proposal *net, const float *d_a, int h, int w,
+                                          double *d_ann, void *stream, double *stage_ms, uint64_t *counters);
+
 /* Diagnostics: number of breadth-first levels the last DT build ran. */
 int pt_table_dt_levels(const pt_table *t);
 

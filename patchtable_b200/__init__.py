@@ -110,6 +110,24 @@ def lib() -> C.CDLL:
     L.pt_table_lookup_profile.argtypes = [vp, vp, C.c_int, C.c_int, vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
     L.pt_descriptor.argtypes = [P, _f32p, C.c_int, C.c_int, _f32p]
     L.pt_tc_gemm_f32.argtypes = [vp, C.c_int, vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp]
+    fp = C.POINTER(C.c_float)
+    L.pt_proposal_create.argtypes = [C.c_uint32, C.POINTER(vp)]
+    L.pt_proposal_free.argtypes = [vp]
+    L.pt_proposal_free.restype = None
+    L.pt_proposal_num_params.restype = C.c_int
+    L.pt_proposal_get_params.argtypes = [vp, _f32p]
+    L.pt_proposal_set_params.argtypes = [vp, _f32p]
+    L.pt_proposal_configure.argtypes = [vp, C.c_float, C.c_int]
+    L.pt_proposal_train_step.argtypes = [vp, vp, vp, C.c_int, C.c_float, C.c_float, fp, vp]
+    L.pt_proposal_gradient.argtypes = [vp, vp, vp, C.c_int, fp, vp, vp]
+    L.pt_proposal_forward.argtypes = [vp, vp, C.c_int, vp, vp]
+    L.pt_proposal_sync.argtypes = [vp, vp]
+    L.pt_table_proposal_samples.argtypes = [vp, vp, C.c_int, C.c_int, vp, vp, vp, vp]
+    L.pt_table_proposal_infer.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp, vp, vp, vp]
+    L.pt_table_lookup_learned.argtypes = [vp, vp, _f32p, C.c_int, C.c_int, _f64p, C.POINTER(C.c_double)]
+    L.pt_table_lookup_learned_device.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp, vp]
+    L.pt_table_lookup_learned_profile.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp, vp, C.POINTER(C.c_double),
+                                                  C.POINTER(C.c_uint64)]
     L.pt_last_error.restype = C.c_char_p
     L.pt_version.restype = C.c_char_p
     L.pt_kernel_launch_count.restype = C.c_int64
@@ -246,6 +264,49 @@ class PatchTable:
                                              C.c_void_p(stream), ms, ctr))
         return dict(zip(self.STAGES, list(ms))), dict(choose_cand=ctr[0], choose_rows=ctr[1],
                                                      pull_cand=ctr[2], pull_rows=ctr[3])
+
+    # -- learned proposals (patchtable_b200.proposal.ProposalNet) -----------------------------
+    def lookup_learned(self, a, net, out=None):
+        """lookup() with the proposal network's candidates for confident patches."""
+        a = _img(a)
+        shape = (a.shape[0] - 7, a.shape[1] - 7, 3)
+        if out is not None:
+            if out.shape != shape or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
+                raise PatchTableError(1, "out must be a C-contiguous float64 array of shape %s" % (shape,))
+            ann = out
+        else:
+            ann = np.empty(shape, np.float64)
+        secs = C.c_double()
+        self._sync_params()
+        _check(lib().pt_table_lookup_learned(self._h, net.handle, a, a.shape[0], a.shape[1], ann, C.byref(secs)))
+        self.last_seconds = secs.value
+        return ann
+
+    def lookup_learned_device(self, net, a_ptr: int, h: int, w: int, ann_ptr: int, stream: int = 0) -> None:
+        self._sync_params()
+        _check(lib().pt_table_lookup_learned_device(self._h, net.handle, C.c_void_p(a_ptr), h, w, C.c_void_p(ann_ptr),
+                                                    C.c_void_p(stream)))
+
+    LEARNED_STAGES = STAGES + ("proposal",)
+
+    def lookup_learned_profile(self, net, a_ptr: int, h: int, w: int, ann_ptr: int, stream: int = 0):
+        ms = (C.c_double * 7)()
+        ctr = (C.c_uint64 * 6)()
+        self._sync_params()
+        _check(lib().pt_table_lookup_learned_profile(self._h, net.handle, C.c_void_p(a_ptr), h, w, C.c_void_p(ann_ptr),
+                                                     C.c_void_p(stream), ms, ctr))
+        return dict(zip(self.LEARNED_STAGES, list(ms))), dict(choose_cand=ctr[0], choose_rows=ctr[1], pull_cand=ctr[2],
+                                                             pull_rows=ctr[3], confident=ctr[4], proposals=ctr[5])
+
+    def proposal_samples(self, a_ptr: int, h: int, w: int, ann_ptr: int, x_ptr: int, lab_ptr: int, stream: int = 0):
+        """Training features (BF16 [P x 16]) and label bytes ([P x 8]) of a query image and its NNF."""
+        _check(lib().pt_table_proposal_samples(self._h, C.c_void_p(a_ptr), h, w, C.c_void_p(ann_ptr), C.c_void_p(x_ptr),
+                                               C.c_void_p(lab_ptr), C.c_void_p(stream)))
+
+    def proposal_infer(self, net, a_ptr: int, h: int, w: int, cand_ptr: int, conf_ptr: int, logits_ptr: int = 0,
+                       stream: int = 0):
+        _check(lib().pt_table_proposal_infer(self._h, net.handle, C.c_void_p(a_ptr), h, w, C.c_void_p(cand_ptr),
+                                             C.c_void_p(conf_ptr), C.c_void_p(logits_ptr or None), C.c_void_p(stream)))
 
     # -- introspection for parity tests --------------------------------------------------------
     def shape(self):

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
+#include "pt_bins.cuh"
 #include "pt_internal.h"
 #include "pt_kernels.h"
 
@@ -42,20 +43,9 @@ struct DtPlan {
     unsigned char elab[1 + 2 * PT_DESC_MAX][2 * PT_DESC_MAX];
 };
 
-/* float -> int conversion with x86 cvttss2si semantics (NaN and out-of-range give INT_MIN), as
-   the reference's `int idx = (v-min_val)*(NMAP-1)/range` compiles on x86-64. */
-__device__ __forceinline__ int cvtt_x86(float f) {
-    if (!(f >= -2147483648.0f && f < 2147483648.0f)) return INT_MIN;
-    return __float2int_rz(f);
-}
-
-/* PatchPartition1D::get_bin, patchtable.h:1298-1325, bit-exact (no fused operations). */
+/* PatchPartition1D::get_bin, patchtable.h:1298-1325 (pt_bins.cuh). */
 __device__ __forceinline__ int get_bin(const BinPlan &c_bins, const int *__restrict__ to_bin, int d, float v) {
-    float t = __fdiv_rn(__fmul_rn(__fsub_rn(v, c_bins.min_val[d]), (float) (PT_NMAP - 1)), c_bins.range[d]);
-    int idx = cvtt_x86(t);
-    if (idx < 0) idx = 0;
-    else if (idx >= PT_NMAP) idx = PT_NMAP - 1;
-    return __ldg(to_bin + d * PT_NMAP + idx);
+    return pt_get_bin(c_bins.min_val[d], c_bins.range[d], to_bin + d * PT_NMAP, v);
 }
 
 __device__ __forceinline__ bool allowed_at(const int *allowed, int allowed_index, long long p) {

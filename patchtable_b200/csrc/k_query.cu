@@ -16,6 +16,8 @@
    already reaches the value it must beat (the partial sum can only grow). */
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "pt_internal.h"
 #include "pt_kernels.h"
 
@@ -84,61 +86,6 @@ __device__ __forceinline__ float ssd_tile(const float4 *atile, int tx, const flo
     return __fadd_rn(__fadd_rn(__fadd_rn(l0, l1), l2), l3);
 }
 
-/* Steps 1-3 for every patch ("choose"): returns the chosen match and its exact distance.  One CTA
-   per 256-patch row segment, with the segment's query rows staged in shared memory. */
-__global__ void __launch_bounds__(TW)
-k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
-              const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
-              int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters) {
-    extern __shared__ float4 atile[];
-    const int x0 = blockIdx.x * TW, y = blockIdx.y;
-    stage_a(atile, a, c_q.aw, c_q.ah, x0, y);
-    __syncthreads();
-    const int x = x0 + threadIdx.x;
-    const bool live = x < c_q.ew;
-    unsigned ne = 0, rows = 0;
-    if (live) {
-        const int p = y * c_q.ew + x;
-        int pos = cur_pos[p];
-        float dstore = cur_d[p];
-        int xb = pt_x(pos), yb = pt_y(pos);
-        float dbest = (float) ((double) dstore * c_q.prop_scale);
-        float dch = dstore;
-        if (do_table) {
-            int v = tcand[p];
-            int xs = pt_x(v) - 7, ys = pt_y(v) - 7;
-            if (xs != xb || ys != yb) {
-                float dc = ssd_tile(atile, threadIdx.x, b, c_q.bw, xs, ys, dbest, rows);
-                ne++;
-                if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
-            }
-        }
-        const int kc_src = pt_xy(xb, yb);
-        const bool repeat = use_done && kc_done[p] == kc_src;
-        bool accepted = false;
-        if (c_q.do_kcoh && !repeat && xb < c_q.bew && yb < c_q.beh) {
-            int ks = c_q.ks;
-            const int2 *kp = kcoh + ((size_t) (yb / ks) * c_q.bew + (xb / ks)) * c_q.kc;
-            int kdx = ks > 1 ? xb % ks : 0, kdy = ks > 1 ? yb % ks : 0;
-            for (int k = 0; k < c_q.kc; k++) {
-                int2 e = kp[k];
-                float kd = __int_as_float(e.y);
-                if ((double) kd >= c_q.triangle * (double) dbest) break;
-                int xs = pt_x(e.x) + kdx, ys = pt_y(e.x) + kdy;
-                if (xs >= c_q.bew) xs = c_q.bew - 1;
-                if (ys >= c_q.beh) ys = c_q.beh - 1;
-                float dc = ssd_tile(atile, threadIdx.x, b, c_q.bw, xs, ys, dbest, rows);
-                ne++;
-                if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; accepted = true; }
-            }
-        }
-        if (c_q.do_kcoh) kc_done[p] = (repeat || !accepted) ? kc_src : -1;
-        ch_pos[p] = pt_xy(xb, yb);
-        ch_d[p] = dch;
-    }
-    count_work(counters, ne, rows);
-}
-
 /* Up to G candidates' sums advanced together row by row, so each query row is read from shared
    memory once per group; each candidate's sum keeps the reference's lane order and stops once its
    partial total reaches `bound`.  Returns the candidates' full sums (+inf when stopped). */
@@ -180,6 +127,106 @@ __device__ __forceinline__ void ssd_group(const float4 *atile, int tx, const flo
 #pragma unroll
     for (int g = 0; g < G; g++)
         out[g] = live[g] ? __fadd_rn(__fadd_rn(__fadd_rn(l[g][0], l[g][1]), l[g][2]), l[g][3]) : finf();
+}
+
+/* Proposals of the learned network for one patch (LEARNED instantiation of k_choose_tile). */
+struct LearnedArgs {
+    const int *cand;          /* n x 8 table entries, -1 = none; NULL on passes without proposals */
+    const float *conf;        /* n: probability of the best proposed cell */
+    float threshold;          /* patches below it keep the plain candidates */
+    int kcoh_confident;       /* confident patches also try k-coherence */
+    unsigned long long *counters;   /* [confident patches, proposals scored] or NULL */
+};
+
+/* Steps 1-3 for every patch ("choose"): returns the chosen match and its exact distance.  One CTA
+   per 256-patch row segment, with the segment's query rows staged in shared memory.  The LEARNED
+   instantiation replaces, for patches whose proposal confidence reaches the threshold, the table
+   candidate by the network's proposals (scored best-first in groups of three) and, unless
+   configured otherwise, skips k-coherence for them. */
+template<bool LEARNED>
+__global__ void __launch_bounds__(TW)
+k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
+              const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
+              int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters, const LearnedArgs la) {
+    extern __shared__ float4 atile[];
+    const int x0 = blockIdx.x * TW, y = blockIdx.y;
+    stage_a(atile, a, c_q.aw, c_q.ah, x0, y);
+    __syncthreads();
+    const int x = x0 + threadIdx.x;
+    const bool live = x < c_q.ew;
+    unsigned ne = 0, rows = 0, n_conf = 0, n_prop = 0;
+    if (live) {
+        const int p = y * c_q.ew + x;
+        int pos = cur_pos[p];
+        float dstore = cur_d[p];
+        int xb = pt_x(pos), yb = pt_y(pos);
+        float dbest = (float) ((double) dstore * c_q.prop_scale);
+        float dch = dstore;
+        bool confident = false;
+        if (LEARNED) confident = la.conf[p] >= la.threshold;
+        if (LEARNED && confident && do_table && la.cand) {
+            int cand[PT_PROP_TOPK];
+            int nc = 0;
+            const int4 *cp = reinterpret_cast<const int4 *>(la.cand + (size_t) p * PT_PROP_TOPK);
+            const int4 c0 = cp[0], c1 = cp[1];
+            const int raw[PT_PROP_TOPK] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+            for (int j = 0; j < PT_PROP_TOPK; j++) {
+                if (raw[j] < 0) continue;
+                const int c = pt_xy(pt_x(raw[j]) - 7, pt_y(raw[j]) - 7);
+                bool dup = c == pt_xy(xb, yb);
+                for (int t = 0; t < nc; t++) dup |= cand[t] == c;
+                if (!dup) cand[nc++] = c;
+            }
+            constexpr int G = 3;
+            for (int g0 = 0; g0 < nc; g0 += G) {
+                float d[G];
+                ssd_group<G>(atile, threadIdx.x, b, c_q.bw, cand + g0, nc - g0, dbest, d, rows);
+#pragma unroll
+                for (int g = 0; g < G; g++)
+                    if (g0 + g < nc && d[g] < dbest) { dbest = d[g]; dch = d[g]; xb = pt_x(cand[g0 + g]); yb = pt_y(cand[g0 + g]); }
+            }
+            ne += nc;
+            n_conf = 1;
+            n_prop = nc;
+        } else if (do_table) {
+            int v = tcand[p];
+            int xs = pt_x(v) - 7, ys = pt_y(v) - 7;
+            if (xs != xb || ys != yb) {
+                float dc = ssd_tile(atile, threadIdx.x, b, c_q.bw, xs, ys, dbest, rows);
+                ne++;
+                if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
+            }
+        }
+        const int kc_src = pt_xy(xb, yb);
+        const bool repeat = use_done && kc_done[p] == kc_src;
+        bool accepted = false;
+        const bool kc_here = !LEARNED || !confident || la.kcoh_confident;
+        if (c_q.do_kcoh && kc_here && !repeat && xb < c_q.bew && yb < c_q.beh) {
+            int ks = c_q.ks;
+            const int2 *kp = kcoh + ((size_t) (yb / ks) * c_q.bew + (xb / ks)) * c_q.kc;
+            int kdx = ks > 1 ? xb % ks : 0, kdy = ks > 1 ? yb % ks : 0;
+            for (int k = 0; k < c_q.kc; k++) {
+                int2 e = kp[k];
+                float kd = __int_as_float(e.y);
+                if ((double) kd >= c_q.triangle * (double) dbest) break;
+                int xs = pt_x(e.x) + kdx, ys = pt_y(e.x) + kdy;
+                if (xs >= c_q.bew) xs = c_q.bew - 1;
+                if (ys >= c_q.beh) ys = c_q.beh - 1;
+                float dc = ssd_tile(atile, threadIdx.x, b, c_q.bw, xs, ys, dbest, rows);
+                ne++;
+                if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; accepted = true; }
+            }
+        }
+        if (c_q.do_kcoh) kc_done[p] = (repeat || !accepted) ? kc_src : -1;
+        ch_pos[p] = pt_xy(xb, yb);
+        ch_d[p] = dch;
+    }
+    count_work(counters, ne, rows);
+    if (LEARNED && la.counters) {
+        unsigned c = __reduce_add_sync(0xffffffffu, n_conf), q = __reduce_add_sync(0xffffffffu, n_prop);
+        if ((threadIdx.x & 31) == 0) { atomicAdd(la.counters, (unsigned long long) c); atomicAdd(la.counters + 1, (unsigned long long) q); }
+    }
 }
 
 /* Step 4 as a pull: the best of the stored match and every neighbour's chosen offset applied to
@@ -296,8 +343,31 @@ pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const fl
     PT_TRY(make_qplan(s, q));
     (void) n;
     dim3 grid((q.ew + TW - 1) / TW, q.eh);
-    k_choose_tile<<<grid, TW, sizeof(float4) * 8 * ATW, st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d,
-                                                            kc_done, use_done, evals);
+    LearnedArgs none;
+    memset(&none, 0, sizeof(none));
+    k_choose_tile<false><<<grid, TW, sizeof(float4) * 8 * ATW, st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos,
+                                                                   ch_d, kc_done, use_done, evals, none);
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_choose_learned(const QuerySetup &s, const float4 *a, const float4 *b, const int *cur_pos,
+                                   const float *cur_d, const int *tcand, const int2 *kcoh, int do_table, int *ch_pos,
+                                   float *ch_d, int *kc_done, int use_done, const int *lcand, const float *lconf,
+                                   float threshold, int kcoh_confident, unsigned long long *evals,
+                                   unsigned long long *lcounters, cudaStream_t st) {
+    QPlan q;
+    PT_TRY(make_qplan(s, q));
+    if (!lconf) return pt_fail(PT_BAD_ARG, "learned choose without confidences");
+    LearnedArgs la;
+    la.cand = lcand;
+    la.conf = lconf;
+    la.threshold = threshold;
+    la.kcoh_confident = kcoh_confident;
+    la.counters = lcounters;
+    dim3 grid((q.ew + TW - 1) / TW, q.eh);
+    k_choose_tile<true><<<grid, TW, sizeof(float4) * 8 * ATW, st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos,
+                                                                  ch_d, kc_done, use_done, evals, la);
     PT_LAUNCHED();
     return PT_OK;
 }

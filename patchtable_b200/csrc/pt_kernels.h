@@ -76,6 +76,14 @@ pt_status pt_launch_init(int n, int pos, float d, int *cur_pos, float *cur_d, cu
 pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
                            const int *tcand, const int2 *kcoh, int do_table, int *ch_pos,
                            float *ch_d, int *kc_done, int use_done, unsigned long long *evals, cudaStream_t st);
+/* choose with the learned network's proposals (k_proposal.cu) for patches with lconf >= threshold;
+   lcand (n x PT_PROP_TOPK table entries) may be NULL on passes without proposals; lcounters
+   (may be NULL) accumulates {confident patches, proposals scored}. */
+pt_status pt_launch_choose_learned(const QuerySetup &s, const float4 *a, const float4 *b, const int *cur_pos,
+                                   const float *cur_d, const int *tcand, const int2 *kcoh, int do_table, int *ch_pos,
+                                   float *ch_d, int *kc_done, int use_done, const int *lcand, const float *lconf,
+                                   float threshold, int kcoh_confident, unsigned long long *evals,
+                                   unsigned long long *lcounters, cudaStream_t st);
 pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
                          const int *ch_pos, const float *ch_d, int *nxt_pos, float *nxt_d,
                          unsigned long long *evals, cudaStream_t st);
@@ -90,5 +98,19 @@ struct PtTableView {
     const int *to_bin;
     const int2 *kcoh;
     PtBins bins;
+    const float *b_desc;                 /* (h-7) x (w-7) x ds */
+    const float *part;                   /* per grid dimension: centres, left sizes, right sizes */
+    int part_ofs[PT_DESC_MAX];           /* offset of dimension d's centres in part */
+    int nslices[PT_DESC_MAX];
 };
 pt_status pt_table_view(const pt_table *t, PtTableView *v);
+
+/* k_proposal.cu */
+pt_status pt_prop_check_table(const PtTableView &v);
+pt_status pt_launch_prop_samples(const PtTableView &v, const float *qdesc, int n, const double *ann, void *X,
+                                 unsigned char *labels, cudaStream_t st);
+pt_status pt_launch_prop_infer(const PtTableView &v, pt_proposal *q, const float *qdesc, int n, int *cand, float *conf,
+                               float *logits, cudaStream_t st);
+float pt_prop_threshold(const pt_proposal *q);
+int pt_prop_kcoh_confident(const pt_proposal *q);
+pt_status pt_prop_check_error(pt_proposal *q, cudaStream_t st);

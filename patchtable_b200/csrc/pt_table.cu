@@ -90,6 +90,8 @@ struct pt_table {
     std::vector<float> min_val, max_val, range;
     PtBins bins;
     DevBuf<int> to_bin;
+    DevBuf<float> part_dev;           /* per grid dimension: centres, lsizes, rsizes (proposal features) */
+    int part_ofs[PT_DESC_MAX] = {};
     DevBuf<int> table;
     long long add_count = 0;
     int dt_levels = 0;
@@ -103,6 +105,8 @@ struct pt_table {
     DevBuf<int> q_pos[2], q_chpos, q_kcdone;
     DevBuf<float> q_d[2], q_chd;
     DevBuf<double> q_ann;
+    DevBuf<int> q_lcand;              /* learned proposals, P x PT_PROP_TOPK */
+    DevBuf<float> q_lconf;
     DevBuf<unsigned long long> q_counters;
     std::vector<cudaEvent_t> events;
 
@@ -201,6 +205,19 @@ pt_status build_partition(pt_table *t) {
     for (int d = 0; d < G; d++) std::copy(t->part[d].to_bin.begin(), t->part[d].to_bin.end(), flat.begin() + (size_t) d * PT_NMAP);
     PT_CUDA(t->to_bin.reserve(flat.size()));
     PT_CUDA(cudaMemcpyAsync(t->to_bin.p, flat.data(), sizeof(int) * flat.size(), cudaMemcpyHostToDevice, t->st));
+    {
+        std::vector<float> pd;
+        for (int d = 0; d < G; d++) {
+            const PtPartition &P = t->part[d];
+            t->part_ofs[d] = (int) pd.size();
+            pd.insert(pd.end(), P.centers.begin(), P.centers.end());
+            pd.insert(pd.end(), P.lsizes.begin(), P.lsizes.end());
+            pd.insert(pd.end(), P.rsizes.begin(), P.rsizes.end());
+        }
+        PT_CUDA(t->part_dev.reserve(pd.size()));
+        PT_CUDA(cudaMemcpyAsync(t->part_dev.p, pd.data(), sizeof(float) * pd.size(), cudaMemcpyHostToDevice, t->st));
+        PT_CUDA(cudaStreamSynchronize(t->st));
+    }
     memset(&t->bins, 0, sizeof(t->bins));
     t->bins.G = G;
     for (int d = 0; d < G; d++) {
@@ -385,13 +402,13 @@ pt_status ensure_query_buffers(pt_table *t, int h, int w) {
     PT_CUDA(t->q_chpos.reserve(P));
     PT_CUDA(t->q_kcdone.reserve(P));
     PT_CUDA(t->q_chd.reserve(P));
-    PT_CUDA(t->q_counters.reserve(4));
+    PT_CUDA(t->q_counters.reserve(6));
     return PT_OK;
 }
 
 /* Stage timing of one lookup (pt_table_lookup_profile). */
 struct LookupProfile {
-    enum { DESC, CELLS, INIT, CHOOSE, PULL, OUTPUT, NSTAGES };
+    enum { DESC, CELLS, INIT, CHOOSE, PULL, OUTPUT, PROPOSAL, NSTAGES };
     std::vector<std::pair<int, int>> marks;   /* (stage, event index) */
     int next = 0;
 };
@@ -412,20 +429,28 @@ pt_status mark(pt_table *t, LookupProfile *prof, int stage, cudaStream_t st) {
 /* The device part of a lookup: a_rgb (device, h x w x 3) -> d_ann (device doubles).  With prof,
    an event is recorded after every stage and SSD work is counted. */
 pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d_ann, cudaStream_t st,
-                        LookupProfile *prof = nullptr) {
+                        LookupProfile *prof = nullptr, pt_proposal *net = nullptr) {
     const pt_params &p = t->p;
     long long P = (long long) (h - 7) * (w - 7);
     if (P >= (1ll << 31)) return pt_fail(PT_BAD_ARG, "query image too large");
     int n = (int) P;
     PT_TRY(ensure_query_buffers(t, h, w));
     unsigned long long *ctr = prof ? t->q_counters.p : nullptr;
-    if (ctr) PT_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * 4, st));
+    if (ctr) PT_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * 6, st));
     PT_TRY(mark(t, prof, -1, st));
     PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, a_rgb, h, w, p.convert_colorspace, t->q_rgba.p, t->q_desc.p,
                                 t->ds, st));
     PT_TRY(mark(t, prof, LookupProfile::DESC, st));
     PT_TRY(pt_launch_table_candidates(t->bins, t->q_desc.p, t->ds, P, t->to_bin.p, t->table.p, t->q_tcand.p, st));
     PT_TRY(mark(t, prof, LookupProfile::CELLS, st));
+    if (net) {
+        PtTableView v;
+        PT_TRY(pt_table_view(t, &v));
+        PT_CUDA(t->q_lcand.reserve((size_t) P * PT_PROP_TOPK));
+        PT_CUDA(t->q_lconf.reserve(P));
+        PT_TRY(pt_launch_prop_infer(v, net, t->q_desc.p, n, t->q_lcand.p, t->q_lconf.p, nullptr, st));
+        PT_TRY(mark(t, prof, LookupProfile::PROPOSAL, st));
+    }
     QuerySetup qs;
     qs.aw = w; qs.ah = h; qs.bw = t->w; qs.bh = t->h;
     qs.prop_scale = 1.0 / (1 + p.coherence_spatial);
@@ -447,8 +472,14 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
         bool do_table = i == 0 && p.do_table_lookup;
         QuerySetup qi = qs;
         if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
-        PT_TRY(pt_launch_choose(qi, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_tcand.p,
-                                t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, i > 0, ctr, st));
+        if (net)
+            PT_TRY(pt_launch_choose_learned(qi, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_tcand.p,
+                                            t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, i > 0,
+                                            i == 0 ? t->q_lcand.p : nullptr, t->q_lconf.p, pt_prop_threshold(net),
+                                            pt_prop_kcoh_confident(net), ctr, ctr ? ctr + 4 : nullptr, st));
+        else
+            PT_TRY(pt_launch_choose(qi, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_tcand.p,
+                                    t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, i > 0, ctr, st));
         PT_TRY(mark(t, prof, LookupProfile::CHOOSE, st));
         if (p.do_prop) {
             QuerySetup qp = qs;
@@ -464,6 +495,31 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     }
     PT_TRY(pt_launch_output(n, t->q_pos[cur].p, t->q_d[cur].p, d_ann, st));
     PT_TRY(mark(t, prof, LookupProfile::OUTPUT, st));
+    return PT_OK;
+}
+
+/* lookup_device with stage events; stage_ms[nst] receives summed stage times, counters[nctr] the
+   SSD work counters. */
+pt_status profile_impl(pt_table *t, pt_proposal *net, const float *d_a, int h, int w, double *d_ann, cudaStream_t st,
+                       double *stage_ms, int nst, uint64_t *counters, int nctr) {
+    if (!t || !d_a || !d_ann) return pt_fail(PT_BAD_ARG, "null argument");
+    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    LookupProfile prof;
+    PT_TRY(lookup_device(t, d_a, h, w, d_ann, st, &prof, net));
+    PT_CUDA(cudaStreamSynchronize(st));
+    if (net) PT_TRY(pt_prop_check_error(net, st));
+    double ms_all[LookupProfile::NSTAGES] = {0};
+    for (size_t k = 1; k < prof.marks.size(); k++) {
+        float ms = 0;
+        PT_CUDA(cudaEventElapsedTime(&ms, t->events[prof.marks[k - 1].second], t->events[prof.marks[k].second]));
+        ms_all[prof.marks[k].first] += ms;
+    }
+    if (stage_ms) for (int i = 0; i < nst; i++) stage_ms[i] = ms_all[i];
+    if (counters) {
+        unsigned long long c[6];
+        PT_CUDA(cudaMemcpy(c, t->q_counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < nctr; i++) counters[i] = c[i];
+    }
     return PT_OK;
 }
 
@@ -513,24 +569,67 @@ pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int h, int w, do
    (one SSD row = 24 subtractions, multiplications and additions).  Synchronizes the stream. */
 pt_status pt_table_lookup_profile(pt_table *t, const float *d_a, int h, int w, double *d_ann, void *stream,
                                   double *stage_ms, uint64_t *counters) {
-    if (!t || !d_a || !d_ann) return pt_fail(PT_BAD_ARG, "null argument");
+    return profile_impl(t, nullptr, d_a, h, w, d_ann, (cudaStream_t) stream, stage_ms, LookupProfile::PROPOSAL,
+                        counters, 4);
+}
+
+pt_status pt_table_lookup_learned_profile(pt_table *t, pt_proposal *net, const float *d_a, int h, int w, double *d_ann,
+                                          void *stream, double *stage_ms, uint64_t *counters) {
+    if (!net) return pt_fail(PT_BAD_ARG, "null proposal network");
+    return profile_impl(t, net, d_a, h, w, d_ann, (cudaStream_t) stream, stage_ms, LookupProfile::NSTAGES, counters, 6);
+}
+
+pt_status pt_table_lookup_learned(pt_table *t, pt_proposal *net, const float *a, int h, int w, double *ann_out,
+                                  double *seconds) {
+    double T0 = now_s();
+    if (!t || !net || !a || !ann_out) return pt_fail(PT_BAD_ARG, "null argument");
+    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    long long P = (long long) (h - 7) * (w - 7);
+    PT_TRY(ensure_query_buffers(t, h, w));
+    PT_CUDA(t->q_ann.reserve((size_t) P * 3));
+    PT_CUDA(cudaMemcpyAsync(t->q_rgb.p, a, sizeof(float) * (size_t) h * w * 3, cudaMemcpyHostToDevice, t->st));
+    PT_TRY(lookup_device(t, t->q_rgb.p, h, w, t->q_ann.p, t->st, nullptr, net));
+    PT_CUDA(cudaMemcpyAsync(ann_out, t->q_ann.p, sizeof(double) * (size_t) P * 3, cudaMemcpyDeviceToHost, t->st));
+    PT_TRY(pt_prop_check_error(net, t->st));
+    if (seconds) *seconds = now_s() - T0;
+    return PT_OK;
+}
+
+pt_status pt_table_lookup_learned_device(pt_table *t, pt_proposal *net, const float *d_a, int h, int w, double *d_ann,
+                                         void *stream) {
+    if (!t || !net || !d_a || !d_ann) return pt_fail(PT_BAD_ARG, "null argument");
+    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    return lookup_device(t, d_a, h, w, d_ann, (cudaStream_t) stream, nullptr, net);
+}
+
+pt_status pt_table_proposal_samples(pt_table *t, const float *d_a, int h, int w, const double *d_ann, void *X,
+                                    uint8_t *labels, void *stream) {
+    if (!t || !d_a || !d_ann || !X || !labels) return pt_fail(PT_BAD_ARG, "null argument");
     if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
     cudaStream_t st = (cudaStream_t) stream;
-    LookupProfile prof;
-    PT_TRY(lookup_device(t, d_a, h, w, d_ann, st, &prof));
-    PT_CUDA(cudaStreamSynchronize(st));
-    if (stage_ms) for (int i = 0; i < LookupProfile::NSTAGES; i++) stage_ms[i] = 0;
-    for (size_t k = 1; k < prof.marks.size(); k++) {
-        float ms = 0;
-        PT_CUDA(cudaEventElapsedTime(&ms, t->events[prof.marks[k - 1].second], t->events[prof.marks[k].second]));
-        if (stage_ms) stage_ms[prof.marks[k].first] += ms;
-    }
-    if (counters) {
-        unsigned long long c[4];
-        PT_CUDA(cudaMemcpy(c, t->q_counters.p, sizeof(c), cudaMemcpyDeviceToHost));
-        for (int i = 0; i < 4; i++) counters[i] = c[i];
-    }
-    return PT_OK;
+    long long P = (long long) (h - 7) * (w - 7);
+    PT_TRY(ensure_query_buffers(t, h, w));
+    PtTableView v;
+    PT_TRY(pt_table_view(t, &v));
+    PT_TRY(pt_prop_check_table(v));
+    PT_TRY(pt_launch_descriptor(t->p.ndims, t->p.nchroma, d_a, h, w, t->p.convert_colorspace, nullptr, t->q_desc.p, t->ds,
+                                st));
+    return pt_launch_prop_samples(v, t->q_desc.p, (int) P, d_ann, X, labels, st);
+}
+
+pt_status pt_table_proposal_infer(pt_table *t, pt_proposal *net, const float *d_a, int h, int w, int32_t *cand,
+                                  float *conf, float *logits, void *stream) {
+    if (!t || !net || !d_a || !cand || !conf) return pt_fail(PT_BAD_ARG, "null argument");
+    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    cudaStream_t st = (cudaStream_t) stream;
+    long long P = (long long) (h - 7) * (w - 7);
+    PT_TRY(ensure_query_buffers(t, h, w));
+    PtTableView v;
+    PT_TRY(pt_table_view(t, &v));
+    PT_TRY(pt_launch_descriptor(t->p.ndims, t->p.nchroma, d_a, h, w, t->p.convert_colorspace, nullptr, t->q_desc.p, t->ds,
+                                st));
+    PT_TRY(pt_launch_prop_infer(v, net, t->q_desc.p, (int) P, cand, conf, logits, st));
+    return pt_prop_check_error(net, st);
 }
 
 pt_status pt_table_lookup_batch(pt_table *t, int n, const float *const *a, const int *h, const int *w,
@@ -655,6 +754,12 @@ pt_status pt_table_view(const pt_table *t, PtTableView *v) {
     v->to_bin = t->to_bin.p;
     v->kcoh = t->kcoh.p;
     v->bins = t->bins;
+    v->b_desc = t->b_desc.p;
+    v->part = t->part_dev.p;
+    for (int d = 0; d < PT_DESC_MAX; d++) {
+        v->part_ofs[d] = d < t->G ? t->part_ofs[d] : 0;
+        v->nslices[d] = d < t->G ? t->nslices[d] : 0;
+    }
     return PT_OK;
 }
 
