@@ -263,14 +263,21 @@ __global__ void k_adam(float *p, const float *g, float *m, float *v, int n, floa
 
 /* ---- fused inference ---- */
 
+/* One CTA per SM, 4 groups of 128 threads; each group runs its own 128-patch tiles through the
+   three layers.  The weights are shared; each group has its own input tile, hidden-activation
+   tile, mbarrier and 128 tensor-memory columns (all three layers accumulate there in turn: a
+   layer's accumulator is read completely before the next layer's MMAs are issued). */
+constexpr int NGROUP = 4;
 constexpr int SM_W1 = 0;                          /* PH x PIN BF16, K-major */
 constexpr int SM_W2 = SM_W1 + PH * PIN * 2;       /* PH x PH */
 constexpr int SM_W3 = SM_W2 + PH * PH * 2;        /* POUT x PH */
-constexpr int SM_X = SM_W3 + POUT * PH * 2;       /* 128 x PIN */
-constexpr int SM_H = SM_X + 128 * PIN * 2;        /* 128 x PH: hidden activations, reused by both layers */
-constexpr int SM_BIAS = SM_H + 128 * PH * 2;      /* b1, b2, b3 (FP32) */
-constexpr int SM_TOTAL = SM_BIAS + (2 * PH + POUT) * 4;
-constexpr int INFER_COLS = 256;                   /* tensor-memory columns: layers 1 and 3 at 0, layer 2 at 128 */
+constexpr int SM_BIAS = SM_W3 + POUT * PH * 2;    /* b1, b2, b3 (FP32) */
+constexpr int SM_GROUPS = ((SM_BIAS + (2 * PH + POUT) * 4 + 127) / 128) * 128;
+constexpr int SM_GX = 0;                          /* per group: 128 x PIN input tile */
+constexpr int SM_GH = 128 * PIN * 2;              /* per group: 128 x PH hidden tile */
+constexpr int SM_GSIZE = SM_GH + 128 * PH * 2;
+constexpr int SM_TOTAL = SM_GROUPS + NGROUP * SM_GSIZE;
+constexpr int INFER_COLS = 128 * NGROUP;          /* all 512 tensor-memory columns of the SM */
 
 /* Stages a rows x K row-major BF16 matrix into the K-major canonical layout. */
 __device__ __forceinline__ void stage_kmajor(unsigned char *dst, const bf16 *__restrict__ src, int rows, int K) {
@@ -298,12 +305,49 @@ __device__ __forceinline__ void epi_hidden(uint32_t taddr, const float *bias, un
     }
 }
 
-/* All threads wait for the commit of the current phase; the outcome is uniform over the CTA. */
-__device__ __forceinline__ bool cta_wait(uint64_t *mbar, unsigned &phase) {
-    const bool ok = __syncthreads_and(ptc::mbar_wait(mbar, phase) ? 1 : 0) != 0;
+/* Barrier of one 128-thread group (named barrier 1 + g; 0 is __syncthreads). */
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory");
+}
+
+/* Group barrier returning whether `v` holds on every thread of the group. */
+__device__ __forceinline__ bool group_and(int g, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r) : "r"((uint32_t) v), "r"(1 + g) : "memory");
+    return r != 0;
+}
+
+/* The group waits for the commit of the current phase; the outcome is uniform over the group. */
+__device__ __forceinline__ bool group_wait(int g, uint64_t *mbar, unsigned &phase) {
+    const bool ok = group_and(g, ptc::mbar_wait(mbar, phase));
     if (ok) phase ^= 1u;
     ptc::tc_fence_after();
     return ok;
+}
+
+/* Writes this thread's features as row r of the input tile. */
+__device__ __forceinline__ void put_x(unsigned char *sX, int r, const float *f) {
+    *reinterpret_cast<uint4 *>(sX + ptc::kmajor_offset(r, 0, 128)) =
+        make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
+    *reinterpret_cast<uint4 *>(sX + ptc::kmajor_offset(r, 8, 128)) =
+        make_uint4(pack_bf16(f[8], f[9]), pack_bf16(f[10], f[11]), pack_bf16(f[12], f[13]), pack_bf16(f[14], f[15]));
+}
+
+__device__ __forceinline__ void tile_features(const PropPlan &pl, const float *part, const int *to_bin,
+                                              const float *qdesc, int ds, int p, int n, float *f, int *bin) {
+    if (p < n) {
+        prop_features(pl, part, to_bin, qdesc + (size_t) p * ds, f, bin);
+    } else {
+#pragma unroll
+        for (int i = 0; i < PIN; i++) f[i] = 0.f;
+#pragma unroll
+        for (int d = 0; d < PD; d++) bin[d] = 0;
+    }
 }
 
 /* Keeps (a, ca) the larger of the two pairs. */
@@ -318,7 +362,7 @@ __device__ __forceinline__ void cmpx(float &a, int &ca, float &b, int &cb) {
    log-softmax of its 5 logits is sorted (descending, 9-comparator network); the beam of the best
    8 prefixes is extended by the pairs (prefix i, class rank k) with (i+1)(k+1) <= 8 -- any other
    pair is beaten by at least 8 of these, as both lists are sorted -- so the new beam is column
-   k = 0 (already in order) with the other 9 pairs inserted.  bs: log-probabilities (-3e38 when
+   k = 0 (already in order) with the other 9 pairs inserted.  bs: log-probabilities (-3.4e38 when
    fewer than 8 cells exist), bc: 3 bits of class per dimension. */
 __device__ __forceinline__ void top_cells(const float *z, const int *bin, const PropPlan &pl, float *bs, int *bc) {
     constexpr float NEG = -3.4e38f;
@@ -379,94 +423,96 @@ __device__ __forceinline__ void top_cells(const float *z, const int *bin, const 
 /* Persistent fused inference over n patches: cand[p*8 + j] = table entry of the j-th most probable
    cell (-1 past the last valid one), conf[p] = probability of the most probable cell; logits
    (optional) receives the 32 raw logits. */
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128 * NGROUP, 1)
 k_prop_infer(const PropPlan pl, const float *__restrict__ part, const int *__restrict__ to_bin,
              const float *__restrict__ qdesc, int ds, int n, const bf16 *__restrict__ w1, const bf16 *__restrict__ w2,
              const bf16 *__restrict__ w3, const float *__restrict__ params, const int *__restrict__ table, int *cand,
              float *conf, float *logits_out, int *err) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t mbar;
+    __shared__ uint64_t mbar[NGROUP];
     __shared__ uint32_t tslot;
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int g = warp >> 2;                 /* group */
+    const int r = tid & 127;                 /* tile row = accumulator lane of this thread */
     float *sbias = reinterpret_cast<float *>(smem + SM_BIAS);
+    unsigned char *sX = smem + SM_GROUPS + g * SM_GSIZE + SM_GX;
+    unsigned char *sH = smem + SM_GROUPS + g * SM_GSIZE + SM_GH;
     if (warp == 0) ptc::tmem_alloc(&tslot, INFER_COLS);
-    if (tid == 0) {
-        ptc::mbar_init(&mbar, 1);
+    if (tid < NGROUP) {
+        ptc::mbar_init(&mbar[tid], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     stage_kmajor(smem + SM_W1, w1, PH, PIN);
     stage_kmajor(smem + SM_W2, w2, PH, PH);
     stage_kmajor(smem + SM_W3, w3, POUT, PH);
-    for (int i = tid; i < PH; i += 128) { sbias[i] = params[OFF_B1 + i]; sbias[PH + i] = params[OFF_B2 + i]; }
-    for (int i = tid; i < POUT; i += 128) sbias[2 * PH + i] = params[OFF_B3 + i];
+    for (int i = tid; i < PH; i += blockDim.x) { sbias[i] = params[OFF_B1 + i]; sbias[PH + i] = params[OFF_B2 + i]; }
+    for (int i = tid; i < POUT; i += blockDim.x) sbias[2 * PH + i] = params[OFF_B3 + i];
     ptc::fence_proxy_async();
     ptc::tc_fence_before();
     __syncthreads();
     ptc::tc_fence_after();
-    const uint32_t tmem = tslot;
-    const uint32_t trow = tmem + ((uint32_t) (warp * 32) << 16);
+    /* group g owns columns [128 g, 128 g + 128); warp (4 g + j) reads lanes [32 j, 32 j + 32) */
+    const uint32_t tcol = tslot + (uint32_t) (g * 128);
+    const uint32_t trow = tcol + ((uint32_t) ((warp & 3) * 32) << 16);
     constexpr uint32_t ID1 = ptc::idesc_bf16_f32(128, PH), ID3 = ptc::idesc_bf16_f32(128, POUT);
-    const uint32_t sW1 = ptc::smem_u32(smem + SM_W1), sW2 = ptc::smem_u32(smem + SM_W2), sW3 = ptc::smem_u32(smem + SM_W3),
-                   sX = ptc::smem_u32(smem + SM_X), sH = ptc::smem_u32(smem + SM_H);
+    const uint32_t aW1 = ptc::smem_u32(smem + SM_W1), aW2 = ptc::smem_u32(smem + SM_W2),
+                   aW3 = ptc::smem_u32(smem + SM_W3), aX = ptc::smem_u32(sX), aH = ptc::smem_u32(sH);
+    const bool issuer = r == 0;
+    uint64_t *bar = &mbar[g];
     unsigned phase = 0;
     bool ok = true;
     const int ntiles = (n + 127) / 128;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int r = tid;                /* accumulator lane = tile row = this thread */
+    const int gstride = gridDim.x * NGROUP;
+    int tile = blockIdx.x * NGROUP + g;
+    float f[PIN];
+    int bin[PD];
+    tile_features(pl, part, to_bin, qdesc, ds, tile * 128 + r, tile < ntiles ? n : 0, f, bin);
+    for (; tile < ntiles; tile += gstride) {
         const int p = tile * 128 + r;
         const bool live = p < n;
-        float f[PIN];
-        int bin[PD];
-        if (live) {
-            prop_features(pl, part, to_bin, qdesc + (size_t) p * ds, f, bin);
-        } else {
-#pragma unroll
-            for (int i = 0; i < PIN; i++) f[i] = 0.f;
-#pragma unroll
-            for (int d = 0; d < PD; d++) bin[d] = 0;
-        }
-        *reinterpret_cast<uint4 *>(smem + SM_X + ptc::kmajor_offset(r, 0, 128)) =
-            make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
-        *reinterpret_cast<uint4 *>(smem + SM_X + ptc::kmajor_offset(r, 8, 128)) =
-            make_uint4(pack_bf16(f[8], f[9]), pack_bf16(f[10], f[11]), pack_bf16(f[12], f[13]), pack_bf16(f[14], f[15]));
+        put_x(sX, r, f);
         ptc::fence_proxy_async();
         ptc::tc_fence_before();
-        __syncthreads();
-        if (tid == 0) {
+        group_sync(g);
+        if (issuer) {
             ptc::tc_fence_after();
-            ptc::mma_bf16(tmem, ptc::smem_desc(sX), ptc::smem_desc(sW1), ID1, 0);
-            ptc::mma_commit(&mbar);
+            ptc::mma_bf16(tcol, ptc::smem_desc(aX), ptc::smem_desc(aW1), ID1, 0);
+            ptc::mma_commit(bar);
         }
-        if (!(ok = cta_wait(&mbar, phase))) break;
-        epi_hidden(trow, sbias, smem + SM_H, r);
+        /* the next tile's features, while the tensor cores work */
+        const int nxt = tile + gstride;
+        float fn[PIN];
+        int binn[PD];
+        tile_features(pl, part, to_bin, qdesc, ds, nxt * 128 + r, nxt < ntiles ? n : 0, fn, binn);
+        if (!(ok = group_wait(g, bar, phase))) break;
+        epi_hidden(trow, sbias, sH, r);
         ptc::fence_proxy_async();
         ptc::tc_fence_before();
-        __syncthreads();
-        if (tid == 0) {
+        group_sync(g);
+        if (issuer) {
             ptc::tc_fence_after();
 #pragma unroll 1
             for (int ks = 0; ks < PH / 16; ks++)
-                ptc::mma_bf16(tmem + PH, ptc::smem_desc(sH + ks * 128 * 32), ptc::smem_desc(sW2 + ks * PH * 32), ID1,
-                              ks > 0);
-            ptc::mma_commit(&mbar);
+                ptc::mma_bf16(tcol, ptc::smem_desc(aH + ks * 128 * 32), ptc::smem_desc(aW2 + ks * PH * 32), ID1, ks > 0);
+            ptc::mma_commit(bar);
         }
-        if (!(ok = cta_wait(&mbar, phase))) break;
-        epi_hidden(trow + PH, sbias + PH, smem + SM_H, r);
+        if (!(ok = group_wait(g, bar, phase))) break;
+        epi_hidden(trow, sbias + PH, sH, r);
         ptc::fence_proxy_async();
         ptc::tc_fence_before();
-        __syncthreads();
-        if (tid == 0) {
+        group_sync(g);
+        if (issuer) {
             ptc::tc_fence_after();
 #pragma unroll 1
             for (int ks = 0; ks < PH / 16; ks++)
-                ptc::mma_bf16(tmem, ptc::smem_desc(sH + ks * 128 * 32), ptc::smem_desc(sW3 + ks * POUT * 32), ID3,
-                              ks > 0);
-            ptc::mma_commit(&mbar);
+                ptc::mma_bf16(tcol, ptc::smem_desc(aH + ks * 128 * 32), ptc::smem_desc(aW3 + ks * POUT * 32), ID3, ks > 0);
+            ptc::mma_commit(bar);
         }
-        if (!(ok = cta_wait(&mbar, phase))) break;
+        if (!(ok = group_wait(g, bar, phase))) break;
         float z[POUT];
         ptc::tmem_ld16(trow, z);
         ptc::tmem_ld16(trow + 16, z + 16);
+        ptc::tc_fence_before();
         if (live) {
 #pragma unroll
             for (int c = 0; c < POUT; c++) z[c] += sbias[2 * PH + c];
@@ -475,8 +521,6 @@ k_prop_infer(const PropPlan pl, const float *__restrict__ part, const int *__res
 #pragma unroll
                 for (int c = 0; c < POUT / 4; c++) lo[c] = make_float4(z[4 * c], z[4 * c + 1], z[4 * c + 2], z[4 * c + 3]);
             }
-            /* masked log-softmax per dimension, then the exact top-8 of the product by beam search
-               (top_cells) */
             float bs[PK];
             int bc[PK];
             top_cells(z, bin, pl, bs, bc);
@@ -497,16 +541,18 @@ k_prop_infer(const PropPlan pl, const float *__restrict__ part, const int *__res
             co[1] = make_int4(out[4], out[5], out[6], out[7]);
             conf[p] = __expf(bs[0]);
         }
-        ptc::tc_fence_before();
-        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < PIN; i++) f[i] = fn[i];
+#pragma unroll
+        for (int d = 0; d < PD; d++) bin[d] = binn[d];
     }
     if (!ok) {
-        if (tid == 0 && err) atomicExch(err, 1);
-        ptc::mbar_wait(&mbar, phase);   /* one more bounded wait for the tensor-core work in flight */
+        if (issuer && err) atomicExch(err, 1);
+        ptc::mbar_wait(bar, phase);   /* one more bounded wait for the tensor-core work in flight */
     }
     ptc::tc_fence_before();
     __syncthreads();
-    if (warp == 0) ptc::tmem_dealloc(tmem, INFER_COLS);
+    if (warp == 0) ptc::tmem_dealloc(tslot, INFER_COLS);
 }
 
 PropPlan make_plan(const PtTableView &v) {
@@ -692,10 +738,11 @@ pt_status pt_launch_prop_infer(const PtTableView &v, pt_proposal *q, const float
     }
     PT_CUDA(cudaFuncSetAttribute(k_prop_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, SM_TOTAL));
     const int ntiles = (n + 127) / 128;
-    /* two CTAs per SM: shared memory bounds residency at two, which also bounds the tensor memory
-       held on an SM at 2 x 256 of its 512 columns */
-    const int grid = ntiles < 2 * nsm ? ntiles : 2 * nsm;
-    k_prop_infer<<<grid, 128, SM_TOTAL, st>>>(make_plan(v), v.part, v.to_bin, qdesc, v.ds, n, q->w1.p, q->w2.p, q->w3.p,
+    /* one CTA per SM: its shared memory (SM_TOTAL) leaves no room for a second, so its allocation
+       of all 512 tensor-memory columns never waits on another CTA of this kernel */
+    const int groups = (ntiles + NGROUP - 1) / NGROUP;
+    const int grid = groups < nsm ? groups : nsm;
+    k_prop_infer<<<grid, 128 * NGROUP, SM_TOTAL, st>>>(make_plan(v), v.part, v.to_bin, qdesc, v.ds, n, q->w1.p, q->w2.p, q->w3.p,
                                               q->p.p, v.table, cand, conf, logits, q->err.p);
     PT_LAUNCHED();
     return PT_OK;

@@ -36,6 +36,7 @@ struct QPlan {
     int radius;              /* query_step + prop_dist */
     int do_kcoh;
     int step;                /* neighbour spacing of this pull pass (jump flooding) */
+    const float4 *b1;        /* b shifted by one pixel: b1[i] = b[i + 1] */
 };
 
 __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
@@ -59,43 +60,72 @@ __device__ __forceinline__ void stage_a(float4 *atile, const float4 *__restrict_
     }
 }
 
-/* patch_dist_exact with the query patch in shared memory, streamed pixel by pixel into the four
-   SSE lanes (interleaved RGB float e = 3p + c goes to lane e & 3, in increasing e per lane, as
-   patchtable.h:349-356 sums it); abandons the sum once a row's partial total reaches `bound`. */
-__device__ __forceinline__ float ssd_tile(const float4 *atile, int tx, const float4 *__restrict__ B, int bw,
+/* One 32-byte read-only load: pixels p[0], p[1]. */
+__device__ __forceinline__ void ld_px2(const float4 *p, float4 &u, float4 &v) {
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w), "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "l"(p));
+}
+
+/* The 8 pixels (x..x+7, y) of b with four 32-byte loads: pixel index i = y*bw + x is read from b
+   when even and from the shifted copy b1 (b1[i-1] = b[i]) when odd, so every load starts on a
+   32-byte boundary (both arrays are 256-byte aligned). */
+__device__ __forceinline__ void load_brow(const QPlan &q, const float4 *__restrict__ B, int x, int y, float4 (&bv)[8]) {
+    const size_t i = (size_t) y * q.bw + x;
+    const float4 *src = (i & 1) ? q.b1 + (i - 1) : B + i;
+#pragma unroll
+    for (int j = 0; j < 4; j++) ld_px2(src + 2 * j, bv[2 * j], bv[2 * j + 1]);
+}
+
+/* Adds one patch row to the four SSE-lane sums of patch_dist_exact (patchtable.h:349-356): the
+   interleaved RGB float e = 3p + c goes to lane e & 3, in increasing e per lane. */
+__device__ __forceinline__ void row_lanes(const float4 (&av)[8], const float4 (&bv)[8], float (&l)[4]) {
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+        const float t0 = __fsub_rn(av[p].x, bv[p].x), t1 = __fsub_rn(av[p].y, bv[p].y), t2 = __fsub_rn(av[p].z, bv[p].z);
+        const float qd[3] = {__fmul_rn(t0, t0), __fmul_rn(t1, t1), __fmul_rn(t2, t2)};
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const int e = (3 * p + c) & 3;
+            l[e] = __fadd_rn(l[e], qd[c]);
+        }
+    }
+}
+
+__device__ __forceinline__ float lane_total(const float (&l)[4]) {
+    return __fadd_rn(__fadd_rn(__fadd_rn(l[0], l[1]), l[2]), l[3]);
+}
+
+/* patch_dist_exact with the query patch in shared memory; abandons the sum once a row's partial
+   total reaches `bound` (+inf returned). */
+__device__ __forceinline__ float ssd_tile(const float4 *atile, int tx, const QPlan &q, const float4 *__restrict__ B,
                                           int bx, int by, float bound, unsigned &rows) {
-    float l0 = 0.f, l1 = 0.f, l2 = 0.f, l3 = 0.f;
+    float l[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
     for (int dy = 0; dy < 8; dy++) {
         rows++;
-        const float4 *ar = atile + dy * ATW + tx;
-        const float4 *br = B + (size_t) (by + dy) * bw + bx;
+        float4 av[8], bv[8];
+        load_brow(q, B, bx, by + dy, bv);
 #pragma unroll
-        for (int p = 0; p < 8; p++) {
-            float4 av = ar[p], bv = __ldg(br + p);
-            float t0 = __fsub_rn(av.x, bv.x), t1 = __fsub_rn(av.y, bv.y), t2 = __fsub_rn(av.z, bv.z);
-            float q0 = __fmul_rn(t0, t0), q1 = __fmul_rn(t1, t1), q2 = __fmul_rn(t2, t2);
-            /* e = 3p, 3p+1, 3p+2 -> lanes (3p) & 3, (3p+1) & 3, (3p+2) & 3 */
-            const int e0 = (3 * p) & 3, e1 = (3 * p + 1) & 3, e2 = (3 * p + 2) & 3;
-            if (e0 == 0) l0 = __fadd_rn(l0, q0); else if (e0 == 1) l1 = __fadd_rn(l1, q0); else if (e0 == 2) l2 = __fadd_rn(l2, q0); else l3 = __fadd_rn(l3, q0);
-            if (e1 == 0) l0 = __fadd_rn(l0, q1); else if (e1 == 1) l1 = __fadd_rn(l1, q1); else if (e1 == 2) l2 = __fadd_rn(l2, q1); else l3 = __fadd_rn(l3, q1);
-            if (e2 == 0) l0 = __fadd_rn(l0, q2); else if (e2 == 1) l1 = __fadd_rn(l1, q2); else if (e2 == 2) l2 = __fadd_rn(l2, q2); else l3 = __fadd_rn(l3, q2);
-        }
-        if (dy < 7 && __fadd_rn(__fadd_rn(__fadd_rn(l0, l1), l2), l3) >= bound) return finf();
+        for (int p = 0; p < 8; p++) av[p] = atile[dy * ATW + tx + p];
+        row_lanes(av, bv, l);
+        if (dy < 7 && lane_total(l) >= bound) return finf();
     }
-    return __fadd_rn(__fadd_rn(__fadd_rn(l0, l1), l2), l3);
+    return lane_total(l);
 }
 
 /* Up to G candidates' sums advanced together row by row, so each query row is read from shared
-   memory once per group; each candidate's sum keeps the reference's lane order and stops once its
-   partial total reaches `bound`.  Returns the candidates' full sums (+inf when stopped). */
+   memory once per group; candidate g takes part when bit g of `valid` is set.  Each sum keeps the
+   reference's lane order and stops once its partial total reaches `bound`.  out[g] = the full sum,
+   or +inf when stopped or not taking part. */
 template<int G>
-__device__ __forceinline__ void ssd_group(const float4 *atile, int tx, const float4 *__restrict__ B, int bw,
-                                          const int *cand, int nc, float bound, float *out, unsigned &rows) {
+__device__ __forceinline__ void ssd_group(const float4 *atile, int tx, const QPlan &q, const float4 *__restrict__ B,
+                                          const int (&cand)[G], unsigned valid, float bound, float (&out)[G],
+                                          unsigned &rows) {
     float l[G][4];
     bool live[G];
 #pragma unroll
-    for (int g = 0; g < G; g++) { l[g][0] = l[g][1] = l[g][2] = l[g][3] = 0.f; live[g] = g < nc; }
+    for (int g = 0; g < G; g++) { l[g][0] = l[g][1] = l[g][2] = l[g][3] = 0.f; live[g] = (valid >> g) & 1; }
 #pragma unroll 1
     for (int dy = 0; dy < 8; dy++) {
         bool any = false;
@@ -109,24 +139,14 @@ __device__ __forceinline__ void ssd_group(const float4 *atile, int tx, const flo
         for (int g = 0; g < G; g++) {
             if (!live[g]) continue;
             rows++;
-            const float4 *br = B + (size_t) (pt_y(cand[g]) + dy) * bw + pt_x(cand[g]);
-#pragma unroll
-            for (int p = 0; p < 8; p++) {
-                float4 bv = __ldg(br + p);
-                float t0 = __fsub_rn(av[p].x, bv.x), t1 = __fsub_rn(av[p].y, bv.y), t2 = __fsub_rn(av[p].z, bv.z);
-                float q[3] = {__fmul_rn(t0, t0), __fmul_rn(t1, t1), __fmul_rn(t2, t2)};
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const int e = (3 * p + c) & 3;   /* SSE lane of interleaved float 3p + c */
-                    l[g][e] = __fadd_rn(l[g][e], q[c]);
-                }
-            }
-            if (dy < 7 && __fadd_rn(__fadd_rn(__fadd_rn(l[g][0], l[g][1]), l[g][2]), l[g][3]) >= bound) live[g] = false;
+            float4 bv[8];
+            load_brow(q, B, pt_x(cand[g]), pt_y(cand[g]) + dy, bv);
+            row_lanes(av, bv, l[g]);
+            if (dy < 7 && lane_total(l[g]) >= bound) live[g] = false;
         }
     }
 #pragma unroll
-    for (int g = 0; g < G; g++)
-        out[g] = live[g] ? __fadd_rn(__fadd_rn(__fadd_rn(l[g][0], l[g][1]), l[g][2]), l[g][3]) : finf();
+    for (int g = 0; g < G; g++) out[g] = live[g] ? lane_total(l[g]) : finf();
 }
 
 /* Proposals of the learned network for one patch (LEARNED instantiation of k_choose_tile). */
@@ -165,35 +185,42 @@ k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__res
         bool confident = false;
         if (LEARNED) confident = la.conf[p] >= la.threshold;
         if (LEARNED && confident && do_table && la.cand) {
-            int cand[PT_PROP_TOPK];
-            int nc = 0;
+            /* the proposals in the network's order, repeats dropped, three at a time */
             const int4 *cp = reinterpret_cast<const int4 *>(la.cand + (size_t) p * PT_PROP_TOPK);
             const int4 c0 = cp[0], c1 = cp[1];
             const int raw[PT_PROP_TOPK] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+            int cand[PT_PROP_TOPK + 1];
+            unsigned keep = 0;
+            const int own = pt_xy(xb, yb);
 #pragma unroll
             for (int j = 0; j < PT_PROP_TOPK; j++) {
-                if (raw[j] < 0) continue;
-                const int c = pt_xy(pt_x(raw[j]) - 7, pt_y(raw[j]) - 7);
-                bool dup = c == pt_xy(xb, yb);
-                for (int t = 0; t < nc; t++) dup |= cand[t] == c;
-                if (!dup) cand[nc++] = c;
+                cand[j] = raw[j] < 0 ? -1 : pt_xy(pt_x(raw[j]) - 7, pt_y(raw[j]) - 7);
+                bool dup = raw[j] < 0 || cand[j] == own;
+#pragma unroll
+                for (int t = 0; t < j; t++) dup |= ((keep >> t) & 1) && cand[t] == cand[j];
+                if (!dup) keep |= 1u << j;
             }
+            cand[PT_PROP_TOPK] = -1;
             constexpr int G = 3;
-            for (int g0 = 0; g0 < nc; g0 += G) {
+#pragma unroll
+            for (int g0 = 0; g0 < PT_PROP_TOPK; g0 += G) {
+                const unsigned m = (keep >> g0) & ((1u << G) - 1);
+                if (!m) continue;
+                const int cg[G] = {cand[g0], cand[g0 + 1], g0 + 2 <= PT_PROP_TOPK ? cand[g0 + 2] : -1};
                 float d[G];
-                ssd_group<G>(atile, threadIdx.x, b, c_q.bw, cand + g0, nc - g0, dbest, d, rows);
+                ssd_group<G>(atile, threadIdx.x, c_q, b, cg, m, dbest, d, rows);
 #pragma unroll
                 for (int g = 0; g < G; g++)
-                    if (g0 + g < nc && d[g] < dbest) { dbest = d[g]; dch = d[g]; xb = pt_x(cand[g0 + g]); yb = pt_y(cand[g0 + g]); }
+                    if (((m >> g) & 1) && d[g] < dbest) { dbest = d[g]; dch = d[g]; xb = pt_x(cg[g]); yb = pt_y(cg[g]); }
             }
-            ne += nc;
+            n_prop = __popc(keep);
+            ne += n_prop;
             n_conf = 1;
-            n_prop = nc;
         } else if (do_table) {
             int v = tcand[p];
             int xs = pt_x(v) - 7, ys = pt_y(v) - 7;
             if (xs != xb || ys != yb) {
-                float dc = ssd_tile(atile, threadIdx.x, b, c_q.bw, xs, ys, dbest, rows);
+                float dc = ssd_tile(atile, threadIdx.x, c_q, b, xs, ys, dbest, rows);
                 ne++;
                 if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
             }
@@ -203,19 +230,48 @@ k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__res
         bool accepted = false;
         const bool kc_here = !LEARNED || !confident || la.kcoh_confident;
         if (c_q.do_kcoh && kc_here && !repeat && xb < c_q.bew && yb < c_q.beh) {
-            int ks = c_q.ks;
+            /* The reference tries the list in order and stops at the first neighbour whose stored
+               distance reaches triangle * best.  Here three neighbours are scored together with the
+               best known before the group as the early-exit bound, then the sequential decisions
+               are replayed: a sum cut short by that looser bound could not have been accepted, and
+               one that completes is exact, so the outcome equals the one-by-one loop. */
+            const int ks = c_q.ks;
             const int2 *kp = kcoh + ((size_t) (yb / ks) * c_q.bew + (xb / ks)) * c_q.kc;
-            int kdx = ks > 1 ? xb % ks : 0, kdy = ks > 1 ? yb % ks : 0;
-            for (int k = 0; k < c_q.kc; k++) {
-                int2 e = kp[k];
-                float kd = __int_as_float(e.y);
-                if ((double) kd >= c_q.triangle * (double) dbest) break;
-                int xs = pt_x(e.x) + kdx, ys = pt_y(e.x) + kdy;
-                if (xs >= c_q.bew) xs = c_q.bew - 1;
-                if (ys >= c_q.beh) ys = c_q.beh - 1;
-                float dc = ssd_tile(atile, threadIdx.x, b, c_q.bw, xs, ys, dbest, rows);
-                ne++;
-                if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; accepted = true; }
+            const int kdx = ks > 1 ? xb % ks : 0, kdy = ks > 1 ? yb % ks : 0;
+            constexpr int G = 3;
+            bool done = false;
+            for (int k = 0; k < c_q.kc && !done; k += G) {
+                int cg[G];
+                float kdg[G];
+                unsigned m = 0;
+#pragma unroll
+                for (int j = 0; j < G; j++) {
+                    cg[j] = 0;
+                    kdg[j] = 0.f;
+                    if (m == (1u << j) - 1 && k + j < c_q.kc) {
+                        const int2 e = kp[k + j];
+                        const float kd = __int_as_float(e.y);
+                        if ((double) kd < c_q.triangle * (double) dbest) {
+                            int xs = pt_x(e.x) + kdx, ys = pt_y(e.x) + kdy;
+                            if (xs >= c_q.bew) xs = c_q.bew - 1;
+                            if (ys >= c_q.beh) ys = c_q.beh - 1;
+                            cg[j] = pt_xy(xs, ys);
+                            kdg[j] = kd;
+                            m |= 1u << j;
+                        }
+                    }
+                }
+                if (m != (1u << G) - 1) done = true;     /* the list ends or stops inside this group */
+                if (!m) break;
+                float d[G];
+                ssd_group<G>(atile, threadIdx.x, c_q, b, cg, m, dbest, d, rows);
+                ne += __popc(m);
+#pragma unroll
+                for (int j = 0; j < G; j++) {
+                    if (!((m >> j) & 1)) continue;
+                    if ((double) kdg[j] >= c_q.triangle * (double) dbest) { done = true; break; }
+                    if (d[j] < dbest) { dbest = d[j]; dch = d[j]; xb = pt_x(cg[j]); yb = pt_y(cg[j]); accepted = true; }
+                }
             }
         }
         if (c_q.do_kcoh) kc_done[p] = (repeat || !accepted) ? kc_src : -1;
@@ -257,8 +313,12 @@ k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restr
             if (pt_x(cp) < c_q.bew && pt_y(cp) < c_q.beh && cp != bpos && ch_d[p] < bd) { bd = ch_d[p]; bpos = cp; }
         }
         constexpr int MAXC = (2 * R + 1) * (2 * R + 1) - 1;
+        /* distinct neighbour candidates sorted by the neighbour's own distance (ties keep the
+           neighbour order), kept in registers: every slot index is known at compile time */
         int cand[MAXC];
         float key[MAXC];
+#pragma unroll
+        for (int t = 0; t < MAXC; t++) { cand[t] = -1; key[t] = finf(); }
         int nc = 0;
         const int S = c_q.step;
 #pragma unroll
@@ -266,31 +326,41 @@ k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restr
 #pragma unroll
             for (int dx = -R; dx <= R; dx++) {
                 if (dx == 0 && dy == 0) continue;
-                int ny = y + S * dy, nx = x + S * dx;
+                const int ny = y + S * dy, nx = x + S * dx;
                 if (ny < 0 || ny >= c_q.eh || nx < 0 || nx >= c_q.ew) continue;
-                int q = ny * c_q.ew + nx;
-                int cp = ch_pos[q];
-                int xs = pt_x(cp) - S * dx, ys = pt_y(cp) - S * dy;
+                const int q = ny * c_q.ew + nx;
+                const int cp = ch_pos[q];
+                const int xs = pt_x(cp) - S * dx, ys = pt_y(cp) - S * dy;
                 if (xs < 0 || ys < 0 || xs >= c_q.bew || ys >= c_q.beh) continue;
                 int c = pt_xy(xs, ys);
                 bool dup = c == bpos;
-                for (int t = 0; t < nc; t++) dup |= cand[t] == c;
+#pragma unroll
+                for (int t = 0; t < MAXC; t++) dup |= cand[t] == c;
                 if (dup) continue;
-                /* insertion by the neighbour's own distance (ties keep neighbour order) */
                 float k = ch_d[q];
-                int t = nc++;
-                while (t > 0 && key[t - 1] > k) { key[t] = key[t - 1]; cand[t] = cand[t - 1]; t--; }
-                key[t] = k;
-                cand[t] = c;
+#pragma unroll
+                for (int t = 0; t < MAXC; t++) {
+                    if (k < key[t]) {
+                        const float tk = key[t]; key[t] = k; k = tk;
+                        const int tc = cand[t]; cand[t] = c; c = tc;
+                    }
+                }
+                nc++;
             }
         }
         constexpr int G = 3;
-        for (int c0 = 0; c0 < nc; c0 += G) {
-            float d[G];
-            ssd_group<G>(atile, threadIdx.x, b, c_q.bw, cand + c0, nc - c0, bd, d, rows);
 #pragma unroll
-            for (int g = 0; g < G; g++)
-                if (c0 + g < nc && d[g] < bd) { bd = d[g]; bpos = cand[c0 + g]; }
+        for (int g0 = 0; g0 < MAXC; g0 += G) {
+            if (g0 < nc) {
+                const int cg[G] = {cand[g0], g0 + 1 < MAXC ? cand[g0 + 1] : -1, g0 + 2 < MAXC ? cand[g0 + 2] : -1};
+                const int left = nc - g0;
+                const unsigned m = left >= G ? (1u << G) - 1 : (1u << left) - 1;
+                float d[G];
+                ssd_group<G>(atile, threadIdx.x, c_q, b, cg, m, bd, d, rows);
+#pragma unroll
+                for (int g = 0; g < G; g++)
+                    if (((m >> g) & 1) && d[g] < bd) { bd = d[g]; bpos = cg[g]; }
+            }
         }
         ne += nc;
         nxt_pos[p] = bpos;
@@ -326,6 +396,8 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     q.radius = s.radius;
     q.do_kcoh = s.kcoherence > 0;
     q.step = s.step < 1 ? 1 : s.step;
+    q.b1 = s.b1;
+    if (!q.b1) return pt_fail(PT_BAD_ARG, "query without the shifted copy of the table image");
     if (q.radius > 2) return pt_fail(PT_UNSUPPORTED, "propagation radius %d > 2 on the GPU path", q.radius);
     return PT_OK;
 }

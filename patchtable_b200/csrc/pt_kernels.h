@@ -50,6 +50,7 @@ struct QuerySetup {
     double prop_scale, triangle_factor;
     int kcoherence, kcoherence_step, radius;
     int step = 1;            /* neighbour spacing of a pull pass */
+    const float4 *b1 = nullptr;   /* the table image shifted by one pixel, b1[i] = b[i + 1] */
     cudaStream_t stream;
 };
 /* Query schedule.  By default two choose + pull passes stand in for each of the reference's
@@ -94,6 +95,7 @@ struct PtTableView {
     pt_params p;
     int h, w, ds;
     const float4 *b_rgba;
+    const float4 *b_rgba1;               /* b_rgba shifted by one pixel (32-byte aligned row loads) */
     const int *table;
     const int *to_bin;
     const int2 *kcoh;

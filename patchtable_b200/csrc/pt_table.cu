@@ -81,6 +81,7 @@ struct pt_table {
     cudaStream_t st = nullptr;
     bool own_stream = false;
     DevBuf<float4> b_rgba;
+    DevBuf<float4> b_rgba1;           /* b_rgba shifted by one pixel, b_rgba1[i] = b_rgba[i + 1] */
     DevBuf<float> b_desc;
     DevBuf<int> allowed;
     std::vector<int> nslices;
@@ -314,6 +315,12 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
                         packed[((size_t) y * t->ew + x) * t->ds + d] = wh0[((size_t) (y + 7) * (w + 7) + (x + 7)) * t->nd + d];
             PT_CUDA(cudaMemcpyAsync(t->b_desc.p, packed.data(), sizeof(float) * packed.size(), cudaMemcpyHostToDevice, t->st));
         }
+        /* The query reads b patch rows with 32-byte loads: from b_rgba at even pixel indices and
+           from this one-pixel-shifted copy at odd ones, so every load is 32-byte aligned. */
+        const size_t npx = (size_t) h * w;
+        PT_CUDA(t->b_rgba1.reserve(npx));
+        PT_CUDA(cudaMemsetAsync(t->b_rgba1.p, 0, sizeof(float4) * npx, t->st));
+        PT_CUDA(cudaMemcpyAsync(t->b_rgba1.p, t->b_rgba.p + 1, sizeof(float4) * (npx - 1), cudaMemcpyDeviceToDevice, t->st));
         PT_CUDA(cudaStreamSynchronize(t->st));
     }
     std::vector<int> allowed_h;
@@ -458,6 +465,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     qs.kcoherence = p.kcoherence;
     qs.kcoherence_step = p.kcoherence_step;
     qs.radius = p.query_step + p.prop_dist;
+    qs.b1 = t->b_rgba1.p;
     qs.stream = st;
     if (qs.radius > 2) qs.radius = 2;
     /* Initial field (patchtable.h:3538-3547): x = b0_ew + 1, dist = DIST_INFINITY. */
@@ -750,6 +758,7 @@ pt_status pt_table_view(const pt_table *t, PtTableView *v) {
     v->p = t->p;
     v->h = t->h; v->w = t->w; v->ds = t->ds;
     v->b_rgba = t->b_rgba.p;
+    v->b_rgba1 = t->b_rgba1.p;
     v->table = t->table.p;
     v->to_bin = t->to_bin.p;
     v->kcoh = t->kcoh.p;
