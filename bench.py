@@ -8,10 +8,13 @@ the reference's default parameters plus -speed 3 -coherence_spatial 4.  One step
 built once before warm-up.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --profile-case query|query-default|infer     (short fixed runs for ncu)
 
 Prints one JSON line (rank 0).  `value` is query patches per second of device time with a already
-in device memory (L2 flushed between steps); `e2e` is the same metric through the public host API
-(pt_table_lookup) with pinned host buffers, copies included.  --impl reference times the
+in device memory (L2 flushed between steps) at the fastest query schedule whose mean NNF distance
+is within 1% of the reference's on this workload; `e2e` is the same metric through the public host
+API (pt_table_lookup) with pinned host buffers, copies included.  config.learned compares the
+learned-proposal query with the plain one at matched quality.  --impl reference times the
 reference's own implementation (oracle/_ref, compiled from its sources) on the host cores.
 """
 from __future__ import annotations
@@ -21,9 +24,8 @@ import ctypes
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
+import threading
 import time
 
 import numpy as np
@@ -36,9 +38,13 @@ WORKLOAD = dict(name="synthetic 1920x1080 match, -speed 3 -coherence_spatial 4",
 METRIC = "query patches/s at matched mean NNF dist (learned vs plain, 1 B200); build s"
 UNIT = "patches/s"
 L2_FLUSH_BYTES = 256 << 20
-# query schedules (passes, first jump) in increasing cost; the bench times the first whose mean NNF
-# distance is within 1% of the reference's on this workload ("matched mean NNF dist")
-SCHEDULES = [(1, 1), (2, 2), (3, 4), (4, 8), (6, 8)]
+# query schedules (passes, first jump, pull candidates per patch; 0 = all); every one is timed and
+# the fastest whose mean NNF distance is within 1% of the reference's is the measured one
+SCHEDULES = [(1, 2, 1), (1, 1, 1), (1, 2, 2), (1, 2, 3), (1, 2, 0), (2, 2, 1), (2, 2, 2), (2, 2, 0), (3, 4, 0),
+             (4, 8, 0)]
+# learned-proposal comparison: schedules tried for both forms against the plain default's quality
+LEARNED_SCHEDULES = [(1, 2, 0), (2, 2, 0), (2, 2, 2), (3, 4, 0), (4, 8, 0)]
+PROPOSAL_WEIGHTS = os.path.join(ROOT, "patchtable_b200", "data", "proposal_weights.npy")
 
 
 def reference_mean_dist():
@@ -57,6 +63,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--profile-case", choices=["query", "query-default", "infer"], default=None)
     return ap.parse_args()
 
 
@@ -70,46 +78,55 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (read-only query)."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons sampled through NVML (read-only) every millisecond while
+    the timed region runs."""
+    NAMES = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap",
+             0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, index: int):
-        self.index = index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        self.p = None
+    def __init__(self, dev_index: int):
+        self.samples = []
+        self.stop_ev = threading.Event()
+        self.th = None
+        self.nv = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            try:
+                uuid = str(torch.cuda.get_device_properties(dev_index).uuid)
+                self.h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except Exception:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(dev_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.nv = pynvml
+        except Exception:
+            self.nv = None
+
+    def _loop(self):
+        nv = self.nv
+        while not self.stop_ev.is_set():
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM),
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+            except Exception:
+                pass
+            time.sleep(0.001)
 
     def start(self):
-        try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.p = None
+        if self.nv is not None:
+            self.th = threading.Thread(target=self._loop, daemon=True)
+            self.th.start()
 
     def stop(self):
-        if self.p is None:
+        if self.nv is None or self.th is None:
             return None
-        self.p.terminate()
-        try:
-            self.p.wait(timeout=5)
-        except Exception:
-            self.p.kill()
-        self.f.flush()
-        rows = []
-        with open(self.f.name) as f:
-            for line in f:
-                parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.f.name)
-        if not rows:
+        self.stop_ev.set()
+        self.th.join(timeout=5)
+        if not self.samples:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({n for _, r in self.samples for bit, n in self.NAMES.items() if r & bit})
+        return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples), "source": "nvml, every 1 ms"}
 
 
 def make_inputs():
@@ -173,6 +190,96 @@ def run_reference(args, rank):
     print(json.dumps(out))
 
 
+def profile_case(name):
+    """Short fixed runs of one kernel family, for ncu captures."""
+    import torch
+    import patchtable_b200 as ptb
+    from patchtable_b200 import synth
+    ctypes.CDLL(None).srand(1)
+    st = torch.cuda.current_stream().cuda_stream
+    if name in ("query", "query-default"):
+        a, b = make_inputs()
+        H, W = a.shape[:2]
+        p = ptb.PatchTableParams(WORKLOAD["switches"])
+        t = ptb.PatchTable(p, b)
+        if name == "query":
+            p.gpu_prop_passes, p.gpu_jump, p.gpu_pull_max = SCHEDULES[0]
+        da = torch.from_numpy(a).cuda()
+        dann = torch.empty((H - 7) * (W - 7) * 3, dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            t.lookup_device(da.data_ptr(), H, W, dann.data_ptr(), st)
+        torch.cuda.synchronize()
+        print("profile case %s: mean NNF dist %.5f" % (name, float(dann.view(-1, 3)[:, 2].clamp(min=0).sqrt().mean())))
+    else:
+        from patchtable_b200.proposal import ProposalNet
+        h, w = 540, 960
+        a, b = synth.pair(h, w, 6000)
+        t = ptb.PatchTable(ptb.PatchTableParams(WORKLOAD["switches"]), b)
+        net = ProposalNet(seed=0)
+        P = (h - 7) * (w - 7)
+        da = torch.from_numpy(a).cuda()
+        cand = torch.empty((P, 8), dtype=torch.int32, device="cuda")
+        conf = torch.empty(P, dtype=torch.float32, device="cuda")
+        for _ in range(3):
+            t.proposal_infer(net, da.data_ptr(), h, w, cand.data_ptr(), conf.data_ptr(), 0, st)
+        torch.cuda.synchronize()
+        print("profile case infer: mean confidence %.5f" % float(conf.mean()))
+
+
+def timed_schedule(table, sched, da, H, W, dann, sptr, flush, reps=3, net=None):
+    """(best device ms of `reps` lookups after one untimed, mean NNF dist) of one schedule."""
+    import torch
+    from patchtable_b200.metrics import get_mean_dist
+    p = table.params
+    p.gpu_prop_passes, p.gpu_jump, p.gpu_pull_max = sched
+    best = None
+    for i in range(reps + 1):
+        flush.zero_()
+        if net is None:
+            st, _ = table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
+        else:
+            st, _ = table.lookup_learned_profile(net, da.data_ptr(), H, W, dann.data_ptr(), sptr)
+        if i > 0:
+            tot = sum(st.values())
+            best = tot if best is None else min(best, tot)
+    torch.cuda.synchronize()
+    return best, get_mean_dist(dann.cpu().numpy())
+
+
+def learned_comparison(table, da, H, W, dann, sptr, flush, P):
+    """The learned-proposal query against the plain one at the plain default schedule's quality."""
+    if not os.path.exists(PROPOSAL_WEIGHTS):
+        return {"unavailable": "no trained proposal weights at patchtable_b200/data/proposal_weights.npy"}
+    from patchtable_b200.proposal import ProposalNet
+    net = ProposalNet.load(PROPOSAL_WEIGHTS)
+    _, target = timed_schedule(table, (0, 0, 0), da, H, W, dann, sptr, flush, reps=1)
+    bar = 1.01 * target
+    out = {"quality_bar": {"mean_nnf_dist": bar, "rule": "within 1% of the plain default schedule's mean"}}
+    rows = {}
+    for label, thr in (("plain", None), ("learned_threshold_0.5", 0.5), ("learned_threshold_0", 0.0)):
+        best = None
+        tried = {}
+        for sched in LEARNED_SCHEDULES:
+            if thr is None:
+                ms, md = timed_schedule(table, sched, da, H, W, dann, sptr, flush)
+            else:
+                net.configure(thr, False)
+                ms, md = timed_schedule(table, sched, da, H, W, dann, sptr, flush, net=net)
+            tried["%d/%d/%d" % sched] = {"ms": ms, "mean_nnf_dist": md}
+            if md <= bar and (best is None or ms < best[0]):
+                best = (ms, sched, md)
+        rows[label] = {"patches_per_s": P / (best[0] / 1000.0) if best else None,
+                       "schedule": "%d/%d/%d" % best[1] if best else None,
+                       "mean_nnf_dist": best[2] if best else None, "tried": tried}
+    out.update(rows)
+    if rows["plain"]["patches_per_s"]:
+        for k in ("learned_threshold_0.5", "learned_threshold_0"):
+            if rows[k]["patches_per_s"]:
+                rows[k]["vs_plain"] = rows[k]["patches_per_s"] / rows["plain"]["patches_per_s"]
+    net.close()
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -188,6 +295,9 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
@@ -209,20 +319,19 @@ def main():
     dann = torch.empty((H - 7, W - 7, 3), dtype=torch.float64, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
+    # the fastest schedule within 1% of the reference's mean NNF distance
     ref_md = reference_mean_dist()
     sched_md = {}
     chosen = None
-    for (passes, jump) in SCHEDULES:
-        params.gpu_prop_passes, params.gpu_jump = passes, jump
-        table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
-        sched_md["%d/%d" % (passes, jump)] = m = mean_dist(dann.cpu().numpy())
-        if m <= 1.01 * ref_md:
-            chosen = (passes, jump)
-            break
-    if chosen is None:
-        chosen = SCHEDULES[-1]
-    params.gpu_prop_passes, params.gpu_jump = chosen
+    for sched in SCHEDULES:
+        ms, m = timed_schedule(table, sched, da, H, W, dann, sptr, flush)
+        sched_md["%d/%d/%d" % sched] = {"ms": ms, "mean_nnf_dist": m}
+        if m <= 1.01 * ref_md and (chosen is None or ms < chosen[0]):
+            chosen = (ms, sched)
+    chosen = chosen[1] if chosen else SCHEDULES[-1]
+    params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = chosen
     for _ in range(max(args.warmup, 3)):
+        flush.zero_()
         table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
     torch.cuda.synchronize()
     md = mean_dist(dann.cpu().numpy())
@@ -233,7 +342,7 @@ def main():
     torch.cuda.synchronize()
     clocks.start()
     ptb.reset_launch_count()
-    step_ms, stages, ctrs = [], {k: 0.0 for k in ptb.PatchTable.STAGES}, {}
+    stages, ctrs = {k: 0.0 for k in ptb.PatchTable.STAGES}, {}
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     tw0 = time.perf_counter()
     for i in range(args.steps):
@@ -280,29 +389,30 @@ def main():
     md_e2e = mean_dist(ann_np)
 
     # the library's default schedule on the same workload, for reference
-    params.gpu_prop_passes, params.gpu_jump = 0, 0
-    dflt_ms = []
-    for i in range(max(3, args.steps // 2)):
-        flush.zero_()
-        st, _ = table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
-        dflt_ms.append(sum(st.values()))
-    default_sched = {"patches_per_s": P / (statistics.mean(dflt_ms[1:] or dflt_ms) / 1000.0),
-                     "mean_nnf_dist": mean_dist(dann.cpu().numpy())}
-    params.gpu_prop_passes, params.gpu_jump = chosen
+    dflt_ms, dflt_md = timed_schedule(table, (0, 0, 0), da, H, W, dann, sptr, flush, reps=max(3, args.steps // 2))
+    default_sched = {"patches_per_s": P / (dflt_ms / 1000.0), "mean_nnf_dist": dflt_md}
+    learned = None
+    if not args.no_learned and rank == 0:
+        learned = learned_comparison(table, da, H, W, dann, sptr, flush, P)
+    params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = chosen
 
-    # roofline of the dominant kernel (HBM-bound accounting)
+    # roofline of the dominant query kernel.  Both query kernels are limited by the L1TEX data
+    # pipe (wavefronts of the scattered 8x8 patch gathers) long before HBM; the HBM figure counts
+    # the kernel's algorithmic bytes, the fp32 figure its SSD arithmetic.
     hbm, peak_kind = peaks()
     passes = chosen[0]
     dom = max(("choose", "pull"), key=lambda k: stages[k])
     per_launch_ms = stages[dom] / (args.steps * passes)
     alg_bytes = {"pull": 56, "choose": 60}[dom] * P
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
-    traffic = None
+    traffic, l1 = None, None
     try:
         with open(os.path.join(ROOT, "profiles", "query_%s_c2.md" % dom)) as f:
             for line in f:
                 if line.startswith("dram_bytes_per_launch:"):
                     traffic = float(line.split(":")[1])
+                if line.startswith("l1tex_wavefront_pct_of_peak:"):
+                    l1 = float(line.split(":")[1])
     except OSError:
         pass
     rows = ctrs.get(dom + "_rows", 0)
@@ -324,15 +434,17 @@ def main():
         "config": {"workload": WORKLOAD["name"], "patches_per_step": P, "image": [H, W], "table_image": list(b.shape[:2]),
                    "build_s": build_s, "mean_nnf_dist": md, "mean_nnf_dist_e2e": md_e2e,
                    "reference_mean_nnf_dist": ref_md,
-                   "schedule": {"passes": chosen[0], "first_jump": chosen[1], "tried": sched_md,
+                   "schedule": {"passes": chosen[0], "first_jump": chosen[1], "pull_max": chosen[2], "tried": sched_md,
                                 "rule": "fastest schedule with mean NNF dist <= 1.01 x the reference's on this workload"},
-                   "library_default_schedule": default_sched, "l2": "flushed between steps (256 MiB write)", "parallelism": "replicas" if world > 1 else "single",
+                   "library_default_schedule": default_sched, "learned": learned,
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": "replicas" if world > 1 else "single",
                    "stage_ms_per_step": {k: v / args.steps for k, v in stages.items()},
                    "outer_event_ms_per_step": sum(outer) / len(outer), "wall_ms_per_step": 1000 * wall / args.steps,
                    "ssd_candidates_per_patch": {k: ctrs.get(k + "_cand", 0) / (args.steps * P) for k in ("choose", "pull")}},
         "roofline": {"bound": "hbm", "kernel": "k_" + dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": alg_bytes,
+                     "limiter": {"unit": "L1TEX data-pipe wavefronts", "pct_of_peak_ncu": l1},
                      "fp32": {"achieved_tflops": fp32_tflops, "flop_per_ssd_row": 72,
                               "ssd_rows_per_launch": rows / (args.steps * passes)}},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(a.nbytes), "d2h_bytes_per_step": int(ann_np.nbytes)},

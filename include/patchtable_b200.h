@@ -60,9 +60,11 @@ typedef struct pt_params {
     /* GPU query schedule (no reference counterpart): number of parallel propagation passes
        that replace the reference's sequential scanline sweeps (0 picks the default), and the
        neighbour spacing of the first pass, halved on each later pass down to 1 (jump
-       flooding; 0 or 1 = plain neighbours). */
+       flooding; 0 or 1 = plain neighbours), and the most neighbour offsets a pull pass scores per
+       patch, best-first by the neighbour's own distance (0 = all of them). */
     int gpu_prop_passes;
     int gpu_jump;
+    int gpu_pull_max;
 } pt_params;
 
 typedef struct pt_table pt_table;

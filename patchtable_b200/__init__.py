@@ -67,6 +67,7 @@ class _Params(C.Structure):
         ("save_filename", C.c_char * PT_PATH_MAX),
         ("gpu_prop_passes", C.c_int),
         ("gpu_jump", C.c_int),
+        ("gpu_pull_max", C.c_int),
     ]
 
 

@@ -37,7 +37,8 @@ def _newer(target: str, deps) -> bool:
 def build(verbose: bool = False, jobs: int = 8) -> str:
     os.makedirs(OBJ, exist_ok=True)
     nvcc = _nvcc()
-    headers = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    headers = (glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
+               glob.glob(os.path.join(ROOT, "include", "*.h")))
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
     cmds, objs = [], []

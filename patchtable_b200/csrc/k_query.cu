@@ -36,6 +36,7 @@ struct QPlan {
     int radius;              /* query_step + prop_dist */
     int do_kcoh;
     int step;                /* neighbour spacing of this pull pass (jump flooding) */
+    int pull_max;            /* most neighbour candidates scored per patch */
     const float4 *b1;        /* b shifted by one pixel: b1[i] = b[i + 1] */
 };
 
@@ -348,6 +349,7 @@ k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restr
                 nc++;
             }
         }
+        if (nc > c_q.pull_max) nc = c_q.pull_max;   /* the best-first prefix of the list */
         constexpr int G = 3;
 #pragma unroll
         for (int g0 = 0; g0 < MAXC; g0 += G) {
@@ -396,6 +398,7 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     q.radius = s.radius;
     q.do_kcoh = s.kcoherence > 0;
     q.step = s.step < 1 ? 1 : s.step;
+    q.pull_max = s.pull_max > 0 ? s.pull_max : 1 << 30;
     q.b1 = s.b1;
     if (!q.b1) return pt_fail(PT_BAD_ARG, "query without the shifted copy of the table image");
     if (q.radius > 2) return pt_fail(PT_UNSUPPORTED, "propagation radius %d > 2 on the GPU path", q.radius);

@@ -50,6 +50,7 @@ struct QuerySetup {
     double prop_scale, triangle_factor;
     int kcoherence, kcoherence_step, radius;
     int step = 1;            /* neighbour spacing of a pull pass */
+    int pull_max = 0;        /* most neighbour candidates a pull scores per patch (0 = all) */
     const float4 *b1 = nullptr;   /* the table image shifted by one pixel, b1[i] = b[i + 1] */
     cudaStream_t stream;
 };

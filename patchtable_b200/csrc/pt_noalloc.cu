@@ -102,6 +102,7 @@ extern "C" pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_
     qs.radius = p.query_step + p.prop_dist;
     if (qs.radius > 2) qs.radius = 2;
     qs.b1 = v.b_rgba1;
+    qs.pull_max = p.gpu_pull_max;
     qs.stream = st;
     PT_TRY(pt_launch_init(n, pt_xy(v.w - 7 + 1, 0), (float) PT_DIST_INF, pos[0], dd[0], st));
     int passes = pt_default_passes(p);

@@ -466,6 +466,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     qs.kcoherence_step = p.kcoherence_step;
     qs.radius = p.query_step + p.prop_dist;
     qs.b1 = t->b_rgba1.p;
+    qs.pull_max = p.gpu_pull_max;
     qs.stream = st;
     if (qs.radius > 2) qs.radius = 2;
     /* Initial field (patchtable.h:3538-3547): x = b0_ew + 1, dist = DIST_INFINITY. */
@@ -718,6 +719,7 @@ pt_status pt_table_set_params(pt_table *t, const pt_params *p) {
     q.kcoherence_iter = p->kcoherence_iter;
     q.gpu_prop_passes = p->gpu_prop_passes;
     q.gpu_jump = p->gpu_jump;
+    q.gpu_pull_max = p->gpu_pull_max;
     if (p->do_rs || p->spatial || p->init_random)
         return pt_fail(PT_UNSUPPORTED, "random/spatial search and init_random are not implemented on the GPU path");
     return PT_OK;

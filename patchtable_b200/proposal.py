@@ -250,6 +250,55 @@ def proposal_hits(table: PatchTable, net: ProposalNet, a: np.ndarray, ann) -> di
                 mean_conf=float(conf.mean()))
 
 
+EVAL_SCHEDULES = ((1, 1, 0), (1, 2, 1), (2, 2, 0), (3, 4, 0), (4, 8, 0))
+
+
+def evaluate(net: ProposalNet, seeds, h: int, w: int, switches: str = DEFAULT_SWITCHES, schedules=EVAL_SCHEDULES,
+             thresholds=(0.5, 0.0), log=None) -> dict:
+    """Plain and learned queries on held-out pairs: per schedule (passes, first jump, pull
+    candidates) the mean NNF distance (mean of sqrt) and the best device time of 3 lookups, averaged
+    over the seeds, plus how often the plain match is among the proposals."""
+    torch = _torch()
+    from .metrics import get_mean_dist
+    P = (h - 7) * (w - 7)
+    st = torch.cuda.current_stream().cuda_stream
+    acc = {}
+    hits = []
+    for seed in seeds:
+        a, b = synth.pair(h, w, seed)
+        _srand(0)
+        params = PatchTableParams(switches)
+        table = PatchTable(params, b)
+        a_d = torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+        ann = torch.empty(P * 3, dtype=torch.float64, device="cuda")
+        params.gpu_prop_passes = 0
+        table.lookup_device(a_d.data_ptr(), h, w, ann.data_ptr(), st)
+        net.configure(0.5, False)
+        hits.append(proposal_hits(table, net, a, ann))
+        for sched in schedules:
+            params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = sched
+            for kind in ("plain",) + tuple("learned_%g" % t for t in thresholds):
+                best = None
+                for rep in range(4):
+                    if kind == "plain":
+                        ms, _ = table.lookup_profile(a_d.data_ptr(), h, w, ann.data_ptr(), st)
+                    else:
+                        net.configure(float(kind.split("_")[1]), False)
+                        ms, _ = table.lookup_learned_profile(net, a_d.data_ptr(), h, w, ann.data_ptr(), st)
+                    if rep:
+                        tot = sum(ms.values())
+                        best = tot if best is None else min(best, tot)
+                md = get_mean_dist(ann.view(h - 7, w - 7, 3).cpu().numpy())
+                acc.setdefault("%d/%d/%d %s" % (sched + (kind,)), []).append((md, best))
+        table.close()
+        if log:
+            log("evaluated seed %d" % seed)
+    rows = {k: {"mean_nnf_dist": float(np.mean([m for m, _ in v])), "ms": float(np.mean([t for _, t in v])),
+                "patches_per_s": P / (float(np.mean([t for _, t in v])) / 1000.0)} for k, v in acc.items()}
+    hit = {k: float(np.mean([hh[k] for hh in hits])) for k in hits[0]}
+    return {"size": [h, w], "seeds": list(seeds), "switches": switches, "proposal_hits": hit, "results": rows}
+
+
 def _main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -263,7 +312,21 @@ def _main():
     t.add_argument("--switches", default=DEFAULT_SWITCHES)
     t.add_argument("--out", required=True)
     t.add_argument("--seed", type=int, default=0)
+    e = sub.add_parser("eval")
+    e.add_argument("--weights", required=True)
+    e.add_argument("--heldout", type=int, default=20)
+    e.add_argument("--size", default="1080x1920")
+    e.add_argument("--switches", default=DEFAULT_SWITCHES)
+    e.add_argument("--out", required=True)
     args = ap.parse_args()
+    if args.cmd == "eval":
+        h, w = (int(v) for v in args.size.split("x"))
+        net = ProposalNet.load(args.weights)
+        res = evaluate(net, HELDOUT_SEEDS[:args.heldout], h, w, args.switches, log=lambda m: print(m, flush=True))
+        with open(args.out, "w") as f:
+            json.dump(res, f, indent=1, sort_keys=True)
+        print(json.dumps(res["proposal_hits"]))
+        return
     if args.cmd == "train":
         h, w = (int(v) for v in args.size.split("x"))
         log = lambda m: print(m, flush=True)
