@@ -403,7 +403,7 @@ def main():
     passes = chosen[0]
     dom = max(("choose", "pull"), key=lambda k: stages[k])
     per_launch_ms = stages[dom] / (args.steps * passes)
-    alg_bytes = {"pull": 56, "choose": 60}[dom] * P
+    alg_bytes = {"pull": 56, "choose": 72}[dom] * P
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
     traffic, l1 = None, None
     try:

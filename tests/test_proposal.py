@@ -244,3 +244,30 @@ def test_learned_threshold_one_is_plain(gpu, libc):
     plain = t.lookup(a)
     learned = t.lookup_learned(a, net)
     assert np.array_equal(plain, learned)
+
+
+WEIGHTS = "patchtable_b200/data/proposal_weights.npy"
+
+
+@pytest.mark.gpu
+def test_trained_network_gains_over_plain(gpu, libc):
+    """The committed network (trained on the plain method's NNFs of pairs 5000-5199) on a held-out
+    pair: with its proposals for every patch, one propagation pass reaches a lower mean NNF
+    distance than the plain query with the same pass, every distance still exact."""
+    import os
+    from oracle.oracle import recompute_dists
+    from patchtable_b200 import proposal as PR
+    from patchtable_b200.metrics import get_mean_dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    net = PR.ProposalNet.load(os.path.join(root, WEIGHTS), threshold=0.0)
+    a, b = synth.pair(540, 960, PR.HELDOUT_SEEDS[0])
+    libc.srand(1)
+    p = ptb.PatchTableParams(PR.DEFAULT_SWITCHES)
+    t = ptb.PatchTable(p, b)
+    p.gpu_prop_passes, p.gpu_jump, p.gpu_pull_max = 1, 1, 0
+    plain = t.lookup(a)
+    learned = t.lookup_learned(a, net)
+    mp, ml = get_mean_dist(plain), get_mean_dist(learned)
+    assert ml <= 0.98 * mp, (ml, mp)
+    rd = recompute_dists(a, b, learned)
+    assert np.all(np.abs(learned[..., 2] - rd) <= 1e-5 * np.maximum(rd, 1e-12) + 1e-9)
