@@ -140,11 +140,35 @@ pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_a, int h, i
                                          void *stream);
 
 /* Batched query (no reference counterpart; the reference matches one image per lookup() call,
-   patchtable.h:4448): n query images of individual sizes against one table, in one persistent
-   launch over the flattened patch index.  a[i] / ann_out[i] are host buffers with the
-   pt_table_lookup layouts. */
+   patchtable.h:4448): n query images of individual sizes against one table.  The images are
+   concatenated on the device and every phase of the query is one launch for all of them
+   (persistent kernels over the flattened list of row segments).  a[i] / ann_out[i] are host
+   buffers with the pt_table_lookup layouts; each ann_out[i] equals what pt_table_lookup returns
+   for a[i] alone. */
 pt_status pt_table_lookup_batch(pt_table *t, int n, const float *const *a, const int *h,
                                 const int *w, double *const *ann_out);
+
+/* Reusable device-side batch (no reference counterpart).  pt_batch_create fixes the image sizes
+   and allocates the concatenated buffers; pt_batch_layout gives each image's first pixel (RGB
+   triples) in the concatenated input and first patch (NNF record) in the concatenated output,
+   and totals[2] = {pixels, patches}.  pt_batch_lookup enqueues the whole query on `stream`
+   (d_rgb: concatenated h x w x 3 floats; d_ann: concatenated (h-7) x (w-7) x 3 doubles) with the
+   table's current parameters.  pt_batch_set_tile / pt_batch_autotune choose how many query
+   patches one CTA covers (32, 64, 128, 256; the results do not depend on it): the autotuner
+   times each on the given inputs and keeps the fastest (ms_out[4] receives the times).
+   pt_batch_capture records the launch sequence for these two buffers and the current parameters
+   into a CUDA graph; pt_batch_replay launches that graph on `stream`. */
+typedef struct pt_batch pt_batch;
+pt_status pt_batch_create(pt_table *t, int n, const int *h, const int *w, pt_batch **out);
+void pt_batch_free(pt_batch *b);
+pt_status pt_batch_layout(const pt_batch *b, int64_t *pixel_offset, int64_t *patch_offset, int64_t *totals);
+pt_status pt_batch_set_tile(pt_batch *b, int patches_per_cta);
+int pt_batch_tile(const pt_batch *b);
+pt_status pt_batch_lookup(pt_batch *b, const float *d_rgb, double *d_ann, void *stream);
+pt_status pt_batch_autotune(pt_batch *b, const float *d_rgb, double *d_ann, void *stream, int *best,
+                            float *ms_out);
+pt_status pt_batch_capture(pt_batch *b, const float *d_rgb, double *d_ann, void *stream);
+pt_status pt_batch_replay(pt_batch *b, void *stream);
 
 /* Diagnostics (no reference counterpart): pt_table_lookup_device with a CUDA event after every
    stage.  stage_ms[6] receives the summed device time of {descriptor, cells, init, choose, pull,

@@ -19,7 +19,7 @@ import os
 
 import numpy as np
 
-__all__ = ["PatchTableParams", "PatchTable", "PatchTableError", "NNF_X", "NNF_Y", "NNF_DIST", "lib",
+__all__ = ["PatchTableParams", "PatchTable", "PatchTableError", "QueryBatch", "NNF_X", "NNF_Y", "NNF_DIST", "lib",
            "descriptor", "launch_count", "reset_launch_count"]
 
 NNF_X, NNF_Y, NNF_DIST = 0, 1, 2
@@ -125,6 +125,18 @@ def lib() -> C.CDLL:
     L.pt_proposal_sync.argtypes = [vp, vp]
     L.pt_table_proposal_samples.argtypes = [vp, vp, C.c_int, C.c_int, vp, vp, vp, vp]
     L.pt_table_proposal_infer.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp, vp, vp, vp]
+    L.pt_table_lookup_batch.argtypes = [vp, C.c_int, vp, vp, vp, vp]
+    L.pt_batch_create.argtypes = [vp, C.c_int, vp, vp, C.POINTER(vp)]
+    L.pt_batch_free.argtypes = [vp]
+    L.pt_batch_free.restype = None
+    L.pt_batch_layout.argtypes = [vp, vp, vp, vp]
+    L.pt_batch_set_tile.argtypes = [vp, C.c_int]
+    L.pt_batch_tile.argtypes = [vp]
+    L.pt_batch_tile.restype = C.c_int
+    L.pt_batch_lookup.argtypes = [vp, vp, vp, vp]
+    L.pt_batch_autotune.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_int), vp]
+    L.pt_batch_capture.argtypes = [vp, vp, vp, vp]
+    L.pt_batch_replay.argtypes = [vp, vp]
     L.pt_table_lookup_learned.argtypes = [vp, vp, _f32p, C.c_int, C.c_int, _f64p, C.POINTER(C.c_double)]
     L.pt_table_lookup_learned_device.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp, vp]
     L.pt_table_lookup_learned_profile.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp, vp, C.POINTER(C.c_double),
@@ -266,6 +278,26 @@ class PatchTable:
         return dict(zip(self.STAGES, list(ms))), dict(choose_cand=ctr[0], choose_rows=ctr[1],
                                                      pull_cand=ctr[2], pull_rows=ctr[3])
 
+    # -- batches ---------------------------------------------------------------------------------
+    def lookup_batch(self, images):
+        """pt_table_lookup_batch: NNFs of several host images (any sizes) in one batched query."""
+        imgs = [_img(x) for x in images]
+        n = len(imgs)
+        if n == 0:
+            return []
+        outs = [np.empty((x.shape[0] - 7, x.shape[1] - 7, 3), np.float64) for x in imgs]
+        A = (C.c_void_p * n)(*[x.ctypes.data for x in imgs])
+        O = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+        H = (C.c_int * n)(*[x.shape[0] for x in imgs])
+        W = (C.c_int * n)(*[x.shape[1] for x in imgs])
+        self._sync_params()
+        _check(lib().pt_table_lookup_batch(self._h, n, A, H, W, O))
+        return outs
+
+    def batch(self, sizes):
+        """A reusable device batch for images of the given (h, w) sizes (QueryBatch)."""
+        return QueryBatch(self, sizes)
+
     # -- learned proposals (patchtable_b200.proposal.ProposalNet) -----------------------------
     def lookup_learned(self, a, net, out=None):
         """lookup() with the proposal network's candidates for confident patches."""
@@ -350,6 +382,67 @@ class PatchTable:
 
     def dt_levels(self) -> int:
         return int(lib().pt_table_dt_levels(self._h))
+
+
+class QueryBatch:
+    """pt_batch: concatenated device buffers for a fixed list of query sizes against one table.
+
+    Inputs and outputs are device addresses of the concatenated images (pixel_offset[i] RGB
+    triples into the input) and NNFs (patch_offset[i] records into the output)."""
+
+    def __init__(self, table: PatchTable, sizes):
+        self.table = table
+        self.sizes = [(int(h), int(w)) for h, w in sizes]
+        n = len(self.sizes)
+        H = (C.c_int * n)(*[h for h, _ in self.sizes])
+        W = (C.c_int * n)(*[w for _, w in self.sizes])
+        hb = C.c_void_p()
+        _check(lib().pt_batch_create(table._h, n, H, W, C.byref(hb)))
+        self._h = hb
+        po = np.empty(n, np.int64)
+        qo = np.empty(n, np.int64)
+        tot = np.empty(2, np.int64)
+        _check(lib().pt_batch_layout(hb, po.ctypes.data_as(C.c_void_p), qo.ctypes.data_as(C.c_void_p),
+                                     tot.ctypes.data_as(C.c_void_p)))
+        self.pixel_offset, self.patch_offset = po, qo
+        self.pixels, self.patches = int(tot[0]), int(tot[1])
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().pt_batch_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def lookup(self, d_rgb: int, d_ann: int, stream: int = 0) -> None:
+        self.table._sync_params()
+        _check(lib().pt_batch_lookup(self._h, C.c_void_p(d_rgb), C.c_void_p(d_ann), C.c_void_p(stream)))
+
+    def set_tile(self, patches_per_cta: int) -> None:
+        _check(lib().pt_batch_set_tile(self._h, int(patches_per_cta)))
+
+    @property
+    def tile(self) -> int:
+        return int(lib().pt_batch_tile(self._h))
+
+    def autotune(self, d_rgb: int, d_ann: int, stream: int = 0):
+        """(best patches per CTA, {patches per CTA: best ms of 3})."""
+        self.table._sync_params()
+        best = C.c_int()
+        ms = (C.c_float * 4)()
+        _check(lib().pt_batch_autotune(self._h, C.c_void_p(d_rgb), C.c_void_p(d_ann), C.c_void_p(stream), C.byref(best), ms))
+        return best.value, dict(zip((32, 64, 128, 256), list(ms)))
+
+    def capture(self, d_rgb: int, d_ann: int, stream: int = 0) -> None:
+        self.table._sync_params()
+        _check(lib().pt_batch_capture(self._h, C.c_void_p(d_rgb), C.c_void_p(d_ann), C.c_void_p(stream)))
+
+    def replay(self, stream: int = 0) -> None:
+        _check(lib().pt_batch_replay(self._h, C.c_void_p(stream)))
 
 
 def descriptor(params: PatchTableParams, img):

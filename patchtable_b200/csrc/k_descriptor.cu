@@ -46,13 +46,13 @@ __device__ __forceinline__ void yuv_exact(float R, float G, float B, float &Y, f
     V = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.615, r), __dmul_rn(-0.51499, g)), __dmul_rn(-0.10001, b)));
 }
 
-__global__ void __launch_bounds__(NT)
-k_descriptor(const DescPlan c_plan, const float *__restrict__ rgb, int h, int w, int convert,
-             float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh, int ew) {
-    extern __shared__ float smem[];
+
+/* One 64 x 8 block of patches with top-left patch (x0, y0). */
+__device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, const float *__restrict__ rgb, int h, int w,
+                                          int convert, float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh,
+                                          int ew, int x0, int y0) {
     float *pix = smem;                               /* 3 planes x RH x RWP */
     float *hs = smem + 3 * RH * RWP;                 /* ncombo x RH x TW */
-    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
     const int tid = threadIdx.x;
     const bool last_col = x0 + TW >= ew, last_row = y0 + TH >= eh;
     const int own_x1 = last_col ? w : x0 + TW, own_y1 = last_row ? h : y0 + TH;
@@ -105,6 +105,34 @@ k_descriptor(const DescPlan c_plan, const float *__restrict__ rgb, int h, int w,
         }
         float4 *dst = reinterpret_cast<float4 *>(desc + ((size_t) py * ew + px) * ds);
         for (int q = 0; q < ds / 4; q++) dst[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
+    }
+}
+
+__global__ void __launch_bounds__(NT)
+k_descriptor(const DescPlan c_plan, const float *__restrict__ rgb, int h, int w, int convert,
+             float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh, int ew) {
+    extern __shared__ float smem[];
+    desc_tile(c_plan, smem, rgb, h, w, convert, rgba, desc, ds, eh, ew, blockIdx.x * TW, blockIdx.y * TH);
+}
+
+/* Persistent descriptor pass over the 64 x 8 tiles of every image of a batch (images, RGBA
+   copies and descriptors concatenated). */
+__global__ void __launch_bounds__(NT)
+k_descriptor_batch(const DescPlan c_plan, const PtBatchImage *__restrict__ imgs, int n, long long ntiles,
+                   const float *__restrict__ rgb, int convert, float4 *__restrict__ rgba, float *__restrict__ desc, int ds) {
+    extern __shared__ float smem[];
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(&imgs[mid].tile_off) <= t) lo = mid; else hi = mid - 1;
+        }
+        const PtBatchImage &g = imgs[lo];
+        const long long lt = t - g.tile_off;
+        const int tpr = (g.ew + TW - 1) / TW;
+        desc_tile(c_plan, smem, rgb + 3 * g.pix_off, g.h, g.w, convert, rgba ? rgba + g.pix_off : nullptr,
+                  desc + g.patch_off * ds, ds, g.eh, g.ew, (int) (lt % tpr) * TW, (int) (lt / tpr) * TH);
+        __syncthreads();                                 /* the next tile reuses the shared memory */
     }
 }
 
@@ -167,6 +195,28 @@ pt_status pt_launch_descriptor(int ndims, int nchroma, const float *rgb, int h, 
     }
     dim3 grid((ew + TW - 1) / TW, (eh + TH - 1) / TH);
     k_descriptor<<<grid, NT, smem, st>>>(plan, rgb, h, w, convert, rgba, desc, ds, eh, ew);
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_descriptor_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
+                                     const float *rgb, int convert, float4 *rgba, float *desc, int ds, cudaStream_t st) {
+    DescPlan plan;
+    PT_TRY(make_plan(ndims, nchroma, plan));
+    if (ntiles <= 0) return PT_OK;
+    const size_t smem = pt_descriptor_smem(0);
+    static int nsm = 0, per = 0;
+    if (!nsm) {
+        int dev = 0;
+        PT_CUDA(cudaGetDevice(&dev));
+        PT_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        PT_CUDA(cudaFuncSetAttribute(k_descriptor_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_descriptor_batch, NT, smem));
+        if (per < 1) per = 1;
+    }
+    const long long g = (long long) per * nsm;
+    k_descriptor_batch<<<(unsigned) (ntiles < g ? ntiles : g), NT, smem, st>>>(plan, imgs, n, ntiles, rgb, convert, rgba, desc,
+                                                                              ds);
     PT_LAUNCHED();
     return PT_OK;
 }

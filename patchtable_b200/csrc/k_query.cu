@@ -38,6 +38,8 @@ struct QPlan {
     int step;                /* neighbour spacing of this pull pass (jump flooding) */
     int pull_max;            /* most neighbour candidates scored per patch */
     const float4 *b1;        /* b shifted by one pixel: b1[i] = b[i + 1] */
+    const int *allowed;      /* b patches that may be matched (allowed[p] == allowed_index), or NULL */
+    int allowed_index;
 };
 
 __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
@@ -49,11 +51,13 @@ __device__ __forceinline__ void count_work(unsigned long long *counters, unsigne
     if ((threadIdx.x & 31) == 0) { atomicAdd(counters, (unsigned long long) c); atomicAdd(counters + 1, (unsigned long long) r); }
 }
 
-constexpr int TW = 256;                   /* query patches per CTA row segment */
-constexpr int ATW = TW + 7;               /* pixels per staged a row */
+constexpr int TWD = 256;                  /* query patches per CTA row segment, single-image launches */
 
-/* Stages the 8 pixel rows under a CTA's row segment of query patches in shared memory. */
+/* Stages the 8 pixel rows under a CTA's row segment of TW query patches in shared memory
+   (TW + 7 pixels per row). */
+template<int TW>
 __device__ __forceinline__ void stage_a(float4 *atile, const float4 *__restrict__ a, int aw, int ah, int x0, int y) {
+    constexpr int ATW = TW + 7;
     for (int i = threadIdx.x; i < 8 * ATW; i += TW) {
         int r = i / ATW, c = i - r * ATW;
         int gx = x0 + c, gy = y + r;
@@ -99,8 +103,10 @@ __device__ __forceinline__ float lane_total(const float (&l)[4]) {
 
 /* patch_dist_exact with the query patch in shared memory; abandons the sum once a row's partial
    total reaches `bound` (+inf returned). */
+template<int TW>
 __device__ __forceinline__ float ssd_tile(const float4 *atile, int tx, const QPlan &q, const float4 *__restrict__ B,
                                           int bx, int by, float bound, unsigned &rows) {
+    constexpr int ATW = TW + 7;
     float l[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
     for (int dy = 0; dy < 8; dy++) {
@@ -119,10 +125,11 @@ __device__ __forceinline__ float ssd_tile(const float4 *atile, int tx, const QPl
    memory once per group; candidate g takes part when bit g of `valid` is set.  Each sum keeps the
    reference's lane order and stops once its partial total reaches `bound`.  out[g] = the full sum,
    or +inf when stopped or not taking part. */
-template<int G>
+template<int TW, int G>
 __device__ __forceinline__ void ssd_group(const float4 *atile, int tx, const QPlan &q, const float4 *__restrict__ B,
                                           const int (&cand)[G], unsigned valid, float bound, float (&out)[G],
                                           unsigned &rows) {
+    constexpr int ATW = TW + 7;
     float l[G][4];
     bool live[G];
 #pragma unroll
@@ -164,14 +171,13 @@ struct LearnedArgs {
    instantiation replaces, for patches whose proposal confidence reaches the threshold, the table
    candidate by the network's proposals (scored best-first in groups of three) and, unless
    configured otherwise, skips k-coherence for them. */
-template<bool LEARNED>
-__global__ void __launch_bounds__(TW)
-k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
-              const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
-              int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters, const LearnedArgs la) {
-    extern __shared__ float4 atile[];
-    const int x0 = blockIdx.x * TW, y = blockIdx.y;
-    stage_a(atile, a, c_q.aw, c_q.ah, x0, y);
+template<int TW, bool LEARNED>
+__device__ __forceinline__ void
+choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const float4 *__restrict__ b,
+           const int *__restrict__ cur_pos, const float *__restrict__ cur_d, const int *__restrict__ tcand,
+           const int2 *__restrict__ kcoh, int do_table, int *ch_pos, float *ch_d, int *kc_done, int use_done,
+           unsigned long long *counters, const LearnedArgs &la, int x0, int y) {
+    stage_a<TW>(atile, a, c_q.aw, c_q.ah, x0, y);
     __syncthreads();
     const int x = x0 + threadIdx.x;
     const bool live = x < c_q.ew;
@@ -209,7 +215,7 @@ k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__res
                 if (!m) continue;
                 const int cg[G] = {cand[g0], cand[g0 + 1], g0 + 2 <= PT_PROP_TOPK ? cand[g0 + 2] : -1};
                 float d[G];
-                ssd_group<G>(atile, threadIdx.x, c_q, b, cg, m, dbest, d, rows);
+                ssd_group<TW, G>(atile, threadIdx.x, c_q, b, cg, m, dbest, d, rows);
 #pragma unroll
                 for (int g = 0; g < G; g++)
                     if (((m >> g) & 1) && d[g] < dbest) { dbest = d[g]; dch = d[g]; xb = pt_x(cg[g]); yb = pt_y(cg[g]); }
@@ -221,7 +227,7 @@ k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__res
             int v = tcand[p];
             int xs = pt_x(v) - 7, ys = pt_y(v) - 7;
             if (xs != xb || ys != yb) {
-                float dc = ssd_tile(atile, threadIdx.x, c_q, b, xs, ys, dbest, rows);
+                float dc = ssd_tile<TW>(atile, threadIdx.x, c_q, b, xs, ys, dbest, rows);
                 ne++;
                 if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
             }
@@ -265,7 +271,7 @@ k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__res
                 if (m != (1u << G) - 1) done = true;     /* the list ends or stops inside this group */
                 if (!m) break;
                 float d[G];
-                ssd_group<G>(atile, threadIdx.x, c_q, b, cg, m, dbest, d, rows);
+                ssd_group<TW, G>(atile, threadIdx.x, c_q, b, cg, m, dbest, d, rows);
                 ne += __popc(m);
 #pragma unroll
                 for (int j = 0; j < G; j++) {
@@ -286,6 +292,16 @@ k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__res
     }
 }
 
+template<bool LEARNED>
+__global__ void __launch_bounds__(TWD)
+k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
+              const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
+              int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters, const LearnedArgs la) {
+    extern __shared__ float4 atile[];
+    choose_seg<TWD, LEARNED>(c_q, atile, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done, use_done,
+                             counters, la, blockIdx.x * TWD, blockIdx.y);
+}
+
 /* Step 4 as a pull: the best of the stored match and every neighbour's chosen offset applied to
    this patch.  The patch's own choice comes first; the distinct neighbour candidates follow in
    increasing order of the distance their neighbour achieved with them (the likeliest good ones
@@ -293,14 +309,12 @@ k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__res
    Neighbours sit `step` patches apart; passes with decreasing steps (jump flooding) carry an
    offset across a region in a logarithmic number of passes, where the reference's sequential
    sweep carries it along a whole row in one sweep. */
-template<int R>
-__global__ void __launch_bounds__(TW)
-k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
-            const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
-            int *nxt_pos, float *nxt_d, unsigned long long *counters) {
-    extern __shared__ float4 atile[];
-    const int x0 = blockIdx.x * TW, y = blockIdx.y;
-    stage_a(atile, a, c_q.aw, c_q.ah, x0, y);
+template<int TW, int R>
+__device__ __forceinline__ void
+pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const float4 *__restrict__ b,
+         const int *__restrict__ cur_pos, const float *__restrict__ cur_d, const int *__restrict__ ch_pos,
+         const float *__restrict__ ch_d, int *nxt_pos, float *nxt_d, unsigned long long *counters, int x0, int y) {
+    stage_a<TW>(atile, a, c_q.aw, c_q.ah, x0, y);
     __syncthreads();
     const int x = x0 + threadIdx.x;
     const bool live = x < c_q.ew;
@@ -333,6 +347,7 @@ k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restr
                 const int cp = ch_pos[q];
                 const int xs = pt_x(cp) - S * dx, ys = pt_y(cp) - S * dy;
                 if (xs < 0 || ys < 0 || xs >= c_q.bew || ys >= c_q.beh) continue;
+                if (c_q.allowed && __ldg(c_q.allowed + (size_t) ys * c_q.bew + xs) != c_q.allowed_index) continue;
                 int c = pt_xy(xs, ys);
                 bool dup = c == bpos;
 #pragma unroll
@@ -358,7 +373,7 @@ k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restr
                 const int left = nc - g0;
                 const unsigned m = left >= G ? (1u << G) - 1 : (1u << left) - 1;
                 float d[G];
-                ssd_group<G>(atile, threadIdx.x, c_q, b, cg, m, bd, d, rows);
+                ssd_group<TW, G>(atile, threadIdx.x, c_q, b, cg, m, bd, d, rows);
 #pragma unroll
                 for (int g = 0; g < G; g++)
                     if (((m >> g) & 1) && d[g] < bd) { bd = d[g]; bpos = cg[g]; }
@@ -369,6 +384,74 @@ k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restr
         nxt_d[p] = bd;
     }
     count_work(counters, ne, rows);
+}
+
+template<int R>
+__global__ void __launch_bounds__(TWD)
+k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
+            const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
+            int *nxt_pos, float *nxt_d, unsigned long long *counters) {
+    extern __shared__ float4 atile[];
+    pull_seg<TWD, R>(c_q, atile, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, counters, blockIdx.x * TWD, blockIdx.y);
+}
+
+/* ---- batched queries: many images, one launch per phase over a flattened segment list ---- */
+
+/* Index of the image that owns flattened segment s (segs[i] = first segment of image i). */
+__device__ __forceinline__ int owner(const PtBatchImage *__restrict__ imgs, int n, long long s, int twi) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&imgs[mid].seg_off[twi]) <= s) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+/* Persistent choose over every row segment of every image: CTA b takes segments b, b + grid, ... */
+template<int TW>
+__global__ void __launch_bounds__(TW)
+k_choose_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, long long nseg, int twi,
+               const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
+               const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
+               int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters) {
+    extern __shared__ float4 atile[];
+    LearnedArgs none;
+    none.cand = nullptr; none.conf = nullptr; none.threshold = 0.f; none.kcoh_confident = 0; none.counters = nullptr;
+    for (long long s = blockIdx.x; s < nseg; s += gridDim.x) {
+        const int i = owner(imgs, n, s, twi);
+        const PtBatchImage &g = imgs[i];
+        const long long ls = s - g.seg_off[twi];
+        const int spr = (g.ew + TW - 1) / TW;
+        const int y = (int) (ls / spr), x0 = (int) (ls % spr) * TW;
+        QPlan q = base;
+        q.aw = g.w; q.ah = g.h; q.ew = g.ew; q.eh = g.eh;
+        const long long o = g.patch_off;
+        choose_seg<TW, false>(q, atile, a + g.pix_off, b, cur_pos + o, cur_d + o, tcand + o, kcoh, do_table, ch_pos + o,
+                              ch_d + o, kc_done + o, use_done, counters, none, x0, y);
+        __syncthreads();                       /* the next segment restages atile */
+    }
+}
+
+template<int TW, int R>
+__global__ void __launch_bounds__(TW)
+k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, long long nseg, int twi,
+             const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
+             const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
+             int *nxt_pos, float *nxt_d, unsigned long long *counters) {
+    extern __shared__ float4 atile[];
+    for (long long s = blockIdx.x; s < nseg; s += gridDim.x) {
+        const int i = owner(imgs, n, s, twi);
+        const PtBatchImage &g = imgs[i];
+        const long long ls = s - g.seg_off[twi];
+        const int spr = (g.ew + TW - 1) / TW;
+        const int y = (int) (ls / spr), x0 = (int) (ls % spr) * TW;
+        QPlan q = base;
+        q.aw = g.w; q.ah = g.h; q.ew = g.ew; q.eh = g.eh;
+        const long long o = g.patch_off;
+        pull_seg<TW, R>(q, atile, a + g.pix_off, b, cur_pos + o, cur_d + o, ch_pos + o, ch_d + o, nxt_pos + o, nxt_d + o,
+                        counters, x0, y);
+        __syncthreads();
+    }
 }
 
 __global__ void k_init(int n, int pos, float d, int *cur_pos, float *cur_d) {
@@ -400,6 +483,8 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     q.step = s.step < 1 ? 1 : s.step;
     q.pull_max = s.pull_max > 0 ? s.pull_max : 1 << 30;
     q.b1 = s.b1;
+    q.allowed = s.allowed;
+    q.allowed_index = s.allowed_index;
     if (!q.b1) return pt_fail(PT_BAD_ARG, "query without the shifted copy of the table image");
     if (q.radius > 2) return pt_fail(PT_UNSUPPORTED, "propagation radius %d > 2 on the GPU path", q.radius);
     return PT_OK;
@@ -417,10 +502,10 @@ pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const fl
     QPlan q;
     PT_TRY(make_qplan(s, q));
     (void) n;
-    dim3 grid((q.ew + TW - 1) / TW, q.eh);
+    dim3 grid((q.ew + TWD - 1) / TWD, q.eh);
     LearnedArgs none;
     memset(&none, 0, sizeof(none));
-    k_choose_tile<false><<<grid, TW, sizeof(float4) * 8 * ATW, st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos,
+    k_choose_tile<false><<<grid, TWD, sizeof(float4) * 8 * (TWD + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos,
                                                                    ch_d, kc_done, use_done, evals, none);
     PT_LAUNCHED();
     return PT_OK;
@@ -440,8 +525,8 @@ pt_status pt_launch_choose_learned(const QuerySetup &s, const float4 *a, const f
     la.threshold = threshold;
     la.kcoh_confident = kcoh_confident;
     la.counters = lcounters;
-    dim3 grid((q.ew + TW - 1) / TW, q.eh);
-    k_choose_tile<true><<<grid, TW, sizeof(float4) * 8 * ATW, st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos,
+    dim3 grid((q.ew + TWD - 1) / TWD, q.eh);
+    k_choose_tile<true><<<grid, TWD, sizeof(float4) * 8 * (TWD + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos,
                                                                   ch_d, kc_done, use_done, evals, la);
     PT_LAUNCHED();
     return PT_OK;
@@ -453,17 +538,84 @@ pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const floa
     QPlan q;
     PT_TRY(make_qplan(s, q));
     (void) n;
-    dim3 grid((q.ew + TW - 1) / TW, q.eh);
+    dim3 grid((q.ew + TWD - 1) / TWD, q.eh);
     if (q.radius <= 1)
-        k_pull_tile<1><<<grid, TW, sizeof(float4) * 8 * ATW, st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals);
+        k_pull_tile<1><<<grid, TWD, sizeof(float4) * 8 * (TWD + 7), st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals);
     else
-        k_pull_tile<2><<<grid, TW, sizeof(float4) * 8 * ATW, st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals);
+        k_pull_tile<2><<<grid, TWD, sizeof(float4) * 8 * (TWD + 7), st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals);
     PT_LAUNCHED();
     return PT_OK;
 }
 
 pt_status pt_launch_output(int n, const int *pos, const float *d, double *ann, cudaStream_t st) {
     k_output<<<(n + NT - 1) / NT, NT, 0, st>>>(n, pos, d, ann);
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+/* ---- batched launchers ---- */
+
+namespace {
+
+constexpr int BATCH_TW[PT_BATCH_NTW] = {32, 64, 128, 256};
+
+template<class K>
+int persistent_grid(K kernel, int threads, size_t smem, long long work) {
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    }
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1) per = 1;
+    const long long g = (long long) per * nsm;
+    return (int) (work < g ? work : g);
+}
+
+}  // namespace
+
+int pt_batch_tw(int twi) { return (twi >= 0 && twi < PT_BATCH_NTW) ? BATCH_TW[twi] : 0; }
+
+pt_status pt_launch_choose_batch(const QuerySetup &s, const PtBatchImage *imgs, int n, long long nseg, int twi,
+                                 const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
+                                 const int *tcand, const int2 *kcoh, int do_table, int *ch_pos, float *ch_d, int *kc_done,
+                                 int use_done, unsigned long long *evals, cudaStream_t st) {
+    QPlan q;
+    PT_TRY(make_qplan(s, q));
+    if (nseg <= 0) return PT_OK;
+#define PT_CHOOSE_B(T) { const size_t sm = sizeof(float4) * 8 * (T + 7); \
+        const int g = persistent_grid(k_choose_batch<T>, T, sm, nseg); \
+        k_choose_batch<T><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, \
+                                            kc_done, use_done, evals); }
+    switch (BATCH_TW[twi]) {
+        case 32: PT_CHOOSE_B(32) break;
+        case 64: PT_CHOOSE_B(64) break;
+        case 128: PT_CHOOSE_B(128) break;
+        default: PT_CHOOSE_B(256) break;
+    }
+#undef PT_CHOOSE_B
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_pull_batch(const QuerySetup &s, const PtBatchImage *imgs, int n, long long nseg, int twi,
+                               const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d, const int *ch_pos,
+                               const float *ch_d, int *nxt_pos, float *nxt_d, unsigned long long *evals, cudaStream_t st) {
+    QPlan q;
+    PT_TRY(make_qplan(s, q));
+    if (nseg <= 0) return PT_OK;
+#define PT_PULL_B(T, RR) { const size_t sm = sizeof(float4) * 8 * (T + 7); \
+        const int g = persistent_grid(k_pull_batch<T, RR>, T, sm, nseg); \
+        k_pull_batch<T, RR><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals); }
+    const bool r1 = q.radius <= 1;
+    switch (BATCH_TW[twi]) {
+        case 32: if (r1) PT_PULL_B(32, 1) else PT_PULL_B(32, 2) break;
+        case 64: if (r1) PT_PULL_B(64, 1) else PT_PULL_B(64, 2) break;
+        case 128: if (r1) PT_PULL_B(128, 1) else PT_PULL_B(128, 2) break;
+        default: if (r1) PT_PULL_B(256, 1) else PT_PULL_B(256, 2) break;
+    }
+#undef PT_PULL_B
     PT_LAUNCHED();
     return PT_OK;
 }

@@ -52,6 +52,8 @@ struct QuerySetup {
     int step = 1;            /* neighbour spacing of a pull pass */
     int pull_max = 0;        /* most neighbour candidates a pull scores per patch (0 = all) */
     const float4 *b1 = nullptr;   /* the table image shifted by one pixel, b1[i] = b[i + 1] */
+    const int *allowed = nullptr; /* b patches a match may use (allowed[p] == allowed_index), or NULL */
+    int allowed_index = 0;
     cudaStream_t stream;
 };
 /* Query schedule.  By default two choose + pull passes stand in for each of the reference's
@@ -91,6 +93,27 @@ pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const floa
                          unsigned long long *evals, cudaStream_t st);
 pt_status pt_launch_output(int n, const int *pos, const float *d, double *ann, cudaStream_t st);
 
+/* Batched queries (pt_batch.cu): the images of a batch are concatenated -- pixels, patches and
+   query state -- and every phase is one persistent launch over the flattened list of row
+   segments.  seg_off[t] is the image's first segment when a CTA covers PT_BATCH_TW(t) patches. */
+#define PT_BATCH_NTW 4
+struct PtBatchImage {
+    int h, w, eh, ew;
+    long long pix_off, patch_off;
+    long long seg_off[PT_BATCH_NTW];
+    long long tile_off;                  /* first 64 x 8 descriptor tile */
+};
+int pt_batch_tw(int twi);
+pt_status pt_launch_choose_batch(const QuerySetup &s, const PtBatchImage *imgs, int n, long long nseg, int twi,
+                                 const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
+                                 const int *tcand, const int2 *kcoh, int do_table, int *ch_pos, float *ch_d, int *kc_done,
+                                 int use_done, unsigned long long *evals, cudaStream_t st);
+pt_status pt_launch_pull_batch(const QuerySetup &s, const PtBatchImage *imgs, int n, long long nseg, int twi,
+                               const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d, const int *ch_pos,
+                               const float *ch_d, int *nxt_pos, float *nxt_d, unsigned long long *evals, cudaStream_t st);
+pt_status pt_launch_descriptor_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
+                                     const float *rgb, int convert, float4 *rgba, float *desc, int ds, cudaStream_t st);
+
 /* Read-only view of a built table, for entry points outside pt_table.cu. */
 struct PtTableView {
     pt_params p;
@@ -102,6 +125,7 @@ struct PtTableView {
     const int2 *kcoh;
     PtBins bins;
     const float *b_desc;                 /* (h-7) x (w-7) x ds */
+    const int *allowed;                  /* (h-7) x (w-7) allowed mask of the build, or NULL */
     const float *part;                   /* per grid dimension: centres, left sizes, right sizes */
     int part_ofs[PT_DESC_MAX];           /* offset of dimension d's centres in part */
     int nslices[PT_DESC_MAX];

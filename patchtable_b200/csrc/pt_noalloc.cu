@@ -103,6 +103,8 @@ extern "C" pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_
     if (qs.radius > 2) qs.radius = 2;
     qs.b1 = v.b_rgba1;
     qs.pull_max = p.gpu_pull_max;
+    qs.allowed = v.allowed;
+    qs.allowed_index = p.allowed_index;
     qs.stream = st;
     PT_TRY(pt_launch_init(n, pt_xy(v.w - 7 + 1, 0), (float) PT_DIST_INF, pos[0], dd[0], st));
     int passes = pt_default_passes(p);

@@ -467,6 +467,8 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     qs.radius = p.query_step + p.prop_dist;
     qs.b1 = t->b_rgba1.p;
     qs.pull_max = p.gpu_pull_max;
+    qs.allowed = t->allowed.p;
+    qs.allowed_index = p.allowed_index;
     qs.stream = st;
     if (qs.radius > 2) qs.radius = 2;
     /* Initial field (patchtable.h:3538-3547): x = b0_ew + 1, dist = DIST_INFINITY. */
@@ -641,12 +643,6 @@ pt_status pt_table_proposal_infer(pt_table *t, pt_proposal *net, const float *d_
     return pt_prop_check_error(net, st);
 }
 
-pt_status pt_table_lookup_batch(pt_table *t, int n, const float *const *a, const int *h, const int *w,
-                                double *const *ann_out) {
-    if (!t || n < 0 || (n > 0 && (!a || !h || !w || !ann_out))) return pt_fail(PT_BAD_ARG, "null argument");
-    for (int i = 0; i < n; i++) PT_TRY(pt_table_lookup(t, a[i], h[i], w[i], ann_out[i], nullptr, nullptr, nullptr));
-    return PT_OK;
-}
 
 int pt_table_shape(const pt_table *t, int *nslices, int64_t *ncells) {
     if (!t) return -1;
@@ -766,6 +762,7 @@ pt_status pt_table_view(const pt_table *t, PtTableView *v) {
     v->kcoh = t->kcoh.p;
     v->bins = t->bins;
     v->b_desc = t->b_desc.p;
+    v->allowed = t->allowed.p;
     v->part = t->part_dev.p;
     for (int d = 0; d < PT_DESC_MAX; d++) {
         v->part_ofs[d] = d < t->G ? t->part_ofs[d] : 0;
