@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--profile-case", choices=["query", "query-default", "infer"], default=None)
     return ap.parse_args()
 
@@ -280,6 +281,98 @@ def learned_comparison(table, da, H, W, dann, sptr, flush, P):
     return out
 
 
+def _event_ms(fn, reps):
+    """Best device time (CUDA events on the current stream) of `reps` calls of fn after one warm-up."""
+    import torch
+    st = torch.cuda.current_stream()
+    fn()
+    best = None
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    return best
+
+
+def uneven_batch_measure():
+    """64 query images with sides uniform in [128, 2048] against one 1920x1080 table: the batched
+    query (autotuned patches per CTA, replayed as one captured CUDA graph) against one
+    pt_table_lookup_device call per image, at 2, 4 and 8 propagation passes."""
+    import torch
+    import patchtable_b200 as ptb
+    from patchtable_b200 import synth
+    from patchtable_b200.metrics import get_mean_dist
+    table_img, queries = synth.uneven_batch()
+    params = ptb.PatchTableParams(WORKLOAD["switches"])
+    ctypes.CDLL(None).srand(1)
+    table = ptb.PatchTable(params, table_img)
+    qb = table.batch([q.shape[:2] for q in queries])
+    rgb = torch.empty(qb.pixels * 3, dtype=torch.float32, device="cuda")
+    for q, o in zip(queries, qb.pixel_offset):
+        rgb[3 * o:3 * o + q.size] = torch.from_numpy(q.ravel()).cuda()
+    ann = torch.empty(qb.patches * 3, dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    P = qb.patches
+
+    def per_image():
+        for q, po, qo in zip(queries, qb.pixel_offset, qb.patch_offset):
+            table.lookup_device(rgb.data_ptr() + 12 * int(po), q.shape[0], q.shape[1], ann.data_ptr() + 24 * int(qo), st)
+
+    rows = {}
+    for passes, jump, pm in ((2, 2, 0), (4, 8, 0), (8, 8, 0), SCHEDULES[0]):
+        params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = passes, jump, pm
+        best, tune = qb.autotune(rgb.data_ptr(), ann.data_ptr(), st)
+        qb.capture(rgb.data_ptr(), ann.data_ptr(), st)
+        g_ms = _event_ms(lambda: qb.replay(st), 3)
+        md = get_mean_dist(ann.view(-1, 3).cpu().numpy()[None])
+        pi_ms = _event_ms(per_image, 2)
+        rows["%d/%d/%d" % (passes, jump, pm)] = {
+            "graph_patches_per_s": P / (g_ms / 1000.0), "per_image_patches_per_s": P / (pi_ms / 1000.0),
+            "speedup": pi_ms / g_ms, "mean_nnf_dist": md, "patches_per_cta": best,
+            "autotune_ms": {str(k): v for k, v in tune.items()}}
+    qb.close()
+    return {"images": len(queries), "patches": P, "table_image": [1080, 1920],
+            "workload": "64 queries, sides U[128, 2048], crops of the warped 2048^2 base (seeds 4000+i)",
+            "schedules": rows}
+
+
+def one_vs_many_measure():
+    """One 1024x768 query against 10 database images (sides U[256, 2048]) packed into one atlas
+    table, seam-straddling patches excluded by the allowed mask."""
+    import torch
+    import patchtable_b200 as ptb
+    from patchtable_b200 import synth
+    from patchtable_b200.metrics import get_mean_dist
+    query, atlas, allowed, boxes = synth.one_vs_many()
+    params = ptb.PatchTableParams(WORKLOAD["switches"])
+    ctypes.CDLL(None).srand(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    table = ptb.PatchTable(params, atlas, allowed_patches=allowed)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    H, W = query.shape[:2]
+    P = (H - 7) * (W - 7)
+    da = torch.from_numpy(query).cuda()
+    dann = torch.empty((H - 7, W - 7, 3), dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    rows = {}
+    for sched in (SCHEDULES[0], (0, 0, 0)):
+        params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = sched
+        ms = _event_ms(lambda: table.lookup_device(da.data_ptr(), H, W, dann.data_ptr(), st), 3)
+        ann = dann.cpu().numpy()
+        ok = bool(np.all(allowed[ann[..., 1].astype(int), ann[..., 0].astype(int)] == 1))
+        rows["%d/%d/%d" % sched] = {"patches_per_s": P / (ms / 1000.0), "ms": ms, "mean_nnf_dist": get_mean_dist(ann),
+                                    "all_matches_allowed": ok}
+    table.close()
+    return {"query": [H, W], "atlas": list(atlas.shape[:2]), "database_images": len(boxes),
+            "allowed_patches": int(allowed.sum()), "build_s": build_s, "schedules": rows}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -329,6 +422,12 @@ def main():
         if m <= 1.01 * ref_md and (chosen is None or ms < chosen[0]):
             chosen = (ms, sched)
     chosen = chosen[1] if chosen else SCHEDULES[-1]
+    # query patches per CTA: the results do not depend on it, only the time does
+    tile_ms = {}
+    for tile in (32, 64, 128, 256):
+        params.gpu_tile = tile
+        tile_ms[tile], _ = timed_schedule(table, chosen, da, H, W, dann, sptr, flush)
+    params.gpu_tile = min(tile_ms, key=tile_ms.get)
     params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = chosen
     for _ in range(max(args.warmup, 3)):
         flush.zero_()
@@ -421,6 +520,12 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(a, b)
+    c4 = c3 = None
+    if rank == 0 and not args.no_batch:
+        del flush
+        torch.cuda.empty_cache()
+        c4 = uneven_batch_measure()
+        c3 = one_vs_many_measure()
 
     if world > 1:
         dist.barrier()
@@ -435,8 +540,10 @@ def main():
                    "build_s": build_s, "mean_nnf_dist": md, "mean_nnf_dist_e2e": md_e2e,
                    "reference_mean_nnf_dist": ref_md,
                    "schedule": {"passes": chosen[0], "first_jump": chosen[1], "pull_max": chosen[2], "tried": sched_md,
+                                "patches_per_cta": params.gpu_tile, "patches_per_cta_ms": {str(k): v for k, v in tile_ms.items()},
                                 "rule": "fastest schedule with mean NNF dist <= 1.01 x the reference's on this workload"},
                    "library_default_schedule": default_sched, "learned": learned,
+                   "uneven_batch": c4, "one_vs_many": c3,
                    "l2": "flushed between steps (256 MiB write)", "parallelism": "replicas" if world > 1 else "single",
                    "stage_ms_per_step": {k: v / args.steps for k, v in stages.items()},
                    "outer_event_ms_per_step": sum(outer) / len(outer), "wall_ms_per_step": 1000 * wall / args.steps,

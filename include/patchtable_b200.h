@@ -61,10 +61,13 @@ typedef struct pt_params {
        that replace the reference's sequential scanline sweeps (0 picks the default), and the
        neighbour spacing of the first pass, halved on each later pass down to 1 (jump
        flooding; 0 or 1 = plain neighbours), and the most neighbour offsets a pull pass scores per
-       patch, best-first by the neighbour's own distance (0 = all of them). */
+       patch, best-first by the neighbour's own distance (0 = all of them), and the query patches one
+       CTA covers in the choose and pull kernels (32, 64, 128 or 256; 0 picks the default, 32; the
+       result does not depend on it). */
     int gpu_prop_passes;
     int gpu_jump;
     int gpu_pull_max;
+    int gpu_tile;
 } pt_params;
 
 typedef struct pt_table pt_table;

@@ -68,6 +68,7 @@ class _Params(C.Structure):
         ("gpu_prop_passes", C.c_int),
         ("gpu_jump", C.c_int),
         ("gpu_pull_max", C.c_int),
+        ("gpu_tile", C.c_int),
     ]
 
 

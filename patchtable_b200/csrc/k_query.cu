@@ -37,6 +37,7 @@ struct QPlan {
     int do_kcoh;
     int step;                /* neighbour spacing of this pull pass (jump flooding) */
     int pull_max;            /* most neighbour candidates scored per patch */
+    int tile;                /* query patches per CTA (single-image launches) */
     const float4 *b1;        /* b shifted by one pixel: b1[i] = b[i + 1] */
     const int *allowed;      /* b patches that may be matched (allowed[p] == allowed_index), or NULL */
     int allowed_index;
@@ -51,7 +52,7 @@ __device__ __forceinline__ void count_work(unsigned long long *counters, unsigne
     if ((threadIdx.x & 31) == 0) { atomicAdd(counters, (unsigned long long) c); atomicAdd(counters + 1, (unsigned long long) r); }
 }
 
-constexpr int TWD = 256;                  /* query patches per CTA row segment, single-image launches */
+constexpr int TWD = 32;                   /* query patches per CTA row segment when none is chosen */
 
 /* Stages the 8 pixel rows under a CTA's row segment of TW query patches in shared memory
    (TW + 7 pixels per row). */
@@ -292,14 +293,14 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
     }
 }
 
-template<bool LEARNED>
-__global__ void __launch_bounds__(TWD)
+template<int TW, bool LEARNED>
+__global__ void __launch_bounds__(TW)
 k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
               const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
               int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters, const LearnedArgs la) {
     extern __shared__ float4 atile[];
-    choose_seg<TWD, LEARNED>(c_q, atile, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done, use_done,
-                             counters, la, blockIdx.x * TWD, blockIdx.y);
+    choose_seg<TW, LEARNED>(c_q, atile, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done, use_done,
+                            counters, la, blockIdx.x * TW, blockIdx.y);
 }
 
 /* Step 4 as a pull: the best of the stored match and every neighbour's chosen offset applied to
@@ -386,13 +387,13 @@ pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const fl
     count_work(counters, ne, rows);
 }
 
-template<int R>
-__global__ void __launch_bounds__(TWD)
+template<int TW, int R>
+__global__ void __launch_bounds__(TW)
 k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
             const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
             int *nxt_pos, float *nxt_d, unsigned long long *counters) {
     extern __shared__ float4 atile[];
-    pull_seg<TWD, R>(c_q, atile, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, counters, blockIdx.x * TWD, blockIdx.y);
+    pull_seg<TW, R>(c_q, atile, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, counters, blockIdx.x * TW, blockIdx.y);
 }
 
 /* ---- batched queries: many images, one launch per phase over a flattened segment list ---- */
@@ -482,6 +483,9 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     q.do_kcoh = s.kcoherence > 0;
     q.step = s.step < 1 ? 1 : s.step;
     q.pull_max = s.pull_max > 0 ? s.pull_max : 1 << 30;
+    q.tile = s.tile > 0 ? s.tile : TWD;
+    if (q.tile != 32 && q.tile != 64 && q.tile != 128 && q.tile != 256)
+        return pt_fail(PT_BAD_ARG, "gpu_tile %d: query patches per CTA must be 32, 64, 128 or 256", s.tile);
     q.b1 = s.b1;
     q.allowed = s.allowed;
     q.allowed_index = s.allowed_index;
@@ -502,11 +506,18 @@ pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const fl
     QPlan q;
     PT_TRY(make_qplan(s, q));
     (void) n;
-    dim3 grid((q.ew + TWD - 1) / TWD, q.eh);
     LearnedArgs none;
     memset(&none, 0, sizeof(none));
-    k_choose_tile<false><<<grid, TWD, sizeof(float4) * 8 * (TWD + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos,
-                                                                   ch_d, kc_done, use_done, evals, none);
+#define PT_CHOOSE_T(T) { dim3 grid((q.ew + T - 1) / T, q.eh); \
+        k_choose_tile<T, false><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, \
+                                                                             ch_pos, ch_d, kc_done, use_done, evals, none); }
+    switch (q.tile) {
+        case 32: PT_CHOOSE_T(32) break;
+        case 64: PT_CHOOSE_T(64) break;
+        case 128: PT_CHOOSE_T(128) break;
+        default: PT_CHOOSE_T(256) break;
+    }
+#undef PT_CHOOSE_T
     PT_LAUNCHED();
     return PT_OK;
 }
@@ -525,9 +536,16 @@ pt_status pt_launch_choose_learned(const QuerySetup &s, const float4 *a, const f
     la.threshold = threshold;
     la.kcoh_confident = kcoh_confident;
     la.counters = lcounters;
-    dim3 grid((q.ew + TWD - 1) / TWD, q.eh);
-    k_choose_tile<true><<<grid, TWD, sizeof(float4) * 8 * (TWD + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos,
-                                                                  ch_d, kc_done, use_done, evals, la);
+#define PT_CHOOSE_L(T) { dim3 grid((q.ew + T - 1) / T, q.eh); \
+        k_choose_tile<T, true><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, \
+                                                                            ch_pos, ch_d, kc_done, use_done, evals, la); }
+    switch (q.tile) {
+        case 32: PT_CHOOSE_L(32) break;
+        case 64: PT_CHOOSE_L(64) break;
+        case 128: PT_CHOOSE_L(128) break;
+        default: PT_CHOOSE_L(256) break;
+    }
+#undef PT_CHOOSE_L
     PT_LAUNCHED();
     return PT_OK;
 }
@@ -538,11 +556,17 @@ pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const floa
     QPlan q;
     PT_TRY(make_qplan(s, q));
     (void) n;
-    dim3 grid((q.ew + TWD - 1) / TWD, q.eh);
-    if (q.radius <= 1)
-        k_pull_tile<1><<<grid, TWD, sizeof(float4) * 8 * (TWD + 7), st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals);
-    else
-        k_pull_tile<2><<<grid, TWD, sizeof(float4) * 8 * (TWD + 7), st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals);
+#define PT_PULL_T(T, RR) { dim3 grid((q.ew + T - 1) / T, q.eh); \
+        k_pull_tile<T, RR><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, \
+                                                                         evals); }
+    const bool r1 = q.radius <= 1;
+    switch (q.tile) {
+        case 32: if (r1) PT_PULL_T(32, 1) else PT_PULL_T(32, 2) break;
+        case 64: if (r1) PT_PULL_T(64, 1) else PT_PULL_T(64, 2) break;
+        case 128: if (r1) PT_PULL_T(128, 1) else PT_PULL_T(128, 2) break;
+        default: if (r1) PT_PULL_T(256, 1) else PT_PULL_T(256, 2) break;
+    }
+#undef PT_PULL_T
     PT_LAUNCHED();
     return PT_OK;
 }

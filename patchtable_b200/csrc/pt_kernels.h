@@ -51,6 +51,7 @@ struct QuerySetup {
     int kcoherence, kcoherence_step, radius;
     int step = 1;            /* neighbour spacing of a pull pass */
     int pull_max = 0;        /* most neighbour candidates a pull scores per patch (0 = all) */
+    int tile = 0;            /* query patches per CTA in choose / pull: 32, 64, 128, 256 (0 = 32) */
     const float4 *b1 = nullptr;   /* the table image shifted by one pixel, b1[i] = b[i + 1] */
     const int *allowed = nullptr; /* b patches a match may use (allowed[p] == allowed_index), or NULL */
     int allowed_index = 0;

@@ -138,7 +138,7 @@ pt_status apply_switches(pt_params *p, const std::vector<std::string> &argv) {
     BOOL_SW(init_random) BOOL_SW(sanitize_input) BOOL_SW(do_table_lookup)
     INT_SW(grid_ndims) DBL_SW(table_ratio) INT_SW(prop_dist)
     BOOL_SW(is_descriptor) BOOL_SW(descriptor_padded)
-    INT_SW(gpu_prop_passes) INT_SW(gpu_jump) INT_SW(gpu_pull_max)
+    INT_SW(gpu_prop_passes) INT_SW(gpu_jump) INT_SW(gpu_pull_max) INT_SW(gpu_tile)
 #undef INT_SW
 #undef BOOL_SW
 #undef DBL_SW
@@ -203,6 +203,7 @@ void pt_params_default(pt_params *p) {
     p->gpu_prop_passes = 0;
     p->gpu_jump = 0;
     p->gpu_pull_max = 0;
+    p->gpu_tile = 0;
     pt_params_set_speed(p, 3);
 }
 

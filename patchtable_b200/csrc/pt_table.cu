@@ -467,6 +467,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     qs.radius = p.query_step + p.prop_dist;
     qs.b1 = t->b_rgba1.p;
     qs.pull_max = p.gpu_pull_max;
+    qs.tile = p.gpu_tile;
     qs.allowed = t->allowed.p;
     qs.allowed_index = p.allowed_index;
     qs.stream = st;
@@ -716,6 +717,7 @@ pt_status pt_table_set_params(pt_table *t, const pt_params *p) {
     q.gpu_prop_passes = p->gpu_prop_passes;
     q.gpu_jump = p->gpu_jump;
     q.gpu_pull_max = p->gpu_pull_max;
+    q.gpu_tile = p->gpu_tile;
     if (p->do_rs || p->spatial || p->init_random)
         return pt_fail(PT_UNSUPPORTED, "random/spatial search and init_random are not implemented on the GPU path");
     return PT_OK;

@@ -140,6 +140,53 @@ def batch_sizes(n: int, lo: int, hi: int, seed: int):
     return [(int(rng.integers(lo, hi + 1)), int(rng.integers(lo, hi + 1))) for _ in range(n)]
 
 
+def uneven_batch(n: int = 64, lo: int = 128, hi: int = 2048, seed: int = 4000):
+    """Uneven query batch against one table: (table image, [query images]).
+
+    A 2048 x 2048 base image (seed); the table image is a 1080 x 1920 crop of it; query i is an
+    (h_i, w_i) crop, sides uniform in [lo, hi] (seed + i), of the base warped once by the smooth
+    random flow (seed + 1).  Warping the base once, instead of every crop, keeps generation to a
+    few seconds; every query is still a warped view of the scene the table indexes."""
+    base = image_a(2048, 2048, seed)
+    wb = warp(base, seed + 1)
+    table = crop(base, 1080, 1920, seed)
+    queries = [crop(wb, h, w, seed + i) for i, (h, w) in enumerate(batch_sizes(n, lo, hi, seed))]
+    return table, queries
+
+
+def one_vs_many(n: int = 10, lo: int = 256, hi: int = 2048, seed: int = 3000, qh: int = 768, qw: int = 1024):
+    """One query against a database of n images packed into one atlas.
+
+    Returns (query, atlas, allowed, boxes): the query is a qh x qw crop of a 2048 x 2048 base image
+    (seed); database image i is a crop, sides uniform in [lo, hi] (seed + 1 + i), of the base warped
+    once (seed + 1).  The images are packed on shelves (tallest first) into one atlas; allowed
+    marks with 1 the patches that lie inside one image (seam-straddling and padding patches get 0),
+    and boxes lists each image's (y, x, h, w) in the atlas."""
+    base = image_a(2048, 2048, seed)
+    wb = warp(base, seed + 1)
+    query = crop(base, qh, qw, seed)
+    sizes = batch_sizes(n, lo, hi, seed + 1)
+    db = [crop(wb, h, w, seed + 1 + i) for i, (h, w) in enumerate(sizes)]
+    order = sorted(range(n), key=lambda i: -db[i].shape[0])
+    width = max(4096, max(x.shape[1] for x in db))
+    boxes = [None] * n
+    y = x = shelf = 0
+    for i in order:
+        h, w = db[i].shape[:2]
+        if x + w > width:
+            y, x, shelf = y + shelf, 0, 0
+        boxes[i] = (y, x, h, w)
+        x += w
+        shelf = max(shelf, h)
+    H = y + shelf
+    atlas = np.zeros((H, width, 3), np.float32)
+    allowed = np.zeros((H - 7, width - 7), np.int32)
+    for i, (y0, x0, h, w) in enumerate(boxes):
+        atlas[y0:y0 + h, x0:x0 + w] = db[i]
+        allowed[y0:y0 + h - 7, x0:x0 + w - 7] = 1
+    return query, atlas, allowed, boxes
+
+
 def write_pfm(path: str, img: np.ndarray) -> None:
     """3-channel little-endian PFM, rows stored bottom-up (solver/pfm.cpp:50-64)."""
     img = np.asarray(img, np.float32)
