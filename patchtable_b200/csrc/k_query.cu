@@ -239,14 +239,14 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
         const bool kc_here = !LEARNED || !confident || la.kcoh_confident;
         if (c_q.do_kcoh && kc_here && !repeat && xb < c_q.bew && yb < c_q.beh) {
             /* The reference tries the list in order and stops at the first neighbour whose stored
-               distance reaches triangle * best.  Here three neighbours are scored together with the
+               distance reaches triangle * best.  Here two neighbours are scored together with the
                best known before the group as the early-exit bound, then the sequential decisions
                are replayed: a sum cut short by that looser bound could not have been accepted, and
                one that completes is exact, so the outcome equals the one-by-one loop. */
             const int ks = c_q.ks;
             const int2 *kp = kcoh + ((size_t) (yb / ks) * c_q.bew + (xb / ks)) * c_q.kc;
             const int kdx = ks > 1 ? xb % ks : 0, kdy = ks > 1 ? yb % ks : 0;
-            constexpr int G = 3;
+            constexpr int G = 2;             /* -speed presets list 2 to 20 neighbours; pairs keep registers low */
             bool done = false;
             for (int k = 0; k < c_q.kc && !done; k += G) {
                 int cg[G];
@@ -293,8 +293,11 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
     }
 }
 
+/* At most 12 x 64 threads' worth of CTAs per SM's register file: the compiler keeps the kernel at
+   80 registers (a few bytes of spills), and the extra resident warps hide the gather latency
+   better than the unrestricted 103-register version (measured: choose 0.70 -> 0.64 ms at 1080p). */
 template<int TW, bool LEARNED>
-__global__ void __launch_bounds__(TW)
+__global__ void __launch_bounds__(TW, (12 * 64) / TW)
 k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
               const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
               int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters, const LearnedArgs la) {
@@ -410,7 +413,7 @@ __device__ __forceinline__ int owner(const PtBatchImage *__restrict__ imgs, int 
 
 /* Persistent choose over every row segment of every image: CTA b takes segments b, b + grid, ... */
 template<int TW>
-__global__ void __launch_bounds__(TW)
+__global__ void __launch_bounds__(TW, (12 * 64) / TW)
 k_choose_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, long long nseg, int twi,
                const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
                const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
