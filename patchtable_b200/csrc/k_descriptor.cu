@@ -110,9 +110,9 @@ __device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, c
 
 __global__ void __launch_bounds__(NT)
 k_descriptor(const DescPlan c_plan, const float *__restrict__ rgb, int h, int w, int convert,
-             float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh, int ew) {
+             float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh, int ew, int ty0) {
     extern __shared__ float smem[];
-    desc_tile(c_plan, smem, rgb, h, w, convert, rgba, desc, ds, eh, ew, blockIdx.x * TW, blockIdx.y * TH);
+    desc_tile(c_plan, smem, rgb, h, w, convert, rgba, desc, ds, eh, ew, blockIdx.x * TW, (blockIdx.y + ty0) * TH);
 }
 
 /* Persistent descriptor pass over the 64 x 8 tiles of every image of a batch (images, RGBA
@@ -183,6 +183,11 @@ size_t pt_descriptor_smem(int ndims) {
 
 pt_status pt_launch_descriptor(int ndims, int nchroma, const float *rgb, int h, int w, int convert, float4 *rgba,
                                float *desc, int ds, cudaStream_t st) {
+    return pt_launch_descriptor_rows(ndims, nchroma, rgb, h, w, convert, rgba, desc, ds, 0, (h - 7 + TH - 1) / TH, st);
+}
+
+pt_status pt_launch_descriptor_rows(int ndims, int nchroma, const float *rgb, int h, int w, int convert, float4 *rgba,
+                                    float *desc, int ds, int trow0, int trows, cudaStream_t st) {
     int eh = h - 7, ew = w - 7;
     DescPlan plan;
     PT_TRY(make_plan(ndims, nchroma, plan));
@@ -193,8 +198,11 @@ pt_status pt_launch_descriptor(int ndims, int nchroma, const float *rgb, int h, 
         PT_CUDA(cudaFuncSetAttribute(k_descriptor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
         attr = true;
     }
-    dim3 grid((ew + TW - 1) / TW, (eh + TH - 1) / TH);
-    k_descriptor<<<grid, NT, smem, st>>>(plan, rgb, h, w, convert, rgba, desc, ds, eh, ew);
+    const int ntr = (eh + TH - 1) / TH;
+    if (trow0 < 0 || trows < 1 || trow0 + trows > ntr)
+        return pt_fail(PT_BAD_ARG, "descriptor tile rows [%d, %d) outside 0..%d", trow0, trow0 + trows, ntr);
+    dim3 grid((ew + TW - 1) / TW, trows);
+    k_descriptor<<<grid, NT, smem, st>>>(plan, rgb, h, w, convert, rgba, desc, ds, eh, ew, trow0);
     PT_LAUNCHED();
     return PT_OK;
 }

@@ -38,6 +38,7 @@ struct QPlan {
     int step;                /* neighbour spacing of this pull pass (jump flooding) */
     int pull_max;            /* most neighbour candidates scored per patch */
     int tile;                /* query patches per CTA (single-image launches) */
+    int row0, rows;          /* patch rows of a single-image launch */
     const float4 *b1;        /* b shifted by one pixel: b1[i] = b[i + 1] */
     const int *allowed;      /* b patches that may be matched (allowed[p] == allowed_index), or NULL */
     int allowed_index;
@@ -303,7 +304,7 @@ k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__res
               int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters, const LearnedArgs la) {
     extern __shared__ float4 atile[];
     choose_seg<TW, LEARNED>(c_q, atile, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done, use_done,
-                            counters, la, blockIdx.x * TW, blockIdx.y);
+                            counters, la, blockIdx.x * TW, blockIdx.y + c_q.row0);
 }
 
 /* Step 4 as a pull: the best of the stored match and every neighbour's chosen offset applied to
@@ -396,7 +397,8 @@ k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restr
             const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
             int *nxt_pos, float *nxt_d, unsigned long long *counters) {
     extern __shared__ float4 atile[];
-    pull_seg<TW, R>(c_q, atile, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, counters, blockIdx.x * TW, blockIdx.y);
+    pull_seg<TW, R>(c_q, atile, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, counters, blockIdx.x * TW,
+                    blockIdx.y + c_q.row0);
 }
 
 /* ---- batched queries: many images, one launch per phase over a flattened segment list ---- */
@@ -487,6 +489,10 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     q.step = s.step < 1 ? 1 : s.step;
     q.pull_max = s.pull_max > 0 ? s.pull_max : 1 << 30;
     q.tile = s.tile > 0 ? s.tile : TWD;
+    q.row0 = s.rows > 0 ? s.row0 : 0;
+    q.rows = s.rows > 0 ? s.rows : q.eh;
+    if (s.rows > 0 && (q.row0 < 0 || q.row0 + q.rows > q.eh))
+        return pt_fail(PT_BAD_ARG, "query rows [%d, %d) outside 0..%d", q.row0, q.row0 + q.rows, q.eh);
     if (q.tile != 32 && q.tile != 64 && q.tile != 128 && q.tile != 256)
         return pt_fail(PT_BAD_ARG, "gpu_tile %d: query patches per CTA must be 32, 64, 128 or 256", s.tile);
     q.b1 = s.b1;
@@ -511,7 +517,7 @@ pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const fl
     (void) n;
     LearnedArgs none;
     memset(&none, 0, sizeof(none));
-#define PT_CHOOSE_T(T) { dim3 grid((q.ew + T - 1) / T, q.eh); \
+#define PT_CHOOSE_T(T) { dim3 grid((q.ew + T - 1) / T, q.rows); \
         k_choose_tile<T, false><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, \
                                                                              ch_pos, ch_d, kc_done, use_done, evals, none); }
     switch (q.tile) {
@@ -539,7 +545,7 @@ pt_status pt_launch_choose_learned(const QuerySetup &s, const float4 *a, const f
     la.threshold = threshold;
     la.kcoh_confident = kcoh_confident;
     la.counters = lcounters;
-#define PT_CHOOSE_L(T) { dim3 grid((q.ew + T - 1) / T, q.eh); \
+#define PT_CHOOSE_L(T) { dim3 grid((q.ew + T - 1) / T, q.rows); \
         k_choose_tile<T, true><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, \
                                                                             ch_pos, ch_d, kc_done, use_done, evals, la); }
     switch (q.tile) {
@@ -559,7 +565,7 @@ pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const floa
     QPlan q;
     PT_TRY(make_qplan(s, q));
     (void) n;
-#define PT_PULL_T(T, RR) { dim3 grid((q.ew + T - 1) / T, q.eh); \
+#define PT_PULL_T(T, RR) { dim3 grid((q.ew + T - 1) / T, q.rows); \
         k_pull_tile<T, RR><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, \
                                                                          evals); }
     const bool r1 = q.radius <= 1;

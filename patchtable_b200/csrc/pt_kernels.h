@@ -11,6 +11,9 @@ pt_status pt_descriptor_check(int ndims, int nchroma);
 /* desc may be NULL (only the RGBA copy is written); rgba may be NULL. */
 pt_status pt_launch_descriptor(int ndims, int nchroma, const float *rgb, int h, int w, int convert, float4 *rgba,
                                float *desc, int ds, cudaStream_t st);
+/* Rows [trow0, trow0 + trows) of 8-patch descriptor tiles only (for banded lookups). */
+pt_status pt_launch_descriptor_rows(int ndims, int nchroma, const float *rgb, int h, int w, int convert, float4 *rgba,
+                                    float *desc, int ds, int trow0, int trows, cudaStream_t st);
 
 /* k_build.cu */
 pt_status pt_launch_fill(int *p, long long n, int v, cudaStream_t st);
@@ -52,6 +55,7 @@ struct QuerySetup {
     int step = 1;            /* neighbour spacing of a pull pass */
     int pull_max = 0;        /* most neighbour candidates a pull scores per patch (0 = all) */
     int tile = 0;            /* query patches per CTA in choose / pull: 32, 64, 128, 256 (0 = 32) */
+    int row0 = 0, rows = 0;  /* patch rows [row0, row0 + rows) of a single-image launch (rows 0 = all) */
     const float4 *b1 = nullptr;   /* the table image shifted by one pixel, b1[i] = b[i + 1] */
     const int *allowed = nullptr; /* b patches a match may use (allowed[p] == allowed_index), or NULL */
     int allowed_index = 0;

@@ -110,9 +110,17 @@ struct pt_table {
     DevBuf<float> q_lconf;
     DevBuf<unsigned long long> q_counters;
     std::vector<cudaEvent_t> events;
+    cudaStream_t st_in = nullptr, st_out = nullptr;    /* banded host lookups: upload / download */
+    cudaStream_t st_choose = nullptr, st_pull = nullptr; /* banded host lookups: later phases */
+    std::vector<cudaEvent_t> band_ev;
 
     ~pt_table() {
         for (auto e : events) cudaEventDestroy(e);
+        for (auto e : band_ev) cudaEventDestroy(e);
+        if (st_in) cudaStreamDestroy(st_in);
+        if (st_out) cudaStreamDestroy(st_out);
+        if (st_choose) cudaStreamDestroy(st_choose);
+        if (st_pull) cudaStreamDestroy(st_pull);
         if (own_stream && st) cudaStreamDestroy(st);
     }
 };
@@ -510,6 +518,103 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     return PT_OK;
 }
 
+/* The host lookup of a one-pass schedule, pipelined over bands of patch rows.  A band needs only
+   its own pixel rows plus 7; its choose also reads the next band's RGBA rows (written by that
+   band's descriptor launch) and its pull the next band's choices.  Four streams carry the phases:
+   upload of band b -> descriptor, table entries and initial state of band b -> choose of band
+   b-1 -> pull and output of band b-2 -> download of band b-2, each waiting on the events its
+   inputs come from.  Consecutive bands' kernels overlap (filling each other's last waves) and the
+   copies overlap the kernels.  Concurrent kernels always touch disjoint rows (bands are at least
+   32 rows; a pull reads at most 16 rows beyond its band).  Every kernel computes exactly what the
+   whole-image launch computes for its rows, so the result is identical. */
+pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_out) {
+    const pt_params &p = t->p;
+    const int eh = h - 7, ew = w - 7;
+    const long long P = (long long) eh * ew;
+    PT_TRY(ensure_query_buffers(t, h, w));
+    PT_CUDA(t->q_ann.reserve((size_t) P * 3));
+    for (cudaStream_t *sp : {&t->st_in, &t->st_out, &t->st_choose, &t->st_pull})
+        if (!*sp) PT_CUDA(cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking));
+    int B = ((eh + 7) / 8 + 7) / 8 * 8;        /* about 8 bands, each a multiple of 8 rows */
+    if (B < 32) B = 32;
+    const int nb = (eh + B - 1) / B;
+    while ((int) t->band_ev.size() < 4 * nb + 1) {
+        cudaEvent_t e;
+        PT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        t->band_ev.push_back(e);
+    }
+    cudaEvent_t *ev_in = t->band_ev.data(), *ev_a = ev_in + nb, *ev_b = ev_a + nb, *ev_c = ev_b + nb;
+    cudaEvent_t ev_start = t->band_ev[4 * nb];
+    cudaStream_t sa = t->st, sb = t->st_choose, sc = t->st_pull;
+    /* the phases start after whatever the table's stream has queued */
+    PT_CUDA(cudaEventRecord(ev_start, sa));
+    for (cudaStream_t s2 : {t->st_in, sb, sc, t->st_out}) PT_CUDA(cudaStreamWaitEvent(s2, ev_start, 0));
+    QuerySetup qs;
+    qs.aw = w; qs.ah = h; qs.bw = t->w; qs.bh = t->h;
+    qs.prop_scale = 1.0 / (1 + p.coherence_spatial);
+    qs.triangle_factor = p.triangle_factor;
+    qs.kcoherence = (p.kcoherence_iter < 0 || p.kcoherence_iter == 0) ? p.kcoherence : 0;
+    qs.kcoherence_step = p.kcoherence_step;
+    qs.radius = std::min(2, p.query_step + p.prop_dist);
+    qs.b1 = t->b_rgba1.p;
+    qs.pull_max = p.gpu_pull_max;
+    qs.tile = p.gpu_tile;
+    qs.allowed = t->allowed.p;
+    qs.allowed_index = p.allowed_index;
+    QuerySetup qp = qs;
+    qp.step = pt_pass_step(0, 1, pt_default_jump(p, 1));
+    const int init_pos = pt_xy(t->ew + 1, 0);
+    for (int b = 0; b <= nb + 1; b++) {
+        if (b < nb) {
+            const int r0 = b * B, r1 = std::min(eh, r0 + B);
+            const int p0 = b == 0 ? 0 : r0 + 7, p1 = b == nb - 1 ? h : r1 + 7;
+            const size_t px0 = (size_t) p0 * w * 3, npx = (size_t) (p1 - p0) * w * 3;
+            PT_CUDA(cudaMemcpyAsync(t->q_rgb.p + px0, a + px0, sizeof(float) * npx, cudaMemcpyHostToDevice, t->st_in));
+            PT_CUDA(cudaEventRecord(ev_in[b], t->st_in));
+            PT_CUDA(cudaStreamWaitEvent(sa, ev_in[b], 0));
+            PT_TRY(pt_launch_descriptor_rows(p.ndims, p.nchroma, t->q_rgb.p, h, w, p.convert_colorspace, t->q_rgba.p,
+                                             t->q_desc.p, t->ds, r0 / 8, (r1 - r0 + 7) / 8, sa));
+            const size_t o = (size_t) r0 * ew;
+            const long long n = (long long) (r1 - r0) * ew;
+            PT_TRY(pt_launch_table_candidates(t->bins, t->q_desc.p + o * t->ds, t->ds, n, t->to_bin.p, t->table.p,
+                                              t->q_tcand.p + o, sa));
+            PT_TRY(pt_launch_init((int) n, init_pos, (float) PT_DIST_INF, t->q_pos[0].p + o, t->q_d[0].p + o, sa));
+            PT_CUDA(cudaEventRecord(ev_a[b], sa));
+        }
+        if (b >= 1 && b - 1 < nb) {
+            const int r0 = (b - 1) * B, r1 = std::min(eh, r0 + B);
+            PT_CUDA(cudaStreamWaitEvent(sb, ev_a[b < nb ? b : nb - 1], 0));
+            QuerySetup qc = qs;
+            qc.row0 = r0;
+            qc.rows = r1 - r0;
+            qc.stream = sb;
+            PT_TRY(pt_launch_choose(qc, (int) P, t->q_rgba.p, t->b_rgba.p, t->q_pos[0].p, t->q_d[0].p, t->q_tcand.p,
+                                    t->kcoh.p, p.do_table_lookup, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, 0, nullptr, sb));
+            PT_CUDA(cudaEventRecord(ev_b[b - 1], sb));
+        }
+        if (b >= 2) {
+            const int r0 = (b - 2) * B, r1 = std::min(eh, r0 + B);
+            PT_CUDA(cudaStreamWaitEvent(sc, ev_b[b - 1 < nb ? b - 1 : nb - 1], 0));
+            QuerySetup qb = qp;
+            qb.row0 = r0;
+            qb.rows = r1 - r0;
+            qb.stream = sc;
+            PT_TRY(pt_launch_pull(qb, (int) P, t->q_rgba.p, t->b_rgba.p, t->q_pos[0].p, t->q_d[0].p, t->q_chpos.p,
+                                  t->q_chd.p, t->q_pos[1].p, t->q_d[1].p, nullptr, sc));
+            const size_t o = (size_t) r0 * ew;
+            const int n = (r1 - r0) * ew;
+            PT_TRY(pt_launch_output(n, t->q_pos[1].p + o, t->q_d[1].p + o, t->q_ann.p + 3 * o, sc));
+            PT_CUDA(cudaEventRecord(ev_c[b - 2], sc));
+            PT_CUDA(cudaStreamWaitEvent(t->st_out, ev_c[b - 2], 0));
+            PT_CUDA(cudaMemcpyAsync(ann_out + 3 * o, t->q_ann.p + 3 * o, sizeof(double) * 3 * (size_t) n,
+                                    cudaMemcpyDeviceToHost, t->st_out));
+        }
+    }
+    PT_CUDA(cudaStreamSynchronize(t->st_out));
+    for (cudaStream_t s2 : {sa, sb, sc}) PT_CUDA(cudaStreamSynchronize(s2));
+    return PT_OK;
+}
+
 /* lookup_device with stage events; stage_ms[nst] receives summed stage times, counters[nctr] the
    SSD work counters. */
 pt_status profile_impl(pt_table *t, pt_proposal *net, const float *d_a, int h, int w, double *d_ann, cudaStream_t st,
@@ -559,6 +664,11 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int h, int w, double *ann
     if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
     if (ann_prev || coh_sv) return pt_fail(PT_UNSUPPORTED, "ann_prev / coherence_temporal_sv are not implemented yet");
     long long P = (long long) (h - 7) * (w - 7);
+    if (pt_default_passes(t->p) == 1 && t->p.do_prop && h - 7 >= 64) {
+        PT_TRY(lookup_banded(t, a, h, w, ann_out));
+        if (seconds) *seconds = now_s() - T0;
+        return PT_OK;
+    }
     PT_TRY(ensure_query_buffers(t, h, w));
     PT_CUDA(t->q_ann.reserve((size_t) P * 3));
     PT_CUDA(cudaMemcpyAsync(t->q_rgb.p, a, sizeof(float) * (size_t) h * w * 3, cudaMemcpyHostToDevice, t->st));
