@@ -99,11 +99,20 @@ pt_status pt_table_create(const pt_params *p, const float *b, int h, int w, int 
 pt_status pt_table_create_with_descriptor(const pt_params *p, const float *b, int h, int w,
                                           const float *wh0, const int32_t *allowed, pt_table **out);
 
-/* PatchTableFixedN(PatchTableParams *, string filename) / load(), patchtable.h:1574-1622. */
+/* PatchTableFixedN(PatchTableParams *, string filename) / load(), patchtable.h:1574-1622: reads
+   the reference's table file (PT_IO if it is not one, PT_BAD_ARG if its descriptor dimensions
+   differ from p->ndims).  The file holds no k-coherence set; it is rebuilt from the stored
+   descriptors when p->kcoherence > 0.  pt_table_create also loads when p->load_filename is set
+   and saves after building when p->save_filename is set, as the reference's constructor does. */
 pt_status pt_table_load(const pt_params *p, const char *filename, pt_table **out);
 
-/* PatchTable<>::save(string), patchtable.h:4470-4490 / PatchTableFixedN::save, :1574-1605. */
+/* PatchTable<>::save(string), patchtable.h:4470-4490 / PatchTableFixedN::save, :1574-1605, in
+   the reference's format (the reference loads it).  The padding rows and columns of wh0, which
+   this library does not keep, are written as 0. */
 pt_status pt_table_save(const pt_table *t, const char *filename);
+
+/* Image size (b0) of a table, e.g. one loaded from a file. */
+pt_status pt_table_image_shape(const pt_table *t, int *h, int *w);
 
 void pt_table_free(pt_table *t);
 

@@ -96,6 +96,9 @@ def lib() -> C.CDLL:
     L.pt_table_create.argtypes = [P, _f32p, C.c_int, C.c_int, C.c_int, vp, C.POINTER(vp)]
     L.pt_table_create_with_descriptor.argtypes = [P, _f32p, C.c_int, C.c_int, _f32p, vp, C.POINTER(vp)]
     L.pt_table_free.argtypes = [vp]
+    L.pt_table_save.argtypes = [vp, C.c_char_p]
+    L.pt_table_load.argtypes = [P, C.c_char_p, C.POINTER(vp)]
+    L.pt_table_image_shape.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.pt_table_free.restype = None
     L.pt_table_set_params.argtypes = [vp, P]
     L.pt_table_lookup.argtypes = [vp, _f32p, C.c_int, C.c_int, _f64p, vp, vp, C.POINTER(C.c_double)]
@@ -226,6 +229,28 @@ class PatchTable:
             _check(lib().pt_table_create_with_descriptor(C.byref(params._p), b, b.shape[0], b.shape[1], wh0, al, C.byref(h)))
         self._h = h
         self.last_seconds = 0.0
+        self._set_shape()
+
+    def _set_shape(self):
+        hh, ww = C.c_int(), C.c_int()
+        _check(lib().pt_table_image_shape(self._h, C.byref(hh), C.byref(ww)))
+        self.shape_b = (hh.value, ww.value, 3)
+
+    def save(self, filename: str) -> None:
+        """PatchTable<>::save (patchtable.h:4470-4490), in the reference's file format."""
+        _check(lib().pt_table_save(self._h, str(filename).encode()))
+
+    @classmethod
+    def load(cls, params: PatchTableParams, filename: str) -> "PatchTable":
+        """PatchTableFixedN(p, filename): a table read from a file in the reference's format."""
+        obj = cls.__new__(cls)
+        obj.params = params
+        h = C.c_void_p()
+        _check(lib().pt_table_load(C.byref(params._p), str(filename).encode(), C.byref(h)))
+        obj._h = h
+        obj.last_seconds = 0.0
+        obj._set_shape()
+        return obj
 
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:

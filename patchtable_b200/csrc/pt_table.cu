@@ -152,6 +152,8 @@ pt_status check_params(const pt_params *p, int h, int w) {
     return PT_OK;
 }
 
+pt_status upload_partition(pt_table *t);
+
 pt_status build_partition(pt_table *t) {
     const int G = t->G;
     t->part.assign(G, PtPartition());
@@ -210,6 +212,13 @@ pt_status build_partition(pt_table *t) {
             P.to_bin[i] = (coord < mid) ? prev_c : next_c;
         }
     }
+    return upload_partition(t);
+}
+
+/* Device copies of the partition: the to_bin tables, the centres / sizes the proposal features
+   read, and the per-dimension get_bin parameters. */
+pt_status upload_partition(pt_table *t) {
+    const int G = t->G;
     std::vector<int> flat((size_t) G * PT_NMAP);
     for (int d = 0; d < G; d++) std::copy(t->part[d].to_bin.begin(), t->part[d].to_bin.end(), flat.begin() + (size_t) d * PT_NMAP);
     PT_CUDA(t->to_bin.reserve(flat.size()));
@@ -642,11 +651,220 @@ pt_status profile_impl(pt_table *t, pt_proposal *net, const float *d_a, int h, i
 
 }  // namespace
 
+namespace {
+
+/* ---- table files in the reference's format ----
+   PatchTableFixedN::save / load (patchtable.h:1574-1593) over the serialisation primitives of
+   patchtable.cpp:499-573: a string is its int32 length and its bytes, a vector its int32 length
+   and its elements, an Array its sizes (a vector<int>) and its elements, all little-endian.  A
+   file holds "PatchTable", the table (sizes = nslices), b0 (h, w, 3), wh0 (h+7, w+7, ndims),
+   nslices, the partition ("PatchPartition", count, then per dimension "PatchPartition1D", to_bin,
+   centers, lsizes, rsizes, min_val, max_val, range, nslices, "EndPatchPartition1D"),
+   "EndPatchPartition" and "EndPatchTable". */
+struct FileOut {
+    FILE *f;
+    bool ok = true;
+    void raw(const void *p, size_t n) { if (ok && n && fwrite(p, 1, n, f) != n) ok = false; }
+    void i32(int v) { raw(&v, 4); }
+    void f32(float v) { raw(&v, 4); }
+    void str(const char *s) { int n = (int) strlen(s); i32(n); raw(s, n); }
+    template<class T> void vec(const std::vector<T> &v) { i32((int) v.size()); raw(v.data(), sizeof(T) * v.size()); }
+};
+
+struct FileIn {
+    FILE *f;
+    bool ok = true;
+    void raw(void *p, size_t n) { if (ok && n && fread(p, 1, n, f) != n) ok = false; }
+    int i32() { int v = 0; raw(&v, 4); return v; }
+    float f32() { float v = 0; raw(&v, 4); return v; }
+    bool id(const char *s) {
+        int n = i32();
+        if (!ok || n != (int) strlen(s)) { ok = false; return false; }
+        std::string got(n, 0);
+        raw(&got[0], n);
+        ok = ok && got == s;
+        return ok;
+    }
+    /* a vector of at most `cap` elements */
+    template<class T> bool vec(std::vector<T> &v, long long cap) {
+        int n = i32();
+        if (!ok || n < 0 || n > cap) { ok = false; return false; }
+        v.resize(n);
+        raw(v.data(), sizeof(T) * (size_t) n);
+        return ok;
+    }
+};
+
+pt_status save_impl(const pt_table *t, const char *filename) {
+    const int h = t->h, w = t->w, nd = t->nd;
+    std::vector<int> cells((size_t) t->ncells);
+    std::vector<float4> rgba((size_t) h * w);
+    std::vector<float> desc((size_t) t->eh * t->ew * t->ds);
+    PT_CUDA(cudaMemcpyAsync(cells.data(), t->table.p, sizeof(int) * cells.size(), cudaMemcpyDeviceToHost, t->st));
+    PT_CUDA(cudaMemcpyAsync(rgba.data(), t->b_rgba.p, sizeof(float4) * rgba.size(), cudaMemcpyDeviceToHost, t->st));
+    PT_CUDA(cudaMemcpyAsync(desc.data(), t->b_desc.p, sizeof(float) * desc.size(), cudaMemcpyDeviceToHost, t->st));
+    PT_CUDA(cudaStreamSynchronize(t->st));
+    std::vector<float> b0((size_t) h * w * 3);
+    for (size_t i = 0; i < rgba.size(); i++) { b0[3 * i] = rgba[i].x; b0[3 * i + 1] = rgba[i].y; b0[3 * i + 2] = rgba[i].z; }
+    /* wh0 holds the descriptor of the patch with top-left (x, y) at (y + 7, x + 7); the partial
+       windows of the reference's "full" padding are not kept by this library and are written as 0 */
+    std::vector<float> wh0((size_t) (h + 7) * (w + 7) * nd, 0.f);
+    for (int y = 0; y < t->eh; y++)
+        for (int x = 0; x < t->ew; x++)
+            for (int d = 0; d < nd; d++)
+                wh0[((size_t) (y + 7) * (w + 7) + (x + 7)) * nd + d] = desc[((size_t) y * t->ew + x) * t->ds + d];
+    FILE *f = fopen(filename, "wb");
+    if (!f) return pt_fail(PT_IO, "cannot open %s for writing", filename);
+    FileOut o{f};
+    o.str("PatchTable");
+    o.vec(t->nslices);
+    o.raw(cells.data(), sizeof(int) * cells.size());
+    o.vec(std::vector<int>{h, w, 3});
+    o.raw(b0.data(), sizeof(float) * b0.size());
+    o.vec(std::vector<int>{h + 7, w + 7, nd});
+    o.raw(wh0.data(), sizeof(float) * wh0.size());
+    o.vec(t->nslices);
+    o.str("PatchPartition");
+    o.i32(t->G);
+    for (int d = 0; d < t->G; d++) {
+        const PtPartition &P = t->part[d];
+        o.str("PatchPartition1D");
+        o.vec(P.to_bin);
+        o.vec(P.centers);
+        o.vec(P.lsizes);
+        o.vec(P.rsizes);
+        o.f32(P.min_val);
+        o.f32(P.max_val);
+        o.f32(P.range);
+        o.i32(P.nslices);
+        o.str("EndPatchPartition1D");
+    }
+    o.str("EndPatchPartition");
+    o.str("EndPatchTable");
+    const bool ok = o.ok;
+    if (fclose(f) != 0 || !ok) return pt_fail(PT_IO, "writing %s failed", filename);
+    return PT_OK;
+}
+
+pt_status load_impl(const pt_params *pin, const char *filename, pt_table **out) {
+    *out = nullptr;
+    FILE *f = fopen(filename, "rb");
+    if (!f) return pt_fail(PT_IO, "cannot open %s", filename);
+    struct Closer { FILE *f; ~Closer() { fclose(f); } } closer{f};
+    FileIn in{f};
+    std::vector<int> tsizes, bsizes, wsizes, nslices;
+    std::vector<int> cells;
+    if (!in.id("PatchTable") || !in.vec(tsizes, PT_DESC_MAX)) return pt_fail(PT_IO, "%s: not a PatchTable file", filename);
+    long long ncells = 1;
+    for (int v : tsizes) {
+        if (v < 1) return pt_fail(PT_IO, "%s: bad table size", filename);
+        ncells *= v;
+        if (ncells >= (1ll << 31)) return pt_fail(PT_IO, "%s: table exceeds 2^31 cells", filename);
+    }
+    cells.resize((size_t) ncells);
+    in.raw(cells.data(), sizeof(int) * cells.size());
+    if (!in.vec(bsizes, 3) || bsizes.size() != 3 || bsizes[2] != 3) return pt_fail(PT_IO, "%s: bad b0 array", filename);
+    const int h = bsizes[0], w = bsizes[1];
+    PT_TRY(check_params(pin, h, w));
+    std::vector<float> b0((size_t) h * w * 3);
+    in.raw(b0.data(), sizeof(float) * b0.size());
+    if (!in.vec(wsizes, 3) || wsizes.size() != 3 || wsizes[0] != h + 7 || wsizes[1] != w + 7)
+        return pt_fail(PT_IO, "%s: bad wh0 array", filename);
+    const int nd = wsizes[2];
+    if (nd != pin->ndims) return pt_fail(PT_BAD_ARG, "%s holds %d descriptor dimensions; the parameters ask for %d", filename, nd, pin->ndims);
+    std::vector<float> wh0((size_t) (h + 7) * (w + 7) * nd);
+    in.raw(wh0.data(), sizeof(float) * wh0.size());
+    if (!in.vec(nslices, PT_DESC_MAX) || nslices != tsizes) return pt_fail(PT_IO, "%s: nslices do not match the table", filename);
+    const int G = (int) nslices.size();
+    if (G < 1 || G > nd) return pt_fail(PT_IO, "%s: %d grid dimensions for %d descriptor dimensions", filename, G, nd);
+    if (!in.id("PatchPartition") || in.i32() != G) return pt_fail(PT_IO, "%s: bad partition", filename);
+    std::unique_ptr<pt_table> t(new pt_table());
+    t->part.assign(G, PtPartition());
+    for (int d = 0; d < G; d++) {
+        PtPartition &P = t->part[d];
+        if (!in.id("PatchPartition1D") || !in.vec(P.to_bin, PT_NMAP) || (int) P.to_bin.size() != PT_NMAP ||
+            !in.vec(P.centers, nslices[d]) || !in.vec(P.lsizes, nslices[d]) || !in.vec(P.rsizes, nslices[d]))
+            return pt_fail(PT_IO, "%s: bad partition of dimension %d", filename, d);
+        P.min_val = in.f32();
+        P.max_val = in.f32();
+        P.range = in.f32();
+        P.nslices = in.i32();
+        if (!in.id("EndPatchPartition1D") || P.nslices != nslices[d] || (int) P.centers.size() != nslices[d] ||
+            (int) P.lsizes.size() != nslices[d] || (int) P.rsizes.size() != nslices[d])
+            return pt_fail(PT_IO, "%s: bad partition of dimension %d", filename, d);
+        for (int v : P.to_bin)
+            if (v < 0 || v >= nslices[d]) return pt_fail(PT_IO, "%s: to_bin entry out of range", filename);
+    }
+    if (!in.id("EndPatchPartition") || !in.id("EndPatchTable")) return pt_fail(PT_IO, "%s: truncated file", filename);
+    for (int v : cells)
+        if (pt_x(v) < 7 || pt_y(v) < 7 || pt_x(v) >= w || pt_y(v) >= h)
+            return pt_fail(PT_IO, "%s: table entry outside the image", filename);
+
+    t->p = *pin;
+    pt_params &p = t->p;
+    p.grid_ndims = G;
+    t->h = h; t->w = w; t->eh = h - 7; t->ew = w - 7;
+    t->nd = nd; t->G = G;
+    t->ds = nd <= 8 ? 8 : 16;
+    PT_TRY(pt_descriptor_check(p.ndims, p.nchroma));
+    PT_CUDA(cudaStreamCreateWithFlags(&t->st, cudaStreamNonBlocking));
+    t->own_stream = true;
+    const long long P = (long long) t->eh * t->ew;
+    {
+        DevBuf<float> rgb;
+        PT_CUDA(rgb.reserve(b0.size()));
+        PT_CUDA(cudaMemcpyAsync(rgb.p, b0.data(), sizeof(float) * b0.size(), cudaMemcpyHostToDevice, t->st));
+        PT_CUDA(t->b_rgba.reserve((size_t) h * w));
+        PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, rgb.p, h, w, p.convert_colorspace, t->b_rgba.p, nullptr, t->ds, t->st));
+        std::vector<float> packed((size_t) P * t->ds, 0.0f);
+        for (int y = 0; y < t->eh; y++)
+            for (int x = 0; x < t->ew; x++)
+                for (int d = 0; d < nd; d++)
+                    packed[((size_t) y * t->ew + x) * t->ds + d] = wh0[((size_t) (y + 7) * (w + 7) + (x + 7)) * nd + d];
+        PT_CUDA(t->b_desc.reserve(packed.size()));
+        PT_CUDA(cudaMemcpyAsync(t->b_desc.p, packed.data(), sizeof(float) * packed.size(), cudaMemcpyHostToDevice, t->st));
+        const size_t npx = (size_t) h * w;
+        PT_CUDA(t->b_rgba1.reserve(npx));
+        PT_CUDA(cudaMemsetAsync(t->b_rgba1.p, 0, sizeof(float4) * npx, t->st));
+        PT_CUDA(cudaMemcpyAsync(t->b_rgba1.p, t->b_rgba.p + 1, sizeof(float4) * (npx - 1), cudaMemcpyDeviceToDevice, t->st));
+        PT_CUDA(cudaStreamSynchronize(t->st));
+    }
+    /* the file has no k-coherence set (the reference's load leaves it empty); it is rebuilt from
+       the stored descriptors */
+    if (p.kcoherence > 0) PT_TRY(build_kcoherence(t.get(), std::vector<int>()));
+    t->nslices = nslices;
+    t->stride.assign(G, 1);
+    t->ncells = 1;
+    for (int d = G - 1; d >= 0; d--) { t->stride[d] = t->ncells; t->ncells *= nslices[d]; }
+    t->min_val.resize(G); t->max_val.resize(G); t->range.resize(G);
+    for (int d = 0; d < G; d++) {
+        t->min_val[d] = t->part[d].min_val;
+        t->max_val[d] = t->part[d].max_val;
+        t->range[d] = t->part[d].range;
+    }
+    PT_TRY(upload_partition(t.get()));
+    PT_CUDA(t->table.reserve(t->ncells));
+    PT_CUDA(cudaMemcpyAsync(t->table.p, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice, t->st));
+    PT_CUDA(cudaStreamSynchronize(t->st));
+    t->add_count = 0;
+    t->dt_levels = 0;
+    *out = t.release();
+    return PT_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 pt_status pt_table_create(const pt_params *p, const float *b, int h, int w, int channels, const int32_t *allowed,
                           pt_table **out) {
-    return create_impl(p, b, h, w, channels, nullptr, allowed, out);
+    if (p && p->load_filename[0]) return load_impl(p, p->load_filename, out);      /* patchtable.h:2591-2594 */
+    PT_TRY(create_impl(p, b, h, w, channels, nullptr, allowed, out));
+    if (p->save_filename[0]) {                                                   /* patchtable.h:3326-3328 */
+        pt_status s = save_impl(*out, p->save_filename);
+        if (s != PT_OK) { pt_table_free(*out); *out = nullptr; return s; }
+    }
+    return PT_OK;
 }
 
 pt_status pt_table_create_with_descriptor(const pt_params *p, const float *b, int h, int w, const float *wh0,
@@ -850,13 +1068,20 @@ pt_status pt_descriptor(const pt_params *p, const float *rgb, int h, int w, floa
 }
 
 pt_status pt_table_save(const pt_table *t, const char *filename) {
-    (void) t; (void) filename;
-    return pt_fail(PT_UNSUPPORTED, "save is not implemented yet");
+    if (!t || !filename) return pt_fail(PT_BAD_ARG, "null argument");
+    return save_impl(t, filename);
 }
 
 pt_status pt_table_load(const pt_params *p, const char *filename, pt_table **out) {
-    (void) p; (void) filename; (void) out;
-    return pt_fail(PT_UNSUPPORTED, "load is not implemented yet");
+    if (!p || !filename || !out) return pt_fail(PT_BAD_ARG, "null argument");
+    return load_impl(p, filename, out);
+}
+
+pt_status pt_table_image_shape(const pt_table *t, int *h, int *w) {
+    if (!t) return pt_fail(PT_BAD_ARG, "null table");
+    if (h) *h = t->h;
+    if (w) *w = t->w;
+    return PT_OK;
 }
 
 int64_t pt_kernel_launch_count(void) { return g_launches; }
