@@ -139,6 +139,14 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int h, int w, double *ann
 pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int h, int w, double *d_ann,
                                  void *stream);
 
+/* Device form of pt_table_lookup with the previous frame's NNF (patchtable.h:3548-3585,
+   4178-4193): d_ann_prev ((h-7) x (w-7) x 3 doubles) seeds the field; d_coh_sv ((h-7) x (w-7)
+   floats, may be NULL) replaces the temporal scale 1/(1+coherence_temporal) per patch when the
+   distance is recomputed (recalc_dist_temporal).  Previous matches outside the table image are
+   clamped (the host form reports them with PT_BAD_ARG when sanitize_input is 0). */
+pt_status pt_table_lookup_device_temporal(pt_table *t, const float *d_a, int h, int w, const double *d_ann_prev,
+                                         const float *d_coh_sv, double *d_ann, void *stream);
+
 /* Zero-allocation form of pt_table_lookup_device (no counterpart in the reference).  For
    callers that may not allocate device memory during queries -- a frame loop with a fixed
    latency budget (cudaMalloc/cudaFree synchronise the device), or an application whose own

@@ -277,8 +277,17 @@ class PatchTable:
             ann = np.empty(shape, np.float64)
         secs = C.c_double()
         self._sync_params()
-        prev = None if ann_prev is None else np.ascontiguousarray(ann_prev, np.float64).ctypes.data_as(C.c_void_p)
-        sv = None if coherence_temporal_sv is None else np.ascontiguousarray(coherence_temporal_sv, np.float32).ctypes.data_as(C.c_void_p)
+        prev_arr = sv_arr = None
+        if ann_prev is not None:
+            prev_arr = np.ascontiguousarray(ann_prev, np.float64)
+            if prev_arr.shape != shape:
+                raise PatchTableError(1, "ann_prev must have shape %s" % (shape,))
+        if coherence_temporal_sv is not None:
+            sv_arr = np.ascontiguousarray(coherence_temporal_sv, np.float32)
+            if sv_arr.shape != shape[:2]:
+                raise PatchTableError(1, "coherence_temporal_sv must have shape %s" % (shape[:2],))
+        prev = None if prev_arr is None else prev_arr.ctypes.data_as(C.c_void_p)
+        sv = None if sv_arr is None else sv_arr.ctypes.data_as(C.c_void_p)
         _check(lib().pt_table_lookup(self._h, a, a.shape[0], a.shape[1], ann, prev, sv, C.byref(secs)))
         self.last_seconds = secs.value
         return ann

@@ -460,6 +460,64 @@ k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, lon
     }
 }
 
+/* patch_dist_exact of a patch of a (RGBA rows in global memory) and a patch of b, in the
+   reference's lane order, without an early exit. */
+__device__ __forceinline__ float ssd_global(const QPlan &q, const float4 *__restrict__ a, int ax, int ay,
+                                           const float4 *__restrict__ B, int bx, int by) {
+    float l[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 1
+    for (int dy = 0; dy < 8; dy++) {
+        float4 av[8], bv[8];
+        load_brow(q, B, bx, by + dy, bv);
+#pragma unroll
+        for (int p = 0; p < 8; p++) av[p] = __ldg(a + (size_t) (ay + dy) * q.aw + ax + p);
+        row_lanes(av, bv, l);
+    }
+    return lane_total(l);
+}
+
+/* Initial field from the previous frame's NNF (patchtable.h:3548-3585): its matches (clamped to
+   the table image when sanitize is set) with either their distance recomputed and scaled by
+   scale_sv[p] (when given) or temporal_scale, or the previous distance times temporal_scale.
+   orig[p] keeps what the end of the lookup restores for a patch that kept this match and this
+   distance (patchtable.h:4178-4193): the scaled distance divided by temporal_scale. */
+__global__ void k_init_temporal(const QPlan q, const double *__restrict__ prev, const float *__restrict__ scale_sv,
+                                int recalc, int sanitize, double temporal_scale, const float4 *__restrict__ a,
+                                const float4 *__restrict__ B, int *cur_pos, float *cur_d, double *orig, int *bad) {
+    const int p = blockIdx.x * NT + threadIdx.x;
+    if (p >= q.ew * q.eh) return;
+    const int x = p % q.ew, y = p / q.ew;
+    int xs = (int) prev[3 * (size_t) p], ys = (int) prev[3 * (size_t) p + 1];
+    if (xs < 0 || ys < 0 || xs >= q.bew || ys >= q.beh) {
+        if (!sanitize) atomicExch(bad, 1);
+        xs = min(max(xs, 0), q.bew - 1);
+        ys = min(max(ys, 0), q.beh - 1);
+    }
+    double scaled;
+    if (recalc) {
+        const float dcur = ssd_global(q, a, x, y, B, xs, ys);
+        scaled = (double) dcur * (scale_sv ? (double) scale_sv[p] : temporal_scale);
+    } else {
+        scaled = prev[3 * (size_t) p + 2] * temporal_scale;
+    }
+    cur_pos[p] = pt_xy(xs, ys);
+    cur_d[p] = (float) scaled;
+    orig[p] = scaled / temporal_scale;
+}
+
+/* The float64 NNF; a patch whose match and distance are still the initial temporal ones gets the
+   unscaled distance back (patchtable.h:4178-4193). */
+__global__ void k_output_temporal(int n, const int *__restrict__ pos, const float *__restrict__ d,
+                                  const int *__restrict__ pos0, const float *__restrict__ d0,
+                                  const double *__restrict__ orig, double *ann) {
+    const int p = blockIdx.x * NT + threadIdx.x;
+    if (p >= n) return;
+    const int v = pos[p];
+    ann[3 * (size_t) p + 0] = pt_x(v);
+    ann[3 * (size_t) p + 1] = pt_y(v);
+    ann[3 * (size_t) p + 2] = (v == pos0[p] && d[p] == d0[p]) ? orig[p] : (double) d[p];
+}
+
 __global__ void k_init(int n, int pos, float d, int *cur_pos, float *cur_d) {
     int p = blockIdx.x * NT + threadIdx.x;
     if (p < n) { cur_pos[p] = pos; cur_d[p] = d; }
@@ -649,6 +707,25 @@ pt_status pt_launch_pull_batch(const QuerySetup &s, const PtBatchImage *imgs, in
         default: if (r1) PT_PULL_B(256, 1) else PT_PULL_B(256, 2) break;
     }
 #undef PT_PULL_B
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_init_temporal(const QuerySetup &s, const double *prev, const float *scale_sv, int recalc, int sanitize,
+                                  double temporal_scale, const float4 *a, const float4 *b, int *cur_pos, float *cur_d,
+                                  double *orig, int *bad, cudaStream_t st) {
+    QPlan q;
+    PT_TRY(make_qplan(s, q));
+    const int n = q.ew * q.eh;
+    k_init_temporal<<<(n + NT - 1) / NT, NT, 0, st>>>(q, prev, scale_sv, recalc, sanitize, temporal_scale, a, b, cur_pos, cur_d,
+                                                     orig, bad);
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_output_temporal(int n, const int *pos, const float *d, const int *pos0, const float *d0,
+                                    const double *orig, double *ann, cudaStream_t st) {
+    k_output_temporal<<<(n + NT - 1) / NT, NT, 0, st>>>(n, pos, d, pos0, d0, orig, ann);
     PT_LAUNCHED();
     return PT_OK;
 }

@@ -97,6 +97,14 @@ pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const floa
                          const int *ch_pos, const float *ch_d, int *nxt_pos, float *nxt_d,
                          unsigned long long *evals, cudaStream_t st);
 pt_status pt_launch_output(int n, const int *pos, const float *d, double *ann, cudaStream_t st);
+/* Temporal lookups (ann_prev): initial field from the previous NNF and the final restore of the
+   unscaled distance (patchtable.h:3548-3585, 4178-4193); *bad becomes 1 when a previous match lies
+   outside the table image and sanitize is off. */
+pt_status pt_launch_init_temporal(const QuerySetup &s, const double *prev, const float *scale_sv, int recalc, int sanitize,
+                                  double temporal_scale, const float4 *a, const float4 *b, int *cur_pos, float *cur_d,
+                                  double *orig, int *bad, cudaStream_t st);
+pt_status pt_launch_output_temporal(int n, const int *pos, const float *d, const int *pos0, const float *d0,
+                                    const double *orig, double *ann, cudaStream_t st);
 
 /* Batched queries (pt_batch.cu): the images of a batch are concatenated -- pixels, patches and
    query state -- and every phase is one persistent launch over the flattened list of row

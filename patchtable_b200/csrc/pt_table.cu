@@ -107,6 +107,9 @@ struct pt_table {
     DevBuf<float> q_d[2], q_chd;
     DevBuf<double> q_ann;
     DevBuf<int> q_lcand;              /* learned proposals, P x PT_PROP_TOPK */
+    DevBuf<double> q_prev, q_torig;   /* temporal lookups: previous NNF (host path), restored distances */
+    DevBuf<float> q_sv, q_td0;
+    DevBuf<int> q_tpos0, q_tbad;
     DevBuf<float> q_lconf;
     DevBuf<unsigned long long> q_counters;
     std::vector<cudaEvent_t> events;
@@ -453,7 +456,8 @@ pt_status mark(pt_table *t, LookupProfile *prof, int stage, cudaStream_t st) {
 /* The device part of a lookup: a_rgb (device, h x w x 3) -> d_ann (device doubles).  With prof,
    an event is recorded after every stage and SSD work is counted. */
 pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d_ann, cudaStream_t st,
-                        LookupProfile *prof = nullptr, pt_proposal *net = nullptr) {
+                        LookupProfile *prof = nullptr, pt_proposal *net = nullptr, const double *d_prev = nullptr,
+                        const float *d_sv = nullptr) {
     const pt_params &p = t->p;
     long long P = (long long) (h - 7) * (w - 7);
     if (P >= (1ll << 31)) return pt_fail(PT_BAD_ARG, "query image too large");
@@ -489,8 +493,21 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     qs.allowed_index = p.allowed_index;
     qs.stream = st;
     if (qs.radius > 2) qs.radius = 2;
-    /* Initial field (patchtable.h:3538-3547): x = b0_ew + 1, dist = DIST_INFINITY. */
-    PT_TRY(pt_launch_init(n, pt_xy(t->ew + 1, 0), (float) PT_DIST_INF, t->q_pos[0].p, t->q_d[0].p, st));
+    const double temporal_scale = 1.0 / (1 + p.coherence_temporal);          /* patchtable.h:3488 */
+    if (d_prev) {
+        PT_CUDA(t->q_tpos0.reserve(P));
+        PT_CUDA(t->q_td0.reserve(P));
+        PT_CUDA(t->q_torig.reserve(P));
+        PT_CUDA(t->q_tbad.reserve(1));
+        PT_CUDA(cudaMemsetAsync(t->q_tbad.p, 0, sizeof(int), st));
+        PT_TRY(pt_launch_init_temporal(qs, d_prev, d_sv, p.recalc_dist_temporal, p.sanitize_input, temporal_scale,
+                                       t->q_rgba.p, t->b_rgba.p, t->q_pos[0].p, t->q_d[0].p, t->q_torig.p, t->q_tbad.p, st));
+        PT_CUDA(cudaMemcpyAsync(t->q_tpos0.p, t->q_pos[0].p, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
+        PT_CUDA(cudaMemcpyAsync(t->q_td0.p, t->q_d[0].p, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+    } else {
+        /* Initial field (patchtable.h:3538-3547): x = b0_ew + 1, dist = DIST_INFINITY. */
+        PT_TRY(pt_launch_init(n, pt_xy(t->ew + 1, 0), (float) PT_DIST_INF, t->q_pos[0].p, t->q_d[0].p, st));
+    }
     PT_TRY(mark(t, prof, LookupProfile::INIT, st));
     int passes = pt_default_passes(p);
     int jump = pt_default_jump(p, passes);
@@ -522,7 +539,10 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
             PT_CUDA(cudaMemcpyAsync(t->q_d[cur].p, t->q_chd.p, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
         }
     }
-    PT_TRY(pt_launch_output(n, t->q_pos[cur].p, t->q_d[cur].p, d_ann, st));
+    if (d_prev && p.coherence_temporal != 0.0)
+        PT_TRY(pt_launch_output_temporal(n, t->q_pos[cur].p, t->q_d[cur].p, t->q_tpos0.p, t->q_td0.p, t->q_torig.p, d_ann, st));
+    else
+        PT_TRY(pt_launch_output(n, t->q_pos[cur].p, t->q_d[cur].p, d_ann, st));
     PT_TRY(mark(t, prof, LookupProfile::OUTPUT, st));
     return PT_OK;
 }
@@ -880,8 +900,28 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int h, int w, double *ann
     double T0 = now_s();
     if (!t || !a || !ann_out) return pt_fail(PT_BAD_ARG, "null argument");
     if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
-    if (ann_prev || coh_sv) return pt_fail(PT_UNSUPPORTED, "ann_prev / coherence_temporal_sv are not implemented yet");
+    if (coh_sv && !ann_prev) return pt_fail(PT_BAD_ARG, "coherence_temporal_sv without ann_prev");
     long long P = (long long) (h - 7) * (w - 7);
+    if (ann_prev) {
+        PT_TRY(ensure_query_buffers(t, h, w));
+        PT_CUDA(t->q_ann.reserve((size_t) P * 3));
+        PT_CUDA(t->q_prev.reserve((size_t) P * 3));
+        PT_CUDA(cudaMemcpyAsync(t->q_prev.p, ann_prev, sizeof(double) * (size_t) P * 3, cudaMemcpyHostToDevice, t->st));
+        if (coh_sv) {
+            PT_CUDA(t->q_sv.reserve(P));
+            PT_CUDA(cudaMemcpyAsync(t->q_sv.p, coh_sv, sizeof(float) * P, cudaMemcpyHostToDevice, t->st));
+        }
+        PT_CUDA(cudaMemcpyAsync(t->q_rgb.p, a, sizeof(float) * (size_t) h * w * 3, cudaMemcpyHostToDevice, t->st));
+        PT_TRY(lookup_device(t, t->q_rgb.p, h, w, t->q_ann.p, t->st, nullptr, nullptr, t->q_prev.p,
+                             coh_sv ? t->q_sv.p : nullptr));
+        PT_CUDA(cudaMemcpyAsync(ann_out, t->q_ann.p, sizeof(double) * (size_t) P * 3, cudaMemcpyDeviceToHost, t->st));
+        int bad = 0;
+        PT_CUDA(cudaMemcpyAsync(&bad, t->q_tbad.p, sizeof(int), cudaMemcpyDeviceToHost, t->st));
+        PT_CUDA(cudaStreamSynchronize(t->st));
+        if (bad) return pt_fail(PT_BAD_ARG, "ann_prev holds matches outside the table image and sanitize_input is 0");
+        if (seconds) *seconds = now_s() - T0;
+        return PT_OK;
+    }
     if (pt_default_passes(t->p) == 1 && t->p.do_prop && h - 7 >= 64) {
         PT_TRY(lookup_banded(t, a, h, w, ann_out));
         if (seconds) *seconds = now_s() - T0;
@@ -895,6 +935,13 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int h, int w, double *ann
     PT_CUDA(cudaStreamSynchronize(t->st));
     if (seconds) *seconds = now_s() - T0;
     return PT_OK;
+}
+
+pt_status pt_table_lookup_device_temporal(pt_table *t, const float *d_a, int h, int w, const double *d_ann_prev,
+                                         const float *d_coh_sv, double *d_ann, void *stream) {
+    if (!t || !d_a || !d_ann || !d_ann_prev) return pt_fail(PT_BAD_ARG, "null argument");
+    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    return lookup_device(t, d_a, h, w, d_ann, (cudaStream_t) stream, nullptr, nullptr, d_ann_prev, d_coh_sv);
 }
 
 pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int h, int w, double *d_ann, void *stream) {
