@@ -45,7 +45,7 @@ typedef struct {
     int nslices[16], n_nslices;       /* explicit -nslices, n_nslices == 0 means automatic */
     int partition_step;
     int populate_random;
-    int run_dt, dt_algo, dt_iters;    /* dt_algo: 1 = prop (the only one restated here) */
+    int run_dt, dt_algo, dt_iters;    /* dt_algo: 1 prop, 4 downsample, 5 hybrid, 6 euclidean */
     int kcoherence, kcoherence_min_dist, kcoherence_step, kcoherence_iter;
     int flann_reset_step, flann_build_step;
     double triangle_factor;
@@ -106,12 +106,16 @@ void gck8(const float *in, int h, int w, int n, int nchroma, float *out) {
                 T(y, x, c) = T(y, x - 1, c) + in_zero(ysrc, xsrc + rread, c) - in_zero(ysrc, xsrc - lread - 1, c);
         }
     }
-    /* Vertical running box sum (gck.h:160-205). */
+    /* Vertical running box sum (gck.h:160-205).  The reference always writes three channels here;
+       with nchroma 0 the first kernel owns one, the extra two land in slots the recurrence below
+       overwrites before reading (or, with fewer than three output channels, past the array's
+       end), so only the first kernel's own channels are written. */
+    const int nc0 = nchroma > 0 ? 3 : 1;
     for (int x = 0; x < OW; x++)
-        for (int c = 0; c < 3; c++) O(0, x, c) = T(rread, x, c);
+        for (int c = 0; c < nc0; c++) O(0, x, c) = T(rread, x, c);
     for (int y = 1; y < OH; y++)
         for (int x = 0; x < OW; x++)
-            for (int c = 0; c < 3; c++)
+            for (int c = 0; c < nc0; c++)
                 O(y, x, c) = O(y - 1, x, c) + T_zero(y + rread, x, c) - T_zero(y - lread - 1, x, c);
     /* Snake-order recurrences for kernels 1..n-1 (gck.h:215-1950, gck.py:364-420):
        out_i(p) = s*out_i(p-d) + out_{i-1}(p) + s*out_{i-1}(p-d), evaluated left to right. */
@@ -239,6 +243,10 @@ vector<int> scale_slices_to_limit(vector<int> nslices, double limit) {
 
 void build_kcoherence(Table &t);
 void dt_prop(Table &t);
+void dt_prop1(Table &t);
+void dt_unmask(Table &t);
+void dt_downsample(Table &t);
+void dt_euclidean(Table &t);
 
 /* PatchTableFixedN constructor, patchtable.h:2584-3373, default path (no product quantisation,
    no k-means, populate_nearest with TABLE_POPULATE_FAST, single table). */
@@ -366,7 +374,10 @@ Table *build(const orc_params &p, const float *b, int h, int w, const int32_t *a
     bool zeros_filled = false;
     if (p.run_dt) {
         if (p.dt_algo == 1) { dt_prop(*t); zeros_filled = (p.dt_iters <= 0); }
-        else { fprintf(stderr, "oracle: only dt_algo prop is restated\n"); abort(); }
+        else if (p.dt_algo == 4) { dt_downsample(*t); zeros_filled = true; }
+        else if (p.dt_algo == 5) { dt_prop1(*t); dt_downsample(*t); dt_unmask(*t); zeros_filled = true; }
+        else if (p.dt_algo == 6) { dt_euclidean(*t); zeros_filled = true; }
+        else { fprintf(stderr, "oracle: dt_algo %d is not restated\n", p.dt_algo); abort(); }
     }
     if (!zeros_filled) {                            /* fill_zeros, patchtable.h:2063-2079 */
         int vfill = xy_to_int(PW - 1, PW - 1);
@@ -420,6 +431,156 @@ void dt_prop(Table &t) {
             }
         }
         cur.swap(nxt);
+    }
+}
+
+const int HI_MASK = 1 << 30;       /* TABLE_HI_MASK, patchtable.h:109-112 */
+
+/* do_dt_prop1, patchtable.h:2306-2325.  Cells are visited in increasing index; each populated
+   cell without the high bit writes its value, with the high bit set, into every adjacent cell
+   that is still unused.  An unused cell therefore ends up with the value of its
+   lowest-indexed populated neighbour. */
+void dt_prop1(Table &t) {
+    int G = t.gnd;
+    for (int64_t j = 0; j < t.ncells; j++) {
+        int32_t v = t.table[j];
+        if (v == UNUSED || (v & HI_MASK)) continue;
+        for (int i = 0; i < G; i++) {
+            int64_t c = (j / t.stride[i]) % t.nslices[i];
+            if (c > 0 && t.table[j - t.stride[i]] == UNUSED) t.table[j - t.stride[i]] = v | HI_MASK;
+            if (c + 1 < t.nslices[i] && t.table[j + t.stride[i]] == UNUSED) t.table[j + t.stride[i]] = v | HI_MASK;
+        }
+    }
+}
+
+/* unmask_table, patchtable.h:2332-2336. */
+void dt_unmask(Table &t) {
+    for (auto &v : t.table) v &= HI_MASK - 1;
+}
+
+namespace {
+
+/* One level of the downsample pyramid: sizes and row-major strides (dimension 0 slowest, like
+   Array's layout). */
+struct Level {
+    vector<int> size;
+    vector<int64_t> stride;
+    vector<int32_t> v;
+    void shape(const vector<int> &s) {
+        size = s;
+        stride.assign(s.size(), 1);
+        int64_t n = 1;
+        for (int d = (int) s.size() - 1; d >= 0; d--) { stride[d] = n; n *= s[d]; }
+        v.assign((size_t) n, UNUSED);
+    }
+};
+
+/* Coordinates of flat index j. */
+void coords_of(int64_t j, const Level &L, vector<int> &c) {
+    for (size_t d = 0; d < L.size.size(); d++) c[d] = (int) ((j / L.stride[d]) % L.size[d]);
+}
+
+}  // namespace
+
+/* do_dt_downsample, patchtable.h:2339-2358, with dt_downsample / dt_upsample (the generated
+   dt_downsample.h).  Each coarser level halves every size (rounding up) until all sizes are 1;
+   a coarse cell takes the first of its up to 2^G children, in lexicographic order with
+   dimension 0 slowest, that holds a value without the high bit, or stays unused.  Going back
+   down, every unused fine cell copies its parent. */
+void dt_downsample(Table &t) {
+    int G = t.gnd;
+    vector<Level> pyr(1);
+    pyr[0].size = t.nslices;
+    pyr[0].stride = t.stride;
+    pyr[0].v = t.table;
+    vector<int> c(G), cc(G);
+    for (;;) {
+        const Level &hi = pyr.back();
+        bool unit = true;
+        for (int s : hi.size) unit = unit && s == 1;
+        if (unit) break;
+        vector<int> ls(G);
+        for (int d = 0; d < G; d++) ls[d] = (hi.size[d] + 1) / 2;
+        Level lo;
+        lo.shape(ls);
+        for (int64_t j = 0; j < (int64_t) lo.v.size(); j++) {
+            coords_of(j, lo, c);
+            /* odometer over the children, last dimension fastest */
+            for (int d = 0; d < G; d++) cc[d] = 2 * c[d];
+            int32_t found = UNUSED;
+            for (;;) {
+                int64_t hj = 0;
+                for (int d = 0; d < G; d++) hj += cc[d] * hi.stride[d];
+                int32_t v = hi.v[hj];
+                if (!(v & HI_MASK) && v != UNUSED) { found = v; break; }
+                int d = G - 1;
+                for (; d >= 0; d--) {
+                    if (++cc[d] < std::min(2 * c[d] + 2, hi.size[d])) break;
+                    cc[d] = 2 * c[d];
+                }
+                if (d < 0) break;
+            }
+            lo.v[j] = found;
+        }
+        pyr.push_back(std::move(lo));
+    }
+    for (size_t k = pyr.size() - 1; k >= 1; k--) {
+        const Level &lo = pyr[k];
+        Level &hi = pyr[k - 1];
+        for (int64_t j = 0; j < (int64_t) hi.v.size(); j++) {
+            if (hi.v[j] != UNUSED) continue;
+            coords_of(j, hi, c);
+            int64_t lj = 0;
+            for (int d = 0; d < G; d++) lj += (c[d] / 2) * lo.stride[d];
+            hi.v[j] = lo.v[lj];
+        }
+    }
+    t.table = pyr[0].v;
+}
+
+/* do_dt_euclidean + euclidean_dt, patchtable.h:4244-4340: the Felzenszwalb-Huttenlocher
+   lower envelope of parabolas, one dimension after another, in single precision.  Distances
+   start at 1E20 for unused cells and 0 for populated ones; the nearest cell's value is carried
+   along in place, so a cell whose parabola lies before it reads the value already moved there
+   in the same line (index_array, patchtable.h:4265). */
+void dt_euclidean(Table &t) {
+    int G = t.gnd;
+    const float INF_F = (float) 1E20;
+    vector<float> dist((size_t) t.ncells);
+    for (int64_t j = 0; j < t.ncells; j++) dist[j] = t.table[j] == UNUSED ? INF_F : 0.0f;
+    int maxn = 0;
+    for (int d = 0; d < G; d++) maxn = std::max(maxn, t.nslices[d]);
+    /* The reference squares ints (curNo*curNo); its build wraps them at 32 bits, which matters
+       from 46341 cells along one dimension on. */
+    auto sq = [](int x) { return (float) (int32_t) ((uint32_t) x * (uint32_t) x); };
+    vector<float> f(maxn), dd(maxn), z(maxn + 1);
+    vector<int> v(maxn);
+    vector<int32_t> idx(maxn);
+    for (int dim = 0; dim < G; dim++) {
+        int n = t.nslices[dim];
+        int64_t st = t.stride[dim];
+        for (int64_t base = 0; base < t.ncells; base++) {
+            if ((base / st) % n != 0) continue;          /* one line per start cell with coord 0 */
+            for (int q = 0; q < n; q++) { f[q] = dist[base + q * st]; idx[q] = t.table[base + q * st]; }
+            int k = 0;
+            v[0] = 0; z[0] = -INF_F; z[1] = INF_F;
+            for (int q = 1; q < n; q++) {
+                float s = ((f[q] + sq(q)) - (f[v[k]] + sq(v[k]))) / (float) (2 * q - 2 * v[k]);
+                while (s <= z[k]) {
+                    k--;
+                    s = ((f[q] + sq(q)) - (f[v[k]] + sq(v[k]))) / (float) (2 * q - 2 * v[k]);
+                }
+                k++;
+                v[k] = q; z[k] = s; z[k + 1] = INF_F;
+            }
+            k = 0;
+            for (int q = 0; q < n; q++) {
+                while (z[k + 1] < (float) q) k++;
+                dd[q] = sq(q - v[k]) + f[v[k]];
+                idx[q] = idx[v[k]];
+            }
+            for (int q = 0; q < n; q++) { dist[base + q * st] = dd[q]; t.table[base + q * st] = idx[q]; }
+        }
     }
 }
 

@@ -440,3 +440,220 @@ pt_status pt_dt_prop(int *table, long long ncells, const int *order_xy, int G, c
     if (levels_out) *levels_out = levels;
     return PT_OK;
 }
+
+/* The other distance transforms of the table build (patchtable.h:3271-3285):
+     do_dt_prop1 + unmask_table  :2306-2336
+     do_dt_downsample            :2339-2358 with dt_downsample / dt_upsample (dt_downsample.h)
+     do_dt_euclidean             :4244-4340
+   All three are pointwise per level or per line, so each runs as independent threads and the
+   result is bit-identical to the sequential loops. */
+namespace {
+
+constexpr int HI_MASK = 1 << 30;        /* TABLE_HI_MASK, patchtable.h:109-112 */
+
+/* A grid of G dimensions laid out row-major (dimension 0 slowest). */
+struct GridShape {
+    int G;
+    long long n;
+    long long stride[PT_DESC_MAX];
+    int size[PT_DESC_MAX];
+};
+
+GridShape grid_shape(int G, const int *size) {
+    GridShape s;
+    s.G = G;
+    s.n = 1;
+    for (int d = G - 1; d >= 0; d--) { s.stride[d] = s.n; s.size[d] = size[d]; s.n *= size[d]; }
+    return s;
+}
+
+/* do_dt_prop1: an unused cell takes, with the high bit set, the value of its lowest-indexed
+   neighbour that was populated before the pass.  Neighbours this pass writes carry the high bit
+   and populated cells are never written, so concurrent writes cannot change what a thread
+   classifies as populated. */
+__global__ void k_dt_prop1(int *table, const GridShape s) {
+    long long j = blockIdx.x * (long long) NT + threadIdx.x;
+    if (j >= s.n || table[j] != PT_UNUSED) return;
+    long long best = -1;
+    int val = 0;
+    for (int d = 0; d < s.G; d++) {
+        int c = (int) ((j / s.stride[d]) % s.size[d]);
+        if (c > 0) {
+            long long k = j - s.stride[d];
+            int v = table[k];
+            if (v != PT_UNUSED && !(v & HI_MASK) && (best < 0 || k < best)) { best = k; val = v; }
+        }
+        if (c + 1 < s.size[d]) {
+            long long k = j + s.stride[d];
+            int v = table[k];
+            if (v != PT_UNUSED && !(v & HI_MASK) && (best < 0 || k < best)) { best = k; val = v; }
+        }
+    }
+    if (best >= 0) table[j] = val | HI_MASK;
+}
+
+__global__ void k_dt_unmask(int *table, long long n) {
+    long long j = blockIdx.x * (long long) NT + threadIdx.x;
+    if (j < n) table[j] &= HI_MASK - 1;
+}
+
+/* dt_downsample: a coarse cell takes the first child, in lexicographic order with dimension 0
+   slowest, holding a value without the high bit; otherwise it is unused.  Only dimensions where
+   the cell has two children enter the enumeration, so its cost is 2^(such dimensions). */
+__global__ void k_dt_down(const int *__restrict__ hi, const GridShape hs, int *lo, const GridShape ls) {
+    long long j = blockIdx.x * (long long) NT + threadIdx.x;
+    if (j >= ls.n) return;
+    long long base = 0;
+    long long twos[PT_DESC_MAX];
+    int m = 0;
+    for (int d = 0; d < ls.G; d++) {
+        int c = (int) ((j / ls.stride[d]) % ls.size[d]);
+        base += 2LL * c * hs.stride[d];
+        if (2 * c + 1 < hs.size[d]) twos[m++] = hs.stride[d];
+    }
+    int out = PT_UNUSED;
+    for (unsigned k = 0; k < (1u << m); k++) {
+        long long h = base;
+        for (int i = 0; i < m; i++)
+            if ((k >> (m - 1 - i)) & 1) h += twos[i];
+        int v = hi[h];
+        if (!(v & HI_MASK) && v != PT_UNUSED) { out = v; break; }
+    }
+    lo[j] = out;
+}
+
+/* dt_upsample: every unused fine cell copies its parent. */
+__global__ void k_dt_up(const int *__restrict__ lo, const GridShape ls, int *hi, const GridShape hs) {
+    long long j = blockIdx.x * (long long) NT + threadIdx.x;
+    if (j >= hs.n || hi[j] != PT_UNUSED) return;
+    long long p = 0;
+    for (int d = 0; d < hs.G; d++) p += (long long) (((j / hs.stride[d]) % hs.size[d]) / 2) * ls.stride[d];
+    hi[j] = lo[p];
+}
+
+__global__ void k_edt_init(const int *__restrict__ table, float *dist, long long n) {
+    long long j = blockIdx.x * (long long) NT + threadIdx.x;
+    if (j < n) dist[j] = table[j] == PT_UNUSED ? 1e20f : 0.0f;
+}
+
+/* euclidean_dt along dimension dim, one thread per line: the lower envelope of the parabolas
+   (q - v)^2 + f(v) with the reference's single-precision operation order, then the distances
+   and, in place along the line, the value of each cell's envelope parabola (index_array,
+   patchtable.h:4265).  The envelope lives in scratch laid out [k][line] so that neighbouring
+   lines touch neighbouring words.  The intersection with the sentinel at -1E20 can never fall
+   at or below it (distances are at most 1E20 and the denominator at least 2), so the k > 0
+   guard never changes a result. */
+__global__ void k_edt_line(int *table, const float *__restrict__ fin, float *fout, const GridShape s, int dim,
+                           long long nlines, int *vs, float *zs) {
+    long long l = blockIdx.x * (long long) NT + threadIdx.x;
+    if (l >= nlines) return;
+    long long base = 0, r = l;
+    for (int d = s.G - 1; d >= 0; d--) {
+        if (d == dim) continue;
+        base += (r % s.size[d]) * s.stride[d];
+        r /= s.size[d];
+    }
+    const int n = s.size[dim];
+    const long long st = s.stride[dim];
+#define V(k) vs[(long long) (k) * nlines + l]
+#define Z(k) zs[(long long) (k) * nlines + l]
+#define F(q) fin[base + (long long) (q) * st]
+    /* Squares of ints wrap at 32 bits as in the reference's build (from 46341 cells on). */
+    auto sq = [](int x) { return (float) (int) ((unsigned) x * (unsigned) x); };
+    auto inter = [&](int q, float fq, int v) {
+        float a = __fadd_rn(fq, sq(q));
+        float b = __fadd_rn(F(v), sq(v));
+        return __fdiv_rn(__fsub_rn(a, b), (float) (2 * q - 2 * v));
+    };
+    int k = 0;
+    V(0) = 0;
+    Z(0) = -1e20f;
+    Z(1) = 1e20f;
+    for (int q = 1; q < n; q++) {
+        float fq = F(q);
+        int v = V(k);
+        float x = inter(q, fq, v);
+        while (k > 0 && x <= Z(k)) {
+            k--;
+            v = V(k);
+            x = inter(q, fq, v);
+        }
+        k++;
+        V(k) = q;
+        Z(k) = x;
+        Z(k + 1) = 1e20f;
+    }
+    k = 0;
+    for (int q = 0; q < n; q++) {
+        while (Z(k + 1) < (float) q) k++;
+        int v = V(k);
+        fout[base + (long long) q * st] = __fadd_rn(sq(q - v), F(v));
+        table[base + (long long) q * st] = table[base + (long long) v * st];
+    }
+#undef V
+#undef Z
+#undef F
+}
+
+}  // namespace
+
+pt_status pt_dt_other(int *table, int G, const int *nslices, int dt_algo, cudaStream_t st) {
+    if (G < 1 || G > PT_DESC_MAX) return pt_fail(PT_BAD_ARG, "grid dims %d outside 1..%d", G, PT_DESC_MAX);
+    GridShape s = grid_shape(G, nslices);
+    if (dt_algo == 5) {
+        k_dt_prop1<<<blocks_for(s.n), NT, 0, st>>>(table, s);
+        PT_LAUNCHED();
+    }
+    if (dt_algo == 4 || dt_algo == 5) {
+        /* Pyramid down to all sizes 1, then back up (do_dt_downsample). */
+        std::vector<GridShape> shapes{s};
+        for (;;) {
+            const GridShape &h = shapes.back();
+            bool unit = true;
+            int ls[PT_DESC_MAX];
+            for (int d = 0; d < G; d++) { unit = unit && h.size[d] == 1; ls[d] = (h.size[d] + 1) / 2; }
+            if (unit) break;
+            shapes.push_back(grid_shape(G, ls));
+        }
+        std::vector<DevBuf<int>> lv(shapes.size());    /* lv[0] unused: level 0 is the table */
+        for (size_t i = 1; i < shapes.size(); i++) PT_CUDA(lv[i].reserve(shapes[i].n));
+        auto level = [&](size_t i) { return i == 0 ? table : lv[i].p; };
+        for (size_t i = 1; i < shapes.size(); i++) {
+            k_dt_down<<<blocks_for(shapes[i].n), NT, 0, st>>>(level(i - 1), shapes[i - 1], level(i), shapes[i]);
+            PT_LAUNCHED();
+        }
+        for (size_t i = shapes.size() - 1; i >= 1; i--) {
+            k_dt_up<<<blocks_for(shapes[i - 1].n), NT, 0, st>>>(level(i), shapes[i], level(i - 1), shapes[i - 1]);
+            PT_LAUNCHED();
+        }
+        if (dt_algo == 5) {
+            k_dt_unmask<<<blocks_for(s.n), NT, 0, st>>>(table, s.n);
+            PT_LAUNCHED();
+        }
+        PT_CUDA(cudaStreamSynchronize(st));            /* the pyramid levels are freed on return */
+        return PT_OK;
+    }
+    if (dt_algo == 6) {
+        int maxn = 0;
+        for (int d = 0; d < G; d++) maxn = std::max(maxn, nslices[d]);
+        long long maxlines = 0;
+        for (int d = 0; d < G; d++) maxlines = std::max(maxlines, s.n / nslices[d]);
+        DevBuf<float> dist[2];
+        DevBuf<int> vs;
+        DevBuf<float> zs;
+        PT_CUDA(dist[0].reserve(s.n));
+        PT_CUDA(dist[1].reserve(s.n));
+        PT_CUDA(vs.reserve(maxlines * maxn));
+        PT_CUDA(zs.reserve(maxlines * (maxn + 1)));
+        k_edt_init<<<blocks_for(s.n), NT, 0, st>>>(table, dist[0].p, s.n);
+        PT_LAUNCHED();
+        for (int d = 0; d < G; d++) {
+            long long nl = s.n / nslices[d];
+            k_edt_line<<<blocks_for(nl), NT, 0, st>>>(table, dist[d & 1].p, dist[(d + 1) & 1].p, s, d, nl, vs.p, zs.p);
+            PT_LAUNCHED();
+        }
+        PT_CUDA(cudaStreamSynchronize(st));
+        return PT_OK;
+    }
+    return pt_fail(PT_UNSUPPORTED, "dt_algo %d is not implemented on the GPU path", dt_algo);
+}

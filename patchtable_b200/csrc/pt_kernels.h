@@ -38,6 +38,9 @@ pt_status pt_launch_table_candidates(const PtBins &bins, const float *desc, int 
 pt_status pt_dt_prop(int *table, long long ncells, const int *order_xy, int G, const int *nslices,
                      const long long *stride, int dt_iters, int run, long long *seeded, int *levels_out,
                      cudaStream_t st);
+/* dt_algo 4 downsample, 5 hybrid (prop1 + downsample + unmask), 6 euclidean on a table whose
+   populated cells hold packed positions. */
+pt_status pt_dt_other(int *table, int G, const int *nslices, int dt_algo, cudaStream_t st);
 pt_status pt_launch_replace(int *table, long long n, int from, int to, cudaStream_t st);
 
 /* k_kcoh.cu */

@@ -144,7 +144,8 @@ pt_status check_params(const pt_params *p, int h, int w) {
     if (p->randomize_dt) return pt_fail(PT_UNSUPPORTED, "randomize_dt is not implemented on the GPU path");
     if (!p->populate_nearest) return pt_fail(PT_UNSUPPORTED, "populate_nearest 0 is not implemented on the GPU path");
     if (p->ntables > 1) return pt_fail(PT_UNSUPPORTED, "ntables > 1 is not implemented on the GPU path");
-    if (p->run_dt && p->dt_algo != 1) return pt_fail(PT_UNSUPPORTED, "dt_algo %d is not implemented on the GPU path", p->dt_algo);
+    if (p->run_dt && p->dt_algo != 1 && p->dt_algo != 4 && p->dt_algo != 5 && p->dt_algo != 6)
+        return pt_fail(PT_UNSUPPORTED, "dt_algo %d is not implemented on the GPU path", p->dt_algo);
     if (p->do_rs || p->spatial) return pt_fail(PT_UNSUPPORTED, "random/spatial search (-do_rs, -spatial) is not implemented on the GPU path");
     if (p->init_random) return pt_fail(PT_UNSUPPORTED, "init_random is not implemented on the GPU path");
     if (p->ndims < 1 || p->ndims > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "ndims %d outside 1..%d", p->ndims, PT_DESC_MAX);
@@ -403,9 +404,13 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
         PT_CUDA(t->table.reserve(t->ncells));
         PT_TRY(pt_launch_fill(t->table.p, t->ncells, PT_UNUSED, t->st));
         PT_TRY(pt_launch_populate(t->bins, t->b_desc.p, t->ds, P, d_rank.p, t->to_bin.p, t->table.p, t->st));
+        /* Distance transform (patchtable.h:3254-3298): prop is the level-synchronous fill; the
+           others run on the resolved table. */
+        bool prop = p.run_dt && p.dt_algo == 1;
         PT_TRY(pt_dt_prop(t->table.p, t->ncells, d_order.p, t->G, t->nslices.data(), t->stride.data(), p.dt_iters,
-                          p.run_dt, &t->add_count, &t->dt_levels, t->st));
-        bool zeros_filled = p.run_dt && p.dt_iters <= 0;
+                          prop, &t->add_count, &t->dt_levels, t->st));
+        if (p.run_dt && !prop) PT_TRY(pt_dt_other(t->table.p, t->G, t->nslices.data(), p.dt_algo, t->st));
+        bool zeros_filled = p.run_dt && (!prop || p.dt_iters <= 0);
         if (!zeros_filled) {                                  /* fill_zeros, patchtable.h:2063-2079 */
             int vfill = pt_xy(7, 7);
             if (!allowed_h.empty())

@@ -31,6 +31,10 @@ CASES = [
     dict(name="small_100x70_speed6", h=70, w=100, seed=15, switches="-speed 6 -limit 0.5"),
     dict(name="c1_320x240", h=240, w=320, seed=1, switches=""),
     dict(name="c1_320x240_coh4", h=240, w=320, seed=1, switches="-coherence_spatial 4"),
+    dict(name="dt_downsample_100x80", h=80, w=100, seed=16, switches="-limit 1 -dt_algo downsample"),
+    dict(name="dt_hybrid_110x90_nd8", h=90, w=110, seed=17, switches="-limit 0.3 -ndims 8 -dt_algo hybrid"),
+    dict(name="dt_euclidean_90x120_nd3", h=120, w=90, seed=18,
+         switches="-limit 2 -ndims 3 -coherence_spatial 4 -dt_algo euclidean"),
 ]
 C2 = dict(name="c2_1920x1080_coh4", h=1080, w=1920, seed=2, switches="-speed 3 -coherence_spatial 4")
 

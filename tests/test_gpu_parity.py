@@ -97,6 +97,36 @@ def test_build_bit_exact_given_descriptors(gpu, oracle, libc, case):
         assert np.array_equal(kg[1], ko[1])
 
 
+DT_CASES = [("-limit 0.5 -nslices 40,9,6,5,4,3,3", 60, 90, 21, False),
+            ("-limit 1 -ndims 8", 73, 41, 5, True),
+            ("-limit 0.05 -grid_ndims 1", 40, 300, 6, False),
+            ("-limit 3 -grid_ndims 2", 50, 60, 7, True)]
+
+
+@pytest.mark.parametrize("algo", ["downsample", "hybrid", "euclidean"])
+@pytest.mark.parametrize("sw,h,w,seed,masked", DT_CASES)
+def test_other_distance_transforms(gpu, oracle, libc, algo, sw, h, w, seed, masked):
+    """dt_algo downsample / hybrid / euclidean: the filled table equals the oracle's bit for bit,
+    including one- and two-dimensional grids and allowed-patch masks (the oracle itself is pinned
+    to the reference by the golden digests)."""
+    a, b = synth.pair(h, w, seed)
+    allowed = None
+    if masked:
+        rng = np.random.default_rng(seed)
+        allowed = (rng.random((h - 7, w - 7)) < 0.7).astype(np.int32)
+    p = ptb.PatchTableParams(sw + " -dt_algo " + algo)
+    srand_all(libc, 1)
+    ot = oracle.build(p.as_dict(), b, allowed=allowed)
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b, wh0=ot.wh0(), allowed_patches=allowed)
+    assert gt.add_count() == ot.add_count()
+    tg = gt.table()
+    assert np.array_equal(tg, ot.table())
+    assert (tg != (1 << 30) - 1).all()
+    ann = gt.lookup(a)
+    check_nnf(oracle, a, b, ann)
+
+
 def check_nnf(oracle, a, b, ann, sample=4000):
     eh, ew = a.shape[0] - 7, a.shape[1] - 7
     beh, bew = b.shape[0] - 7, b.shape[1] - 7

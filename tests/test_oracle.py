@@ -113,6 +113,42 @@ def test_oracle_equals_reference_directly(oracle, reference):
     assert np.array_equal(annr2, anno2)
 
 
+@pytest.mark.parametrize("algo", ["downsample", "hybrid", "euclidean"])
+@pytest.mark.parametrize("sw,h,w,seed,masked", [("-limit 0.5 -nslices 40,9,6,5,4,3,3", 60, 90, 21, False),
+                                                ("-limit 1 -ndims 8", 73, 41, 5, True),
+                                                ("-limit 0.05 -grid_ndims 1", 40, 300, 6, False),
+                                                ("-limit 3 -grid_ndims 2", 50, 60, 7, True)])
+def test_oracle_distance_transforms_equal_reference(oracle, reference, algo, sw, h, w, seed, masked):
+    """dt_algo downsample / hybrid / euclidean tables, with allowed masks.  The reference's
+    downsample is generated for 3..12, 20 and 30 grid dimensions only (it never terminates for
+    others), so one- and two-dimensional grids are compared for euclidean alone."""
+    a, b = synth.pair(h, w, seed)
+    allowed = None
+    if masked:
+        rng = np.random.default_rng(seed)
+        allowed = (rng.random((h - 7, w - 7)) < 0.7).astype(np.int32)
+    s = sw + " -dt_algo " + algo
+    P = reference.params(s)
+    oracle.srand(1)
+    ot = oracle.build(P, b, allowed=allowed)
+    if len(ot.shape()[0]) < 3 and algo != "euclidean":
+        assert (ot.table() != (1 << 30) - 1).all()
+        return
+    reference.srand(1)
+    rt = reference.build(s, b, allowed=allowed)
+    assert np.array_equal(rt.table(), ot.table())
+
+
+def test_oracle_descriptor_without_chroma_is_a_prefix(oracle):
+    """With nchroma 0 the kernels fill channels in order, so fewer dims give a prefix of more
+    dims (the reference itself only builds ndims >= 3)."""
+    _, b = synth.pair(30, 41, 8)
+    d4 = oracle.descriptor(ptb.PatchTableParams("-ndims 4 -nchroma 0").as_dict(), b)
+    for n in (1, 2, 3):
+        dn = oracle.descriptor(ptb.PatchTableParams("-ndims %d -nchroma 0" % n).as_dict(), b)
+        assert np.array_equal(dn, d4[..., :n])
+
+
 def test_vidpair0_known_answer():
     """The reference's own sample pair (patchtable/vidpair0) at -speed 3: the published mean
     distance 0.130757 (patchtable/match_ours_full.txt:4) came from FLANN's approximate k-coherence;
