@@ -89,8 +89,13 @@ pt_status pt_params_from_switches(pt_params *p, const char *switches);
 /* PatchTable<float,float,int32_t>(PatchTableParams *p, const Array<float> &b,
    Array<int32_t> *allowed_patches = NULL), patchtable.h:4397-4424 -> PatchTableFixedN ctor
    patchtable.h:2584-3373.  b is h x w x 3 float RGB (row-major, channels interleaved);
-   allowed is (h-7) x (w-7) int32 or NULL.  In descriptor mode (p->is_descriptor) b is
-   h x w x channels descriptors. */
+   allowed is (h-7) x (w-7) int32 or NULL.  In descriptor mode (p->is_descriptor, 3 <= channels
+   <= 16) b is h x w x channels descriptors, the table takes ndims = channels and nchroma = 0
+   (patchtable.h:4398-4401), every pixel is a patch (every pixel but a 7-wide border with
+   p->descriptor_padded, patchtable.h:2498-2507), allowed holds one entry per such patch, and
+   distances are patch_dist_approx of the descriptors (patchtable.h:376-437).  Descriptor mode
+   tables serve pt_table_lookup, pt_table_lookup_device(_temporal) and pt_table_lookup_profile;
+   batches, learned proposals and table files return PT_UNSUPPORTED. */
 pt_status pt_table_create(const pt_params *p, const float *b, int h, int w, int channels,
                           const int32_t *allowed, pt_table **out);
 
@@ -129,7 +134,8 @@ pt_status pt_table_set_params(pt_table *t, const pt_params *p);
    a: h x w x 3 host floats.  ann_out: (h-7) x (w-7) x 3 host doubles [NNF_X, NNF_Y, NNF_DIST]
    (patchtable.h:175-177).  ann_prev: same layout or NULL.  coh_sv: (h-7) x (w-7) floats or NULL.
    *seconds (may be NULL) receives the wall time of the call including a's descriptor, like the
-   reference's return value (patchtable.h:3477, 4211). */
+   reference's return value (patchtable.h:3477, 4211).  In descriptor mode a is h x w x ndims
+   descriptors and the NNF has h x w records ((h-14) x (w-14) with descriptor_padded). */
 pt_status pt_table_lookup(pt_table *t, const float *a, int h, int w, double *ann_out,
                           const double *ann_prev, const float *coh_sv, double *seconds);
 

@@ -48,6 +48,7 @@ class OrcParams(C.Structure):
         ("allowed_index", C.c_int),
         ("recalc_dist_temporal", C.c_int), ("sanitize_input", C.c_int), ("init_random", C.c_int),
         ("convert_colorspace", C.c_int),
+        ("is_descriptor", C.c_int), ("descriptor_padded", C.c_int),
     ]
 
 
@@ -86,6 +87,8 @@ class Oracle:
         L.orc_descriptor.argtypes = [C.POINTER(OrcParams), _f32p, C.c_int, C.c_int, _f32p]
         L.orc_patch_dist.restype = C.c_float
         L.orc_patch_dist.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f32p, C.c_int, C.c_int, C.c_int]
+        L.orc_patch_dist_approx.restype = C.c_float
+        L.orc_patch_dist_approx.argtypes = [_f32p, _f32p, C.c_int]
         L.orc_scale_slices.argtypes = [_i32p, C.c_int, C.c_double, _i32p]
         L.orc_srand.argtypes = [C.c_uint]
 
@@ -116,6 +119,11 @@ class Oracle:
     def patch_dist(self, a, ax, ay, b, bx, by) -> float:
         return self.lib.orc_patch_dist(a, a.shape[1], ax, ay, b, b.shape[1], bx, by)
 
+    def patch_dist_approx(self, av, bv, nd: int) -> float:
+        """Descriptor-mode distance of two vectors (each at least max(nd, 4) floats: with 3
+        dimensions the fourth float takes part, as in the reference)."""
+        return self.lib.orc_patch_dist_approx(np.ascontiguousarray(av, np.float32), np.ascontiguousarray(bv, np.float32), nd)
+
     def scale_slices(self, ns, limit):
         ns = np.ascontiguousarray(ns, np.int32)
         out = np.empty_like(ns)
@@ -124,14 +132,27 @@ class Oracle:
 
     def build(self, params: dict, b, allowed=None, wh0=None) -> "OracleTable":
         b = np.ascontiguousarray(b, np.float32)
+        if params.get("is_descriptor"):
+            # the reference's constructor takes ndims from the input and drops chroma (patchtable.h:4398-4401)
+            params = dict(params, ndims=b.shape[2], nchroma=0)
         p = params_from_dict(params)
         h = self.lib.orc_build(C.byref(p), b, b.shape[0], b.shape[1], _opt(allowed, np.int32), _opt(wh0, np.float32))
         return OracleTable(self, h, params, b.shape)
 
 
+def virtual_shape(params: dict, shape):
+    """Image whose (h-7) x (w-7) patches the table or query covers: the image itself, or in
+    descriptor mode the virtual image around the descriptors (patchtable.h:2489-2507)."""
+    H, W = shape[0], shape[1]
+    if params.get("is_descriptor"):
+        return (H - 7, W - 7) if params.get("descriptor_padded") else (H + 7, W + 7)
+    return (H, W)
+
+
 class OracleTable:
     def __init__(self, orc: Oracle, handle, params, bshape):
-        self.orc, self.h, self.params, self.bshape = orc, handle, params, bshape
+        self.orc, self.h, self.params = orc, handle, params
+        self.bshape = virtual_shape(params, bshape) + (3,)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -178,7 +199,8 @@ class OracleTable:
 
     def lookup(self, a, ann_prev=None, coh_sv=None):
         a = np.ascontiguousarray(a, np.float32)
-        ann = np.zeros((a.shape[0] - 7, a.shape[1] - 7, 3), np.float64)
+        vh, vw = virtual_shape(self.params, a.shape)
+        ann = np.zeros((vh - 7, vw - 7, 3), np.float64)
         self.orc.lib.orc_lookup(self.h, a, a.shape[0], a.shape[1], ann, _opt(ann_prev, np.float64), _opt(coh_sv, np.float32))
         return ann
 
@@ -259,7 +281,8 @@ class Reference:
         secs = C.c_double()
         h = self.lib.ptref_create(switches.encode(), b, b.shape[0], b.shape[1], b.shape[2],
                                   _opt(allowed, np.int32), verbose, C.byref(secs))
-        t = RefTable(self, h, b.shape, self.params(switches))
+        params = self.params(switches)
+        t = RefTable(self, h, virtual_shape(params, b.shape) + (3,), params)
         t.build_seconds = secs.value
         return t
 
@@ -314,7 +337,8 @@ class RefTable:
 
     def lookup(self, a, ann_prev=None):
         a = np.ascontiguousarray(a, np.float32)
-        ann = np.zeros((a.shape[0] - 7, a.shape[1] - 7, 3), np.float64)
+        vh, vw = virtual_shape(self.params, a.shape)
+        ann = np.zeros((vh - 7, vw - 7, 3), np.float64)
         secs = self.ref.lib.ptref_lookup(self.h, a, a.shape[0], a.shape[1], a.shape[2], ann, _opt(ann_prev, np.float64))
         return ann, secs
 

@@ -55,6 +55,7 @@ typedef struct {
     int allowed_index;
     int recalc_dist_temporal, sanitize_input, init_random;
     int convert_colorspace;
+    int is_descriptor, descriptor_padded;   /* descriptor mode: b and a are ndims-channel images */
 } orc_params;
 
 }
@@ -178,6 +179,45 @@ struct Partition1D {
     }
 };
 
+/* ------------------------------------------------------------------------------------------
+   Descriptor-mode distance: patch_dist_approx<float, TABLE_NCHANNELS>, patchtable.h:376-437
+   (TABLE_SSE).  Four lanes from the first four floats (also with 3 dimensions, where the fourth
+   float is whatever follows in memory); with exactly 8, 12 or 16 dimensions further blocks of
+   four are added lane-wise and the lanes summed 0+1+2+3, otherwise the lanes are summed first
+   and the remaining dimensions added one by one.
+   ------------------------------------------------------------------------------------------ */
+float patch_dist_approx(const float *avec, const float *bvec, int nd) {
+    float l[4];
+    for (int q = 0; q < 4; q++) { float d = avec[q] - bvec[q]; l[q] = d * d; }
+    if (nd == 8 || nd == 12 || nd == 16 || nd == 20) {
+        for (int n = 1; n < nd / 4; n++)
+            for (int q = 0; q < 4; q++) { float d = avec[4 * n + q] - bvec[4 * n + q]; l[q] = l[q] + d * d; }
+        return l[0] + l[1] + l[2] + l[3];
+    }
+    float s = l[0] + l[1] + l[2] + l[3];
+    for (int i = 4; i < nd; i++) { float d = avec[i] - bvec[i]; s += d * d; }
+    return s;
+}
+
+/* get_padded_descriptor in descriptor mode, patchtable.h:2498-2507: an unpadded H x W x nd input
+   goes to offset (7, 7) of a zeroed (H+14) x (W+14) x nd image (copy_rect); a padded input is that
+   image already.  vh x vw is the virtual image whose patches are the input's pixels
+   (TABLE_IMG_HEIGHT / TABLE_IMG_WIDTH, patchtable.h:2489-2490). */
+void padded_input(const orc_params &p, const float *in, int H, int W, vector<float> &wh, int &vh, int &vw) {
+    const int nd = p.ndims;
+    if (p.descriptor_padded) {
+        wh.assign(in, in + (size_t) H * W * nd);
+        vh = H - 7; vw = W - 7;
+        return;
+    }
+    const int WH = H + 14, WW = W + 14;
+    wh.assign((size_t) WH * WW * nd, 0.0f);
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++)
+            for (int c = 0; c < nd; c++) wh[((size_t) (y + 7) * WW + (x + 7)) * nd + c] = in[((size_t) y * W + x) * nd + c];
+    vh = H + 7; vw = W + 7;
+}
+
 struct Table {
     orc_params p;
     int h, w;                   /* b size */
@@ -253,12 +293,20 @@ void dt_euclidean(Table &t);
 Table *build(const orc_params &p, const float *b, int h, int w, const int32_t *allowed, const float *wh0_in) {
     Table *t = new Table();
     t->p = p;
-    t->h = h; t->w = w;
     t->nd = p.ndims;
     t->gnd = p.grid_ndims < 0 ? p.ndims : p.grid_ndims;
-    t->b0.assign(b, b + (size_t) h * w * 3);
-    if (wh0_in) t->wh0.assign(wh0_in, wh0_in + (size_t) (h + 7) * (w + 7) * p.ndims);
-    else padded_descriptor(p, b, h, w, t->wh0);
+    if (p.is_descriptor) {
+        /* b is h x w x ndims descriptors (the caller sets ndims = channels, nchroma = 0 as the
+           reference's constructor does, patchtable.h:4398-4401); b0 is unused. */
+        int vh, vw;
+        padded_input(p, b, h, w, t->wh0, vh, vw);
+        h = vh; w = vw;
+    } else {
+        t->b0.assign(b, b + (size_t) h * w * 3);
+        if (wh0_in) t->wh0.assign(wh0_in, wh0_in + (size_t) (h + 7) * (w + 7) * p.ndims);
+        else padded_descriptor(p, b, h, w, t->wh0);
+    }
+    t->h = h; t->w = w;
     if (allowed) t->allowed.assign(allowed, allowed + (size_t) (h - 7) * (w - 7));
     const int xmin = 7, ymin = 7, xmax = w, ymax = h;   /* gck_xmin/xmax, patchtable_params.h:14-17 */
 
@@ -639,7 +687,11 @@ void build_kcoherence(Table &t) {
                 /* Exact distance of each match to this patch, then sort (dist, pos, valid). */
                 for (int i = 0; i < knn; i++) {
                     int v = matched_indices[i];
-                    matched_dists[i] = patch_dist_exact(t.b0.data(), t.w, x - xmin, y - ymin, t.b0.data(), t.w, int_to_x(v), int_to_y(v));
+                    if (p.is_descriptor)   /* TABLE_PREPARE_B_DIST / TABLE_LOOKUP_PATCH_DIST, patchtable.h:310-320 */
+                        matched_dists[i] = patch_dist_approx(&t.wh0[((size_t) y * t.WW() + x) * nd],
+                                                             &t.wh0[((size_t) (int_to_y(v) + 7) * t.WW() + int_to_x(v) + 7) * nd], nd);
+                    else
+                        matched_dists[i] = patch_dist_exact(t.b0.data(), t.w, x - xmin, y - ymin, t.b0.data(), t.w, int_to_x(v), int_to_y(v));
                 }
                 triples.resize(knn);
                 for (int i = 0; i < knn; i++) triples[i] = std::make_pair(matched_dists[i], std::make_pair(matched_indices[i], (int) is_valid[i]));
@@ -666,12 +718,17 @@ void build_kcoherence(Table &t) {
     }
 }
 
-/* lookup_templated<is_descriptor=0, use_allowed_patches>, patchtable.h:3468-4217. */
+/* lookup_templated<is_descriptor, use_allowed_patches>, patchtable.h:3468-4217.  In descriptor
+   mode a is ah x aw x ndims descriptors, every distance is patch_dist_approx of the two padded
+   descriptor vectors and propagation scores candidates one by one instead of through the
+   summed-area table (patchtable.h:3943, 4043-4060). */
 double lookup(Table &t, const float *a, int ah, int aw, double *ann, const double *ann_prev,
               const float *coh_sv) {
     const orc_params &p = t.p;
     vector<float> &a_wh = t.lookup_wh;
-    padded_descriptor(p, a, ah, aw, a_wh);
+    const bool desc = p.is_descriptor;
+    if (desc) padded_input(p, a, ah, aw, a_wh, ah, aw);
+    else padded_descriptor(p, a, ah, aw, a_wh);
     const int nd = t.nd, G = t.gnd;
     const int awhw = aw + 7;
     double prop_scale = 1.0 / (1 + p.coherence_spatial);
@@ -682,6 +739,9 @@ double lookup(Table &t, const float *a, int ah, int aw, double *ann, const doubl
     bool use_allowed = !t.allowed.empty();
     auto ANN = [&](int y, int x, int c) -> double & { return ann[((size_t) y * ann_w + x) * 3 + c]; };
     auto dist = [&](int ax, int ay, int bx, int by) {
+        if (desc)
+            return patch_dist_approx(&a_wh[((size_t) (ay + 7) * awhw + ax + 7) * nd],
+                                     &t.wh0[((size_t) (by + 7) * t.WW() + bx + 7) * nd], nd);
         return patch_dist_exact(a, aw, ax, ay, t.b0.data(), t.w, bx, by);
     };
     vector<float> lookup_dist_orig;
@@ -804,13 +864,13 @@ double lookup(Table &t, const float *a, int ah, int aw, double *ann, const doubl
                     else if (bx_shift + dx_max > b_w) dx_max = b_w - bx_shift;
                     if (by_shift + dy_min < 0) dy_min = -by_shift;
                     else if (by_shift + dy_max > b_h) dy_max = b_h - by_shift;
-                    if (dx_min > 0 || dy_min > 0) {
+                    if (!desc && (dx_min > 0 || dy_min > 0)) {
                         if (dx_min > 0)
                             for (int dy = dy_min > 0 ? dy_min - 1 : dy_min; dy < dy_max; dy++) sat[(size_t) (dy + 1) * sat_w + dx_min] = 0;
                         if (dy_min > 0)
                             for (int dx = dx_min; dx < dx_max; dx++) sat[(size_t) dy_min * sat_w + dx + 1] = 0;
                     }
-                    for (int dy = dy_min; dy < dy_max; dy++) {
+                    for (int dy = dy_min; dy < dy_max && !desc; dy++) {
                         const float *a_row = a + ((size_t) (ay_shift + dy) * aw + ax_shift) * 3;
                         const float *b_row = t.b0.data() + ((size_t) (by_shift + dy) * t.w + bx_shift) * 3;
                         float *sat_row = &sat[(size_t) (dy + 1) * sat_w + 1];
@@ -833,7 +893,8 @@ double lookup(Table &t, const float *a, int ah, int aw, double *ann, const doubl
                             int xs = dx + bx_shift;
                             if (use_allowed && !t.is_allowed(ys, xs)) { missing = true; continue; }
                             int dx2 = dx + PW;
-                            float dc = s1[dx] - s1[dx2] - s2[dx] + s2[dx2];
+                            float dc = desc ? dist(ax_shift + dx, ay_shift + dy, xs, ys)
+                                            : s1[dx] - s1[dx2] - s2[dx] + s2[dx2];
                             double *ap = &ANN(ay_shift + dy, ax_shift + dx, 0);
                             if (dc < ap[2]) { ap[0] = xs; ap[1] = ys; ap[2] = dc; }
                         }
@@ -905,6 +966,9 @@ void orc_rgb2yuv(const float *in, int h, int w, float *out) { rgb2yuv(in, h * w,
 
 void orc_gck(const float *yuv, int h, int w, int n, int nchroma, float *out) { gck8(yuv, h, w, n, nchroma, out); }
 
+/* patch_dist_approx of two descriptor vectors. */
+float orc_patch_dist_approx(const float *a, const float *b, int nd) { return patch_dist_approx(a, b, nd); }
+
 /* Padded descriptor of an RGB image: (h+7) x (w+7) x ndims. */
 void orc_descriptor(const orc_params *p, const float *rgb, int h, int w, float *out) {
     vector<float> wh;
@@ -961,7 +1025,8 @@ void orc_get_kcoherence(void *tv, int32_t *pos, float *dist) {
     memcpy(dist, t->kc_dist.data(), sizeof(float) * t->kc_dist.size());
 }
 
-/* ann_out: (ah-7) x (aw-7) x 3 doubles [x, y, dist]. ann_prev / coh_sv may be NULL. */
+/* ann_out: (ah-7) x (aw-7) x 3 doubles [x, y, dist]; in descriptor mode a is ah x aw x ndims and
+   ann_out ah x aw x 3 (padded: (ah-14) x (aw-14) x 3).  ann_prev / coh_sv may be NULL. */
 void orc_lookup(void *tv, const float *a, int ah, int aw, double *ann_out, const double *ann_prev, const float *coh_sv) {
     lookup(*(Table *) tv, a, ah, aw, ann_out, ann_prev, coh_sv);
 }

@@ -47,7 +47,7 @@ PatchTableFixedN<float, float, D, int32_t> *fixed(RefTable *r);
 #define PTREF_FIXED(D) \
     template<> PatchTableFixedN<float, float, D, int32_t> *fixed<D>(RefTable *r) { return r->t->p##D; }
 PTREF_FIXED(3) PTREF_FIXED(4) PTREF_FIXED(5) PTREF_FIXED(6) PTREF_FIXED(7) PTREF_FIXED(8)
-PTREF_FIXED(9) PTREF_FIXED(10) PTREF_FIXED(11) PTREF_FIXED(12)
+PTREF_FIXED(9) PTREF_FIXED(10) PTREF_FIXED(11) PTREF_FIXED(12) PTREF_FIXED(13) PTREF_FIXED(14) PTREF_FIXED(15)
 
 /* Calls f(fixed table) for the table's compile-time dimension count. */
 #define PTREF_DISPATCH(r, BODY) \
@@ -62,6 +62,9 @@ PTREF_FIXED(9) PTREF_FIXED(10) PTREF_FIXED(11) PTREF_FIXED(12)
         case 10: { auto T = fixed<10>(r); BODY; } break; \
         case 11: { auto T = fixed<11>(r); BODY; } break; \
         case 12: { auto T = fixed<12>(r); BODY; } break; \
+        case 13: { auto T = fixed<13>(r); BODY; } break; \
+        case 14: { auto T = fixed<14>(r); BODY; } break; \
+        case 15: { auto T = fixed<15>(r); BODY; } break; \
         default: return -1; \
     }
 
@@ -85,7 +88,14 @@ void *ptref_params_new(const char *switches) {
     std::vector<const char *> argv;
     argv.push_back("patchtable");
     for (auto &t : toks) argv.push_back(t.c_str());
-    return new PatchTableParams((int) argv.size(), argv.data());
+    PatchTableParams *p = new PatchTableParams((int) argv.size(), argv.data());
+    /* PatchTableParams does not parse these two; the CLI's match command reads -is_descriptor
+       itself (patchtable_main.cpp:240-242) and analogy.cpp:853 sets descriptor_padded. */
+    for (size_t i = 0; i + 1 < toks.size(); i++) {
+        if (toks[i] == "-is_descriptor") p->is_descriptor = atoi(toks[i + 1].c_str()) != 0;
+        if (toks[i] == "-descriptor_padded") p->descriptor_padded = atoi(toks[i + 1].c_str()) != 0;
+    }
+    return p;
 }
 
 void ptref_params_free(void *p) { delete (PatchTableParams *) p; }
@@ -100,7 +110,7 @@ int ptref_params_get(void *pv, const char *name, double *out) {
     F(coherence_temporal) F(kcoherence) F(kcoherence_min_dist) F(kcoherence_iter)
     F(kcoherence_step) F(prop_iters) F(flann_reset_step) F(flann_build_step) F(query_iters) F(triangle_factor)
     F(populate_random) F(populate_nearest) F(partition_step) F(run_dt) F(do_table_lookup)
-    F(is_descriptor) F(allowed_index) F(recalc_dist_temporal) F(sanitize_input) F(init_random)
+    F(is_descriptor) F(descriptor_padded) F(allowed_index) F(recalc_dist_temporal) F(sanitize_input) F(init_random)
     F(dim_algo) F(colorspace) F(convert_colorspace) F(flann_checks) F(flann_eps) F(table_ratio)
     F(verbose) F(randomize_dt) F(incoherence) F(lookup_algo) F(kcoherence_algo)
 #undef F
@@ -152,7 +162,11 @@ double ptref_lookup(void *rv, const float *a, int h, int w, int channels, double
     Array<double> ann;
     Array<double> *prev = NULL;
     int pw = r->p->patch_w;
-    int eh = r->p->is_descriptor ? h : h - pw + 1, ew = r->p->is_descriptor ? w : w - pw + 1;
+    int eh = h - pw + 1, ew = w - pw + 1;
+    if (r->p->is_descriptor) {                         /* get_padded_descriptor, patchtable.h:2498-2507 */
+        eh = r->p->descriptor_padded ? h - 2 * (pw - 1) : h;
+        ew = r->p->descriptor_padded ? w - 2 * (pw - 1) : w;
+    }
     if (ann_prev) {
         prev = new Array<double>(eh, ew, 3);
         memcpy(prev->data, ann_prev, sizeof(double) * (size_t) prev->nelems);

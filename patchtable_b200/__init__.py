@@ -208,22 +208,37 @@ def _img(x, channels=3):
     return x
 
 
+def _virtual(params, shape):
+    """The image whose (h-7) x (w-7) patches an input covers: the image itself, or in descriptor
+    mode the virtual image around its pixels (patchtable.h:2489-2507)."""
+    if params.is_descriptor:
+        d = -7 if params.descriptor_padded else 7
+        return shape[0] + d, shape[1] + d
+    return shape[0], shape[1]
+
+
 class PatchTable:
-    """PatchTable<float, float, int32_t> (patchtable/patchtable.h:4359-4491) on the GPU."""
+    """PatchTable<float, float, int32_t> (patchtable/patchtable.h:4359-4491) on the GPU.
+
+    With params.is_descriptor, b and the queries are H x W x C descriptor images (3 <= C <= 16;
+    the table takes ndims = C) and the NNF has one record per pixel (per interior pixel with
+    params.descriptor_padded: (H-14) x (W-14))."""
 
     def __init__(self, params: PatchTableParams, b, allowed_patches=None, wh0=None):
-        b = _img(b)
+        b = np.asarray(b)
+        b = _img(b, b.shape[2] if (params.is_descriptor and b.ndim == 3) else 3)
         self.params = params
         self.shape_b = b.shape
         h = C.c_void_p()
         al = None
+        vh, vw = _virtual(params, b.shape)
         if allowed_patches is not None:
             allowed_patches = np.ascontiguousarray(allowed_patches, np.int32)
-            if allowed_patches.shape != (b.shape[0] - 7, b.shape[1] - 7):
-                raise PatchTableError(1, "allowed_patches must be (h-7) x (w-7)")
+            if allowed_patches.shape != (vh - 7, vw - 7):
+                raise PatchTableError(1, "allowed_patches must be %d x %d (one entry per patch)" % (vh - 7, vw - 7))
             al = allowed_patches.ctypes.data_as(C.c_void_p)
         if wh0 is None:
-            _check(lib().pt_table_create(C.byref(params._p), b, b.shape[0], b.shape[1], 3, al, C.byref(h)))
+            _check(lib().pt_table_create(C.byref(params._p), b, b.shape[0], b.shape[1], b.shape[2], al, C.byref(h)))
         else:
             wh0 = np.ascontiguousarray(wh0, np.float32)
             _check(lib().pt_table_create_with_descriptor(C.byref(params._p), b, b.shape[0], b.shape[1], wh0, al, C.byref(h)))
@@ -267,8 +282,10 @@ class PatchTable:
         """PatchTable::lookup (patchtable.h:4448): returns the NNF (written into `out` when given,
         e.g. a pinned buffer); the wall time of the call (including a's descriptor, like the
         reference's return value) is in self.last_seconds."""
-        a = _img(a)
-        shape = (a.shape[0] - 7, a.shape[1] - 7, 3)
+        a = np.asarray(a)
+        a = _img(a, a.shape[2] if (self.params.is_descriptor and a.ndim == 3) else 3)
+        vh, vw = _virtual(self.params, a.shape)
+        shape = (vh - 7, vw - 7, 3)
         if out is not None:
             if out.shape != shape or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
                 raise PatchTableError(1, "out must be a C-contiguous float64 array of shape %s" % (shape,))
@@ -316,7 +333,7 @@ class PatchTable:
     # -- batches ---------------------------------------------------------------------------------
     def lookup_batch(self, images):
         """pt_table_lookup_batch: NNFs of several host images (any sizes) in one batched query."""
-        imgs = [_img(x) for x in images]
+        imgs = [_img(x, np.shape(x)[2] if (self.params.is_descriptor and np.ndim(x) == 3) else 3) for x in images]
         n = len(imgs)
         if n == 0:
             return []

@@ -228,3 +228,41 @@ pt_status pt_launch_descriptor_batch(int ndims, int nchroma, const PtBatchImage 
     PT_LAUNCHED();
     return PT_OK;
 }
+
+namespace {
+
+/* get_padded_descriptor in descriptor mode (patchtable.h:2498-2507): an unpadded input sits at
+   offset 7 of a zero-padded (H+14) x (W+14) image, a padded input is that image already, and the
+   patch at (x, y) is pixel (x+7, y+7) of it.  With 3 dimensions slot 3 holds the next pixel's
+   first channel, the value the reference's four-float load picks up (pt_descdist.cuh). */
+__global__ void k_desc_input(const float *__restrict__ in, int H, int W, int nd, int padded, int ew, int eh,
+                             float *desc, int ds) {
+    const long long p = blockIdx.x * (long long) NT + threadIdx.x;
+    if (p >= (long long) ew * eh) return;
+    const int x = (int) (p % ew), y = (int) (p / ew);
+    const int off = padded ? 0 : 7;
+    auto at = [&](int py, int px, int c) -> float {
+        const int iy = py - off, ix = px - off;
+        return (iy >= 0 && iy < H && ix >= 0 && ix < W) ? __ldg(in + ((size_t) iy * W + ix) * nd + c) : 0.0f;
+    };
+    float *o = desc + p * ds;
+    for (int c = 0; c < ds; c++) {
+        float v = 0.0f;
+        if (c < nd) v = at(y + 7, x + 7, c);
+        else if (nd == 3 && c == 3) v = at(y + 7, x + 8, 0);
+        o[c] = v;
+    }
+}
+
+}  // namespace
+
+pt_status pt_launch_descriptor_input(const float *in, int H, int W, int nd, int padded, float *desc, int ds,
+                                     cudaStream_t st) {
+    const int ew = padded ? W - 14 : W, eh = padded ? H - 14 : H;
+    if (ew < 1 || eh < 1) return pt_fail(PT_BAD_ARG, "descriptor image %dx%d has no patches", W, H);
+    if (nd < 3 || nd > ds || ds > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "descriptor dimensions %d outside 3..%d", nd, PT_DESC_MAX);
+    const long long P = (long long) ew * eh;
+    k_desc_input<<<(unsigned) ((P + NT - 1) / NT), NT, 0, st>>>(in, H, W, nd, padded, ew, eh, desc, ds);
+    PT_LAUNCHED();
+    return PT_OK;
+}

@@ -21,6 +21,7 @@
 #include <cub/cub.cuh>
 
 #include "pt_internal.h"
+#include "pt_descdist.cuh"
 #include "pt_kernels.h"
 
 namespace {
@@ -108,6 +109,20 @@ __global__ void k_kc_ssd(const float4 *__restrict__ b, int bw, const int *__rest
     if (q >= Q || j >= knn[q]) return;
     int v = tpos[nbr[(size_t) q * Kc + j]];
     ssd[(size_t) q * Kc + j] = ssd_exact(b, bw, pt_x(qpos[q]), pt_y(qpos[q]), b, bw, pt_x(v), pt_y(v));
+}
+
+/* Descriptor mode: patch_dist_approx of the two patches' descriptor store entries
+   (TABLE_LOOKUP_PATCH_DIST with is_descriptor, patchtable.h:310-320). */
+__global__ void k_kc_desc(const float4 *__restrict__ bdesc, int ds4, int nd, int ew, const int *__restrict__ nbr, int Kc,
+                          int Q, const int *__restrict__ qpos, const int *__restrict__ tpos, const int *__restrict__ knn,
+                          float *ssd) {
+    long long t = blockIdx.x * 256ll + threadIdx.x;
+    int q = (int) (t / Kc), j = (int) (t % Kc);
+    if (q >= Q || j >= knn[q]) return;
+    int v = tpos[nbr[(size_t) q * Kc + j]];
+    float4 a[4];
+    pt_desc_load(bdesc + ((size_t) pt_y(qpos[q]) * ew + pt_x(qpos[q])) * ds4, 4 * ds4, a);
+    ssd[(size_t) q * Kc + j] = pt_desc_dist(a, bdesc + ((size_t) pt_y(v) * ew + pt_x(v)) * ds4, nd);
 }
 
 /* The sequential selection of one segment with incoming stale bit `bin` (the flag at index
@@ -202,7 +217,7 @@ pt_status pt_gather_rows(const float *desc, int ds, int nd, const int *rows, int
     return PT_OK;
 }
 
-pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *train, int N, int nd, const int *tpos,
+pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *bdesc, int ds, int ew, const float *train, int N, int nd, const int *tpos,
                         const float *qdesc, const int *qpos, const int *qcell, int Q, const int *seg_start, int nseg,
                         int kc, int min_dist, int2 *kcoh, int *max_knn_out, cudaStream_t st) {
     if (kc < 1 || kc >= 32) return pt_fail(PT_UNSUPPORTED, "kcoherence must be in 1..31");
@@ -232,7 +247,11 @@ pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *train, int N,
         PT_CUDA(cudaStreamSynchronize(st));
         if (overflow) { Kc *= 2; continue; }
         long long tot = (long long) Q * Kc;
-        k_kc_ssd<<<(unsigned) ((tot + 255) / 256), 256, 0, st>>>(b_rgba, bw, nbr.p, Kc, Q, qpos, tpos, knn.p, ssd.p);
+        if (bdesc)
+            k_kc_desc<<<(unsigned) ((tot + 255) / 256), 256, 0, st>>>(reinterpret_cast<const float4 *>(bdesc), ds / 4, nd, ew,
+                                                                      nbr.p, Kc, Q, qpos, tpos, knn.p, ssd.p);
+        else
+            k_kc_ssd<<<(unsigned) ((tot + 255) / 256), 256, 0, st>>>(b_rgba, bw, nbr.p, Kc, Q, qpos, tpos, knn.p, ssd.p);
         PT_LAUNCHED();
         DevBuf<int2> o0, o1;
         DevBuf<unsigned char> fn, pre;

@@ -19,6 +19,7 @@
 #include <cstring>
 
 #include "pt_internal.h"
+#include "pt_descdist.cuh"
 #include "pt_kernels.h"
 
 namespace {
@@ -42,6 +43,9 @@ struct QPlan {
     const float4 *b1;        /* b shifted by one pixel: b1[i] = b[i + 1] */
     const int *allowed;      /* b patches that may be matched (allowed[p] == allowed_index), or NULL */
     int allowed_index;
+    const float4 *adesc;     /* descriptor mode: query descriptor store (ds4 float4 per patch), or NULL */
+    const float4 *bdesc;     /* descriptor mode: table descriptor store */
+    int ds4, nd;             /* float4 per store entry, descriptor dimensions */
 };
 
 __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
@@ -54,6 +58,7 @@ __device__ __forceinline__ void count_work(unsigned long long *counters, unsigne
 }
 
 constexpr int TWD = 32;                   /* query patches per CTA row segment when none is chosen */
+constexpr int TWD_DESC = 64;              /* query patches per CTA in descriptor mode */
 
 /* Stages the 8 pixel rows under a CTA's row segment of TW query patches in shared memory
    (TW + 7 pixels per row). */
@@ -159,6 +164,46 @@ __device__ __forceinline__ void ssd_group(const float4 *atile, int tx, const QPl
     for (int g = 0; g < G; g++) out[g] = live[g] ? lane_total(l[g]) : finf();
 }
 
+/* The query patch a distance is taken from: its RGB rows staged in shared memory (image mode) or
+   its descriptor in registers (descriptor mode, DESC instantiations). */
+struct AQuery {
+    const float4 *atile;
+    int tx;
+    float4 v[4];
+};
+
+/* One candidate's distance: patch_dist_exact (image mode, abandoned at `bound`) or
+   patch_dist_approx of the descriptors (descriptor mode, always complete: a complete sum at or
+   above the bound is rejected by the caller exactly as an abandoned one). */
+template<int TW, bool DESC>
+__device__ __forceinline__ float dist1(const AQuery &aq, const QPlan &q, const float4 *__restrict__ B, int bx, int by,
+                                       float bound, unsigned &rows) {
+    if constexpr (DESC) {
+        rows++;
+        return pt_desc_dist(aq.v, q.bdesc + ((size_t) by * q.bew + bx) * q.ds4, q.nd);
+    } else {
+        return ssd_tile<TW>(aq.atile, aq.tx, q, B, bx, by, bound, rows);
+    }
+}
+
+template<int TW, int G, bool DESC>
+__device__ __forceinline__ void dist_group(const AQuery &aq, const QPlan &q, const float4 *__restrict__ B,
+                                           const int (&cand)[G], unsigned valid, float bound, float (&out)[G],
+                                           unsigned &rows) {
+    if constexpr (DESC) {
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            out[g] = finf();
+            if ((valid >> g) & 1) {
+                rows++;
+                out[g] = pt_desc_dist(aq.v, q.bdesc + ((size_t) pt_y(cand[g]) * q.bew + pt_x(cand[g])) * q.ds4, q.nd);
+            }
+        }
+    } else {
+        ssd_group<TW, G>(aq.atile, aq.tx, q, B, cand, valid, bound, out, rows);
+    }
+}
+
 /* Proposals of the learned network for one patch (LEARNED instantiation of k_choose_tile). */
 struct LearnedArgs {
     const int *cand;          /* n x 8 table entries, -1 = none; NULL on passes without proposals */
@@ -173,19 +218,25 @@ struct LearnedArgs {
    instantiation replaces, for patches whose proposal confidence reaches the threshold, the table
    candidate by the network's proposals (scored best-first in groups of three) and, unless
    configured otherwise, skips k-coherence for them. */
-template<int TW, bool LEARNED>
+template<int TW, bool LEARNED, bool DESC>
 __device__ __forceinline__ void
 choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const float4 *__restrict__ b,
            const int *__restrict__ cur_pos, const float *__restrict__ cur_d, const int *__restrict__ tcand,
            const int2 *__restrict__ kcoh, int do_table, int *ch_pos, float *ch_d, int *kc_done, int use_done,
            unsigned long long *counters, const LearnedArgs &la, int x0, int y) {
-    stage_a<TW>(atile, a, c_q.aw, c_q.ah, x0, y);
-    __syncthreads();
+    if constexpr (!DESC) {
+        stage_a<TW>(atile, a, c_q.aw, c_q.ah, x0, y);
+        __syncthreads();
+    }
     const int x = x0 + threadIdx.x;
     const bool live = x < c_q.ew;
     unsigned ne = 0, rows = 0, n_conf = 0, n_prop = 0;
     if (live) {
         const int p = y * c_q.ew + x;
+        AQuery aq;
+        aq.atile = atile;
+        aq.tx = threadIdx.x;
+        if constexpr (DESC) pt_desc_load(c_q.adesc + (size_t) p * c_q.ds4, 4 * c_q.ds4, aq.v);
         int pos = cur_pos[p];
         float dstore = cur_d[p];
         int xb = pt_x(pos), yb = pt_y(pos);
@@ -217,7 +268,7 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
                 if (!m) continue;
                 const int cg[G] = {cand[g0], cand[g0 + 1], g0 + 2 <= PT_PROP_TOPK ? cand[g0 + 2] : -1};
                 float d[G];
-                ssd_group<TW, G>(atile, threadIdx.x, c_q, b, cg, m, dbest, d, rows);
+                dist_group<TW, G, DESC>(aq, c_q, b, cg, m, dbest, d, rows);
 #pragma unroll
                 for (int g = 0; g < G; g++)
                     if (((m >> g) & 1) && d[g] < dbest) { dbest = d[g]; dch = d[g]; xb = pt_x(cg[g]); yb = pt_y(cg[g]); }
@@ -229,7 +280,7 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
             int v = tcand[p];
             int xs = pt_x(v) - 7, ys = pt_y(v) - 7;
             if (xs != xb || ys != yb) {
-                float dc = ssd_tile<TW>(atile, threadIdx.x, c_q, b, xs, ys, dbest, rows);
+                float dc = dist1<TW, DESC>(aq, c_q, b, xs, ys, dbest, rows);
                 ne++;
                 if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
             }
@@ -273,7 +324,7 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
                 if (m != (1u << G) - 1) done = true;     /* the list ends or stops inside this group */
                 if (!m) break;
                 float d[G];
-                ssd_group<TW, G>(atile, threadIdx.x, c_q, b, cg, m, dbest, d, rows);
+                dist_group<TW, G, DESC>(aq, c_q, b, cg, m, dbest, d, rows);
                 ne += __popc(m);
 #pragma unroll
                 for (int j = 0; j < G; j++) {
@@ -297,14 +348,14 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
 /* At most 12 x 64 threads' worth of CTAs per SM's register file: the compiler keeps the kernel at
    80 registers (a few bytes of spills), and the extra resident warps hide the gather latency
    better than the unrestricted 103-register version (measured: choose 0.70 -> 0.64 ms at 1080p). */
-template<int TW, bool LEARNED>
+template<int TW, bool LEARNED, bool DESC>
 __global__ void __launch_bounds__(TW, (12 * 64) / TW)
 k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
               const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
               int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters, const LearnedArgs la) {
     extern __shared__ float4 atile[];
-    choose_seg<TW, LEARNED>(c_q, atile, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done, use_done,
-                            counters, la, blockIdx.x * TW, blockIdx.y + c_q.row0);
+    choose_seg<TW, LEARNED, DESC>(c_q, atile, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done,
+                                  use_done, counters, la, blockIdx.x * TW, blockIdx.y + c_q.row0);
 }
 
 /* Step 4 as a pull: the best of the stored match and every neighbour's chosen offset applied to
@@ -314,18 +365,24 @@ k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__res
    Neighbours sit `step` patches apart; passes with decreasing steps (jump flooding) carry an
    offset across a region in a logarithmic number of passes, where the reference's sequential
    sweep carries it along a whole row in one sweep. */
-template<int TW, int R>
+template<int TW, int R, bool DESC>
 __device__ __forceinline__ void
 pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const float4 *__restrict__ b,
          const int *__restrict__ cur_pos, const float *__restrict__ cur_d, const int *__restrict__ ch_pos,
          const float *__restrict__ ch_d, int *nxt_pos, float *nxt_d, unsigned long long *counters, int x0, int y) {
-    stage_a<TW>(atile, a, c_q.aw, c_q.ah, x0, y);
-    __syncthreads();
+    if constexpr (!DESC) {
+        stage_a<TW>(atile, a, c_q.aw, c_q.ah, x0, y);
+        __syncthreads();
+    }
     const int x = x0 + threadIdx.x;
     const bool live = x < c_q.ew;
     unsigned ne = 0, rows = 0;
     if (live) {
         const int p = y * c_q.ew + x;
+        AQuery aq;
+        aq.atile = atile;
+        aq.tx = threadIdx.x;
+        if constexpr (DESC) pt_desc_load(c_q.adesc + (size_t) p * c_q.ds4, 4 * c_q.ds4, aq.v);
         int bpos = cur_pos[p];
         float bd = cur_d[p];
         {
@@ -378,7 +435,7 @@ pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const fl
                 const int left = nc - g0;
                 const unsigned m = left >= G ? (1u << G) - 1 : (1u << left) - 1;
                 float d[G];
-                ssd_group<TW, G>(atile, threadIdx.x, c_q, b, cg, m, bd, d, rows);
+                dist_group<TW, G, DESC>(aq, c_q, b, cg, m, bd, d, rows);
 #pragma unroll
                 for (int g = 0; g < G; g++)
                     if (((m >> g) & 1) && d[g] < bd) { bd = d[g]; bpos = cg[g]; }
@@ -391,14 +448,14 @@ pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const fl
     count_work(counters, ne, rows);
 }
 
-template<int TW, int R>
+template<int TW, int R, bool DESC>
 __global__ void __launch_bounds__(TW)
 k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
             const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
             int *nxt_pos, float *nxt_d, unsigned long long *counters) {
     extern __shared__ float4 atile[];
-    pull_seg<TW, R>(c_q, atile, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, counters, blockIdx.x * TW,
-                    blockIdx.y + c_q.row0);
+    pull_seg<TW, R, DESC>(c_q, atile, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, counters, blockIdx.x * TW,
+                          blockIdx.y + c_q.row0);
 }
 
 /* ---- batched queries: many images, one launch per phase over a flattened segment list ---- */
@@ -432,7 +489,7 @@ k_choose_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, l
         QPlan q = base;
         q.aw = g.w; q.ah = g.h; q.ew = g.ew; q.eh = g.eh;
         const long long o = g.patch_off;
-        choose_seg<TW, false>(q, atile, a + g.pix_off, b, cur_pos + o, cur_d + o, tcand + o, kcoh, do_table, ch_pos + o,
+        choose_seg<TW, false, false>(q, atile, a + g.pix_off, b, cur_pos + o, cur_d + o, tcand + o, kcoh, do_table, ch_pos + o,
                               ch_d + o, kc_done + o, use_done, counters, none, x0, y);
         __syncthreads();                       /* the next segment restages atile */
     }
@@ -454,7 +511,7 @@ k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, lon
         QPlan q = base;
         q.aw = g.w; q.ah = g.h; q.ew = g.ew; q.eh = g.eh;
         const long long o = g.patch_off;
-        pull_seg<TW, R>(q, atile, a + g.pix_off, b, cur_pos + o, cur_d + o, ch_pos + o, ch_d + o, nxt_pos + o, nxt_d + o,
+        pull_seg<TW, R, false>(q, atile, a + g.pix_off, b, cur_pos + o, cur_d + o, ch_pos + o, ch_d + o, nxt_pos + o, nxt_d + o,
                         counters, x0, y);
         __syncthreads();
     }
@@ -495,7 +552,14 @@ __global__ void k_init_temporal(const QPlan q, const double *__restrict__ prev, 
     }
     double scaled;
     if (recalc) {
-        const float dcur = ssd_global(q, a, x, y, B, xs, ys);
+        float dcur;
+        if (q.adesc) {
+            float4 v[4];
+            pt_desc_load(q.adesc + (size_t) p * q.ds4, 4 * q.ds4, v);
+            dcur = pt_desc_dist(v, q.bdesc + ((size_t) ys * q.bew + xs) * q.ds4, q.nd);
+        } else {
+            dcur = ssd_global(q, a, x, y, B, xs, ys);
+        }
         scaled = (double) dcur * (scale_sv ? (double) scale_sv[p] : temporal_scale);
     } else {
         scaled = prev[3 * (size_t) p + 2] * temporal_scale;
@@ -556,7 +620,16 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     q.b1 = s.b1;
     q.allowed = s.allowed;
     q.allowed_index = s.allowed_index;
-    if (!q.b1) return pt_fail(PT_BAD_ARG, "query without the shifted copy of the table image");
+    q.adesc = reinterpret_cast<const float4 *>(s.adesc);
+    q.bdesc = reinterpret_cast<const float4 *>(s.bdesc);
+    q.ds4 = s.ds / 4;
+    q.nd = s.nd;
+    if (q.adesc) {
+        if (!q.bdesc || (s.ds != 8 && s.ds != 16) || q.nd < 3 || q.nd > s.ds)
+            return pt_fail(PT_BAD_ARG, "descriptor query: store of %d floats for %d dimensions", s.ds, q.nd);
+    } else if (!q.b1) {
+        return pt_fail(PT_BAD_ARG, "query without the shifted copy of the table image");
+    }
     if (q.radius > 2) return pt_fail(PT_UNSUPPORTED, "propagation radius %d > 2 on the GPU path", q.radius);
     return PT_OK;
 }
@@ -575,9 +648,18 @@ pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const fl
     (void) n;
     LearnedArgs none;
     memset(&none, 0, sizeof(none));
+    if (q.adesc) {                       /* descriptor mode: one tile width, nothing staged */
+        constexpr int T = TWD_DESC;
+        dim3 grid((q.ew + T - 1) / T, q.rows);
+        k_choose_tile<T, false, true><<<grid, T, 0, st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d,
+                                                          kc_done, use_done, evals, none);
+        PT_LAUNCHED();
+        return PT_OK;
+    }
 #define PT_CHOOSE_T(T) { dim3 grid((q.ew + T - 1) / T, q.rows); \
-        k_choose_tile<T, false><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, \
-                                                                             ch_pos, ch_d, kc_done, use_done, evals, none); }
+        k_choose_tile<T, false, false><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, \
+                                                                                    do_table, ch_pos, ch_d, kc_done, use_done, \
+                                                                                    evals, none); }
     switch (q.tile) {
         case 32: PT_CHOOSE_T(32) break;
         case 64: PT_CHOOSE_T(64) break;
@@ -597,6 +679,7 @@ pt_status pt_launch_choose_learned(const QuerySetup &s, const float4 *a, const f
     QPlan q;
     PT_TRY(make_qplan(s, q));
     if (!lconf) return pt_fail(PT_BAD_ARG, "learned choose without confidences");
+    if (q.adesc) return pt_fail(PT_UNSUPPORTED, "learned proposals in descriptor mode");
     LearnedArgs la;
     la.cand = lcand;
     la.conf = lconf;
@@ -604,8 +687,9 @@ pt_status pt_launch_choose_learned(const QuerySetup &s, const float4 *a, const f
     la.kcoh_confident = kcoh_confident;
     la.counters = lcounters;
 #define PT_CHOOSE_L(T) { dim3 grid((q.ew + T - 1) / T, q.rows); \
-        k_choose_tile<T, true><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, \
-                                                                            ch_pos, ch_d, kc_done, use_done, evals, la); }
+        k_choose_tile<T, true, false><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, \
+                                                                                   do_table, ch_pos, ch_d, kc_done, use_done, \
+                                                                                   evals, la); }
     switch (q.tile) {
         case 32: PT_CHOOSE_L(32) break;
         case 64: PT_CHOOSE_L(64) break;
@@ -623,10 +707,18 @@ pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const floa
     QPlan q;
     PT_TRY(make_qplan(s, q));
     (void) n;
-#define PT_PULL_T(T, RR) { dim3 grid((q.ew + T - 1) / T, q.rows); \
-        k_pull_tile<T, RR><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, \
-                                                                         evals); }
     const bool r1 = q.radius <= 1;
+    if (q.adesc) {
+        constexpr int T = TWD_DESC;
+        dim3 grid((q.ew + T - 1) / T, q.rows);
+        if (r1) k_pull_tile<T, 1, true><<<grid, T, 0, st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals);
+        else k_pull_tile<T, 2, true><<<grid, T, 0, st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals);
+        PT_LAUNCHED();
+        return PT_OK;
+    }
+#define PT_PULL_T(T, RR) { dim3 grid((q.ew + T - 1) / T, q.rows); \
+        k_pull_tile<T, RR, false><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, \
+                                                                                nxt_pos, nxt_d, evals); }
     switch (q.tile) {
         case 32: if (r1) PT_PULL_T(32, 1) else PT_PULL_T(32, 2) break;
         case 64: if (r1) PT_PULL_T(64, 1) else PT_PULL_T(64, 2) break;

@@ -14,6 +14,10 @@ pt_status pt_launch_descriptor(int ndims, int nchroma, const float *rgb, int h, 
 /* Rows [trow0, trow0 + trows) of 8-patch descriptor tiles only (for banded lookups). */
 pt_status pt_launch_descriptor_rows(int ndims, int nchroma, const float *rgb, int h, int w, int convert, float4 *rgba,
                                     float *desc, int ds, int trow0, int trows, cudaStream_t st);
+/* Descriptor mode: the store entries (ds floats per patch) of an H x W x nd descriptor image,
+   padded (descriptor_padded: patches (H-14) x (W-14)) or not (patches H x W). */
+pt_status pt_launch_descriptor_input(const float *in, int H, int W, int nd, int padded, float *desc, int ds,
+                                     cudaStream_t st);
 
 /* k_build.cu */
 pt_status pt_launch_fill(int *p, long long n, int v, cudaStream_t st);
@@ -46,7 +50,9 @@ pt_status pt_launch_replace(int *table, long long n, int from, int to, cudaStrea
 /* k_kcoh.cu */
 pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, int Q, int K, int *out, cudaStream_t st);
 pt_status pt_gather_rows(const float *desc, int ds, int nd, const int *rows, int n, float *out, cudaStream_t st);
-pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *train, int N, int nd, const int *tpos,
+/* Exact distances from b_rgba (image mode) or, when bdesc is set, from the descriptor store
+   (descriptor mode: ds floats per patch, ew patches per row). */
+pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *bdesc, int ds, int ew, const float *train, int N, int nd, const int *tpos,
                         const float *qdesc, const int *qpos, const int *qcell, int Q, const int *seg_start, int nseg,
                         int kc, int min_dist, int2 *kcoh, int *max_knn_out, cudaStream_t st);
 
@@ -62,6 +68,11 @@ struct QuerySetup {
     const float4 *b1 = nullptr;   /* the table image shifted by one pixel, b1[i] = b[i + 1] */
     const int *allowed = nullptr; /* b patches a match may use (allowed[p] == allowed_index), or NULL */
     int allowed_index = 0;
+    /* Descriptor mode (is_descriptor): distances are patch_dist_approx between the query's and the
+       table's descriptor store entries (pt_descdist.cuh) instead of RGB patch SSDs. */
+    const float *adesc = nullptr; /* query descriptors, (ah-7) x (aw-7) entries of ds floats, or NULL */
+    const float *bdesc = nullptr; /* table descriptors, (bh-7) x (bw-7) entries of ds floats */
+    int ds = 8, nd = 0;
     cudaStream_t stream;
 };
 /* Query schedule.  By default two choose + pull passes stand in for each of the reference's

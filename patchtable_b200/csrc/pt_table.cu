@@ -78,6 +78,11 @@ struct pt_table {
     pt_params p;
     int h = 0, w = 0, eh = 0, ew = 0;
     int nd = 0, G = 0, ds = 8;
+    /* Descriptor mode (is_descriptor): b and the queries are descriptor images and h x w is the
+       virtual image whose (h-7) x (w-7) patches are their pixels (get_padded_descriptor,
+       patchtable.h:2498-2507); no RGB copy of b exists. */
+    bool desc_mode = false;
+    int in_padded = 0;
     cudaStream_t st = nullptr;
     bool own_stream = false;
     DevBuf<float4> b_rgba;
@@ -135,9 +140,9 @@ pt_status check_params(const pt_params *p, int h, int w) {
     if (p->patch_w != 8) return pt_fail(PT_UNSUPPORTED, "patch_w=%d: only 8x8 patches are supported (gck.h)", p->patch_w);
     if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
     if (w > 65535 || h > 16383) return pt_fail(PT_BAD_ARG, "image %dx%d exceeds the packed position range (XY_TO_INT)", w, h);
-    if (p->is_descriptor) return pt_fail(PT_UNSUPPORTED, "descriptor mode is not implemented on the GPU path");
     if (p->dim_algo != 0) return pt_fail(PT_UNSUPPORTED, "dim_algo pca is not implemented on the GPU path");
-    if (p->convert_colorspace && p->colorspace != 0) return pt_fail(PT_UNSUPPORTED, "colorspace lab is not implemented on the GPU path");
+    if (!p->is_descriptor && p->convert_colorspace && p->colorspace != 0)
+        return pt_fail(PT_UNSUPPORTED, "colorspace lab is not implemented on the GPU path");
     if (p->lookup_algo != 0) return pt_fail(PT_UNSUPPORTED, "only lookup_algo table is implemented on the GPU path");
     if (p->kcoherence && p->kcoherence_algo != 0) return pt_fail(PT_UNSUPPORTED, "only kcoherence_algo flann (exact search) is implemented");
     if (p->incoherence) return pt_fail(PT_UNSUPPORTED, "incoherence is not implemented on the GPU path");
@@ -294,8 +299,9 @@ pt_status build_kcoherence(pt_table *t, const std::vector<int> &allowed) {
     PT_CUDA(cudaMemcpyAsync(d_seg.p, seg.data(), sizeof(int) * nseg, cudaMemcpyHostToDevice, t->st));
     PT_TRY(pt_gather_rows(t->b_desc.p, t->ds, t->nd, d_trows.p, N, train.p, t->st));
     PT_TRY(pt_gather_rows(t->b_desc.p, t->ds, t->nd, d_qrows.p, Q, qdesc.p, t->st));
-    PT_TRY(pt_kcoherence(t->b_rgba.p, t->w, train.p, N, t->nd, d_tpos.p, qdesc.p, d_qpos.p, d_qcell.p, Q, d_seg.p,
-                         nseg, p.kcoherence, p.kcoherence_min_dist, t->kcoh.p, &t->kc_list, t->st));
+    PT_TRY(pt_kcoherence(t->b_rgba.p, t->w, t->desc_mode ? t->b_desc.p : nullptr, t->ds, t->ew, train.p, N, t->nd,
+                         d_tpos.p, qdesc.p, d_qpos.p, d_qcell.p, Q, d_seg.p, nseg, p.kcoherence, p.kcoherence_min_dist,
+                         t->kcoh.p, &t->kc_list, t->st));
     return PT_OK;
 }
 
@@ -304,22 +310,46 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
     if (!out) return pt_fail(PT_BAD_ARG, "null output pointer");
     *out = nullptr;
     if (!b) return pt_fail(PT_BAD_ARG, "null image");
-    PT_TRY(check_params(pin, h, w));
-    if (channels != 3) return pt_fail(PT_BAD_ARG, "expected a 3-channel RGB image, got %d channels", channels);
+    /* Descriptor mode takes ndims from the input and no chroma (patchtable.h:4398-4401); its
+       patches are the input's pixels, so the build runs on the virtual image around them. */
+    pt_params pd = *pin;
+    int vh = h, vw = w;
+    if (pin->is_descriptor) {
+        if (wh0) return pt_fail(PT_UNSUPPORTED, "a precomputed padded descriptor in descriptor mode");
+        if (channels < 3 || channels > PT_DESC_MAX)
+            return pt_fail(PT_UNSUPPORTED, "descriptor mode with %d channels (3..%d are supported)", channels, PT_DESC_MAX);
+        pd.ndims = channels;
+        pd.nchroma = 0;
+        vh = pin->descriptor_padded ? h - 7 : h + 7;
+        vw = pin->descriptor_padded ? w - 7 : w + 7;
+    } else if (channels != 3) {
+        return pt_fail(PT_BAD_ARG, "expected a 3-channel RGB image, got %d channels", channels);
+    }
+    PT_TRY(check_params(&pd, vh, vw));
     std::unique_ptr<pt_table> t(new pt_table());
-    t->p = *pin;
+    t->p = pd;
     pt_params &p = t->p;
     if (p.grid_ndims < 0) p.grid_ndims = p.ndims;          /* patchtable.h:2603 */
-    t->h = h; t->w = w; t->eh = h - 7; t->ew = w - 7;
+    t->h = vh; t->w = vw; t->eh = vh - 7; t->ew = vw - 7;
     t->nd = p.ndims; t->G = p.grid_ndims;
     t->ds = p.ndims <= 8 ? 8 : 16;
-    PT_TRY(pt_descriptor_check(p.ndims, p.nchroma));
+    t->desc_mode = p.is_descriptor != 0;
+    t->in_padded = p.descriptor_padded;
+    if (!t->desc_mode) PT_TRY(pt_descriptor_check(p.ndims, p.nchroma));
     PT_CUDA(cudaStreamCreateWithFlags(&t->st, cudaStreamNonBlocking));
     t->own_stream = true;
     const long long P = (long long) t->eh * t->ew;
 
+    if (t->desc_mode) {
+        DevBuf<float> in;
+        const size_t nin = (size_t) h * w * channels;
+        PT_CUDA(in.reserve(nin));
+        PT_CUDA(cudaMemcpyAsync(in.p, b, sizeof(float) * nin, cudaMemcpyHostToDevice, t->st));
+        PT_CUDA(t->b_desc.reserve((size_t) P * t->ds));
+        PT_TRY(pt_launch_descriptor_input(in.p, h, w, channels, t->in_padded, t->b_desc.p, t->ds, t->st));
+        PT_CUDA(cudaStreamSynchronize(t->st));
+    } else {
     /* Descriptor of b (get_padded_descriptor, patchtable.h:2492-2546) and the RGBA copy kept as b0. */
-    {
         DevBuf<float> rgb;
         PT_CUDA(rgb.reserve((size_t) h * w * 3));
         PT_CUDA(cudaMemcpyAsync(rgb.p, b, sizeof(float) * (size_t) h * w * 3, cudaMemcpyHostToDevice, t->st));
@@ -424,9 +454,36 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
     return PT_OK;
 }
 
+/* Input dimensions of a query on the virtual image h x w (descriptor mode) and the floats it holds. */
+void query_input_dims(const pt_table *t, int h, int w, int &ih, int &iw, size_t &floats) {
+    if (t->desc_mode) {
+        ih = t->in_padded ? h + 7 : h - 7;
+        iw = t->in_padded ? w + 7 : w - 7;
+        floats = (size_t) ih * iw * t->nd;
+    } else {
+        ih = h; iw = w;
+        floats = (size_t) h * w * 3;
+    }
+}
+
+/* The virtual image of a query input of h x w (pixels or descriptors). */
+pt_status query_dims(const pt_table *t, int h, int w, int &vh, int &vw) {
+    if (t->desc_mode) {
+        vh = t->in_padded ? h - 7 : h + 7;
+        vw = t->in_padded ? w - 7 : w + 7;
+    } else {
+        vh = h; vw = w;
+    }
+    if (vh < 8 || vw < 8) return pt_fail(PT_BAD_ARG, "query %dx%d holds no patch", w, h);
+    return PT_OK;
+}
+
 pt_status ensure_query_buffers(pt_table *t, int h, int w) {
     long long P = (long long) (h - 7) * (w - 7);
-    PT_CUDA(t->q_rgb.reserve((size_t) h * w * 3));
+    int ih, iw;
+    size_t in_floats;
+    query_input_dims(t, h, w, ih, iw, in_floats);
+    PT_CUDA(t->q_rgb.reserve(std::max((size_t) h * w * 3, in_floats)));
     PT_CUDA(t->q_rgba.reserve((size_t) h * w));
     PT_CUDA(t->q_desc.reserve((size_t) P * t->ds));
     PT_CUDA(t->q_tcand.reserve(P));
@@ -471,8 +528,16 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     unsigned long long *ctr = prof ? t->q_counters.p : nullptr;
     if (ctr) PT_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * 6, st));
     PT_TRY(mark(t, prof, -1, st));
-    PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, a_rgb, h, w, p.convert_colorspace, t->q_rgba.p, t->q_desc.p,
-                                t->ds, st));
+    if (t->desc_mode) {
+        if (net) return pt_fail(PT_UNSUPPORTED, "learned proposals in descriptor mode");
+        int ih, iw;
+        size_t nin;
+        query_input_dims(t, h, w, ih, iw, nin);
+        PT_TRY(pt_launch_descriptor_input(a_rgb, ih, iw, t->nd, t->in_padded, t->q_desc.p, t->ds, st));
+    } else {
+        PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, a_rgb, h, w, p.convert_colorspace, t->q_rgba.p, t->q_desc.p,
+                                    t->ds, st));
+    }
     PT_TRY(mark(t, prof, LookupProfile::DESC, st));
     PT_TRY(pt_launch_table_candidates(t->bins, t->q_desc.p, t->ds, P, t->to_bin.p, t->table.p, t->q_tcand.p, st));
     PT_TRY(mark(t, prof, LookupProfile::CELLS, st));
@@ -497,6 +562,12 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     qs.allowed = t->allowed.p;
     qs.allowed_index = p.allowed_index;
     qs.stream = st;
+    if (t->desc_mode) {
+        qs.adesc = t->q_desc.p;
+        qs.bdesc = t->b_desc.p;
+        qs.ds = t->ds;
+        qs.nd = t->nd;
+    }
     if (qs.radius > 2) qs.radius = 2;
     const double temporal_scale = 1.0 / (1 + p.coherence_temporal);          /* patchtable.h:3488 */
     if (d_prev) {
@@ -651,10 +722,11 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
 
 /* lookup_device with stage events; stage_ms[nst] receives summed stage times, counters[nctr] the
    SSD work counters. */
-pt_status profile_impl(pt_table *t, pt_proposal *net, const float *d_a, int h, int w, double *d_ann, cudaStream_t st,
+pt_status profile_impl(pt_table *t, pt_proposal *net, const float *d_a, int ih, int iw, double *d_ann, cudaStream_t st,
                        double *stage_ms, int nst, uint64_t *counters, int nctr) {
     if (!t || !d_a || !d_ann) return pt_fail(PT_BAD_ARG, "null argument");
-    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    int h, w;
+    PT_TRY(query_dims(t, ih, iw, h, w));
     LookupProfile prof;
     PT_TRY(lookup_device(t, d_a, h, w, d_ann, st, &prof, net));
     PT_CUDA(cudaStreamSynchronize(st));
@@ -721,6 +793,7 @@ struct FileIn {
 };
 
 pt_status save_impl(const pt_table *t, const char *filename) {
+    if (t->desc_mode) return pt_fail(PT_UNSUPPORTED, "saving a descriptor mode table");
     const int h = t->h, w = t->w, nd = t->nd;
     std::vector<int> cells((size_t) t->ncells);
     std::vector<float4> rgba((size_t) h * w);
@@ -773,6 +846,7 @@ pt_status save_impl(const pt_table *t, const char *filename) {
 
 pt_status load_impl(const pt_params *pin, const char *filename, pt_table **out) {
     *out = nullptr;
+    if (pin->is_descriptor) return pt_fail(PT_UNSUPPORTED, "loading a descriptor mode table");
     FILE *f = fopen(filename, "rb");
     if (!f) return pt_fail(PT_IO, "cannot open %s", filename);
     struct Closer { FILE *f; ~Closer() { fclose(f); } } closer{f};
@@ -900,13 +974,15 @@ pt_status pt_table_create_with_descriptor(const pt_params *p, const float *b, in
 
 void pt_table_free(pt_table *t) { delete t; }
 
-pt_status pt_table_lookup(pt_table *t, const float *a, int h, int w, double *ann_out, const double *ann_prev,
+pt_status pt_table_lookup(pt_table *t, const float *a, int ih, int iw, double *ann_out, const double *ann_prev,
                           const float *coh_sv, double *seconds) {
     double T0 = now_s();
     if (!t || !a || !ann_out) return pt_fail(PT_BAD_ARG, "null argument");
-    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    int h, w;
+    PT_TRY(query_dims(t, ih, iw, h, w));
     if (coh_sv && !ann_prev) return pt_fail(PT_BAD_ARG, "coherence_temporal_sv without ann_prev");
     long long P = (long long) (h - 7) * (w - 7);
+    const size_t in_floats = (size_t) ih * iw * (t->desc_mode ? t->nd : 3);
     if (ann_prev) {
         PT_TRY(ensure_query_buffers(t, h, w));
         PT_CUDA(t->q_ann.reserve((size_t) P * 3));
@@ -916,7 +992,7 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int h, int w, double *ann
             PT_CUDA(t->q_sv.reserve(P));
             PT_CUDA(cudaMemcpyAsync(t->q_sv.p, coh_sv, sizeof(float) * P, cudaMemcpyHostToDevice, t->st));
         }
-        PT_CUDA(cudaMemcpyAsync(t->q_rgb.p, a, sizeof(float) * (size_t) h * w * 3, cudaMemcpyHostToDevice, t->st));
+        PT_CUDA(cudaMemcpyAsync(t->q_rgb.p, a, sizeof(float) * in_floats, cudaMemcpyHostToDevice, t->st));
         PT_TRY(lookup_device(t, t->q_rgb.p, h, w, t->q_ann.p, t->st, nullptr, nullptr, t->q_prev.p,
                              coh_sv ? t->q_sv.p : nullptr));
         PT_CUDA(cudaMemcpyAsync(ann_out, t->q_ann.p, sizeof(double) * (size_t) P * 3, cudaMemcpyDeviceToHost, t->st));
@@ -927,14 +1003,14 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int h, int w, double *ann
         if (seconds) *seconds = now_s() - T0;
         return PT_OK;
     }
-    if (pt_default_passes(t->p) == 1 && t->p.do_prop && h - 7 >= 64) {
+    if (!t->desc_mode && pt_default_passes(t->p) == 1 && t->p.do_prop && h - 7 >= 64) {
         PT_TRY(lookup_banded(t, a, h, w, ann_out));
         if (seconds) *seconds = now_s() - T0;
         return PT_OK;
     }
     PT_TRY(ensure_query_buffers(t, h, w));
     PT_CUDA(t->q_ann.reserve((size_t) P * 3));
-    PT_CUDA(cudaMemcpyAsync(t->q_rgb.p, a, sizeof(float) * (size_t) h * w * 3, cudaMemcpyHostToDevice, t->st));
+    PT_CUDA(cudaMemcpyAsync(t->q_rgb.p, a, sizeof(float) * in_floats, cudaMemcpyHostToDevice, t->st));
     PT_TRY(lookup_device(t, t->q_rgb.p, h, w, t->q_ann.p, t->st));
     PT_CUDA(cudaMemcpyAsync(ann_out, t->q_ann.p, sizeof(double) * (size_t) P * 3, cudaMemcpyDeviceToHost, t->st));
     PT_CUDA(cudaStreamSynchronize(t->st));
@@ -942,16 +1018,18 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int h, int w, double *ann
     return PT_OK;
 }
 
-pt_status pt_table_lookup_device_temporal(pt_table *t, const float *d_a, int h, int w, const double *d_ann_prev,
+pt_status pt_table_lookup_device_temporal(pt_table *t, const float *d_a, int ih, int iw, const double *d_ann_prev,
                                          const float *d_coh_sv, double *d_ann, void *stream) {
     if (!t || !d_a || !d_ann || !d_ann_prev) return pt_fail(PT_BAD_ARG, "null argument");
-    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    int h, w;
+    PT_TRY(query_dims(t, ih, iw, h, w));
     return lookup_device(t, d_a, h, w, d_ann, (cudaStream_t) stream, nullptr, nullptr, d_ann_prev, d_coh_sv);
 }
 
-pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int h, int w, double *d_ann, void *stream) {
+pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int ih, int iw, double *d_ann, void *stream) {
     if (!t || !d_a || !d_ann) return pt_fail(PT_BAD_ARG, "null argument");
-    if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    int h, w;
+    PT_TRY(query_dims(t, ih, iw, h, w));
     return lookup_device(t, d_a, h, w, d_ann, (cudaStream_t) stream);
 }
 
@@ -1142,6 +1220,9 @@ int64_t pt_kernel_launch_count(void) { return g_launches; }
 
 pt_status pt_table_view(const pt_table *t, PtTableView *v) {
     if (!t || !v) return pt_fail(PT_BAD_ARG, "null argument");
+    if (t->desc_mode)
+        return pt_fail(PT_UNSUPPORTED, "descriptor mode tables serve pt_table_lookup, pt_table_lookup_device(_temporal) "
+                                       "and the profile only");
     v->p = t->p;
     v->h = t->h; v->w = t->w; v->ds = t->ds;
     v->b_rgba = t->b_rgba.p;

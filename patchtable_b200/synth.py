@@ -124,6 +124,22 @@ def pair(h: int, w: int, seed: int):
     return a, b
 
 
+def descriptor_pair(h: int, w: int, channels: int = 8, seed: int = 0):
+    """A pair of h x w x channels descriptor images for descriptor mode (is_descriptor): fixed
+    random linear features of the 3x3 grid of pixels 2 apart around each pixel (edge-replicated)
+    of ``pair(h, w, seed)``, so b's descriptors follow a's under the same warp."""
+    a, b = pair(h, w, seed)
+    rng = _rng(seed + 12345)
+    taps = [(dy, dx) for dy in (-2, 0, 2) for dx in (-2, 0, 2)]
+    proj = (rng.standard_normal((channels, 3 * len(taps))) / np.sqrt(3 * len(taps))).astype(np.float32)
+
+    def feat(img):
+        pad = np.pad(img, ((2, 2), (2, 2), (0, 0)), mode="edge")
+        stack = np.concatenate([pad[2 + dy:2 + dy + h, 2 + dx:2 + dx + w] for dy, dx in taps], axis=2)
+        return np.ascontiguousarray(stack @ proj.T, dtype=np.float32)
+    return feat(a), feat(b)
+
+
 def crop(img: np.ndarray, h: int, w: int, seed: int) -> np.ndarray:
     """Random h x w crop (clamped to the image)."""
     rng = _rng(seed)

@@ -37,6 +37,17 @@ CASES = [
          switches="-limit 2 -ndims 3 -coherence_spatial 4 -dt_algo euclidean"),
 ]
 C2 = dict(name="c2_1920x1080_coh4", h=1080, w=1920, seed=2, switches="-speed 3 -coherence_spatial 4")
+# Descriptor mode (is_descriptor): synth.descriptor_pair inputs.  Three channels are left out: the
+# reference's fourth SSE lane then reads padding that Array::resize leaves uninitialised
+# (solver/array.h:286-287).
+DESC_CASES = [
+    dict(name="desc8_60x80", h=60, w=80, c=8, seed=41, switches="-limit 0.2 -is_descriptor 1"),
+    dict(name="desc6_k4_50x70", h=50, w=70, c=6, seed=42, switches="-limit 0.2 -kcoherence 4 -is_descriptor 1"),
+    dict(name="desc12_g6_45x66", h=45, w=66, c=12, seed=43, switches="-limit 0.3 -grid_ndims 6 -is_descriptor 1"),
+    dict(name="desc7_padded_52x61", h=52, w=61, c=7, seed=44,
+         switches="-limit 0.1 -is_descriptor 1 -descriptor_padded 1 -coherence_spatial 2"),
+    dict(name="desc15_40x48", h=40, w=48, c=15, seed=45, switches="-limit 0.5 -is_descriptor 1"),
+]
 
 
 def digest(arr) -> str:
@@ -68,6 +79,23 @@ def run_case(ref: Reference, case: dict, full: bool = True) -> dict:
     return out
 
 
+def run_desc_case(ref: Reference, case: dict) -> dict:
+    a, b = synth.descriptor_pair(case["h"], case["w"], case["c"], case["seed"])
+    ref.srand(1)
+    t = ref.build(case["switches"], b)
+    ann, _ = t.lookup(a)
+    out = dict(case)
+    out["nslices"] = t.shape()[0]
+    out["table"] = digest(t.table())
+    if t.params["kcoherence"] > 0:
+        kp, kd = t.kcoherence()
+        out["kcoh_pos"] = digest(kp)
+        out["kcoh_dist"] = digest(kd)
+    out["ann"] = digest(ann)
+    out["mean_dist"] = mean_dist(ann)
+    return out
+
+
 def vidpair0(ref: Reference) -> dict:
     from PIL import Image
     base = "/root/reference/patchtable/vidpair0"
@@ -87,6 +115,7 @@ def vidpair0(ref: Reference) -> dict:
 def main():
     ref = Reference()
     res = {"cases": [run_case(ref, c) for c in CASES]}
+    res["desc"] = [run_desc_case(ref, c) for c in DESC_CASES]
     res["c2"] = run_case(ref, C2, full=False)
     res["vidpair0"] = vidpair0(ref)
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle_golden.json")

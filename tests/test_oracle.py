@@ -149,6 +149,58 @@ def test_oracle_descriptor_without_chroma_is_a_prefix(oracle):
         assert np.array_equal(dn, d4[..., :n])
 
 
+@pytest.mark.parametrize("case", GOLDEN["desc"], ids=[c["name"] for c in GOLDEN["desc"]])
+def test_oracle_descriptor_mode_matches_reference_digests(oracle, case):
+    """Descriptor mode (is_descriptor): table, k-coherence set and NNF of the restatement equal
+    the reference's, whose digests the golden file records."""
+    a, b = synth.descriptor_pair(case["h"], case["w"], case["c"], case["seed"])
+    P = ptb.PatchTableParams(case["switches"]).as_dict()
+    oracle.srand(1)
+    t = oracle.build(P, b)
+    assert t.shape()[0] == case["nslices"]
+    assert digest(t.table()) == case["table"]
+    if "kcoh_pos" in case:
+        kp, kd = t.kcoherence()
+        assert digest(kp) == case["kcoh_pos"] and digest(kd) == case["kcoh_dist"]
+    ann = t.lookup(a)
+    assert digest(ann) == case["ann"]
+    assert mean_dist(ann) == case["mean_dist"]
+
+
+def test_oracle_descriptor_three_channels(oracle, reference):
+    """With 3 channels the reference's fourth SSE lane reads the next pixel's first channel, and
+    for the last column that is padding Array::resize leaves uninitialised (solver/array.h:286-287),
+    so only the table -- which never reads it -- is compared; the restatement reads zeros there."""
+    a, b = synth.descriptor_pair(30, 33, 3, 46)
+    s = "-limit 0.05 -kcoherence 2 -is_descriptor 1"
+    P = reference.params(s)
+    reference.srand(1)
+    rt = reference.build(s, b)
+    oracle.srand(1)
+    ot = oracle.build(P, b)
+    assert np.array_equal(rt.table(), ot.table())
+
+
+def test_patch_dist_approx_lane_order(oracle):
+    """patch_dist_approx's lane grouping: blocks of four for 8/12/16 dimensions, lanes then a
+    sequential tail otherwise, and the fourth float taking part with 3 dimensions."""
+    rng = np.random.default_rng(3)
+    for nd in (3, 4, 5, 7, 8, 11, 12, 15, 16):
+        av = rng.random(16, dtype=np.float32)
+        bv = rng.random(16, dtype=np.float32)
+        d = (av - bv) * (av - bv)
+        l = d[:4].copy()
+        if nd in (8, 12, 16):
+            for n in range(1, nd // 4):
+                l = l + d[4 * n:4 * n + 4]
+            want = ((l[0] + l[1]) + l[2]) + l[3]
+        else:
+            want = ((l[0] + l[1]) + l[2]) + l[3]
+            for i in range(4, nd):
+                want = np.float32(want + d[i])
+        assert oracle.patch_dist_approx(av, bv, nd) == np.float32(want), nd
+
+
 def test_vidpair0_known_answer():
     """The reference's own sample pair (patchtable/vidpair0) at -speed 3: the published mean
     distance 0.130757 (patchtable/match_ours_full.txt:4) came from FLANN's approximate k-coherence;
