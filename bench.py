@@ -205,6 +205,7 @@ def profile_case(name):
         t = ptb.PatchTable(p, b)
         if name == "query":
             p.gpu_prop_passes, p.gpu_jump, p.gpu_pull_max = SCHEDULES[0]
+            p.gpu_tile = 64          # the CTA width the timed run's sweep selects on B200
         da = torch.from_numpy(a).cuda()
         dann = torch.empty((H - 7) * (W - 7) * 3, dtype=torch.float64, device="cuda")
         for _ in range(2):

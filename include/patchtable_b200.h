@@ -121,6 +121,12 @@ pt_status pt_table_image_shape(const pt_table *t, int *h, int *w);
 
 void pt_table_free(pt_table *t);
 
+/* With ntables > 1 the table keeps ntables-1 further tables of b, built like the reference's
+   (patchtable.h:3359-3371: limit int(limit / table_ratio^i), no k-coherence) and tried in order in
+   the query's table step (patchtable.h:3711-3735).  *out receives further table i (0-based) as a
+   handle owned by t (do not free it), for inspection with the accessors below. */
+pt_status pt_table_subtable(pt_table *t, int i, pt_table **out);
+
 /* The reference's table keeps a pointer to the caller's PatchTableParams (patchtable.h:1546) and
    lookup() reads the query fields from it on every call (prop_iters, query_step, prop_dist,
    do_prop, do_table_lookup, coherence_spatial/temporal, recalc_dist_temporal, sanitize_input,

@@ -49,6 +49,7 @@ class OrcParams(C.Structure):
         ("recalc_dist_temporal", C.c_int), ("sanitize_input", C.c_int), ("init_random", C.c_int),
         ("convert_colorspace", C.c_int),
         ("is_descriptor", C.c_int), ("descriptor_padded", C.c_int),
+        ("ntables", C.c_int), ("table_ratio", C.c_double),
     ]
 
 
@@ -87,6 +88,8 @@ class Oracle:
         L.orc_descriptor.argtypes = [C.POINTER(OrcParams), _f32p, C.c_int, C.c_int, _f32p]
         L.orc_patch_dist.restype = C.c_float
         L.orc_patch_dist.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f32p, C.c_int, C.c_int, C.c_int]
+        L.orc_subtable.restype = C.c_void_p
+        L.orc_subtable.argtypes = [C.c_void_p, C.c_int]
         L.orc_patch_dist_approx.restype = C.c_float
         L.orc_patch_dist_approx.argtypes = [_f32p, _f32p, C.c_int]
         L.orc_scale_slices.argtypes = [_i32p, C.c_int, C.c_double, _i32p]
@@ -153,8 +156,21 @@ class OracleTable:
     def __init__(self, orc: Oracle, handle, params, bshape):
         self.orc, self.h, self.params = orc, handle, params
         self.bshape = virtual_shape(params, bshape) + (3,)
+        self.owner = None
+
+    def sub_table(self, i: int) -> "OracleTable":
+        """Further table i of an ntables > 1 build (owned by this table)."""
+        h = self.orc.lib.orc_subtable(self.h, i)
+        if not h:
+            raise IndexError(i)
+        sub = OracleTable.__new__(OracleTable)
+        sub.orc, sub.h, sub.params, sub.bshape = self.orc, h, dict(self.params, kcoherence=0), self.bshape
+        sub.owner = self
+        return sub
 
     def __del__(self):
+        if getattr(self, "owner", None) is not None:
+            return
         if getattr(self, "h", None):
             self.orc.lib.orc_free(self.h)
             self.h = None

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <vector>
 #include "knn_exact.h"
 #include "gck_steps.h"
@@ -56,6 +57,8 @@ typedef struct {
     int recalc_dist_temporal, sanitize_input, init_random;
     int convert_colorspace;
     int is_descriptor, descriptor_padded;   /* descriptor mode: b and a are ndims-channel images */
+    int ntables;                            /* further tables at limit / table_ratio^i */
+    double table_ratio;
 } orc_params;
 
 }
@@ -238,6 +241,8 @@ struct Table {
     vector<float> min_val, max_val, range;
     /* Scratch reused across lookups, like lookup_buffer/lookup_wh (patchtable.h:1507-1509). */
     vector<float> lookup_wh;
+    /* ntables > 1: the further tables (tables, patchtable.h:1491) */
+    vector<std::unique_ptr<Table>> subs;
 
     int WW() const { return w + 7; }
     float whv(int y, int x, int i) const { return wh0[((size_t) y * WW() + x) * nd + i]; }
@@ -291,6 +296,7 @@ void dt_euclidean(Table &t);
 /* PatchTableFixedN constructor, patchtable.h:2584-3373, default path (no product quantisation,
    no k-means, populate_nearest with TABLE_POPULATE_FAST, single table). */
 Table *build(const orc_params &p, const float *b, int h, int w, const int32_t *allowed, const float *wh0_in) {
+    const int h_in = h, w_in = w;
     Table *t = new Table();
     t->p = p;
     t->nd = p.ndims;
@@ -436,6 +442,15 @@ Table *build(const orc_params &p, const float *b, int h, int w, const int32_t *a
                     if (t->is_allowed(y - ymin, x - xmin)) { vfill = xy_to_int(x, y); found = true; break; }
         }
         for (auto &v : t->table) if (v == UNUSED) v = vfill;
+    }
+    /* Further tables, patchtable.h:3359-3371: the same b at limit int(limit / table_ratio^i),
+       without k-coherence, each drawing its own populate order from rand() in turn. */
+    for (int i = 1; i < p.ntables; i++) {
+        orc_params pc = p;
+        pc.limit = (double) (int) (pc.limit * (1.0 / pow(p.table_ratio, i)));
+        pc.kcoherence = 0;
+        pc.ntables = 1;
+        t->subs.emplace_back(build(pc, b, h_in, w_in, allowed, nullptr));
     }
     return t;
 }
@@ -809,6 +824,18 @@ double lookup(Table &t, const float *a, int ah, int aw, double *ann, const doubl
                         float dc = dist(x, y, xs, ys);
                         if (dc < dbest) { dbest = dc; xbest = xs; ybest = ys; }
                     }
+                    int xprev = xs, yprev = ys;          /* further tables, patchtable.h:3711-3735 */
+                    for (const auto &u : t.subs) {
+                        int64_t idx1 = 0;
+                        for (int i = 0; i < G; i++) idx1 += (int64_t) u->part[i].get_bin(wh_p[i]) * u->stride[i];
+                        int v1 = u->table[idx1];
+                        int xs1 = int_to_x(v1) - pw1, ys1 = int_to_y(v1) - pw1;
+                        if ((xs1 != xbest || ys1 != ybest) && (xs1 != xprev || ys1 != yprev)) {
+                            float dc = dist(x, y, xs1, ys1);
+                            if (dc < dbest) { dbest = dc; xbest = xs1; ybest = ys1; }
+                        }
+                        xprev = xs1; yprev = ys1;
+                    }
                 }
                 if (do_kcoh) {                            /* patchtable.h:3750-3851 */
                     int ks = p.kcoherence_step;
@@ -991,6 +1018,12 @@ void *orc_build(const orc_params *p, const float *b, int h, int w, const int32_t
 }
 
 void orc_free(void *t) { delete (Table *) t; }
+
+/* Further table i of an ntables > 1 build (owned by t), or NULL. */
+void *orc_subtable(void *tv, int i) {
+    Table *t = (Table *) tv;
+    return i >= 0 && i < (int) t->subs.size() ? t->subs[i].get() : nullptr;
+}
 
 int orc_table_shape(void *tv, int *nslices, long long *ncells) {
     Table *t = (Table *) tv;

@@ -96,6 +96,7 @@ def lib() -> C.CDLL:
     L.pt_table_create.argtypes = [P, _f32p, C.c_int, C.c_int, C.c_int, vp, C.POINTER(vp)]
     L.pt_table_create_with_descriptor.argtypes = [P, _f32p, C.c_int, C.c_int, _f32p, vp, C.POINTER(vp)]
     L.pt_table_free.argtypes = [vp]
+    L.pt_table_subtable.argtypes = [vp, C.c_int, C.POINTER(vp)]
     L.pt_table_save.argtypes = [vp, C.c_char_p]
     L.pt_table_load.argtypes = [P, C.c_char_p, C.POINTER(vp)]
     L.pt_table_image_shape.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
@@ -267,7 +268,24 @@ class PatchTable:
         obj._set_shape()
         return obj
 
+    def sub_table(self, i: int) -> "PatchTable":
+        """Further table i of a multi-table (ntables > 1) build, owned by this table."""
+        h = C.c_void_p()
+        _check(lib().pt_table_subtable(self._h, i, C.byref(h)))
+        obj = PatchTable.__new__(PatchTable)
+        obj.params = PatchTableParams()
+        C.memmove(C.byref(obj.params._p), C.byref(self.params._p), C.sizeof(obj.params._p))
+        obj.params.kcoherence = 0
+        obj._h = h
+        obj._owner = self
+        obj.last_seconds = 0.0
+        obj._set_shape()
+        return obj
+
     def close(self) -> None:
+        if getattr(self, "_owner", None) is not None:      # a further table belongs to its owner
+            self._h = C.c_void_p()
+            return
         if getattr(self, "_h", None) and self._h.value:
             lib().pt_table_free(self._h)
             self._h = C.c_void_p()

@@ -46,6 +46,8 @@ struct QPlan {
     const float4 *adesc;     /* descriptor mode: query descriptor store (ds4 float4 per patch), or NULL */
     const float4 *bdesc;     /* descriptor mode: table descriptor store */
     int ds4, nd;             /* float4 per store entry, descriptor dimensions */
+    const int *tcand_more;   /* further tables' entries, [table][patch] (ntables > 1), or NULL */
+    int ntc;
 };
 
 __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
@@ -283,6 +285,20 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
                 float dc = dist1<TW, DESC>(aq, c_q, b, xs, ys, dbest, rows);
                 ne++;
                 if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
+            }
+            /* Further tables (patchtable.h:3711-3735): each entry is scored unless it equals the
+               best so far or the previous table's entry. */
+            const size_t np = (size_t) c_q.ew * c_q.eh;
+            for (int k = 0; k < c_q.ntc; k++) {
+                const int v1 = c_q.tcand_more[(size_t) k * np + p];
+                const int xs1 = pt_x(v1) - 7, ys1 = pt_y(v1) - 7;
+                if ((xs1 != xb || ys1 != yb) && (xs1 != xs || ys1 != ys)) {
+                    float dc = dist1<TW, DESC>(aq, c_q, b, xs1, ys1, dbest, rows);
+                    ne++;
+                    if (dc < dbest) { dbest = dc; dch = dc; xb = xs1; yb = ys1; }
+                }
+                xs = xs1;
+                ys = ys1;
             }
         }
         const int kc_src = pt_xy(xb, yb);
@@ -624,6 +640,8 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     q.bdesc = reinterpret_cast<const float4 *>(s.bdesc);
     q.ds4 = s.ds / 4;
     q.nd = s.nd;
+    q.tcand_more = s.ntcand_more > 0 ? s.tcand_more : nullptr;
+    q.ntc = q.tcand_more ? s.ntcand_more : 0;
     if (q.adesc) {
         if (!q.bdesc || (s.ds != 8 && s.ds != 16) || q.nd < 3 || q.nd > s.ds)
             return pt_fail(PT_BAD_ARG, "descriptor query: store of %d floats for %d dimensions", s.ds, q.nd);

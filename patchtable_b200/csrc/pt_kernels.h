@@ -73,6 +73,10 @@ struct QuerySetup {
     const float *adesc = nullptr; /* query descriptors, (ah-7) x (aw-7) entries of ds floats, or NULL */
     const float *bdesc = nullptr; /* table descriptors, (bh-7) x (bw-7) entries of ds floats */
     int ds = 8, nd = 0;
+    /* Further tables (ntables > 1, patchtable.h:3711-3738): their entries for every query patch,
+       [table][patch], tried after the first table's in the table step. */
+    const int *tcand_more = nullptr;
+    int ntcand_more = 0;
     cudaStream_t stream;
 };
 /* Query schedule.  By default two choose + pull passes stand in for each of the reference's

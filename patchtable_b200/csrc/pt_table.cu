@@ -103,6 +103,10 @@ struct pt_table {
     int dt_levels = 0;
     DevBuf<int2> kcoh;
     int kc_list = 0;
+    /* ntables > 1: the further tables at limit / table_ratio^i (patchtable.h:3359-3371) and their
+       entries for the current query, [table][patch] */
+    std::vector<std::unique_ptr<pt_table>> subs;
+    DevBuf<int> q_tcand_more;
     /* query scratch, reused across lookups (like lookup_buffer/lookup_wh, patchtable.h:1507-1509) */
     DevBuf<float> q_rgb;
     DevBuf<float4> q_rgba;
@@ -148,7 +152,7 @@ pt_status check_params(const pt_params *p, int h, int w) {
     if (p->incoherence) return pt_fail(PT_UNSUPPORTED, "incoherence is not implemented on the GPU path");
     if (p->randomize_dt) return pt_fail(PT_UNSUPPORTED, "randomize_dt is not implemented on the GPU path");
     if (!p->populate_nearest) return pt_fail(PT_UNSUPPORTED, "populate_nearest 0 is not implemented on the GPU path");
-    if (p->ntables > 1) return pt_fail(PT_UNSUPPORTED, "ntables > 1 is not implemented on the GPU path");
+    if (p->ntables > 16) return pt_fail(PT_UNSUPPORTED, "ntables %d > 16", p->ntables);
     if (p->run_dt && p->dt_algo != 1 && p->dt_algo != 4 && p->dt_algo != 5 && p->dt_algo != 6)
         return pt_fail(PT_UNSUPPORTED, "dt_algo %d is not implemented on the GPU path", p->dt_algo);
     if (p->do_rs || p->spatial) return pt_fail(PT_UNSUPPORTED, "random/spatial search (-do_rs, -spatial) is not implemented on the GPU path");
@@ -540,6 +544,14 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     }
     PT_TRY(mark(t, prof, LookupProfile::DESC, st));
     PT_TRY(pt_launch_table_candidates(t->bins, t->q_desc.p, t->ds, P, t->to_bin.p, t->table.p, t->q_tcand.p, st));
+    if (!t->subs.empty()) {
+        PT_CUDA(t->q_tcand_more.reserve((size_t) P * t->subs.size()));
+        for (size_t i = 0; i < t->subs.size(); i++) {
+            const pt_table *u = t->subs[i].get();
+            PT_TRY(pt_launch_table_candidates(u->bins, t->q_desc.p, t->ds, P, u->to_bin.p, u->table.p,
+                                              t->q_tcand_more.p + i * (size_t) P, st));
+        }
+    }
     PT_TRY(mark(t, prof, LookupProfile::CELLS, st));
     if (net) {
         PtTableView v;
@@ -567,6 +579,10 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
         qs.bdesc = t->b_desc.p;
         qs.ds = t->ds;
         qs.nd = t->nd;
+    }
+    if (!t->subs.empty()) {
+        qs.tcand_more = t->q_tcand_more.p;
+        qs.ntcand_more = (int) t->subs.size();
     }
     if (qs.radius > 2) qs.radius = 2;
     const double temporal_scale = 1.0 / (1 + p.coherence_temporal);          /* patchtable.h:3488 */
@@ -955,6 +971,26 @@ pt_status load_impl(const pt_params *pin, const char *filename, pt_table **out) 
 
 extern "C" {
 
+/* The further tables of ntables > 1 (patchtable.h:3359-3371): each is a full table of b at
+   limit int(limit / table_ratio^i), without k-coherence, built after the first (and after its
+   save, which each further table then repeats with the same file name, as in the reference).
+   A caller-supplied descriptor of b (wh0) serves them too: it is the descriptor they would
+   compute from b. */
+pt_status build_subtables(pt_table *t, const float *b, int h, int w, int channels, const int32_t *allowed,
+                          const float *wh0) {
+    for (int i = 1; i < t->p.ntables; i++) {
+        pt_params pc = t->p;
+        pc.limit = (double) (int) (pc.limit * (1.0 / pow(pc.table_ratio, i)));
+        pc.kcoherence = 0;
+        pc.ntables = 1;
+        pt_table *u = nullptr;
+        if (wh0) PT_TRY(create_impl(&pc, b, h, w, channels, wh0, allowed, &u));
+        else PT_TRY(pt_table_create(&pc, b, h, w, channels, allowed, &u));
+        t->subs.emplace_back(u);
+    }
+    return PT_OK;
+}
+
 pt_status pt_table_create(const pt_params *p, const float *b, int h, int w, int channels, const int32_t *allowed,
                           pt_table **out) {
     if (p && p->load_filename[0]) return load_impl(p, p->load_filename, out);      /* patchtable.h:2591-2594 */
@@ -963,13 +999,25 @@ pt_status pt_table_create(const pt_params *p, const float *b, int h, int w, int 
         pt_status s = save_impl(*out, p->save_filename);
         if (s != PT_OK) { pt_table_free(*out); *out = nullptr; return s; }
     }
-    return PT_OK;
+    pt_status s = build_subtables(*out, b, h, w, channels, allowed, nullptr);
+    if (s != PT_OK) { pt_table_free(*out); *out = nullptr; }
+    return s;
 }
 
 pt_status pt_table_create_with_descriptor(const pt_params *p, const float *b, int h, int w, const float *wh0,
                                           const int32_t *allowed, pt_table **out) {
     if (!wh0) return pt_fail(PT_BAD_ARG, "null descriptor");
-    return create_impl(p, b, h, w, 3, wh0, allowed, out);
+    PT_TRY(create_impl(p, b, h, w, 3, wh0, allowed, out));
+    pt_status s = build_subtables(*out, b, h, w, 3, allowed, wh0);
+    if (s != PT_OK) { pt_table_free(*out); *out = nullptr; }
+    return s;
+}
+
+pt_status pt_table_subtable(pt_table *t, int i, pt_table **out) {
+    if (!t || !out) return pt_fail(PT_BAD_ARG, "null argument");
+    if (i < 0 || i >= (int) t->subs.size()) return pt_fail(PT_BAD_ARG, "table %d of %d further tables", i, (int) t->subs.size());
+    *out = t->subs[i].get();
+    return PT_OK;
 }
 
 void pt_table_free(pt_table *t) { delete t; }
@@ -1003,7 +1051,7 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int ih, int iw, double *a
         if (seconds) *seconds = now_s() - T0;
         return PT_OK;
     }
-    if (!t->desc_mode && pt_default_passes(t->p) == 1 && t->p.do_prop && h - 7 >= 64) {
+    if (!t->desc_mode && t->subs.empty() && pt_default_passes(t->p) == 1 && t->p.do_prop && h - 7 >= 64) {
         PT_TRY(lookup_banded(t, a, h, w, ann_out));
         if (seconds) *seconds = now_s() - T0;
         return PT_OK;
@@ -1220,9 +1268,9 @@ int64_t pt_kernel_launch_count(void) { return g_launches; }
 
 pt_status pt_table_view(const pt_table *t, PtTableView *v) {
     if (!t || !v) return pt_fail(PT_BAD_ARG, "null argument");
-    if (t->desc_mode)
-        return pt_fail(PT_UNSUPPORTED, "descriptor mode tables serve pt_table_lookup, pt_table_lookup_device(_temporal) "
-                                       "and the profile only");
+    if (t->desc_mode || !t->subs.empty())
+        return pt_fail(PT_UNSUPPORTED, "descriptor mode and multi-table tables serve pt_table_lookup, "
+                                       "pt_table_lookup_device(_temporal) and the profile only");
     v->p = t->p;
     v->h = t->h; v->w = t->w; v->ds = t->ds;
     v->b_rgba = t->b_rgba.p;

@@ -127,6 +127,37 @@ def test_other_distance_transforms(gpu, oracle, libc, algo, sw, h, w, seed, mask
     check_nnf(oracle, a, b, ann)
 
 
+@pytest.mark.parametrize("sw", ["-limit 1 -ntables 3 -coherence_spatial 2", "-speed 3 -ntables 4",
+                                "-limit 0.5 -ntables 2 -table_ratio 4 -kcoherence 3"])
+def test_multiple_tables(gpu, oracle, libc, sw):
+    """ntables > 1: every further table equals the oracle's bit for bit (same rand() stream, limit
+    int(limit / table_ratio^i), no k-coherence), and the query tries their entries."""
+    a, b = synth.pair(90, 120, 7)
+    p = ptb.PatchTableParams(sw)
+    srand_all(libc, 1)
+    ot = oracle.build(p.as_dict(), b)
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b, wh0=ot.wh0())
+    assert np.array_equal(gt.table(), ot.table())
+    for i in range(p.ntables - 1):
+        gs, os_ = gt.sub_table(i), ot.sub_table(i)
+        assert gs.shape()[0] == os_.shape()[0]
+        assert np.array_equal(gs.table(), os_.table()), i
+    with pytest.raises(ptb.PatchTableError):
+        gt.sub_table(p.ntables - 1)
+    ann = gt.lookup(a)
+    check_nnf(oracle, a, b, ann)
+    assert mean_dist(ann) <= MEAN_DIST_SLACK * mean_dist(ot.lookup(a))
+    # the table step with more tables is never worse than with the first one alone
+    q = ptb.PatchTableParams(sw + " -do_prop 0 -kcoherence 0 -prop_iters 1")
+    one = ptb.PatchTableParams(sw + " -do_prop 0 -kcoherence 0 -prop_iters 1 -ntables 1")
+    srand_all(libc, 1)
+    tm = ptb.PatchTable(q, b)
+    srand_all(libc, 1)
+    t1 = ptb.PatchTable(one, b)
+    assert (tm.lookup(a)[..., 2] <= t1.lookup(a)[..., 2]).all()
+
+
 def check_nnf(oracle, a, b, ann, sample=4000):
     eh, ew = a.shape[0] - 7, a.shape[1] - 7
     beh, bew = b.shape[0] - 7, b.shape[1] - 7
@@ -212,7 +243,7 @@ def test_constant_image(gpu, libc):
     assert np.allclose(ann[..., 2], 64 * 3 * 0.0625)
 
 
-@pytest.mark.parametrize("sw", ["-do_rs 1", "-spatial 1", "-dt_algo raster", "-ntables 2", "-dim_algo pca"])
+@pytest.mark.parametrize("sw", ["-do_rs 1", "-spatial 1", "-dt_algo raster", "-ntables 17", "-dim_algo pca"])
 def test_unsupported_options_fail_loudly(gpu, sw):
     _, b = synth.pair(40, 40, 1)
     with pytest.raises(ptb.PatchTableError) as e:

@@ -201,6 +201,23 @@ def test_patch_dist_approx_lane_order(oracle):
         assert oracle.patch_dist_approx(av, bv, nd) == np.float32(want), nd
 
 
+@pytest.mark.parametrize("sw", ["-limit 1 -ntables 3", "-speed 3 -ntables 4"])
+def test_oracle_multiple_tables_equal_reference(oracle, reference, sw):
+    """ntables > 1: the NNF depends on every further table, and the restatement's equals the
+    reference's bit for bit."""
+    a, b = synth.pair(90, 120, 7)
+    P = reference.params(sw)
+    reference.srand(3)
+    rt = reference.build(sw, b)
+    oracle.srand(3)
+    ot = oracle.build(P, b)
+    assert np.array_equal(rt.table(), ot.table())
+    reference.srand(9)
+    annr, _ = rt.lookup(a)
+    oracle.srand(9)
+    assert np.array_equal(annr, ot.lookup(a))
+
+
 def test_vidpair0_known_answer():
     """The reference's own sample pair (patchtable/vidpair0) at -speed 3: the published mean
     distance 0.130757 (patchtable/match_ours_full.txt:4) came from FLANN's approximate k-coherence;
