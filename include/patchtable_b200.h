@@ -68,6 +68,9 @@ typedef struct pt_params {
     int gpu_jump;
     int gpu_pull_max;
     int gpu_tile;
+    /* -dim_algo pca (patch_pca.h): random patches fitted, mean subtracted from them, first channel
+       from the patch mean (patchtable.cpp:86-89, 226-228). */
+    int pca_samples, pca_subtract_mean, pca_mean;
 } pt_params;
 
 typedef struct pt_table pt_table;

@@ -50,6 +50,7 @@ class OrcParams(C.Structure):
         ("convert_colorspace", C.c_int),
         ("is_descriptor", C.c_int), ("descriptor_padded", C.c_int),
         ("ntables", C.c_int), ("table_ratio", C.c_double),
+        ("dim_algo", C.c_int), ("pca_samples", C.c_int), ("pca_subtract_mean", C.c_int), ("pca_mean", C.c_int),
     ]
 
 

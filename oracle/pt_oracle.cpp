@@ -59,6 +59,7 @@ typedef struct {
     int is_descriptor, descriptor_padded;   /* descriptor mode: b and a are ndims-channel images */
     int ntables;                            /* further tables at limit / table_ratio^i */
     double table_ratio;
+    int dim_algo, pca_samples, pca_subtract_mean, pca_mean;   /* dim_algo 1: PCA descriptor */
 } orc_params;
 
 }
@@ -221,6 +222,14 @@ void padded_input(const orc_params &p, const float *in, int H, int W, vector<flo
     vh = H + 7; vw = W + 7;
 }
 
+/* -dim_algo pca basis (see pca_fit). */
+const int PCA_D = PW * PW * 3;
+
+struct Pca {
+    vector<float> mean;     /* PCA_D */
+    vector<float> basis;    /* ndims x PCA_D */
+};
+
 struct Table {
     orc_params p;
     int h, w;                   /* b size */
@@ -243,6 +252,8 @@ struct Table {
     vector<float> lookup_wh;
     /* ntables > 1: the further tables (tables, patchtable.h:1491) */
     vector<std::unique_ptr<Table>> subs;
+    /* -dim_algo pca: the basis fitted on b (PatchTableFixedN::pca) */
+    Pca pca;
 
     int WW() const { return w + 7; }
     float whv(int y, int x, int i) const { return wh0[((size_t) y * WW() + x) * nd + i]; }
@@ -258,6 +269,111 @@ void padded_descriptor(const orc_params &p, const float *rgb, int h, int w, vect
     else memcpy(yuv.data(), rgb, sizeof(float) * yuv.size());
     wh.assign((size_t) (h + 7) * (w + 7) * p.ndims, 0.0f);
     gck8(yuv.data(), h, w, p.ndims - p.nchroma * 2, p.nchroma, wh.data());
+}
+
+/* ------------------------------------------------------------------------------------------
+   -dim_algo pca, patch_pca.h.  OpenCV is not available, so cv::PCA(DATA_AS_ROW, maxComponents
+   = ndims) is restated from its published definition: sample mean (zero without
+   pca_subtract_mean), covariance (1/n) sum (x - mean)(x - mean)^T in double, its eigenvectors by
+   cyclic Jacobi rotations, ordered by decreasing eigenvalue and signed so that the entry of
+   largest magnitude is positive.  Parity with the reference is unpinned here (its OpenCV is
+   absent); the restatement pins the GPU path's fit and projection.
+   ------------------------------------------------------------------------------------------ */
+/* extract_patches + get_patch_pca, patch_pca.h:14-52, on the colour-converted image. */
+void pca_fit(const orc_params &p, const float *img, int h, int w, Pca &out) {
+    const int n = p.pca_samples, aew = w - PW + 1, aeh = h - PW + 1;
+    vector<double> X((size_t) n * PCA_D);
+    for (int i = 0; i < n; i++) {
+        int ax = rand() % aew;
+        int ay = rand() % aeh;
+        int k = 0;
+        for (int dy = 0; dy < PW; dy++)
+            for (int dx = 0; dx < PW; dx++)
+                for (int c = 0; c < 3; c++) X[(size_t) i * PCA_D + k++] = img[((size_t) (ay + dy) * w + ax + dx) * 3 + c];
+    }
+    vector<double> mu(PCA_D, 0.0);
+    if (p.pca_subtract_mean) {
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < PCA_D; j++) mu[j] += X[(size_t) i * PCA_D + j];
+        for (int j = 0; j < PCA_D; j++) mu[j] /= n;
+    }
+    vector<double> A((size_t) PCA_D * PCA_D, 0.0);
+    for (int i = 0; i < n; i++)
+        for (int a = 0; a < PCA_D; a++) {
+            double da = X[(size_t) i * PCA_D + a] - mu[a];
+            for (int b = a; b < PCA_D; b++) A[(size_t) a * PCA_D + b] += da * (X[(size_t) i * PCA_D + b] - mu[b]);
+        }
+    for (int a = 0; a < PCA_D; a++)
+        for (int b = a; b < PCA_D; b++) { A[(size_t) a * PCA_D + b] /= n; A[(size_t) b * PCA_D + a] = A[(size_t) a * PCA_D + b]; }
+    /* cyclic Jacobi */
+    vector<double> V((size_t) PCA_D * PCA_D, 0.0);
+    for (int i = 0; i < PCA_D; i++) V[(size_t) i * PCA_D + i] = 1.0;
+    for (int sweep = 0; sweep < 100; sweep++) {
+        double off = 0.0, on = 0.0;
+        for (int i = 0; i < PCA_D; i++)
+            for (int j = 0; j < PCA_D; j++) {
+                double v = A[(size_t) i * PCA_D + j];
+                if (i == j) on += v * v; else off += v * v;
+            }
+        if (off == 0.0 || off <= 1e-30 * on) break;
+        for (int r = 0; r < PCA_D - 1; r++)
+            for (int q = r + 1; q < PCA_D; q++) {
+                double arq = A[(size_t) r * PCA_D + q];
+                if (arq == 0.0) continue;
+                double theta = (A[(size_t) q * PCA_D + q] - A[(size_t) r * PCA_D + r]) / (2.0 * arq);
+                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+                for (int k = 0; k < PCA_D; k++) {
+                    double x = A[(size_t) k * PCA_D + r], y = A[(size_t) k * PCA_D + q];
+                    A[(size_t) k * PCA_D + r] = c * x - sn * y;
+                    A[(size_t) k * PCA_D + q] = sn * x + c * y;
+                }
+                for (int k = 0; k < PCA_D; k++) {
+                    double x = A[(size_t) r * PCA_D + k], y = A[(size_t) q * PCA_D + k];
+                    A[(size_t) r * PCA_D + k] = c * x - sn * y;
+                    A[(size_t) q * PCA_D + k] = sn * x + c * y;
+                }
+                for (int k = 0; k < PCA_D; k++) {
+                    double x = V[(size_t) k * PCA_D + r], y = V[(size_t) k * PCA_D + q];
+                    V[(size_t) k * PCA_D + r] = c * x - sn * y;
+                    V[(size_t) k * PCA_D + q] = sn * x + c * y;
+                }
+            }
+    }
+    vector<int> ord(PCA_D);
+    for (int i = 0; i < PCA_D; i++) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return A[(size_t) x * PCA_D + x] > A[(size_t) y * PCA_D + y]; });
+    out.mean.resize(PCA_D);
+    for (int j = 0; j < PCA_D; j++) out.mean[j] = (float) mu[j];
+    out.basis.assign((size_t) p.ndims * PCA_D, 0.0f);
+    for (int k = 0; k < p.ndims; k++) {
+        int col = ord[k], big = 0;
+        for (int j = 1; j < PCA_D; j++)
+            if (fabs(V[(size_t) j * PCA_D + col]) > fabs(V[(size_t) big * PCA_D + col])) big = j;
+        double sg = V[(size_t) big * PCA_D + col] < 0 ? -1.0 : 1.0;
+        for (int j = 0; j < PCA_D; j++) out.basis[(size_t) k * PCA_D + j] = (float) (sg * V[(size_t) j * PCA_D + col]);
+    }
+}
+
+/* apply_patch_pca, patch_pca.h:54-110 (pca_mean off): channel k of the patch at (x, y) goes to
+   wh(y+7, x+7, k); the projection sums (v_j - mean_j) * basis_kj in j order, in float. */
+void pca_apply(const orc_params &p, const Pca &pca, const float *img, int h, int w, vector<float> &wh) {
+    const int nd = p.ndims, WW = w + PW - 1;
+    wh.assign((size_t) (h + PW - 1) * WW * nd, 0.0f);
+    vector<float> v(PCA_D);
+    for (int ay = 0; ay + PW <= h; ay++)
+        for (int ax = 0; ax + PW <= w; ax++) {
+            int k = 0;
+            for (int dy = 0; dy < PW; dy++)
+                for (int dx = 0; dx < PW; dx++)
+                    for (int c = 0; c < 3; c++) v[k++] = img[((size_t) (ay + dy) * w + ax + dx) * 3 + c];
+            float *o = &wh[((size_t) (ay + PW - 1) * WW + ax + PW - 1) * nd];
+            for (int ch = 0; ch < nd; ch++) {
+                float acc = 0.0f;
+                for (int j = 0; j < PCA_D; j++) acc = acc + (v[j] - pca.mean[j]) * pca.basis[(size_t) ch * PCA_D + j];
+                o[ch] = acc;
+            }
+        }
 }
 
 /* scale_slices_to_limit, patchtable.cpp:611-642 (product and multiply: solver/util.cpp:186-205). */
@@ -309,8 +425,16 @@ Table *build(const orc_params &p, const float *b, int h, int w, const int32_t *a
         h = vh; w = vw;
     } else {
         t->b0.assign(b, b + (size_t) h * w * 3);
+        if (p.dim_algo == 1) {                           /* reduce_dim, patchtable.h:1709-1713 */
+            vector<float> img((size_t) h * w * 3);
+            if (p.convert_colorspace) rgb2yuv(b, h * w, img.data());
+            else memcpy(img.data(), b, sizeof(float) * img.size());
+            pca_fit(p, img.data(), h, w, t->pca);
+            if (!wh0_in) pca_apply(p, t->pca, img.data(), h, w, t->wh0);
+        } else if (!wh0_in) {
+            padded_descriptor(p, b, h, w, t->wh0);
+        }
         if (wh0_in) t->wh0.assign(wh0_in, wh0_in + (size_t) (h + 7) * (w + 7) * p.ndims);
-        else padded_descriptor(p, b, h, w, t->wh0);
     }
     t->h = h; t->w = w;
     if (allowed) t->allowed.assign(allowed, allowed + (size_t) (h - 7) * (w - 7));
@@ -742,8 +866,16 @@ double lookup(Table &t, const float *a, int ah, int aw, double *ann, const doubl
     const orc_params &p = t.p;
     vector<float> &a_wh = t.lookup_wh;
     const bool desc = p.is_descriptor;
-    if (desc) padded_input(p, a, ah, aw, a_wh, ah, aw);
-    else padded_descriptor(p, a, ah, aw, a_wh);
+    if (desc) {
+        padded_input(p, a, ah, aw, a_wh, ah, aw);
+    } else if (p.dim_algo == 1) {
+        vector<float> img((size_t) ah * aw * 3);
+        if (p.convert_colorspace) rgb2yuv(a, ah * aw, img.data());
+        else memcpy(img.data(), a, sizeof(float) * img.size());
+        pca_apply(p, t.pca, img.data(), ah, aw, a_wh);
+    } else {
+        padded_descriptor(p, a, ah, aw, a_wh);
+    }
     const int nd = t.nd, G = t.gnd;
     const int awhw = aw + 7;
     double prop_scale = 1.0 / (1 + p.coherence_spatial);

@@ -113,6 +113,7 @@ int ptref_params_get(void *pv, const char *name, double *out) {
     F(is_descriptor) F(descriptor_padded) F(allowed_index) F(recalc_dist_temporal) F(sanitize_input) F(init_random)
     F(dim_algo) F(colorspace) F(convert_colorspace) F(flann_checks) F(flann_eps) F(table_ratio)
     F(verbose) F(randomize_dt) F(incoherence) F(lookup_algo) F(kcoherence_algo)
+    F(pca_samples) F(pca_subtract_mean) F(pca_mean)
 #undef F
     return -1;
 }

@@ -69,6 +69,7 @@ class _Params(C.Structure):
         ("gpu_jump", C.c_int),
         ("gpu_pull_max", C.c_int),
         ("gpu_tile", C.c_int),
+        ("pca_samples", C.c_int), ("pca_subtract_mean", C.c_int), ("pca_mean", C.c_int),
     ]
 
 

@@ -47,16 +47,13 @@ __device__ __forceinline__ void yuv_exact(float R, float G, float B, float &Y, f
 }
 
 
-/* One 64 x 8 block of patches with top-left patch (x0, y0). */
-__device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, const float *__restrict__ rgb, int h, int w,
-                                          int convert, float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh,
-                                          int ew, int x0, int y0) {
-    float *pix = smem;                               /* 3 planes x RH x RWP */
-    float *hs = smem + 3 * RH * RWP;                 /* ncombo x RH x TW */
+/* The colour-converted pixels under a 64 x 8 block of patches with top-left patch (x0, y0), as
+   3 planes of RH x RWP floats; the block also writes the RGBA copy of the pixels it owns. */
+__device__ __forceinline__ void stage_pix(float *pix, const float *__restrict__ rgb, int h, int w, int convert,
+                                          float4 *__restrict__ rgba, int eh, int ew, int x0, int y0) {
     const int tid = threadIdx.x;
     const bool last_col = x0 + TW >= ew, last_row = y0 + TH >= eh;
     const int own_x1 = last_col ? w : x0 + TW, own_y1 = last_row ? h : y0 + TH;
-
     for (int i = tid; i < RH * RW; i += NT) {
         int r = i / RW, c = i % RW;
         int gy = y0 + r, gx = x0 + c;
@@ -72,6 +69,16 @@ __device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, c
         pix[(1 * RH + r) * RWP + c] = U;
         pix[(2 * RH + r) * RWP + c] = V;
     }
+}
+
+/* One 64 x 8 block of patches with top-left patch (x0, y0). */
+__device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, const float *__restrict__ rgb, int h, int w,
+                                          int convert, float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh,
+                                          int ew, int x0, int y0) {
+    float *pix = smem;                               /* 3 planes x RH x RWP */
+    float *hs = smem + 3 * RH * RWP;                 /* ncombo x RH x TW */
+    const int tid = threadIdx.x;
+    stage_pix(pix, rgb, h, w, convert, rgba, eh, ew, x0, y0);
     __syncthreads();
 
     const int ncombo = c_plan.ncombo;
@@ -133,6 +140,53 @@ k_descriptor_batch(const DescPlan c_plan, const PtBatchImage *__restrict__ imgs,
         desc_tile(c_plan, smem, rgb + 3 * g.pix_off, g.h, g.w, convert, rgba ? rgba + g.pix_off : nullptr,
                   desc + g.patch_off * ds, ds, g.eh, g.ew, (int) (lt % tpr) * TW, (int) (lt / tpr) * TH);
         __syncthreads();                                 /* the next tile reuses the shared memory */
+    }
+}
+
+/* -dim_algo pca projection (apply_patch_pca, patch_pca.h:60-110): descriptor channel k of a
+   patch = sum over the patch's 192 values v_j (row, column, channel order) of (v_j - mean_j) *
+   basis[k][j], accumulated in j order with separately rounded products and sums.  Each thread
+   projects two patches of the block (rows pi and pi + 4) so that every basis load serves both;
+   all lanes read the same basis word, a broadcast. */
+__global__ void __launch_bounds__(NT)
+k_pca(const float *__restrict__ rgb, int h, int w, int convert, float4 *__restrict__ rgba,
+      const float *__restrict__ mean, const float *__restrict__ basis, int ncomp, float *__restrict__ desc, int ds,
+      int eh, int ew) {
+    __shared__ float pix[3 * RH * RWP];
+    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+    stage_pix(pix, rgb, h, w, convert, rgba, eh, ew, x0, y0);
+    __syncthreads();
+    const int pj = threadIdx.x % TW, pi = threadIdx.x / TW;        /* pi in 0..3 */
+    float acc[2][PT_DESC_MAX];
+#pragma unroll
+    for (int k = 0; k < PT_DESC_MAX; k++) acc[0][k] = acc[1][k] = 0.f;
+#pragma unroll 1
+    for (int dy = 0; dy < 8; dy++)
+#pragma unroll 1
+        for (int dx = 0; dx < 8; dx++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const int j = (dy * 8 + dx) * 3 + c;
+                const float mj = __ldg(mean + j);
+                const float d0 = __fsub_rn(pix[(c * RH + pi + dy) * RWP + pj + dx], mj);
+                const float d1 = __fsub_rn(pix[(c * RH + pi + 4 + dy) * RWP + pj + dx], mj);
+#pragma unroll
+                for (int k = 0; k < PT_DESC_MAX; k++) {
+                    if (k < ncomp) {
+                        const float bk = __ldg(basis + k * PT_PCA_DIM + j);
+                        acc[0][k] = __fadd_rn(acc[0][k], __fmul_rn(d0, bk));
+                        acc[1][k] = __fadd_rn(acc[1][k], __fmul_rn(d1, bk));
+                    }
+                }
+            }
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+        const int py = y0 + pi + 4 * u, px = x0 + pj;
+        if (py >= eh || px >= ew) continue;
+        float *o = desc + ((size_t) py * ew + px) * ds;
+#pragma unroll
+        for (int k = 0; k < PT_DESC_MAX; k++)
+            if (k < ds) o[k] = k < ncomp ? acc[u][k] : 0.f;
     }
 }
 
@@ -263,6 +317,17 @@ pt_status pt_launch_descriptor_input(const float *in, int H, int W, int nd, int 
     if (nd < 3 || nd > ds || ds > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "descriptor dimensions %d outside 3..%d", nd, PT_DESC_MAX);
     const long long P = (long long) ew * eh;
     k_desc_input<<<(unsigned) ((P + NT - 1) / NT), NT, 0, st>>>(in, H, W, nd, padded, ew, eh, desc, ds);
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_pca(const float *rgb, int h, int w, int convert, float4 *rgba, const float *mean, const float *basis,
+                        int ncomp, float *desc, int ds, cudaStream_t st) {
+    const int ew = w - 7, eh = h - 7;
+    if (ew < 1 || eh < 1) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    if (ncomp < 1 || ncomp > ds || ds > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "PCA with %d components", ncomp);
+    dim3 grid((ew + TW - 1) / TW, (eh + TH - 1) / TH);
+    k_pca<<<grid, NT, 0, st>>>(rgb, h, w, convert, rgba, mean, basis, ncomp, desc, ds, eh, ew);
     PT_LAUNCHED();
     return PT_OK;
 }

@@ -14,6 +14,14 @@ pt_status pt_launch_descriptor(int ndims, int nchroma, const float *rgb, int h, 
 /* Rows [trow0, trow0 + trows) of 8-patch descriptor tiles only (for banded lookups). */
 pt_status pt_launch_descriptor_rows(int ndims, int nchroma, const float *rgb, int h, int w, int convert, float4 *rgba,
                                     float *desc, int ds, int trow0, int trows, cudaStream_t st);
+/* -dim_algo pca: the basis fit on the host (pt_pca.cpp: mean[PT_PCA_DIM], basis[ncomp][PT_PCA_DIM],
+   consuming 2 x samples rand() values like the reference) and the projection of every patch of an
+   RGB image (k_descriptor.cu), which also writes the RGBA copy when rgba is set. */
+#define PT_PCA_DIM 192
+pt_status pt_pca_fit(const float *rgb, int h, int w, int convert, int samples, int subtract_mean, int ncomp,
+                     std::vector<float> &mean, std::vector<float> &basis);
+pt_status pt_launch_pca(const float *rgb, int h, int w, int convert, float4 *rgba, const float *mean, const float *basis,
+                        int ncomp, float *desc, int ds, cudaStream_t st);
 /* Descriptor mode: the store entries (ds floats per patch) of an H x W x nd descriptor image,
    padded (descriptor_padded: patches (H-14) x (W-14)) or not (patches H x W). */
 pt_status pt_launch_descriptor_input(const float *in, int H, int W, int nd, int padded, float *desc, int ds,

@@ -139,6 +139,7 @@ pt_status apply_switches(pt_params *p, const std::vector<std::string> &argv) {
     INT_SW(grid_ndims) DBL_SW(table_ratio) INT_SW(prop_dist)
     BOOL_SW(is_descriptor) BOOL_SW(descriptor_padded)
     INT_SW(gpu_prop_passes) INT_SW(gpu_jump) INT_SW(gpu_pull_max) INT_SW(gpu_tile)
+    INT_SW(pca_samples) BOOL_SW(pca_mean) BOOL_SW(pca_subtract_mean)
 #undef INT_SW
 #undef BOOL_SW
 #undef DBL_SW
@@ -198,6 +199,9 @@ void pt_params_default(pt_params *p) {
     p->prop_dist = 0;
     p->incoherence = 0;
     p->triangle_factor = 2.0;
+    p->pca_samples = 1000;
+    p->pca_mean = 0;
+    p->pca_subtract_mean = 1;
     p->sanitize_input = 1;
     p->do_table_lookup = 1;
     p->gpu_prop_passes = 0;

@@ -1,0 +1,129 @@
+/* -dim_algo pca: the patch basis of the table image (get_patch_pca, patchtable/patch_pca.h:45-52).
+
+   The reference samples pca_samples patches at (rand() % (w-7), rand() % (h-7)) of the colour-
+   converted image (extract_patches, patch_pca.h:14-43), each a 192-vector ordered (row, column,
+   channel), and hands them to cv::PCA with DATA_AS_ROW and maxComponents = ndims: the sample mean
+   (or zero when pca_subtract_mean is off) and the leading eigenvectors of the covariance
+   (1/n) sum (x - mean)(x - mean)^T.  OpenCV is not part of this build, so the decomposition is
+   the published cyclic Jacobi method, in double precision; eigenvectors are ordered by
+   decreasing eigenvalue and signed so that their largest-magnitude entry is positive (OpenCV
+   leaves the sign to its solver).  The fit runs on the host: a thousand samples and a 192 x 192
+   matrix; the projection of every patch runs on the GPU (k_descriptor.cu). */
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <numeric>
+#include <vector>
+
+#include "pt_internal.h"
+#include "pt_kernels.h"
+
+namespace {
+
+/* ARRAY_RGB2YUV (solver/array.h:1124-1126) in double, as the GPU descriptor kernels compute it. */
+inline void yuv_host(float R, float G, float B, float &Y, float &U, float &V) {
+    const double r = R, g = G, b = B;
+    Y = (float) ((0.299 * r + 0.587 * g) + 0.114 * b);
+    U = (float) ((-0.14713 * r + -0.28886 * g) + 0.436 * b);
+    V = (float) ((0.615 * r + -0.51499 * g) + -0.10001 * b);
+}
+
+/* Eigen-decomposition of the symmetric n x n matrix a (row-major, destroyed) by cyclic Jacobi
+   rotations; vals[k] and column k of vecs (row-major n x n) are the pairs. */
+void jacobi_eigen(std::vector<double> &a, int n, std::vector<double> &vals, std::vector<double> &vecs) {
+    vecs.assign((size_t) n * n, 0.0);
+    for (int i = 0; i < n; i++) vecs[(size_t) i * n + i] = 1.0;
+    auto A = [&](int i, int j) -> double & { return a[(size_t) i * n + j]; };
+    for (int sweep = 0; sweep < 100; sweep++) {
+        double off = 0.0, diag = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) (i == j ? diag : off) += A(i, j) * A(i, j);
+        if (off <= 1e-30 * diag || off == 0.0) break;
+        for (int p = 0; p < n - 1; p++)
+            for (int q = p + 1; q < n; q++) {
+                const double apq = A(p, q);
+                if (apq == 0.0) continue;
+                const double theta = (A(q, q) - A(p, p)) / (2.0 * apq);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < n; k++) {           /* columns p, q */
+                    const double akp = A(k, p), akq = A(k, q);
+                    A(k, p) = c * akp - s * akq;
+                    A(k, q) = s * akp + c * akq;
+                }
+                for (int k = 0; k < n; k++) {           /* rows p, q */
+                    const double apk = A(p, k), aqk = A(q, k);
+                    A(p, k) = c * apk - s * aqk;
+                    A(q, k) = s * apk + c * aqk;
+                }
+                for (int k = 0; k < n; k++) {
+                    double &vkp = vecs[(size_t) k * n + p], &vkq = vecs[(size_t) k * n + q];
+                    const double x = vkp, y = vkq;
+                    vkp = c * x - s * y;
+                    vkq = s * x + c * y;
+                }
+            }
+    }
+    vals.resize(n);
+    for (int i = 0; i < n; i++) vals[i] = A(i, i);
+}
+
+}  // namespace
+
+pt_status pt_pca_fit(const float *rgb, int h, int w, int convert, int samples, int subtract_mean, int ncomp,
+                     std::vector<float> &mean_out, std::vector<float> &basis_out) {
+    constexpr int D = PT_PCA_DIM;
+    if (samples < 1) return pt_fail(PT_BAD_ARG, "pca_samples must be >= 1");
+    if (ncomp < 1 || ncomp > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "PCA with %d components", ncomp);
+    const int aew = w - 7, aeh = h - 7;
+    std::vector<double> X((size_t) samples * D);
+    for (int i = 0; i < samples; i++) {
+        const int ax = rand() % aew;                   /* extract_patches, patch_pca.h:25-26 */
+        const int ay = rand() % aeh;
+        double *row = &X[(size_t) i * D];
+        int k = 0;
+        for (int dy = 0; dy < 8; dy++)
+            for (int dx = 0; dx < 8; dx++) {
+                const float *px = rgb + ((size_t) (ay + dy) * w + ax + dx) * 3;
+                float c0 = px[0], c1 = px[1], c2 = px[2];
+                if (convert) yuv_host(px[0], px[1], px[2], c0, c1, c2);
+                row[k++] = c0; row[k++] = c1; row[k++] = c2;
+            }
+    }
+    std::vector<double> mean(D, 0.0);
+    if (subtract_mean) {
+        for (int i = 0; i < samples; i++)
+            for (int j = 0; j < D; j++) mean[j] += X[(size_t) i * D + j];
+        for (int j = 0; j < D; j++) mean[j] /= samples;
+    }
+    std::vector<double> C((size_t) D * D, 0.0);
+    for (int i = 0; i < samples; i++) {
+        const double *row = &X[(size_t) i * D];
+        double d[D];
+        for (int j = 0; j < D; j++) d[j] = row[j] - mean[j];
+        for (int a = 0; a < D; a++)
+            for (int b = a; b < D; b++) C[(size_t) a * D + b] += d[a] * d[b];
+    }
+    for (int a = 0; a < D; a++)
+        for (int b = a; b < D; b++) {
+            C[(size_t) a * D + b] /= samples;
+            C[(size_t) b * D + a] = C[(size_t) a * D + b];
+        }
+    std::vector<double> vals, vecs;
+    jacobi_eigen(C, D, vals, vecs);
+    std::vector<int> order(D);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return vals[x] > vals[y]; });
+    mean_out.resize(D);
+    for (int j = 0; j < D; j++) mean_out[j] = (float) mean[j];
+    basis_out.assign((size_t) ncomp * D, 0.0f);
+    for (int k = 0; k < ncomp; k++) {
+        const int col = order[k];
+        int big = 0;
+        for (int j = 1; j < D; j++)
+            if (std::fabs(vecs[(size_t) j * D + col]) > std::fabs(vecs[(size_t) big * D + col])) big = j;
+        const double sgn = vecs[(size_t) big * D + col] < 0 ? -1.0 : 1.0;
+        for (int j = 0; j < D; j++) basis_out[(size_t) k * D + j] = (float) (sgn * vecs[(size_t) j * D + col]);
+    }
+    return PT_OK;
+}

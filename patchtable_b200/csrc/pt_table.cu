@@ -83,6 +83,9 @@ struct pt_table {
        patchtable.h:2498-2507); no RGB copy of b exists. */
     bool desc_mode = false;
     int in_padded = 0;
+    /* -dim_algo pca: the basis fitted on b (patch_pca.h), used for b and every query */
+    bool pca = false;
+    DevBuf<float> pca_mean, pca_basis;
     cudaStream_t st = nullptr;
     bool own_stream = false;
     DevBuf<float4> b_rgba;
@@ -144,7 +147,10 @@ pt_status check_params(const pt_params *p, int h, int w) {
     if (p->patch_w != 8) return pt_fail(PT_UNSUPPORTED, "patch_w=%d: only 8x8 patches are supported (gck.h)", p->patch_w);
     if (h < 8 || w < 8) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
     if (w > 65535 || h > 16383) return pt_fail(PT_BAD_ARG, "image %dx%d exceeds the packed position range (XY_TO_INT)", w, h);
-    if (p->dim_algo != 0) return pt_fail(PT_UNSUPPORTED, "dim_algo pca is not implemented on the GPU path");
+    if (p->dim_algo == 1 && (p->is_descriptor || p->pca_mean))
+        return pt_fail(PT_UNSUPPORTED, "dim_algo pca with %s is not implemented on the GPU path",
+                       p->is_descriptor ? "is_descriptor" : "pca_mean");
+    if (p->dim_algo != 0 && p->dim_algo != 1) return pt_fail(PT_BAD_ARG, "dim_algo %d", p->dim_algo);
     if (!p->is_descriptor && p->convert_colorspace && p->colorspace != 0)
         return pt_fail(PT_UNSUPPORTED, "colorspace lab is not implemented on the GPU path");
     if (p->lookup_algo != 0) return pt_fail(PT_UNSUPPORTED, "only lookup_algo table is implemented on the GPU path");
@@ -339,7 +345,7 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
     t->ds = p.ndims <= 8 ? 8 : 16;
     t->desc_mode = p.is_descriptor != 0;
     t->in_padded = p.descriptor_padded;
-    if (!t->desc_mode) PT_TRY(pt_descriptor_check(p.ndims, p.nchroma));
+    if (!t->desc_mode && p.dim_algo == 0) PT_TRY(pt_descriptor_check(p.ndims, p.nchroma));
     PT_CUDA(cudaStreamCreateWithFlags(&t->st, cudaStreamNonBlocking));
     t->own_stream = true;
     const long long P = (long long) t->eh * t->ew;
@@ -359,8 +365,22 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
         PT_CUDA(cudaMemcpyAsync(rgb.p, b, sizeof(float) * (size_t) h * w * 3, cudaMemcpyHostToDevice, t->st));
         PT_CUDA(t->b_rgba.reserve((size_t) h * w));
         PT_CUDA(t->b_desc.reserve((size_t) P * t->ds));
-        PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, rgb.p, h, w, p.convert_colorspace, t->b_rgba.p, t->b_desc.p,
-                                    t->ds, t->st));
+        if (p.dim_algo == 1) {
+            /* reduce_dim with TABLE_DIM_ALGO_PCA (patchtable.h:1709-1713): fit on b, then project */
+            std::vector<float> mean, basis;
+            PT_TRY(pt_pca_fit(b, h, w, p.convert_colorspace, p.pca_samples, p.pca_subtract_mean, p.ndims, mean, basis));
+            t->pca = true;
+            PT_CUDA(t->pca_mean.reserve(mean.size()));
+            PT_CUDA(t->pca_basis.reserve(basis.size()));
+            PT_CUDA(cudaMemcpyAsync(t->pca_mean.p, mean.data(), sizeof(float) * mean.size(), cudaMemcpyHostToDevice, t->st));
+            PT_CUDA(cudaMemcpyAsync(t->pca_basis.p, basis.data(), sizeof(float) * basis.size(), cudaMemcpyHostToDevice, t->st));
+            PT_TRY(pt_launch_pca(rgb.p, h, w, p.convert_colorspace, t->b_rgba.p, t->pca_mean.p, t->pca_basis.p, p.ndims,
+                                 t->b_desc.p, t->ds, t->st));
+            PT_CUDA(cudaStreamSynchronize(t->st));     /* the host vectors go out of scope */
+        } else {
+            PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, rgb.p, h, w, p.convert_colorspace, t->b_rgba.p, t->b_desc.p,
+                                        t->ds, t->st));
+        }
         if (wh0) {
             /* Caller-supplied padded descriptor (wh0_no_copy): interior patches only. */
             std::vector<float> packed((size_t) P * t->ds, 0.0f);
@@ -538,6 +558,9 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
         size_t nin;
         query_input_dims(t, h, w, ih, iw, nin);
         PT_TRY(pt_launch_descriptor_input(a_rgb, ih, iw, t->nd, t->in_padded, t->q_desc.p, t->ds, st));
+    } else if (t->pca) {
+        PT_TRY(pt_launch_pca(a_rgb, h, w, p.convert_colorspace, t->q_rgba.p, t->pca_mean.p, t->pca_basis.p, t->nd,
+                             t->q_desc.p, t->ds, st));
     } else {
         PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, a_rgb, h, w, p.convert_colorspace, t->q_rgba.p, t->q_desc.p,
                                     t->ds, st));
@@ -809,7 +832,7 @@ struct FileIn {
 };
 
 pt_status save_impl(const pt_table *t, const char *filename) {
-    if (t->desc_mode) return pt_fail(PT_UNSUPPORTED, "saving a descriptor mode table");
+    if (t->desc_mode || t->pca) return pt_fail(PT_UNSUPPORTED, "saving a descriptor mode or PCA table");
     const int h = t->h, w = t->w, nd = t->nd;
     std::vector<int> cells((size_t) t->ncells);
     std::vector<float4> rgba((size_t) h * w);
@@ -862,7 +885,7 @@ pt_status save_impl(const pt_table *t, const char *filename) {
 
 pt_status load_impl(const pt_params *pin, const char *filename, pt_table **out) {
     *out = nullptr;
-    if (pin->is_descriptor) return pt_fail(PT_UNSUPPORTED, "loading a descriptor mode table");
+    if (pin->is_descriptor || pin->dim_algo != 0) return pt_fail(PT_UNSUPPORTED, "loading a descriptor mode or PCA table");
     FILE *f = fopen(filename, "rb");
     if (!f) return pt_fail(PT_IO, "cannot open %s", filename);
     struct Closer { FILE *f; ~Closer() { fclose(f); } } closer{f};
@@ -1051,7 +1074,7 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int ih, int iw, double *a
         if (seconds) *seconds = now_s() - T0;
         return PT_OK;
     }
-    if (!t->desc_mode && t->subs.empty() && pt_default_passes(t->p) == 1 && t->p.do_prop && h - 7 >= 64) {
+    if (!t->desc_mode && !t->pca && t->subs.empty() && pt_default_passes(t->p) == 1 && t->p.do_prop && h - 7 >= 64) {
         PT_TRY(lookup_banded(t, a, h, w, ann_out));
         if (seconds) *seconds = now_s() - T0;
         return PT_OK;
@@ -1268,8 +1291,8 @@ int64_t pt_kernel_launch_count(void) { return g_launches; }
 
 pt_status pt_table_view(const pt_table *t, PtTableView *v) {
     if (!t || !v) return pt_fail(PT_BAD_ARG, "null argument");
-    if (t->desc_mode || !t->subs.empty())
-        return pt_fail(PT_UNSUPPORTED, "descriptor mode and multi-table tables serve pt_table_lookup, "
+    if (t->desc_mode || t->pca || !t->subs.empty())
+        return pt_fail(PT_UNSUPPORTED, "descriptor mode, PCA and multi-table tables serve pt_table_lookup, "
                                        "pt_table_lookup_device(_temporal) and the profile only");
     v->p = t->p;
     v->h = t->h; v->w = t->w; v->ds = t->ds;

@@ -243,7 +243,7 @@ def test_constant_image(gpu, libc):
     assert np.allclose(ann[..., 2], 64 * 3 * 0.0625)
 
 
-@pytest.mark.parametrize("sw", ["-do_rs 1", "-spatial 1", "-dt_algo raster", "-ntables 17", "-dim_algo pca"])
+@pytest.mark.parametrize("sw", ["-do_rs 1", "-spatial 1", "-dt_algo raster", "-ntables 17", "-dim_algo pca -pca_mean 1"])
 def test_unsupported_options_fail_loudly(gpu, sw):
     _, b = synth.pair(40, 40, 1)
     with pytest.raises(ptb.PatchTableError) as e:
