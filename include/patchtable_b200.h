@@ -133,8 +133,10 @@ pt_status pt_table_subtable(pt_table *t, int i, pt_table **out);
 /* The reference's table keeps a pointer to the caller's PatchTableParams (patchtable.h:1546) and
    lookup() reads the query fields from it on every call (prop_iters, query_step, prop_dist,
    do_prop, do_table_lookup, coherence_spatial/temporal, recalc_dist_temporal, sanitize_input,
-   triangle_factor, kcoherence_iter).  This copies those fields (and the GPU schedule fields) into
-   the table; fields that shaped the build are left unchanged. */
+   triangle_factor, kcoherence_iter, do_rs, spatial).  This copies those fields (and the GPU
+   schedule fields) into the table; fields that shaped the build are left unchanged.  The random
+   search (do_rs) draws its neighbour from a hash of the patch and pass instead of rand(), so it
+   is deterministic and consumes no rand() values. */
 pt_status pt_table_set_params(pt_table *t, const pt_params *p);
 
 /* double PatchTable<>::lookup(const Array<float> &a, Array<double> &ann,

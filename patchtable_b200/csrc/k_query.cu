@@ -48,7 +48,15 @@ struct QPlan {
     int ds4, nd;             /* float4 per store entry, descriptor dimensions */
     const int *tcand_more;   /* further tables' entries, [table][patch] (ntables > 1), or NULL */
     int ntc;
+    int spatial, do_rs, pass; /* spatial search radius, random search, pass index (its seed) */
 };
+
+/* lowbias32 integer hash (C. Wellons' published constants): the random search's choice of
+   neighbour for a patch in a pass, in place of the reference's sequential rand() stream. */
+__device__ __forceinline__ unsigned mix32(unsigned x) {
+    x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+    return x;
+}
 
 __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
 
@@ -351,6 +359,53 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
             }
         }
         if (c_q.do_kcoh) kc_done[p] = (repeat || !accepted) ? kc_src : -1;
+        const bool have = xb < c_q.bew && yb < c_q.beh;
+        if (c_q.spatial > 0 && have) {
+            /* Spatial search (patchtable.h:3855-3873): every other patch of the (2s+1)^2 window
+               around the best match, rows then columns, scored in pairs and replayed in order. */
+            const int S = c_q.spatial, xb0 = xb, yb0 = yb;
+            int symin = yb0 - S, symax = yb0 + S + 1, sxmin = xb0 - S, sxmax = xb0 + S + 1;
+            if (symin < 0) symin = 0; else if (symax > c_q.beh) symax = c_q.beh;
+            if (sxmin < 0) sxmin = 0; else if (sxmax > c_q.bew) sxmax = c_q.bew;
+            if (symax > c_q.beh) symax = c_q.beh;          /* windows wider than b */
+            if (sxmax > c_q.bew) sxmax = c_q.bew;
+            const int swd = sxmax - sxmin, nwin = (symax - symin) * swd;
+            constexpr int G = 2;
+            for (int i0 = 0; i0 < nwin; i0 += G) {
+                int cg[G];
+                unsigned m = 0;
+#pragma unroll
+                for (int j = 0; j < G; j++) {
+                    cg[j] = 0;
+                    const int i = i0 + j;
+                    if (i >= nwin) continue;
+                    const int ys = symin + i / swd, xs = sxmin + i % swd;
+                    if (xs == xb0 && ys == yb0) continue;
+                    if (c_q.allowed && __ldg(c_q.allowed + (size_t) ys * c_q.bew + xs) != c_q.allowed_index) continue;
+                    cg[j] = pt_xy(xs, ys);
+                    m |= 1u << j;
+                }
+                if (!m) continue;
+                float d[G];
+                dist_group<TW, G, DESC>(aq, c_q, b, cg, m, dbest, d, rows);
+                ne += __popc(m);
+#pragma unroll
+                for (int j = 0; j < G; j++)
+                    if (((m >> j) & 1) && d[j] < dbest) { dbest = d[j]; dch = d[j]; xb = pt_x(cg[j]); yb = pt_y(cg[j]); }
+            }
+        } else if (c_q.do_rs && have) {
+            /* Random search (patchtable.h:3874-3903): one of the 8 neighbours of the best match.
+               dx, dy + 1 for r = 0..7 are packed two bits each: {-1,0,1,-1,1,-1,0,1},
+               {-1,-1,-1,0,0,1,1,1}. */
+            const unsigned r = mix32((unsigned) p * 2654435761u + (unsigned) c_q.pass * 0x9e3779b9u + 0x6a09e667u) & 7u;
+            const int xs = xb + (int) ((37412u >> (2 * r)) & 3u) - 1, ys = yb + (int) ((43328u >> (2 * r)) & 3u) - 1;
+            if (xs >= 0 && xs < c_q.bew && ys >= 0 && ys < c_q.beh &&
+                (!c_q.allowed || __ldg(c_q.allowed + (size_t) ys * c_q.bew + xs) == c_q.allowed_index)) {
+                const float dc = dist1<TW, DESC>(aq, c_q, b, xs, ys, dbest, rows);
+                ne++;
+                if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
+            }
+        }
         ch_pos[p] = pt_xy(xb, yb);
         ch_d[p] = dch;
     }
@@ -642,6 +697,9 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     q.nd = s.nd;
     q.tcand_more = s.ntcand_more > 0 ? s.tcand_more : nullptr;
     q.ntc = q.tcand_more ? s.ntcand_more : 0;
+    q.spatial = s.spatial > 0 ? s.spatial : 0;
+    q.do_rs = s.do_rs;
+    q.pass = s.pass;
     if (q.adesc) {
         if (!q.bdesc || (s.ds != 8 && s.ds != 16) || q.nd < 3 || q.nd > s.ds)
             return pt_fail(PT_BAD_ARG, "descriptor query: store of %d floats for %d dimensions", s.ds, q.nd);

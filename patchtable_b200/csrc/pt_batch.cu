@@ -61,6 +61,8 @@ pt_status run(pt_batch *B, const float *d_rgb, double *d_ann, cudaStream_t st) {
     qs.triangle_factor = p.triangle_factor;
     qs.kcoherence = p.kcoherence;
     qs.kcoherence_step = p.kcoherence_step;
+    qs.spatial = p.spatial;
+    qs.do_rs = p.do_rs;
     qs.radius = std::min(2, p.query_step + p.prop_dist);
     qs.b1 = v.b_rgba1;
     qs.pull_max = p.gpu_pull_max;
@@ -75,6 +77,7 @@ pt_status run(pt_batch *B, const float *d_rgb, double *d_ann, cudaStream_t st) {
     for (int i = 0; i < passes; i++) {
         const bool do_table = i == 0 && p.do_table_lookup;
         QuerySetup qi = qs;
+        qi.pass = i;
         if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
         PT_TRY(pt_launch_choose_batch(qi, B->d_imgs.p, B->n, B->nseg[B->twi], B->twi, B->rgba.p, v.b_rgba, B->pos[cur].p,
                                       B->dd[cur].p, B->tcand.p, v.kcoh, do_table, B->chpos.p, B->chd.p, B->kcdone.p, i > 0,

@@ -85,6 +85,9 @@ struct QuerySetup {
        [table][patch], tried after the first table's in the table step. */
     const int *tcand_more = nullptr;
     int ntcand_more = 0;
+    /* Random / spatial search after k-coherence (do_rs, spatial; patchtable.h:3854-3905) and the
+       index of the pass, which seeds the random search. */
+    int spatial = 0, do_rs = 0, pass = 0;
     cudaStream_t stream;
 };
 /* Query schedule.  By default two choose + pull passes stand in for each of the reference's

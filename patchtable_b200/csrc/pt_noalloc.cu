@@ -99,6 +99,8 @@ extern "C" pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_
     qs.triangle_factor = p.triangle_factor;
     qs.kcoherence = p.kcoherence;
     qs.kcoherence_step = p.kcoherence_step;
+    qs.spatial = p.spatial;
+    qs.do_rs = p.do_rs;
     qs.radius = p.query_step + p.prop_dist;
     if (qs.radius > 2) qs.radius = 2;
     qs.b1 = v.b_rgba1;
@@ -113,6 +115,7 @@ extern "C" pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_
     for (int i = 0; i < passes; i++) {
         bool do_table = i == 0 && p.do_table_lookup;
         QuerySetup qi = qs;
+        qi.pass = i;
         if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
         PT_TRY(pt_launch_choose(qi, n, rgba, v.b_rgba, pos[cur], dd[cur], tcand, v.kcoh, do_table, chpos, chd,
                                 kcdone, i > 0, nullptr, st));

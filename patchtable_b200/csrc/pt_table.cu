@@ -161,7 +161,6 @@ pt_status check_params(const pt_params *p, int h, int w) {
     if (p->ntables > 16) return pt_fail(PT_UNSUPPORTED, "ntables %d > 16", p->ntables);
     if (p->run_dt && p->dt_algo != 1 && p->dt_algo != 4 && p->dt_algo != 5 && p->dt_algo != 6)
         return pt_fail(PT_UNSUPPORTED, "dt_algo %d is not implemented on the GPU path", p->dt_algo);
-    if (p->do_rs || p->spatial) return pt_fail(PT_UNSUPPORTED, "random/spatial search (-do_rs, -spatial) is not implemented on the GPU path");
     if (p->init_random) return pt_fail(PT_UNSUPPORTED, "init_random is not implemented on the GPU path");
     if (p->ndims < 1 || p->ndims > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "ndims %d outside 1..%d", p->ndims, PT_DESC_MAX);
     int G = p->grid_ndims < 0 ? p->ndims : p->grid_ndims;
@@ -590,6 +589,8 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     qs.triangle_factor = p.triangle_factor;
     qs.kcoherence = p.kcoherence;
     qs.kcoherence_step = p.kcoherence_step;
+    qs.spatial = p.spatial;
+    qs.do_rs = p.do_rs;
     qs.radius = p.query_step + p.prop_dist;
     qs.b1 = t->b_rgba1.p;
     qs.pull_max = p.gpu_pull_max;
@@ -632,6 +633,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
            on every pass unless restricted to iteration 0 (kcoherence_iter). */
         bool do_table = i == 0 && p.do_table_lookup;
         QuerySetup qi = qs;
+        qi.pass = i;
         if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
         if (net)
             PT_TRY(pt_launch_choose_learned(qi, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_tcand.p,
@@ -699,6 +701,8 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     qs.triangle_factor = p.triangle_factor;
     qs.kcoherence = (p.kcoherence_iter < 0 || p.kcoherence_iter == 0) ? p.kcoherence : 0;
     qs.kcoherence_step = p.kcoherence_step;
+    qs.spatial = p.spatial;
+    qs.do_rs = p.do_rs;
     qs.radius = std::min(2, p.query_step + p.prop_dist);
     qs.b1 = t->b_rgba1.p;
     qs.pull_max = p.gpu_pull_max;
@@ -1247,8 +1251,9 @@ pt_status pt_table_set_params(pt_table *t, const pt_params *p) {
     q.gpu_jump = p->gpu_jump;
     q.gpu_pull_max = p->gpu_pull_max;
     q.gpu_tile = p->gpu_tile;
-    if (p->do_rs || p->spatial || p->init_random)
-        return pt_fail(PT_UNSUPPORTED, "random/spatial search and init_random are not implemented on the GPU path");
+    q.do_rs = p->do_rs;
+    q.spatial = p->spatial;
+    if (p->init_random) return pt_fail(PT_UNSUPPORTED, "init_random is not implemented on the GPU path");
     return PT_OK;
 }
 

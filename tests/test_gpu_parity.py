@@ -158,6 +158,41 @@ def test_multiple_tables(gpu, oracle, libc, sw):
     assert (tm.lookup(a)[..., 2] <= t1.lookup(a)[..., 2]).all()
 
 
+@pytest.mark.parametrize("spatial", [1, 2])
+def test_spatial_search_exact(gpu, oracle, libc, spatial):
+    """With one pass and no propagation every patch is independent in the reference too: table
+    entry, then the spatial search around it (patchtable.h:3855-3873).  In descriptor mode both
+    sides see identical query descriptors, hence identical table entries, and the GPU result
+    equals the oracle's bit for bit."""
+    a, b = synth.descriptor_pair(70, 90, 8, 23)
+    sw = ("-limit 0.5 -kcoherence 0 -do_prop 0 -prop_iters 1 -spatial %d -gpu_prop_passes 1 -is_descriptor 1"
+          % spatial)
+    p = ptb.PatchTableParams(sw)
+    srand_all(libc, 1)
+    ot = oracle.build(p.as_dict(), b)
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b)
+    assert np.array_equal(gt.table(), ot.table())
+    assert np.array_equal(gt.lookup(a), ot.lookup(a))
+
+
+@pytest.mark.parametrize("speed", list(range(10)))
+def test_every_speed_preset(gpu, oracle, libc, speed):
+    """Every -speed preset (patchtable.cpp:138-149: random and spatial search, k-coherence up to 20,
+    query_step up to 10) runs, with a mean distance at most 1 % above the oracle's."""
+    a, b = synth.pair(150, 200, 30 + speed)
+    p = ptb.PatchTableParams("-speed %d -limit 2" % speed)
+    srand_all(libc, 1)
+    ot = oracle.build(p.as_dict(), b)
+    srand_all(libc, 5)
+    mo = mean_dist(ot.lookup(a))
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b)
+    ann = gt.lookup(a)
+    check_nnf(oracle, a, b, ann)
+    assert mean_dist(ann) <= MEAN_DIST_SLACK * mo, (mean_dist(ann), mo)
+
+
 def check_nnf(oracle, a, b, ann, sample=4000):
     eh, ew = a.shape[0] - 7, a.shape[1] - 7
     beh, bew = b.shape[0] - 7, b.shape[1] - 7
@@ -243,7 +278,8 @@ def test_constant_image(gpu, libc):
     assert np.allclose(ann[..., 2], 64 * 3 * 0.0625)
 
 
-@pytest.mark.parametrize("sw", ["-do_rs 1", "-spatial 1", "-dt_algo raster", "-ntables 17", "-dim_algo pca -pca_mean 1"])
+@pytest.mark.parametrize("sw", ["-init_random 1", "-populate_nearest 0", "-dt_algo raster", "-ntables 17",
+                                "-dim_algo pca -pca_mean 1"])
 def test_unsupported_options_fail_loudly(gpu, sw):
     _, b = synth.pair(40, 40, 1)
     with pytest.raises(ptb.PatchTableError) as e:
