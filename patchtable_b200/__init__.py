@@ -70,6 +70,7 @@ class _Params(C.Structure):
         ("gpu_pull_max", C.c_int),
         ("gpu_tile", C.c_int),
         ("pca_samples", C.c_int), ("pca_subtract_mean", C.c_int), ("pca_mean", C.c_int),
+        ("gpu_bands", C.c_int),
     ]
 
 

@@ -139,7 +139,7 @@ pt_status apply_switches(pt_params *p, const std::vector<std::string> &argv) {
     INT_SW(grid_ndims) DBL_SW(table_ratio) INT_SW(prop_dist)
     BOOL_SW(is_descriptor) BOOL_SW(descriptor_padded)
     INT_SW(gpu_prop_passes) INT_SW(gpu_jump) INT_SW(gpu_pull_max) INT_SW(gpu_tile)
-    INT_SW(pca_samples) BOOL_SW(pca_mean) BOOL_SW(pca_subtract_mean)
+    INT_SW(pca_samples) BOOL_SW(pca_mean) BOOL_SW(pca_subtract_mean) INT_SW(gpu_bands)
 #undef INT_SW
 #undef BOOL_SW
 #undef DBL_SW

@@ -40,6 +40,9 @@ def test_banded_host_lookup_equals_device(gpu, libc, h, w, sw):
     pinned = np.empty_like(host)
     t.lookup(a, out=pinned)
     assert np.array_equal(pinned, dev)
+    for bands in (1, 5, 40):                 # the band count changes only the overlap
+        p.gpu_bands = bands
+        assert np.array_equal(t.lookup(a), dev), bands
 
 
 def test_banded_with_allowed_mask(gpu, libc):
