@@ -71,15 +71,32 @@ constexpr int TWD = 32;                   /* query patches per CTA row segment w
 constexpr int TWD_DESC = 64;              /* query patches per CTA in descriptor mode */
 
 /* Stages the 8 pixel rows under a CTA's row segment of TW query patches in shared memory
-   (TW + 7 pixels per row). */
+   (TW + 7 pixels per row) as packed RGB, 3 floats per pixel: a lane reading channel c of its 8
+   pixels touches word 3 * pixel + c, so each warp-wide 4-byte load hits 32 distinct banks in one
+   wavefront, and a row costs 24 wavefronts instead of the 32 of 16-byte RGBA loads. */
 template<int TW>
 __device__ __forceinline__ void stage_a(float4 *atile, const float4 *__restrict__ a, int aw, int ah, int x0, int y) {
     constexpr int ATW = TW + 7;
+    float *at = reinterpret_cast<float *>(atile);
     for (int i = threadIdx.x; i < 8 * ATW; i += TW) {
         int r = i / ATW, c = i - r * ATW;
         int gx = x0 + c, gy = y + r;
-        atile[i] = (gx < aw && gy < ah) ? __ldg(a + (size_t) gy * aw + gx) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 v = (gx < aw && gy < ah) ? __ldg(a + (size_t) gy * aw + gx) : make_float4(0.f, 0.f, 0.f, 0.f);
+        at[3 * i] = v.x;
+        at[3 * i + 1] = v.y;
+        at[3 * i + 2] = v.z;
     }
+}
+
+/* Shared-memory bytes of a staged query tile of TW patches. */
+constexpr size_t atile_bytes(int TW) { return sizeof(float) * 3 * 8 * (TW + 7); }
+
+/* Query row dy of the patch at tile column tx. */
+template<int TW>
+__device__ __forceinline__ void load_arow(const float4 *atile, int dy, int tx, float4 (&av)[8]) {
+    const float *at = reinterpret_cast<const float *>(atile) + 3 * (dy * (TW + 7) + tx);
+#pragma unroll
+    for (int p = 0; p < 8; p++) av[p] = make_float4(at[3 * p], at[3 * p + 1], at[3 * p + 2], 0.f);
 }
 
 /* One 32-byte read-only load: pixels p[0], p[1]. */
@@ -123,15 +140,13 @@ __device__ __forceinline__ float lane_total(const float (&l)[4]) {
 template<int TW>
 __device__ __forceinline__ float ssd_tile(const float4 *atile, int tx, const QPlan &q, const float4 *__restrict__ B,
                                           int bx, int by, float bound, unsigned &rows) {
-    constexpr int ATW = TW + 7;
     float l[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
     for (int dy = 0; dy < 8; dy++) {
         rows++;
         float4 av[8], bv[8];
         load_brow(q, B, bx, by + dy, bv);
-#pragma unroll
-        for (int p = 0; p < 8; p++) av[p] = atile[dy * ATW + tx + p];
+        load_arow<TW>(atile, dy, tx, av);
         row_lanes(av, bv, l);
         if (dy < 7 && lane_total(l) >= bound) return finf();
     }
@@ -146,7 +161,6 @@ template<int TW, int G>
 __device__ __forceinline__ void ssd_group(const float4 *atile, int tx, const QPlan &q, const float4 *__restrict__ B,
                                           const int (&cand)[G], unsigned valid, float bound, float (&out)[G],
                                           unsigned &rows) {
-    constexpr int ATW = TW + 7;
     float l[G][4];
     bool live[G];
 #pragma unroll
@@ -158,8 +172,7 @@ __device__ __forceinline__ void ssd_group(const float4 *atile, int tx, const QPl
         for (int g = 0; g < G; g++) any |= live[g];
         if (!any) break;
         float4 av[8];
-#pragma unroll
-        for (int p = 0; p < 8; p++) av[p] = atile[dy * ATW + tx + p];
+        load_arow<TW>(atile, dy, tx, av);
 #pragma unroll
         for (int g = 0; g < G; g++) {
             if (!live[g]) continue;
@@ -733,7 +746,7 @@ pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const fl
         return PT_OK;
     }
 #define PT_CHOOSE_T(T) { dim3 grid((q.ew + T - 1) / T, q.rows); \
-        k_choose_tile<T, false, false><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, \
+        k_choose_tile<T, false, false><<<grid, T, atile_bytes(T), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, \
                                                                                     do_table, ch_pos, ch_d, kc_done, use_done, \
                                                                                     evals, none); }
     switch (q.tile) {
@@ -763,7 +776,7 @@ pt_status pt_launch_choose_learned(const QuerySetup &s, const float4 *a, const f
     la.kcoh_confident = kcoh_confident;
     la.counters = lcounters;
 #define PT_CHOOSE_L(T) { dim3 grid((q.ew + T - 1) / T, q.rows); \
-        k_choose_tile<T, true, false><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, \
+        k_choose_tile<T, true, false><<<grid, T, atile_bytes(T), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, \
                                                                                    do_table, ch_pos, ch_d, kc_done, use_done, \
                                                                                    evals, la); }
     switch (q.tile) {
@@ -793,7 +806,7 @@ pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const floa
         return PT_OK;
     }
 #define PT_PULL_T(T, RR) { dim3 grid((q.ew + T - 1) / T, q.rows); \
-        k_pull_tile<T, RR, false><<<grid, T, sizeof(float4) * 8 * (T + 7), st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, \
+        k_pull_tile<T, RR, false><<<grid, T, atile_bytes(T), st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, \
                                                                                 nxt_pos, nxt_d, evals); }
     switch (q.tile) {
         case 32: if (r1) PT_PULL_T(32, 1) else PT_PULL_T(32, 2) break;
@@ -843,7 +856,7 @@ pt_status pt_launch_choose_batch(const QuerySetup &s, const PtBatchImage *imgs, 
     QPlan q;
     PT_TRY(make_qplan(s, q));
     if (nseg <= 0) return PT_OK;
-#define PT_CHOOSE_B(T) { const size_t sm = sizeof(float4) * 8 * (T + 7); \
+#define PT_CHOOSE_B(T) { const size_t sm = atile_bytes(T); \
         const int g = persistent_grid(k_choose_batch<T>, T, sm, nseg); \
         k_choose_batch<T><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, \
                                             kc_done, use_done, evals); }
@@ -864,7 +877,7 @@ pt_status pt_launch_pull_batch(const QuerySetup &s, const PtBatchImage *imgs, in
     QPlan q;
     PT_TRY(make_qplan(s, q));
     if (nseg <= 0) return PT_OK;
-#define PT_PULL_B(T, RR) { const size_t sm = sizeof(float4) * 8 * (T + 7); \
+#define PT_PULL_B(T, RR) { const size_t sm = atile_bytes(T); \
         const int g = persistent_grid(k_pull_batch<T, RR>, T, sm, nseg); \
         k_pull_batch<T, RR><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals); }
     const bool r1 = q.radius <= 1;
