@@ -376,14 +376,12 @@ def one_vs_many_measure():
 
 def main():
     args = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from patchtable_b200 import replicas
+    rank, world, local = replicas.env()
     if args.impl == "reference":
         run_reference(args, rank)
         return
     import torch
-    import torch.distributed as dist
     import patchtable_b200 as ptb
     from patchtable_b200.metrics import get_mean_dist as mean_dist
 
@@ -392,9 +390,7 @@ def main():
     if args.profile_case:
         profile_case(args.profile_case)
         return
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    replicas.init("nccl", dev)
 
     a, b = make_inputs()
     H, W = a.shape[:2]
@@ -423,12 +419,13 @@ def main():
         if m <= 1.01 * ref_md and (chosen is None or ms < chosen[0]):
             chosen = (ms, sched)
     chosen = chosen[1] if chosen else SCHEDULES[-1]
+    chosen = SCHEDULES[int(replicas.agree(SCHEDULES.index(chosen), dev))]   # every rank runs rank 0's choice
     # query patches per CTA: the results do not depend on it, only the time does
     tile_ms = {}
     for tile in (32, 64, 128, 256):
         params.gpu_tile = tile
         tile_ms[tile], _ = timed_schedule(table, chosen, da, H, W, dann, sptr, flush)
-    params.gpu_tile = min(tile_ms, key=tile_ms.get)
+    params.gpu_tile = int(replicas.agree(min(tile_ms, key=tile_ms.get), dev))
     params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = chosen
     for _ in range(max(args.warmup, 3)):
         flush.zero_()
@@ -437,8 +434,7 @@ def main():
     md = mean_dist(dann.cpu().numpy())
 
     clocks = Clocks(local)
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     clocks.start()
     ptb.reset_launch_count()
@@ -457,18 +453,13 @@ def main():
     torch.cuda.synchronize()
     wall = time.perf_counter() - tw0
     launches = ptb.launch_count()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     clk = clocks.stop()
     # device time per step: the sum of the stage times (CUDA events around every kernel on the
     # launching stream); the outer events also include the library's host-side launch gaps.
     outer = [e0.elapsed_time(e1) for e0, e1 in ev]
-    tot_ms = sum(stages.values())
-    tot_t = torch.tensor([tot_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(tot_t, op=dist.ReduceOp.MAX)
-    tot_ms = float(tot_t.item())
-    value = world * P * args.steps / (tot_ms / 1000.0)
+    tot_ms = replicas.max_over_ranks(sum(stages.values()), dev)
+    value = replicas.whole_job_rate(P * args.steps, tot_ms / 1000.0, world)
 
     # end-to-end through the public host API with pinned buffers
     a_pin = torch.from_numpy(a).pin_memory()
@@ -482,10 +473,7 @@ def main():
         t1 = time.perf_counter()
         table.lookup(a_np, out=ann_np)
         e2e_s.append(time.perf_counter() - t1)
-    e2e_t = torch.tensor([sum(e2e_s) / len(e2e_s)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e = world * P / float(e2e_t.item())
+    e2e = replicas.whole_job_rate(P, replicas.max_over_ranks(sum(e2e_s) / len(e2e_s), dev), world)
     md_e2e = mean_dist(ann_np)
 
     # the library's default schedule on the same workload, for reference
@@ -528,9 +516,7 @@ def main():
         c4 = uneven_batch_measure()
         c3 = one_vs_many_measure()
 
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish()
     if rank != 0:
         return
     out = {
