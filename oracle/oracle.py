@@ -51,6 +51,7 @@ class OrcParams(C.Structure):
         ("is_descriptor", C.c_int), ("descriptor_padded", C.c_int),
         ("ntables", C.c_int), ("table_ratio", C.c_double),
         ("dim_algo", C.c_int), ("pca_samples", C.c_int), ("pca_subtract_mean", C.c_int), ("pca_mean", C.c_int),
+        ("colorspace", C.c_int),
     ]
 
 
@@ -85,6 +86,7 @@ class Oracle:
         L.orc_get_kcoherence.argtypes = [C.c_void_p, _i32p, _f32p]
         L.orc_lookup.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, _f64p, C.c_void_p, C.c_void_p]
         L.orc_rgb2yuv.argtypes = [_f32p, C.c_int, C.c_int, _f32p]
+        L.orc_rgb2lab.argtypes = [_f32p, C.c_int, C.c_int, _f32p]
         L.orc_gck.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
         L.orc_descriptor.argtypes = [C.POINTER(OrcParams), _f32p, C.c_int, C.c_int, _f32p]
         L.orc_patch_dist.restype = C.c_float
@@ -103,6 +105,12 @@ class Oracle:
         img = np.ascontiguousarray(img, np.float32)
         out = np.empty_like(img)
         self.lib.orc_rgb2yuv(img, img.shape[0], img.shape[1], out)
+        return out
+
+    def rgb2lab(self, img):
+        img = np.ascontiguousarray(img, np.float32)
+        out = np.empty_like(img)
+        self.lib.orc_rgb2lab(img, img.shape[0], img.shape[1], out)
         return out
 
     def gck(self, yuv, n: int, nchroma: int):

@@ -60,6 +60,7 @@ typedef struct {
     int ntables;                            /* further tables at limit / table_ratio^i */
     double table_ratio;
     int dim_algo, pca_samples, pca_subtract_mean, pca_mean;   /* dim_algo 1: PCA descriptor */
+    int colorspace;                         /* 0 YUV, 1 Lab (when convert_colorspace) */
 } orc_params;
 
 }
@@ -77,6 +78,53 @@ void rgb2yuv(const float *in, int n, float *out) {
         out[3 * i + 1] = (float) (-0.14713 * R + -0.28886 * G + 0.436 * B);
         out[3 * i + 2] = (float) (0.615 * R + -0.51499 * G + -0.10001 * B);
     }
+}
+
+/* ------------------------------------------------------------------------------------------
+   Colour conversion -colorspace lab: Array::rgb2lab = rgb2xyz then xyz2lab (solver/array.h:
+   1213-1292, D50 white, Bruce Lindbloom's formulas) with the powers read from PowTable<float,
+   1024> (solver/array.h:221-237): entry i holds (float) pow((i + 0.5) / 1024, p), p stored as a
+   float, and a value v reads entry int(v * 1024.0f) clamped to the table.  Constants are double,
+   pixels float, as in the reference.
+   ------------------------------------------------------------------------------------------ */
+struct PowTab {
+    float t[1024];
+    explicit PowTab(float p) {
+        for (int i = 0; i < 1024; i++) t[i] = (float) pow((i + 0.5) / 1024 * (double) 1.0f, (double) p);
+    }
+    float operator()(float v) const {
+        int i = (int) (v * 1024.0f);
+        if (i < 0) i = 0; else if (i >= 1024) i = 1023;
+        return t[i];
+    }
+};
+
+void rgb2lab(const float *in, int n, float *out) {
+    static const PowTab p24(2.4f), p13((float) (1.0 / 3.0));
+    for (int k = 0; k < n; k++) {
+        float c[3];
+        for (int j = 0; j < 3; j++) {
+            float v = in[3 * k + j];
+            c[j] = (v <= 0.04045) ? (float) (v / 12.92) : p24((float) ((v + 0.055) / 1.055));
+        }
+        float X = (float) (0.4360747 * c[0] + 0.3850649 * c[1] + 0.1430804 * c[2]);
+        float Y = (float) (0.2225045 * c[0] + 0.7168786 * c[1] + 0.0606169 * c[2]);
+        float Z = (float) (0.0139322 * c[0] + 0.0971045 * c[1] + 0.7141733 * c[2]);
+        float xr = (float) (X / 0.9642), yr = (float) (Y / 1.0000), zr = (float) (Z / 0.8249);
+        float fx = (xr > 0.008856) ? p13(xr) : (float) ((903.3 * xr + 16) / 116);
+        float fy = (yr > 0.008856) ? p13(yr) : (float) ((903.3 * yr + 16) / 116);
+        float fz = (zr > 0.008856) ? p13(zr) : (float) ((903.3 * zr + 16) / 116);
+        out[3 * k + 0] = 116 * fy - 16;
+        out[3 * k + 1] = 500 * (fx - fy);
+        out[3 * k + 2] = 200 * (fy - fz);
+    }
+}
+
+/* The colour conversion of get_padded_descriptor (patchtable.h:2510-2522). */
+void convert_color(const orc_params &p, const float *in, int n, float *out) {
+    if (!p.convert_colorspace) memcpy(out, in, sizeof(float) * 3 * (size_t) n);
+    else if (p.colorspace == 1) rgb2lab(in, n, out);
+    else rgb2yuv(in, n, out);
 }
 
 /* ------------------------------------------------------------------------------------------
@@ -265,8 +313,7 @@ struct Table {
 /* get_padded_descriptor for RGB input (patchtable.h:2492-2546): YUV then gck. */
 void padded_descriptor(const orc_params &p, const float *rgb, int h, int w, vector<float> &wh) {
     vector<float> yuv((size_t) h * w * 3);
-    if (p.convert_colorspace) rgb2yuv(rgb, h * w, yuv.data());
-    else memcpy(yuv.data(), rgb, sizeof(float) * yuv.size());
+    convert_color(p, rgb, h * w, yuv.data());
     wh.assign((size_t) (h + 7) * (w + 7) * p.ndims, 0.0f);
     gck8(yuv.data(), h, w, p.ndims - p.nchroma * 2, p.nchroma, wh.data());
 }
@@ -427,8 +474,7 @@ Table *build(const orc_params &p, const float *b, int h, int w, const int32_t *a
         t->b0.assign(b, b + (size_t) h * w * 3);
         if (p.dim_algo == 1) {                           /* reduce_dim, patchtable.h:1709-1713 */
             vector<float> img((size_t) h * w * 3);
-            if (p.convert_colorspace) rgb2yuv(b, h * w, img.data());
-            else memcpy(img.data(), b, sizeof(float) * img.size());
+            convert_color(p, b, h * w, img.data());
             pca_fit(p, img.data(), h, w, t->pca);
             if (!wh0_in) pca_apply(p, t->pca, img.data(), h, w, t->wh0);
         } else if (!wh0_in) {
@@ -870,8 +916,7 @@ double lookup(Table &t, const float *a, int ah, int aw, double *ann, const doubl
         padded_input(p, a, ah, aw, a_wh, ah, aw);
     } else if (p.dim_algo == 1) {
         vector<float> img((size_t) ah * aw * 3);
-        if (p.convert_colorspace) rgb2yuv(a, ah * aw, img.data());
-        else memcpy(img.data(), a, sizeof(float) * img.size());
+        convert_color(p, a, ah * aw, img.data());
         pca_apply(p, t.pca, img.data(), ah, aw, a_wh);
     } else {
         padded_descriptor(p, a, ah, aw, a_wh);
@@ -1122,6 +1167,8 @@ extern "C" {
 void orc_srand(unsigned s) { srand(s); }
 
 void orc_rgb2yuv(const float *in, int h, int w, float *out) { rgb2yuv(in, h * w, out); }
+
+void orc_rgb2lab(const float *in, int h, int w, float *out) { rgb2lab(in, h * w, out); }
 
 void orc_gck(const float *yuv, int h, int w, int n, int nchroma, float *out) { gck8(yuv, h, w, n, nchroma, out); }
 

@@ -15,6 +15,7 @@
    used by the distance kernels. */
 #include <cuda_runtime.h>
 #include <cstdio>
+#include <mutex>
 
 #include "pt_internal.h"
 #include "wh_tables.h"
@@ -47,6 +48,43 @@ __device__ __forceinline__ void yuv_exact(float R, float G, float B, float &Y, f
 }
 
 
+/* -colorspace lab: Array::rgb2lab (solver/array.h:1246-1256) = rgb2xyz (:1213-1244) then xyz2lab
+   (:1264-1292), whose powers come from PowTable (solver/array.h:221-237): 1024 entries
+   table[i] = (float) pow((i + 0.5) / 1024, p) for p = (float) 2.4 and (float) (1/3), read at
+   int(v * 1024.0f) clamped to the table.  The tables are filled once per device from the host
+   C library's pow, the arithmetic around them is the reference's double / float mix. */
+__device__ float g_lab_pow[2][PT_LAB_N];
+
+__device__ __forceinline__ float lab_tab(int t, float v) {
+    int i = __float2int_rz(__fmul_rn(v, (float) PT_LAB_N));
+    i = i < 0 ? 0 : (i >= PT_LAB_N ? PT_LAB_N - 1 : i);
+    return g_lab_pow[t][i];
+}
+
+__device__ __forceinline__ float srgb_linear(float c) {
+    const double cd = c;
+    if (cd <= 0.04045) return __double2float_rn(__ddiv_rn(cd, 12.92));
+    return lab_tab(0, __double2float_rn(__ddiv_rn(__dadd_rn(cd, 0.055), 1.055)));
+}
+
+__device__ __forceinline__ float lab_f(float r) {
+    if ((double) r > 0.008856) return lab_tab(1, r);
+    return __double2float_rn(__ddiv_rn(__dadd_rn(__dmul_rn(903.3, (double) r), 16.0), 116.0));
+}
+
+__device__ __forceinline__ void lab_exact(float R, float G, float B, float &L, float &A, float &Bo) {
+    const double r = srgb_linear(R), g = srgb_linear(G), b = srgb_linear(B);
+    const float X = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.4360747, r), __dmul_rn(0.3850649, g)), __dmul_rn(0.1430804, b)));
+    const float Y = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.2225045, r), __dmul_rn(0.7168786, g)), __dmul_rn(0.0606169, b)));
+    const float Z = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.0139322, r), __dmul_rn(0.0971045, g)), __dmul_rn(0.7141733, b)));
+    const float fx = lab_f(__double2float_rn(__ddiv_rn((double) X, 0.9642)));
+    const float fy = lab_f(__double2float_rn(__ddiv_rn((double) Y, 1.0)));
+    const float fz = lab_f(__double2float_rn(__ddiv_rn((double) Z, 0.8249)));
+    L = __fsub_rn(__fmul_rn(116.0f, fy), 16.0f);
+    A = __fmul_rn(500.0f, __fsub_rn(fx, fy));
+    Bo = __fmul_rn(200.0f, __fsub_rn(fy, fz));
+}
+
 /* The colour-converted pixels under a 64 x 8 block of patches with top-left patch (x0, y0), as
    3 planes of RH x RWP floats; the block also writes the RGBA copy of the pixels it owns. */
 __device__ __forceinline__ void stage_pix(float *pix, const float *__restrict__ rgb, int h, int w, int convert,
@@ -64,7 +102,8 @@ __device__ __forceinline__ void stage_pix(float *pix, const float *__restrict__ 
             if (rgba && gy < own_y1 && gx < own_x1) rgba[(size_t) gy * w + gx] = make_float4(R, G, B, 0.f);
         }
         float Y = R, U = G, V = B;
-        if (convert) yuv_exact(R, G, B, Y, U, V);
+        if (convert == PT_COLOR_YUV) yuv_exact(R, G, B, Y, U, V);
+        else if (convert == PT_COLOR_LAB) lab_exact(R, G, B, Y, U, V);
         pix[(0 * RH + r) * RWP + c] = Y;
         pix[(1 * RH + r) * RWP + c] = U;
         pix[(2 * RH + r) * RWP + c] = V;
@@ -242,6 +281,7 @@ pt_status pt_launch_descriptor(int ndims, int nchroma, const float *rgb, int h, 
 
 pt_status pt_launch_descriptor_rows(int ndims, int nchroma, const float *rgb, int h, int w, int convert, float4 *rgba,
                                     float *desc, int ds, int trow0, int trows, cudaStream_t st) {
+    if (convert == PT_COLOR_LAB) PT_TRY(pt_lab_tables_ready());
     int eh = h - 7, ew = w - 7;
     DescPlan plan;
     PT_TRY(make_plan(ndims, nchroma, plan));
@@ -263,6 +303,7 @@ pt_status pt_launch_descriptor_rows(int ndims, int nchroma, const float *rgb, in
 
 pt_status pt_launch_descriptor_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
                                      const float *rgb, int convert, float4 *rgba, float *desc, int ds, cudaStream_t st) {
+    if (convert == PT_COLOR_LAB) PT_TRY(pt_lab_tables_ready());
     DescPlan plan;
     PT_TRY(make_plan(ndims, nchroma, plan));
     if (ntiles <= 0) return PT_OK;
@@ -323,11 +364,27 @@ pt_status pt_launch_descriptor_input(const float *in, int H, int W, int nd, int 
 
 pt_status pt_launch_pca(const float *rgb, int h, int w, int convert, float4 *rgba, const float *mean, const float *basis,
                         int ncomp, float *desc, int ds, cudaStream_t st) {
+    if (convert == PT_COLOR_LAB) PT_TRY(pt_lab_tables_ready());
     const int ew = w - 7, eh = h - 7;
     if (ew < 1 || eh < 1) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
     if (ncomp < 1 || ncomp > ds || ds > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "PCA with %d components", ncomp);
     dim3 grid((ew + TW - 1) / TW, (eh + TH - 1) / TH);
     k_pca<<<grid, NT, 0, st>>>(rgb, h, w, convert, rgba, mean, basis, ncomp, desc, ds, eh, ew);
     PT_LAUNCHED();
+    return PT_OK;
+}
+
+/* Fills the PowTable stand-ins of -colorspace lab on the current device (once per device). */
+pt_status pt_lab_tables_ready() {
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    PT_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 64 && done[dev]) return PT_OK;
+    float tab[2][PT_LAB_N];
+    pt_lab_pow_tables(tab);
+    PT_CUDA(cudaMemcpyToSymbol(g_lab_pow, tab, sizeof(tab)));
+    if (dev < 64) done[dev] = true;
     return PT_OK;
 }

@@ -52,7 +52,7 @@ pt_status run(pt_batch *B, const float *d_rgb, double *d_ann, cudaStream_t st) {
     PT_TRY(pt_table_view(B->t, &v));
     const pt_params &p = v.p;
     const int ds = v.ds;
-    PT_TRY(pt_launch_descriptor_batch(p.ndims, p.nchroma, B->d_imgs.p, B->n, B->ntiles, d_rgb, p.convert_colorspace,
+    PT_TRY(pt_launch_descriptor_batch(p.ndims, p.nchroma, B->d_imgs.p, B->n, B->ntiles, d_rgb, pt_color_mode(p),
                                       B->rgba.p, B->desc.p, ds, st));
     PT_TRY(pt_launch_table_candidates(v.bins, B->desc.p, ds, B->P, v.to_bin, v.table, B->tcand.p, st));
     QuerySetup qs;

@@ -6,6 +6,18 @@
 
 #include "pt_internal.h"
 
+/* Colour conversion before the descriptor (get_padded_descriptor, patchtable.h:2510-2522):
+   none, ARRAY_RGB2YUV, or Array::rgb2lab with its PowTable lookups. */
+#define PT_COLOR_NONE 0
+#define PT_COLOR_YUV 1
+#define PT_COLOR_LAB 2
+#define PT_LAB_N 1024
+inline int pt_color_mode(const pt_params &p) { return p.convert_colorspace ? (p.colorspace == 1 ? PT_COLOR_LAB : PT_COLOR_YUV) : PT_COLOR_NONE; }
+/* PowTable<float, 1024> contents for p = 2.4 and 1/3 (pt_pca.cpp) and their upload to the
+   current device, once (k_descriptor.cu). */
+void pt_lab_pow_tables(float (*tab)[PT_LAB_N]);
+pt_status pt_lab_tables_ready();
+
 /* k_descriptor.cu */
 pt_status pt_descriptor_check(int ndims, int nchroma);
 /* desc may be NULL (only the RGBA copy is written); rgba may be NULL. */

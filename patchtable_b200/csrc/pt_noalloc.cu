@@ -91,7 +91,7 @@ extern "C" pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_
 
     long long P = (long long) (h - 7) * (w - 7);
     int n = (int) P;
-    PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, d_a, h, w, p.convert_colorspace, rgba, desc, 8, st));
+    PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, d_a, h, w, pt_color_mode(p), rgba, desc, 8, st));
     PT_TRY(pt_launch_table_candidates(v.bins, desc, 8, P, v.to_bin, v.table, tcand, st));
     QuerySetup qs;
     qs.aw = w; qs.ah = h; qs.bw = v.w; qs.bh = v.h;

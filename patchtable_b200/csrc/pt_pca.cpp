@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <numeric>
+#include <memory>
 #include <vector>
 
 #include "pt_internal.h"
@@ -27,6 +28,37 @@ inline void yuv_host(float R, float G, float B, float &Y, float &U, float &V) {
     U = (float) ((-0.14713 * r + -0.28886 * g) + 0.436 * b);
     V = (float) ((0.615 * r + -0.51499 * g) + -0.10001 * b);
 }
+
+/* Array::rgb2lab as the GPU descriptor kernels compute it (k_descriptor.cu: lab_exact). */
+struct LabHost {
+    float tab[2][PT_LAB_N];
+    LabHost() { pt_lab_pow_tables(tab); }
+    float look(int t, float v) const {
+        int i = (int) (v * (float) PT_LAB_N);
+        i = i < 0 ? 0 : (i >= PT_LAB_N ? PT_LAB_N - 1 : i);
+        return tab[t][i];
+    }
+    float lin(float c) const {
+        const double cd = c;
+        if (cd <= 0.04045) return (float) (cd / 12.92);
+        return look(0, (float) ((cd + 0.055) / 1.055));
+    }
+    float f(float r) const {
+        if ((double) r > 0.008856) return look(1, r);
+        return (float) ((903.3 * (double) r + 16.0) / 116.0);
+    }
+    void operator()(float R, float G, float B, float &L, float &A, float &Bo) const {
+        const double r = lin(R), g = lin(G), b = lin(B);
+        const float X = (float) ((0.4360747 * r + 0.3850649 * g) + 0.1430804 * b);
+        const float Y = (float) ((0.2225045 * r + 0.7168786 * g) + 0.0606169 * b);
+        const float Z = (float) ((0.0139322 * r + 0.0971045 * g) + 0.7141733 * b);
+        const float fx = f((float) ((double) X / 0.9642)), fy = f((float) ((double) Y / 1.0)),
+                    fz = f((float) ((double) Z / 0.8249));
+        L = 116.0f * fy - 16.0f;
+        A = 500.0f * (fx - fy);
+        Bo = 200.0f * (fy - fz);
+    }
+};
 
 /* Eigen-decomposition of the symmetric n x n matrix a (row-major, destroyed) by cyclic Jacobi
    rotations; vals[k] and column k of vecs (row-major n x n) are the pairs. */
@@ -77,6 +109,8 @@ pt_status pt_pca_fit(const float *rgb, int h, int w, int convert, int samples, i
     if (ncomp < 1 || ncomp > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "PCA with %d components", ncomp);
     const int aew = w - 7, aeh = h - 7;
     std::vector<double> X((size_t) samples * D);
+    std::unique_ptr<LabHost> lab;
+    if (convert == PT_COLOR_LAB) lab.reset(new LabHost());
     for (int i = 0; i < samples; i++) {
         const int ax = rand() % aew;                   /* extract_patches, patch_pca.h:25-26 */
         const int ay = rand() % aeh;
@@ -86,7 +120,8 @@ pt_status pt_pca_fit(const float *rgb, int h, int w, int convert, int samples, i
             for (int dx = 0; dx < 8; dx++) {
                 const float *px = rgb + ((size_t) (ay + dy) * w + ax + dx) * 3;
                 float c0 = px[0], c1 = px[1], c2 = px[2];
-                if (convert) yuv_host(px[0], px[1], px[2], c0, c1, c2);
+                if (convert == PT_COLOR_YUV) yuv_host(px[0], px[1], px[2], c0, c1, c2);
+                else if (convert == PT_COLOR_LAB) (*lab)(px[0], px[1], px[2], c0, c1, c2);
                 row[k++] = c0; row[k++] = c1; row[k++] = c2;
             }
     }
@@ -126,4 +161,14 @@ pt_status pt_pca_fit(const float *rgb, int h, int w, int convert, int samples, i
         for (int j = 0; j < D; j++) basis_out[(size_t) k * D + j] = (float) (sgn * vecs[(size_t) j * D + col]);
     }
     return PT_OK;
+}
+
+void pt_lab_pow_tables(float (*tab)[PT_LAB_N]) {
+    /* PowTable(real p, real upper = 1), solver/array.h:221-237, with p stored as float */
+    const float p[2] = {2.4f, (float) (1.0 / 3.0)};
+    for (int t = 0; t < 2; t++)
+        for (int i = 0; i < PT_LAB_N; i++) {
+            const double v = (i + 0.5) / PT_LAB_N * (double) 1.0f;
+            tab[t][i] = (float) std::pow(v, (double) p[t]);
+        }
 }

@@ -151,8 +151,8 @@ pt_status check_params(const pt_params *p, int h, int w) {
         return pt_fail(PT_UNSUPPORTED, "dim_algo pca with %s is not implemented on the GPU path",
                        p->is_descriptor ? "is_descriptor" : "pca_mean");
     if (p->dim_algo != 0 && p->dim_algo != 1) return pt_fail(PT_BAD_ARG, "dim_algo %d", p->dim_algo);
-    if (!p->is_descriptor && p->convert_colorspace && p->colorspace != 0)
-        return pt_fail(PT_UNSUPPORTED, "colorspace lab is not implemented on the GPU path");
+    if (p->convert_colorspace && p->colorspace != 0 && p->colorspace != 1)
+        return pt_fail(PT_BAD_ARG, "colorspace %d", p->colorspace);
     if (p->lookup_algo != 0) return pt_fail(PT_UNSUPPORTED, "only lookup_algo table is implemented on the GPU path");
     if (p->kcoherence && p->kcoherence_algo != 0) return pt_fail(PT_UNSUPPORTED, "only kcoherence_algo flann (exact search) is implemented");
     if (p->incoherence) return pt_fail(PT_UNSUPPORTED, "incoherence is not implemented on the GPU path");
@@ -367,17 +367,17 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
         if (p.dim_algo == 1) {
             /* reduce_dim with TABLE_DIM_ALGO_PCA (patchtable.h:1709-1713): fit on b, then project */
             std::vector<float> mean, basis;
-            PT_TRY(pt_pca_fit(b, h, w, p.convert_colorspace, p.pca_samples, p.pca_subtract_mean, p.ndims, mean, basis));
+            PT_TRY(pt_pca_fit(b, h, w, pt_color_mode(p), p.pca_samples, p.pca_subtract_mean, p.ndims, mean, basis));
             t->pca = true;
             PT_CUDA(t->pca_mean.reserve(mean.size()));
             PT_CUDA(t->pca_basis.reserve(basis.size()));
             PT_CUDA(cudaMemcpyAsync(t->pca_mean.p, mean.data(), sizeof(float) * mean.size(), cudaMemcpyHostToDevice, t->st));
             PT_CUDA(cudaMemcpyAsync(t->pca_basis.p, basis.data(), sizeof(float) * basis.size(), cudaMemcpyHostToDevice, t->st));
-            PT_TRY(pt_launch_pca(rgb.p, h, w, p.convert_colorspace, t->b_rgba.p, t->pca_mean.p, t->pca_basis.p, p.ndims,
+            PT_TRY(pt_launch_pca(rgb.p, h, w, pt_color_mode(p), t->b_rgba.p, t->pca_mean.p, t->pca_basis.p, p.ndims,
                                  t->b_desc.p, t->ds, t->st));
             PT_CUDA(cudaStreamSynchronize(t->st));     /* the host vectors go out of scope */
         } else {
-            PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, rgb.p, h, w, p.convert_colorspace, t->b_rgba.p, t->b_desc.p,
+            PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, rgb.p, h, w, pt_color_mode(p), t->b_rgba.p, t->b_desc.p,
                                         t->ds, t->st));
         }
         if (wh0) {
@@ -558,10 +558,10 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
         query_input_dims(t, h, w, ih, iw, nin);
         PT_TRY(pt_launch_descriptor_input(a_rgb, ih, iw, t->nd, t->in_padded, t->q_desc.p, t->ds, st));
     } else if (t->pca) {
-        PT_TRY(pt_launch_pca(a_rgb, h, w, p.convert_colorspace, t->q_rgba.p, t->pca_mean.p, t->pca_basis.p, t->nd,
+        PT_TRY(pt_launch_pca(a_rgb, h, w, pt_color_mode(p), t->q_rgba.p, t->pca_mean.p, t->pca_basis.p, t->nd,
                              t->q_desc.p, t->ds, st));
     } else {
-        PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, a_rgb, h, w, p.convert_colorspace, t->q_rgba.p, t->q_desc.p,
+        PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, a_rgb, h, w, pt_color_mode(p), t->q_rgba.p, t->q_desc.p,
                                     t->ds, st));
     }
     PT_TRY(mark(t, prof, LookupProfile::DESC, st));
@@ -721,7 +721,7 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
             PT_CUDA(cudaMemcpyAsync(t->q_rgb.p + px0, a + px0, sizeof(float) * npx, cudaMemcpyHostToDevice, t->st_in));
             PT_CUDA(cudaEventRecord(ev_in[b], t->st_in));
             PT_CUDA(cudaStreamWaitEvent(sa, ev_in[b], 0));
-            PT_TRY(pt_launch_descriptor_rows(p.ndims, p.nchroma, t->q_rgb.p, h, w, p.convert_colorspace, t->q_rgba.p,
+            PT_TRY(pt_launch_descriptor_rows(p.ndims, p.nchroma, t->q_rgb.p, h, w, pt_color_mode(p), t->q_rgba.p,
                                              t->q_desc.p, t->ds, r0 / 8, (r1 - r0 + 7) / 8, sa));
             const size_t o = (size_t) r0 * ew;
             const long long n = (long long) (r1 - r0) * ew;
@@ -958,7 +958,7 @@ pt_status load_impl(const pt_params *pin, const char *filename, pt_table **out) 
         PT_CUDA(rgb.reserve(b0.size()));
         PT_CUDA(cudaMemcpyAsync(rgb.p, b0.data(), sizeof(float) * b0.size(), cudaMemcpyHostToDevice, t->st));
         PT_CUDA(t->b_rgba.reserve((size_t) h * w));
-        PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, rgb.p, h, w, p.convert_colorspace, t->b_rgba.p, nullptr, t->ds, t->st));
+        PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, rgb.p, h, w, pt_color_mode(p), t->b_rgba.p, nullptr, t->ds, t->st));
         std::vector<float> packed((size_t) P * t->ds, 0.0f);
         for (int y = 0; y < t->eh; y++)
             for (int x = 0; x < t->ew; x++)
@@ -1158,7 +1158,7 @@ pt_status pt_table_proposal_samples(pt_table *t, const float *d_a, int h, int w,
     PtTableView v;
     PT_TRY(pt_table_view(t, &v));
     PT_TRY(pt_prop_check_table(v));
-    PT_TRY(pt_launch_descriptor(t->p.ndims, t->p.nchroma, d_a, h, w, t->p.convert_colorspace, nullptr, t->q_desc.p, t->ds,
+    PT_TRY(pt_launch_descriptor(t->p.ndims, t->p.nchroma, d_a, h, w, pt_color_mode(t->p), nullptr, t->q_desc.p, t->ds,
                                 st));
     return pt_launch_prop_samples(v, t->q_desc.p, (int) P, d_ann, X, labels, st);
 }
@@ -1172,7 +1172,7 @@ pt_status pt_table_proposal_infer(pt_table *t, pt_proposal *net, const float *d_
     PT_TRY(ensure_query_buffers(t, h, w));
     PtTableView v;
     PT_TRY(pt_table_view(t, &v));
-    PT_TRY(pt_launch_descriptor(t->p.ndims, t->p.nchroma, d_a, h, w, t->p.convert_colorspace, nullptr, t->q_desc.p, t->ds,
+    PT_TRY(pt_launch_descriptor(t->p.ndims, t->p.nchroma, d_a, h, w, pt_color_mode(t->p), nullptr, t->q_desc.p, t->ds,
                                 st));
     PT_TRY(pt_launch_prop_infer(v, net, t->q_desc.p, (int) P, cand, conf, logits, st));
     return pt_prop_check_error(net, st);
@@ -1267,7 +1267,7 @@ pt_status pt_descriptor(const pt_params *p, const float *rgb, int h, int w, floa
     PT_CUDA(d_rgb.reserve((size_t) h * w * 3));
     PT_CUDA(d_desc.reserve((size_t) P * ds));
     PT_CUDA(cudaMemcpy(d_rgb.p, rgb, sizeof(float) * (size_t) h * w * 3, cudaMemcpyHostToDevice));
-    PT_TRY(pt_launch_descriptor(p->ndims, p->nchroma, d_rgb.p, h, w, p->convert_colorspace, nullptr, d_desc.p, ds, 0));
+    PT_TRY(pt_launch_descriptor(p->ndims, p->nchroma, d_rgb.p, h, w, pt_color_mode(*p), nullptr, d_desc.p, ds, 0));
     std::vector<float> tmp((size_t) P * ds);
     PT_CUDA(cudaMemcpy(tmp.data(), d_desc.p, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost));
     for (long long i = 0; i < P; i++)

@@ -37,6 +37,7 @@ CASES = [
          switches="-limit 2 -ndims 3 -coherence_spatial 4 -dt_algo euclidean"),
     dict(name="ntables3_90x60", h=60, w=90, seed=19, switches="-limit 1 -ntables 3 -coherence_spatial 2"),
     dict(name="ntables2_ratio4_k3_70x80", h=80, w=70, seed=20, switches="-limit 0.5 -ntables 2 -table_ratio 4 -kcoherence 3"),
+    dict(name="lab_100x80_k2", h=80, w=100, seed=24, switches="-limit 1 -colorspace lab -kcoherence 2"),
 ]
 C2 = dict(name="c2_1920x1080_coh4", h=1080, w=1920, seed=2, switches="-speed 3 -coherence_spatial 4")
 # Descriptor mode (is_descriptor): synth.descriptor_pair inputs.  Three channels are left out: the

@@ -36,11 +36,12 @@ def _masks():
     return gen.masks(16)
 
 
-def exact_descriptor(oracle, img, ndims, nchroma, convert=True):
-    """float64 descriptor of every full patch, from the oracle's (bit-exact) YUV image, and the
-    sum of |terms| of each projection."""
+def exact_descriptor(oracle, img, ndims, nchroma, convert=True, lab=False):
+    """float64 descriptor of every full patch, from the oracle's (bit-exact) YUV or Lab image,
+    and the sum of |terms| of each projection."""
     from numpy.lib.stride_tricks import sliding_window_view
-    yuv = (oracle.rgb2yuv(img) if convert else img).astype(np.float64)
+    conv = oracle.rgb2lab if lab else oracle.rgb2yuv
+    yuv = (conv(img) if convert else img).astype(np.float64)
     H, W, _ = yuv.shape
     win = sliding_window_view(yuv, (8, 8), axis=(0, 1))[:H - 7, :W - 7]
     ms = _masks()
@@ -58,12 +59,13 @@ def exact_descriptor(oracle, img, ndims, nchroma, convert=True):
 
 
 @pytest.mark.parametrize("h,w,sw", [(240, 320, ""), (53, 37, "-ndims 8"), (8, 8, "-ndims 7"), (9, 200, "-colorspace rgb"),
-                                    (71, 66, "-ndims 4 -nchroma 0"), (130, 90, "-ndims 12 -nchroma 1")])
+                                    (71, 66, "-ndims 4 -nchroma 0"), (130, 90, "-ndims 12 -nchroma 1"),
+                                    (90, 120, "-colorspace lab"), (64, 70, "-colorspace lab -ndims 8")])
 def test_descriptor_accuracy(gpu, oracle, h, w, sw):
     _, b = synth.pair(h, w, 3)
     p = ptb.PatchTableParams(sw)
     got = ptb.descriptor(p, b).astype(np.float64)
-    ex, mag = exact_descriptor(oracle, b, p.ndims, p.nchroma, convert=p.convert_colorspace)
+    ex, mag = exact_descriptor(oracle, b, p.ndims, p.nchroma, convert=p.convert_colorspace, lab=p.colorspace == 1)
     orc = oracle.descriptor(p.as_dict(), b)[7:h, 7:w].astype(np.float64)
     tol = DESC_TOL * mag + 1e-30
     assert (np.abs(got - ex) <= tol).all()

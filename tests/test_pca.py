@@ -22,7 +22,8 @@ pytestmark = pytest.mark.gpu
 
 CASES = [("-dim_algo pca -limit 1", 120, 160, 11), ("-dim_algo pca -ndims 8 -kcoherence 2 -limit 2", 100, 130, 12),
          ("-dim_algo pca -ndims 4 -pca_subtract_mean 0 -pca_samples 300 -limit 0.5", 90, 70, 13),
-         ("-dim_algo pca -ndims 12 -colorspace rgb -limit 3", 80, 110, 14)]
+         ("-dim_algo pca -ndims 12 -colorspace rgb -limit 3", 80, 110, 14),
+         ("-dim_algo pca -colorspace lab -limit 1", 90, 120, 15)]
 
 
 @pytest.mark.parametrize("sw,h,w,seed", CASES)
