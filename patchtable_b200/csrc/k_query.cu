@@ -653,6 +653,29 @@ __global__ void k_init_temporal(const QPlan q, const double *__restrict__ prev, 
     orig[p] = scaled / temporal_scale;
 }
 
+/* init_random (patchtable.h:3522-3537): a random match per patch with its distance; the match
+   comes from a hash of the patch index instead of two rand() calls. */
+__global__ void k_init_random(const QPlan q, const float4 *__restrict__ a, const float4 *__restrict__ B, int *cur_pos,
+                              float *cur_d) {
+    const int p = blockIdx.x * NT + threadIdx.x;
+    if (p >= q.ew * q.eh) return;
+    const int x = p % q.ew, y = p / q.ew;
+    unsigned hsh = mix32((unsigned) p * 0x9e3779b1u + 0x85ebca6bu);
+    const int xs = (int) (hsh % (unsigned) q.bew);
+    hsh = mix32(hsh ^ 0x27d4eb2fu);
+    const int ys = (int) (hsh % (unsigned) q.beh);
+    float d;
+    if (q.adesc) {
+        float4 v[4];
+        pt_desc_load(q.adesc + (size_t) p * q.ds4, 4 * q.ds4, v);
+        d = pt_desc_dist(v, q.bdesc + ((size_t) ys * q.bew + xs) * q.ds4, q.nd);
+    } else {
+        d = ssd_global(q, a, x, y, B, xs, ys);
+    }
+    cur_pos[p] = pt_xy(xs, ys);
+    cur_d[p] = d;
+}
+
 /* The float64 NNF; a patch whose match and distance are still the initial temporal ones gets the
    unscaled distance back (patchtable.h:4178-4193). */
 __global__ void k_output_temporal(int n, const int *__restrict__ pos, const float *__restrict__ d,
@@ -907,6 +930,16 @@ pt_status pt_launch_init_temporal(const QuerySetup &s, const double *prev, const
 pt_status pt_launch_output_temporal(int n, const int *pos, const float *d, const int *pos0, const float *d0,
                                     const double *orig, double *ann, cudaStream_t st) {
     k_output_temporal<<<(n + NT - 1) / NT, NT, 0, st>>>(n, pos, d, pos0, d0, orig, ann);
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_init_random(const QuerySetup &s, const float4 *a, const float4 *b, int *cur_pos, float *cur_d,
+                                cudaStream_t st) {
+    QPlan q;
+    PT_TRY(make_qplan(s, q));
+    const int n = q.ew * q.eh;
+    k_init_random<<<(n + NT - 1) / NT, NT, 0, st>>>(q, a, b, cur_pos, cur_d);
     PT_LAUNCHED();
     return PT_OK;
 }

@@ -141,6 +141,9 @@ pt_status pt_launch_output(int n, const int *pos, const float *d, double *ann, c
 /* Temporal lookups (ann_prev): initial field from the previous NNF and the final restore of the
    unscaled distance (patchtable.h:3548-3585, 4178-4193); *bad becomes 1 when a previous match lies
    outside the table image and sanitize is off. */
+/* init_random: a hashed random match and its distance per patch. */
+pt_status pt_launch_init_random(const QuerySetup &s, const float4 *a, const float4 *b, int *cur_pos, float *cur_d,
+                                cudaStream_t st);
 pt_status pt_launch_init_temporal(const QuerySetup &s, const double *prev, const float *scale_sv, int recalc, int sanitize,
                                   double temporal_scale, const float4 *a, const float4 *b, int *cur_pos, float *cur_d,
                                   double *orig, int *bad, cudaStream_t st);

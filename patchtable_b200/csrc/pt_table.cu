@@ -161,7 +161,6 @@ pt_status check_params(const pt_params *p, int h, int w) {
     if (p->ntables > 16) return pt_fail(PT_UNSUPPORTED, "ntables %d > 16", p->ntables);
     if (p->run_dt && p->dt_algo != 1 && p->dt_algo != 4 && p->dt_algo != 5 && p->dt_algo != 6)
         return pt_fail(PT_UNSUPPORTED, "dt_algo %d is not implemented on the GPU path", p->dt_algo);
-    if (p->init_random) return pt_fail(PT_UNSUPPORTED, "init_random is not implemented on the GPU path");
     if (p->ndims < 1 || p->ndims > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "ndims %d outside 1..%d", p->ndims, PT_DESC_MAX);
     int G = p->grid_ndims < 0 ? p->ndims : p->grid_ndims;
     if (G < 1 || G > p->ndims) return pt_fail(PT_BAD_ARG, "grid_ndims %d outside 1..ndims", G);
@@ -610,12 +609,16 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     }
     if (qs.radius > 2) qs.radius = 2;
     const double temporal_scale = 1.0 / (1 + p.coherence_temporal);          /* patchtable.h:3488 */
-    if (d_prev) {
+    if (d_prev) {                             /* no bad previous matches so far (read by the host lookup) */
+        PT_CUDA(t->q_tbad.reserve(1));
+        PT_CUDA(cudaMemsetAsync(t->q_tbad.p, 0, sizeof(int), st));
+    }
+    if (p.init_random) {                      /* takes precedence over ann_prev, patchtable.h:3522-3537 */
+        PT_TRY(pt_launch_init_random(qs, t->q_rgba.p, t->b_rgba.p, t->q_pos[0].p, t->q_d[0].p, st));
+    } else if (d_prev) {
         PT_CUDA(t->q_tpos0.reserve(P));
         PT_CUDA(t->q_td0.reserve(P));
         PT_CUDA(t->q_torig.reserve(P));
-        PT_CUDA(t->q_tbad.reserve(1));
-        PT_CUDA(cudaMemsetAsync(t->q_tbad.p, 0, sizeof(int), st));
         PT_TRY(pt_launch_init_temporal(qs, d_prev, d_sv, p.recalc_dist_temporal, p.sanitize_input, temporal_scale,
                                        t->q_rgba.p, t->b_rgba.p, t->q_pos[0].p, t->q_d[0].p, t->q_torig.p, t->q_tbad.p, st));
         PT_CUDA(cudaMemcpyAsync(t->q_tpos0.p, t->q_pos[0].p, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
@@ -656,7 +659,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
             PT_CUDA(cudaMemcpyAsync(t->q_d[cur].p, t->q_chd.p, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
         }
     }
-    if (d_prev && p.coherence_temporal != 0.0)
+    if (d_prev && !p.init_random && p.coherence_temporal != 0.0)
         PT_TRY(pt_launch_output_temporal(n, t->q_pos[cur].p, t->q_d[cur].p, t->q_tpos0.p, t->q_td0.p, t->q_torig.p, d_ann, st));
     else
         PT_TRY(pt_launch_output(n, t->q_pos[cur].p, t->q_d[cur].p, d_ann, st));
@@ -1079,7 +1082,8 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int ih, int iw, double *a
         if (seconds) *seconds = now_s() - T0;
         return PT_OK;
     }
-    if (!t->desc_mode && !t->pca && t->subs.empty() && pt_default_passes(t->p) == 1 && t->p.do_prop && h - 7 >= 64) {
+    if (!t->desc_mode && !t->pca && t->subs.empty() && !t->p.init_random && pt_default_passes(t->p) == 1 && t->p.do_prop &&
+        h - 7 >= 64) {
         PT_TRY(lookup_banded(t, a, h, w, ann_out));
         if (seconds) *seconds = now_s() - T0;
         return PT_OK;
@@ -1255,7 +1259,7 @@ pt_status pt_table_set_params(pt_table *t, const pt_params *p) {
     q.gpu_bands = p->gpu_bands;
     q.do_rs = p->do_rs;
     q.spatial = p->spatial;
-    if (p->init_random) return pt_fail(PT_UNSUPPORTED, "init_random is not implemented on the GPU path");
+    q.init_random = p->init_random;
     return PT_OK;
 }
 
@@ -1298,8 +1302,8 @@ int64_t pt_kernel_launch_count(void) { return g_launches; }
 
 pt_status pt_table_view(const pt_table *t, PtTableView *v) {
     if (!t || !v) return pt_fail(PT_BAD_ARG, "null argument");
-    if (t->desc_mode || t->pca || !t->subs.empty())
-        return pt_fail(PT_UNSUPPORTED, "descriptor mode, PCA and multi-table tables serve pt_table_lookup, "
+    if (t->desc_mode || t->pca || !t->subs.empty() || t->p.init_random)
+        return pt_fail(PT_UNSUPPORTED, "descriptor mode, PCA, multi-table tables and init_random serve pt_table_lookup, "
                                        "pt_table_lookup_device(_temporal) and the profile only");
     v->p = t->p;
     v->h = t->h; v->w = t->w; v->ds = t->ds;

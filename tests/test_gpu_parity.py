@@ -195,6 +195,29 @@ def test_every_speed_preset(gpu, oracle, libc, speed):
     assert mean_dist(ann) <= MEAN_DIST_SLACK * mo, (mean_dist(ann), mo)
 
 
+def test_init_random(gpu, oracle, libc):
+    """init_random (patchtable.h:3522-3537) starts every patch from a random match with its exact
+    distance; the table step and propagation then refine it like the reference's."""
+    a, b = synth.pair(120, 150, 25)
+    p = ptb.PatchTableParams("-limit 2 -init_random 1")
+    srand_all(libc, 1)
+    ot = oracle.build(p.as_dict(), b)
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b)
+    ann = gt.lookup(a)
+    check_nnf(oracle, a, b, ann)
+    srand_all(libc, 2)
+    assert mean_dist(ann) <= MEAN_DIST_SLACK * mean_dist(ot.lookup(a))
+    # without table lookup or propagation the field is the random start itself: exact distances
+    q = ptb.PatchTableParams("-limit 2 -init_random 1 -do_table_lookup 0 -do_prop 0 -kcoherence 0")
+    srand_all(libc, 1)
+    t0 = ptb.PatchTable(q, b)
+    start = t0.lookup(a)
+    check_nnf(oracle, a, b, start)
+    assert np.array_equal(start, t0.lookup(a))          # the hashed start does not depend on rand()
+    assert mean_dist(start) > 2 * mean_dist(ann)
+
+
 def check_nnf(oracle, a, b, ann, sample=4000):
     eh, ew = a.shape[0] - 7, a.shape[1] - 7
     beh, bew = b.shape[0] - 7, b.shape[1] - 7
@@ -280,7 +303,7 @@ def test_constant_image(gpu, libc):
     assert np.allclose(ann[..., 2], 64 * 3 * 0.0625)
 
 
-@pytest.mark.parametrize("sw", ["-init_random 1", "-populate_nearest 0", "-dt_algo raster", "-ntables 17",
+@pytest.mark.parametrize("sw", ["-randomize_dt 1", "-populate_nearest 0", "-dt_algo raster", "-ntables 17",
                                 "-dim_algo pca -pca_mean 1"])
 def test_unsupported_options_fail_loudly(gpu, sw):
     _, b = synth.pair(40, 40, 1)
