@@ -5,11 +5,11 @@
 
    Structure: train points are sorted by a Morton code of their quantised descriptor, cut into
    buckets of 32 consecutive points, and a complete binary tree of axis-aligned bounding boxes is
-   built over the buckets (implicit heap layout, one launch per level).  Each query thread
+   built over the buckets (implicit heap layout, one launch per level).  Each query
    descends the tree depth first, nearer child first, and skips a subtree only when the box's
    lower bound exceeds the current k-th distance by more than the float rounding of a distance
    could account for -- so the result equals an exhaustive search.  Queries are processed in
-   Morton order so the threads of a warp walk similar paths. */
+   Morton order and each warp walks the tree together (k_knn_warp). */
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
@@ -20,15 +20,6 @@ namespace {
 
 constexpr int NT = 128;
 constexpr int BUCKET = 32;
-
-__device__ __forceinline__ float knn_dist(const float *q, const float *p, int nd) {
-    float s = 0.f;
-    for (int i = 0; i < nd; i++) {
-        float t = __fsub_rn(q[i], p[i]);
-        s = __fadd_rn(s, __fmul_rn(t, t));
-    }
-    return s;
-}
 
 __global__ void k_range(const float *__restrict__ pts, int N, int nd, float *mn, float *mx) {
     __shared__ float smin[PT_DESC_MAX][NT], smax[PT_DESC_MAX][NT];
@@ -99,7 +90,7 @@ __global__ void k_inner_box(int first, int count, int nd, float *lo, float *hi) 
     }
 }
 
-/* Squared distance from q to a box, rounded down enough to be a lower bound of knn_dist. */
+/* Squared distance from q to a box, rounded down enough to be a lower bound of the squared distance. */
 __device__ __forceinline__ float box_lb(const float *q, const float *lo, const float *hi, int nd) {
     float s = 0.f;
     for (int d = 0; d < nd; d++) {
@@ -111,51 +102,100 @@ __device__ __forceinline__ float box_lb(const float *q, const float *lo, const f
 
 __device__ __forceinline__ bool before(float d, int i, float d2, int i2) { return d < d2 || (d == d2 && i < i2); }
 
+/* The search, with the 32 queries of a warp walking the tree together: a node is opened
+   when any lane's lower bound admits it, the traversal stack is shared by the warp, and a
+   leaf's points are staged once in shared memory and read back by every lane as broadcasts.
+   The lanes' paths through the tree are nearly the same (queries in Morton order), so the warp
+   does the union of its lanes' work without divergence.  Lanes score only leaves their own bound
+   admits, with the same rounding and tie rule, so the result equals the per-thread search. */
+constexpr int KNN_STACK = 64;
+constexpr int PSTRIDE = PT_DESC_MAX + 1;            /* staged point stride (odd: no bank conflicts) */
+
 template<int K>
 __global__ void __launch_bounds__(NT)
-k_knn_tree(const float *__restrict__ sp, const int *__restrict__ sidx, int N, int nd, int L,
+k_knn_warp(const float *__restrict__ sp, const int *__restrict__ sidx, int N, int nd, int L,
            const float *__restrict__ lo, const float *__restrict__ hi, const float *__restrict__ qdesc,
            const int *__restrict__ qorder, int Q, int *out) {
-    int t = blockIdx.x * NT + threadIdx.x;
-    if (t >= Q) return;
-    int q = qorder[t];
+    __shared__ int stk_s[NT / 32][KNN_STACK];
+    __shared__ float pts_s[NT / 32][BUCKET * PSTRIDE];
+    __shared__ int pid_s[NT / 32][BUCKET];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int t = blockIdx.x * NT + threadIdx.x;
+    const bool active = t < Q;
+    const int q = active ? qorder[t] : 0;
     float qv[PT_DESC_MAX];
-    for (int d = 0; d < nd; d++) qv[d] = qdesc[(size_t) q * nd + d];
+#pragma unroll
+    for (int d = 0; d < PT_DESC_MAX; d++) qv[d] = (active && d < nd) ? qdesc[(size_t) q * nd + d] : 0.f;
     float kd[K];
     int ki[K];
 #pragma unroll
     for (int j = 0; j < K; j++) { kd[j] = __int_as_float(0x7f800000); ki[j] = 0x7fffffff; }
-    int stack[48];
-    int sp_top = 0;
-    stack[sp_top++] = 1;
-    while (sp_top > 0) {
-        int node = stack[--sp_top];
-        if (box_lb(qv, lo + (size_t) node * nd, hi + (size_t) node * nd, nd) > kd[K - 1]) continue;
+    int *stk = stk_s[wid];
+    float *pts = pts_s[wid];
+    int *pid = pid_s[wid];
+    if (lane == 0) stk[0] = 1;
+    __syncwarp();
+    int top = 1;
+    while (top > 0) {
+        const int node = stk[--top];
+        __syncwarp();
+        const float lb = active ? box_lb(qv, lo + (size_t) node * nd, hi + (size_t) node * nd, nd) : 0.f;
+        const bool want = active && !(lb > kd[K - 1]);
+        if (!__any_sync(FULL, want)) continue;
         if (node >= L) {
-            int j = node - L;
-            int i1 = min(N, (j + 1) * BUCKET);
-            for (int i = j * BUCKET; i < i1; i++) {
-                float d = knn_dist(qv, sp + (size_t) i * nd, nd);
-                int id = sidx[i];
-                if (!before(d, id, kd[K - 1], ki[K - 1])) continue;
+            const int base = (node - L) * BUCKET;
+            const int cnt = min(BUCKET, N - base);
+            if (lane < cnt) {
+                const float *src = sp + (size_t) (base + lane) * nd;
+                for (int d = 0; d < nd; d++) pts[lane * PSTRIDE + d] = src[d];
+                pid[lane] = sidx[base + lane];
+            }
+            __syncwarp();
+            if (want) {
+                for (int m = 0; m < cnt; m++) {
+                    const float *pv = pts + m * PSTRIDE;
+                    float dsum = 0.f;
 #pragma unroll
-                for (int s = K - 1; s >= 0; s--) {
-                    if (before(d, id, kd[s], ki[s])) {
-                        if (s > 0 && before(d, id, kd[s - 1], ki[s - 1])) { kd[s] = kd[s - 1]; ki[s] = ki[s - 1]; }
-                        else { kd[s] = d; ki[s] = id; }
+                    for (int d = 0; d < PT_DESC_MAX; d++) {
+                        if (d < nd) {
+                            const float e = __fsub_rn(qv[d], pv[d]);
+                            dsum = __fadd_rn(dsum, __fmul_rn(e, e));
+                        }
+                    }
+                    const int id = pid[m];
+                    if (!before(dsum, id, kd[K - 1], ki[K - 1])) continue;
+#pragma unroll
+                    for (int s2 = K - 1; s2 >= 0; s2--) {
+                        if (before(dsum, id, kd[s2], ki[s2])) {
+                            if (s2 > 0 && before(dsum, id, kd[s2 - 1], ki[s2 - 1])) { kd[s2] = kd[s2 - 1]; ki[s2] = ki[s2 - 1]; }
+                            else { kd[s2] = dsum; ki[s2] = id; }
+                        }
                     }
                 }
             }
+            __syncwarp();                        /* the next leaf restages the points */
             continue;
         }
-        int c0 = 2 * node, c1 = 2 * node + 1;
-        float l0 = box_lb(qv, lo + (size_t) c0 * nd, hi + (size_t) c0 * nd, nd);
-        float l1 = box_lb(qv, lo + (size_t) c1 * nd, hi + (size_t) c1 * nd, nd);
-        if (sp_top + 2 > 48) continue;           /* cannot happen: depth <= 31 */
-        if (l0 <= l1) { stack[sp_top++] = c1; stack[sp_top++] = c0; }
-        else { stack[sp_top++] = c0; stack[sp_top++] = c1; }
+        const int c0 = 2 * node, c1 = 2 * node + 1;
+        float l0 = 0.f, l1 = 0.f;
+        if (want) {
+            l0 = box_lb(qv, lo + (size_t) c0 * nd, hi + (size_t) c0 * nd, nd);
+            l1 = box_lb(qv, lo + (size_t) c1 * nd, hi + (size_t) c1 * nd, nd);
+        }
+        float s0 = l0, s1 = l1;                   /* nearer child (for the warp) first */
+#pragma unroll
+        for (int o = 16; o; o >>= 1) { s0 += __shfl_xor_sync(FULL, s0, o); s1 += __shfl_xor_sync(FULL, s1, o); }
+        if (top + 2 > KNN_STACK) continue;        /* cannot happen: depth <= 31 */
+        if (lane == 0) {
+            if (s0 <= s1) { stk[top] = c1; stk[top + 1] = c0; }
+            else { stk[top] = c0; stk[top + 1] = c1; }
+        }
+        __syncwarp();
+        top += 2;
     }
-    for (int j = 0; j < K; j++) out[(size_t) q * K + j] = ki[j] == 0x7fffffff ? -1 : ki[j];
+    if (active)
+        for (int j = 0; j < K; j++) out[(size_t) q * K + j] = ki[j] == 0x7fffffff ? -1 : ki[j];
 }
 
 }  // namespace
@@ -224,9 +264,9 @@ pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, i
     }
     dim3 grid((Q + NT - 1) / NT);
     switch (K) {
-        case 16: k_knn_tree<16><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
-        case 32: k_knn_tree<32><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
-        case 64: k_knn_tree<64><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
+        case 16: k_knn_warp<16><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
+        case 32: k_knn_warp<32><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
+        case 64: k_knn_warp<64><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
         default: return pt_fail(PT_UNSUPPORTED, "knn K=%d", K);
     }
     PT_LAUNCHED();
