@@ -532,8 +532,11 @@ pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const fl
     count_work(counters, ne, rows);
 }
 
+/* At most 14 x 64 threads' worth of CTAs per SM (73 registers, 10 bytes of spills): the pull is
+   latency-bound, and the extra resident warps hide the gathers (measured at 1080p with one
+   candidate per patch: 0.341 -> 0.286 ms; at 16 x 64 the spills grow to 200 bytes and it slows). */
 template<int TW, int R, bool DESC>
-__global__ void __launch_bounds__(TW)
+__global__ void __launch_bounds__(TW, (14 * 64) / TW)
 k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
             const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
             int *nxt_pos, float *nxt_d, unsigned long long *counters) {
@@ -580,7 +583,7 @@ k_choose_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, l
 }
 
 template<int TW, int R>
-__global__ void __launch_bounds__(TW)
+__global__ void __launch_bounds__(TW, (14 * 64) / TW)
 k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, long long nseg, int twi,
              const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
              const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
