@@ -150,11 +150,15 @@ __device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, c
             }
         }
         float4 *dst = reinterpret_cast<float4 *>(desc + ((size_t) py * ew + px) * ds);
-        for (int q = 0; q < ds / 4; q++) dst[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
+#pragma unroll
+        for (int q = 0; q < PT_DESC_MAX / 4; q++)
+            if (q < ds / 4) dst[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
     }
 }
 
-__global__ void __launch_bounds__(NT)
+/* Four CTAs per SM (64 registers; shared memory sized to the plan's filters): the kernel is
+   issue-bound and the extra warps fill the barrier gaps (0.105 -> 0.093 ms at 1080p). */
+__global__ void __launch_bounds__(NT, 4)
 k_descriptor(const DescPlan c_plan, const float *__restrict__ rgb, int h, int w, int convert,
              float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh, int ew, int ty0) {
     extern __shared__ float smem[];
@@ -287,9 +291,9 @@ pt_status pt_launch_descriptor_rows(int ndims, int nchroma, const float *rgb, in
     PT_TRY(make_plan(ndims, nchroma, plan));
     if (eh < 1 || ew < 1) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
     static bool attr = false;
-    size_t smem = pt_descriptor_smem(0);
+    size_t smem = sizeof(float) * (3 * RH * RWP + plan.ncombo * RH * TW);
     if (!attr) {
-        PT_CUDA(cudaFuncSetAttribute(k_descriptor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        PT_CUDA(cudaFuncSetAttribute(k_descriptor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) pt_descriptor_smem(0)));
         attr = true;
     }
     const int ntr = (eh + TH - 1) / TH;
