@@ -8,7 +8,7 @@ the reference's default parameters plus -speed 3 -coherence_spatial 4.  One step
 built once before warm-up.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-  python bench.py --profile-case query|query-default|infer     (short fixed runs for ncu)
+  python bench.py --profile-case query|query-default|infer|build  (short fixed runs for ncu)
 
 Prints one JSON line (rank 0).  `value` is query patches per second of device time with a already
 in device memory (L2 flushed between steps) at the fastest query schedule whose mean NNF distance
@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
-    ap.add_argument("--profile-case", choices=["query", "query-default", "infer"], default=None)
+    ap.add_argument("--profile-case", choices=["query", "query-default", "infer", "build"], default=None)
     return ap.parse_args()
 
 
@@ -198,6 +198,13 @@ def profile_case(name):
     from patchtable_b200 import synth
     ctypes.CDLL(None).srand(1)
     st = torch.cuda.current_stream().cuda_stream
+    if name == "build":
+        h, w = 540, 960
+        a, b = synth.pair(h, w, 2)
+        t = ptb.PatchTable(ptb.PatchTableParams(WORKLOAD["switches"]), b)
+        torch.cuda.synchronize()
+        print("profile case build: %d cells" % t.shape()[1])
+        return
     if name in ("query", "query-default"):
         a, b = make_inputs()
         H, W = a.shape[:2]
