@@ -118,3 +118,15 @@ def test_atlas_with_allowed_patches(gpu, oracle, libc):
     assert mean_dist(ann) <= MEAN_DIST_SLACK * mean_dist(ot.lookup(a))
     qb_ann = gt.lookup_batch([a])[0]
     assert np.array_equal(qb_ann, ann)
+
+
+@pytest.mark.parametrize("sw", ["-speed 3 -coherence_spatial 4 -limit 2 -colorspace lab",
+                                "-speed 3 -limit 2 -colorspace rgb -spatial 1"])
+def test_batch_other_colour_spaces_and_search(gpu, libc, sw):
+    """The batched descriptor and choose kernels follow the table's colour space and search
+    options exactly as the single-image query does."""
+    t, b = _table(libc, sw)
+    imgs = _queries(500)[:4]
+    single = [t.lookup(x) for x in imgs]
+    for s, h in zip(single, t.lookup_batch(imgs)):
+        assert np.array_equal(s, h)

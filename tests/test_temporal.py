@@ -65,3 +65,15 @@ def test_per_patch_scale_and_sanitize(gpu, oracle, libc):
         t.lookup(a, ann_prev=bad)
     with pytest.raises(ptb.PatchTableError):
         t.lookup(a, ann_prev=prev[:-1])
+
+
+def test_temporal_with_multiple_tables(gpu, libc):
+    """ann_prev seeding composes with further tables: the seeded lookup never ends worse than its
+    seed and its distances are exact."""
+    a, b = synth.pair(120, 150, 88)
+    p = ptb.PatchTableParams("-limit 2 -ntables 3 -coherence_temporal 0")
+    libc.srand(1)
+    t = ptb.PatchTable(p, b)
+    first = t.lookup(a)
+    again = t.lookup(a, ann_prev=first)
+    assert (again[..., 2] <= first[..., 2]).all()
