@@ -46,7 +46,7 @@ typedef struct {
     int nslices[16], n_nslices;       /* explicit -nslices, n_nslices == 0 means automatic */
     int partition_step;
     int populate_random;
-    int run_dt, dt_algo, dt_iters;    /* dt_algo: 1 prop, 4 downsample, 5 hybrid, 6 euclidean */
+    int run_dt, dt_algo, dt_iters;    /* dt_algo: 1 prop, 2 brute, 4 downsample, 5 hybrid, 6 euclidean */
     int kcoherence, kcoherence_min_dist, kcoherence_step, kcoherence_iter;
     int flann_reset_step, flann_build_step;
     double triangle_factor;
@@ -455,9 +455,13 @@ void dt_prop1(Table &t);
 void dt_unmask(Table &t);
 void dt_downsample(Table &t);
 void dt_euclidean(Table &t);
+void dt_brute(Table &t);
 
 /* PatchTableFixedN constructor, patchtable.h:2584-3373, default path (no product quantisation,
-   no k-means, populate_nearest with TABLE_POPULATE_FAST, single table). */
+   no k-means, TABLE_POPULATE_FAST).  With TABLE_POPULATE_FAST (patchtable.h:37) populate never
+   reaches add_patch (patchtable.h:3127-3159), so populate_nearest has no effect and randomize_dt
+   collects no adjacency: do_after_dt (patchtable.h:1831-1866) finds every set empty and changes
+   no cell.  Neither switch is read here. */
 Table *build(const orc_params &p, const float *b, int h, int w, const int32_t *allowed, const float *wh0_in) {
     const int h_in = h, w_in = w;
     Table *t = new Table();
@@ -598,6 +602,7 @@ Table *build(const orc_params &p, const float *b, int h, int w, const int32_t *a
     bool zeros_filled = false;
     if (p.run_dt) {
         if (p.dt_algo == 1) { dt_prop(*t); zeros_filled = (p.dt_iters <= 0); }
+        else if (p.dt_algo == 2) { dt_brute(*t); zeros_filled = true; }
         else if (p.dt_algo == 4) { dt_downsample(*t); zeros_filled = true; }
         else if (p.dt_algo == 5) { dt_prop1(*t); dt_downsample(*t); dt_unmask(*t); zeros_filled = true; }
         else if (p.dt_algo == 6) { dt_euclidean(*t); zeros_filled = true; }
@@ -814,6 +819,39 @@ void dt_euclidean(Table &t) {
             }
             for (int q = 0; q < n; q++) { dist[base + q * st] = dd[q]; t.table[base + q * st] = idx[q]; }
         }
+    }
+}
+
+/* do_dt_brute, patchtable.h:2364-2413: every cell takes, over the whole valid patch region of b
+   (the allowed mask is not consulted), the patch nearest the cell under patch_dist_to_grid<0>
+   (patchtable.h:1403-1425) with TABLE_INFINITY_NORM: the largest over grid dimensions of
+   |wh - centre| / (rsize when wh - centre > 0, else lsize), maxima taken as (a > b ? a : b).
+   The first patch in raster order seeds the search and a later one replaces it only when
+   strictly nearer, so ties keep the earliest. */
+void dt_brute(Table &t) {
+    const int G = t.gnd;
+    vector<int> gi(G);
+    for (int64_t j = 0; j < t.ncells; j++) {
+        for (int i = 0; i < G; i++) gi[i] = (int) ((j / t.stride[i]) % t.nslices[i]);
+        auto dist = [&](int x, int y) {
+            float ans = 0;
+            for (int i = 0; i < G; i++) {
+                const Partition1D &P = t.part[i];
+                float delta = t.whv(y, x, i) - P.centers[gi[i]];
+                float sz = delta > 0 ? P.rsizes[gi[i]] : P.lsizes[gi[i]];
+                delta = std::fabs(delta) / sz;
+                ans = ans > delta ? ans : delta;
+            }
+            return ans;
+        };
+        int xb = PW - 1, yb = PW - 1;
+        float db = dist(xb, yb);
+        for (int y = PW - 1; y < t.h; y++)
+            for (int x = PW - 1; x < t.w; x++) {
+                float d = dist(x, y);
+                if (d < db) { db = d; xb = x; yb = y; }
+            }
+        t.table[j] = xy_to_int(xb, yb);
     }
 }
 

@@ -7,6 +7,7 @@
      get_bin                  :1298-1325
      populate (fast, random)  :3121-3159
      do_dt_prop               :2081-2165  (edge labels PropEdge :1435-1447)
+     do_dt_brute              :2364-2413  (patch_dist_to_grid :1403-1425)
 
    The DT is the reference's breadth-first fill, run level-synchronously: in each level every
    frontier element claims the unused neighbours its label allows with atomicMin on
@@ -595,6 +596,60 @@ __global__ void k_edt_line(int *table, const float *__restrict__ fin, float *fou
 #undef F
 }
 
+/* do_dt_brute (patchtable.h:2364-2413): every cell takes the patch of b nearest its grid centre
+   under patch_dist_to_grid<0> with TABLE_INFINITY_NORM (patchtable.h:1403-1425),
+   max_d |wh_d - centre_d| / (rsize_d if wh_d - centre_d > 0 else lsize_d), over the whole valid
+   patch region in raster order (the allowed mask is not consulted); patch 0 seeds the search and
+   only a strictly smaller distance replaces it, so ties keep the earliest patch.  One thread per
+   cell, descriptors streamed through shared memory in tiles that every thread of the CTA reads
+   (broadcast loads).  The arithmetic is the reference's single-precision sequence: IEEE
+   subtract and divide, maxima as (a > b ? a : b), so a NaN from a zero-width cell behaves as it
+   does there.  Work is cells x patches x G: a validation algorithm, as in the reference. */
+struct BrutePart {
+    int ofs[PT_DESC_MAX];     /* per dimension: centres at ofs, lsizes at ofs + n, rsizes at ofs + 2n */
+};
+
+constexpr int BRUTE_TILE = 128;
+
+template<int G>
+__global__ void __launch_bounds__(NT) k_dt_brute(int *table, const GridShape s, const BrutePart bp,
+                                                 const float *__restrict__ part, const float *__restrict__ desc,
+                                                 int ds, long long P, int ew) {
+    __shared__ float tile[BRUTE_TILE * G];
+    const long long j = blockIdx.x * (long long) NT + threadIdx.x;
+    const bool live = j < s.n;
+    float c[G], lo[G], hi[G];
+#pragma unroll
+    for (int d = 0; d < G; d++) {
+        const int n = s.size[d];
+        const int g = live ? (int) ((j / s.stride[d]) % n) : 0;
+        c[d] = part[bp.ofs[d] + g];
+        lo[d] = part[bp.ofs[d] + n + g];
+        hi[d] = part[bp.ofs[d] + 2 * n + g];
+    }
+    float best = 0.f;
+    long long bestp = 0;
+    for (long long base = 0; base < P; base += BRUTE_TILE) {
+        const int m = (int) (P - base < BRUTE_TILE ? P - base : BRUTE_TILE);
+        __syncthreads();
+        for (int k = threadIdx.x; k < m * G; k += NT) tile[k] = desc[(base + k / G) * ds + k % G];
+        __syncthreads();
+        if (!live) continue;
+        for (int q = 0; q < m; q++) {
+            float ans = 0.f;
+#pragma unroll
+            for (int d = 0; d < G; d++) {
+                const float delta = __fsub_rn(tile[q * G + d], c[d]);
+                const float v = __fdiv_rn(fabsf(delta), delta > 0.f ? hi[d] : lo[d]);
+                ans = ans > v ? ans : v;
+            }
+            if (base + q == 0) best = ans;
+            else if (ans < best) { best = ans; bestp = base + q; }
+        }
+    }
+    if (live) table[j] = pt_xy((int) (bestp % ew) + 7, (int) (bestp / ew) + 7);
+}
+
 }  // namespace
 
 pt_status pt_dt_other(int *table, int G, const int *nslices, int dt_algo, cudaStream_t st) {
@@ -656,4 +711,22 @@ pt_status pt_dt_other(int *table, int G, const int *nslices, int dt_algo, cudaSt
         return PT_OK;
     }
     return pt_fail(PT_UNSUPPORTED, "dt_algo %d is not implemented on the GPU path", dt_algo);
+}
+
+pt_status pt_dt_brute(int *table, int G, const int *nslices, const float *part, const int *part_ofs, const float *desc,
+                      int ds, long long P, int ew, cudaStream_t st) {
+    if (G < 1 || G > PT_DESC_MAX) return pt_fail(PT_BAD_ARG, "grid dims %d outside 1..%d", G, PT_DESC_MAX);
+    if (P < 1 || ew < 1) return pt_fail(PT_BAD_ARG, "brute distance transform over %lld patches", P);
+    const GridShape s = grid_shape(G, nslices);
+    BrutePart bp;
+    for (int d = 0; d < PT_DESC_MAX; d++) bp.ofs[d] = d < G ? part_ofs[d] : 0;
+    switch (G) {
+#define PT_BRUTE_CASE(g) case g: k_dt_brute<g><<<blocks_for(s.n), NT, 0, st>>>(table, s, bp, part, desc, ds, P, ew); break;
+        PT_BRUTE_CASE(1) PT_BRUTE_CASE(2) PT_BRUTE_CASE(3) PT_BRUTE_CASE(4) PT_BRUTE_CASE(5) PT_BRUTE_CASE(6)
+        PT_BRUTE_CASE(7) PT_BRUTE_CASE(8) PT_BRUTE_CASE(9) PT_BRUTE_CASE(10) PT_BRUTE_CASE(11) PT_BRUTE_CASE(12)
+        PT_BRUTE_CASE(13) PT_BRUTE_CASE(14) PT_BRUTE_CASE(15) PT_BRUTE_CASE(16)
+#undef PT_BRUTE_CASE
+    }
+    PT_LAUNCHED();
+    return PT_OK;
 }

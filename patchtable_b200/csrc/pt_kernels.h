@@ -65,6 +65,11 @@ pt_status pt_dt_prop(int *table, long long ncells, const int *order_xy, int G, c
 /* dt_algo 4 downsample, 5 hybrid (prop1 + downsample + unmask), 6 euclidean on a table whose
    populated cells hold packed positions. */
 pt_status pt_dt_other(int *table, int G, const int *nslices, int dt_algo, cudaStream_t st);
+/* dt_algo 2 brute: every cell takes the nearest of the P patches of the descriptor store (ds floats
+   per patch, ew patches per row) under the partition's infinity norm; part / part_ofs hold each
+   grid dimension's centres, lsizes and rsizes. */
+pt_status pt_dt_brute(int *table, int G, const int *nslices, const float *part, const int *part_ofs, const float *desc,
+                      int ds, long long P, int ew, cudaStream_t st);
 pt_status pt_launch_replace(int *table, long long n, int from, int to, cudaStream_t st);
 
 /* k_kcoh.cu */

@@ -156,10 +156,11 @@ pt_status check_params(const pt_params *p, int h, int w) {
     if (p->lookup_algo != 0) return pt_fail(PT_UNSUPPORTED, "only lookup_algo table is implemented on the GPU path");
     if (p->kcoherence && p->kcoherence_algo != 0) return pt_fail(PT_UNSUPPORTED, "only kcoherence_algo flann (exact search) is implemented");
     if (p->incoherence) return pt_fail(PT_UNSUPPORTED, "incoherence is not implemented on the GPU path");
-    if (p->randomize_dt) return pt_fail(PT_UNSUPPORTED, "randomize_dt is not implemented on the GPU path");
-    if (!p->populate_nearest) return pt_fail(PT_UNSUPPORTED, "populate_nearest 0 is not implemented on the GPU path");
+    /* randomize_dt and populate_nearest change nothing in the reference's build: with
+       TABLE_POPULATE_FAST (patchtable.h:37) populate never calls add_patch (patchtable.h:3127-3159),
+       so no adjacency is collected and do_after_dt (patchtable.h:1831-1866) keeps every cell. */
     if (p->ntables > 16) return pt_fail(PT_UNSUPPORTED, "ntables %d > 16", p->ntables);
-    if (p->run_dt && p->dt_algo != 1 && p->dt_algo != 4 && p->dt_algo != 5 && p->dt_algo != 6)
+    if (p->run_dt && p->dt_algo != 1 && p->dt_algo != 2 && p->dt_algo != 4 && p->dt_algo != 5 && p->dt_algo != 6)
         return pt_fail(PT_UNSUPPORTED, "dt_algo %d is not implemented on the GPU path", p->dt_algo);
     if (p->ndims < 1 || p->ndims > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "ndims %d outside 1..%d", p->ndims, PT_DESC_MAX);
     int G = p->grid_ndims < 0 ? p->ndims : p->grid_ndims;
@@ -461,7 +462,11 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
         bool prop = p.run_dt && p.dt_algo == 1;
         PT_TRY(pt_dt_prop(t->table.p, t->ncells, d_order.p, t->G, t->nslices.data(), t->stride.data(), p.dt_iters,
                           prop, &t->add_count, &t->dt_levels, t->st));
-        if (p.run_dt && !prop) PT_TRY(pt_dt_other(t->table.p, t->G, t->nslices.data(), p.dt_algo, t->st));
+        if (p.run_dt && p.dt_algo == 2)
+            PT_TRY(pt_dt_brute(t->table.p, t->G, t->nslices.data(), t->part_dev.p, t->part_ofs, t->b_desc.p, t->ds, P, t->ew,
+                               t->st));
+        else if (p.run_dt && !prop)
+            PT_TRY(pt_dt_other(t->table.p, t->G, t->nslices.data(), p.dt_algo, t->st));
         bool zeros_filled = p.run_dt && (!prop || p.dt_iters <= 0);
         if (!zeros_filled) {                                  /* fill_zeros, patchtable.h:2063-2079 */
             int vfill = pt_xy(7, 7);

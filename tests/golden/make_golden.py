@@ -38,6 +38,10 @@ CASES = [
     dict(name="ntables3_90x60", h=60, w=90, seed=19, switches="-limit 1 -ntables 3 -coherence_spatial 2"),
     dict(name="ntables2_ratio4_k3_70x80", h=80, w=70, seed=20, switches="-limit 0.5 -ntables 2 -table_ratio 4 -kcoherence 3"),
     dict(name="lab_100x80_k2", h=80, w=100, seed=24, switches="-limit 1 -colorspace lab -kcoherence 2"),
+    dict(name="dt_brute_80x60", h=60, w=80, seed=25, switches="-limit 0.003 -dt_algo brute -coherence_spatial 2"),
+    dict(name="dt_brute_g2_70x50", h=50, w=70, seed=26, switches="-limit 0.0008 -grid_ndims 2 -dt_algo brute"),
+    # The same pair and switches as tiny_64x48: both options leave the reference's table unchanged.
+    dict(name="noop_switches_64x48", h=48, w=64, seed=11, switches="-limit 1 -randomize_dt 1 -populate_nearest 0"),
 ]
 C2 = dict(name="c2_1920x1080_coh4", h=1080, w=1920, seed=2, switches="-speed 3 -coherence_spatial 4")
 # Descriptor mode (is_descriptor): synth.descriptor_pair inputs.  Three channels are left out: the
@@ -117,6 +121,7 @@ def vidpair0(ref: Reference) -> dict:
 
 def main():
     ref = Reference()
+    ref.set_threads(1)          # do_dt_brute shares one grid_index vector across its OpenMP loop (patchtable.h:2370-2376)
     res = {"cases": [run_case(ref, c) for c in CASES]}
     res["desc"] = [run_desc_case(ref, c) for c in DESC_CASES]
     res["c2"] = run_case(ref, C2, full=False)

@@ -129,6 +129,43 @@ def test_other_distance_transforms(gpu, oracle, libc, algo, sw, h, w, seed, mask
     check_nnf(oracle, a, b, ann)
 
 
+BRUTE_CASES = [("-limit 0.002", 60, 90, 21, False), ("-limit 0.004 -ndims 8", 43, 71, 5, True),
+               ("-limit 0.0005 -grid_ndims 2", 40, 60, 6, False), ("-limit 0.003 -nchroma 0 -ndims 5", 50, 50, 8, True),
+               ("-limit 0.01 -grid_ndims 7 -ndims 7", 80, 100, 9, False)]
+
+
+@pytest.mark.parametrize("sw,h,w,seed,masked", BRUTE_CASES)
+def test_brute_distance_transform(gpu, oracle, libc, sw, h, w, seed, masked):
+    """dt_algo brute: each cell's nearest patch under the partition's infinity norm equals the
+    oracle's bit for bit (the oracle is pinned to the reference directly and by golden digests)."""
+    a, b = synth.pair(h, w, seed)
+    allowed = None
+    if masked:
+        rng = np.random.default_rng(seed)
+        allowed = (rng.random((h - 7, w - 7)) < 0.7).astype(np.int32)
+    p = ptb.PatchTableParams(sw + " -dt_algo brute")
+    srand_all(libc, 1)
+    ot = oracle.build(p.as_dict(), b, allowed=allowed)
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b, wh0=ot.wh0(), allowed_patches=allowed)
+    assert np.array_equal(gt.table(), ot.table())
+    ann = gt.lookup(a)
+    check_nnf(oracle, a, b, ann)
+
+
+def test_switches_without_effect(gpu, libc):
+    """-randomize_dt 1 -populate_nearest 0 are accepted and, as in the reference's build, change
+    neither the table nor the query."""
+    a, b = synth.pair(70, 90, 12)
+    out = []
+    for sw in ("-limit 0.5", "-limit 0.5 -randomize_dt 1 -populate_nearest 0"):
+        srand_all(libc, 1)
+        t = ptb.PatchTable(ptb.PatchTableParams(sw), b)
+        out.append((t.table(), t.lookup(a)))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
 @pytest.mark.parametrize("sw", ["-limit 1 -ntables 3 -coherence_spatial 2", "-speed 3 -ntables 4",
                                 "-limit 0.5 -ntables 2 -table_ratio 4 -kcoherence 3"])
 def test_multiple_tables(gpu, oracle, libc, sw):
@@ -303,7 +340,7 @@ def test_constant_image(gpu, libc):
     assert np.allclose(ann[..., 2], 64 * 3 * 0.0625)
 
 
-@pytest.mark.parametrize("sw", ["-randomize_dt 1", "-populate_nearest 0", "-dt_algo raster", "-ntables 17",
+@pytest.mark.parametrize("sw", ["-incoherence 1", "-dt_algo raster", "-dt_algo kdtree", "-ntables 17",
                                 "-dim_algo pca -pca_mean 1"])
 def test_unsupported_options_fail_loudly(gpu, sw):
     _, b = synth.pair(40, 40, 1)

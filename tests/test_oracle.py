@@ -139,6 +139,42 @@ def test_oracle_distance_transforms_equal_reference(oracle, reference, algo, sw,
     assert np.array_equal(rt.table(), ot.table())
 
 
+BRUTE_CASES = [("-limit 0.002", 60, 90, 21, False), ("-limit 0.004 -ndims 8", 43, 71, 5, True),
+               ("-limit 0.0005 -grid_ndims 2", 40, 60, 6, False), ("-limit 0.003 -nchroma 0 -ndims 5", 50, 50, 8, True)]
+
+
+@pytest.mark.parametrize("sw,h,w,seed,masked", BRUTE_CASES)
+def test_oracle_brute_distance_transform_equals_reference(oracle, reference, sw, h, w, seed, masked):
+    """dt_algo brute: every cell holds the patch nearest its centre over the whole patch region,
+    masked patches included.  The reference's loop shares one index vector across OpenMP threads
+    (patchtable.h:2370-2376), so it is run on one thread."""
+    a, b = synth.pair(h, w, seed)
+    allowed = None
+    if masked:
+        rng = np.random.default_rng(seed)
+        allowed = (rng.random((h - 7, w - 7)) < 0.7).astype(np.int32)
+    s = sw + " -dt_algo brute"
+    P = reference.params(s)
+    oracle.srand(1)
+    ot = oracle.build(P, b, allowed=allowed)
+    reference.set_threads(1)
+    reference.srand(1)
+    rt = reference.build(s, b, allowed=allowed)
+    assert np.array_equal(rt.table(), ot.table())
+
+
+def test_switches_without_effect_in_the_reference():
+    """-randomize_dt 1 -populate_nearest 0 produce the reference's default table, k-coherence set
+    and NNF: with TABLE_POPULATE_FAST populate never reaches add_patch, so no adjacency is
+    collected and do_after_dt keeps every cell (patchtable.h:37, 1831-1866, 3127-3159)."""
+    cases = {c["name"]: c for c in GOLDEN["cases"]}
+    noop, base = dict(cases["noop_switches_64x48"]), dict(cases["tiny_64x48"])
+    for c in (noop, base):
+        c.pop("name")
+        c.pop("switches")
+    assert noop == base
+
+
 def test_oracle_descriptor_without_chroma_is_a_prefix(oracle):
     """With nchroma 0 the kernels fill channels in order, so fewer dims give a prefix of more
     dims (the reference itself only builds ndims >= 3)."""
