@@ -80,6 +80,7 @@ class Oracle:
         L.orc_free.argtypes = [C.c_void_p]
         L.orc_table_shape.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
         L.orc_table_add_count.argtypes = [C.c_void_p]
+        L.orc_kc_max_knn.argtypes = [C.c_void_p]
         L.orc_get_table.argtypes = [C.c_void_p, _i32p]
         L.orc_get_wh0.argtypes = [C.c_void_p, _f32p]
         L.orc_get_partition.argtypes = [C.c_void_p, C.c_int, _f32p, _f32p, _f32p, _i32p, _f32p]
@@ -192,6 +193,10 @@ class OracleTable:
 
     def add_count(self) -> int:
         return self.orc.lib.orc_table_add_count(self.h)
+
+    def kc_max_knn(self) -> int:
+        """Longest neighbour list (knn) the k-coherence search asked for."""
+        return self.orc.lib.orc_kc_max_knn(self.h)
 
     def table(self):
         ns, nc = self.shape()

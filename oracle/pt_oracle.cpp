@@ -292,6 +292,7 @@ struct Table {
     vector<int32_t> table;
     vector<Partition1D> part;
     int table_add_count = 0;
+    int kc_max_knn = 0;         /* longest neighbour list the k-coherence search asked for */
     int kc_h = 0, kc_w = 0;
     vector<int32_t> kc_pos;     /* kc_h x kc_w x kcoherence */
     vector<float> kc_dist;
@@ -937,6 +938,7 @@ void build_kcoherence(Table &t) {
                 break;
             }
             prev_knn = knn;
+            t.kc_max_knn = std::max(t.kc_max_knn, knn);
         }
     }
 }
@@ -1250,6 +1252,7 @@ int orc_table_shape(void *tv, int *nslices, long long *ncells) {
 }
 
 int orc_table_add_count(void *tv) { return ((Table *) tv)->table_add_count; }
+int orc_kc_max_knn(void *tv) { return ((Table *) tv)->kc_max_knn; }
 
 void orc_get_table(void *tv, int32_t *out) {
     Table *t = (Table *) tv;

@@ -16,7 +16,9 @@
 
    The nearest-neighbour search (k_knn.cu) is exact, ranked by (float squared L2 summed in
    dimension order without fused operations, point index); FLANN's approximate tree is not
-   reproduced. */
+   reproduced.  Lists of up to 64 neighbours keep their validity flags in one 64-bit word; longer
+   ones (up to PT_KNN_WIDE_MAX, reached when most of a patch's nearest descriptors lie within
+   kcoherence_min_dist, e.g. inside a flat region) use the *_wide kernels with multi-word flags. */
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
@@ -181,6 +183,93 @@ __global__ void k_kc_select(const int *__restrict__ seg_start, int nseg, int Q, 
     fn[s] = (unsigned char) (b0 | (b1 << 1));   /* the segment's map of the carried bit */
 }
 
+/* Lists longer than 64 (Kc = 128 .. PT_KNN_WIDE_MAX): the same validity bits and selection with
+   the flags held in W = Kc / 64 words and the per-patch sort in global scratch. */
+constexpr int KW_WORDS = PT_KNN_WIDE_MAX / 64;
+
+__device__ __forceinline__ unsigned long long below(int n, int w) {     /* bits [64w, n) of word w */
+    const int lo = 64 * w;
+    return n >= lo + 64 ? ~0ull : (n <= lo ? 0ull : ((1ull << (n - lo)) - 1));
+}
+
+__global__ void k_kc_valid_wide(const int *__restrict__ nbr, int Kc, int Q, const int *__restrict__ qpos,
+                                const int *__restrict__ tpos, int min_dist2, int kc, int knn0,
+                                unsigned long long *valid, int *m_out) {
+    int q = blockIdx.x * 256 + threadIdx.x;
+    if (q >= Q) return;
+    const int W = Kc / 64;
+    int qx = pt_x(qpos[q]), qy = pt_y(qpos[q]);
+    unsigned long long *vq = valid + (size_t) q * W;
+    for (int w = 0; w < W; w++) {
+        unsigned long long bits = 0;
+        for (int b = 0; b < 64; b++) {
+            int v = tpos[nbr[(size_t) q * Kc + 64 * w + b]];
+            int dx = pt_x(v) - qx, dy = pt_y(v) - qy;
+            if (dx * dx + dy * dy >= min_dist2) bits |= 1ull << b;
+        }
+        vq[w] = bits;
+    }
+    int m = 0;
+    for (int k = knn0; k <= Kc; k *= 2) {
+        int c = 0;
+        for (int w = 0; w < W; w++) c += __popcll(vq[w] & below(k, w));
+        if (c >= kc) { m = k; break; }
+    }
+    m_out[q] = m;
+}
+
+__device__ int select_segment_wide(int q0, int q1, int bin, int kc, int knn0, int Kc, const int *__restrict__ nbr,
+                                   const int *__restrict__ tpos, const unsigned long long *__restrict__ valid,
+                                   const int *__restrict__ knn, const float *__restrict__ ssd, int2 *outp,
+                                   float *sd, int *sp, int *so) {
+    const int W = Kc / 64;
+    unsigned long long F[KW_WORDS];
+    for (int w = 0; w < KW_WORDS; w++) F[w] = 0ull;
+    if (bin) F[kc >> 6] |= 1ull << (kc & 63);
+    int S = knn0;
+    for (int q = q0; q < q1; q++) {
+        const int kq = knn[q];
+        const unsigned long long *vb = valid + (size_t) q * W;
+        int r = 0, nv = 0;
+        while (r < kq) { if ((vb[r >> 6] >> (r & 63)) & 1ull) nv++; r++; if (nv >= kc) break; }
+        unsigned long long flags[KW_WORDS];
+        for (int w = 0; w < W; w++) flags[w] = (vb[w] & below(r, w)) | (F[w] & below(S, w) & ~below(r, w));
+        for (int j = 0; j < kq; j++) {
+            float d = ssd[(size_t) q * Kc + j];
+            int p = tpos[nbr[(size_t) q * Kc + j]];
+            int t = j;
+            while (t > 0 && (sd[t - 1] > d || (sd[t - 1] == d && sp[t - 1] > p))) {
+                sd[t] = sd[t - 1]; sp[t] = sp[t - 1]; so[t] = so[t - 1]; t--;
+            }
+            sd[t] = d; sp[t] = p; so[t] = j;
+        }
+        for (int w = 0; w < KW_WORDS; w++) F[w] = 0ull;
+        int cv = 0;
+        for (int t = 0; t < kq; t++) {
+            const int o = so[t];
+            const int f = (int) ((flags[o >> 6] >> (o & 63)) & 1ull);
+            if (f) F[t >> 6] |= 1ull << (t & 63);
+            if (f && cv < kc) { outp[(size_t) q * kc + cv] = make_int2(sp[t], __float_as_int(sd[t])); cv++; }
+        }
+        S = kq;
+    }
+    return (int) ((F[kc >> 6] >> (kc & 63)) & 1ull);
+}
+
+__global__ void k_kc_select_wide(const int *__restrict__ seg_start, int nseg, int Q, int kc, int knn0, int Kc,
+                                 const int *__restrict__ nbr, const int *__restrict__ tpos,
+                                 const unsigned long long *__restrict__ valid, const int *__restrict__ knn,
+                                 const float *__restrict__ ssd, int2 *out0, int2 *out1, unsigned char *fn,
+                                 float *sd, int *sp, int *so) {
+    int s = blockIdx.x * 64 + threadIdx.x;
+    if (s >= nseg) return;
+    int q0 = seg_start[s], q1 = (s + 1 < nseg) ? seg_start[s + 1] : Q;
+    const size_t o = (size_t) s * Kc;
+    int b0 = select_segment_wide(q0, q1, 0, kc, knn0, Kc, nbr, tpos, valid, knn, ssd, out0, sd + o, sp + o, so + o);
+    int b1 = select_segment_wide(q0, q1, 1, kc, knn0, Kc, nbr, tpos, valid, knn, ssd, out1, sd + o, sp + o, so + o);
+    fn[s] = (unsigned char) (b0 | (b1 << 1));
+}
+
 /* Composition of bit maps f encoded as (f(0) | f(1) << 1): apply a, then b. */
 struct ComposeOp {
     __device__ unsigned char operator()(unsigned char a, unsigned char b) const {
@@ -225,7 +314,10 @@ pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *bdesc, int ds
     int Kc = 16;
     while (Kc < 2 * knn0) Kc *= 2;
     for (;;) {
-        if (Kc > 64) return pt_fail(PT_UNSUPPORTED, "k-coherence needs more than 64 neighbours for some patch");
+        if (Kc > PT_KNN_WIDE_MAX)
+            return pt_fail(PT_UNSUPPORTED, "k-coherence needs more than %d neighbours for some patch", PT_KNN_WIDE_MAX);
+        const bool wide = Kc > 64;
+        const int W = wide ? Kc / 64 : 1;
         if (Kc > N) return pt_fail(PT_BAD_ARG, "k-coherence: image has too few patches (%d)", N);
         DevBuf<int> nbr, mm, knn, ovf;
         DevBuf<unsigned long long> valid;
@@ -234,10 +326,14 @@ pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *bdesc, int ds
         PT_CUDA(mm.reserve(Q));
         PT_CUDA(knn.reserve(Q));
         PT_CUDA(ovf.reserve(1));
-        PT_CUDA(valid.reserve(Q));
+        PT_CUDA(valid.reserve((size_t) Q * W));
         PT_CUDA(ssd.reserve((size_t) Q * Kc));
         PT_TRY(pt_launch_knn(train, N, nd, qdesc, Q, Kc, nbr.p, st));
-        k_kc_valid<<<(Q + 255) / 256, 256, 0, st>>>(nbr.p, Kc, Q, qpos, tpos, min_dist * min_dist, kc, knn0, valid.p, mm.p);
+        if (wide)
+            k_kc_valid_wide<<<(Q + 255) / 256, 256, 0, st>>>(nbr.p, Kc, Q, qpos, tpos, min_dist * min_dist, kc, knn0, valid.p,
+                                                             mm.p);
+        else
+            k_kc_valid<<<(Q + 255) / 256, 256, 0, st>>>(nbr.p, Kc, Q, qpos, tpos, min_dist * min_dist, kc, knn0, valid.p, mm.p);
         PT_LAUNCHED();
         PT_CUDA(cudaMemsetAsync(ovf.p, 0, sizeof(int), st));
         k_kc_chain<<<(nseg + 255) / 256, 256, 0, st>>>(seg_start, nseg, Q, mm.p, knn0, Kc, knn.p, ovf.p);
@@ -259,8 +355,18 @@ pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *bdesc, int ds
         PT_CUDA(o1.reserve((size_t) Q * kc));
         PT_CUDA(fn.reserve(nseg));
         PT_CUDA(pre.reserve(nseg));
-        k_kc_select<<<(nseg + 63) / 64, 64, 0, st>>>(seg_start, nseg, Q, kc, knn0, Kc, nbr.p, tpos, valid.p, knn.p,
-                                                    ssd.p, o0.p, o1.p, fn.p);
+        DevBuf<float> wsd;
+        DevBuf<int> wsp, wso;
+        if (wide) {
+            PT_CUDA(wsd.reserve((size_t) nseg * Kc));
+            PT_CUDA(wsp.reserve((size_t) nseg * Kc));
+            PT_CUDA(wso.reserve((size_t) nseg * Kc));
+            k_kc_select_wide<<<(nseg + 63) / 64, 64, 0, st>>>(seg_start, nseg, Q, kc, knn0, Kc, nbr.p, tpos, valid.p, knn.p,
+                                                             ssd.p, o0.p, o1.p, fn.p, wsd.p, wsp.p, wso.p);
+        } else {
+            k_kc_select<<<(nseg + 63) / 64, 64, 0, st>>>(seg_start, nseg, Q, kc, knn0, Kc, nbr.p, tpos, valid.p, knn.p,
+                                                        ssd.p, o0.p, o1.p, fn.p);
+        }
         PT_LAUNCHED();
         size_t tb = 0;
         PT_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tb, fn.p, pre.p, ComposeOp(), nseg, st));

@@ -198,9 +198,121 @@ k_knn_warp(const float *__restrict__ sp, const int *__restrict__ sidx, int N, in
         for (int j = 0; j < K; j++) out[(size_t) q * K + j] = ki[j] == 0x7fffffff ? -1 : ki[j];
 }
 
+/* The same search for K = 128 .. 1024 (sets that need that many neighbours: thin images, or
+   narrow flat regions where the nearest descriptors all lie within kcoherence_min_dist).  The
+   sorted list lives in global memory (wd: distances, out: indices, K per query); a leaf's
+   admissible points are first sorted in a 32-entry buffer and then merged into the list from the
+   back in one pass, keeping the K smallest.  Traversal, rounding and tie rule are those of
+   k_knn_warp, so its first 64 entries equal that kernel's result. */
+__global__ void __launch_bounds__(NT)
+k_knn_wide(const float *__restrict__ sp, const int *__restrict__ sidx, int N, int nd, int L,
+           const float *__restrict__ lo, const float *__restrict__ hi, const float *__restrict__ qdesc,
+           const int *__restrict__ qorder, int Q, int K, float *wd, int *out) {
+    __shared__ int stk_s[NT / 32][KNN_STACK];
+    __shared__ float pts_s[NT / 32][BUCKET * PSTRIDE];
+    __shared__ int pid_s[NT / 32][BUCKET];
+    const unsigned FULL = 0xffffffffu;
+    const float INF = __int_as_float(0x7f800000);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int t = blockIdx.x * NT + threadIdx.x;
+    const bool active = t < Q;
+    const int q = active ? qorder[t] : 0;
+    float qv[PT_DESC_MAX];
+#pragma unroll
+    for (int d = 0; d < PT_DESC_MAX; d++) qv[d] = (active && d < nd) ? qdesc[(size_t) q * nd + d] : 0.f;
+    float *ld = wd + (size_t) q * K;
+    int *li = out + (size_t) q * K;
+    if (active)
+        for (int j = 0; j < K; j++) { ld[j] = INF; li[j] = 0x7fffffff; }
+    float worst_d = INF;
+    int worst_i = 0x7fffffff;
+    int *stk = stk_s[wid];
+    float *pts = pts_s[wid];
+    int *pid = pid_s[wid];
+    if (lane == 0) stk[0] = 1;
+    __syncwarp();
+    int top = 1;
+    while (top > 0) {
+        const int node = stk[--top];
+        __syncwarp();
+        const float lb = active ? box_lb(qv, lo + (size_t) node * nd, hi + (size_t) node * nd, nd) : 0.f;
+        const bool want = active && !(lb > worst_d);
+        if (!__any_sync(FULL, want)) continue;
+        if (node >= L) {
+            const int base = (node - L) * BUCKET;
+            const int cnt = min(BUCKET, N - base);
+            if (lane < cnt) {
+                const float *src = sp + (size_t) (base + lane) * nd;
+                for (int d = 0; d < nd; d++) pts[lane * PSTRIDE + d] = src[d];
+                pid[lane] = sidx[base + lane];
+            }
+            __syncwarp();
+            if (want) {
+                float bd[BUCKET];
+                int bi[BUCKET];
+                int nb = 0;
+                for (int m = 0; m < cnt; m++) {
+                    const float *pv = pts + m * PSTRIDE;
+                    float dsum = 0.f;
+#pragma unroll
+                    for (int d = 0; d < PT_DESC_MAX; d++) {
+                        if (d < nd) {
+                            const float e = __fsub_rn(qv[d], pv[d]);
+                            dsum = __fadd_rn(dsum, __fmul_rn(e, e));
+                        }
+                    }
+                    const int id = pid[m];
+                    if (!before(dsum, id, worst_d, worst_i)) continue;
+                    int s2 = nb++;
+                    while (s2 > 0 && before(dsum, id, bd[s2 - 1], bi[s2 - 1])) { bd[s2] = bd[s2 - 1]; bi[s2] = bi[s2 - 1]; s2--; }
+                    bd[s2] = dsum;
+                    bi[s2] = id;
+                }
+                if (nb > 0) {
+                    /* backward merge: the union's largest go to virtual slots K .. K+nb-1 and drop out */
+                    int ia = K - 1, ib = nb - 1;
+                    for (int p = K + nb - 1; ib >= 0; p--) {
+                        if (ia < 0 || before(ld[ia], li[ia], bd[ib], bi[ib])) {
+                            if (p < K) { ld[p] = bd[ib]; li[p] = bi[ib]; }
+                            ib--;
+                        } else {
+                            if (p < K) { ld[p] = ld[ia]; li[p] = li[ia]; }
+                            ia--;
+                        }
+                    }
+                    worst_d = ld[K - 1];
+                    worst_i = li[K - 1];
+                }
+            }
+            __syncwarp();                        /* the next leaf restages the points */
+            continue;
+        }
+        const int c0 = 2 * node, c1 = 2 * node + 1;
+        float l0 = 0.f, l1 = 0.f;
+        if (want) {
+            l0 = box_lb(qv, lo + (size_t) c0 * nd, hi + (size_t) c0 * nd, nd);
+            l1 = box_lb(qv, lo + (size_t) c1 * nd, hi + (size_t) c1 * nd, nd);
+        }
+        float s0 = l0, s1 = l1;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) { s0 += __shfl_xor_sync(FULL, s0, o); s1 += __shfl_xor_sync(FULL, s1, o); }
+        if (top + 2 > KNN_STACK) continue;        /* cannot happen: depth <= 31 */
+        if (lane == 0) {
+            if (s0 <= s1) { stk[top] = c1; stk[top + 1] = c0; }
+            else { stk[top] = c0; stk[top + 1] = c1; }
+        }
+        __syncwarp();
+        top += 2;
+    }
+    if (active)
+        for (int j = 0; j < K; j++)
+            if (li[j] == 0x7fffffff) li[j] = -1;
+}
+
 }  // namespace
 
-/* Exact top-K (K in {16, 32, 64}) train indices of every query, ascending (dist, index). */
+/* Exact top-K (K in {16, 32, 64}, or a power of two up to PT_KNN_WIDE_MAX) train indices of every
+   query, ascending (dist, index). */
 pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, int Q, int K, int *out, cudaStream_t st) {
     if (N < 1 || Q < 1) return PT_OK;
     if (nd < 1 || nd > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "knn: %d dims", nd);
@@ -263,6 +375,15 @@ pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, i
         PT_LAUNCHED();
     }
     dim3 grid((Q + NT - 1) / NT);
+    if (K > 64) {
+        if (K > PT_KNN_WIDE_MAX || (K & (K - 1))) return pt_fail(PT_UNSUPPORTED, "knn K=%d", K);
+        DevBuf<float> wd;
+        PT_CUDA(wd.reserve((size_t) Q * K));
+        k_knn_wide<<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, K, wd.p, out);
+        PT_LAUNCHED();
+        PT_CUDA(cudaStreamSynchronize(st));
+        return PT_OK;
+    }
     switch (K) {
         case 16: k_knn_warp<16><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
         case 32: k_knn_warp<32><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;

@@ -73,6 +73,7 @@ pt_status pt_dt_brute(int *table, int G, const int *nslices, const float *part, 
 pt_status pt_launch_replace(int *table, long long n, int from, int to, cudaStream_t st);
 
 /* k_kcoh.cu */
+#define PT_KNN_WIDE_MAX 1024                 /* largest neighbour list of the k-coherence search */
 pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, int Q, int K, int *out, cudaStream_t st);
 pt_status pt_gather_rows(const float *desc, int ds, int nd, const int *rows, int n, float *out, cudaStream_t st);
 /* Exact distances from b_rgba (image mode) or, when bdesc is set, from the descriptor store

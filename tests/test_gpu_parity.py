@@ -129,6 +129,37 @@ def test_other_distance_transforms(gpu, oracle, libc, algo, sw, h, w, seed, mask
     check_nnf(oracle, a, b, ann)
 
 
+def _flat_bar(h, w, seed, x0, x1):
+    """A seeded pair with one constant vertical bar: the bar's patches share one descriptor, so
+    their nearest neighbours are each other, most of them within kcoherence_min_dist."""
+    a, b = synth.pair(h, w, seed)
+    a, b = a.copy(), b.copy()
+    a[:, x0:x1] = 0.5
+    b[:, x0:x1] = 0.5
+    return a, b
+
+
+@pytest.mark.parametrize("args,sw,knn_min", [((60, 90, 73, 30, 44), "-limit 0.2 -kcoherence 4", 16),
+                                             ((70, 80, 74, 20, 60), "-limit 0.2 -kcoherence 6 -kcoherence_min_dist 14", 256),
+                                             ((64, 72, 75, 10, 70), "-limit 0.2 -kcoherence 3 -kcoherence_min_dist 12", 128)])
+def test_kcoherence_long_neighbour_lists(gpu, oracle, libc, args, sw, knn_min):
+    """k-coherence sets whose search needs more than 64 neighbours (the reference doubles knn
+    without bound): the set, the table and the query equal the oracle's, which is pinned to the
+    reference on the same inputs."""
+    a, b = _flat_bar(*args)
+    p = ptb.PatchTableParams(sw)
+    srand_all(libc, 1)
+    ot = oracle.build(p.as_dict(), b)
+    assert ot.kc_max_knn() >= knn_min
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b, wh0=ot.wh0())
+    kg, ko = gt.kcoherence(), ot.kcoherence()
+    assert np.array_equal(kg[0], ko[0])
+    assert np.array_equal(kg[1], ko[1])
+    assert np.array_equal(gt.table(), ot.table())
+    check_nnf(oracle, a, b, gt.lookup(a))
+
+
 BRUTE_CASES = [("-limit 0.002", 60, 90, 21, False), ("-limit 0.004 -ndims 8", 43, 71, 5, True),
                ("-limit 0.0005 -grid_ndims 2", 40, 60, 6, False), ("-limit 0.003 -nchroma 0 -ndims 5", 50, 50, 8, True),
                ("-limit 0.01 -grid_ndims 7 -ndims 7", 80, 100, 9, False)]
@@ -328,6 +359,24 @@ def test_small_and_degenerate_images(gpu, libc):
         assert (ann[..., 0] < w - 7).all() and (ann[..., 1] < h - 7).all()
     with pytest.raises(ptb.PatchTableError):
         ptb.PatchTable(ptb.PatchTableParams("-limit 0.01"), synth.pair(8, 8, 1)[1])   # k-coherence needs neighbours
+
+
+@pytest.mark.parametrize("h,w", [(12, 65535), (16383, 9)])
+def test_maximum_extents(gpu, oracle, libc, h, w):
+    """The largest sides of b a packed position XY_TO_INT holds (x < 2^16; y < 2^14 keeps every
+    position below TABLE_UNUSED): the table builds and the query returns exact distances; one
+    pixel more along that side is rejected for the table.  Query positions are never packed, so a
+    query one pixel larger is answered like any other."""
+    a, b = synth.pair(h, w, 61)
+    srand_all(libc, 1)
+    t = ptb.PatchTable(ptb.PatchTableParams("-limit 0.05 -kcoherence 2"), b)
+    check_nnf(oracle, a, b, t.lookup(a))
+    hh, ww = (h, w + 1) if w == 65535 else (h + 1, w)
+    with pytest.raises(ptb.PatchTableError) as e:
+        ptb.PatchTable(ptb.PatchTableParams("-limit 0.05"), np.zeros((hh, ww, 3), np.float32))
+    assert e.value.status == 1
+    a2 = synth.image_a(hh, ww, 62)
+    check_nnf(oracle, a2, b, t.lookup(a2))
 
 
 def test_constant_image(gpu, libc):

@@ -163,6 +163,31 @@ def test_oracle_brute_distance_transform_equals_reference(oracle, reference, sw,
     assert np.array_equal(rt.table(), ot.table())
 
 
+@pytest.mark.parametrize("args,sw", [((60, 90, 73, 30, 44), "-limit 0.2 -kcoherence 4"),
+                                     ((70, 80, 74, 20, 60), "-limit 0.2 -kcoherence 6 -kcoherence_min_dist 14"),
+                                     ((64, 72, 75, 10, 70), "-limit 0.2 -kcoherence 3 -kcoherence_min_dist 12")])
+def test_oracle_long_neighbour_lists_equal_reference(oracle, reference, args, sw):
+    """A constant bar makes the k-coherence search double knn past 64 (to 448 in the second
+    case); the set, table and NNF still equal the reference's."""
+    h, w, seed, x0, x1 = args
+    a, b = synth.pair(h, w, seed)
+    a, b = a.copy(), b.copy()
+    a[:, x0:x1] = 0.5
+    b[:, x0:x1] = 0.5
+    P = reference.params(sw)
+    oracle.srand(1)
+    ot = oracle.build(P, b)
+    reference.srand(1)
+    rt = reference.build(sw, b)
+    kr, ko = rt.kcoherence(), ot.kcoherence()
+    assert np.array_equal(kr[0], ko[0]) and np.array_equal(kr[1], ko[1])
+    assert np.array_equal(rt.table(), ot.table())
+    reference.srand(5)
+    annr, _ = rt.lookup(a)
+    oracle.srand(5)
+    assert np.array_equal(annr, ot.lookup(a))
+
+
 def test_switches_without_effect_in_the_reference():
     """-randomize_dt 1 -populate_nearest 0 produce the reference's default table, k-coherence set
     and NNF: with TABLE_POPULATE_FAST populate never reaches add_patch, so no adjacency is
