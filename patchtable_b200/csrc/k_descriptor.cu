@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <mutex>
 
+#include "pt_bins.cuh"
 #include "pt_internal.h"
 #include "wh_tables.h"
 #include "pt_kernels.h"
@@ -27,6 +28,18 @@ constexpr int TW = 64, TH = 8;            /* patches per CTA */
 constexpr int RW = TW + 7, RH = TH + 7;   /* pixel region per CTA */
 constexpr int RWP = RW + 1;               /* padded smem row */
 constexpr int NT = 256;
+
+/* The table step fused into the query's descriptor pass: each patch's cell (get_bin over the grid
+   dimensions, exactly as k_table_cand computes it from stored descriptors) and its entry
+   tcand[p] = table[cell], so the plain query never stores or re-reads its descriptors. */
+struct CellPlan {
+    int G;
+    float min_val[PT_DESC_MAX], range[PT_DESC_MAX];
+    long long stride[PT_DESC_MAX];
+    const int *to_bin;
+    const int *table;
+    int *tcand;
+};
 
 struct DescPlan {
     int nd;                               /* output channels */
@@ -110,10 +123,12 @@ __device__ __forceinline__ void stage_pix(float *pix, const float *__restrict__ 
     }
 }
 
-/* One 64 x 8 block of patches with top-left patch (x0, y0). */
+/* One 64 x 8 block of patches with top-left patch (x0, y0).  With CELLS the table entry of each
+   patch's cell is written to cp.tcand (and the descriptor only where desc is set). */
+template<bool CELLS = false>
 __device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, const float *__restrict__ rgb, int h, int w,
                                           int convert, float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh,
-                                          int ew, int x0, int y0) {
+                                          int ew, int x0, int y0, const CellPlan *cp = nullptr) {
     float *pix = smem;                               /* 3 planes x RH x RWP */
     float *hs = smem + 3 * RH * RWP;                 /* ncombo x RH x TW */
     const int tid = threadIdx.x;
@@ -135,7 +150,7 @@ __device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, c
     for (int i = tid; i < TW * TH; i += NT) {
         int pi = i / TW, pj = i % TW;
         int py = y0 + pi, px = x0 + pj;
-        if (py >= eh || px >= ew || desc == nullptr) continue;
+        if (py >= eh || px >= ew || (!CELLS && desc == nullptr)) continue;
         float out[PT_DESC_MAX];
 #pragma unroll
         for (int c = 0; c < PT_DESC_MAX; c++) {
@@ -148,6 +163,14 @@ __device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, c
             } else {
                 out[c] = 0.f;
             }
+        }
+        if (CELLS) {
+            long long cell = 0;
+#pragma unroll
+            for (int d = 0; d < PT_DESC_MAX; d++)
+                if (d < cp->G) cell += (long long) pt_get_bin(cp->min_val[d], cp->range[d], cp->to_bin + d * PT_NMAP, out[d]) * cp->stride[d];
+            cp->tcand[(size_t) py * ew + px] = __ldg(cp->table + cell);
+            if (desc == nullptr) continue;
         }
         float4 *dst = reinterpret_cast<float4 *>(desc + ((size_t) py * ew + px) * ds);
 #pragma unroll
@@ -163,6 +186,13 @@ k_descriptor(const DescPlan c_plan, const float *__restrict__ rgb, int h, int w,
              float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh, int ew, int ty0) {
     extern __shared__ float smem[];
     desc_tile(c_plan, smem, rgb, h, w, convert, rgba, desc, ds, eh, ew, blockIdx.x * TW, (blockIdx.y + ty0) * TH);
+}
+
+__global__ void __launch_bounds__(NT, 4)
+k_descriptor_cells(const DescPlan c_plan, const CellPlan cp, const float *__restrict__ rgb, int h, int w, int convert,
+                   float4 *__restrict__ rgba, int eh, int ew, int ty0) {
+    extern __shared__ float smem[];
+    desc_tile<true>(c_plan, smem, rgb, h, w, convert, rgba, nullptr, 0, eh, ew, blockIdx.x * TW, (blockIdx.y + ty0) * TH, &cp);
 }
 
 /* Persistent descriptor pass over the 64 x 8 tiles of every image of a batch (images, RGBA
@@ -301,6 +331,37 @@ pt_status pt_launch_descriptor_rows(int ndims, int nchroma, const float *rgb, in
         return pt_fail(PT_BAD_ARG, "descriptor tile rows [%d, %d) outside 0..%d", trow0, trow0 + trows, ntr);
     dim3 grid((ew + TW - 1) / TW, trows);
     k_descriptor<<<grid, NT, smem, st>>>(plan, rgb, h, w, convert, rgba, desc, ds, eh, ew, trow0);
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_descriptor_cells(int ndims, int nchroma, const float *rgb, int h, int w, int convert, float4 *rgba,
+                                     const PtBins &bins, const int *to_bin, const int *table, int *tcand, int trow0,
+                                     int trows, cudaStream_t st) {
+    if (convert == PT_COLOR_LAB) PT_TRY(pt_lab_tables_ready());
+    int eh = h - 7, ew = w - 7;
+    DescPlan plan;
+    PT_TRY(make_plan(ndims, nchroma, plan));
+    if (eh < 1 || ew < 1) return pt_fail(PT_BAD_ARG, "image %dx%d is smaller than one 8x8 patch", w, h);
+    if (bins.G < 1 || bins.G > ndims) return pt_fail(PT_BAD_ARG, "grid dims %d outside 1..%d", bins.G, ndims);
+    CellPlan cp;
+    memset(&cp, 0, sizeof(cp));
+    cp.G = bins.G;
+    for (int d = 0; d < bins.G; d++) { cp.min_val[d] = bins.min_val[d]; cp.range[d] = bins.range[d]; cp.stride[d] = bins.stride[d]; }
+    cp.to_bin = to_bin;
+    cp.table = table;
+    cp.tcand = tcand;
+    static bool attr = false;
+    size_t smem = sizeof(float) * (3 * RH * RWP + plan.ncombo * RH * TW);
+    if (!attr) {
+        PT_CUDA(cudaFuncSetAttribute(k_descriptor_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) pt_descriptor_smem(0)));
+        attr = true;
+    }
+    const int ntr = (eh + TH - 1) / TH;
+    if (trow0 < 0 || trows < 1 || trow0 + trows > ntr)
+        return pt_fail(PT_BAD_ARG, "descriptor tile rows [%d, %d) outside 0..%d", trow0, trow0 + trows, ntr);
+    dim3 grid((ew + TW - 1) / TW, trows);
+    k_descriptor_cells<<<grid, NT, smem, st>>>(plan, cp, rgb, h, w, convert, rgba, eh, ew, trow0);
     PT_LAUNCHED();
     return PT_OK;
 }

@@ -59,6 +59,11 @@ pt_status pt_launch_cells(const PtBins &bins, const float *desc, int ds, long lo
 /* Table entry of every query patch's cell (patchtable.h:3675-3686): tcand[p] = table[cell(p)]. */
 pt_status pt_launch_table_candidates(const PtBins &bins, const float *desc, int ds, long long P, const int *to_bin,
                                      const int *table, int *tcand, cudaStream_t st);
+/* The descriptor pass of query tile rows [trow0, trow0 + trows) fused with the table step: writes
+   the RGBA copy and tcand[p] = table[cell(p)] for every patch of those rows, no descriptors. */
+pt_status pt_launch_descriptor_cells(int ndims, int nchroma, const float *rgb, int h, int w, int convert, float4 *rgba,
+                                     const PtBins &bins, const int *to_bin, const int *table, int *tcand, int trow0,
+                                     int trows, cudaStream_t st);
 pt_status pt_dt_prop(int *table, long long ncells, const int *order_xy, int G, const int *nslices,
                      const long long *stride, int dt_iters, int run, long long *seeded, int *levels_out,
                      cudaStream_t st);

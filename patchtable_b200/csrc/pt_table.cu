@@ -564,12 +564,18 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     } else if (t->pca) {
         PT_TRY(pt_launch_pca(a_rgb, h, w, pt_color_mode(p), t->q_rgba.p, t->pca_mean.p, t->pca_basis.p, t->nd,
                              t->q_desc.p, t->ds, st));
-    } else {
+    } else if (net || !t->subs.empty()) {
         PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, a_rgb, h, w, pt_color_mode(p), t->q_rgba.p, t->q_desc.p,
                                     t->ds, st));
     }
+    /* The plain single-table query needs its descriptors only for the table step: one fused pass. */
+    const bool fused = !t->desc_mode && !t->pca && !net && t->subs.empty();
+    if (fused)
+        PT_TRY(pt_launch_descriptor_cells(p.ndims, p.nchroma, a_rgb, h, w, pt_color_mode(p), t->q_rgba.p, t->bins,
+                                          t->to_bin.p, t->table.p, t->q_tcand.p, 0, (h - 7 + 7) / 8, st));
     PT_TRY(mark(t, prof, LookupProfile::DESC, st));
-    PT_TRY(pt_launch_table_candidates(t->bins, t->q_desc.p, t->ds, P, t->to_bin.p, t->table.p, t->q_tcand.p, st));
+    if (!fused)
+        PT_TRY(pt_launch_table_candidates(t->bins, t->q_desc.p, t->ds, P, t->to_bin.p, t->table.p, t->q_tcand.p, st));
     if (!t->subs.empty()) {
         PT_CUDA(t->q_tcand_more.reserve((size_t) P * t->subs.size()));
         for (size_t i = 0; i < t->subs.size(); i++) {
@@ -729,12 +735,10 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
             PT_CUDA(cudaMemcpyAsync(t->q_rgb.p + px0, a + px0, sizeof(float) * npx, cudaMemcpyHostToDevice, t->st_in));
             PT_CUDA(cudaEventRecord(ev_in[b], t->st_in));
             PT_CUDA(cudaStreamWaitEvent(sa, ev_in[b], 0));
-            PT_TRY(pt_launch_descriptor_rows(p.ndims, p.nchroma, t->q_rgb.p, h, w, pt_color_mode(p), t->q_rgba.p,
-                                             t->q_desc.p, t->ds, r0 / 8, (r1 - r0 + 7) / 8, sa));
+            PT_TRY(pt_launch_descriptor_cells(p.ndims, p.nchroma, t->q_rgb.p, h, w, pt_color_mode(p), t->q_rgba.p,
+                                              t->bins, t->to_bin.p, t->table.p, t->q_tcand.p, r0 / 8, (r1 - r0 + 7) / 8, sa));
             const size_t o = (size_t) r0 * ew;
             const long long n = (long long) (r1 - r0) * ew;
-            PT_TRY(pt_launch_table_candidates(t->bins, t->q_desc.p + o * t->ds, t->ds, n, t->to_bin.p, t->table.p,
-                                              t->q_tcand.p + o, sa));
             PT_TRY(pt_launch_init((int) n, init_pos, (float) PT_DIST_INF, t->q_pos[0].p + o, t->q_d[0].p + o, sa));
             PT_CUDA(cudaEventRecord(ev_a[b], sa));
         }
