@@ -48,6 +48,10 @@ struct DescPlan {
     signed char combo_h[PT_DESC_MAX][8];
     int ch_combo[PT_DESC_MAX];
     signed char ch_v[PT_DESC_MAX][8];
+    /* the same signs as +-1.0f: a fused multiply-add by +-1 rounds exactly like the add or
+       subtract it stands for, and reads the sign straight from the parameter bank */
+    float combo_hf[PT_DESC_MAX][8];
+    float ch_vf[PT_DESC_MAX][8];
 };
 
 
@@ -136,13 +140,20 @@ __device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, c
     __syncthreads();
 
     const int ncombo = c_plan.ncombo;
-    for (int i = tid; i < ncombo * RH * TW; i += NT) {
-        int m = i / (RH * TW), rem = i % (RH * TW), r = rem / TW, j = rem % TW;
-        const float *row = pix + (c_plan.combo_plane[m] * RH + r) * RWP + j;
-        float s = 0.f;
+    for (int m = 0; m < ncombo; m++) {                /* one filter at a time: its signs stay in registers */
+        float sg[8];
 #pragma unroll
-        for (int b = 0; b < 8; b++) s = c_plan.combo_h[m][b] > 0 ? __fadd_rn(s, row[b]) : __fsub_rn(s, row[b]);
-        hs[(m * RH + r) * TW + j] = s;
+        for (int b = 0; b < 8; b++) sg[b] = c_plan.combo_hf[m][b];
+        const float *plane = pix + c_plan.combo_plane[m] * RH * RWP;
+        float *dst = hs + m * RH * TW;
+        for (int i = tid; i < RH * TW; i += NT) {
+            const int r = i / TW, j = i % TW;
+            const float *row = plane + r * RWP + j;
+            float s = 0.f;
+#pragma unroll
+            for (int b = 0; b < 8; b++) s = __fmaf_rn(sg[b], row[b], s);
+            dst[i] = s;
+        }
     }
     __syncthreads();
 
@@ -158,7 +169,7 @@ __device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, c
                 const float *col = hs + (c_plan.ch_combo[c] * RH + pi) * TW + pj;
                 float s = 0.f;
 #pragma unroll
-                for (int a = 0; a < 8; a++) s = c_plan.ch_v[c][a] > 0 ? __fadd_rn(s, col[a * TW]) : __fsub_rn(s, col[a * TW]);
+                for (int a = 0; a < 8; a++) s = __fmaf_rn(c_plan.ch_vf[c][a], col[a * TW], s);
                 out[c] = s;
             } else {
                 out[c] = 0.f;
@@ -283,7 +294,7 @@ static pt_status make_plan(int ndims, int nchroma, DescPlan &plan) {
         }
         int m = plan.ncombo++;
         plan.combo_plane[m] = plane;
-        for (int b = 0; b < 8; b++) plan.combo_h[m][b] = PT_WH_H[k][b];
+        for (int b = 0; b < 8; b++) { plan.combo_h[m][b] = PT_WH_H[k][b]; plan.combo_hf[m][b] = PT_WH_H[k][b] > 0 ? 1.f : -1.f; }
         return m;
     };
     for (int k = 0; k < n; k++) {
@@ -292,7 +303,7 @@ static pt_status make_plan(int ndims, int nchroma, DescPlan &plan) {
         for (int c = 0; c < nc; c++) {
             int ch = c0 + c;
             plan.ch_combo[ch] = combo_of(c, k);
-            for (int a = 0; a < 8; a++) plan.ch_v[ch][a] = PT_WH_V[k][a];
+            for (int a = 0; a < 8; a++) { plan.ch_v[ch][a] = PT_WH_V[k][a]; plan.ch_vf[ch][a] = PT_WH_V[k][a] > 0 ? 1.f : -1.f; }
         }
     }
     return PT_OK;
