@@ -260,8 +260,9 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
         aq.atile = atile;
         aq.tx = threadIdx.x;
         if constexpr (DESC) pt_desc_load(c_q.adesc + (size_t) p * c_q.ds4, 4 * c_q.ds4, aq.v);
-        int pos = cur_pos[p];
-        float dstore = cur_d[p];
+        /* no state arrays: the initial field, x = b's ew + 1 and DIST_INFINITY (patchtable.h:3538-3547) */
+        int pos = cur_pos ? cur_pos[p] : pt_xy(c_q.bew + 1, 0);
+        float dstore = cur_d ? cur_d[p] : (float) PT_DIST_INF;
         int xb = pt_x(pos), yb = pt_y(pos);
         float dbest = (float) ((double) dstore * c_q.prop_scale);
         float dch = dstore;
@@ -467,8 +468,8 @@ pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const fl
         aq.atile = atile;
         aq.tx = threadIdx.x;
         if constexpr (DESC) pt_desc_load(c_q.adesc + (size_t) p * c_q.ds4, 4 * c_q.ds4, aq.v);
-        int bpos = cur_pos[p];
-        float bd = cur_d[p];
+        int bpos = cur_pos ? cur_pos[p] : pt_xy(c_q.bew + 1, 0);      /* null: the initial field */
+        float bd = cur_d ? cur_d[p] : (float) PT_DIST_INF;
         {
             int cp = ch_pos[p];
             if (pt_x(cp) < c_q.bew && pt_y(cp) < c_q.beh && cp != bpos && ch_d[p] < bd) { bd = ch_d[p]; bpos = cp; }

@@ -634,10 +634,12 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
                                        t->q_rgba.p, t->b_rgba.p, t->q_pos[0].p, t->q_d[0].p, t->q_torig.p, t->q_tbad.p, st));
         PT_CUDA(cudaMemcpyAsync(t->q_tpos0.p, t->q_pos[0].p, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
         PT_CUDA(cudaMemcpyAsync(t->q_td0.p, t->q_d[0].p, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
-    } else {
+    } else if (net) {
         /* Initial field (patchtable.h:3538-3547): x = b0_ew + 1, dist = DIST_INFINITY. */
         PT_TRY(pt_launch_init(n, pt_xy(t->ew + 1, 0), (float) PT_DIST_INF, t->q_pos[0].p, t->q_d[0].p, st));
     }
+    /* Otherwise the first pass reads no state arrays: its kernels start from the initial field. */
+    const bool fresh = !p.init_random && !d_prev && !net;
     PT_TRY(mark(t, prof, LookupProfile::INIT, st));
     int passes = pt_default_passes(p);
     int jump = pt_default_jump(p, passes);
@@ -655,14 +657,16 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
                                             i == 0 ? t->q_lcand.p : nullptr, t->q_lconf.p, pt_prop_threshold(net),
                                             pt_prop_kcoh_confident(net), ctr, ctr ? ctr + 4 : nullptr, st));
         else
-            PT_TRY(pt_launch_choose(qi, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_tcand.p,
-                                    t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, i > 0, ctr, st));
+            PT_TRY(pt_launch_choose(qi, n, t->q_rgba.p, t->b_rgba.p, fresh && i == 0 ? nullptr : t->q_pos[cur].p,
+                                    fresh && i == 0 ? nullptr : t->q_d[cur].p, t->q_tcand.p, t->kcoh.p, do_table,
+                                    t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, i > 0, ctr, st));
         PT_TRY(mark(t, prof, LookupProfile::CHOOSE, st));
         if (p.do_prop) {
             QuerySetup qp = qs;
             qp.step = pt_pass_step(i, passes, jump);
-            PT_TRY(pt_launch_pull(qp, n, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_chpos.p,
-                                  t->q_chd.p, t->q_pos[1 - cur].p, t->q_d[1 - cur].p, ctr ? ctr + 2 : nullptr, st));
+            PT_TRY(pt_launch_pull(qp, n, t->q_rgba.p, t->b_rgba.p, fresh && i == 0 ? nullptr : t->q_pos[cur].p,
+                                  fresh && i == 0 ? nullptr : t->q_d[cur].p, t->q_chpos.p, t->q_chd.p,
+                                  t->q_pos[1 - cur].p, t->q_d[1 - cur].p, ctr ? ctr + 2 : nullptr, st));
             PT_TRY(mark(t, prof, LookupProfile::PULL, st));
             cur = 1 - cur;
         } else {
@@ -681,9 +685,9 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
 /* The host lookup of a one-pass schedule, pipelined over bands of patch rows.  A band needs only
    its own pixel rows plus 7; its choose also reads the next band's RGBA rows (written by that
    band's descriptor launch) and its pull the next band's choices.  Four streams carry the phases:
-   upload of band b -> descriptor, table entries and initial state of band b -> choose of band
+   upload of band b -> descriptor and table entries of band b (one fused pass) -> choose of band
    b-1 -> pull and output of band b-2 -> download of band b-2, each waiting on the events its
-   inputs come from.  Consecutive bands' kernels overlap (filling each other's last waves) and the
+   inputs come from; choose and pull start from the initial field without reading state arrays.  Consecutive bands' kernels overlap (filling each other's last waves) and the
    copies overlap the kernels.  Concurrent kernels always touch disjoint rows (bands are at least
    32 rows; a pull reads at most 16 rows beyond its band).  Every kernel computes exactly what the
    whole-image launch computes for its rows, so the result is identical. */
@@ -726,7 +730,6 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     qs.allowed_index = p.allowed_index;
     QuerySetup qp = qs;
     qp.step = pt_pass_step(0, 1, pt_default_jump(p, 1));
-    const int init_pos = pt_xy(t->ew + 1, 0);
     for (int b = 0; b <= nb + 1; b++) {
         if (b < nb) {
             const int r0 = b * B, r1 = std::min(eh, r0 + B);
@@ -737,9 +740,6 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
             PT_CUDA(cudaStreamWaitEvent(sa, ev_in[b], 0));
             PT_TRY(pt_launch_descriptor_cells(p.ndims, p.nchroma, t->q_rgb.p, h, w, pt_color_mode(p), t->q_rgba.p,
                                               t->bins, t->to_bin.p, t->table.p, t->q_tcand.p, r0 / 8, (r1 - r0 + 7) / 8, sa));
-            const size_t o = (size_t) r0 * ew;
-            const long long n = (long long) (r1 - r0) * ew;
-            PT_TRY(pt_launch_init((int) n, init_pos, (float) PT_DIST_INF, t->q_pos[0].p + o, t->q_d[0].p + o, sa));
             PT_CUDA(cudaEventRecord(ev_a[b], sa));
         }
         if (b >= 1 && b - 1 < nb) {
@@ -749,8 +749,8 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
             qc.row0 = r0;
             qc.rows = r1 - r0;
             qc.stream = sb;
-            PT_TRY(pt_launch_choose(qc, (int) P, t->q_rgba.p, t->b_rgba.p, t->q_pos[0].p, t->q_d[0].p, t->q_tcand.p,
-                                    t->kcoh.p, p.do_table_lookup, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, 0, nullptr, sb));
+            PT_TRY(pt_launch_choose(qc, (int) P, t->q_rgba.p, t->b_rgba.p, nullptr, nullptr, t->q_tcand.p, t->kcoh.p,
+                                    p.do_table_lookup, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, 0, nullptr, sb));
             PT_CUDA(cudaEventRecord(ev_b[b - 1], sb));
         }
         if (b >= 2) {
@@ -760,8 +760,8 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
             qb.row0 = r0;
             qb.rows = r1 - r0;
             qb.stream = sc;
-            PT_TRY(pt_launch_pull(qb, (int) P, t->q_rgba.p, t->b_rgba.p, t->q_pos[0].p, t->q_d[0].p, t->q_chpos.p,
-                                  t->q_chd.p, t->q_pos[1].p, t->q_d[1].p, nullptr, sc));
+            PT_TRY(pt_launch_pull(qb, (int) P, t->q_rgba.p, t->b_rgba.p, nullptr, nullptr, t->q_chpos.p, t->q_chd.p,
+                                  t->q_pos[1].p, t->q_d[1].p, nullptr, sc));
             const size_t o = (size_t) r0 * ew;
             const int n = (r1 - r0) * ew;
             PT_TRY(pt_launch_output(n, t->q_pos[1].p + o, t->q_d[1].p + o, t->q_ann.p + 3 * o, sc));
