@@ -49,6 +49,7 @@ struct QPlan {
     const int *tcand_more;   /* further tables' entries, [table][patch] (ntables > 1), or NULL */
     int ntc;
     int spatial, do_rs, pass; /* spatial search radius, random search, pass index (its seed) */
+    double *ann;             /* last pull: the float64 NNF written directly, or NULL */
 };
 
 /* lowbias32 integer hash (C. Wellons' published constants): the random search's choice of
@@ -527,8 +528,15 @@ pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const fl
             }
         }
         ne += nc;
-        nxt_pos[p] = bpos;
-        nxt_d[p] = bd;
+        if (c_q.ann) {                          /* k_output fused: x, y, dist of the final field */
+            double *o = c_q.ann + 3 * (size_t) p;
+            o[0] = pt_x(bpos);
+            o[1] = pt_y(bpos);
+            o[2] = bd;
+        } else {
+            nxt_pos[p] = bpos;
+            nxt_d[p] = bd;
+        }
     }
     count_work(counters, ne, rows);
 }
@@ -740,6 +748,7 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     q.spatial = s.spatial > 0 ? s.spatial : 0;
     q.do_rs = s.do_rs;
     q.pass = s.pass;
+    q.ann = s.ann;
     if (q.adesc) {
         if (!q.bdesc || (s.ds != 8 && s.ds != 16) || q.nd < 3 || q.nd > s.ds)
             return pt_fail(PT_BAD_ARG, "descriptor query: store of %d floats for %d dimensions", s.ds, q.nd);

@@ -111,6 +111,9 @@ struct QuerySetup {
     /* Random / spatial search after k-coherence (do_rs, spatial; patchtable.h:3854-3905) and the
        index of the pass, which seeds the random search. */
     int spatial = 0, do_rs = 0, pass = 0;
+    /* Last pull of a query: the NNF is written here directly (x, y, dist as float64 per patch,
+       the output step fused) instead of the next state arrays; NULL otherwise. */
+    double *ann = nullptr;
     cudaStream_t stream;
 };
 /* Query schedule.  By default two choose + pull passes stand in for each of the reference's

@@ -640,6 +640,8 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     }
     /* Otherwise the first pass reads no state arrays: its kernels start from the initial field. */
     const bool fresh = !p.init_random && !d_prev && !net;
+    /* the last pull writes the NNF itself unless the temporal output has to restore distances */
+    const bool direct_out = p.do_prop && pt_default_passes(p) > 0 && !(d_prev && !p.init_random && p.coherence_temporal != 0.0);
     PT_TRY(mark(t, prof, LookupProfile::INIT, st));
     int passes = pt_default_passes(p);
     int jump = pt_default_jump(p, passes);
@@ -664,6 +666,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
         if (p.do_prop) {
             QuerySetup qp = qs;
             qp.step = pt_pass_step(i, passes, jump);
+            if (i == passes - 1 && direct_out) qp.ann = d_ann;
             PT_TRY(pt_launch_pull(qp, n, t->q_rgba.p, t->b_rgba.p, fresh && i == 0 ? nullptr : t->q_pos[cur].p,
                                   fresh && i == 0 ? nullptr : t->q_d[cur].p, t->q_chpos.p, t->q_chd.p,
                                   t->q_pos[1 - cur].p, t->q_d[1 - cur].p, ctr ? ctr + 2 : nullptr, st));
@@ -676,7 +679,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     }
     if (d_prev && !p.init_random && p.coherence_temporal != 0.0)
         PT_TRY(pt_launch_output_temporal(n, t->q_pos[cur].p, t->q_d[cur].p, t->q_tpos0.p, t->q_td0.p, t->q_torig.p, d_ann, st));
-    else
+    else if (!direct_out)
         PT_TRY(pt_launch_output(n, t->q_pos[cur].p, t->q_d[cur].p, d_ann, st));
     PT_TRY(mark(t, prof, LookupProfile::OUTPUT, st));
     return PT_OK;
@@ -760,11 +763,11 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
             qb.row0 = r0;
             qb.rows = r1 - r0;
             qb.stream = sc;
+            qb.ann = t->q_ann.p;                            /* the pull writes the band's NNF rows */
             PT_TRY(pt_launch_pull(qb, (int) P, t->q_rgba.p, t->b_rgba.p, nullptr, nullptr, t->q_chpos.p, t->q_chd.p,
                                   t->q_pos[1].p, t->q_d[1].p, nullptr, sc));
             const size_t o = (size_t) r0 * ew;
             const int n = (r1 - r0) * ew;
-            PT_TRY(pt_launch_output(n, t->q_pos[1].p + o, t->q_d[1].p + o, t->q_ann.p + 3 * o, sc));
             PT_CUDA(cudaEventRecord(ev_c[b - 2], sc));
             PT_CUDA(cudaStreamWaitEvent(t->st_out, ev_c[b - 2], 0));
             PT_CUDA(cudaMemcpyAsync(ann_out + 3 * o, t->q_ann.p + 3 * o, sizeof(double) * 3 * (size_t) n,
