@@ -71,8 +71,9 @@ typedef struct pt_params {
     /* -dim_algo pca (patch_pca.h): random patches fitted, mean subtracted from them, first channel
        from the patch mean (patchtable.cpp:86-89, 226-228). */
     int pca_samples, pca_subtract_mean, pca_mean;
-    /* Row bands of the pipelined host lookup (no reference counterpart; 0 picks about 16): uploads,
-       kernels and downloads of consecutive bands overlap.  The result does not depend on it. */
+    /* Row bands of the pipelined host lookup (no reference counterpart; 0 sizes them so that a
+       band's launches fill whole waves of the GPU): uploads, kernels and downloads of consecutive
+       bands overlap.  The result does not depend on it. */
     int gpu_bands;
 } pt_params;
 

@@ -702,9 +702,33 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     PT_CUDA(t->q_ann.reserve((size_t) P * 3));
     for (cudaStream_t *sp : {&t->st_in, &t->st_out, &t->st_choose, &t->st_pull})
         if (!*sp) PT_CUDA(cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking));
-    const int want = p.gpu_bands > 0 ? p.gpu_bands : 16;      /* 16: measured best at 1080p (1.84 ms vs 1.97 at 8) */
-    int B = ((eh + want - 1) / want + 7) / 8 * 8;   /* about `want` bands, each a multiple of 8 rows */
-    if (B < 32) B = 32;
+    int B = 0;
+    if (p.gpu_bands <= 0) {
+        /* Default: the band's choose launch fills whole waves.  A choose CTA of tw patches is
+           resident 12 * 64 / tw times per SM, so one wave covers sms * 768 / (tw * segments) patch
+           rows; B is the largest multiple of 8 rows within k waves, for the smallest k giving at
+           least 32 rows and at most 24 bands (measured e2e: 720p 9 bands 0.71 ms, 1080p 20 bands
+           of 56 rows = 0.95 wave 1.35 ms against 1.41 at 16 bands of 1.22 waves, 1440p 17 bands).
+           Fewer than 8 bands would lose the overlap: then about 16 bands. */
+        static int sms = 0;
+        if (!sms) {
+            int dev = 0;
+            PT_CUDA(cudaGetDevice(&dev));
+            PT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        }
+        const int tw = (p.gpu_tile == 64 || p.gpu_tile == 128 || p.gpu_tile == 256) ? p.gpu_tile : 32;
+        const double rows_wave = (double) sms * (12 * 64 / tw) / ((ew + tw - 1) / tw);
+        for (int k = 1; k <= 64; k++) {
+            B = (int) (k * rows_wave / 8) * 8;
+            if (B >= 32 && (eh + B - 1) / B <= 24) break;
+        }
+        if (B < 32 || (eh + B - 1) / B < 8 || (eh + B - 1) / B > 24) B = 0;
+    }
+    if (B == 0) {
+        const int want = p.gpu_bands > 0 ? p.gpu_bands : 16;
+        B = ((eh + want - 1) / want + 7) / 8 * 8;       /* about `want` bands, each a multiple of 8 rows */
+        if (B < 32) B = 32;
+    }
     const int nb = (eh + B - 1) / B;
     while ((int) t->band_ev.size() < 4 * nb + 1) {
         cudaEvent_t e;
