@@ -499,7 +499,10 @@ def main():
     passes = chosen[0]
     dom = max(("choose", "pull"), key=lambda k: stages[k])
     per_launch_ms = stages[dom] / (args.steps * passes)
-    alg_bytes = {"pull": 56, "choose": 72}[dom] * P
+    # bytes per patch averaged over the passes: the first pass reads no state (8 B), the last pull
+    # writes the float64 NNF (24 B) in place of the next state (8 B)
+    later = (passes - 1) / passes
+    alg_bytes = {"choose": 64 + 8 * later, "pull": 40 + 8 * later + (24 + 8 * (passes - 1)) / passes}[dom] * P
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
     traffic, l1 = None, None
     try:
