@@ -132,7 +132,7 @@ __device__ __forceinline__ void stage_pix(float *pix, const float *__restrict__ 
 template<bool CELLS = false>
 __device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, const float *__restrict__ rgb, int h, int w,
                                           int convert, float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh,
-                                          int ew, int x0, int y0, const CellPlan *cp = nullptr) {
+                                          int ew, int x0, int y0, const CellPlan *cp = nullptr, int *tcand = nullptr) {
     float *pix = smem;                               /* 3 planes x RH x RWP */
     float *hs = smem + 3 * RH * RWP;                 /* ncombo x RH x TW */
     const int tid = threadIdx.x;
@@ -180,7 +180,7 @@ __device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, c
 #pragma unroll
             for (int d = 0; d < PT_DESC_MAX; d++)
                 if (d < cp->G) cell += (long long) pt_get_bin(cp->min_val[d], cp->range[d], cp->to_bin + d * PT_NMAP, out[d]) * cp->stride[d];
-            cp->tcand[(size_t) py * ew + px] = __ldg(cp->table + cell);
+            tcand[(size_t) py * ew + px] = __ldg(cp->table + cell);
             if (desc == nullptr) continue;
         }
         float4 *dst = reinterpret_cast<float4 *>(desc + ((size_t) py * ew + px) * ds);
@@ -203,13 +203,16 @@ __global__ void __launch_bounds__(NT, 4)
 k_descriptor_cells(const DescPlan c_plan, const CellPlan cp, const float *__restrict__ rgb, int h, int w, int convert,
                    float4 *__restrict__ rgba, int eh, int ew, int ty0) {
     extern __shared__ float smem[];
-    desc_tile<true>(c_plan, smem, rgb, h, w, convert, rgba, nullptr, 0, eh, ew, blockIdx.x * TW, (blockIdx.y + ty0) * TH, &cp);
+    desc_tile<true>(c_plan, smem, rgb, h, w, convert, rgba, nullptr, 0, eh, ew, blockIdx.x * TW, (blockIdx.y + ty0) * TH, &cp,
+                    cp.tcand);
 }
 
 /* Persistent descriptor pass over the 64 x 8 tiles of every image of a batch (images, RGBA
-   copies and descriptors concatenated). */
+   copies and descriptors concatenated); with CELLS the table entries of the patches' cells are
+   written instead of the descriptors. */
+template<bool CELLS>
 __global__ void __launch_bounds__(NT)
-k_descriptor_batch(const DescPlan c_plan, const PtBatchImage *__restrict__ imgs, int n, long long ntiles,
+k_descriptor_batch(const DescPlan c_plan, const CellPlan cp, const PtBatchImage *__restrict__ imgs, int n, long long ntiles,
                    const float *__restrict__ rgb, int convert, float4 *__restrict__ rgba, float *__restrict__ desc, int ds) {
     extern __shared__ float smem[];
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -221,8 +224,9 @@ k_descriptor_batch(const DescPlan c_plan, const PtBatchImage *__restrict__ imgs,
         const PtBatchImage &g = imgs[lo];
         const long long lt = t - g.tile_off;
         const int tpr = (g.ew + TW - 1) / TW;
-        desc_tile(c_plan, smem, rgb + 3 * g.pix_off, g.h, g.w, convert, rgba ? rgba + g.pix_off : nullptr,
-                  desc + g.patch_off * ds, ds, g.eh, g.ew, (int) (lt % tpr) * TW, (int) (lt / tpr) * TH);
+        desc_tile<CELLS>(c_plan, smem, rgb + 3 * g.pix_off, g.h, g.w, convert, rgba ? rgba + g.pix_off : nullptr,
+                         CELLS ? nullptr : desc + g.patch_off * ds, ds, g.eh, g.ew, (int) (lt % tpr) * TW, (int) (lt / tpr) * TH,
+                         &cp, CELLS ? cp.tcand + g.patch_off : nullptr);
         __syncthreads();                                 /* the next tile reuses the shared memory */
     }
 }
@@ -377,8 +381,12 @@ pt_status pt_launch_descriptor_cells(int ndims, int nchroma, const float *rgb, i
     return PT_OK;
 }
 
-pt_status pt_launch_descriptor_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
-                                     const float *rgb, int convert, float4 *rgba, float *desc, int ds, cudaStream_t st) {
+namespace {
+
+template<bool CELLS>
+pt_status launch_descriptor_batch(int ndims, int nchroma, const CellPlan &cp, const PtBatchImage *imgs, int n,
+                                  long long ntiles, const float *rgb, int convert, float4 *rgba, float *desc, int ds,
+                                  cudaStream_t st) {
     if (convert == PT_COLOR_LAB) PT_TRY(pt_lab_tables_ready());
     DescPlan plan;
     PT_TRY(make_plan(ndims, nchroma, plan));
@@ -389,15 +397,38 @@ pt_status pt_launch_descriptor_batch(int ndims, int nchroma, const PtBatchImage 
         int dev = 0;
         PT_CUDA(cudaGetDevice(&dev));
         PT_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        PT_CUDA(cudaFuncSetAttribute(k_descriptor_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-        PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_descriptor_batch, NT, smem));
+        PT_CUDA(cudaFuncSetAttribute(k_descriptor_batch<CELLS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_descriptor_batch<CELLS>, NT, smem));
         if (per < 1) per = 1;
     }
     const long long g = (long long) per * nsm;
-    k_descriptor_batch<<<(unsigned) (ntiles < g ? ntiles : g), NT, smem, st>>>(plan, imgs, n, ntiles, rgb, convert, rgba, desc,
-                                                                              ds);
+    k_descriptor_batch<CELLS><<<(unsigned) (ntiles < g ? ntiles : g), NT, smem, st>>>(plan, cp, imgs, n, ntiles, rgb, convert,
+                                                                                     rgba, desc, ds);
     PT_LAUNCHED();
     return PT_OK;
+}
+
+}  // namespace
+
+pt_status pt_launch_descriptor_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
+                                     const float *rgb, int convert, float4 *rgba, float *desc, int ds, cudaStream_t st) {
+    CellPlan cp;
+    memset(&cp, 0, sizeof(cp));
+    return launch_descriptor_batch<false>(ndims, nchroma, cp, imgs, n, ntiles, rgb, convert, rgba, desc, ds, st);
+}
+
+pt_status pt_launch_descriptor_cells_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
+                                           const float *rgb, int convert, float4 *rgba, const PtBins &bins, const int *to_bin,
+                                           const int *table, int *tcand, cudaStream_t st) {
+    if (bins.G < 1 || bins.G > ndims) return pt_fail(PT_BAD_ARG, "grid dims %d outside 1..%d", bins.G, ndims);
+    CellPlan cp;
+    memset(&cp, 0, sizeof(cp));
+    cp.G = bins.G;
+    for (int d = 0; d < bins.G; d++) { cp.min_val[d] = bins.min_val[d]; cp.range[d] = bins.range[d]; cp.stride[d] = bins.stride[d]; }
+    cp.to_bin = to_bin;
+    cp.table = table;
+    cp.tcand = tcand;
+    return launch_descriptor_batch<true>(ndims, nchroma, cp, imgs, n, ntiles, rgb, convert, rgba, nullptr, 0, st);
 }
 
 namespace {

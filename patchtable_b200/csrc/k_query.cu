@@ -585,7 +585,8 @@ k_choose_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, l
         QPlan q = base;
         q.aw = g.w; q.ah = g.h; q.ew = g.ew; q.eh = g.eh;
         const long long o = g.patch_off;
-        choose_seg<TW, false, false>(q, atile, a + g.pix_off, b, cur_pos + o, cur_d + o, tcand + o, kcoh, do_table, ch_pos + o,
+        choose_seg<TW, false, false>(q, atile, a + g.pix_off, b, cur_pos ? cur_pos + o : nullptr, cur_d ? cur_d + o : nullptr,
+                                     tcand + o, kcoh, do_table, ch_pos + o,
                               ch_d + o, kc_done + o, use_done, counters, none, x0, y);
         __syncthreads();                       /* the next segment restages atile */
     }
@@ -607,7 +608,9 @@ k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, lon
         QPlan q = base;
         q.aw = g.w; q.ah = g.h; q.ew = g.ew; q.eh = g.eh;
         const long long o = g.patch_off;
-        pull_seg<TW, R, false>(q, atile, a + g.pix_off, b, cur_pos + o, cur_d + o, ch_pos + o, ch_d + o, nxt_pos + o, nxt_d + o,
+        if (base.ann) q.ann = base.ann + 3 * o;        /* last pass: this image's NNF records */
+        pull_seg<TW, R, false>(q, atile, a + g.pix_off, b, cur_pos ? cur_pos + o : nullptr, cur_d ? cur_d + o : nullptr, ch_pos + o,
+                               ch_d + o, nxt_pos + o, nxt_d + o,
                         counters, x0, y);
         __syncthreads();
     }

@@ -1,11 +1,11 @@
 /* Batched queries: many query images of any sizes against one table, in one pass of launches.
 
    The reference matches one image per lookup() call (patchtable/patchtable.h:4448).  A batch
-   concatenates its images -- RGB pixels, RGBA copies, descriptors, query state and the float64
+   concatenates its images -- RGB pixels, RGBA copies, table entries, query state and the float64
    NNF -- and runs every phase of the query once for all of them: one descriptor launch over the
-   flattened list of 64 x 8 descriptor tiles, one table-candidate, one init and one output launch
-   over the flattened patch index, and per propagation pass one choose and one pull launch over the
-   flattened list of row segments.  The choose / pull / descriptor launches are persistent (as many
+   flattened list of 64 x 8 descriptor tiles that also looks each patch's cell up in the table,
+   and per propagation pass one choose and one pull launch over the flattened list of row segments
+   (the first pass starts from the initial field, the last pull writes the NNF).  The choose / pull / descriptor launches are persistent (as many
    CTAs as fit on the GPU, each walking the list); each CTA finds the image that owns its segment by
    binary search over per-image prefix counts.  Every patch is computed exactly as the
    single-image query computes it, so each image's NNF equals its own pt_table_lookup_device
@@ -30,7 +30,6 @@ struct pt_batch {
     long long npix = 0, P = 0, ntiles = 0, nseg[PT_BATCH_NTW] = {0, 0, 0, 0};
     int twi = PT_BATCH_NTW - 1;           /* 256 query patches per CTA until tuned */
     DevBuf<float4> rgba;
-    DevBuf<float> desc;
     DevBuf<int> tcand, pos[2], chpos, kcdone;
     DevBuf<float> dd[2], chd;
     cudaStream_t cap_stream = nullptr;
@@ -52,9 +51,10 @@ pt_status run(pt_batch *B, const float *d_rgb, double *d_ann, cudaStream_t st) {
     PT_TRY(pt_table_view(B->t, &v));
     const pt_params &p = v.p;
     const int ds = v.ds;
-    PT_TRY(pt_launch_descriptor_batch(p.ndims, p.nchroma, B->d_imgs.p, B->n, B->ntiles, d_rgb, pt_color_mode(p),
-                                      B->rgba.p, B->desc.p, ds, st));
-    PT_TRY(pt_launch_table_candidates(v.bins, B->desc.p, ds, B->P, v.to_bin, v.table, B->tcand.p, st));
+    (void) ds;
+    /* descriptors are needed only for the table step: one fused pass writes the table entries */
+    PT_TRY(pt_launch_descriptor_cells_batch(p.ndims, p.nchroma, B->d_imgs.p, B->n, B->ntiles, d_rgb, pt_color_mode(p),
+                                            B->rgba.p, v.bins, v.to_bin, v.table, B->tcand.p, st));
     QuerySetup qs;
     qs.aw = 0; qs.ah = 0; qs.bw = v.w; qs.bh = v.h;
     qs.prop_scale = 1.0 / (1 + p.coherence_spatial);
@@ -70,8 +70,10 @@ pt_status run(pt_batch *B, const float *d_rgb, double *d_ann, cudaStream_t st) {
     qs.allowed_index = p.allowed_index;
     qs.stream = st;
     const int n = (int) B->P;
-    PT_TRY(pt_launch_init(n, pt_xy(v.w - 7 + 1, 0), (float) PT_DIST_INF, B->pos[0].p, B->dd[0].p, st));
+    /* the first pass starts from the initial field without state arrays; the last pull writes
+       the NNF */
     const int passes = pt_default_passes(p);
+    const bool direct_out = p.do_prop && passes > 0;
     const int jump = pt_default_jump(p, passes);
     int cur = 0;
     for (int i = 0; i < passes; i++) {
@@ -79,20 +81,24 @@ pt_status run(pt_batch *B, const float *d_rgb, double *d_ann, cudaStream_t st) {
         QuerySetup qi = qs;
         qi.pass = i;
         if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
-        PT_TRY(pt_launch_choose_batch(qi, B->d_imgs.p, B->n, B->nseg[B->twi], B->twi, B->rgba.p, v.b_rgba, B->pos[cur].p,
-                                      B->dd[cur].p, B->tcand.p, v.kcoh, do_table, B->chpos.p, B->chd.p, B->kcdone.p, i > 0,
-                                      nullptr, st));
+        PT_TRY(pt_launch_choose_batch(qi, B->d_imgs.p, B->n, B->nseg[B->twi], B->twi, B->rgba.p, v.b_rgba,
+                                      i == 0 ? nullptr : B->pos[cur].p, i == 0 ? nullptr : B->dd[cur].p, B->tcand.p, v.kcoh,
+                                      do_table, B->chpos.p, B->chd.p, B->kcdone.p, i > 0, nullptr, st));
         if (p.do_prop) {
             QuerySetup qp = qs;
             qp.step = pt_pass_step(i, passes, jump);
-            PT_TRY(pt_launch_pull_batch(qp, B->d_imgs.p, B->n, B->nseg[B->twi], B->twi, B->rgba.p, v.b_rgba, B->pos[cur].p,
-                                        B->dd[cur].p, B->chpos.p, B->chd.p, B->pos[1 - cur].p, B->dd[1 - cur].p, nullptr, st));
+            if (i == passes - 1 && direct_out) qp.ann = d_ann;
+            PT_TRY(pt_launch_pull_batch(qp, B->d_imgs.p, B->n, B->nseg[B->twi], B->twi, B->rgba.p, v.b_rgba,
+                                        i == 0 ? nullptr : B->pos[cur].p, i == 0 ? nullptr : B->dd[cur].p, B->chpos.p, B->chd.p,
+                                        B->pos[1 - cur].p, B->dd[1 - cur].p, nullptr, st));
             cur = 1 - cur;
         } else {
             PT_CUDA(cudaMemcpyAsync(B->pos[cur].p, B->chpos.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
             PT_CUDA(cudaMemcpyAsync(B->dd[cur].p, B->chd.p, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
         }
     }
+    if (direct_out) return PT_OK;
+    if (passes == 0) PT_TRY(pt_launch_init(n, pt_xy(v.w - 7 + 1, 0), (float) PT_DIST_INF, B->pos[0].p, B->dd[0].p, st));
     return pt_launch_output(n, B->pos[cur].p, B->dd[cur].p, d_ann, st);
 }
 
@@ -139,7 +145,7 @@ pt_status pt_batch_create(pt_table *t, int n, const int *h, const int *w, pt_bat
     B->ntiles = tiles;
     for (int k = 0; k < PT_BATCH_NTW; k++) B->nseg[k] = seg[k];
     auto fail = [&](pt_status s) { delete B; return s; };
-    if (B->d_imgs.reserve(n) || B->rgba.reserve(pix) || B->desc.reserve((size_t) pat * v.ds) || B->tcand.reserve(pat) ||
+    if (B->d_imgs.reserve(n) || B->rgba.reserve(pix) || B->tcand.reserve(pat) ||
         B->pos[0].reserve(pat) || B->pos[1].reserve(pat) || B->dd[0].reserve(pat) || B->dd[1].reserve(pat) ||
         B->chpos.reserve(pat) || B->chd.reserve(pat) || B->kcdone.reserve(pat))
         return fail(pt_fail(PT_OOM, "batch buffers for %lld pixels / %lld patches", pix, pat));

@@ -184,6 +184,11 @@ pt_status pt_launch_pull_batch(const QuerySetup &s, const PtBatchImage *imgs, in
                                const float *ch_d, int *nxt_pos, float *nxt_d, unsigned long long *evals, cudaStream_t st);
 pt_status pt_launch_descriptor_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
                                      const float *rgb, int convert, float4 *rgba, float *desc, int ds, cudaStream_t st);
+/* The batch's descriptor pass fused with the table step: tcand[p] = table[cell(p)] for every
+   patch of every image, no descriptors stored. */
+pt_status pt_launch_descriptor_cells_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
+                                           const float *rgb, int convert, float4 *rgba, const PtBins &bins, const int *to_bin,
+                                           const int *table, int *tcand, cudaStream_t st);
 
 /* Read-only view of a built table, for entry points outside pt_table.cu. */
 struct PtTableView {
