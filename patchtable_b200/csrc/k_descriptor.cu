@@ -410,13 +410,6 @@ pt_status launch_descriptor_batch(int ndims, int nchroma, const CellPlan &cp, co
 
 }  // namespace
 
-pt_status pt_launch_descriptor_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
-                                     const float *rgb, int convert, float4 *rgba, float *desc, int ds, cudaStream_t st) {
-    CellPlan cp;
-    memset(&cp, 0, sizeof(cp));
-    return launch_descriptor_batch<false>(ndims, nchroma, cp, imgs, n, ntiles, rgb, convert, rgba, desc, ds, st);
-}
-
 pt_status pt_launch_descriptor_cells_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
                                            const float *rgb, int convert, float4 *rgba, const PtBins &bins, const int *to_bin,
                                            const int *table, int *tcand, cudaStream_t st) {

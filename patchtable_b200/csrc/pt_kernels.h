@@ -182,8 +182,6 @@ pt_status pt_launch_choose_batch(const QuerySetup &s, const PtBatchImage *imgs, 
 pt_status pt_launch_pull_batch(const QuerySetup &s, const PtBatchImage *imgs, int n, long long nseg, int twi,
                                const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d, const int *ch_pos,
                                const float *ch_d, int *nxt_pos, float *nxt_d, unsigned long long *evals, cudaStream_t st);
-pt_status pt_launch_descriptor_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
-                                     const float *rgb, int convert, float4 *rgba, float *desc, int ds, cudaStream_t st);
 /* The batch's descriptor pass fused with the table step: tcand[p] = table[cell(p)] for every
    patch of every image, no descriptors stored. */
 pt_status pt_launch_descriptor_cells_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
