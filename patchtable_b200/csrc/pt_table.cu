@@ -634,12 +634,12 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
                                        t->q_rgba.p, t->b_rgba.p, t->q_pos[0].p, t->q_d[0].p, t->q_torig.p, t->q_tbad.p, st));
         PT_CUDA(cudaMemcpyAsync(t->q_tpos0.p, t->q_pos[0].p, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
         PT_CUDA(cudaMemcpyAsync(t->q_td0.p, t->q_d[0].p, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
-    } else if (net) {
+    } else if (net || pt_default_passes(p) == 0) {
         /* Initial field (patchtable.h:3538-3547): x = b0_ew + 1, dist = DIST_INFINITY. */
         PT_TRY(pt_launch_init(n, pt_xy(t->ew + 1, 0), (float) PT_DIST_INF, t->q_pos[0].p, t->q_d[0].p, st));
     }
     /* Otherwise the first pass reads no state arrays: its kernels start from the initial field. */
-    const bool fresh = !p.init_random && !d_prev && !net;
+    const bool fresh = !p.init_random && !d_prev && !net && pt_default_passes(p) > 0;
     /* the last pull writes the NNF itself unless the temporal output has to restore distances */
     const bool direct_out = p.do_prop && pt_default_passes(p) > 0 && !(d_prev && !p.init_random && p.coherence_temporal != 0.0);
     PT_TRY(mark(t, prof, LookupProfile::INIT, st));

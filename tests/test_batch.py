@@ -130,3 +130,22 @@ def test_batch_other_colour_spaces_and_search(gpu, libc, sw):
     single = [t.lookup(x) for x in imgs]
     for s, h in zip(single, t.lookup_batch(imgs)):
         assert np.array_equal(s, h)
+
+
+@pytest.mark.parametrize("sw", ["-speed 3 -do_prop 0 -limit 2", "-speed 3 -prop_iters 0 -limit 2"])
+def test_schedules_without_propagation(gpu, oracle, libc, sw):
+    """Without propagation the last step is not a pull (the output is written by its own launch)
+    and with no iterations the field stays the initial one: batches, device and host lookups all
+    agree, and with prop_iters 0 the NNF equals the oracle's initial field exactly."""
+    t, b = _table(libc, sw)
+    imgs = _queries(700)[:4]
+    single = [t.lookup(x) for x in imgs]
+    for s, h in zip(single, t.lookup_batch(imgs)):
+        assert np.array_equal(s, h)
+    if "-prop_iters 0" in sw:
+        ot = oracle.build(t.params.as_dict(), b)
+        for x, s in zip(imgs, single):
+            assert np.array_equal(s, ot.lookup(x))
+    else:
+        for x, s in zip(imgs, single):
+            check_nnf(oracle, x, b, s, sample=300)
