@@ -10,7 +10,8 @@ built once before warm-up.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
   python bench.py --profile-case query|query-default|infer|build  (short fixed runs for ncu)
 
-Prints one JSON line (rank 0).  `value` is query patches per second of device time with a already
+Prints one JSON line (rank 0).  `value` is query patches per second of device time (one CUDA event
+pair around each pt_table_lookup_device call) with a already
 in device memory (L2 flushed between steps) at the fastest query schedule whose mean NNF distance
 is within 1% of the reference's on this workload; `e2e` is the same metric through the public host
 API (pt_table_lookup) with pinned host buffers, copies included.  config.learned compares the
@@ -236,21 +237,27 @@ def profile_case(name):
 
 
 def timed_schedule(table, sched, da, H, W, dann, sptr, flush, reps=3, net=None):
-    """(best device ms of `reps` lookups after one untimed, mean NNF dist) of one schedule."""
+    """(best device ms of `reps` lookups after one untimed, mean NNF dist) of one schedule: one CUDA
+    event pair around each production call (pt_table_lookup_device or its learned form)."""
     import torch
     from patchtable_b200.metrics import get_mean_dist
     p = table.params
     p.gpu_prop_passes, p.gpu_jump, p.gpu_pull_max = sched
+    stream = torch.cuda.current_stream()
     best = None
     for i in range(reps + 1):
         flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         if net is None:
-            st, _ = table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
+            table.lookup_device(da.data_ptr(), H, W, dann.data_ptr(), sptr)
         else:
-            st, _ = table.lookup_learned_profile(net, da.data_ptr(), H, W, dann.data_ptr(), sptr)
+            table.lookup_learned_device(net, da.data_ptr(), H, W, dann.data_ptr(), sptr)
+        e1.record(stream)
+        e1.synchronize()
         if i > 0:
-            tot = sum(st.values())
-            best = tot if best is None else min(best, tot)
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
     torch.cuda.synchronize()
     return best, get_mean_dist(dann.cpu().numpy())
 
@@ -436,37 +443,44 @@ def main():
     params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = chosen
     for _ in range(max(args.warmup, 3)):
         flush.zero_()
-        table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
+        table.lookup_device(da.data_ptr(), H, W, dann.data_ptr(), sptr)
     torch.cuda.synchronize()
     md = mean_dist(dann.cpu().numpy())
 
+    # the timed region: one CUDA event pair around each production call (pt_table_lookup_device)
     clocks = Clocks(local)
     replicas.barrier()
     torch.cuda.synchronize()
     clocks.start()
     ptb.reset_launch_count()
-    stages, ctrs = {k: 0.0 for k in ptb.PatchTable.STAGES}, {}
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     tw0 = time.perf_counter()
     for i in range(args.steps):
         flush.zero_()                       # evict L2 between steps (outside the timed events)
         ev[i][0].record(stream)
-        st, c = table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
+        table.lookup_device(da.data_ptr(), H, W, dann.data_ptr(), sptr)
         ev[i][1].record(stream)
-        for k, v in st.items():
-            stages[k] += v
-        for k, v in c.items():
-            ctrs[k] = ctrs.get(k, 0) + v
     torch.cuda.synchronize()
     wall = time.perf_counter() - tw0
     launches = ptb.launch_count()
     replicas.barrier()
     clk = clocks.stop()
-    # device time per step: the sum of the stage times (CUDA events around every kernel on the
-    # launching stream); the outer events also include the library's host-side launch gaps.
-    outer = [e0.elapsed_time(e1) for e0, e1 in ev]
-    tot_ms = replicas.max_over_ranks(sum(stages.values()), dev)
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    tot_ms = replicas.max_over_ranks(sum(step_ms), dev)
     value = replicas.whole_job_rate(P * args.steps, tot_ms / 1000.0, world)
+    md_timed = mean_dist(dann.cpu().numpy())
+
+    # per-kernel breakdown for the roofline: the same steps again through the diagnostic entry
+    # point, which records a CUDA event after every kernel on the launching stream
+    stages, ctrs = {k: 0.0 for k in ptb.PatchTable.STAGES}, {}
+    for i in range(args.steps):
+        flush.zero_()
+        st, c = table.lookup_profile(da.data_ptr(), H, W, dann.data_ptr(), sptr)
+        for k, v in st.items():
+            stages[k] += v
+        for k, v in c.items():
+            ctrs[k] = ctrs.get(k, 0) + v
+    torch.cuda.synchronize()
 
     # end-to-end through the public host API with pinned buffers
     a_pin = torch.from_numpy(a).pin_memory()
@@ -483,6 +497,14 @@ def main():
         e2e_s.append(time.perf_counter() - t1)
     e2e = replicas.whole_job_rate(P, replicas.max_over_ranks(sum(e2e_s) / len(e2e_s), dev), world)
     md_e2e = mean_dist(ann_np)
+    # the transfer floor of e2e: the same bytes copied alone between pinned host and device memory
+    dann_flat = dann.view(-1)
+    h2d_ms = _event_ms(lambda: da.copy_(a_pin, non_blocking=True), 5)
+    d2h_ms = _event_ms(lambda: ann_pin.view(-1).copy_(dann_flat, non_blocking=True), 5)
+    e2e_mean_ms = 1000 * sum(e2e_s) / len(e2e_s)
+    transfer = {"h2d_ms": h2d_ms, "d2h_ms": d2h_ms, "h2d_gbs": a.nbytes / h2d_ms / 1e6, "d2h_gbs": ann_np.nbytes / d2h_ms / 1e6,
+                "floor_ms": max(h2d_ms, d2h_ms), "floor_frac_of_e2e": max(h2d_ms, d2h_ms) / e2e_mean_ms,
+                "note": "floor = the slower of the two copies alone (perfect overlap of upload, kernels and download)"}
 
     # the library's default schedule on the same workload, for reference
     dflt_ms, dflt_md = timed_schedule(table, (0, 0, 0), da, H, W, dann, sptr, flush, reps=max(3, args.steps // 2))
@@ -504,7 +526,9 @@ def main():
     later = (passes - 1) / passes
     alg_bytes = {"choose": 64 + 8 * later, "pull": 40 + 8 * later + (24 + 8 * (passes - 1)) / passes}[dom] * P
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
-    traffic, l1 = None, None
+    # DRAM traffic and the L1 data-pipe share cannot be measured inside this run: they come from
+    # the committed ncu summary of the same kernel and schedule, which names its source revision
+    traffic, l1, prof_src = None, None, {"file": "profiles/query_%s_c2.md" % dom, "source_revision": None}
     try:
         with open(os.path.join(ROOT, "profiles", "query_%s_c2.md" % dom)) as f:
             for line in f:
@@ -512,6 +536,8 @@ def main():
                     traffic = float(line.split(":")[1])
                 if line.startswith("l1tex_wavefront_pct_of_peak:"):
                     l1 = float(line.split(":")[1])
+                if line.startswith("source_revision:"):
+                    prof_src["source_revision"] = line.split(":", 1)[1].strip()
     except OSError:
         pass
     rows = ctrs.get(dom + "_rows", 0)
@@ -543,13 +569,16 @@ def main():
                                 "patches_per_cta": params.gpu_tile, "patches_per_cta_ms": {str(k): v for k, v in tile_ms.items()},
                                 "rule": "fastest schedule with mean NNF dist <= 1.01 x the reference's on this workload"},
                    "library_default_schedule": default_sched, "learned": learned,
-                   "uneven_batch": c4, "one_vs_many": c3,
+                   "uneven_batch": c4, "one_vs_many": c3, "mean_nnf_dist_timed": md_timed,
                    "l2": "flushed between steps (256 MiB write)", "parallelism": "replicas" if world > 1 else "single",
+                   "timing": "one CUDA event pair around each pt_table_lookup_device call on its stream",
+                   "step_ms": {"min": min(step_ms), "median": float(np.median(step_ms)), "max": max(step_ms)},
                    "stage_ms_per_step": {k: v / args.steps for k, v in stages.items()},
-                   "outer_event_ms_per_step": sum(outer) / len(outer), "wall_ms_per_step": 1000 * wall / args.steps,
+                   "stage_ms_source": "pt_table_lookup_profile (an event after every kernel), same steps, run after the timed region",
+                   "e2e_transfer": transfer, "wall_ms_per_step": 1000 * wall / args.steps,
                    "ssd_candidates_per_patch": {k: ctrs.get(k + "_cand", 0) / (args.steps * P) for k in ("choose", "pull")}},
         "roofline": {"bound": "hbm", "kernel": "k_" + dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_kind,
+                     "frac": achieved / hbm, "traffic": traffic, "traffic_source": prof_src, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "limiter": {"unit": "L1TEX data-pipe wavefronts", "pct_of_peak_ncu": l1},
                      "fp32": {"achieved_tflops": fp32_tflops, "flop_per_ssd_row": 72,

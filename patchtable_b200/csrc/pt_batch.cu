@@ -80,10 +80,11 @@ pt_status run(pt_batch *B, const float *d_rgb, double *d_ann, cudaStream_t st) {
         const bool do_table = i == 0 && p.do_table_lookup;
         QuerySetup qi = qs;
         qi.pass = i;
-        if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
+        if (!pt_pass_kcoh(p, i, passes)) qi.kcoherence = 0;
+        const int use_done = i > 0 && pt_pass_kcoh(p, i - 1, passes);
         PT_TRY(pt_launch_choose_batch(qi, B->d_imgs.p, B->n, B->nseg[B->twi], B->twi, B->rgba.p, v.b_rgba,
                                       i == 0 ? nullptr : B->pos[cur].p, i == 0 ? nullptr : B->dd[cur].p, B->tcand.p, v.kcoh,
-                                      do_table, B->chpos.p, B->chd.p, B->kcdone.p, i > 0, nullptr, st));
+                                      do_table, B->chpos.p, B->chd.p, B->kcdone.p, use_done, nullptr, st));
         if (p.do_prop) {
             QuerySetup qp = qs;
             qp.step = pt_pass_step(i, passes, jump);

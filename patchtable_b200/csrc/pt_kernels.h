@@ -129,6 +129,16 @@ inline int pt_default_jump(const pt_params &p, int passes) {
     for (int i = 1; i < passes && j < 8; i++) j *= 2;
     return j;
 }
+/* Whether choose pass i of `passes` runs k-coherence.  The reference runs it on every sweep, or
+   only on sweep kcoherence_iter when that is >= 0 (patchtable.h:3612); GPU pass i stands in for
+   sweep floor(i * prop_iters / passes), i.e. passes 2n and 2n+1 for sweep n by default. */
+inline bool pt_pass_kcoh(const pt_params &p, int i, int passes) {
+    if (p.kcoherence <= 0) return false;
+    if (p.kcoherence_iter < 0) return true;
+    const int iters = p.prop_iters > 0 ? p.prop_iters : 1;
+    const int sweep = passes > 0 ? (int) ((long long) i * iters / passes) : 0;
+    return sweep == p.kcoherence_iter;
+}
 /* Neighbour spacing of pull pass i: halving from `jump` down to 1, then 1. */
 inline int pt_pass_step(int i, int n, int jump) {
     (void) n;

@@ -105,6 +105,7 @@ extern "C" pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_
     if (qs.radius > 2) qs.radius = 2;
     qs.b1 = v.b_rgba1;
     qs.pull_max = p.gpu_pull_max;
+    qs.tile = p.gpu_tile;
     qs.allowed = v.allowed;
     qs.allowed_index = p.allowed_index;
     qs.stream = st;
@@ -116,9 +117,10 @@ extern "C" pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_
         bool do_table = i == 0 && p.do_table_lookup;
         QuerySetup qi = qs;
         qi.pass = i;
-        if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
+        if (!pt_pass_kcoh(p, i, passes)) qi.kcoherence = 0;
+        const int use_done = i > 0 && pt_pass_kcoh(p, i - 1, passes);
         PT_TRY(pt_launch_choose(qi, n, rgba, v.b_rgba, pos[cur], dd[cur], tcand, v.kcoh, do_table, chpos, chd,
-                                kcdone, i > 0, nullptr, st));
+                                kcdone, use_done, nullptr, st));
         if (p.do_prop) {
             QuerySetup qp = qs;
             qp.step = pt_pass_step(i, passes, jump);

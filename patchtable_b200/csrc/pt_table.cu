@@ -648,20 +648,22 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     int cur = 0;
     for (int i = 0; i < passes; i++) {
         /* Pass 0 plays the reference's first iteration (table lookup, :3641); k-coherence runs
-           on every pass unless restricted to iteration 0 (kcoherence_iter). */
+           on the passes of the sweeps that kcoherence_iter selects.  A pass skips a repeated
+           k-coherence search only when the previous pass ran one (and so wrote kc_done). */
         bool do_table = i == 0 && p.do_table_lookup;
         QuerySetup qi = qs;
         qi.pass = i;
-        if (!(p.kcoherence_iter < 0 || (p.kcoherence_iter == 0 ? i == 0 : i > 0))) qi.kcoherence = 0;
+        if (!pt_pass_kcoh(p, i, passes)) qi.kcoherence = 0;
+        const int use_done = i > 0 && pt_pass_kcoh(p, i - 1, passes);
         if (net)
             PT_TRY(pt_launch_choose_learned(qi, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_tcand.p,
-                                            t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, i > 0,
+                                            t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, use_done,
                                             i == 0 ? t->q_lcand.p : nullptr, t->q_lconf.p, pt_prop_threshold(net),
                                             pt_prop_kcoh_confident(net), ctr, ctr ? ctr + 4 : nullptr, st));
         else
             PT_TRY(pt_launch_choose(qi, n, t->q_rgba.p, t->b_rgba.p, fresh && i == 0 ? nullptr : t->q_pos[cur].p,
                                     fresh && i == 0 ? nullptr : t->q_d[cur].p, t->q_tcand.p, t->kcoh.p, do_table,
-                                    t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, i > 0, ctr, st));
+                                    t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, use_done, ctr, st));
         PT_TRY(mark(t, prof, LookupProfile::CHOOSE, st));
         if (p.do_prop) {
             QuerySetup qp = qs;
@@ -745,7 +747,7 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     qs.aw = w; qs.ah = h; qs.bw = t->w; qs.bh = t->h;
     qs.prop_scale = 1.0 / (1 + p.coherence_spatial);
     qs.triangle_factor = p.triangle_factor;
-    qs.kcoherence = (p.kcoherence_iter < 0 || p.kcoherence_iter == 0) ? p.kcoherence : 0;
+    qs.kcoherence = pt_pass_kcoh(p, 0, 1) ? p.kcoherence : 0;
     qs.kcoherence_step = p.kcoherence_step;
     qs.spatial = p.spatial;
     qs.do_rs = p.do_rs;

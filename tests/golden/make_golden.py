@@ -9,11 +9,15 @@ the restatement to the reference on machines where the reference cannot be built
 Also records the reference's result on the repository's sample pair patchtable/vidpair0 (the pair
 of patchtable/match_ours_full.txt:4, mean_dist 0.130757 at -speed 3 with the original FLANN).
 
-Run here (needs /root/reference and a built oracle/_ref):  python tests/golden/make_golden.py
+Needs the reference checkout ($PATCHTABLE_REFERENCE, else the location oracle/Makefile reads) and a
+built oracle/_ref:
+    python tests/golden/make_golden.py          every entry
+    python tests/golden/make_golden.py --c2     only the 1920x1080 entry (digests of every stage)
 """
 import hashlib
 import json
 import os
+import subprocess
 import sys
 
 import numpy as np
@@ -103,9 +107,18 @@ def run_desc_case(ref: Reference, case: dict) -> dict:
     return out
 
 
+def reference_dir() -> str:
+    env = os.environ.get("PATCHTABLE_REFERENCE")
+    if env:
+        return env
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "print-ref"], stdout=subprocess.PIPE,
+                       text=True, check=True)
+    return r.stdout.strip()
+
+
 def vidpair0(ref: Reference) -> dict:
     from PIL import Image
-    base = "/root/reference/patchtable/vidpair0"
+    base = os.path.join(reference_dir(), "patchtable", "vidpair0")
 
     def load(fn):
         # load_color_image for PNG: (real)(px * (1/255.0)), solver/array.h:1676-1680
@@ -122,11 +135,16 @@ def vidpair0(ref: Reference) -> dict:
 def main():
     ref = Reference()
     ref.set_threads(1)          # do_dt_brute shares one grid_index vector across its OpenMP loop (patchtable.h:2370-2376)
-    res = {"cases": [run_case(ref, c) for c in CASES]}
-    res["desc"] = [run_desc_case(ref, c) for c in DESC_CASES]
-    res["c2"] = run_case(ref, C2, full=False)
-    res["vidpair0"] = vidpair0(ref)
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle_golden.json")
+    if "--c2" in sys.argv:
+        with open(path) as f:
+            res = json.load(f)
+        res["c2"] = run_case(ref, C2, full=True)
+    else:
+        res = {"cases": [run_case(ref, c) for c in CASES]}
+        res["desc"] = [run_desc_case(ref, c) for c in DESC_CASES]
+        res["c2"] = run_case(ref, C2, full=True)
+        res["vidpair0"] = vidpair0(ref)
     with open(path, "w") as f:
         json.dump(res, f, indent=1)
     print(json.dumps({c["name"]: c["mean_dist"] for c in res["cases"] + [res["c2"], res["vidpair0"]]}, indent=1))

@@ -305,8 +305,11 @@ def check_nnf(oracle, a, b, ann, sample=4000):
 
 
 @pytest.mark.parametrize("seed,sw", [(1, ""), (2, ""), (3, "-coherence_spatial 4"), (1, "-coherence_spatial 4"),
-                                     (4, "-kcoherence 4 -prop_iters 3"), (5, "-speed 6")])
+                                     (4, "-kcoherence 4 -prop_iters 3"), (5, "-speed 6"), (6, "-kcoherence_iter 1"),
+                                     (7, "-kcoherence 4 -kcoherence_iter 0"), (8, "-kcoherence_iter 2 -prop_iters 3")])
 def test_nnf_quality_and_distances(gpu, oracle, libc, seed, sw):
+    """Exact distances and the mean within 1% of the oracle's; -kcoherence_iter n restricts
+    k-coherence to the passes of sweep n (patchtable.h:3612), and repeated lookups are identical."""
     a, b = synth.pair(240, 320, seed)
     p = ptb.PatchTableParams(sw + " -limit 10")
     srand_all(libc, 1)
@@ -318,6 +321,7 @@ def test_nnf_quality_and_distances(gpu, oracle, libc, seed, sw):
     check_nnf(oracle, a, b, ann)
     mg = mean_dist(ann)
     assert mg <= MEAN_DIST_SLACK * mo, (mg, mo)
+    assert np.array_equal(ann, gt.lookup(a))
 
 
 def test_query_of_another_size_and_reuse(gpu, oracle, libc):

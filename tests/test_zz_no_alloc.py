@@ -23,13 +23,15 @@ def _fn():
     return f
 
 
-def test_noalloc_lookup_matches_device_lookup_on_consecutive_calls():
+@pytest.mark.parametrize("sw", ["-limit 2", "-limit 2 -prop_iters 0", "-limit 2 -do_prop 0", "-limit 2 -gpu_tile 128",
+                                "-limit 2 -kcoherence_iter 1 -gpu_tile 64"])
+def test_noalloc_lookup_matches_device_lookup_on_consecutive_calls(sw):
     import torch
     assert torch.cuda.is_available()
     noalloc = _fn()
     C.CDLL(None).srand(1)
     _, b = synth.pair(200, 260, 41)
-    table = ptb.PatchTable(ptb.PatchTableParams("-limit 2"), b)
+    table = ptb.PatchTable(ptb.PatchTableParams(sw), b)
     stream = torch.cuda.current_stream().cuda_stream
     # two calls in a row on the same image, then a call on an image of another size
     for (h, w, seed) in [(300, 400, 42), (300, 400, 42), (257, 509, 43)]:
@@ -42,6 +44,33 @@ def test_noalloc_lookup_matches_device_lookup_on_consecutive_calls():
         assert st == 0, ptb.lib().pt_last_error()
         torch.cuda.synchronize()
         assert torch.equal(expect, got)
+    table.close()
+
+
+def test_noalloc_lookup_allocates_no_device_memory():
+    """After a first call (which may load the kernels), further calls leave the device's free
+    memory unchanged: nothing is allocated, not even temporarily for the call's duration."""
+    import torch
+    noalloc = _fn()
+    C.CDLL(None).srand(1)
+    _, b = synth.pair(150, 190, 45)
+    table = ptb.PatchTable(ptb.PatchTableParams("-limit 1"), b)
+    stream = torch.cuda.current_stream().cuda_stream
+    h, w = 240, 320
+    da = torch.from_numpy(synth.image_a(h, w, 46)).cuda()
+    out = torch.empty((h - 7, w - 7, 3), dtype=torch.float64, device="cuda")
+    assert noalloc(table._h, da.data_ptr(), h, w, out.data_ptr(), stream) == 0, ptb.lib().pt_last_error()
+    torch.cuda.synchronize()
+    first = out.clone()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        assert noalloc(table._h, da.data_ptr(), h, w, out.data_ptr(), stream) == 0, ptb.lib().pt_last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.equal(first, out)
+    table.close()
 
 
 def test_noalloc_rejects_images_over_the_limit():
