@@ -20,6 +20,7 @@
 #include <memory>
 #include <vector>
 #include "knn_exact.h"
+#include "pca_jacobi.h"
 #include "gck_steps.h"
 
 using std::vector;
@@ -320,87 +321,37 @@ void padded_descriptor(const orc_params &p, const float *rgb, int h, int w, vect
 }
 
 /* ------------------------------------------------------------------------------------------
-   -dim_algo pca, patch_pca.h.  OpenCV is not available, so cv::PCA(DATA_AS_ROW, maxComponents
-   = ndims) is restated from its published definition: sample mean (zero without
-   pca_subtract_mean), covariance (1/n) sum (x - mean)(x - mean)^T in double, its eigenvectors by
-   cyclic Jacobi rotations, ordered by decreasing eigenvalue and signed so that the entry of
-   largest magnitude is positive.  Parity with the reference is unpinned here (its OpenCV is
-   absent); the restatement pins the GPU path's fit and projection.
+   -dim_algo pca, patch_pca.h.  cv::PCA(DATA_AS_ROW, maxComponents = ndims) is restated in
+   pca_jacobi.h (sample mean or zero mean, covariance, cyclic Jacobi eigenvectors); the same
+   header stands in for OpenCV in the reference build, so the reference's own sampling and
+   projection (patch_pca.h:14-113) run there and pin this restatement by digest.
    ------------------------------------------------------------------------------------------ */
-/* extract_patches + get_patch_pca, patch_pca.h:14-52, on the colour-converted image. */
+/* The 192-vector the reference builds for the patch at (ax, ay) (extract_patches and
+   apply_patch_pca, patch_pca.h:30-37, 87-96): for row dy, column dx and channel c it reads
+   arow[dx] [c], where arow points at float 0 of pixel (ax, ay + dy) of the interleaved image, so
+   entry (dy, dx, c) is float dx + c of that row -- floats 0..9, i.e. the first three pixels and a
+   third, not pixel dx.  Restated as written, since the descriptor values depend on it. */
+inline void pca_patch_vector(const float *img, int w, int ax, int ay, float *v) {
+    int k = 0;
+    for (int dy = 0; dy < PW; dy++) {
+        const float *arow = img + ((size_t) (ay + dy) * w + ax) * 3;
+        for (int dx = 0; dx < PW; dx++)
+            for (int c = 0; c < 3; c++) v[k++] = arow[dx + c];
+    }
+}
+
+/* extract_patches + get_patch_pca, patch_pca.h:14-52, on the colour-converted image: sample i is
+   the patch at (rand() % (w-7), rand() % (h-7)). */
 void pca_fit(const orc_params &p, const float *img, int h, int w, Pca &out) {
     const int n = p.pca_samples, aew = w - PW + 1, aeh = h - PW + 1;
-    vector<double> X((size_t) n * PCA_D);
+    vector<float> X((size_t) n * PCA_D);
     for (int i = 0; i < n; i++) {
         int ax = rand() % aew;
         int ay = rand() % aeh;
-        int k = 0;
-        for (int dy = 0; dy < PW; dy++)
-            for (int dx = 0; dx < PW; dx++)
-                for (int c = 0; c < 3; c++) X[(size_t) i * PCA_D + k++] = img[((size_t) (ay + dy) * w + ax + dx) * 3 + c];
+        pca_patch_vector(img, w, ax, ay, &X[(size_t) i * PCA_D]);
     }
-    vector<double> mu(PCA_D, 0.0);
-    if (p.pca_subtract_mean) {
-        for (int i = 0; i < n; i++)
-            for (int j = 0; j < PCA_D; j++) mu[j] += X[(size_t) i * PCA_D + j];
-        for (int j = 0; j < PCA_D; j++) mu[j] /= n;
-    }
-    vector<double> A((size_t) PCA_D * PCA_D, 0.0);
-    for (int i = 0; i < n; i++)
-        for (int a = 0; a < PCA_D; a++) {
-            double da = X[(size_t) i * PCA_D + a] - mu[a];
-            for (int b = a; b < PCA_D; b++) A[(size_t) a * PCA_D + b] += da * (X[(size_t) i * PCA_D + b] - mu[b]);
-        }
-    for (int a = 0; a < PCA_D; a++)
-        for (int b = a; b < PCA_D; b++) { A[(size_t) a * PCA_D + b] /= n; A[(size_t) b * PCA_D + a] = A[(size_t) a * PCA_D + b]; }
-    /* cyclic Jacobi */
-    vector<double> V((size_t) PCA_D * PCA_D, 0.0);
-    for (int i = 0; i < PCA_D; i++) V[(size_t) i * PCA_D + i] = 1.0;
-    for (int sweep = 0; sweep < 100; sweep++) {
-        double off = 0.0, on = 0.0;
-        for (int i = 0; i < PCA_D; i++)
-            for (int j = 0; j < PCA_D; j++) {
-                double v = A[(size_t) i * PCA_D + j];
-                if (i == j) on += v * v; else off += v * v;
-            }
-        if (off == 0.0 || off <= 1e-30 * on) break;
-        for (int r = 0; r < PCA_D - 1; r++)
-            for (int q = r + 1; q < PCA_D; q++) {
-                double arq = A[(size_t) r * PCA_D + q];
-                if (arq == 0.0) continue;
-                double theta = (A[(size_t) q * PCA_D + q] - A[(size_t) r * PCA_D + r]) / (2.0 * arq);
-                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-                double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
-                for (int k = 0; k < PCA_D; k++) {
-                    double x = A[(size_t) k * PCA_D + r], y = A[(size_t) k * PCA_D + q];
-                    A[(size_t) k * PCA_D + r] = c * x - sn * y;
-                    A[(size_t) k * PCA_D + q] = sn * x + c * y;
-                }
-                for (int k = 0; k < PCA_D; k++) {
-                    double x = A[(size_t) r * PCA_D + k], y = A[(size_t) q * PCA_D + k];
-                    A[(size_t) r * PCA_D + k] = c * x - sn * y;
-                    A[(size_t) q * PCA_D + k] = sn * x + c * y;
-                }
-                for (int k = 0; k < PCA_D; k++) {
-                    double x = V[(size_t) k * PCA_D + r], y = V[(size_t) k * PCA_D + q];
-                    V[(size_t) k * PCA_D + r] = c * x - sn * y;
-                    V[(size_t) k * PCA_D + q] = sn * x + c * y;
-                }
-            }
-    }
-    vector<int> ord(PCA_D);
-    for (int i = 0; i < PCA_D; i++) ord[i] = i;
-    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return A[(size_t) x * PCA_D + x] > A[(size_t) y * PCA_D + y]; });
-    out.mean.resize(PCA_D);
-    for (int j = 0; j < PCA_D; j++) out.mean[j] = (float) mu[j];
-    out.basis.assign((size_t) p.ndims * PCA_D, 0.0f);
-    for (int k = 0; k < p.ndims; k++) {
-        int col = ord[k], big = 0;
-        for (int j = 1; j < PCA_D; j++)
-            if (fabs(V[(size_t) j * PCA_D + col]) > fabs(V[(size_t) big * PCA_D + col])) big = j;
-        double sg = V[(size_t) big * PCA_D + col] < 0 ? -1.0 : 1.0;
-        for (int j = 0; j < PCA_D; j++) out.basis[(size_t) k * PCA_D + j] = (float) (sg * V[(size_t) j * PCA_D + col]);
-    }
+    const vector<float> zero(PCA_D, 0.0f);
+    pt_pca_jacobi_fit(X.data(), n, PCA_D, !p.pca_subtract_mean, zero.data(), p.ndims, out.mean, out.basis);
 }
 
 /* apply_patch_pca, patch_pca.h:54-110 (pca_mean off): channel k of the patch at (x, y) goes to
@@ -411,16 +362,9 @@ void pca_apply(const orc_params &p, const Pca &pca, const float *img, int h, int
     vector<float> v(PCA_D);
     for (int ay = 0; ay + PW <= h; ay++)
         for (int ax = 0; ax + PW <= w; ax++) {
-            int k = 0;
-            for (int dy = 0; dy < PW; dy++)
-                for (int dx = 0; dx < PW; dx++)
-                    for (int c = 0; c < 3; c++) v[k++] = img[((size_t) (ay + dy) * w + ax + dx) * 3 + c];
-            float *o = &wh[((size_t) (ay + PW - 1) * WW + ax + PW - 1) * nd];
-            for (int ch = 0; ch < nd; ch++) {
-                float acc = 0.0f;
-                for (int j = 0; j < PCA_D; j++) acc = acc + (v[j] - pca.mean[j]) * pca.basis[(size_t) ch * PCA_D + j];
-                o[ch] = acc;
-            }
+            pca_patch_vector(img, w, ax, ay, v.data());
+            pt_pca_project(v.data(), PCA_D, pca.mean.data(), pca.basis.data(), nd,
+                           &wh[((size_t) (ay + PW - 1) * WW + ax + PW - 1) * nd]);
         }
 }
 

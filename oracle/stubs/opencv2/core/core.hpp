@@ -1,12 +1,16 @@
 /* Stand-in for the OpenCV names the reference mentions (solver/array.h:37, 95-129, 1441-1545,
    3221-3285; patchtable/patch_pca.h:5-113).  OpenCV is only reached by non-default options
-   (-dim_algo pca, image resizing in apps); the container type works, the algorithms abort. */
+   (-dim_algo pca, image resizing in apps).  The container type works; cv::PCA is the published
+   method restated in oracle/pca_jacobi.h (single-channel float data as rows, the mean given or
+   sampled), so the reference's own patch sampling and projection loop run; the other
+   algorithms abort. */
 #ifndef PTSTUB_OPENCV_CORE_HPP
 #define PTSTUB_OPENCV_CORE_HPP
 #include <vector>
 #include <cstdio>
 #include <cstdlib>
 #include <cstdint>
+#include "../../../pca_jacobi.h"
 #define PTSTUB_CV_MAKETYPE(depth, cn) ((depth) + (((cn) - 1) << 3))
 #define CV_8U 0
 #define CV_16U 2
@@ -50,8 +54,24 @@ class Mat { public:
     static Mat zeros(int r, int c, int t) { return Mat(r, c, t); }
 };
 class PCA { public:
-    PCA(const Mat &, const Mat &, int, int) { ptstub_cv_abort("PCA"); }
-    void project(const Mat &, Mat &) const { ptstub_cv_abort("PCA::project"); }
+    std::vector<float> mean_, basis_;
+    int d_ = 0, k_ = 0;
+    /* data: n x d CV_32FC1 rows; mean: empty (sample mean) or 1 x d CV_32FC1. */
+    PCA(const Mat &data, const Mat &mean, int flags, int maxComponents) {
+        if (flags != CV_PCA_DATA_AS_ROW || data.type_ != CV_32FC1 || data.rows < 1 ||
+            (mean.rows && (mean.rows != 1 || mean.cols != data.cols || mean.type_ != CV_32FC1)))
+            ptstub_cv_abort("PCA with these arguments");
+        d_ = data.cols;
+        k_ = maxComponents > 0 && maxComponents < d_ ? maxComponents : d_;
+        pt_pca_jacobi_fit(data.ptr<float>(0), data.rows, d_, mean.rows > 0, mean.rows ? mean.ptr<float>(0) : nullptr, k_,
+                          mean_, basis_);
+    }
+    void project(const Mat &vec, Mat &result) const {
+        if (vec.rows != 1 || vec.cols != d_ || vec.type_ != CV_32FC1 || result.rows != 1 || result.cols < k_ ||
+            result.type_ != CV_32FC1)
+            ptstub_cv_abort("PCA::project with these arguments");
+        pt_pca_project(vec.ptr<float>(0), d_, mean_.data(), basis_.data(), k_, result.ptr<float>(0));
+    }
 };
 inline void resize(const Mat &, Mat &, Size, double = 0, double = 0, int = 0) { ptstub_cv_abort("resize"); }
 inline void GaussianBlur(const Mat &, Mat &, Size, double, double = 0, int = 0) { ptstub_cv_abort("GaussianBlur"); }

@@ -232,9 +232,11 @@ k_descriptor_batch(const DescPlan c_plan, const CellPlan cp, const PtBatchImage 
 }
 
 /* -dim_algo pca projection (apply_patch_pca, patch_pca.h:60-110): descriptor channel k of a
-   patch = sum over the patch's 192 values v_j (row, column, channel order) of (v_j - mean_j) *
-   basis[k][j], accumulated in j order with separately rounded products and sums.  Each thread
-   projects two patches of the block (rows pi and pi + 4) so that every basis load serves both;
+   patch = sum over the patch's 192 values v_j of (v_j - mean_j) * basis[k][j], accumulated in j
+   order with separately rounded products and sums.  Value j = (dy * 8 + dx) * 3 + c is float
+   dx + c of the interleaved patch row dy, as the reference reads it (its row pointer advances by
+   dx floats, patch_pca.h:87-96): pixel (dx + c) / 3 of the first four, channel (dx + c) % 3.
+   Each thread projects two patches of the block (rows pi and pi + 4) so that every basis load serves both;
    all lanes read the same basis word, a broadcast. */
 __global__ void __launch_bounds__(NT)
 k_pca(const float *__restrict__ rgb, int h, int w, int convert, float4 *__restrict__ rgba,
@@ -256,8 +258,9 @@ k_pca(const float *__restrict__ rgb, int h, int w, int convert, float4 *__restri
             for (int c = 0; c < 3; c++) {
                 const int j = (dy * 8 + dx) * 3 + c;
                 const float mj = __ldg(mean + j);
-                const float d0 = __fsub_rn(pix[(c * RH + pi + dy) * RWP + pj + dx], mj);
-                const float d1 = __fsub_rn(pix[(c * RH + pi + 4 + dy) * RWP + pj + dx], mj);
+                const int f = dx + c, fc = f % 3, fx = f / 3;        /* float f of the row: pixel fx, channel fc */
+                const float d0 = __fsub_rn(pix[(fc * RH + pi + dy) * RWP + pj + fx], mj);
+                const float d1 = __fsub_rn(pix[(fc * RH + pi + 4 + dy) * RWP + pj + fx], mj);
 #pragma unroll
                 for (int k = 0; k < PT_DESC_MAX; k++) {
                     if (k < ncomp) {

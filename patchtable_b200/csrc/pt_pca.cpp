@@ -1,8 +1,9 @@
 /* -dim_algo pca: the patch basis of the table image (get_patch_pca, patchtable/patch_pca.h:45-52).
 
    The reference samples pca_samples patches at (rand() % (w-7), rand() % (h-7)) of the colour-
-   converted image (extract_patches, patch_pca.h:14-43), each a 192-vector ordered (row, column,
-   channel), and hands them to cv::PCA with DATA_AS_ROW and maxComponents = ndims: the sample mean
+   converted image (extract_patches, patch_pca.h:14-43), each a 192-vector whose entry (row dy,
+   column dx, channel c) is float dx + c of the interleaved patch row (the row pointer is indexed
+   by dx floats, patch_pca.h:31-36, not by pixels), and hands them to cv::PCA with DATA_AS_ROW and maxComponents = ndims: the sample mean
    (or zero when pca_subtract_mean is off) and the leading eigenvectors of the covariance
    (1/n) sum (x - mean)(x - mean)^T.  OpenCV is not part of this build, so the decomposition is
    the published cyclic Jacobi method, in double precision; eigenvectors are ordered by
@@ -116,14 +117,20 @@ pt_status pt_pca_fit(const float *rgb, int h, int w, int convert, int samples, i
         const int ay = rand() % aeh;
         double *row = &X[(size_t) i * D];
         int k = 0;
-        for (int dy = 0; dy < 8; dy++)
-            for (int dx = 0; dx < 8; dx++) {
-                const float *px = rgb + ((size_t) (ay + dy) * w + ax + dx) * 3;
+        for (int dy = 0; dy < 8; dy++) {
+            /* the first four colour-converted pixels of the patch row, interleaved: entry (dy, dx, c)
+               is float dx + c of the row (patch_pca.h:31-36 index the row pointer by dx floats) */
+            float conv[12];
+            for (int q = 0; q < 4; q++) {
+                const float *px = rgb + ((size_t) (ay + dy) * w + ax + q) * 3;
                 float c0 = px[0], c1 = px[1], c2 = px[2];
                 if (convert == PT_COLOR_YUV) yuv_host(px[0], px[1], px[2], c0, c1, c2);
                 else if (convert == PT_COLOR_LAB) (*lab)(px[0], px[1], px[2], c0, c1, c2);
-                row[k++] = c0; row[k++] = c1; row[k++] = c2;
+                conv[3 * q] = c0; conv[3 * q + 1] = c1; conv[3 * q + 2] = c2;
             }
+            for (int dx = 0; dx < 8; dx++)
+                for (int c = 0; c < 3; c++) row[k++] = conv[dx + c];
+        }
     }
     std::vector<double> mean(D, 0.0);
     if (subtract_mean) {

@@ -13,6 +13,7 @@ Needs the reference checkout ($PATCHTABLE_REFERENCE, else the location oracle/Ma
 built oracle/_ref:
     python tests/golden/make_golden.py          every entry
     python tests/golden/make_golden.py --c2     only the 1920x1080 entry (digests of every stage)
+    python tests/golden/make_golden.py --add    append the entries of CASES that the file lacks
 """
 import hashlib
 import json
@@ -46,6 +47,14 @@ CASES = [
     dict(name="dt_brute_g2_70x50", h=50, w=70, seed=26, switches="-limit 0.0008 -grid_ndims 2 -dt_algo brute"),
     # The same pair and switches as tiny_64x48: both options leave the reference's table unchanged.
     dict(name="noop_switches_64x48", h=48, w=64, seed=11, switches="-limit 1 -randomize_dt 1 -populate_nearest 0"),
+    # -dim_algo pca: the reference's own patch sampling and projection (patch_pca.h) around the
+    # cv::PCA stand-in of oracle/pca_jacobi.h.
+    dict(name="pca_160x120", h=120, w=160, seed=11, switches="-dim_algo pca -limit 1"),
+    dict(name="pca_nd8_k2_130x100", h=100, w=130, seed=12, switches="-dim_algo pca -ndims 8 -kcoherence 2 -limit 2"),
+    dict(name="pca_nd4_nomean_70x90", h=90, w=70, seed=13,
+         switches="-dim_algo pca -ndims 4 -pca_subtract_mean 0 -pca_samples 300 -limit 0.5"),
+    dict(name="pca_nd12_rgb_110x80", h=80, w=110, seed=14, switches="-dim_algo pca -ndims 12 -colorspace rgb -limit 3"),
+    dict(name="pca_lab_120x90", h=90, w=120, seed=15, switches="-dim_algo pca -colorspace lab -limit 1"),
 ]
 C2 = dict(name="c2_1920x1080_coh4", h=1080, w=1920, seed=2, switches="-speed 3 -coherence_spatial 4")
 # Descriptor mode (is_descriptor): synth.descriptor_pair inputs.  Three channels are left out: the
@@ -65,6 +74,15 @@ def digest(arr) -> str:
     return hashlib.sha256(np.ascontiguousarray(arr).tobytes()).hexdigest()
 
 
+def wh0_digest(wh0, case: dict) -> str:
+    """Digest of a descriptor image.  apply_patch_pca writes only the patch positions
+    (patch_pca.h:82-83) and leaves the 7-pixel border of its freshly resized array uninitialised
+    (solver/array.h:286-287), so PCA descriptors are compared on the patch positions only."""
+    if "-dim_algo pca" in case["switches"]:
+        return digest(wh0[7:case["h"], 7:case["w"]])
+    return digest(wh0)
+
+
 def run_case(ref: Reference, case: dict, full: bool = True) -> dict:
     a, b = synth.pair(case["h"], case["w"], case["seed"])
     ref.srand(1)
@@ -77,7 +95,7 @@ def run_case(ref: Reference, case: dict, full: bool = True) -> dict:
         ns, _ = t.shape()
         out["nslices"] = ns
         out["add_count"] = t.add_count()
-        out["wh0"] = digest(t.wh0())
+        out["wh0"] = wh0_digest(t.wh0(), case)
         out["table"] = digest(t.table())
         parts = [t.partition(d) for d in range(len(ns))]
         out["partition"] = digest(np.concatenate([np.concatenate([p["centers"], p["lsizes"], p["rsizes"],
@@ -140,6 +158,11 @@ def main():
         with open(path) as f:
             res = json.load(f)
         res["c2"] = run_case(ref, C2, full=True)
+    elif "--add" in sys.argv:
+        with open(path) as f:
+            res = json.load(f)
+        have = {c["name"] for c in res["cases"]}
+        res["cases"] += [run_case(ref, c) for c in CASES if c["name"] not in have]
     else:
         res = {"cases": [run_case(ref, c) for c in CASES]}
         res["desc"] = [run_desc_case(ref, c) for c in DESC_CASES]

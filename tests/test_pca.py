@@ -1,11 +1,14 @@
 """-dim_algo pca: the patch-PCA descriptor (patchtable/patch_pca.h) on the GPU.
 
 The reference fits cv::PCA on pca_samples random patches (consuming rand()) and projects every
-patch onto the leading ndims eigenvectors.  OpenCV is not available, so parity with the reference
-is unpinned; the oracle restates the published PCA (sample mean, covariance, Jacobi
-eigenvectors ordered by eigenvalue, largest entry positive) and the GPU path must agree with it:
-descriptors to float rounding of the independently computed bases, tables bit-exact given the
-oracle's descriptors, NNF distances exact and mean distance within 1 %."""
+patch onto the leading ndims eigenvectors; its patch vectors hold floats dx + c of each patch row
+(the row pointer is indexed by dx floats).  OpenCV is not available: oracle/pca_jacobi.h restates
+the published PCA (sample mean, covariance, Jacobi eigenvectors ordered by eigenvalue, largest
+entry positive) and stands in for cv::PCA inside the reference build, so the reference's own
+sampling and projection run and pin the oracle by digest (tests/golden, pca_* cases).  The GPU
+path must agree with the oracle: descriptors to float rounding of the independently computed
+bases, tables bit-exact given the oracle's descriptors, NNF distances exact and mean distance
+within 1 %."""
 import ctypes
 
 import numpy as np
