@@ -416,6 +416,7 @@ def main():
     table = ptb.PatchTable(params, b)
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
+    build_stage_ms = table.build_profile()
 
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
@@ -561,7 +562,7 @@ def main():
         "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded generator, patchtable_b200/synth.py)",
         "config": {"workload": WORKLOAD["name"], "patches_per_step": P, "image": [H, W], "table_image": list(b.shape[:2]),
-                   "build_s": build_s, "mean_nnf_dist": md, "mean_nnf_dist_e2e": md_e2e,
+                   "build_s": build_s, "build_stage_ms": build_stage_ms, "mean_nnf_dist": md, "mean_nnf_dist_e2e": md_e2e,
                    "e2e_ms": {"mean": 1000 * sum(e2e_s) / len(e2e_s), "median": 1000 * float(np.median(e2e_s)),
                               "min": 1000 * min(e2e_s), "max": 1000 * max(e2e_s), "calls": len(e2e_s)},
                    "reference_mean_nnf_dist": ref_md,

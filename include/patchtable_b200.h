@@ -218,6 +218,20 @@ pt_status pt_batch_replay(pt_batch *b, void *stream);
 pt_status pt_table_lookup_profile(pt_table *t, const float *d_a, int h, int w, double *d_ann,
                                   void *stream, double *stage_ms, uint64_t *counters);
 
+/* Diagnostics (no reference counterpart; the reference prints its own stage times when verbose,
+   patchtable.h:2531-2580, 3107-3117): wall-clock milliseconds of the table build's stages, each
+   ended with the stream drained.  ms[PT_BUILD_NSTAGES] = {descriptor (upload, descriptor, shifted
+   copy), k-coherence, range + partition, populate order (host shuffle), populate + distance
+   transform, total}. */
+#define PT_BUILD_DESCRIPTOR 0
+#define PT_BUILD_KCOHERENCE 1
+#define PT_BUILD_PARTITION 2
+#define PT_BUILD_SHUFFLE 3
+#define PT_BUILD_POPULATE_DT 4
+#define PT_BUILD_TOTAL 5
+#define PT_BUILD_NSTAGES 6
+pt_status pt_table_build_profile(const pt_table *t, double *ms, int n);
+
 /* Diagnostics (no reference counterpart): C = A * B^T in FP32 through the hand-written tcgen05
    BF16 GEMM of the proposal network.  A [M x K], B [N x K] row-major BF16 device arrays (lda, ldb
    multiples of 8; K a multiple of 16; N in {16, 32, 64, 128, 256}); C [M x N] FP32, ldc.
@@ -313,6 +327,23 @@ int64_t pt_table_add_count(const pt_table *t);
 
 /* Descriptor of an RGB image as the query computes it: (h-7) x (w-7) x ndims floats. */
 pt_status pt_descriptor(const pt_params *p, const float *rgb, int h, int w, float *out);
+
+/* Bound on every wait inside this library's device kernels (no reference counterpart; the
+   reference has no device waits): a grid-barrier wait of the table build gives up after `polls`
+   polls (about 0.1 us each), every block of the launch then leaves, and the call returns
+   PT_TIMEOUT with the device still usable.  Process-wide; returns the previous bound.  A negative
+   value restores the default, 2^24 polls (seconds).  0 makes any wait give up at once, which the
+   tests use to exercise the error path. */
+int64_t pt_set_spin_limit(int64_t polls);
+
+/* Cap on the device memory this library holds at once (no reference counterpart): an allocation
+   that would pass `bytes` fails as if the device were full and the call returns PT_OOM, leaving
+   earlier tables intact.  Process-wide; returns the previous cap; a negative value removes the
+   cap (the default).  Lets an application share the GPU with a fixed budget, and lets the tests
+   drive the out-of-memory path without exhausting the device.  pt_device_bytes_in_use gives the
+   bytes the library currently holds (the zero-allocation query's static array is not counted). */
+int64_t pt_set_device_alloc_limit(int64_t bytes);
+int64_t pt_device_bytes_in_use(void);
 
 /* Device kernel launches issued by this thread since the last reset (evidence counter). */
 int64_t pt_kernel_launch_count(void);

@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
     L.pt_table_add_count.argtypes = [vp]
     L.pt_table_add_count.restype = C.c_int64
     L.pt_table_dt_levels.argtypes = [vp]
+    L.pt_table_build_profile.argtypes = [vp, C.POINTER(C.c_double), C.c_int]
     L.pt_table_lookup_profile.argtypes = [vp, vp, C.c_int, C.c_int, vp, vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
     L.pt_descriptor.argtypes = [P, _f32p, C.c_int, C.c_int, _f32p]
     L.pt_tc_gemm_f32.argtypes = [vp, C.c_int, vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp]
@@ -150,6 +151,11 @@ def lib() -> C.CDLL:
                                                   C.POINTER(C.c_uint64)]
     L.pt_last_error.restype = C.c_char_p
     L.pt_version.restype = C.c_char_p
+    L.pt_set_spin_limit.argtypes = [C.c_int64]
+    L.pt_set_spin_limit.restype = C.c_int64
+    L.pt_set_device_alloc_limit.argtypes = [C.c_int64]
+    L.pt_set_device_alloc_limit.restype = C.c_int64
+    L.pt_device_bytes_in_use.restype = C.c_int64
     L.pt_kernel_launch_count.restype = C.c_int64
     L.pt_kernel_launch_count_reset.restype = None
     _lib = L
@@ -455,6 +461,14 @@ class PatchTable:
     def dt_levels(self) -> int:
         return int(lib().pt_table_dt_levels(self._h))
 
+    BUILD_STAGES = ("descriptor", "kcoherence", "partition", "shuffle", "populate_dt", "total")
+
+    def build_profile(self):
+        """Wall-clock milliseconds of the build's stages (each ended with the stream drained)."""
+        ms = (C.c_double * len(self.BUILD_STAGES))()
+        _check(lib().pt_table_build_profile(self._h, ms, len(self.BUILD_STAGES)))
+        return dict(zip(self.BUILD_STAGES, list(ms)))
+
 
 class QueryBatch:
     """pt_batch: concatenated device buffers for a fixed list of query sizes against one table.
@@ -523,6 +537,22 @@ def descriptor(params: PatchTableParams, img):
     out = np.empty((img.shape[0] - 7, img.shape[1] - 7, params.ndims), np.float32)
     _check(lib().pt_descriptor(C.byref(params._p), img, img.shape[0], img.shape[1], out))
     return out
+
+
+def set_spin_limit(polls: int) -> int:
+    """Polls after which a device-side wait of the library gives up (PT_TIMEOUT); negative restores
+    the default.  Returns the previous value."""
+    return int(lib().pt_set_spin_limit(int(polls)))
+
+
+def set_device_alloc_limit(nbytes: int) -> int:
+    """Cap on the device memory the library holds (PT_OOM beyond it); negative removes the cap.
+    Returns the previous cap."""
+    return int(lib().pt_set_device_alloc_limit(int(nbytes)))
+
+
+def device_bytes_in_use() -> int:
+    return int(lib().pt_device_bytes_in_use())
 
 
 def launch_count() -> int:

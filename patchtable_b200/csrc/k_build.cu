@@ -1,20 +1,12 @@
-/* Table build kernels: per-dimension range, quantile samples, cell assignment + populate, and the
-   propagation distance transform.
+/* Table build kernels: per-dimension range, quantile samples, the query's cell lookup, and the
+   distance transforms other than prop (populate and the prop DT are one cooperative launch,
+   k_table_build.cu).
 
    References (patchtable/patchtable.h):
      set_min_max              :1758-1778
      PatchPartition1D         :1172-1286  (quantile centres; the to_bin table is built on the host)
      get_bin                  :1298-1325
-     populate (fast, random)  :3121-3159
-     do_dt_prop               :2081-2165  (edge labels PropEdge :1435-1447)
-     do_dt_brute              :2364-2413  (patch_dist_to_grid :1403-1425)
-
-   The DT is the reference's breadth-first fill, run level-synchronously: in each level every
-   frontier element claims the unused neighbours its label allows with atomicMin on
-   (element index, edge index), so the winner of a cell is exactly the element the sequential
-   loop would have reached first; winners are then written in (element, edge) order by an
-   exclusive scan, which reproduces the order of the reference's next frontier list.  The filled
-   table is therefore bit-identical to the reference's. */
+     do_dt_brute              :2364-2413  (patch_dist_to_grid :1403-1425) */
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
@@ -31,17 +23,6 @@ struct BinPlan {
     float min_val[PT_DESC_MAX];
     float range[PT_DESC_MAX];
     long long stride[PT_DESC_MAX];
-};
-
-struct DtPlan {
-    int G;
-    long long ncells;
-    long long stride[PT_DESC_MAX];
-    int nslices[PT_DESC_MAX];
-    int nedges[1 + 2 * PT_DESC_MAX];
-    signed char edim[1 + 2 * PT_DESC_MAX][2 * PT_DESC_MAX];
-    signed char edir[1 + 2 * PT_DESC_MAX][2 * PT_DESC_MAX];
-    unsigned char elab[1 + 2 * PT_DESC_MAX][2 * PT_DESC_MAX];
 };
 
 /* PatchPartition1D::get_bin, patchtable.h:1298-1325 (pt_bins.cuh). */
@@ -97,31 +78,6 @@ __global__ void k_pick(const float *sorted, const int *idx, int n, float *out) {
     if (i < n) out[i] = sorted[idx[i]];
 }
 
-/* Cell index of every allowed patch, then first-visitor-wins in shuffled order: the smallest
-   shuffle rank reaching a cell is kept (populate_random, patchtable.h:3142-3154). */
-__global__ void k_populate(const BinPlan c_bins, const float *__restrict__ desc, int ds, long long P, const int *__restrict__ rank,
-                           const int *__restrict__ to_bin, int *table) {
-    long long p = blockIdx.x * (long long) NT + threadIdx.x;
-    if (p >= P) return;
-    int r = rank[p];
-    if (r < 0) return;
-    const float *v = desc + p * ds;
-    long long cell = 0;
-    for (int d = 0; d < c_bins.G; d++) cell += (long long) get_bin(c_bins, to_bin, d, v[d]) * c_bins.stride[d];
-    atomicMin(table + cell, r);
-}
-
-/* Cell index of query descriptors (table lookup, patchtable.h:3675-3680). */
-__global__ void k_cells(const BinPlan c_bins, const float *__restrict__ desc, int ds, long long P, const int *__restrict__ to_bin,
-                        long long *cells) {
-    long long p = blockIdx.x * (long long) NT + threadIdx.x;
-    if (p >= P) return;
-    const float *v = desc + p * ds;
-    long long cell = 0;
-    for (int d = 0; d < c_bins.G; d++) cell += (long long) get_bin(c_bins, to_bin, d, v[d]) * c_bins.stride[d];
-    cells[p] = cell;
-}
-
 /* Table candidate of every query patch: the cell's stored patch (patchtable.h:3675-3686). */
 __global__ void k_table_cand(const BinPlan c_bins, const float *__restrict__ desc, int ds, long long P,
                              const int *__restrict__ to_bin, const int *__restrict__ table, int *tcand) {
@@ -133,136 +89,9 @@ __global__ void k_table_cand(const BinPlan c_bins, const float *__restrict__ des
     tcand[p] = __ldg(table + cell);
 }
 
-constexpr int SEG = 4096;   /* cells per block in the ordered compaction */
-
-/* Converts winning shuffle ranks to packed positions and counts seeded cells per block. */
-__global__ void k_resolve(int *table, long long ncells, const int *__restrict__ order_xy, int *block_count) {
-    __shared__ int cnt;
-    if (threadIdx.x == 0) cnt = 0;
-    __syncthreads();
-    long long base = (long long) blockIdx.x * SEG;
-    int local = 0;
-    for (int i = threadIdx.x; i < SEG; i += NT) {
-        long long j = base + i;
-        if (j >= ncells) break;
-        int v = table[j];
-        if (v != PT_UNUSED) { table[j] = order_xy[v]; local++; }
-    }
-    atomicAdd(&cnt, local);
-    __syncthreads();
-    if (threadIdx.x == 0) block_count[blockIdx.x] = cnt;
-}
-
-/* Emits seeded cells in increasing cell order as the first frontier (label 0), patchtable.h:2087-2093. */
-__global__ void k_seed(const int *__restrict__ table, long long ncells, const int *__restrict__ block_off,
-                       int *fidx, int *fval, unsigned char *flab) {
-    typedef cub::BlockScan<int, NT> Scan;
-    __shared__ typename Scan::TempStorage tmp;
-    __shared__ int running;
-    if (threadIdx.x == 0) running = block_off[blockIdx.x];
-    __syncthreads();
-    long long base = (long long) blockIdx.x * SEG;
-    for (int i0 = 0; i0 < SEG; i0 += NT) {
-        long long j = base + i0 + threadIdx.x;
-        int v = (j < ncells) ? table[j] : PT_UNUSED;
-        int f = v != PT_UNUSED, off, tot;
-        Scan(tmp).ExclusiveSum(f, off, tot);
-        if (f) { int o = running + off; fidx[o] = (int) j; fval[o] = v; flab[o] = 0; }
-        __syncthreads();
-        if (threadIdx.x == 0) running += tot;
-        __syncthreads();
-    }
-}
-
-/* Level step 1: every frontier element claims the unused, in-range neighbours of its label's
-   edges; the smallest (element, edge) key wins (patchtable.h:2131-2156). */
-__global__ void k_dt_claim(const DtPlan c_dt, int n, const int *__restrict__ fidx, const unsigned char *__restrict__ flab,
-                           const int *__restrict__ table, unsigned *claim) {
-    int i = blockIdx.x * NT + threadIdx.x;
-    if (i >= n) return;
-    long long g = fidx[i];
-    int lab = flab[i];
-    int ne = c_dt.nedges[lab];
-    for (int e = 0; e < ne; e++) {
-        int dim = c_dt.edim[lab][e], dir = c_dt.edir[lab][e];
-        long long gp = g + dir * c_dt.stride[dim];
-        if (gp < 0 || gp >= c_dt.ncells || table[gp] != PT_UNUSED) continue;
-        long long dp = (g / c_dt.stride[dim]) % c_dt.nslices[dim] + dir;
-        if (dp < 0 || dp >= c_dt.nslices[dim]) continue;
-        atomicMin(claim + gp, ((unsigned) i << 5) | (unsigned) e);
-    }
-}
-
-/* Level step 2: number of cells each element won. */
-__global__ void k_dt_count(const DtPlan c_dt, int n, const int *__restrict__ fidx, const unsigned char *__restrict__ flab,
-                           const int *__restrict__ table, const unsigned *__restrict__ claim, int *cnt) {
-    int i = blockIdx.x * NT + threadIdx.x;
-    if (i >= n) return;
-    long long g = fidx[i];
-    int lab = flab[i];
-    int ne = c_dt.nedges[lab], c = 0;
-    for (int e = 0; e < ne; e++) {
-        int dim = c_dt.edim[lab][e], dir = c_dt.edir[lab][e];
-        long long gp = g + dir * c_dt.stride[dim];
-        if (gp < 0 || gp >= c_dt.ncells || table[gp] != PT_UNUSED) continue;
-        if (claim[gp] == (((unsigned) i << 5) | (unsigned) e)) c++;
-    }
-    cnt[i] = c;
-}
-
-/* Level step 3: winners fill their cells and append (cell, value, edge label) to the next
-   frontier at their scanned offsets, i.e. in (element, edge) order. */
-__global__ void k_dt_emit(const DtPlan c_dt, int n, const int *__restrict__ fidx, const int *__restrict__ fval,
-                          const unsigned char *__restrict__ flab, const unsigned *__restrict__ claim,
-                          const int *__restrict__ off, int *table, int *nidx, int *nval, unsigned char *nlab) {
-    int i = blockIdx.x * NT + threadIdx.x;
-    if (i >= n) return;
-    long long g = fidx[i];
-    int lab = flab[i], val = fval[i];
-    int ne = c_dt.nedges[lab], o = off[i];
-    for (int e = 0; e < ne; e++) {
-        int dim = c_dt.edim[lab][e], dir = c_dt.edir[lab][e];
-        long long gp = g + dir * c_dt.stride[dim];
-        /* Claims persist across levels: a filled cell's old key must not match. Only the winner
-           writes gp in this level, so the winner itself still reads PT_UNUSED here. */
-        if (gp < 0 || gp >= c_dt.ncells || table[gp] != PT_UNUSED) continue;
-        if (claim[gp] == (((unsigned) i << 5) | (unsigned) e)) {
-            table[gp] = val;
-            nidx[o] = (int) gp; nval[o] = val; nlab[o] = c_dt.elab[lab][e];
-            o++;
-        }
-    }
-}
-
-__global__ void k_fill(int *p, long long n, int v) {
-    for (long long i = blockIdx.x * (long long) NT + threadIdx.x; i < n; i += (long long) gridDim.x * NT) p[i] = v;
-}
-
-__global__ void k_replace(int *p, long long n, int from, int to) {
-    for (long long i = blockIdx.x * (long long) NT + threadIdx.x; i < n; i += (long long) gridDim.x * NT)
-        if (p[i] == from) p[i] = to;
-}
-
-__global__ void k_fill_u32(unsigned *p, long long n, unsigned v) {
-    for (long long i = blockIdx.x * (long long) NT + threadIdx.x; i < n; i += (long long) gridDim.x * NT) p[i] = v;
-}
-
 inline int blocks_for(long long n) { return (int) ((n + NT - 1) / NT); }
 
 }  // namespace
-
-pt_status pt_launch_fill(int *p, long long n, int v, cudaStream_t st) {
-    k_fill<<<1184, NT, 0, st>>>(p, n, v);
-    PT_LAUNCHED();
-    return PT_OK;
-}
-
-/* fill_zeros, patchtable.h:2063-2079: cells the DT left unused take one fixed patch. */
-pt_status pt_launch_replace(int *table, long long n, int from, int to, cudaStream_t st) {
-    k_replace<<<1184, NT, 0, st>>>(table, n, from, to);
-    PT_LAUNCHED();
-    return PT_OK;
-}
 
 pt_status pt_launch_minmax(const float *desc, int ds, int G, long long P, const int *allowed, int allowed_index,
                            float *hmin, float *hmax, cudaStream_t st) {
@@ -326,119 +155,10 @@ static BinPlan bin_plan(const PtBins &bins) {
     return b;
 }
 
-pt_status pt_launch_populate(const PtBins &bins, const float *desc, int ds, long long P, const int *rank,
-                             const int *to_bin, int *table, cudaStream_t st) {
-    k_populate<<<blocks_for(P), NT, 0, st>>>(bin_plan(bins), desc, ds, P, rank, to_bin, table);
-    PT_LAUNCHED();
-    return PT_OK;
-}
-
-pt_status pt_launch_cells(const PtBins &bins, const float *desc, int ds, long long P, const int *to_bin,
-                          long long *cells, cudaStream_t st) {
-    k_cells<<<blocks_for(P), NT, 0, st>>>(bin_plan(bins), desc, ds, P, to_bin, cells);
-    PT_LAUNCHED();
-    return PT_OK;
-}
-
 pt_status pt_launch_table_candidates(const PtBins &bins, const float *desc, int ds, long long P, const int *to_bin,
                                      const int *table, int *tcand, cudaStream_t st) {
     k_table_cand<<<blocks_for(P), NT, 0, st>>>(bin_plan(bins), desc, ds, P, to_bin, table, tcand);
     PT_LAUNCHED();
-    return PT_OK;
-}
-
-/* do_dt_prop on the device.  table holds shuffle ranks of the winning patches on entry and
-   packed positions on exit; *seeded receives table_add_count. */
-pt_status pt_dt_prop(int *table, long long ncells, const int *order_xy, int G, const int *nslices,
-                     const long long *stride, int dt_iters, int run, long long *seeded, int *levels_out,
-                     cudaStream_t st) {
-    if (ncells >= (1ll << 31)) return pt_fail(PT_UNSUPPORTED, "tables above 2^31 cells are not supported");
-    if (2 * G > 32) return pt_fail(PT_UNSUPPORTED, "grid dims > 16");
-    DtPlan plan;
-    memset(&plan, 0, sizeof(plan));
-    plan.G = G;
-    plan.ncells = ncells;
-    for (int d = 0; d < G; d++) { plan.stride[d] = stride[d]; plan.nslices[d] = nslices[d]; }
-    /* Edge lists by label (patchtable.h:2101-2120): label 0 -> every (dim, -1), (dim, +1);
-       label of (i, dir) = 2i + 1 + (dir+1)/2 -> (i, dir) then (j, -1), (j, +1) for j > i. */
-    auto add = [&](int lab, int dim, int dir) {
-        int e = plan.nedges[lab]++;
-        plan.edim[lab][e] = (signed char) dim;
-        plan.edir[lab][e] = (signed char) dir;
-        plan.elab[lab][e] = (unsigned char) (2 * dim + 1 + (dir + 1) / 2);
-    };
-    for (int i = 0; i < G; i++) { add(0, i, -1); add(0, i, 1); }
-    for (int i = 0; i < G; i++)
-        for (int dir = -1; dir <= 1; dir += 2) {
-            int lab = 2 * i + 1 + (dir + 1) / 2;
-            add(lab, i, dir);
-            for (int j = i + 1; j < G; j++) { add(lab, j, -1); add(lab, j, 1); }
-        }
-
-    long long nblk = (ncells + SEG - 1) / SEG;
-    DevBuf<int> bcount, boff;
-    PT_CUDA(bcount.reserve(nblk + 1));
-    PT_CUDA(boff.reserve(nblk + 1));
-    k_resolve<<<(unsigned) nblk, NT, 0, st>>>(table, ncells, order_xy, bcount.p);
-    PT_LAUNCHED();
-    size_t tb = 0;
-    PT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, bcount.p, boff.p, (int) nblk + 1, st));
-    DevBuf<unsigned char> tmp;
-    PT_CUDA(tmp.reserve(tb));
-    PT_CUDA(cudaMemsetAsync(bcount.p + nblk, 0, sizeof(int), st));
-    PT_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tb, bcount.p, boff.p, (int) nblk + 1, st));
-    pt_count_launches(1);
-    int nseed = 0;
-    PT_CUDA(cudaMemcpyAsync(&nseed, boff.p + nblk, sizeof(int), cudaMemcpyDeviceToHost, st));
-    PT_CUDA(cudaStreamSynchronize(st));
-    *seeded = nseed;
-    if (levels_out) *levels_out = 0;
-    if (!run) return PT_OK;
-    long long cap = std::max<long long>(nseed, ncells - nseed);
-    DevBuf<int> fi[2], fv[2], cnt, off;
-    DevBuf<unsigned char> fl[2];
-    for (int k = 0; k < 2; k++) {
-        PT_CUDA(fi[k].reserve(cap));
-        PT_CUDA(fv[k].reserve(cap));
-        PT_CUDA(fl[k].reserve(cap));
-    }
-    PT_CUDA(cnt.reserve(cap + 1));
-    PT_CUDA(off.reserve(cap + 1));
-    DevBuf<unsigned> claim;
-    PT_CUDA(claim.reserve(ncells));
-    k_fill_u32<<<1184, NT, 0, st>>>(claim.p, ncells, 0xffffffffu);
-    PT_LAUNCHED();
-    k_seed<<<(unsigned) nblk, NT, 0, st>>>(table, ncells, boff.p, fi[0].p, fv[0].p, fl[0].p);
-    PT_LAUNCHED();
-    size_t tb2 = 0;
-    PT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb2, cnt.p, off.p, (int) (cap + 1), st));
-    PT_CUDA(tmp.reserve(tb2));
-    int n = nseed, cur = 0, levels = 0;
-    if ((long long) n >= (1ll << 27) || ncells - nseed >= (1ll << 27))
-        return pt_fail(PT_UNSUPPORTED, "DT frontier above 2^27 elements is not supported");
-    for (int iter = 0;; iter++) {
-        if (dt_iters > 0 && iter > dt_iters) break;
-        if (n == 0) break;
-        k_dt_claim<<<blocks_for(n), NT, 0, st>>>(plan, n, fi[cur].p, fl[cur].p, table, claim.p);
-        PT_LAUNCHED();
-        k_dt_count<<<blocks_for(n), NT, 0, st>>>(plan, n, fi[cur].p, fl[cur].p, table, claim.p, cnt.p);
-        PT_LAUNCHED();
-        PT_CUDA(cudaMemsetAsync(cnt.p + n, 0, sizeof(int), st));
-        size_t need = 0;
-        PT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, need, cnt.p, off.p, n + 1, st));
-        PT_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, need, cnt.p, off.p, n + 1, st));
-        pt_count_launches(1);
-        k_dt_emit<<<blocks_for(n), NT, 0, st>>>(plan, n, fi[cur].p, fv[cur].p, fl[cur].p, claim.p, off.p, table,
-                                               fi[1 - cur].p, fv[1 - cur].p, fl[1 - cur].p);
-        PT_LAUNCHED();
-        int nn = 0;
-        PT_CUDA(cudaMemcpyAsync(&nn, off.p + n, sizeof(int), cudaMemcpyDeviceToHost, st));
-        PT_CUDA(cudaStreamSynchronize(st));
-        n = nn;
-        cur = 1 - cur;
-        levels++;
-    }
-    if (levels_out) *levels_out = levels;
     return PT_OK;
 }
 

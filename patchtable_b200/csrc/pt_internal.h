@@ -32,6 +32,12 @@ PT_HD int pt_y(int v) { return v >> 16; }
 pt_status pt_fail(pt_status s, const char *fmt, ...);
 /* Counts device kernel launches issued by the library (pt_kernel_launch_count). */
 void pt_count_launches(int n);
+/* Polls after which a device-side wait gives up (pt_set_spin_limit). */
+long long pt_spin_limit();
+/* Device-allocation accounting of DevBuf (pt_set_device_alloc_limit): admits `bytes` more or
+   refuses when the library's live device allocations would exceed the limit. */
+bool pt_alloc_admit(size_t bytes);
+void pt_alloc_release(size_t bytes);
 
 #define PT_TRY(expr) do { pt_status _s = (expr); if (_s != PT_OK) return _s; } while (0)
 
@@ -59,15 +65,22 @@ template<class T> struct DevBuf {
     DevBuf() {}
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
-    ~DevBuf() { if (p) cudaFree(p); }
+    ~DevBuf() { release(); }
     cudaError_t reserve(size_t count) {
         if (count <= n && p) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr; n = 0;
-        cudaError_t e = cudaMalloc((void **) &p, sizeof(T) * (count ? count : 1));
-        if (e == cudaSuccess) n = count;
+        release();
+        const size_t bytes = sizeof(T) * (count ? count : 1);
+        if (!pt_alloc_admit(bytes)) return cudaErrorMemoryAllocation;
+        cudaError_t e = cudaMalloc((void **) &p, bytes);
+        if (e == cudaSuccess) { n = count; held = bytes; }
+        else { p = nullptr; pt_alloc_release(bytes); }
         return e;
     }
-    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    void release() {
+        if (p) { cudaFree(p); pt_alloc_release(held); }
+        p = nullptr; n = 0; held = 0;
+    }
+private:
+    size_t held = 0;
 };
 #endif

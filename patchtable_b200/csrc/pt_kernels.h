@@ -40,7 +40,6 @@ pt_status pt_launch_descriptor_input(const float *in, int H, int W, int nd, int 
                                      cudaStream_t st);
 
 /* k_build.cu */
-pt_status pt_launch_fill(int *p, long long n, int v, cudaStream_t st);
 pt_status pt_launch_minmax(const float *desc, int ds, int G, long long P, const int *allowed, int allowed_index,
                            float *hmin, float *hmax, cudaStream_t st);
 pt_status pt_quantile_values(const float *desc, int ds, int d, int eh, int ew, int step, const int *allowed,
@@ -52,10 +51,6 @@ struct PtBins {
     float min_val[PT_DESC_MAX], range[PT_DESC_MAX];
     long long stride[PT_DESC_MAX];
 };
-pt_status pt_launch_populate(const PtBins &bins, const float *desc, int ds, long long P, const int *rank,
-                             const int *to_bin, int *table, cudaStream_t st);
-pt_status pt_launch_cells(const PtBins &bins, const float *desc, int ds, long long P, const int *to_bin,
-                          long long *cells, cudaStream_t st);
 /* Table entry of every query patch's cell (patchtable.h:3675-3686): tcand[p] = table[cell(p)]. */
 pt_status pt_launch_table_candidates(const PtBins &bins, const float *desc, int ds, long long P, const int *to_bin,
                                      const int *table, int *tcand, cudaStream_t st);
@@ -64,9 +59,14 @@ pt_status pt_launch_table_candidates(const PtBins &bins, const float *desc, int 
 pt_status pt_launch_descriptor_cells(int ndims, int nchroma, const float *rgb, int h, int w, int convert, float4 *rgba,
                                      const PtBins &bins, const int *to_bin, const int *table, int *tcand, int trow0,
                                      int trows, cudaStream_t st);
-pt_status pt_dt_prop(int *table, long long ncells, const int *order_xy, int G, const int *nslices,
-                     const long long *stride, int dt_iters, int run, long long *seeded, int *levels_out,
-                     cudaStream_t st);
+/* k_table_build.cu: the table's cells in one cooperative launch -- fill with TABLE_UNUSED, populate in
+   shuffle-rank order (rank[p] < 0: patch not allowed; order_xy[rank] = packed position), the
+   propagation DT when run_dt (at most dt_iters levels when > 0), and fill_zeros with vfill when
+   asked.  *seeded receives table_add_count, *levels the DT levels run.  Grid-barrier waits give up
+   after pt_spin_limit() polls and the call returns PT_TIMEOUT. */
+pt_status pt_build_cells(const PtBins &bins, const int *nslices, const float *desc, int ds, long long P, const int *rank,
+                         const int *to_bin, const int *order_xy, int *table, long long ncells, int run_dt, int dt_iters,
+                         int fill_zeros, int vfill, long long *seeded, int *levels, cudaStream_t st);
 /* dt_algo 4 downsample, 5 hybrid (prop1 + downsample + unmask), 6 euclidean on a table whose
    populated cells hold packed positions. */
 pt_status pt_dt_other(int *table, int G, const int *nslices, int dt_algo, cudaStream_t st);
@@ -75,7 +75,6 @@ pt_status pt_dt_other(int *table, int G, const int *nslices, int dt_algo, cudaSt
    grid dimension's centres, lsizes and rsizes. */
 pt_status pt_dt_brute(int *table, int G, const int *nslices, const float *part, const int *part_ofs, const float *desc,
                       int ds, long long P, int ew, cudaStream_t st);
-pt_status pt_launch_replace(int *table, long long n, int from, int to, cudaStream_t st);
 
 /* k_kcoh.cu */
 #define PT_KNN_WIDE_MAX 1024                 /* largest neighbour list of the k-coherence search */

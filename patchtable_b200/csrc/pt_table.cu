@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -74,6 +75,27 @@ pt_status pt_fail(pt_status s, const char *fmt, ...) {
 
 void pt_count_launches(int n) { g_launches += n; }
 
+namespace {
+std::atomic<long long> g_alloc_live{0};
+std::atomic<long long> g_alloc_limit{-1};
+}  // namespace
+
+bool pt_alloc_admit(size_t bytes) {
+    const long long lim = g_alloc_limit.load();
+    const long long now = g_alloc_live.fetch_add((long long) bytes) + (long long) bytes;
+    if (lim >= 0 && now > lim) {
+        g_alloc_live.fetch_sub((long long) bytes);
+        return false;
+    }
+    return true;
+}
+
+void pt_alloc_release(size_t bytes) { g_alloc_live.fetch_sub((long long) bytes); }
+
+extern "C" int64_t pt_set_device_alloc_limit(int64_t bytes) { return g_alloc_limit.exchange(bytes < 0 ? -1 : bytes); }
+
+extern "C" int64_t pt_device_bytes_in_use(void) { return g_alloc_live.load(); }
+
 struct pt_table {
     pt_params p;
     int h = 0, w = 0, eh = 0, ew = 0;
@@ -104,6 +126,8 @@ struct pt_table {
     DevBuf<int> table;
     long long add_count = 0;
     int dt_levels = 0;
+    /* wall-clock milliseconds of the build stages (pt_table_build_profile) */
+    double build_ms[PT_BUILD_NSTAGES] = {};
     DevBuf<int2> kcoh;
     int kc_list = 0;
     /* ntables > 1: the further tables at limit / table_ratio^i (patchtable.h:3359-3371) and their
@@ -348,6 +372,16 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
     PT_CUDA(cudaStreamCreateWithFlags(&t->st, cudaStreamNonBlocking));
     t->own_stream = true;
     const long long P = (long long) t->eh * t->ew;
+    /* stage clock: every stage ends with the stream drained */
+    const double t_start = now_s();
+    double t_mark = t_start;
+    auto stage_done = [&](int k) -> pt_status {
+        PT_CUDA(cudaStreamSynchronize(t->st));
+        const double t1 = now_s();
+        t->build_ms[k] += 1000.0 * (t1 - t_mark);
+        t_mark = t1;
+        return PT_OK;
+    };
 
     if (t->desc_mode) {
         DevBuf<float> in;
@@ -403,9 +437,11 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
         PT_CUDA(t->allowed.reserve(P));
         PT_CUDA(cudaMemcpyAsync(t->allowed.p, allowed, sizeof(int) * P, cudaMemcpyHostToDevice, t->st));
     }
+    PT_TRY(stage_done(PT_BUILD_DESCRIPTOR));
 
     /* k-coherence is computed before the table in the reference (patchtable.h:2653). */
     if (p.kcoherence > 0) PT_TRY(build_kcoherence(t.get(), allowed_h));
+    PT_TRY(stage_done(PT_BUILD_KCOHERENCE));
 
     /* set_min_max + set_nslices (patchtable.h:1758-1810, 2567-2582). */
     t->min_val.assign(t->G, 0.f);
@@ -430,6 +466,7 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
     for (int d = t->G - 1; d >= 0; d--) { t->stride[d] = t->ncells; t->ncells *= t->nslices[d]; }
     if (t->ncells >= (1ll << 31)) return pt_fail(PT_UNSUPPORTED, "table of %lld cells exceeds 2^31", t->ncells);
     PT_TRY(build_partition(t.get()));
+    PT_TRY(stage_done(PT_BUILD_PARTITION));
 
     /* Populate in std::random_shuffle order (patchtable.h:3142-3154): the permutation is drawn
        from the C library rand(), consuming it exactly as the reference does. */
@@ -448,6 +485,7 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
         int v = order_xy[i];
         rank[(size_t) (pt_y(v) - 7) * t->ew + (pt_x(v) - 7)] = (int) i;
     }
+    PT_TRY(stage_done(PT_BUILD_SHUFFLE));
     {
         DevBuf<int> d_rank, d_order;
         PT_CUDA(d_rank.reserve(P));
@@ -455,28 +493,27 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
         PT_CUDA(cudaMemcpyAsync(d_rank.p, rank.data(), sizeof(int) * P, cudaMemcpyHostToDevice, t->st));
         PT_CUDA(cudaMemcpyAsync(d_order.p, order_xy.data(), sizeof(int) * order_xy.size(), cudaMemcpyHostToDevice, t->st));
         PT_CUDA(t->table.reserve(t->ncells));
-        PT_TRY(pt_launch_fill(t->table.p, t->ncells, PT_UNUSED, t->st));
-        PT_TRY(pt_launch_populate(t->bins, t->b_desc.p, t->ds, P, d_rank.p, t->to_bin.p, t->table.p, t->st));
-        /* Distance transform (patchtable.h:3254-3298): prop is the level-synchronous fill; the
-           others run on the resolved table. */
-        bool prop = p.run_dt && p.dt_algo == 1;
-        PT_TRY(pt_dt_prop(t->table.p, t->ncells, d_order.p, t->G, t->nslices.data(), t->stride.data(), p.dt_iters,
-                          prop, &t->add_count, &t->dt_levels, t->st));
+        /* Distance transform (patchtable.h:3254-3298): prop is the level-synchronous fill inside
+           the cooperative build launch; the others run on its resolved table. */
+        const bool prop = p.run_dt && p.dt_algo == 1;
+        /* fill_zeros (patchtable.h:2063-2079) after no DT or a prop DT cut short by dt_iters */
+        const bool fill_zeros = !p.run_dt || (prop && p.dt_iters > 0);
+        int vfill = pt_xy(7, 7);
+        if (!allowed_h.empty())
+            for (long long i = 0; i < P; i++)
+                if (allowed_h[i] == p.allowed_index) { vfill = pt_xy((int) (i % t->ew) + 7, (int) (i / t->ew) + 7); break; }
+        PT_TRY(pt_build_cells(t->bins, t->nslices.data(), t->b_desc.p, t->ds, P, d_rank.p, t->to_bin.p, d_order.p,
+                              t->table.p, t->ncells, prop, p.dt_iters, fill_zeros, vfill, &t->add_count, &t->dt_levels,
+                              t->st));
         if (p.run_dt && p.dt_algo == 2)
             PT_TRY(pt_dt_brute(t->table.p, t->G, t->nslices.data(), t->part_dev.p, t->part_ofs, t->b_desc.p, t->ds, P, t->ew,
                                t->st));
         else if (p.run_dt && !prop)
             PT_TRY(pt_dt_other(t->table.p, t->G, t->nslices.data(), p.dt_algo, t->st));
-        bool zeros_filled = p.run_dt && (!prop || p.dt_iters <= 0);
-        if (!zeros_filled) {                                  /* fill_zeros, patchtable.h:2063-2079 */
-            int vfill = pt_xy(7, 7);
-            if (!allowed_h.empty())
-                for (long long i = 0; i < P; i++)
-                    if (allowed_h[i] == p.allowed_index) { vfill = pt_xy((int) (i % t->ew) + 7, (int) (i / t->ew) + 7); break; }
-            PT_TRY(pt_launch_replace(t->table.p, t->ncells, PT_UNUSED, vfill, t->st));
-        }
         PT_CUDA(cudaStreamSynchronize(t->st));
     }
+    PT_TRY(stage_done(PT_BUILD_POPULATE_DT));
+    t->build_ms[PT_BUILD_TOTAL] = 1000.0 * (now_s() - t_start);
     *out = t.release();
     return PT_OK;
 }
@@ -1226,6 +1263,12 @@ int pt_table_shape(const pt_table *t, int *nslices, int64_t *ncells) {
     if (nslices) for (int i = 0; i < PT_MAX_DIMS; i++) nslices[i] = i < t->G ? t->nslices[i] : 0;
     if (ncells) *ncells = t->ncells;
     return t->G;
+}
+
+pt_status pt_table_build_profile(const pt_table *t, double *ms, int n) {
+    if (!t || !ms || n < 0) return pt_fail(PT_BAD_ARG, "null argument");
+    for (int i = 0; i < n; i++) ms[i] = i < PT_BUILD_NSTAGES ? t->build_ms[i] : 0.0;
+    return PT_OK;
 }
 
 pt_status pt_table_get_cells(const pt_table *t, int32_t *out) {
