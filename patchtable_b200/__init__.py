@@ -151,6 +151,8 @@ def lib() -> C.CDLL:
                                                   C.POINTER(C.c_uint64)]
     L.pt_last_error.restype = C.c_char_p
     L.pt_version.restype = C.c_char_p
+    L.pt_set_host_threads.argtypes = [C.c_int]
+    L.pt_table_last_transfer.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.pt_set_spin_limit.argtypes = [C.c_int64]
     L.pt_set_spin_limit.restype = C.c_int64
     L.pt_set_device_alloc_limit.argtypes = [C.c_int64]
@@ -461,6 +463,12 @@ class PatchTable:
     def dt_levels(self) -> int:
         return int(lib().pt_table_dt_levels(self._h))
 
+    def last_transfer(self):
+        """(host->device bytes, device->host bytes) of the last host lookup."""
+        h2d, d2h = C.c_int64(), C.c_int64()
+        _check(lib().pt_table_last_transfer(self._h, C.byref(h2d), C.byref(d2h)))
+        return int(h2d.value), int(d2h.value)
+
     BUILD_STAGES = ("descriptor", "kcoherence", "partition", "shuffle", "populate_dt", "total")
 
     def build_profile(self):
@@ -537,6 +545,11 @@ def descriptor(params: PatchTableParams, img):
     out = np.empty((img.shape[0] - 7, img.shape[1] - 7, params.ndims), np.float32)
     _check(lib().pt_descriptor(C.byref(params._p), img, img.shape[0], img.shape[1], out))
     return out
+
+
+def set_host_threads(n: int) -> int:
+    """Host threads that widen downloaded NNFs to float64 (n <= 0: default).  Returns the previous count."""
+    return int(lib().pt_set_host_threads(int(n)))
 
 
 def set_spin_limit(polls: int) -> int:

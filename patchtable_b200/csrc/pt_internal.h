@@ -83,4 +83,27 @@ template<class T> struct DevBuf {
 private:
     size_t held = 0;
 };
+
+/* Page-locked host memory owned by a table (download staging); freed with cudaFreeHost. */
+template<class T> struct PinnedBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    PinnedBuf() {}
+    PinnedBuf(const PinnedBuf &) = delete;
+    PinnedBuf &operator=(const PinnedBuf &) = delete;
+    ~PinnedBuf() { if (p) cudaFreeHost(p); }
+    cudaError_t reserve(size_t count) {
+        if (count <= n && p) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr; n = 0;
+        cudaError_t e = cudaMallocHost((void **) &p, sizeof(T) * (count ? count : 1));
+        if (e == cudaSuccess) n = count;
+        else p = nullptr;
+        return e;
+    }
+};
 #endif
+
+/* pt_host.cpp: ann[3i .. 3i+2] = (x, y, dist) of pos[i] / dist[i] for i < n, in float64, split
+   across the library's host threads (pt_set_host_threads). */
+void pt_expand_nnf(const int *pos, const float *dist, long long n, double *ann);

@@ -152,6 +152,9 @@ struct pt_table {
     cudaStream_t st_in = nullptr, st_out = nullptr;    /* banded host lookups: upload / download */
     cudaStream_t st_choose = nullptr, st_pull = nullptr; /* banded host lookups: later phases */
     std::vector<cudaEvent_t> band_ev;
+    PinnedBuf<int> h_pos;             /* banded host lookups: packed field downloaded per band */
+    PinnedBuf<float> h_d;
+    long long last_h2d = 0, last_d2h = 0;   /* bytes copied by the last host lookup */
 
     ~pt_table() {
         for (auto e : events) cudaEventDestroy(e);
@@ -728,17 +731,20 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
    its own pixel rows plus 7; its choose also reads the next band's RGBA rows (written by that
    band's descriptor launch) and its pull the next band's choices.  Four streams carry the phases:
    upload of band b -> descriptor and table entries of band b (one fused pass) -> choose of band
-   b-1 -> pull and output of band b-2 -> download of band b-2, each waiting on the events its
-   inputs come from; choose and pull start from the initial field without reading state arrays.  Consecutive bands' kernels overlap (filling each other's last waves) and the
-   copies overlap the kernels.  Concurrent kernels always touch disjoint rows (bands are at least
-   32 rows; a pull reads at most 16 rows beyond its band).  Every kernel computes exactly what the
-   whole-image launch computes for its rows, so the result is identical. */
+   b-1 -> pull of band b-2 -> download of band b-2, each waiting on the events its inputs come
+   from; choose and pull start from the initial field without reading state arrays.  Consecutive
+   bands' kernels overlap (filling each other's last waves) and the copies overlap the kernels.
+   Concurrent kernels always touch disjoint rows (bands are at least 32 rows; a pull reads at most
+   16 rows beyond its band).  Every kernel computes exactly what the whole-image launch computes
+   for its rows, so the result is identical.  The download carries the packed field (int32
+   position, float32 distance: 8 bytes per patch instead of the float64 record's 24) into pinned
+   staging; once a band has arrived, the host threads widen it into the caller's float64 buffer
+   while later bands are still computed and copied. */
 pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_out) {
     const pt_params &p = t->p;
     const int eh = h - 7, ew = w - 7;
     const long long P = (long long) eh * ew;
     PT_TRY(ensure_query_buffers(t, h, w));
-    PT_CUDA(t->q_ann.reserve((size_t) P * 3));
     for (cudaStream_t *sp : {&t->st_in, &t->st_out, &t->st_choose, &t->st_pull})
         if (!*sp) PT_CUDA(cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking));
     int B = 0;
@@ -769,13 +775,15 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
         if (B < 32) B = 32;
     }
     const int nb = (eh + B - 1) / B;
-    while ((int) t->band_ev.size() < 4 * nb + 1) {
+    while ((int) t->band_ev.size() < 5 * nb + 1) {
         cudaEvent_t e;
         PT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         t->band_ev.push_back(e);
     }
-    cudaEvent_t *ev_in = t->band_ev.data(), *ev_a = ev_in + nb, *ev_b = ev_a + nb, *ev_c = ev_b + nb;
-    cudaEvent_t ev_start = t->band_ev[4 * nb];
+    PT_CUDA(t->h_pos.reserve(P));
+    PT_CUDA(t->h_d.reserve(P));
+    cudaEvent_t *ev_in = t->band_ev.data(), *ev_a = ev_in + nb, *ev_b = ev_a + nb, *ev_c = ev_b + nb, *ev_d = ev_c + nb;
+    cudaEvent_t ev_start = t->band_ev[5 * nb];
     cudaStream_t sa = t->st, sb = t->st_choose, sc = t->st_pull;
     /* the phases start after whatever the table's stream has queued */
     PT_CUDA(cudaEventRecord(ev_start, sa));
@@ -826,16 +834,26 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
             qb.row0 = r0;
             qb.rows = r1 - r0;
             qb.stream = sc;
-            qb.ann = t->q_ann.p;                            /* the pull writes the band's NNF rows */
+            /* the pull writes the band's final field (packed position, float distance) */
             PT_TRY(pt_launch_pull(qb, (int) P, t->q_rgba.p, t->b_rgba.p, nullptr, nullptr, t->q_chpos.p, t->q_chd.p,
                                   t->q_pos[1].p, t->q_d[1].p, nullptr, sc));
             const size_t o = (size_t) r0 * ew;
-            const int n = (r1 - r0) * ew;
+            const size_t n = (size_t) (r1 - r0) * ew;
             PT_CUDA(cudaEventRecord(ev_c[b - 2], sc));
             PT_CUDA(cudaStreamWaitEvent(t->st_out, ev_c[b - 2], 0));
-            PT_CUDA(cudaMemcpyAsync(ann_out + 3 * o, t->q_ann.p + 3 * o, sizeof(double) * 3 * (size_t) n,
-                                    cudaMemcpyDeviceToHost, t->st_out));
+            PT_CUDA(cudaMemcpyAsync(t->h_pos.p + o, t->q_pos[1].p + o, sizeof(int) * n, cudaMemcpyDeviceToHost, t->st_out));
+            PT_CUDA(cudaMemcpyAsync(t->h_d.p + o, t->q_d[1].p + o, sizeof(float) * n, cudaMemcpyDeviceToHost, t->st_out));
+            PT_CUDA(cudaEventRecord(ev_d[b - 2], t->st_out));
         }
+    }
+    t->last_h2d = (long long) sizeof(float) * h * w * 3;
+    t->last_d2h = (long long) (sizeof(int) + sizeof(float)) * P;
+    /* widen each band as soon as it has arrived */
+    for (int b = 0; b < nb; b++) {
+        PT_CUDA(cudaEventSynchronize(ev_d[b]));
+        const int r0 = b * B, r1 = std::min(eh, r0 + B);
+        const size_t o = (size_t) r0 * ew;
+        pt_expand_nnf(t->h_pos.p + o, t->h_d.p + o, (long long) (r1 - r0) * ew, ann_out + 3 * o);
     }
     PT_CUDA(cudaStreamSynchronize(t->st_out));
     for (cudaStream_t s2 : {sa, sb, sc}) PT_CUDA(cudaStreamSynchronize(s2));
@@ -1150,6 +1168,8 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int ih, int iw, double *a
         PT_TRY(lookup_device(t, t->q_rgb.p, h, w, t->q_ann.p, t->st, nullptr, nullptr, t->q_prev.p,
                              coh_sv ? t->q_sv.p : nullptr));
         PT_CUDA(cudaMemcpyAsync(ann_out, t->q_ann.p, sizeof(double) * (size_t) P * 3, cudaMemcpyDeviceToHost, t->st));
+        t->last_h2d = (long long) (sizeof(double) * 3 * P + sizeof(float) * in_floats + (coh_sv ? sizeof(float) * P : 0));
+        t->last_d2h = (long long) sizeof(double) * 3 * P;
         int bad = 0;
         PT_CUDA(cudaMemcpyAsync(&bad, t->q_tbad.p, sizeof(int), cudaMemcpyDeviceToHost, t->st));
         PT_CUDA(cudaStreamSynchronize(t->st));
@@ -1169,7 +1189,16 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int ih, int iw, double *a
     PT_TRY(lookup_device(t, t->q_rgb.p, h, w, t->q_ann.p, t->st));
     PT_CUDA(cudaMemcpyAsync(ann_out, t->q_ann.p, sizeof(double) * (size_t) P * 3, cudaMemcpyDeviceToHost, t->st));
     PT_CUDA(cudaStreamSynchronize(t->st));
+    t->last_h2d = (long long) (sizeof(float) * in_floats);
+    t->last_d2h = (long long) sizeof(double) * 3 * P;
     if (seconds) *seconds = now_s() - T0;
+    return PT_OK;
+}
+
+pt_status pt_table_last_transfer(const pt_table *t, int64_t *h2d_bytes, int64_t *d2h_bytes) {
+    if (!t || !h2d_bytes || !d2h_bytes) return pt_fail(PT_BAD_ARG, "null argument");
+    *h2d_bytes = t->last_h2d;
+    *d2h_bytes = t->last_d2h;
     return PT_OK;
 }
 
