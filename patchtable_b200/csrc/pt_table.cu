@@ -96,6 +96,14 @@ extern "C" int64_t pt_set_device_alloc_limit(int64_t bytes) { return g_alloc_lim
 
 extern "C" int64_t pt_device_bytes_in_use(void) { return g_alloc_live.load(); }
 
+/* What a recorded banded-lookup graph depends on besides the query image's address (compared
+   bytewise; zero-filled before use). */
+struct BandKey {
+    pt_params p;
+    int h, w, B;
+    const void *bufs[10];
+};
+
 struct pt_table {
     pt_params p;
     int h = 0, w = 0, eh = 0, ew = 0;
@@ -154,9 +162,26 @@ struct pt_table {
     std::vector<cudaEvent_t> band_ev;
     PinnedBuf<int> h_pos;             /* banded host lookups: packed field downloaded per band */
     PinnedBuf<float> h_d;
+    /* banded host lookups replayed as a CUDA graph: the graph, its upload nodes (by offset into
+       the query image), the image it currently reads and what it was recorded for */
+    cudaGraph_t band_graph = nullptr;
+    cudaGraphExec_t band_exec = nullptr;
+    std::vector<std::pair<cudaGraphNode_t, size_t>> band_h2d;
+    const float *band_a = nullptr;
+    bool band_seen = false;
+    BandKey band_key_v;
+    void drop_band_graph() {
+        if (band_exec) cudaGraphExecDestroy(band_exec);
+        if (band_graph) cudaGraphDestroy(band_graph);
+        band_exec = nullptr;
+        band_graph = nullptr;
+        band_h2d.clear();
+        band_seen = false;
+    }
     long long last_h2d = 0, last_d2h = 0;   /* bytes copied by the last host lookup */
 
     ~pt_table() {
+        drop_band_graph();
         for (auto e : events) cudaEventDestroy(e);
         for (auto e : band_ev) cudaEventDestroy(e);
         if (st_in) cudaStreamDestroy(st_in);
@@ -739,14 +764,15 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
    for its rows, so the result is identical.  The download carries the packed field (int32
    position, float32 distance: 8 bytes per patch instead of the float64 record's 24) into pinned
    staging; once a band has arrived, the host threads widen it into the caller's float64 buffer
-   while later bands are still computed and copied. */
-pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_out) {
+   while later bands are still computed and copied.
+
+   The sequence is about a hundred copies, launches and event operations.  When the query image
+   sits in page-locked memory and the same sizes, parameters and buffers come again, it is
+   recorded once into a CUDA graph and replayed with one launch (the upload nodes are pointed at
+   the caller's image each time), so the host's enqueue cost stays off the critical path. */
+int band_rows(const pt_table *t, int h, int w) {
     const pt_params &p = t->p;
     const int eh = h - 7, ew = w - 7;
-    const long long P = (long long) eh * ew;
-    PT_TRY(ensure_query_buffers(t, h, w));
-    for (cudaStream_t *sp : {&t->st_in, &t->st_out, &t->st_choose, &t->st_pull})
-        if (!*sp) PT_CUDA(cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking));
     int B = 0;
     if (p.gpu_bands <= 0) {
         /* Default: the band's choose launch fills whole waves.  A choose CTA of tw patches is
@@ -758,8 +784,9 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
         static int sms = 0;
         if (!sms) {
             int dev = 0;
-            PT_CUDA(cudaGetDevice(&dev));
-            PT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (sms < 1) sms = 148;
         }
         const int tw = (p.gpu_tile == 64 || p.gpu_tile == 128 || p.gpu_tile == 256) ? p.gpu_tile : 32;
         const double rows_wave = (double) sms * (12 * 64 / tw) / ((ew + tw - 1) / tw);
@@ -774,18 +801,19 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
         B = ((eh + want - 1) / want + 7) / 8 * 8;       /* about `want` bands, each a multiple of 8 rows */
         if (B < 32) B = 32;
     }
-    const int nb = (eh + B - 1) / B;
-    while ((int) t->band_ev.size() < 5 * nb + 1) {
-        cudaEvent_t e;
-        PT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        t->band_ev.push_back(e);
-    }
-    PT_CUDA(t->h_pos.reserve(P));
-    PT_CUDA(t->h_d.reserve(P));
+    return B;
+}
+
+/* Enqueues the band pipeline on the table's streams, starting after the work queued on t->st and
+   joining every stream back into t->st at the end.  ev_d[b] (recorded as an external event, so it
+   also fires inside a graph) marks band b's download. */
+pt_status enqueue_bands(pt_table *t, const float *a, int h, int w, int B, int nb) {
+    const pt_params &p = t->p;
+    const int eh = h - 7, ew = w - 7;
+    const long long P = (long long) eh * ew;
     cudaEvent_t *ev_in = t->band_ev.data(), *ev_a = ev_in + nb, *ev_b = ev_a + nb, *ev_c = ev_b + nb, *ev_d = ev_c + nb;
-    cudaEvent_t ev_start = t->band_ev[5 * nb];
+    cudaEvent_t ev_start = t->band_ev[5 * nb], *ev_join = &t->band_ev[5 * nb + 1];
     cudaStream_t sa = t->st, sb = t->st_choose, sc = t->st_pull;
-    /* the phases start after whatever the table's stream has queued */
     PT_CUDA(cudaEventRecord(ev_start, sa));
     for (cudaStream_t s2 : {t->st_in, sb, sc, t->st_out}) PT_CUDA(cudaStreamWaitEvent(s2, ev_start, 0));
     QuerySetup qs;
@@ -843,20 +871,106 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
             PT_CUDA(cudaStreamWaitEvent(t->st_out, ev_c[b - 2], 0));
             PT_CUDA(cudaMemcpyAsync(t->h_pos.p + o, t->q_pos[1].p + o, sizeof(int) * n, cudaMemcpyDeviceToHost, t->st_out));
             PT_CUDA(cudaMemcpyAsync(t->h_d.p + o, t->q_d[1].p + o, sizeof(float) * n, cudaMemcpyDeviceToHost, t->st_out));
-            PT_CUDA(cudaEventRecord(ev_d[b - 2], t->st_out));
+            PT_CUDA(cudaEventRecordWithFlags(ev_d[b - 2], t->st_out, cudaEventRecordExternal));
         }
+    }
+    int k = 0;
+    for (cudaStream_t s2 : {t->st_in, sb, sc, t->st_out}) {
+        PT_CUDA(cudaEventRecord(ev_join[k], s2));
+        PT_CUDA(cudaStreamWaitEvent(sa, ev_join[k], 0));
+        k++;
+    }
+    return PT_OK;
+}
+
+BandKey band_key(const pt_table *t, int h, int w, int B) {
+    BandKey k;
+    memset(&k, 0, sizeof(k));
+    k.p = t->p;
+    k.h = h; k.w = w; k.B = B;
+    const void *b[10] = {t->q_rgb.p, t->q_rgba.p, t->q_tcand.p, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p,
+                         t->q_pos[1].p, t->q_d[1].p, t->h_pos.p, t->h_d.p};
+    memcpy(k.bufs, b, sizeof(b));
+    return k;
+}
+
+pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_out) {
+    const int eh = h - 7, ew = w - 7;
+    const long long P = (long long) eh * ew;
+    PT_TRY(ensure_query_buffers(t, h, w));
+    for (cudaStream_t *sp : {&t->st_in, &t->st_out, &t->st_choose, &t->st_pull})
+        if (!*sp) PT_CUDA(cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking));
+    const int B = band_rows(t, h, w), nb = (eh + B - 1) / B;
+    if ((int) t->band_ev.size() < 5 * nb + 5) {
+        t->drop_band_graph();                  /* its event nodes name the old events */
+        while ((int) t->band_ev.size() < 5 * nb + 5) {
+            cudaEvent_t e;
+            PT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            t->band_ev.push_back(e);
+        }
+    }
+    PT_CUDA(t->h_pos.reserve(P));
+    PT_CUDA(t->h_d.reserve(P));
+    cudaPointerAttributes attr;
+    const bool pinned = cudaPointerGetAttributes(&attr, a) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    const BandKey key = band_key(t, h, w, B);
+    const bool same = t->band_seen && memcmp(&key, &t->band_key_v, sizeof(key)) == 0;
+    if (!pinned || !same) {
+        /* enqueue directly; a second call with the same key and a page-locked image records the graph */
+        t->drop_band_graph();
+        PT_TRY(enqueue_bands(t, a, h, w, B, nb));
+        memcpy(&t->band_key_v, &key, sizeof(key));
+        t->band_seen = pinned;
+    } else {
+        if (!t->band_exec) {
+            cudaGraph_t g = nullptr;
+            PT_CUDA(cudaStreamBeginCapture(t->st, cudaStreamCaptureModeThreadLocal));
+            pt_status s = enqueue_bands(t, a, h, w, B, nb);
+            cudaError_t e = cudaStreamEndCapture(t->st, &g);
+            if (s != PT_OK) { if (g) cudaGraphDestroy(g); return s; }
+            if (e != cudaSuccess) return pt_fail(PT_CUDA_ERR, "capturing the banded lookup: %s", cudaGetErrorString(e));
+            t->band_graph = g;
+            PT_CUDA(cudaGraphInstantiate(&t->band_exec, g, 0));
+            /* the upload nodes, by their offset into the query image */
+            size_t nn = 0;
+            PT_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+            std::vector<cudaGraphNode_t> nodes(nn);
+            PT_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+            const char *lo = (const char *) a, *hi = lo + sizeof(float) * (size_t) h * w * 3;
+            for (cudaGraphNode_t nd : nodes) {
+                cudaGraphNodeType ty;
+                PT_CUDA(cudaGraphNodeGetType(nd, &ty));
+                if (ty != cudaGraphNodeTypeMemcpy) continue;
+                cudaMemcpy3DParms mp;
+                PT_CUDA(cudaGraphMemcpyNodeGetParams(nd, &mp));
+                const char *src = (const char *) mp.srcPtr.ptr;
+                if (src >= lo && src < hi) t->band_h2d.push_back({nd, (size_t) (src - lo)});
+            }
+            t->band_a = a;
+        } else if (t->band_a != a) {
+            for (auto &u : t->band_h2d) {
+                cudaMemcpy3DParms mp;
+                PT_CUDA(cudaGraphMemcpyNodeGetParams(u.first, &mp));
+                mp.srcPtr.ptr = (void *) ((const char *) a + u.second);
+                PT_CUDA(cudaGraphExecMemcpyNodeSetParams(t->band_exec, u.first, &mp));
+            }
+            t->band_a = a;
+        }
+        PT_CUDA(cudaGraphLaunch(t->band_exec, t->st));
+        pt_count_launches(3 * nb);
     }
     t->last_h2d = (long long) sizeof(float) * h * w * 3;
     t->last_d2h = (long long) (sizeof(int) + sizeof(float)) * P;
     /* widen each band as soon as it has arrived */
+    cudaEvent_t *ev_d = t->band_ev.data() + 4 * nb;
     for (int b = 0; b < nb; b++) {
         PT_CUDA(cudaEventSynchronize(ev_d[b]));
         const int r0 = b * B, r1 = std::min(eh, r0 + B);
         const size_t o = (size_t) r0 * ew;
         pt_expand_nnf(t->h_pos.p + o, t->h_d.p + o, (long long) (r1 - r0) * ew, ann_out + 3 * o);
     }
-    PT_CUDA(cudaStreamSynchronize(t->st_out));
-    for (cudaStream_t s2 : {sa, sb, sc}) PT_CUDA(cudaStreamSynchronize(s2));
+    PT_CUDA(cudaStreamSynchronize(t->st));
     return PT_OK;
 }
 

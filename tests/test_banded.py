@@ -56,3 +56,35 @@ def test_banded_with_allowed_mask(gpu, libc):
     host = t.lookup(a)
     assert np.array_equal(host, _device(t, a))
     assert np.all(allowed[host[..., 1].astype(int), host[..., 0].astype(int)] == 1)
+
+
+def test_banded_graph_replay_with_page_locked_images(gpu, libc):
+    """A page-locked query image seen again with the same sizes and parameters is answered by
+    replaying the recorded band graph; a second page-locked image re-points its upload nodes, a
+    pageable one is enqueued directly, a parameter change records anew.  Every answer equals the
+    device lookup's, and the host threads' count does not change it."""
+    import torch
+    a, b = synth.pair(300, 420, 81)
+    a2 = synth.image_a(300, 420, 82)
+    p = ptb.PatchTableParams("-speed 3 -coherence_spatial 4 -limit 2")
+    libc.srand(1)
+    t = ptb.PatchTable(p, b)
+    p.gpu_prop_passes, p.gpu_pull_max = 1, 1
+    want, want2 = _device(t, a), _device(t, a2)
+    pa = torch.from_numpy(a).pin_memory().numpy()
+    pa2 = torch.from_numpy(a2).pin_memory().numpy()
+    out = torch.empty(want.shape, dtype=torch.float64).pin_memory().numpy()
+    for img, ref in ((pa, want), (pa, want), (pa, want), (pa2, want2), (pa, want), (a2, want2), (pa, want)):
+        out[:] = -1
+        t.lookup(img, out=out)
+        assert np.array_equal(out, ref)
+    p.gpu_tile = 64
+    for _ in range(3):
+        assert np.array_equal(t.lookup(pa), want)
+    old = ptb.set_host_threads(1)
+    try:
+        assert np.array_equal(t.lookup(pa), want)
+    finally:
+        ptb.set_host_threads(old)
+    assert t.last_transfer() == (a.nbytes, 8 * want.shape[0] * want.shape[1])
+    t.close()
