@@ -805,9 +805,9 @@ int band_rows(const pt_table *t, int h, int w) {
 }
 
 /* Enqueues the band pipeline on the table's streams, starting after the work queued on t->st and
-   joining every stream back into t->st at the end.  ev_d[b] (recorded as an external event, so it
-   also fires inside a graph) marks band b's download. */
-pt_status enqueue_bands(pt_table *t, const float *a, int h, int w, int B, int nb) {
+   joining every stream back into t->st at the end.  ev_d[b] marks band b's download (while
+   capturing, as an external event node, so that the replayed graph records it too). */
+pt_status enqueue_bands(pt_table *t, const float *a, int h, int w, int B, int nb, bool capturing) {
     const pt_params &p = t->p;
     const int eh = h - 7, ew = w - 7;
     const long long P = (long long) eh * ew;
@@ -871,7 +871,8 @@ pt_status enqueue_bands(pt_table *t, const float *a, int h, int w, int B, int nb
             PT_CUDA(cudaStreamWaitEvent(t->st_out, ev_c[b - 2], 0));
             PT_CUDA(cudaMemcpyAsync(t->h_pos.p + o, t->q_pos[1].p + o, sizeof(int) * n, cudaMemcpyDeviceToHost, t->st_out));
             PT_CUDA(cudaMemcpyAsync(t->h_d.p + o, t->q_d[1].p + o, sizeof(float) * n, cudaMemcpyDeviceToHost, t->st_out));
-            PT_CUDA(cudaEventRecordWithFlags(ev_d[b - 2], t->st_out, cudaEventRecordExternal));
+            if (capturing) PT_CUDA(cudaEventRecordWithFlags(ev_d[b - 2], t->st_out, cudaEventRecordExternal));
+            else PT_CUDA(cudaEventRecord(ev_d[b - 2], t->st_out));
         }
     }
     int k = 0;
@@ -919,14 +920,14 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     if (!pinned || !same) {
         /* enqueue directly; a second call with the same key and a page-locked image records the graph */
         t->drop_band_graph();
-        PT_TRY(enqueue_bands(t, a, h, w, B, nb));
+        PT_TRY(enqueue_bands(t, a, h, w, B, nb, false));
         memcpy(&t->band_key_v, &key, sizeof(key));
         t->band_seen = pinned;
     } else {
         if (!t->band_exec) {
             cudaGraph_t g = nullptr;
             PT_CUDA(cudaStreamBeginCapture(t->st, cudaStreamCaptureModeThreadLocal));
-            pt_status s = enqueue_bands(t, a, h, w, B, nb);
+            pt_status s = enqueue_bands(t, a, h, w, B, nb, true);
             cudaError_t e = cudaStreamEndCapture(t->st, &g);
             if (s != PT_OK) { if (g) cudaGraphDestroy(g); return s; }
             if (e != cudaSuccess) return pt_fail(PT_CUDA_ERR, "capturing the banded lookup: %s", cudaGetErrorString(e));
