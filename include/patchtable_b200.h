@@ -348,9 +348,11 @@ int64_t pt_device_bytes_in_use(void);
 /* Host threads that widen the downloaded NNF to float64 in pt_table_lookup (no reference
    counterpart; the reference's lookup writes its float64 field directly, patchtable.h:3500): the
    GPU sends 8 bytes per patch (packed position, float distance) and these threads write the
-   24-byte records into the caller's buffer while later rows are still computed.  n <= 0 restores
-   the default, min(8, hardware threads).  Returns the previous count.  Not to be called while a
-   lookup runs. */
+   24-byte records into the caller's buffer while later rows are still computed.  n = 0 restores
+   the default, min(8, hardware threads); n < 0 turns the host widening off (the GPU writes the
+   float64 records and they are copied as they are: three times the bytes over PCIe, no host
+   work).  Returns the previous count (-1 when widening was off).  Not to be called while a lookup
+   runs. */
 int pt_set_host_threads(int n);
 /* Bytes the last pt_table_lookup on this table copied host -> device and device -> host. */
 pt_status pt_table_last_transfer(const pt_table *t, int64_t *h2d_bytes, int64_t *d2h_bytes);

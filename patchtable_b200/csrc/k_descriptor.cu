@@ -127,6 +127,24 @@ __device__ __forceinline__ void stage_pix(float *pix, const float *__restrict__ 
     }
 }
 
+/* A patch's descriptor: its table entry (CELLS) and / or its store record (desc set). */
+template<bool CELLS>
+__device__ __forceinline__ void emit_patch(const float (&out)[PT_DESC_MAX], size_t p, const CellPlan *cp, int *tcand,
+                                           float *desc, int ds) {
+    if (CELLS) {
+        long long cell = 0;
+#pragma unroll
+        for (int d = 0; d < PT_DESC_MAX; d++)
+            if (d < cp->G) cell += (long long) pt_get_bin(cp->min_val[d], cp->range[d], cp->to_bin + d * PT_NMAP, out[d]) * cp->stride[d];
+        tcand[p] = __ldg(cp->table + cell);
+    }
+    if (desc == nullptr) return;
+    float4 *dst = reinterpret_cast<float4 *>(desc + p * ds);
+#pragma unroll
+    for (int q = 0; q < PT_DESC_MAX / 4; q++)
+        if (q < ds / 4) dst[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
+}
+
 /* One 64 x 8 block of patches with top-left patch (x0, y0).  With CELLS the table entry of each
    patch's cell is written to cp.tcand (and the descriptor only where desc is set). */
 template<bool CELLS = false>
@@ -139,54 +157,63 @@ __device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, c
     stage_pix(pix, rgb, h, w, convert, rgba, eh, ew, x0, y0);
     __syncthreads();
 
+    /* horizontal filters: each item is 4 consecutive outputs of one row, read as a 12-float window
+       (three 16-byte shared loads) and summed tap by tap in the filter's order */
     const int ncombo = c_plan.ncombo;
+    constexpr int HQ = TW / 4;                         /* 4-output items per row */
     for (int m = 0; m < ncombo; m++) {                /* one filter at a time: its signs stay in registers */
         float sg[8];
 #pragma unroll
         for (int b = 0; b < 8; b++) sg[b] = c_plan.combo_hf[m][b];
         const float *plane = pix + c_plan.combo_plane[m] * RH * RWP;
         float *dst = hs + m * RH * TW;
-        for (int i = tid; i < RH * TW; i += NT) {
-            const int r = i / TW, j = i % TW;
-            const float *row = plane + r * RWP + j;
-            float s = 0.f;
+        for (int i = tid; i < RH * HQ; i += NT) {
+            const int r = i / HQ, j0 = (i % HQ) * 4;
+            const float4 *row = reinterpret_cast<const float4 *>(plane + r * RWP + j0);
+            const float4 u0 = row[0], u1 = row[1], u2 = row[2];
+            const float x[11] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w, u2.x, u2.y, u2.z};
+            float o[4];
 #pragma unroll
-            for (int b = 0; b < 8; b++) s = __fmaf_rn(sg[b], row[b], s);
-            dst[i] = s;
+            for (int q = 0; q < 4; q++) {
+                float acc = 0.f;
+#pragma unroll
+                for (int b = 0; b < 8; b++) acc = __fmaf_rn(sg[b], x[q + b], acc);
+                o[q] = acc;
+            }
+            *reinterpret_cast<float4 *>(dst + r * TW + j0) = make_float4(o[0], o[1], o[2], o[3]);
         }
     }
     __syncthreads();
 
+    /* vertical filters: each thread takes two vertically adjacent patches of one column and reads
+       the 9 filtered rows under them once per channel */
     const int nd = c_plan.nd;
-    for (int i = tid; i < TW * TH; i += NT) {
-        int pi = i / TW, pj = i % TW;
-        int py = y0 + pi, px = x0 + pj;
-        if (py >= eh || px >= ew || (!CELLS && desc == nullptr)) continue;
-        float out[PT_DESC_MAX];
+    for (int i = tid; i < TW * (TH / 2); i += NT) {
+        const int pj = i % TW, pi = 2 * (i / TW);
+        const int px = x0 + pj, py = y0 + pi;
+        if (px >= ew || py >= eh || (!CELLS && desc == nullptr)) continue;
+        const bool two = py + 1 < eh;
+        float out0[PT_DESC_MAX], out1[PT_DESC_MAX];
 #pragma unroll
         for (int c = 0; c < PT_DESC_MAX; c++) {
+            out0[c] = out1[c] = 0.f;
             if (c < nd) {
                 const float *col = hs + (c_plan.ch_combo[c] * RH + pi) * TW + pj;
-                float s = 0.f;
+                float y[9];
 #pragma unroll
-                for (int a = 0; a < 8; a++) s = __fmaf_rn(c_plan.ch_vf[c][a], col[a * TW], s);
-                out[c] = s;
-            } else {
-                out[c] = 0.f;
+                for (int a = 0; a < 9; a++) y[a] = col[a * TW];
+                float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+                for (int a = 0; a < 8; a++) {
+                    s0 = __fmaf_rn(c_plan.ch_vf[c][a], y[a], s0);
+                    s1 = __fmaf_rn(c_plan.ch_vf[c][a], y[a + 1], s1);
+                }
+                out0[c] = s0;
+                out1[c] = s1;
             }
         }
-        if (CELLS) {
-            long long cell = 0;
-#pragma unroll
-            for (int d = 0; d < PT_DESC_MAX; d++)
-                if (d < cp->G) cell += (long long) pt_get_bin(cp->min_val[d], cp->range[d], cp->to_bin + d * PT_NMAP, out[d]) * cp->stride[d];
-            tcand[(size_t) py * ew + px] = __ldg(cp->table + cell);
-            if (desc == nullptr) continue;
-        }
-        float4 *dst = reinterpret_cast<float4 *>(desc + ((size_t) py * ew + px) * ds);
-#pragma unroll
-        for (int q = 0; q < PT_DESC_MAX / 4; q++)
-            if (q < ds / 4) dst[q] = make_float4(out[4 * q], out[4 * q + 1], out[4 * q + 2], out[4 * q + 3]);
+        emit_patch<CELLS>(out0, (size_t) py * ew + px, cp, tcand, desc, ds);
+        if (two) emit_patch<CELLS>(out1, (size_t) (py + 1) * ew + px, cp, tcand, desc, ds);
     }
 }
 
@@ -195,27 +222,33 @@ __device__ __forceinline__ void desc_tile(const DescPlan &c_plan, float *smem, c
 __global__ void __launch_bounds__(NT, 4)
 k_descriptor(const DescPlan c_plan, const float *__restrict__ rgb, int h, int w, int convert,
              float4 *__restrict__ rgba, float *__restrict__ desc, int ds, int eh, int ew, int ty0) {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     desc_tile(c_plan, smem, rgb, h, w, convert, rgba, desc, ds, eh, ew, blockIdx.x * TW, (blockIdx.y + ty0) * TH);
 }
 
 __global__ void __launch_bounds__(NT, 4)
 k_descriptor_cells(const DescPlan c_plan, const CellPlan cp, const float *__restrict__ rgb, int h, int w, int convert,
                    float4 *__restrict__ rgba, int eh, int ew, int ty0) {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     desc_tile<true>(c_plan, smem, rgb, h, w, convert, rgba, nullptr, 0, eh, ew, blockIdx.x * TW, (blockIdx.y + ty0) * TH, &cp,
                     cp.tcand);
 }
 
 /* Persistent descriptor pass over the 64 x 8 tiles of every image of a batch (images, RGBA
-   copies and descriptors concatenated); with CELLS the table entries of the patches' cells are
-   written instead of the descriptors. */
+   copies and descriptors concatenated), the tiles handed out by a work counter; with CELLS the
+   table entries of the patches' cells are written instead of the descriptors. */
 template<bool CELLS>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 4)
 k_descriptor_batch(const DescPlan c_plan, const CellPlan cp, const PtBatchImage *__restrict__ imgs, int n, long long ntiles,
-                   const float *__restrict__ rgb, int convert, float4 *__restrict__ rgba, float *__restrict__ desc, int ds) {
-    extern __shared__ float smem[];
-    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+                   const float *__restrict__ rgb, int convert, float4 *__restrict__ rgba, float *__restrict__ desc, int ds,
+                   unsigned long long *work) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ long long s_next;
+    for (;;) {
+        if (threadIdx.x == 0) s_next = (long long) atomicAdd(work, 1ull);   /* tiles go out one at a time */
+        __syncthreads();
+        const long long t = s_next;
+        if (t >= ntiles) break;
         int lo = 0, hi = n - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
@@ -227,7 +260,7 @@ k_descriptor_batch(const DescPlan c_plan, const CellPlan cp, const PtBatchImage 
         desc_tile<CELLS>(c_plan, smem, rgb + 3 * g.pix_off, g.h, g.w, convert, rgba ? rgba + g.pix_off : nullptr,
                          CELLS ? nullptr : desc + g.patch_off * ds, ds, g.eh, g.ew, (int) (lt % tpr) * TW, (int) (lt / tpr) * TH,
                          &cp, CELLS ? cp.tcand + g.patch_off : nullptr);
-        __syncthreads();                                 /* the next tile reuses the shared memory */
+        __syncthreads();                                 /* the next tile reuses the shared memory and s_next */
     }
 }
 
@@ -389,24 +422,34 @@ namespace {
 template<bool CELLS>
 pt_status launch_descriptor_batch(int ndims, int nchroma, const CellPlan &cp, const PtBatchImage *imgs, int n,
                                   long long ntiles, const float *rgb, int convert, float4 *rgba, float *desc, int ds,
-                                  cudaStream_t st) {
+                                  unsigned long long *work, cudaStream_t st) {
     if (convert == PT_COLOR_LAB) PT_TRY(pt_lab_tables_ready());
     DescPlan plan;
     PT_TRY(make_plan(ndims, nchroma, plan));
     if (ntiles <= 0) return PT_OK;
-    const size_t smem = pt_descriptor_smem(0);
-    static int nsm = 0, per = 0;
+    /* shared memory for this plan's filters only, as the single-image pass sizes it */
+    const size_t smem = sizeof(float) * (3 * RH * RWP + plan.ncombo * RH * TW);
+    static int nsm = 0;
+    static size_t per_smem[PT_DESC_MAX + 1] = {};
+    static int per_n[PT_DESC_MAX + 1] = {};
     if (!nsm) {
         int dev = 0;
         PT_CUDA(cudaGetDevice(&dev));
         PT_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        PT_CUDA(cudaFuncSetAttribute(k_descriptor_batch<CELLS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-        PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_descriptor_batch<CELLS>, NT, smem));
-        if (per < 1) per = 1;
+        PT_CUDA(cudaFuncSetAttribute(k_descriptor_batch<CELLS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int) pt_descriptor_smem(0)));
     }
-    const long long g = (long long) per * nsm;
+    const int slot = plan.ncombo;
+    if (per_smem[slot] != smem) {
+        int per = 0;
+        PT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_descriptor_batch<CELLS>, NT, smem));
+        per_n[slot] = per < 1 ? 1 : per;
+        per_smem[slot] = smem;
+    }
+    const long long g = (long long) per_n[slot] * nsm;
+    PT_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st));
     k_descriptor_batch<CELLS><<<(unsigned) (ntiles < g ? ntiles : g), NT, smem, st>>>(plan, cp, imgs, n, ntiles, rgb, convert,
-                                                                                     rgba, desc, ds);
+                                                                                     rgba, desc, ds, work);
     PT_LAUNCHED();
     return PT_OK;
 }
@@ -415,7 +458,7 @@ pt_status launch_descriptor_batch(int ndims, int nchroma, const CellPlan &cp, co
 
 pt_status pt_launch_descriptor_cells_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
                                            const float *rgb, int convert, float4 *rgba, const PtBins &bins, const int *to_bin,
-                                           const int *table, int *tcand, cudaStream_t st) {
+                                           const int *table, int *tcand, unsigned long long *work, cudaStream_t st) {
     if (bins.G < 1 || bins.G > ndims) return pt_fail(PT_BAD_ARG, "grid dims %d outside 1..%d", bins.G, ndims);
     CellPlan cp;
     memset(&cp, 0, sizeof(cp));
@@ -424,7 +467,7 @@ pt_status pt_launch_descriptor_cells_batch(int ndims, int nchroma, const PtBatch
     cp.to_bin = to_bin;
     cp.table = table;
     cp.tcand = tcand;
-    return launch_descriptor_batch<true>(ndims, nchroma, cp, imgs, n, ntiles, rgb, convert, rgba, nullptr, 0, st);
+    return launch_descriptor_batch<true>(ndims, nchroma, cp, imgs, n, ntiles, rgb, convert, rgba, nullptr, 0, work, st);
 }
 
 namespace {

@@ -37,9 +37,9 @@ __global__ void k_gather_rows(const float *__restrict__ desc, int ds, int nd, co
     out[t] = desc[(size_t) rows[i] * ds + d];
 }
 
-/* Validity bits of each query's sorted neighbour list and m = the smallest knn0 * 2^j whose
-   prefix holds `kc` valid neighbours (0 when the list of Kc entries is too short). */
-__global__ void k_kc_valid(const int *__restrict__ nbr, int Kc, int Q, const int *__restrict__ qpos,
+/* Validity bits of each query's sorted neighbour list (Kc entries per query) and m = the smallest
+   knn0 * 2^j <= klim whose prefix holds `kc` valid neighbours (0 when none does). */
+__global__ void k_kc_valid(const int *__restrict__ nbr, int Kc, int klim, int Q, const int *__restrict__ qpos,
                            const int *__restrict__ tpos, int min_dist2, int kc, int knn0,
                            unsigned long long *valid, int *m_out) {
     int q = blockIdx.x * 256 + threadIdx.x;
@@ -53,7 +53,7 @@ __global__ void k_kc_valid(const int *__restrict__ nbr, int Kc, int Q, const int
     }
     valid[q] = bits;
     int m = 0;
-    for (int k = knn0; k <= Kc; k *= 2) {
+    for (int k = knn0; k <= klim; k *= 2) {
         unsigned long long mask = k >= 64 ? ~0ull : ((1ull << k) - 1);
         if (__popcll(bits & mask) >= kc) { m = k; break; }
     }
@@ -311,12 +311,26 @@ pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *bdesc, int ds
                         int kc, int min_dist, int2 *kcoh, int *max_knn_out, cudaStream_t st) {
     if (kc < 1 || kc >= 32) return pt_fail(PT_UNSUPPORTED, "kcoherence must be in 1..31");
     int knn0 = kc + 1;
-    int Kc = 16;
-    while (Kc < 2 * knn0) Kc *= 2;
+    int Kcap = 16;
+    while (Kcap < 2 * knn0) Kcap *= 2;
     for (;;) {
-        if (Kc > PT_KNN_WIDE_MAX)
+        if (Kcap > PT_KNN_WIDE_MAX)
             return pt_fail(PT_UNSUPPORTED, "k-coherence needs more than %d neighbours for some patch", PT_KNN_WIDE_MAX);
-        const bool wide = Kc > 64;
+        const bool wide = Kcap > 64;
+        /* The knn chain only takes the values knn0 * 2^j: with a capacity of Kcap neighbours the
+           longest list any patch can use is klim, the largest of them within Kcap, so the search
+           asks for the smallest supported width Kc >= klim (fewer neighbours to keep sorted and a
+           tighter pruning bound); the first klim entries are the same as in a wider search. */
+        int klim = knn0;
+        while (2 * klim <= Kcap) klim *= 2;
+        int Kc = Kcap;
+        if (!wide) {
+            static const int widths[] = {12, 16, 24, 32, 48, 64};
+            for (int wv : widths)
+                if (wv >= klim) { Kc = wv; break; }
+        } else {
+            klim = Kcap;
+        }
         const int W = wide ? Kc / 64 : 1;
         if (Kc > N) return pt_fail(PT_BAD_ARG, "k-coherence: image has too few patches (%d)", N);
         DevBuf<int> nbr, mm, knn, ovf;
@@ -333,15 +347,16 @@ pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *bdesc, int ds
             k_kc_valid_wide<<<(Q + 255) / 256, 256, 0, st>>>(nbr.p, Kc, Q, qpos, tpos, min_dist * min_dist, kc, knn0, valid.p,
                                                              mm.p);
         else
-            k_kc_valid<<<(Q + 255) / 256, 256, 0, st>>>(nbr.p, Kc, Q, qpos, tpos, min_dist * min_dist, kc, knn0, valid.p, mm.p);
+            k_kc_valid<<<(Q + 255) / 256, 256, 0, st>>>(nbr.p, Kc, klim, Q, qpos, tpos, min_dist * min_dist, kc, knn0,
+                                                        valid.p, mm.p);
         PT_LAUNCHED();
         PT_CUDA(cudaMemsetAsync(ovf.p, 0, sizeof(int), st));
-        k_kc_chain<<<(nseg + 255) / 256, 256, 0, st>>>(seg_start, nseg, Q, mm.p, knn0, Kc, knn.p, ovf.p);
+        k_kc_chain<<<(nseg + 255) / 256, 256, 0, st>>>(seg_start, nseg, Q, mm.p, knn0, klim, knn.p, ovf.p);
         PT_LAUNCHED();
         int overflow = 0;
         PT_CUDA(cudaMemcpyAsync(&overflow, ovf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         PT_CUDA(cudaStreamSynchronize(st));
-        if (overflow) { Kc *= 2; continue; }
+        if (overflow) { Kcap *= 2; continue; }
         long long tot = (long long) Q * Kc;
         if (bdesc)
             k_kc_desc<<<(unsigned) ((tot + 255) / 256), 256, 0, st>>>(reinterpret_cast<const float4 *>(bdesc), ds / 4, nd, ew,
@@ -376,7 +391,7 @@ pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *bdesc, int ds
         pt_count_launches(1);
         k_kc_finish<<<(nseg + 255) / 256, 256, 0, st>>>(seg_start, nseg, Q, kc, pre.p, o0.p, o1.p, qcell, kcoh);
         PT_LAUNCHED();
-        if (max_knn_out) *max_knn_out = Kc;
+        if (max_knn_out) *max_knn_out = klim;
         PT_CUDA(cudaStreamSynchronize(st));
         return PT_OK;
     }

@@ -311,8 +311,8 @@ k_knn_wide(const float *__restrict__ sp, const int *__restrict__ sidx, int N, in
 
 }  // namespace
 
-/* Exact top-K (K in {16, 32, 64}, or a power of two up to PT_KNN_WIDE_MAX) train indices of every
-   query, ascending (dist, index). */
+/* Exact top-K (K in {12, 16, 24, 32, 48, 64}, or a power of two up to PT_KNN_WIDE_MAX) train
+   indices of every query, ascending (dist, index). */
 pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, int Q, int K, int *out, cudaStream_t st) {
     if (N < 1 || Q < 1) return PT_OK;
     if (nd < 1 || nd > PT_DESC_MAX) return pt_fail(PT_UNSUPPORTED, "knn: %d dims", nd);
@@ -384,12 +384,12 @@ pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, i
         PT_CUDA(cudaStreamSynchronize(st));
         return PT_OK;
     }
+#define PT_KNN_K(KK) case KK: k_knn_warp<KK><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
     switch (K) {
-        case 16: k_knn_warp<16><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
-        case 32: k_knn_warp<32><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
-        case 64: k_knn_warp<64><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
+        PT_KNN_K(12) PT_KNN_K(16) PT_KNN_K(24) PT_KNN_K(32) PT_KNN_K(48) PT_KNN_K(64)
         default: return pt_fail(PT_UNSUPPORTED, "knn K=%d", K);
     }
+#undef PT_KNN_K
     PT_LAUNCHED();
     PT_CUDA(cudaStreamSynchronize(st));
     return PT_OK;

@@ -40,7 +40,8 @@ struct QPlan {
     int pull_max;            /* most neighbour candidates scored per patch */
     int tile;                /* query patches per CTA (single-image launches) */
     int row0, rows;          /* patch rows of a single-image launch */
-    const float4 *b1;        /* b shifted by one pixel: b1[i] = b[i + 1] */
+    const float *bq;         /* b as packed RGB in eight copies, copy k shifted by k pixels */
+    size_t bq_stride;        /* floats from one copy to the next */
     const int *allowed;      /* b patches that may be matched (allowed[p] == allowed_index), or NULL */
     int allowed_index;
     const float4 *adesc;     /* descriptor mode: query descriptor store (ds4 float4 per patch), or NULL */
@@ -92,43 +93,40 @@ __device__ __forceinline__ void stage_a(float4 *atile, const float4 *__restrict_
 /* Shared-memory bytes of a staged query tile of TW patches. */
 constexpr size_t atile_bytes(int TW) { return sizeof(float) * 3 * 8 * (TW + 7); }
 
-/* Query row dy of the patch at tile column tx. */
+/* Query row dy of the patch at tile column tx: its 24 interleaved RGB floats. */
 template<int TW>
-__device__ __forceinline__ void load_arow(const float4 *atile, int dy, int tx, float4 (&av)[8]) {
+__device__ __forceinline__ void load_arow(const float4 *atile, int dy, int tx, float (&av)[24]) {
     const float *at = reinterpret_cast<const float *>(atile) + 3 * (dy * (TW + 7) + tx);
 #pragma unroll
-    for (int p = 0; p < 8; p++) av[p] = make_float4(at[3 * p], at[3 * p + 1], at[3 * p + 2], 0.f);
+    for (int e = 0; e < 24; e++) av[e] = at[e];
 }
 
-/* One 32-byte read-only load: pixels p[0], p[1]. */
-__device__ __forceinline__ void ld_px2(const float4 *p, float4 &u, float4 &v) {
+/* One 32-byte read-only load: 8 floats. */
+__device__ __forceinline__ void ld_f8(const float *p, float *v) {
     asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-        : "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w), "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
         : "l"(p));
 }
 
-/* The 8 pixels (x..x+7, y) of b with four 32-byte loads: pixel index i = y*bw + x is read from b
-   when even and from the shifted copy b1 (b1[i-1] = b[i]) when odd, so every load starts on a
-   32-byte boundary (both arrays are 256-byte aligned). */
-__device__ __forceinline__ void load_brow(const QPlan &q, const float4 *__restrict__ B, int x, int y, float4 (&bv)[8]) {
+/* The 8 pixels (x..x+7, y) of b as 24 interleaved RGB floats, with three 32-byte loads.  The
+   table keeps b as packed RGB in eight copies, copy k shifted by k pixels (bq[k * stride + m] =
+   rgb[3 * k + m]); the row starting at pixel index i = y * bw + x is read from copy i & 7 at float
+   3 * (i - (i & 7)), which is 32-byte aligned, so a row is exactly three sectors. */
+__device__ __forceinline__ void load_brow(const QPlan &q, int x, int y, float (&bv)[24]) {
     const size_t i = (size_t) y * q.bw + x;
-    const float4 *src = (i & 1) ? q.b1 + (i - 1) : B + i;
+    const size_t k = i & 7;
+    const float *src = q.bq + k * q.bq_stride + 3 * (i - k);
 #pragma unroll
-    for (int j = 0; j < 4; j++) ld_px2(src + 2 * j, bv[2 * j], bv[2 * j + 1]);
+    for (int j = 0; j < 3; j++) ld_f8(src + 8 * j, bv + 8 * j);
 }
 
 /* Adds one patch row to the four SSE-lane sums of patch_dist_exact (patchtable.h:349-356): the
-   interleaved RGB float e = 3p + c goes to lane e & 3, in increasing e per lane. */
-__device__ __forceinline__ void row_lanes(const float4 (&av)[8], const float4 (&bv)[8], float (&l)[4]) {
+   interleaved RGB float e goes to lane e & 3, in increasing e per lane. */
+__device__ __forceinline__ void row_lanes(const float (&av)[24], const float (&bv)[24], float (&l)[4]) {
 #pragma unroll
-    for (int p = 0; p < 8; p++) {
-        const float t0 = __fsub_rn(av[p].x, bv[p].x), t1 = __fsub_rn(av[p].y, bv[p].y), t2 = __fsub_rn(av[p].z, bv[p].z);
-        const float qd[3] = {__fmul_rn(t0, t0), __fmul_rn(t1, t1), __fmul_rn(t2, t2)};
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const int e = (3 * p + c) & 3;
-            l[e] = __fadd_rn(l[e], qd[c]);
-        }
+    for (int e = 0; e < 24; e++) {
+        const float t = __fsub_rn(av[e], bv[e]);
+        l[e & 3] = __fadd_rn(l[e & 3], __fmul_rn(t, t));
     }
 }
 
@@ -141,12 +139,13 @@ __device__ __forceinline__ float lane_total(const float (&l)[4]) {
 template<int TW>
 __device__ __forceinline__ float ssd_tile(const float4 *atile, int tx, const QPlan &q, const float4 *__restrict__ B,
                                           int bx, int by, float bound, unsigned &rows) {
+    (void) B;
     float l[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
     for (int dy = 0; dy < 8; dy++) {
         rows++;
-        float4 av[8], bv[8];
-        load_brow(q, B, bx, by + dy, bv);
+        float av[24], bv[24];
+        load_brow(q, bx, by + dy, bv);
         load_arow<TW>(atile, dy, tx, av);
         row_lanes(av, bv, l);
         if (dy < 7 && lane_total(l) >= bound) return finf();
@@ -172,14 +171,14 @@ __device__ __forceinline__ void ssd_group(const float4 *atile, int tx, const QPl
 #pragma unroll
         for (int g = 0; g < G; g++) any |= live[g];
         if (!any) break;
-        float4 av[8];
+        float av[24];
         load_arow<TW>(atile, dy, tx, av);
 #pragma unroll
         for (int g = 0; g < G; g++) {
             if (!live[g]) continue;
             rows++;
-            float4 bv[8];
-            load_brow(q, B, pt_x(cand[g]), pt_y(cand[g]) + dy, bv);
+            float bv[24];
+            load_brow(q, pt_x(cand[g]), pt_y(cand[g]) + dy, bv);
             row_lanes(av, bv, l[g]);
             if (dy < 7 && lane_total(l[g]) >= bound) live[g] = false;
         }
@@ -566,17 +565,29 @@ __device__ __forceinline__ int owner(const PtBatchImage *__restrict__ imgs, int 
     return lo;
 }
 
-/* Persistent choose over every row segment of every image: CTA b takes segments b, b + grid, ... */
+/* The next row segment for this CTA from the launch's work counter (zeroed before the launch):
+   segments go out in order, one at a time, to whichever CTA is free, so uneven segment costs
+   cannot leave some CTAs with a longer share. */
+__device__ __forceinline__ long long next_segment(unsigned long long *work) {
+    __shared__ long long s_next;
+    __syncthreads();                           /* the previous segment is done with s_next and atile */
+    if (threadIdx.x == 0) s_next = (long long) atomicAdd(work, 1ull);
+    __syncthreads();
+    return s_next;
+}
+
+/* Persistent choose over every row segment of every image, handed out by a work counter. */
 template<int TW>
 __global__ void __launch_bounds__(TW, (12 * 64) / TW)
 k_choose_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, long long nseg, int twi,
                const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
                const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
-               int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters) {
+               int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters,
+               unsigned long long *work) {
     extern __shared__ float4 atile[];
     LearnedArgs none;
     none.cand = nullptr; none.conf = nullptr; none.threshold = 0.f; none.kcoh_confident = 0; none.counters = nullptr;
-    for (long long s = blockIdx.x; s < nseg; s += gridDim.x) {
+    for (long long s = next_segment(work); s < nseg; s = next_segment(work)) {
         const int i = owner(imgs, n, s, twi);
         const PtBatchImage &g = imgs[i];
         const long long ls = s - g.seg_off[twi];
@@ -588,7 +599,6 @@ k_choose_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, l
         choose_seg<TW, false, false>(q, atile, a + g.pix_off, b, cur_pos ? cur_pos + o : nullptr, cur_d ? cur_d + o : nullptr,
                                      tcand + o, kcoh, do_table, ch_pos + o,
                               ch_d + o, kc_done + o, use_done, counters, none, x0, y);
-        __syncthreads();                       /* the next segment restages atile */
     }
 }
 
@@ -597,9 +607,9 @@ __global__ void __launch_bounds__(TW, (14 * 64) / TW)
 k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, long long nseg, int twi,
              const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
              const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
-             int *nxt_pos, float *nxt_d, unsigned long long *counters) {
+             int *nxt_pos, float *nxt_d, unsigned long long *counters, unsigned long long *work) {
     extern __shared__ float4 atile[];
-    for (long long s = blockIdx.x; s < nseg; s += gridDim.x) {
+    for (long long s = next_segment(work); s < nseg; s = next_segment(work)) {
         const int i = owner(imgs, n, s, twi);
         const PtBatchImage &g = imgs[i];
         const long long ls = s - g.seg_off[twi];
@@ -612,7 +622,6 @@ k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, lon
         pull_seg<TW, R, false>(q, atile, a + g.pix_off, b, cur_pos ? cur_pos + o : nullptr, cur_d ? cur_d + o : nullptr, ch_pos + o,
                                ch_d + o, nxt_pos + o, nxt_d + o,
                         counters, x0, y);
-        __syncthreads();
     }
 }
 
@@ -620,13 +629,17 @@ k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, lon
    reference's lane order, without an early exit. */
 __device__ __forceinline__ float ssd_global(const QPlan &q, const float4 *__restrict__ a, int ax, int ay,
                                            const float4 *__restrict__ B, int bx, int by) {
+    (void) B;
     float l[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
     for (int dy = 0; dy < 8; dy++) {
-        float4 av[8], bv[8];
-        load_brow(q, B, bx, by + dy, bv);
+        float av[24], bv[24];
+        load_brow(q, bx, by + dy, bv);
 #pragma unroll
-        for (int p = 0; p < 8; p++) av[p] = __ldg(a + (size_t) (ay + dy) * q.aw + ax + p);
+        for (int p = 0; p < 8; p++) {
+            const float4 v = __ldg(a + (size_t) (ay + dy) * q.aw + ax + p);
+            av[3 * p] = v.x; av[3 * p + 1] = v.y; av[3 * p + 2] = v.z;
+        }
         row_lanes(av, bv, l);
     }
     return lane_total(l);
@@ -739,7 +752,8 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
         return pt_fail(PT_BAD_ARG, "query rows [%d, %d) outside 0..%d", q.row0, q.row0 + q.rows, q.eh);
     if (q.tile != 32 && q.tile != 64 && q.tile != 128 && q.tile != 256)
         return pt_fail(PT_BAD_ARG, "gpu_tile %d: query patches per CTA must be 32, 64, 128 or 256", s.tile);
-    q.b1 = s.b1;
+    q.bq = s.bq;
+    q.bq_stride = s.bq_stride;
     q.allowed = s.allowed;
     q.allowed_index = s.allowed_index;
     q.adesc = reinterpret_cast<const float4 *>(s.adesc);
@@ -755,10 +769,19 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     if (q.adesc) {
         if (!q.bdesc || (s.ds != 8 && s.ds != 16) || q.nd < 3 || q.nd > s.ds)
             return pt_fail(PT_BAD_ARG, "descriptor query: store of %d floats for %d dimensions", s.ds, q.nd);
-    } else if (!q.b1) {
-        return pt_fail(PT_BAD_ARG, "query without the shifted copy of the table image");
+    } else if (!q.bq) {
+        return pt_fail(PT_BAD_ARG, "query without the packed copies of the table image");
     }
     if (q.radius > 2) return pt_fail(PT_UNSUPPORTED, "propagation radius %d > 2 on the GPU path", q.radius);
+    return PT_OK;
+}
+
+pt_status pt_make_bq(const float *rgb, int h, int w, float *bq, cudaStream_t st) {
+    const size_t n = (size_t) h * w * 3, stride = pt_bq_stride(h, w);
+    PT_CUDA(cudaMemsetAsync(bq, 0, sizeof(float) * stride * PT_BQ_COPIES, st));
+    for (int k = 0; k < PT_BQ_COPIES; k++)
+        if (n > (size_t) (3 * k))
+            PT_CUDA(cudaMemcpyAsync(bq + k * stride, rgb + 3 * k, sizeof(float) * (n - 3 * k), cudaMemcpyDeviceToDevice, st));
     return PT_OK;
 }
 
@@ -891,14 +914,15 @@ int pt_batch_tw(int twi) { return (twi >= 0 && twi < PT_BATCH_NTW) ? BATCH_TW[tw
 pt_status pt_launch_choose_batch(const QuerySetup &s, const PtBatchImage *imgs, int n, long long nseg, int twi,
                                  const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
                                  const int *tcand, const int2 *kcoh, int do_table, int *ch_pos, float *ch_d, int *kc_done,
-                                 int use_done, unsigned long long *evals, cudaStream_t st) {
+                                 int use_done, unsigned long long *evals, unsigned long long *work, cudaStream_t st) {
     QPlan q;
     PT_TRY(make_qplan(s, q));
     if (nseg <= 0) return PT_OK;
+    PT_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st));
 #define PT_CHOOSE_B(T) { const size_t sm = atile_bytes(T); \
         const int g = persistent_grid(k_choose_batch<T>, T, sm, nseg); \
         k_choose_batch<T><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, \
-                                            kc_done, use_done, evals); }
+                                            kc_done, use_done, evals, work); }
     switch (BATCH_TW[twi]) {
         case 32: PT_CHOOSE_B(32) break;
         case 64: PT_CHOOSE_B(64) break;
@@ -912,13 +936,16 @@ pt_status pt_launch_choose_batch(const QuerySetup &s, const PtBatchImage *imgs, 
 
 pt_status pt_launch_pull_batch(const QuerySetup &s, const PtBatchImage *imgs, int n, long long nseg, int twi,
                                const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d, const int *ch_pos,
-                               const float *ch_d, int *nxt_pos, float *nxt_d, unsigned long long *evals, cudaStream_t st) {
+                               const float *ch_d, int *nxt_pos, float *nxt_d, unsigned long long *evals,
+                               unsigned long long *work, cudaStream_t st) {
     QPlan q;
     PT_TRY(make_qplan(s, q));
     if (nseg <= 0) return PT_OK;
+    PT_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st));
 #define PT_PULL_B(T, RR) { const size_t sm = atile_bytes(T); \
         const int g = persistent_grid(k_pull_batch<T, RR>, T, sm, nseg); \
-        k_pull_batch<T, RR><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals); }
+        k_pull_batch<T, RR><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals, \
+                                              work); }
     const bool r1 = q.radius <= 1;
     switch (BATCH_TW[twi]) {
         case 32: if (r1) PT_PULL_B(32, 1) else PT_PULL_B(32, 2) break;

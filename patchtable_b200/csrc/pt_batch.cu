@@ -5,9 +5,10 @@
    NNF -- and runs every phase of the query once for all of them: one descriptor launch over the
    flattened list of 64 x 8 descriptor tiles that also looks each patch's cell up in the table,
    and per propagation pass one choose and one pull launch over the flattened list of row segments
-   (the first pass starts from the initial field, the last pull writes the NNF).  The choose / pull / descriptor launches are persistent (as many
-   CTAs as fit on the GPU, each walking the list); each CTA finds the image that owns its segment by
-   binary search over per-image prefix counts.  Every patch is computed exactly as the
+   (the first pass starts from the initial field, the last pull writes the NNF).  The choose /
+   pull / descriptor launches are persistent (as many CTAs as fit on the GPU); a work counter per
+   launch hands the segments out one at a time to whichever CTA is free, and each CTA finds the
+   image that owns its segment by binary search over per-image prefix counts.  Every patch is computed exactly as the
    single-image query computes it, so each image's NNF equals its own pt_table_lookup_device
    result.
 
@@ -32,6 +33,7 @@ struct pt_batch {
     DevBuf<float4> rgba;
     DevBuf<int> tcand, pos[2], chpos, kcdone;
     DevBuf<float> dd[2], chd;
+    DevBuf<unsigned long long> work;      /* work counters of the persistent launches */
     cudaStream_t cap_stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -54,7 +56,7 @@ pt_status run(pt_batch *B, const float *d_rgb, double *d_ann, cudaStream_t st) {
     (void) ds;
     /* descriptors are needed only for the table step: one fused pass writes the table entries */
     PT_TRY(pt_launch_descriptor_cells_batch(p.ndims, p.nchroma, B->d_imgs.p, B->n, B->ntiles, d_rgb, pt_color_mode(p),
-                                            B->rgba.p, v.bins, v.to_bin, v.table, B->tcand.p, st));
+                                            B->rgba.p, v.bins, v.to_bin, v.table, B->tcand.p, B->work.p, st));
     QuerySetup qs;
     qs.aw = 0; qs.ah = 0; qs.bw = v.w; qs.bh = v.h;
     qs.prop_scale = 1.0 / (1 + p.coherence_spatial);
@@ -64,7 +66,8 @@ pt_status run(pt_batch *B, const float *d_rgb, double *d_ann, cudaStream_t st) {
     qs.spatial = p.spatial;
     qs.do_rs = p.do_rs;
     qs.radius = std::min(2, p.query_step + p.prop_dist);
-    qs.b1 = v.b_rgba1;
+    qs.bq = v.bq;
+    qs.bq_stride = v.bq_stride;
     qs.pull_max = p.gpu_pull_max;
     qs.allowed = v.allowed;
     qs.allowed_index = p.allowed_index;
@@ -84,14 +87,14 @@ pt_status run(pt_batch *B, const float *d_rgb, double *d_ann, cudaStream_t st) {
         const int use_done = i > 0 && pt_pass_kcoh(p, i - 1, passes);
         PT_TRY(pt_launch_choose_batch(qi, B->d_imgs.p, B->n, B->nseg[B->twi], B->twi, B->rgba.p, v.b_rgba,
                                       i == 0 ? nullptr : B->pos[cur].p, i == 0 ? nullptr : B->dd[cur].p, B->tcand.p, v.kcoh,
-                                      do_table, B->chpos.p, B->chd.p, B->kcdone.p, use_done, nullptr, st));
+                                      do_table, B->chpos.p, B->chd.p, B->kcdone.p, use_done, nullptr, B->work.p + 1, st));
         if (p.do_prop) {
             QuerySetup qp = qs;
             qp.step = pt_pass_step(i, passes, jump);
             if (i == passes - 1 && direct_out) qp.ann = d_ann;
             PT_TRY(pt_launch_pull_batch(qp, B->d_imgs.p, B->n, B->nseg[B->twi], B->twi, B->rgba.p, v.b_rgba,
                                         i == 0 ? nullptr : B->pos[cur].p, i == 0 ? nullptr : B->dd[cur].p, B->chpos.p, B->chd.p,
-                                        B->pos[1 - cur].p, B->dd[1 - cur].p, nullptr, st));
+                                        B->pos[1 - cur].p, B->dd[1 - cur].p, nullptr, B->work.p + 2, st));
             cur = 1 - cur;
         } else {
             PT_CUDA(cudaMemcpyAsync(B->pos[cur].p, B->chpos.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
@@ -148,7 +151,7 @@ pt_status pt_batch_create(pt_table *t, int n, const int *h, const int *w, pt_bat
     auto fail = [&](pt_status s) { delete B; return s; };
     if (B->d_imgs.reserve(n) || B->rgba.reserve(pix) || B->tcand.reserve(pat) ||
         B->pos[0].reserve(pat) || B->pos[1].reserve(pat) || B->dd[0].reserve(pat) || B->dd[1].reserve(pat) ||
-        B->chpos.reserve(pat) || B->chd.reserve(pat) || B->kcdone.reserve(pat))
+        B->chpos.reserve(pat) || B->chd.reserve(pat) || B->kcdone.reserve(pat) || B->work.reserve(3))
         return fail(pt_fail(PT_OOM, "batch buffers for %lld pixels / %lld patches", pix, pat));
     if (cudaMemcpy(B->d_imgs.p, B->imgs.data(), sizeof(PtBatchImage) * n, cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(pt_fail(PT_CUDA_ERR, "batch geometry upload"));

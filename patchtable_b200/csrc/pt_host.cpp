@@ -7,7 +7,10 @@
    float64 field would (8 instead of 24 per patch); the conversion is exact (positions are
    integers below 2^16, a float distance is a double exactly).  The widening of one band of rows
    runs while the GPU still computes and sends the following bands. */
+#include <emmintrin.h>
+
 #include <algorithm>
+#include <cstdint>
 #include <condition_variable>
 #include <functional>
 #include <mutex>
@@ -85,6 +88,7 @@ private:
 
 std::mutex g_pool_mu;
 int g_threads = 0;                 /* 0: not chosen yet */
+bool g_widen = true;               /* false: the GPU writes float64 records and they are copied */
 Pool *g_pool = nullptr;
 
 int default_threads() {
@@ -101,26 +105,51 @@ Pool &pool() {
 
 }  // namespace
 
+bool pt_host_widen() {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    return g_widen;
+}
+
+/* Records [i0, i1) of the packed field as float64 triples.  Pairs of patches (48 bytes) go out as
+   three 16-byte streaming stores when the destination is 16-byte aligned, so the output lines are
+   written without first being read into the cache. */
+static void widen_range(const int *pos, const float *dist, long long i0, long long i1, double *ann) {
+    long long i = i0;
+    auto one = [&](long long k) {
+        const int v = pos[k];
+        double *o = ann + 3 * k;
+        o[0] = pt_x(v);
+        o[1] = pt_y(v);
+        o[2] = dist[k];
+    };
+    if (i < i1 && (((uintptr_t) (ann + 3 * i)) & 15)) one(i++);
+    for (; i + 2 <= i1; i += 2) {
+        const int v0 = pos[i], v1 = pos[i + 1];
+        double *o = ann + 3 * i;
+        _mm_stream_pd(o, _mm_set_pd((double) pt_y(v0), (double) pt_x(v0)));
+        _mm_stream_pd(o + 2, _mm_set_pd((double) pt_x(v1), (double) dist[i]));
+        _mm_stream_pd(o + 4, _mm_set_pd((double) dist[i + 1], (double) pt_y(v1)));
+    }
+    if (i < i1) one(i);
+    _mm_sfence();
+}
+
 void pt_expand_nnf(const int *pos, const float *dist, long long n, double *ann) {
     if (n <= 0) return;
     Pool &pl = pool();
     const int parts = (int) std::min<long long>(pl.size() + 1, std::max<long long>(1, n / 4096));
-    const long long per = (n + parts - 1) / parts;
+    long long per = (n + parts - 1) / parts;
+    per = (per + 1) & ~1ll;                 /* even: a part's pairs keep the alignment of the whole */
     pl.run(parts, [&](int k) {
-        const long long i0 = k * per, i1 = std::min(n, i0 + per);
-        for (long long i = i0; i < i1; i++) {
-            const int v = pos[i];
-            double *o = ann + 3 * i;
-            o[0] = pt_x(v);
-            o[1] = pt_y(v);
-            o[2] = dist[i];
-        }
+        const long long i0 = std::min(n, k * per), i1 = std::min(n, i0 + per);
+        widen_range(pos, dist, i0, i1, ann);
     });
 }
 
 extern "C" int pt_set_host_threads(int n) {
     std::lock_guard<std::mutex> g(g_pool_mu);
-    const int old = g_threads ? g_threads : default_threads();
+    const int old = !g_widen ? -1 : (g_threads ? g_threads : default_threads());
+    g_widen = n >= 0;
     const int want = n > 0 ? std::min(n, 256) : default_threads();
     if (want != g_threads) {
         delete g_pool;          /* joins the old workers */

@@ -107,3 +107,5 @@ template<class T> struct PinnedBuf {
 /* pt_host.cpp: ann[3i .. 3i+2] = (x, y, dist) of pos[i] / dist[i] for i < n, in float64, split
    across the library's host threads (pt_set_host_threads). */
 void pt_expand_nnf(const int *pos, const float *dist, long long n, double *ann);
+/* false when pt_set_host_threads(n < 0) asked for float64 records written on the GPU instead. */
+bool pt_host_widen();

@@ -87,6 +87,11 @@ pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *bdesc, int ds
                         int kc, int min_dist, int2 *kcoh, int *max_knn_out, cudaStream_t st);
 
 /* k_query.cu */
+#define PT_BQ_COPIES 8
+/* Floats from one packed copy of an h x w table image to the next (256-byte aligned). */
+inline size_t pt_bq_stride(int h, int w) { return ((size_t) h * w * 3 + 63) / 64 * 64; }
+/* Fills the PT_BQ_COPIES shifted packed copies from the device RGB image (k_query.cu). */
+pt_status pt_make_bq(const float *rgb, int h, int w, float *bq, cudaStream_t st);
 struct QuerySetup {
     int aw, ah, bw, bh;
     double prop_scale, triangle_factor;
@@ -95,7 +100,11 @@ struct QuerySetup {
     int pull_max = 0;        /* most neighbour candidates a pull scores per patch (0 = all) */
     int tile = 0;            /* query patches per CTA in choose / pull: 32, 64, 128, 256 (0 = 32) */
     int row0 = 0, rows = 0;  /* patch rows [row0, row0 + rows) of a single-image launch (rows 0 = all) */
-    const float4 *b1 = nullptr;   /* the table image shifted by one pixel, b1[i] = b[i + 1] */
+    /* the table image as packed RGB in PT_BQ_COPIES copies, copy k shifted by k pixels
+       (bq[k * bq_stride + m] = rgb[3 * k + m]): every 8-pixel patch row is one 96-byte,
+       32-byte-aligned read from copy (pixel index & 7) */
+    const float *bq = nullptr;
+    size_t bq_stride = 0;
     const int *allowed = nullptr; /* b patches a match may use (allowed[p] == allowed_index), or NULL */
     int allowed_index = 0;
     /* Descriptor mode (is_descriptor): distances are patch_dist_approx between the query's and the
@@ -175,7 +184,7 @@ pt_status pt_launch_output_temporal(int n, const int *pos, const float *d, const
 
 /* Batched queries (pt_batch.cu): the images of a batch are concatenated -- pixels, patches and
    query state -- and every phase is one persistent launch over the flattened list of row
-   segments.  seg_off[t] is the image's first segment when a CTA covers PT_BATCH_TW(t) patches. */
+   segments, handed out one at a time through a work counter (`work`, zeroed by the launcher).  seg_off[t] is the image's first segment when a CTA covers PT_BATCH_TW(t) patches. */
 #define PT_BATCH_NTW 4
 struct PtBatchImage {
     int h, w, eh, ew;
@@ -187,22 +196,24 @@ int pt_batch_tw(int twi);
 pt_status pt_launch_choose_batch(const QuerySetup &s, const PtBatchImage *imgs, int n, long long nseg, int twi,
                                  const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
                                  const int *tcand, const int2 *kcoh, int do_table, int *ch_pos, float *ch_d, int *kc_done,
-                                 int use_done, unsigned long long *evals, cudaStream_t st);
+                                 int use_done, unsigned long long *evals, unsigned long long *work, cudaStream_t st);
 pt_status pt_launch_pull_batch(const QuerySetup &s, const PtBatchImage *imgs, int n, long long nseg, int twi,
                                const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d, const int *ch_pos,
-                               const float *ch_d, int *nxt_pos, float *nxt_d, unsigned long long *evals, cudaStream_t st);
+                               const float *ch_d, int *nxt_pos, float *nxt_d, unsigned long long *evals,
+                               unsigned long long *work, cudaStream_t st);
 /* The batch's descriptor pass fused with the table step: tcand[p] = table[cell(p)] for every
    patch of every image, no descriptors stored. */
 pt_status pt_launch_descriptor_cells_batch(int ndims, int nchroma, const PtBatchImage *imgs, int n, long long ntiles,
                                            const float *rgb, int convert, float4 *rgba, const PtBins &bins, const int *to_bin,
-                                           const int *table, int *tcand, cudaStream_t st);
+                                           const int *table, int *tcand, unsigned long long *work, cudaStream_t st);
 
 /* Read-only view of a built table, for entry points outside pt_table.cu. */
 struct PtTableView {
     pt_params p;
     int h, w, ds;
     const float4 *b_rgba;
-    const float4 *b_rgba1;               /* b_rgba shifted by one pixel (32-byte aligned row loads) */
+    const float *bq;                     /* packed RGB copies of b (QuerySetup::bq) */
+    size_t bq_stride;
     const int *table;
     const int *to_bin;
     const int2 *kcoh;

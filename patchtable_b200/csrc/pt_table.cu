@@ -100,8 +100,8 @@ extern "C" int64_t pt_device_bytes_in_use(void) { return g_alloc_live.load(); }
    bytewise; zero-filled before use). */
 struct BandKey {
     pt_params p;
-    int h, w, B;
-    const void *bufs[10];
+    int h, w, B, widen;
+    const void *bufs[12];
 };
 
 struct pt_table {
@@ -119,7 +119,7 @@ struct pt_table {
     cudaStream_t st = nullptr;
     bool own_stream = false;
     DevBuf<float4> b_rgba;
-    DevBuf<float4> b_rgba1;           /* b_rgba shifted by one pixel, b_rgba1[i] = b_rgba[i + 1] */
+    DevBuf<float> b_bq;               /* b as packed RGB, PT_BQ_COPIES copies shifted by 0..7 pixels */
     DevBuf<float> b_desc;
     DevBuf<int> allowed;
     std::vector<int> nslices;
@@ -451,12 +451,10 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
                         packed[((size_t) y * t->ew + x) * t->ds + d] = wh0[((size_t) (y + 7) * (w + 7) + (x + 7)) * t->nd + d];
             PT_CUDA(cudaMemcpyAsync(t->b_desc.p, packed.data(), sizeof(float) * packed.size(), cudaMemcpyHostToDevice, t->st));
         }
-        /* The query reads b patch rows with 32-byte loads: from b_rgba at even pixel indices and
-           from this one-pixel-shifted copy at odd ones, so every load is 32-byte aligned. */
-        const size_t npx = (size_t) h * w;
-        PT_CUDA(t->b_rgba1.reserve(npx));
-        PT_CUDA(cudaMemsetAsync(t->b_rgba1.p, 0, sizeof(float4) * npx, t->st));
-        PT_CUDA(cudaMemcpyAsync(t->b_rgba1.p, t->b_rgba.p + 1, sizeof(float4) * (npx - 1), cudaMemcpyDeviceToDevice, t->st));
+        /* The query reads a b patch row as 24 packed floats from one of eight shifted copies, so
+           every row is one 32-byte-aligned 96-byte read (k_query.cu load_brow). */
+        PT_CUDA(t->b_bq.reserve(pt_bq_stride(h, w) * PT_BQ_COPIES));
+        PT_TRY(pt_make_bq(rgb.p, h, w, t->b_bq.p, t->st));
         PT_CUDA(cudaStreamSynchronize(t->st));
     }
     std::vector<int> allowed_h;
@@ -667,7 +665,8 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     qs.spatial = p.spatial;
     qs.do_rs = p.do_rs;
     qs.radius = p.query_step + p.prop_dist;
-    qs.b1 = t->b_rgba1.p;
+    qs.bq = t->b_bq.p;
+    qs.bq_stride = pt_bq_stride(t->h, t->w);
     qs.pull_max = p.gpu_pull_max;
     qs.tile = p.gpu_tile;
     qs.allowed = t->allowed.p;
@@ -807,7 +806,8 @@ int band_rows(const pt_table *t, int h, int w) {
 /* Enqueues the band pipeline on the table's streams, starting after the work queued on t->st and
    joining every stream back into t->st at the end.  ev_d[b] marks band b's download (while
    capturing, as an external event node, so that the replayed graph records it too). */
-pt_status enqueue_bands(pt_table *t, const float *a, int h, int w, int B, int nb, bool capturing) {
+pt_status enqueue_bands(pt_table *t, const float *a, double *ann_out, int h, int w, int B, int nb, bool capturing,
+                        bool widen) {
     const pt_params &p = t->p;
     const int eh = h - 7, ew = w - 7;
     const long long P = (long long) eh * ew;
@@ -825,7 +825,8 @@ pt_status enqueue_bands(pt_table *t, const float *a, int h, int w, int B, int nb
     qs.spatial = p.spatial;
     qs.do_rs = p.do_rs;
     qs.radius = std::min(2, p.query_step + p.prop_dist);
-    qs.b1 = t->b_rgba1.p;
+    qs.bq = t->b_bq.p;
+    qs.bq_stride = pt_bq_stride(t->h, t->w);
     qs.pull_max = p.gpu_pull_max;
     qs.tile = p.gpu_tile;
     qs.allowed = t->allowed.p;
@@ -862,15 +863,22 @@ pt_status enqueue_bands(pt_table *t, const float *a, int h, int w, int B, int nb
             qb.row0 = r0;
             qb.rows = r1 - r0;
             qb.stream = sc;
-            /* the pull writes the band's final field (packed position, float distance) */
+            /* the pull writes the band's final field: packed position and float distance, or
+               (without host widening) the float64 records */
+            if (!widen) qb.ann = t->q_ann.p;
             PT_TRY(pt_launch_pull(qb, (int) P, t->q_rgba.p, t->b_rgba.p, nullptr, nullptr, t->q_chpos.p, t->q_chd.p,
                                   t->q_pos[1].p, t->q_d[1].p, nullptr, sc));
             const size_t o = (size_t) r0 * ew;
             const size_t n = (size_t) (r1 - r0) * ew;
             PT_CUDA(cudaEventRecord(ev_c[b - 2], sc));
             PT_CUDA(cudaStreamWaitEvent(t->st_out, ev_c[b - 2], 0));
-            PT_CUDA(cudaMemcpyAsync(t->h_pos.p + o, t->q_pos[1].p + o, sizeof(int) * n, cudaMemcpyDeviceToHost, t->st_out));
-            PT_CUDA(cudaMemcpyAsync(t->h_d.p + o, t->q_d[1].p + o, sizeof(float) * n, cudaMemcpyDeviceToHost, t->st_out));
+            if (widen) {
+                PT_CUDA(cudaMemcpyAsync(t->h_pos.p + o, t->q_pos[1].p + o, sizeof(int) * n, cudaMemcpyDeviceToHost, t->st_out));
+                PT_CUDA(cudaMemcpyAsync(t->h_d.p + o, t->q_d[1].p + o, sizeof(float) * n, cudaMemcpyDeviceToHost, t->st_out));
+            } else {
+                PT_CUDA(cudaMemcpyAsync(ann_out + 3 * o, t->q_ann.p + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost,
+                                        t->st_out));
+            }
             if (capturing) PT_CUDA(cudaEventRecordWithFlags(ev_d[b - 2], t->st_out, cudaEventRecordExternal));
             else PT_CUDA(cudaEventRecord(ev_d[b - 2], t->st_out));
         }
@@ -884,13 +892,14 @@ pt_status enqueue_bands(pt_table *t, const float *a, int h, int w, int B, int nb
     return PT_OK;
 }
 
-BandKey band_key(const pt_table *t, int h, int w, int B) {
+BandKey band_key(const pt_table *t, int h, int w, int B, bool widen, const double *ann_out) {
     BandKey k;
     memset(&k, 0, sizeof(k));
     k.p = t->p;
-    k.h = h; k.w = w; k.B = B;
-    const void *b[10] = {t->q_rgb.p, t->q_rgba.p, t->q_tcand.p, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p,
-                         t->q_pos[1].p, t->q_d[1].p, t->h_pos.p, t->h_d.p};
+    k.h = h; k.w = w; k.B = B; k.widen = widen;
+    /* without widening the download nodes write the caller's buffer: part of the key */
+    const void *b[12] = {t->q_rgb.p, t->q_rgba.p, t->q_tcand.p, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p,
+                         t->q_pos[1].p, t->q_d[1].p, t->h_pos.p, t->h_d.p, t->q_ann.p, widen ? nullptr : ann_out};
     memcpy(k.bufs, b, sizeof(b));
     return k;
 }
@@ -910,24 +919,29 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
             t->band_ev.push_back(e);
         }
     }
-    PT_CUDA(t->h_pos.reserve(P));
-    PT_CUDA(t->h_d.reserve(P));
+    const bool widen = pt_host_widen();
+    if (widen) {
+        PT_CUDA(t->h_pos.reserve(P));
+        PT_CUDA(t->h_d.reserve(P));
+    } else {
+        PT_CUDA(t->q_ann.reserve((size_t) P * 3));
+    }
     cudaPointerAttributes attr;
     const bool pinned = cudaPointerGetAttributes(&attr, a) == cudaSuccess && attr.type == cudaMemoryTypeHost;
     cudaGetLastError();
-    const BandKey key = band_key(t, h, w, B);
+    const BandKey key = band_key(t, h, w, B, widen, ann_out);
     const bool same = t->band_seen && memcmp(&key, &t->band_key_v, sizeof(key)) == 0;
     if (!pinned || !same) {
         /* enqueue directly; a second call with the same key and a page-locked image records the graph */
         t->drop_band_graph();
-        PT_TRY(enqueue_bands(t, a, h, w, B, nb, false));
+        PT_TRY(enqueue_bands(t, a, ann_out, h, w, B, nb, false, widen));
         memcpy(&t->band_key_v, &key, sizeof(key));
         t->band_seen = pinned;
     } else {
         if (!t->band_exec) {
             cudaGraph_t g = nullptr;
             PT_CUDA(cudaStreamBeginCapture(t->st, cudaStreamCaptureModeThreadLocal));
-            pt_status s = enqueue_bands(t, a, h, w, B, nb, true);
+            pt_status s = enqueue_bands(t, a, ann_out, h, w, B, nb, true, widen);
             cudaError_t e = cudaStreamEndCapture(t->st, &g);
             if (s != PT_OK) { if (g) cudaGraphDestroy(g); return s; }
             if (e != cudaSuccess) return pt_fail(PT_CUDA_ERR, "capturing the banded lookup: %s", cudaGetErrorString(e));
@@ -962,10 +976,10 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
         pt_count_launches(3 * nb);
     }
     t->last_h2d = (long long) sizeof(float) * h * w * 3;
-    t->last_d2h = (long long) (sizeof(int) + sizeof(float)) * P;
+    t->last_d2h = (long long) (widen ? sizeof(int) + sizeof(float) : 3 * sizeof(double)) * P;
     /* widen each band as soon as it has arrived */
     cudaEvent_t *ev_d = t->band_ev.data() + 4 * nb;
-    for (int b = 0; b < nb; b++) {
+    for (int b = 0; b < nb && widen; b++) {
         PT_CUDA(cudaEventSynchronize(ev_d[b]));
         const int r0 = b * B, r1 = std::min(eh, r0 + B);
         const size_t o = (size_t) r0 * ew;
@@ -1177,10 +1191,8 @@ pt_status load_impl(const pt_params *pin, const char *filename, pt_table **out) 
                     packed[((size_t) y * t->ew + x) * t->ds + d] = wh0[((size_t) (y + 7) * (w + 7) + (x + 7)) * nd + d];
         PT_CUDA(t->b_desc.reserve(packed.size()));
         PT_CUDA(cudaMemcpyAsync(t->b_desc.p, packed.data(), sizeof(float) * packed.size(), cudaMemcpyHostToDevice, t->st));
-        const size_t npx = (size_t) h * w;
-        PT_CUDA(t->b_rgba1.reserve(npx));
-        PT_CUDA(cudaMemsetAsync(t->b_rgba1.p, 0, sizeof(float4) * npx, t->st));
-        PT_CUDA(cudaMemcpyAsync(t->b_rgba1.p, t->b_rgba.p + 1, sizeof(float4) * (npx - 1), cudaMemcpyDeviceToDevice, t->st));
+        PT_CUDA(t->b_bq.reserve(pt_bq_stride(h, w) * PT_BQ_COPIES));
+        PT_TRY(pt_make_bq(rgb.p, h, w, t->b_bq.p, t->st));
         PT_CUDA(cudaStreamSynchronize(t->st));
     }
     /* the file has no k-coherence set (the reference's load leaves it empty); it is rebuilt from
@@ -1533,7 +1545,8 @@ pt_status pt_table_view(const pt_table *t, PtTableView *v) {
     v->p = t->p;
     v->h = t->h; v->w = t->w; v->ds = t->ds;
     v->b_rgba = t->b_rgba.p;
-    v->b_rgba1 = t->b_rgba1.p;
+    v->bq = t->b_bq.p;
+    v->bq_stride = pt_bq_stride(t->h, t->w);
     v->table = t->table.p;
     v->to_bin = t->to_bin.p;
     v->kcoh = t->kcoh.p;
