@@ -305,6 +305,14 @@ pt_status pt_table_lookup_learned_device(pt_table *t, pt_proposal *net, const fl
 pt_status pt_table_lookup_learned_profile(pt_table *t, pt_proposal *net, const float *d_a, int h, int w,
                                           double *d_ann, void *stream, double *stage_ms, uint64_t *counters);
 
+/* Diagnostics: the learned query with proposals supplied by the caller instead of the network
+   (d_cand: P x PT_PROP_TOPK table entries, -1 = none; d_conf: P confidences; patches with
+   d_conf >= threshold use them), e.g. the plain method's own converged matches, which bounds what
+   any proposal network could gain.  Outputs as pt_table_lookup_learned_profile. */
+pt_status pt_table_lookup_proposed_profile(pt_table *t, const float *d_a, int h, int w, const int32_t *d_cand,
+                                           const float *d_conf, float threshold, int kcoh_confident, double *d_ann,
+                                           void *stream, double *stage_ms, uint64_t *counters);
+
 /* Diagnostics: number of breadth-first levels the last DT build ran. */
 int pt_table_dt_levels(const pt_table *t);
 

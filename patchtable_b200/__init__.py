@@ -147,6 +147,8 @@ def lib() -> C.CDLL:
     L.pt_batch_replay.argtypes = [vp, vp]
     L.pt_table_lookup_learned.argtypes = [vp, vp, _f32p, C.c_int, C.c_int, _f64p, C.POINTER(C.c_double)]
     L.pt_table_lookup_learned_device.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp, vp]
+    L.pt_table_lookup_proposed_profile.argtypes = [vp, vp, C.c_int, C.c_int, vp, vp, C.c_float, C.c_int, vp, vp,
+                                                   C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
     L.pt_table_lookup_learned_profile.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp, vp, C.POINTER(C.c_double),
                                                   C.POINTER(C.c_uint64)]
     L.pt_last_error.restype = C.c_char_p
@@ -408,6 +410,18 @@ class PatchTable:
         self._sync_params()
         _check(lib().pt_table_lookup_learned_profile(self._h, net.handle, C.c_void_p(a_ptr), h, w, C.c_void_p(ann_ptr),
                                                      C.c_void_p(stream), ms, ctr))
+        return dict(zip(self.LEARNED_STAGES, list(ms))), dict(choose_cand=ctr[0], choose_rows=ctr[1], pull_cand=ctr[2],
+                                                             pull_rows=ctr[3], confident=ctr[4], proposals=ctr[5])
+
+    def lookup_proposed_profile(self, a_ptr: int, h: int, w: int, cand_ptr: int, conf_ptr: int, threshold: float,
+                                ann_ptr: int, stream: int = 0, kcoh_confident: bool = False):
+        """The learned query with caller-supplied proposals (device P x 8 table entries, P confidences)."""
+        ms = (C.c_double * 7)()
+        ctr = (C.c_uint64 * 6)()
+        self._sync_params()
+        _check(lib().pt_table_lookup_proposed_profile(self._h, C.c_void_p(a_ptr), h, w, C.c_void_p(cand_ptr),
+                                                      C.c_void_p(conf_ptr), C.c_float(threshold), int(kcoh_confident),
+                                                      C.c_void_p(ann_ptr), C.c_void_p(stream), ms, ctr))
         return dict(zip(self.LEARNED_STAGES, list(ms))), dict(choose_cand=ctr[0], choose_rows=ctr[1], pull_cand=ctr[2],
                                                              pull_rows=ctr[3], confident=ctr[4], proposals=ctr[5])
 

@@ -40,8 +40,7 @@ struct QPlan {
     int pull_max;            /* most neighbour candidates scored per patch */
     int tile;                /* query patches per CTA (single-image launches) */
     int row0, rows;          /* patch rows of a single-image launch */
-    const float *bq;         /* b as packed RGB in eight copies, copy k shifted by k pixels */
-    size_t bq_stride;        /* floats from one copy to the next */
+    const float4 *b1;        /* b shifted by one pixel: b1[i] = b[i + 1] */
     const int *allowed;      /* b patches that may be matched (allowed[p] == allowed_index), or NULL */
     int allowed_index;
     const float4 *adesc;     /* descriptor mode: query descriptor store (ds4 float4 per patch), or NULL */
@@ -93,40 +92,43 @@ __device__ __forceinline__ void stage_a(float4 *atile, const float4 *__restrict_
 /* Shared-memory bytes of a staged query tile of TW patches. */
 constexpr size_t atile_bytes(int TW) { return sizeof(float) * 3 * 8 * (TW + 7); }
 
-/* Query row dy of the patch at tile column tx: its 24 interleaved RGB floats. */
+/* Query row dy of the patch at tile column tx. */
 template<int TW>
-__device__ __forceinline__ void load_arow(const float4 *atile, int dy, int tx, float (&av)[24]) {
+__device__ __forceinline__ void load_arow(const float4 *atile, int dy, int tx, float4 (&av)[8]) {
     const float *at = reinterpret_cast<const float *>(atile) + 3 * (dy * (TW + 7) + tx);
 #pragma unroll
-    for (int e = 0; e < 24; e++) av[e] = at[e];
+    for (int p = 0; p < 8; p++) av[p] = make_float4(at[3 * p], at[3 * p + 1], at[3 * p + 2], 0.f);
 }
 
-/* One 32-byte read-only load: 8 floats. */
-__device__ __forceinline__ void ld_f8(const float *p, float *v) {
+/* One 32-byte read-only load: pixels p[0], p[1]. */
+__device__ __forceinline__ void ld_px2(const float4 *p, float4 &u, float4 &v) {
     asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+        : "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w), "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
         : "l"(p));
 }
 
-/* The 8 pixels (x..x+7, y) of b as 24 interleaved RGB floats, with three 32-byte loads.  The
-   table keeps b as packed RGB in eight copies, copy k shifted by k pixels (bq[k * stride + m] =
-   rgb[3 * k + m]); the row starting at pixel index i = y * bw + x is read from copy i & 7 at float
-   3 * (i - (i & 7)), which is 32-byte aligned, so a row is exactly three sectors. */
-__device__ __forceinline__ void load_brow(const QPlan &q, int x, int y, float (&bv)[24]) {
+/* The 8 pixels (x..x+7, y) of b with four 32-byte loads: pixel index i = y*bw + x is read from b
+   when even and from the shifted copy b1 (b1[i-1] = b[i]) when odd, so every load starts on a
+   32-byte boundary (both arrays are 256-byte aligned). */
+__device__ __forceinline__ void load_brow(const QPlan &q, const float4 *__restrict__ B, int x, int y, float4 (&bv)[8]) {
     const size_t i = (size_t) y * q.bw + x;
-    const size_t k = i & 7;
-    const float *src = q.bq + k * q.bq_stride + 3 * (i - k);
+    const float4 *src = (i & 1) ? q.b1 + (i - 1) : B + i;
 #pragma unroll
-    for (int j = 0; j < 3; j++) ld_f8(src + 8 * j, bv + 8 * j);
+    for (int j = 0; j < 4; j++) ld_px2(src + 2 * j, bv[2 * j], bv[2 * j + 1]);
 }
 
 /* Adds one patch row to the four SSE-lane sums of patch_dist_exact (patchtable.h:349-356): the
-   interleaved RGB float e goes to lane e & 3, in increasing e per lane. */
-__device__ __forceinline__ void row_lanes(const float (&av)[24], const float (&bv)[24], float (&l)[4]) {
+   interleaved RGB float e = 3p + c goes to lane e & 3, in increasing e per lane. */
+__device__ __forceinline__ void row_lanes(const float4 (&av)[8], const float4 (&bv)[8], float (&l)[4]) {
 #pragma unroll
-    for (int e = 0; e < 24; e++) {
-        const float t = __fsub_rn(av[e], bv[e]);
-        l[e & 3] = __fadd_rn(l[e & 3], __fmul_rn(t, t));
+    for (int p = 0; p < 8; p++) {
+        const float t0 = __fsub_rn(av[p].x, bv[p].x), t1 = __fsub_rn(av[p].y, bv[p].y), t2 = __fsub_rn(av[p].z, bv[p].z);
+        const float qd[3] = {__fmul_rn(t0, t0), __fmul_rn(t1, t1), __fmul_rn(t2, t2)};
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const int e = (3 * p + c) & 3;
+            l[e] = __fadd_rn(l[e], qd[c]);
+        }
     }
 }
 
@@ -139,13 +141,12 @@ __device__ __forceinline__ float lane_total(const float (&l)[4]) {
 template<int TW>
 __device__ __forceinline__ float ssd_tile(const float4 *atile, int tx, const QPlan &q, const float4 *__restrict__ B,
                                           int bx, int by, float bound, unsigned &rows) {
-    (void) B;
     float l[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
     for (int dy = 0; dy < 8; dy++) {
         rows++;
-        float av[24], bv[24];
-        load_brow(q, bx, by + dy, bv);
+        float4 av[8], bv[8];
+        load_brow(q, B, bx, by + dy, bv);
         load_arow<TW>(atile, dy, tx, av);
         row_lanes(av, bv, l);
         if (dy < 7 && lane_total(l) >= bound) return finf();
@@ -171,14 +172,14 @@ __device__ __forceinline__ void ssd_group(const float4 *atile, int tx, const QPl
 #pragma unroll
         for (int g = 0; g < G; g++) any |= live[g];
         if (!any) break;
-        float av[24];
+        float4 av[8];
         load_arow<TW>(atile, dy, tx, av);
 #pragma unroll
         for (int g = 0; g < G; g++) {
             if (!live[g]) continue;
             rows++;
-            float bv[24];
-            load_brow(q, pt_x(cand[g]), pt_y(cand[g]) + dy, bv);
+            float4 bv[8];
+            load_brow(q, B, pt_x(cand[g]), pt_y(cand[g]) + dy, bv);
             row_lanes(av, bv, l[g]);
             if (dy < 7 && lane_total(l[g]) >= bound) live[g] = false;
         }
@@ -629,17 +630,13 @@ k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, lon
    reference's lane order, without an early exit. */
 __device__ __forceinline__ float ssd_global(const QPlan &q, const float4 *__restrict__ a, int ax, int ay,
                                            const float4 *__restrict__ B, int bx, int by) {
-    (void) B;
     float l[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
     for (int dy = 0; dy < 8; dy++) {
-        float av[24], bv[24];
-        load_brow(q, bx, by + dy, bv);
+        float4 av[8], bv[8];
+        load_brow(q, B, bx, by + dy, bv);
 #pragma unroll
-        for (int p = 0; p < 8; p++) {
-            const float4 v = __ldg(a + (size_t) (ay + dy) * q.aw + ax + p);
-            av[3 * p] = v.x; av[3 * p + 1] = v.y; av[3 * p + 2] = v.z;
-        }
+        for (int p = 0; p < 8; p++) av[p] = __ldg(a + (size_t) (ay + dy) * q.aw + ax + p);
         row_lanes(av, bv, l);
     }
     return lane_total(l);
@@ -752,8 +749,7 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
         return pt_fail(PT_BAD_ARG, "query rows [%d, %d) outside 0..%d", q.row0, q.row0 + q.rows, q.eh);
     if (q.tile != 32 && q.tile != 64 && q.tile != 128 && q.tile != 256)
         return pt_fail(PT_BAD_ARG, "gpu_tile %d: query patches per CTA must be 32, 64, 128 or 256", s.tile);
-    q.bq = s.bq;
-    q.bq_stride = s.bq_stride;
+    q.b1 = s.b1;
     q.allowed = s.allowed;
     q.allowed_index = s.allowed_index;
     q.adesc = reinterpret_cast<const float4 *>(s.adesc);
@@ -769,19 +765,10 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     if (q.adesc) {
         if (!q.bdesc || (s.ds != 8 && s.ds != 16) || q.nd < 3 || q.nd > s.ds)
             return pt_fail(PT_BAD_ARG, "descriptor query: store of %d floats for %d dimensions", s.ds, q.nd);
-    } else if (!q.bq) {
-        return pt_fail(PT_BAD_ARG, "query without the packed copies of the table image");
+    } else if (!q.b1) {
+        return pt_fail(PT_BAD_ARG, "query without the shifted copy of the table image");
     }
     if (q.radius > 2) return pt_fail(PT_UNSUPPORTED, "propagation radius %d > 2 on the GPU path", q.radius);
-    return PT_OK;
-}
-
-pt_status pt_make_bq(const float *rgb, int h, int w, float *bq, cudaStream_t st) {
-    const size_t n = (size_t) h * w * 3, stride = pt_bq_stride(h, w);
-    PT_CUDA(cudaMemsetAsync(bq, 0, sizeof(float) * stride * PT_BQ_COPIES, st));
-    for (int k = 0; k < PT_BQ_COPIES; k++)
-        if (n > (size_t) (3 * k))
-            PT_CUDA(cudaMemcpyAsync(bq + k * stride, rgb + 3 * k, sizeof(float) * (n - 3 * k), cudaMemcpyDeviceToDevice, st));
     return PT_OK;
 }
 

@@ -66,8 +66,7 @@ pt_status run(pt_batch *B, const float *d_rgb, double *d_ann, cudaStream_t st) {
     qs.spatial = p.spatial;
     qs.do_rs = p.do_rs;
     qs.radius = std::min(2, p.query_step + p.prop_dist);
-    qs.bq = v.bq;
-    qs.bq_stride = v.bq_stride;
+    qs.b1 = v.b_rgba1;
     qs.pull_max = p.gpu_pull_max;
     qs.allowed = v.allowed;
     qs.allowed_index = p.allowed_index;

@@ -87,11 +87,6 @@ pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *bdesc, int ds
                         int kc, int min_dist, int2 *kcoh, int *max_knn_out, cudaStream_t st);
 
 /* k_query.cu */
-#define PT_BQ_COPIES 8
-/* Floats from one packed copy of an h x w table image to the next (256-byte aligned). */
-inline size_t pt_bq_stride(int h, int w) { return ((size_t) h * w * 3 + 63) / 64 * 64; }
-/* Fills the PT_BQ_COPIES shifted packed copies from the device RGB image (k_query.cu). */
-pt_status pt_make_bq(const float *rgb, int h, int w, float *bq, cudaStream_t st);
 struct QuerySetup {
     int aw, ah, bw, bh;
     double prop_scale, triangle_factor;
@@ -100,11 +95,7 @@ struct QuerySetup {
     int pull_max = 0;        /* most neighbour candidates a pull scores per patch (0 = all) */
     int tile = 0;            /* query patches per CTA in choose / pull: 32, 64, 128, 256 (0 = 32) */
     int row0 = 0, rows = 0;  /* patch rows [row0, row0 + rows) of a single-image launch (rows 0 = all) */
-    /* the table image as packed RGB in PT_BQ_COPIES copies, copy k shifted by k pixels
-       (bq[k * bq_stride + m] = rgb[3 * k + m]): every 8-pixel patch row is one 96-byte,
-       32-byte-aligned read from copy (pixel index & 7) */
-    const float *bq = nullptr;
-    size_t bq_stride = 0;
+    const float4 *b1 = nullptr;   /* the table image shifted by one pixel, b1[i] = b[i + 1] */
     const int *allowed = nullptr; /* b patches a match may use (allowed[p] == allowed_index), or NULL */
     int allowed_index = 0;
     /* Descriptor mode (is_descriptor): distances are patch_dist_approx between the query's and the
@@ -212,8 +203,7 @@ struct PtTableView {
     pt_params p;
     int h, w, ds;
     const float4 *b_rgba;
-    const float *bq;                     /* packed RGB copies of b (QuerySetup::bq) */
-    size_t bq_stride;
+    const float4 *b_rgba1;               /* b_rgba shifted by one pixel (32-byte aligned row loads) */
     const int *table;
     const int *to_bin;
     const int2 *kcoh;

@@ -103,8 +103,7 @@ extern "C" pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_
     qs.do_rs = p.do_rs;
     qs.radius = p.query_step + p.prop_dist;
     if (qs.radius > 2) qs.radius = 2;
-    qs.bq = v.bq;
-    qs.bq_stride = v.bq_stride;
+    qs.b1 = v.b_rgba1;
     qs.pull_max = p.gpu_pull_max;
     qs.tile = p.gpu_tile;
     qs.allowed = v.allowed;

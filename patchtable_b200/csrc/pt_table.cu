@@ -119,7 +119,7 @@ struct pt_table {
     cudaStream_t st = nullptr;
     bool own_stream = false;
     DevBuf<float4> b_rgba;
-    DevBuf<float> b_bq;               /* b as packed RGB, PT_BQ_COPIES copies shifted by 0..7 pixels */
+    DevBuf<float4> b_rgba1;           /* b_rgba shifted by one pixel, b_rgba1[i] = b_rgba[i + 1] */
     DevBuf<float> b_desc;
     DevBuf<int> allowed;
     std::vector<int> nslices;
@@ -451,10 +451,12 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
                         packed[((size_t) y * t->ew + x) * t->ds + d] = wh0[((size_t) (y + 7) * (w + 7) + (x + 7)) * t->nd + d];
             PT_CUDA(cudaMemcpyAsync(t->b_desc.p, packed.data(), sizeof(float) * packed.size(), cudaMemcpyHostToDevice, t->st));
         }
-        /* The query reads a b patch row as 24 packed floats from one of eight shifted copies, so
-           every row is one 32-byte-aligned 96-byte read (k_query.cu load_brow). */
-        PT_CUDA(t->b_bq.reserve(pt_bq_stride(h, w) * PT_BQ_COPIES));
-        PT_TRY(pt_make_bq(rgb.p, h, w, t->b_bq.p, t->st));
+        /* The query reads b patch rows with 32-byte loads: from b_rgba at even pixel indices and
+           from this one-pixel-shifted copy at odd ones, so every load is 32-byte aligned. */
+        const size_t npx = (size_t) h * w;
+        PT_CUDA(t->b_rgba1.reserve(npx));
+        PT_CUDA(cudaMemsetAsync(t->b_rgba1.p, 0, sizeof(float4) * npx, t->st));
+        PT_CUDA(cudaMemcpyAsync(t->b_rgba1.p, t->b_rgba.p + 1, sizeof(float4) * (npx - 1), cudaMemcpyDeviceToDevice, t->st));
         PT_CUDA(cudaStreamSynchronize(t->st));
     }
     std::vector<int> allowed_h;
@@ -605,11 +607,20 @@ pt_status mark(pt_table *t, LookupProfile *prof, int stage, cudaStream_t st) {
     return PT_OK;
 }
 
+/* Proposals handed in by the caller instead of the network's (pt_table_lookup_proposed_profile). */
+struct ExtProposals {
+    const int *cand;          /* P x PT_PROP_TOPK table entries, -1 = none */
+    const float *conf;        /* P confidences */
+    float threshold;
+    int kcoh_confident;
+};
+
 /* The device part of a lookup: a_rgb (device, h x w x 3) -> d_ann (device doubles).  With prof,
    an event is recorded after every stage and SSD work is counted. */
 pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d_ann, cudaStream_t st,
                         LookupProfile *prof = nullptr, pt_proposal *net = nullptr, const double *d_prev = nullptr,
-                        const float *d_sv = nullptr) {
+                        const float *d_sv = nullptr, const ExtProposals *ext = nullptr) {
+    const bool learned = net || ext;
     const pt_params &p = t->p;
     long long P = (long long) (h - 7) * (w - 7);
     if (P >= (1ll << 31)) return pt_fail(PT_BAD_ARG, "query image too large");
@@ -619,7 +630,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     if (ctr) PT_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * 6, st));
     PT_TRY(mark(t, prof, -1, st));
     if (t->desc_mode) {
-        if (net) return pt_fail(PT_UNSUPPORTED, "learned proposals in descriptor mode");
+        if (learned) return pt_fail(PT_UNSUPPORTED, "learned proposals in descriptor mode");
         int ih, iw;
         size_t nin;
         query_input_dims(t, h, w, ih, iw, nin);
@@ -627,12 +638,12 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     } else if (t->pca) {
         PT_TRY(pt_launch_pca(a_rgb, h, w, pt_color_mode(p), t->q_rgba.p, t->pca_mean.p, t->pca_basis.p, t->nd,
                              t->q_desc.p, t->ds, st));
-    } else if (net || !t->subs.empty()) {
+    } else if (learned || !t->subs.empty()) {
         PT_TRY(pt_launch_descriptor(p.ndims, p.nchroma, a_rgb, h, w, pt_color_mode(p), t->q_rgba.p, t->q_desc.p,
                                     t->ds, st));
     }
     /* The plain single-table query needs its descriptors only for the table step: one fused pass. */
-    const bool fused = !t->desc_mode && !t->pca && !net && t->subs.empty();
+    const bool fused = !t->desc_mode && !t->pca && !learned && t->subs.empty();
     if (fused)
         PT_TRY(pt_launch_descriptor_cells(p.ndims, p.nchroma, a_rgb, h, w, pt_color_mode(p), t->q_rgba.p, t->bins,
                                           t->to_bin.p, t->table.p, t->q_tcand.p, 0, (h - 7 + 7) / 8, st));
@@ -648,7 +659,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
         }
     }
     PT_TRY(mark(t, prof, LookupProfile::CELLS, st));
-    if (net) {
+    if (net && !ext) {
         PtTableView v;
         PT_TRY(pt_table_view(t, &v));
         PT_CUDA(t->q_lcand.reserve((size_t) P * PT_PROP_TOPK));
@@ -665,8 +676,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     qs.spatial = p.spatial;
     qs.do_rs = p.do_rs;
     qs.radius = p.query_step + p.prop_dist;
-    qs.bq = t->b_bq.p;
-    qs.bq_stride = pt_bq_stride(t->h, t->w);
+    qs.b1 = t->b_rgba1.p;
     qs.pull_max = p.gpu_pull_max;
     qs.tile = p.gpu_tile;
     qs.allowed = t->allowed.p;
@@ -698,12 +708,12 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
                                        t->q_rgba.p, t->b_rgba.p, t->q_pos[0].p, t->q_d[0].p, t->q_torig.p, t->q_tbad.p, st));
         PT_CUDA(cudaMemcpyAsync(t->q_tpos0.p, t->q_pos[0].p, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
         PT_CUDA(cudaMemcpyAsync(t->q_td0.p, t->q_d[0].p, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
-    } else if (net || pt_default_passes(p) == 0) {
+    } else if (learned || pt_default_passes(p) == 0) {
         /* Initial field (patchtable.h:3538-3547): x = b0_ew + 1, dist = DIST_INFINITY. */
         PT_TRY(pt_launch_init(n, pt_xy(t->ew + 1, 0), (float) PT_DIST_INF, t->q_pos[0].p, t->q_d[0].p, st));
     }
     /* Otherwise the first pass reads no state arrays: its kernels start from the initial field. */
-    const bool fresh = !p.init_random && !d_prev && !net && pt_default_passes(p) > 0;
+    const bool fresh = !p.init_random && !d_prev && !learned && pt_default_passes(p) > 0;
     /* the last pull writes the NNF itself unless the temporal output has to restore distances */
     const bool direct_out = p.do_prop && pt_default_passes(p) > 0 && !(d_prev && !p.init_random && p.coherence_temporal != 0.0);
     PT_TRY(mark(t, prof, LookupProfile::INIT, st));
@@ -719,11 +729,13 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
         qi.pass = i;
         if (!pt_pass_kcoh(p, i, passes)) qi.kcoherence = 0;
         const int use_done = i > 0 && pt_pass_kcoh(p, i - 1, passes);
-        if (net)
+        if (learned)
             PT_TRY(pt_launch_choose_learned(qi, t->q_rgba.p, t->b_rgba.p, t->q_pos[cur].p, t->q_d[cur].p, t->q_tcand.p,
                                             t->kcoh.p, do_table, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p, use_done,
-                                            i == 0 ? t->q_lcand.p : nullptr, t->q_lconf.p, pt_prop_threshold(net),
-                                            pt_prop_kcoh_confident(net), ctr, ctr ? ctr + 4 : nullptr, st));
+                                            i == 0 ? (ext ? ext->cand : t->q_lcand.p) : nullptr,
+                                            ext ? ext->conf : t->q_lconf.p, ext ? ext->threshold : pt_prop_threshold(net),
+                                            ext ? ext->kcoh_confident : pt_prop_kcoh_confident(net), ctr,
+                                            ctr ? ctr + 4 : nullptr, st));
         else
             PT_TRY(pt_launch_choose(qi, n, t->q_rgba.p, t->b_rgba.p, fresh && i == 0 ? nullptr : t->q_pos[cur].p,
                                     fresh && i == 0 ? nullptr : t->q_d[cur].p, t->q_tcand.p, t->kcoh.p, do_table,
@@ -825,8 +837,7 @@ pt_status enqueue_bands(pt_table *t, const float *a, double *ann_out, int h, int
     qs.spatial = p.spatial;
     qs.do_rs = p.do_rs;
     qs.radius = std::min(2, p.query_step + p.prop_dist);
-    qs.bq = t->b_bq.p;
-    qs.bq_stride = pt_bq_stride(t->h, t->w);
+    qs.b1 = t->b_rgba1.p;
     qs.pull_max = p.gpu_pull_max;
     qs.tile = p.gpu_tile;
     qs.allowed = t->allowed.p;
@@ -992,12 +1003,12 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
 /* lookup_device with stage events; stage_ms[nst] receives summed stage times, counters[nctr] the
    SSD work counters. */
 pt_status profile_impl(pt_table *t, pt_proposal *net, const float *d_a, int ih, int iw, double *d_ann, cudaStream_t st,
-                       double *stage_ms, int nst, uint64_t *counters, int nctr) {
+                       double *stage_ms, int nst, uint64_t *counters, int nctr, const ExtProposals *ext = nullptr) {
     if (!t || !d_a || !d_ann) return pt_fail(PT_BAD_ARG, "null argument");
     int h, w;
     PT_TRY(query_dims(t, ih, iw, h, w));
     LookupProfile prof;
-    PT_TRY(lookup_device(t, d_a, h, w, d_ann, st, &prof, net));
+    PT_TRY(lookup_device(t, d_a, h, w, d_ann, st, &prof, net, nullptr, nullptr, ext));
     PT_CUDA(cudaStreamSynchronize(st));
     if (net) PT_TRY(pt_prop_check_error(net, st));
     double ms_all[LookupProfile::NSTAGES] = {0};
@@ -1191,8 +1202,10 @@ pt_status load_impl(const pt_params *pin, const char *filename, pt_table **out) 
                     packed[((size_t) y * t->ew + x) * t->ds + d] = wh0[((size_t) (y + 7) * (w + 7) + (x + 7)) * nd + d];
         PT_CUDA(t->b_desc.reserve(packed.size()));
         PT_CUDA(cudaMemcpyAsync(t->b_desc.p, packed.data(), sizeof(float) * packed.size(), cudaMemcpyHostToDevice, t->st));
-        PT_CUDA(t->b_bq.reserve(pt_bq_stride(h, w) * PT_BQ_COPIES));
-        PT_TRY(pt_make_bq(rgb.p, h, w, t->b_bq.p, t->st));
+        const size_t npx = (size_t) h * w;
+        PT_CUDA(t->b_rgba1.reserve(npx));
+        PT_CUDA(cudaMemsetAsync(t->b_rgba1.p, 0, sizeof(float4) * npx, t->st));
+        PT_CUDA(cudaMemcpyAsync(t->b_rgba1.p, t->b_rgba.p + 1, sizeof(float4) * (npx - 1), cudaMemcpyDeviceToDevice, t->st));
         PT_CUDA(cudaStreamSynchronize(t->st));
     }
     /* the file has no k-coherence set (the reference's load leaves it empty); it is rebuilt from
@@ -1358,6 +1371,15 @@ pt_status pt_table_lookup_learned_profile(pt_table *t, pt_proposal *net, const f
                                           void *stream, double *stage_ms, uint64_t *counters) {
     if (!net) return pt_fail(PT_BAD_ARG, "null proposal network");
     return profile_impl(t, net, d_a, h, w, d_ann, (cudaStream_t) stream, stage_ms, LookupProfile::NSTAGES, counters, 6);
+}
+
+pt_status pt_table_lookup_proposed_profile(pt_table *t, const float *d_a, int h, int w, const int32_t *d_cand,
+                                           const float *d_conf, float threshold, int kcoh_confident, double *d_ann,
+                                           void *stream, double *stage_ms, uint64_t *counters) {
+    if (!d_cand || !d_conf) return pt_fail(PT_BAD_ARG, "null proposals");
+    ExtProposals ext{d_cand, d_conf, threshold, kcoh_confident};
+    return profile_impl(t, nullptr, d_a, h, w, d_ann, (cudaStream_t) stream, stage_ms, LookupProfile::NSTAGES, counters, 6,
+                        &ext);
 }
 
 pt_status pt_table_lookup_learned(pt_table *t, pt_proposal *net, const float *a, int h, int w, double *ann_out,
@@ -1545,8 +1567,7 @@ pt_status pt_table_view(const pt_table *t, PtTableView *v) {
     v->p = t->p;
     v->h = t->h; v->w = t->w; v->ds = t->ds;
     v->b_rgba = t->b_rgba.p;
-    v->bq = t->b_bq.p;
-    v->bq_stride = pt_bq_stride(t->h, t->w);
+    v->b_rgba1 = t->b_rgba1.p;
     v->table = t->table.p;
     v->to_bin = t->to_bin.p;
     v->kcoh = t->kcoh.p;

@@ -15,6 +15,7 @@ memory and shuffles sample indices.
 
     python -m patchtable_b200.proposal train --pairs 200 --size 240x320 --out weights.npy
     python -m patchtable_b200.proposal eval --weights weights.npy --heldout 20 --size 1080x1920
+    python -m patchtable_b200.proposal ablation --weights weights.npy --heldout 5 --out ablation.json
 """
 from __future__ import annotations
 
@@ -299,6 +300,98 @@ def evaluate(net: ProposalNet, seeds, h: int, w: int, switches: str = DEFAULT_SW
     return {"size": [h, w], "seeds": list(seeds), "switches": switches, "proposal_hits": hit, "results": rows}
 
 
+ABLATION_SCHEDULES = ((1, 2, 1), (1, 2, 0), (2, 2, 0), (3, 4, 0), (4, 8, 0))
+
+
+def ablation(net: ProposalNet, seeds, h: int, w: int, switches: str = DEFAULT_SWITCHES, schedules=ABLATION_SCHEDULES,
+             log=None) -> dict:
+    """What a proposal network can gain at most, on held-out pairs.
+
+    For every schedule, the mean NNF distance and the device time of: the plain query; the learned
+    query with this network's proposals (threshold 0.5 and 0); and the learned query with *perfect*
+    proposals -- each patch's own match in the plain method's converged (default-schedule) field,
+    offered as its only proposal with confidence 1 -- timed without any inference cost.  The perfect
+    proposals bound every network of this form: a network can at best reach their quality, and must
+    add its inference time.  Also recorded: how often the converged match is among this network's 8
+    proposals (recall@8) and how often a label exists at all (the match's bin offsets within the
+    5^G window the network scores), with labels taken from the converged field and from a one-pass
+    field."""
+    torch = _torch()
+    from .metrics import get_mean_dist
+    P = (h - 7) * (w - 7)
+    st = torch.cuda.current_stream().cuda_stream
+    acc, hits, windows, inf_ms = {}, [], {"converged": [], "one_pass": []}, []
+
+    def best_of(fn, reps=4):
+        best = None
+        for r in range(reps):
+            ms, _ = fn()
+            if r:
+                tot = sum(ms.values())
+                best = tot if best is None else min(best, tot)
+        return best
+
+    for seed in seeds:
+        a, b = synth.pair(h, w, seed)
+        _srand(0)
+        params = PatchTableParams(switches)
+        table = PatchTable(params, b)
+        a_d = torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+        ann = torch.empty(P * 3, dtype=torch.float64, device="cuda")
+        params.gpu_prop_passes = 0
+        table.lookup_device(a_d.data_ptr(), h, w, ann.data_ptr(), st)
+        conv = ann.clone()
+        # perfect proposals: the converged match (packed padded position) in slot 0, confidence 1
+        A = conv.view(P, 3)
+        perfect = torch.full((P, TOPK), -1, dtype=torch.int32, device="cuda")
+        perfect[:, 0] = (A[:, 0].to(torch.int32) + 7) | ((A[:, 1].to(torch.int32) + 7) << 16)
+        ones = torch.ones(P, dtype=torch.float32, device="cuda")
+        net.configure(0.5, False)
+        hits.append(proposal_hits(table, net, a, conv))
+        X = torch.empty((P, IN), dtype=torch.bfloat16, device="cuda")
+        L = torch.empty((P, 8), dtype=torch.uint8, device="cuda")
+        table.proposal_samples(a_d.data_ptr(), h, w, conv.data_ptr(), X.data_ptr(), L.data_ptr(), st)
+        windows["converged"].append(label_stats(L)["exact_window"])
+        params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = 1, 2, 1
+        table.lookup_device(a_d.data_ptr(), h, w, ann.data_ptr(), st)
+        table.proposal_samples(a_d.data_ptr(), h, w, ann.data_ptr(), X.data_ptr(), L.data_ptr(), st)
+        windows["one_pass"].append(label_stats(L)["exact_window"])
+        cand = torch.empty((P, TOPK), dtype=torch.int32, device="cuda")
+        conf = torch.empty(P, dtype=torch.float32, device="cuda")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = None
+        for r in range(4):
+            e0.record()
+            table.proposal_infer(net, a_d.data_ptr(), h, w, cand.data_ptr(), conf.data_ptr(), 0, st)
+            e1.record()
+            e1.synchronize()
+            if r:
+                best = e0.elapsed_time(e1) if best is None else min(best, e0.elapsed_time(e1))
+        inf_ms.append(best)
+        for sched in schedules:
+            params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = sched
+            arms = {"plain": lambda: table.lookup_profile(a_d.data_ptr(), h, w, ann.data_ptr(), st),
+                    "perfect_proposals": lambda: table.lookup_proposed_profile(
+                        a_d.data_ptr(), h, w, perfect.data_ptr(), ones.data_ptr(), 0.5, ann.data_ptr(), st)}
+            for thr in (0.5, 0.0):
+                arms["network_%g" % thr] = (lambda t_=thr: (net.configure(t_, False), table.lookup_learned_profile(
+                    net, a_d.data_ptr(), h, w, ann.data_ptr(), st))[1])
+            for kind, fn in arms.items():
+                ms = best_of(fn)
+                md = get_mean_dist(ann.view(h - 7, w - 7, 3).cpu().numpy())
+                acc.setdefault("%d/%d/%d %s" % (sched + (kind,)), []).append((md, ms))
+        table.close()
+        if log:
+            log("ablation seed %d" % seed)
+    rows = {k: {"mean_nnf_dist": float(np.mean([m for m, _ in v])), "ms": float(np.mean([t for _, t in v]))}
+            for k, v in acc.items()}
+    return {"size": [h, w], "seeds": list(seeds), "switches": switches,
+            "inference_ms": float(np.mean(inf_ms)),
+            "recall_at_8": {k: float(np.mean([hh[k] for hh in hits])) for k in hits[0]},
+            "label_in_window": {k: float(np.mean(v)) for k, v in windows.items()},
+            "results": rows}
+
+
 def _main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -318,7 +411,21 @@ def _main():
     e.add_argument("--size", default="1080x1920")
     e.add_argument("--switches", default=DEFAULT_SWITCHES)
     e.add_argument("--out", required=True)
+    b = sub.add_parser("ablation")
+    b.add_argument("--weights", required=True)
+    b.add_argument("--heldout", type=int, default=5)
+    b.add_argument("--size", default="1080x1920")
+    b.add_argument("--switches", default=DEFAULT_SWITCHES)
+    b.add_argument("--out", required=True)
     args = ap.parse_args()
+    if args.cmd == "ablation":
+        h, w = (int(v) for v in args.size.split("x"))
+        net = ProposalNet.load(args.weights)
+        res = ablation(net, HELDOUT_SEEDS[:args.heldout], h, w, args.switches, log=lambda m: print(m, flush=True))
+        with open(args.out, "w") as f:
+            json.dump(res, f, indent=1, sort_keys=True)
+        print(json.dumps({k: res[k] for k in ("inference_ms", "recall_at_8", "label_in_window")}))
+        return
     if args.cmd == "eval":
         h, w = (int(v) for v in args.size.split("x"))
         net = ProposalNet.load(args.weights)
