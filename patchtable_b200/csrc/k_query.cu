@@ -431,11 +431,11 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
     }
 }
 
-/* At most 12 x 64 threads' worth of CTAs per SM's register file: the compiler keeps the kernel at
-   80 registers (a few bytes of spills), and the extra resident warps hide the gather latency
-   better than the unrestricted 103-register version (measured: choose 0.70 -> 0.64 ms at 1080p). */
+/* At least 10 x 64 threads' worth of CTAs per SM: the register budget this leaves keeps the gather
+   latency hidden without the spills of tighter caps (measured at 1080p, 64 patches per CTA:
+   choose 0.70 ms unrestricted, 0.611 at 10 x 64, 0.619 at 12 x 64, 0.625 at 16 x 64). */
 template<int TW, bool LEARNED, bool DESC>
-__global__ void __launch_bounds__(TW, (12 * 64) / TW)
+__global__ void __launch_bounds__(TW, (10 * 64) / TW)
 k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
               const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
               int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters, const LearnedArgs la) {
@@ -579,7 +579,7 @@ __device__ __forceinline__ long long next_segment(unsigned long long *work) {
 
 /* Persistent choose over every row segment of every image, handed out by a work counter. */
 template<int TW>
-__global__ void __launch_bounds__(TW, (12 * 64) / TW)
+__global__ void __launch_bounds__(TW, (10 * 64) / TW)
 k_choose_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, long long nseg, int twi,
                const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
                const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,

@@ -96,14 +96,6 @@ extern "C" int64_t pt_set_device_alloc_limit(int64_t bytes) { return g_alloc_lim
 
 extern "C" int64_t pt_device_bytes_in_use(void) { return g_alloc_live.load(); }
 
-/* What a recorded banded-lookup graph depends on besides the query image's address (compared
-   bytewise; zero-filled before use). */
-struct BandKey {
-    pt_params p;
-    int h, w, B, widen;
-    const void *bufs[12];
-};
-
 struct pt_table {
     pt_params p;
     int h = 0, w = 0, eh = 0, ew = 0;
@@ -162,26 +154,9 @@ struct pt_table {
     std::vector<cudaEvent_t> band_ev;
     PinnedBuf<int> h_pos;             /* banded host lookups: packed field downloaded per band */
     PinnedBuf<float> h_d;
-    /* banded host lookups replayed as a CUDA graph: the graph, its upload nodes (by offset into
-       the query image), the image it currently reads and what it was recorded for */
-    cudaGraph_t band_graph = nullptr;
-    cudaGraphExec_t band_exec = nullptr;
-    std::vector<std::pair<cudaGraphNode_t, size_t>> band_h2d;
-    const float *band_a = nullptr;
-    bool band_seen = false;
-    BandKey band_key_v;
-    void drop_band_graph() {
-        if (band_exec) cudaGraphExecDestroy(band_exec);
-        if (band_graph) cudaGraphDestroy(band_graph);
-        band_exec = nullptr;
-        band_graph = nullptr;
-        band_h2d.clear();
-        band_seen = false;
-    }
     long long last_h2d = 0, last_d2h = 0;   /* bytes copied by the last host lookup */
 
     ~pt_table() {
-        drop_band_graph();
         for (auto e : events) cudaEventDestroy(e);
         for (auto e : band_ev) cudaEventDestroy(e);
         if (st_in) cudaStreamDestroy(st_in);
@@ -775,20 +750,16 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
    for its rows, so the result is identical.  The download carries the packed field (int32
    position, float32 distance: 8 bytes per patch instead of the float64 record's 24) into pinned
    staging; once a band has arrived, the host threads widen it into the caller's float64 buffer
-   while later bands are still computed and copied.
-
-   The sequence is about a hundred copies, launches and event operations.  When the query image
-   sits in page-locked memory and the same sizes, parameters and buffers come again, it is
-   recorded once into a CUDA graph and replayed with one launch (the upload nodes are pointed at
-   the caller's image each time), so the host's enqueue cost stays off the critical path. */
+   while later bands are still computed and copied.  The launches are enqueued directly: replaying
+   the same sequence as a recorded CUDA graph measured slower (1.45 against 1.29 ms at 1080p). */
 int band_rows(const pt_table *t, int h, int w) {
     const pt_params &p = t->p;
     const int eh = h - 7, ew = w - 7;
     int B = 0;
     if (p.gpu_bands <= 0) {
         /* Default: the band's choose launch fills whole waves.  A choose CTA of tw patches is
-           resident 12 * 64 / tw times per SM, so one wave covers sms * 768 / (tw * segments) patch
-           rows; B is the largest multiple of 8 rows within k waves, for the smallest k giving at
+           resident about 10 * 64 / tw times per SM, so one wave covers sms * 640 / (tw * segments)
+           patch rows; B is the largest multiple of 8 rows within k waves, for the smallest k giving at
            least 32 rows and at most 24 bands (measured e2e: 720p 9 bands 0.71 ms, 1080p 20 bands
            of 56 rows = 0.95 wave 1.35 ms against 1.41 at 16 bands of 1.22 waves, 1440p 17 bands).
            Fewer than 8 bands would lose the overlap: then about 16 bands. */
@@ -800,7 +771,7 @@ int band_rows(const pt_table *t, int h, int w) {
             if (sms < 1) sms = 148;
         }
         const int tw = (p.gpu_tile == 64 || p.gpu_tile == 128 || p.gpu_tile == 256) ? p.gpu_tile : 32;
-        const double rows_wave = (double) sms * (12 * 64 / tw) / ((ew + tw - 1) / tw);
+        const double rows_wave = (double) sms * (10 * 64 / tw) / ((ew + tw - 1) / tw);
         for (int k = 1; k <= 64; k++) {
             B = (int) (k * rows_wave / 8) * 8;
             if (B >= 32 && (eh + B - 1) / B <= 24) break;
@@ -816,10 +787,8 @@ int band_rows(const pt_table *t, int h, int w) {
 }
 
 /* Enqueues the band pipeline on the table's streams, starting after the work queued on t->st and
-   joining every stream back into t->st at the end.  ev_d[b] marks band b's download (while
-   capturing, as an external event node, so that the replayed graph records it too). */
-pt_status enqueue_bands(pt_table *t, const float *a, double *ann_out, int h, int w, int B, int nb, bool capturing,
-                        bool widen) {
+   joining every stream back into t->st at the end.  ev_d[b] marks band b's download. */
+pt_status enqueue_bands(pt_table *t, const float *a, double *ann_out, int h, int w, int B, int nb, bool widen) {
     const pt_params &p = t->p;
     const int eh = h - 7, ew = w - 7;
     const long long P = (long long) eh * ew;
@@ -890,8 +859,7 @@ pt_status enqueue_bands(pt_table *t, const float *a, double *ann_out, int h, int
                 PT_CUDA(cudaMemcpyAsync(ann_out + 3 * o, t->q_ann.p + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost,
                                         t->st_out));
             }
-            if (capturing) PT_CUDA(cudaEventRecordWithFlags(ev_d[b - 2], t->st_out, cudaEventRecordExternal));
-            else PT_CUDA(cudaEventRecord(ev_d[b - 2], t->st_out));
+            PT_CUDA(cudaEventRecord(ev_d[b - 2], t->st_out));
         }
     }
     int k = 0;
@@ -903,18 +871,6 @@ pt_status enqueue_bands(pt_table *t, const float *a, double *ann_out, int h, int
     return PT_OK;
 }
 
-BandKey band_key(const pt_table *t, int h, int w, int B, bool widen, const double *ann_out) {
-    BandKey k;
-    memset(&k, 0, sizeof(k));
-    k.p = t->p;
-    k.h = h; k.w = w; k.B = B; k.widen = widen;
-    /* without widening the download nodes write the caller's buffer: part of the key */
-    const void *b[12] = {t->q_rgb.p, t->q_rgba.p, t->q_tcand.p, t->q_chpos.p, t->q_chd.p, t->q_kcdone.p,
-                         t->q_pos[1].p, t->q_d[1].p, t->h_pos.p, t->h_d.p, t->q_ann.p, widen ? nullptr : ann_out};
-    memcpy(k.bufs, b, sizeof(b));
-    return k;
-}
-
 pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_out) {
     const int eh = h - 7, ew = w - 7;
     const long long P = (long long) eh * ew;
@@ -922,13 +878,10 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     for (cudaStream_t *sp : {&t->st_in, &t->st_out, &t->st_choose, &t->st_pull})
         if (!*sp) PT_CUDA(cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking));
     const int B = band_rows(t, h, w), nb = (eh + B - 1) / B;
-    if ((int) t->band_ev.size() < 5 * nb + 5) {
-        t->drop_band_graph();                  /* its event nodes name the old events */
-        while ((int) t->band_ev.size() < 5 * nb + 5) {
-            cudaEvent_t e;
-            PT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-            t->band_ev.push_back(e);
-        }
+    while ((int) t->band_ev.size() < 5 * nb + 5) {
+        cudaEvent_t e;
+        PT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        t->band_ev.push_back(e);
     }
     const bool widen = pt_host_widen();
     if (widen) {
@@ -937,55 +890,7 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     } else {
         PT_CUDA(t->q_ann.reserve((size_t) P * 3));
     }
-    cudaPointerAttributes attr;
-    const bool pinned = cudaPointerGetAttributes(&attr, a) == cudaSuccess && attr.type == cudaMemoryTypeHost;
-    cudaGetLastError();
-    const BandKey key = band_key(t, h, w, B, widen, ann_out);
-    const bool same = t->band_seen && memcmp(&key, &t->band_key_v, sizeof(key)) == 0;
-    if (!pinned || !same) {
-        /* enqueue directly; a second call with the same key and a page-locked image records the graph */
-        t->drop_band_graph();
-        PT_TRY(enqueue_bands(t, a, ann_out, h, w, B, nb, false, widen));
-        memcpy(&t->band_key_v, &key, sizeof(key));
-        t->band_seen = pinned;
-    } else {
-        if (!t->band_exec) {
-            cudaGraph_t g = nullptr;
-            PT_CUDA(cudaStreamBeginCapture(t->st, cudaStreamCaptureModeThreadLocal));
-            pt_status s = enqueue_bands(t, a, ann_out, h, w, B, nb, true, widen);
-            cudaError_t e = cudaStreamEndCapture(t->st, &g);
-            if (s != PT_OK) { if (g) cudaGraphDestroy(g); return s; }
-            if (e != cudaSuccess) return pt_fail(PT_CUDA_ERR, "capturing the banded lookup: %s", cudaGetErrorString(e));
-            t->band_graph = g;
-            PT_CUDA(cudaGraphInstantiate(&t->band_exec, g, 0));
-            /* the upload nodes, by their offset into the query image */
-            size_t nn = 0;
-            PT_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
-            std::vector<cudaGraphNode_t> nodes(nn);
-            PT_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
-            const char *lo = (const char *) a, *hi = lo + sizeof(float) * (size_t) h * w * 3;
-            for (cudaGraphNode_t nd : nodes) {
-                cudaGraphNodeType ty;
-                PT_CUDA(cudaGraphNodeGetType(nd, &ty));
-                if (ty != cudaGraphNodeTypeMemcpy) continue;
-                cudaMemcpy3DParms mp;
-                PT_CUDA(cudaGraphMemcpyNodeGetParams(nd, &mp));
-                const char *src = (const char *) mp.srcPtr.ptr;
-                if (src >= lo && src < hi) t->band_h2d.push_back({nd, (size_t) (src - lo)});
-            }
-            t->band_a = a;
-        } else if (t->band_a != a) {
-            for (auto &u : t->band_h2d) {
-                cudaMemcpy3DParms mp;
-                PT_CUDA(cudaGraphMemcpyNodeGetParams(u.first, &mp));
-                mp.srcPtr.ptr = (void *) ((const char *) a + u.second);
-                PT_CUDA(cudaGraphExecMemcpyNodeSetParams(t->band_exec, u.first, &mp));
-            }
-            t->band_a = a;
-        }
-        PT_CUDA(cudaGraphLaunch(t->band_exec, t->st));
-        pt_count_launches(3 * nb);
-    }
+    PT_TRY(enqueue_bands(t, a, ann_out, h, w, B, nb, widen));
     t->last_h2d = (long long) sizeof(float) * h * w * 3;
     t->last_d2h = (long long) (widen ? sizeof(int) + sizeof(float) : 3 * sizeof(double)) * P;
     /* widen each band as soon as it has arrived */

@@ -312,10 +312,12 @@ def ablation(net: ProposalNet, seeds, h: int, w: int, switches: str = DEFAULT_SW
     proposals -- each patch's own match in the plain method's converged (default-schedule) field,
     offered as its only proposal with confidence 1 -- timed without any inference cost.  The perfect
     proposals bound every network of this form: a network can at best reach their quality, and must
-    add its inference time.  Also recorded: how often the converged match is among this network's 8
-    proposals (recall@8) and how often a label exists at all (the match's bin offsets within the
-    5^G window the network scores), with labels taken from the converged field and from a one-pass
-    field."""
+    add its inference time.  Two partial forms show how the gain falls with recall: perfect
+    proposals only for patches whose match lies in the class space (bin offsets within the 5^G
+    window the network scores), and only for a random subset as large as this network's recall.
+    Also recorded: how often the converged match is among this network's 8 proposals (recall@8)
+    and how often a label exists at all, with labels taken from the converged field and from a
+    one-pass field."""
     torch = _torch()
     from .metrics import get_mean_dist
     P = (h - 7) * (w - 7)
@@ -352,6 +354,13 @@ def ablation(net: ProposalNet, seeds, h: int, w: int, switches: str = DEFAULT_SW
         L = torch.empty((P, 8), dtype=torch.uint8, device="cuda")
         table.proposal_samples(a_d.data_ptr(), h, w, conv.data_ptr(), X.data_ptr(), L.data_ptr(), st)
         windows["converged"].append(label_stats(L)["exact_window"])
+        # perfect proposals for the patches a network of this class space could name at all (the
+        # match's bin offsets inside the window), and for a random subset the size of this
+        # network's recall: the other patches keep the plain candidates
+        in_window = (L[:, 6] != 0).to(torch.float32)
+        g = torch.Generator(device="cuda")
+        g.manual_seed(seed)
+        at_recall = (torch.rand(P, device="cuda", generator=g) < hits[-1]["hit"]).to(torch.float32)
         params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = 1, 2, 1
         table.lookup_device(a_d.data_ptr(), h, w, ann.data_ptr(), st)
         table.proposal_samples(a_d.data_ptr(), h, w, ann.data_ptr(), X.data_ptr(), L.data_ptr(), st)
@@ -370,9 +379,10 @@ def ablation(net: ProposalNet, seeds, h: int, w: int, switches: str = DEFAULT_SW
         inf_ms.append(best)
         for sched in schedules:
             params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = sched
-            arms = {"plain": lambda: table.lookup_profile(a_d.data_ptr(), h, w, ann.data_ptr(), st),
-                    "perfect_proposals": lambda: table.lookup_proposed_profile(
-                        a_d.data_ptr(), h, w, perfect.data_ptr(), ones.data_ptr(), 0.5, ann.data_ptr(), st)}
+            arms = {"plain": lambda: table.lookup_profile(a_d.data_ptr(), h, w, ann.data_ptr(), st)}
+            for name, cf in (("perfect_proposals", ones), ("perfect_in_window", in_window), ("perfect_at_net_recall", at_recall)):
+                arms[name] = (lambda c_=cf: table.lookup_proposed_profile(
+                    a_d.data_ptr(), h, w, perfect.data_ptr(), c_.data_ptr(), 0.5, ann.data_ptr(), st))
             for thr in (0.5, 0.0):
                 arms["network_%g" % thr] = (lambda t_=thr: (net.configure(t_, False), table.lookup_learned_profile(
                     net, a_d.data_ptr(), h, w, ann.data_ptr(), st))[1])

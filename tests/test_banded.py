@@ -58,11 +58,10 @@ def test_banded_with_allowed_mask(gpu, libc):
     assert np.all(allowed[host[..., 1].astype(int), host[..., 0].astype(int)] == 1)
 
 
-def test_banded_graph_replay_with_page_locked_images(gpu, libc):
-    """A page-locked query image seen again with the same sizes and parameters is answered by
-    replaying the recorded band graph; a second page-locked image re-points its upload nodes, a
-    pageable one is enqueued directly, a parameter change records anew.  Every answer equals the
-    device lookup's, and the host threads' count does not change it."""
+def test_banded_repeated_lookups_page_locked_and_pageable(gpu, libc):
+    """Repeated host lookups of page-locked and pageable images, with the packed download widened
+    by one or several host threads or the float64 records downloaded as they are: every answer
+    equals the device lookup's, and the transfer accounting matches the mode."""
     import torch
     a, b = synth.pair(300, 420, 81)
     a2 = synth.image_a(300, 420, 82)
@@ -74,17 +73,17 @@ def test_banded_graph_replay_with_page_locked_images(gpu, libc):
     pa = torch.from_numpy(a).pin_memory().numpy()
     pa2 = torch.from_numpy(a2).pin_memory().numpy()
     out = torch.empty(want.shape, dtype=torch.float64).pin_memory().numpy()
-    for img, ref in ((pa, want), (pa, want), (pa, want), (pa2, want2), (pa, want), (a2, want2), (pa, want)):
-        out[:] = -1
-        t.lookup(img, out=out)
-        assert np.array_equal(out, ref)
-    p.gpu_tile = 64
-    for _ in range(3):
-        assert np.array_equal(t.lookup(pa), want)
-    old = ptb.set_host_threads(1)
+    old = ptb.set_host_threads(0)
     try:
-        assert np.array_equal(t.lookup(pa), want)
+        for threads in (0, 1, 3, -1):
+            ptb.set_host_threads(threads)
+            for img, ref in ((pa, want), (pa, want), (pa2, want2), (a2, want2), (pa, want)):
+                out[:] = -1
+                t.lookup(img, out=out)
+                assert np.array_equal(out, ref), threads
+            assert np.array_equal(t.lookup(a2), want2)
+            per_patch = 24 if threads < 0 else 8
+            assert t.last_transfer() == (a.nbytes, per_patch * want.shape[0] * want.shape[1])
     finally:
         ptb.set_host_threads(old)
-    assert t.last_transfer() == (a.nbytes, 8 * want.shape[0] * want.shape[1])
     t.close()
