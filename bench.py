@@ -8,7 +8,7 @@ the reference's default parameters plus -speed 3 -coherence_spatial 4.  One step
 built once before warm-up.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-  python bench.py --profile-case query|query-default|infer|build  (short fixed runs for ncu)
+  python bench.py --profile-case query|query-default|infer|build|build-c2  (short fixed runs for ncu)
 
 Prints one JSON line (rank 0).  `value` is query patches per second of device time (one CUDA event
 pair around each pt_table_lookup_device call) with a already
@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
-    ap.add_argument("--profile-case", choices=["query", "query-default", "infer", "build"], default=None)
+    ap.add_argument("--profile-case", choices=["query", "query-default", "infer", "build", "build-c2"], default=None)
     return ap.parse_args()
 
 
@@ -199,12 +199,12 @@ def profile_case(name):
     from patchtable_b200 import synth
     ctypes.CDLL(None).srand(1)
     st = torch.cuda.current_stream().cuda_stream
-    if name == "build":
-        h, w = 540, 960
+    if name in ("build", "build-c2"):
+        h, w = (540, 960) if name == "build" else (WORKLOAD["h"], WORKLOAD["w"])
         a, b = synth.pair(h, w, 2)
         t = ptb.PatchTable(ptb.PatchTableParams(WORKLOAD["switches"]), b)
         torch.cuda.synchronize()
-        print("profile case build: %d cells" % t.shape()[1])
+        print("profile case %s: %d cells, stages %s" % (name, t.shape()[1], t.build_profile()))
         return
     if name in ("query", "query-default"):
         a, b = make_inputs()
