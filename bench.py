@@ -355,6 +355,39 @@ def uneven_batch_measure():
             "schedules": rows}
 
 
+def uneven_batch_sharded(dev, world, rank):
+    """The 64-image batch split by image over the ranks (cost-balanced by patch count): every rank
+    builds the table and answers its share as one batched query (graph replay, 1 pass / jump 2 /
+    1 pull candidate); the whole job's rate is all patches over the slowest rank's time."""
+    import torch
+    import patchtable_b200 as ptb
+    from patchtable_b200 import replicas, synth
+    table_img, queries = synth.uneven_batch()
+    costs = [(q.shape[0] - 7) * (q.shape[1] - 7) for q in queries]
+    mine = replicas.shard_by_cost(costs, world)[rank]
+    params = ptb.PatchTableParams(WORKLOAD["switches"])
+    ctypes.CDLL(None).srand(1)
+    table = ptb.PatchTable(params, table_img)
+    params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = SCHEDULES[0]
+    qs = [queries[i] for i in mine]
+    qb = table.batch([q.shape[:2] for q in qs])
+    rgb = torch.empty(qb.pixels * 3, dtype=torch.float32, device=dev)
+    for q, o in zip(qs, qb.pixel_offset):
+        rgb[3 * o:3 * o + q.size] = torch.from_numpy(q.ravel()).to(dev)
+    ann = torch.empty(qb.patches * 3, dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream().cuda_stream
+    qb.set_tile(32)
+    qb.capture(rgb.data_ptr(), ann.data_ptr(), st)
+    replicas.barrier()
+    ms = _event_ms(lambda: qb.replay(st), 3)
+    slow = replicas.max_over_ranks(ms, dev)
+    qb.close()
+    table.close()
+    return {"images": len(queries), "patches": sum(costs), "ranks": world, "my_images": len(mine),
+            "slowest_rank_ms": slow, "patches_per_s": sum(costs) / (slow / 1000.0),
+            "split": "by image, most patches first to the least-loaded rank"}
+
+
 def one_vs_many_measure():
     """One 1024x768 query against 10 database images (sides U[256, 2048]) packed into one atlas
     table, seam-straddling patches excluded by the allowed mask."""
@@ -552,12 +585,15 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(a, b)
-    c4 = c3 = None
-    if rank == 0 and not args.no_batch:
+    c4 = c3 = c4s = None
+    if not args.no_batch:
         del flush
         torch.cuda.empty_cache()
-        c4 = uneven_batch_measure()
-        c3 = one_vs_many_measure()
+        if world > 1:
+            c4s = uneven_batch_sharded(dev, world, rank)
+        elif rank == 0:
+            c4 = uneven_batch_measure()
+            c3 = one_vs_many_measure()
 
     replicas.finish()
     if rank != 0:
@@ -575,7 +611,7 @@ def main():
                                 "patches_per_cta": params.gpu_tile, "patches_per_cta_ms": {str(k): v for k, v in tile_ms.items()},
                                 "rule": "fastest schedule with mean NNF dist <= 1.01 x the reference's on this workload"},
                    "library_default_schedule": default_sched, "learned": learned,
-                   "uneven_batch": c4, "one_vs_many": c3, "mean_nnf_dist_timed": md_timed,
+                   "uneven_batch": c4, "uneven_batch_sharded": c4s, "one_vs_many": c3, "mean_nnf_dist_timed": md_timed,
                    "l2": "flushed between steps (256 MiB write)", "parallelism": "replicas" if world > 1 else "single",
                    "timing": "one CUDA event pair around each pt_table_lookup_device call on its stream",
                    "step_ms": {"min": min(step_ms), "median": float(np.median(step_ms)), "max": max(step_ms)},

@@ -2,7 +2,8 @@
 
 The query path shards without any exchange: query patches are independent given the table and
 separate images need nothing from each other, so every rank builds its own table and answers its
-own queries.  The only collective steps are the host-side agreements of a run -- a barrier around
+own queries -- the same workload on every rank (replicas), or its share of a set of images
+(shard_by_cost) when the images are the work.  The only collective steps are the host-side agreements of a run -- a barrier around
 the timed region, the slowest rank's time, and rank 0's choice of a setting -- which every rank
 takes in the same order.  The same helpers run on CPU with the gloo backend.
 """
@@ -59,6 +60,20 @@ def agree(x: float, device="cpu") -> float:
     t = torch.tensor([float(x)], dtype=torch.float64, device=device)
     dist.broadcast(t, src=0)
     return float(t.item())
+
+
+def shard_by_cost(costs, world: int):
+    """Splits items with the given costs (e.g. query patches per image) over `world` ranks: the
+    most expensive first, each to the rank with the least total so far (ties: lowest rank), so the
+    largest share exceeds the mean by less than one item.  Returns one sorted index list per rank;
+    every rank computes the same split without communicating."""
+    load = [0] * world
+    shards = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda k: (-costs[k], k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        shards[r].append(i)
+        load[r] += costs[i]
+    return [sorted(s) for s in shards]
 
 
 def whole_job_rate(units_per_rank: float, seconds: float, world: int) -> float:
