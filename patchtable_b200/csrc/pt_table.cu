@@ -788,15 +788,33 @@ int band_rows(const pt_table *t, int h, int w) {
 
 /* Enqueues the band pipeline on the table's streams, starting after the work queued on t->st and
    joining every stream back into t->st at the end.  ev_d[b] marks band b's download. */
-pt_status enqueue_bands(pt_table *t, const float *a, double *ann_out, int h, int w, int B, int nb, bool widen) {
+/* Where a band pipeline's input comes from and its output goes: a host image uploaded band by band
+   into the table's buffer (a set) or a device image (d_in set); the packed field downloaded for
+   host widening (widen), the float64 records downloaded to ann_out, or -- d_out set -- written by
+   the pull to device memory and not downloaded. */
+struct BandIO {
+    const float *a = nullptr;
+    const float *d_in = nullptr;
+    double *ann_out = nullptr;
+    double *d_out = nullptr;
+    bool widen = false;
+    cudaStream_t origin = nullptr;    /* the pipeline starts after and joins into this stream */
+};
+
+pt_status enqueue_bands(pt_table *t, const BandIO &io, int h, int w, int B, int nb) {
     const pt_params &p = t->p;
     const int eh = h - 7, ew = w - 7;
     const long long P = (long long) eh * ew;
+    const float *a = io.a;
+    double *ann_out = io.ann_out;
+    const bool widen = io.widen;
+    const float *rgb = io.d_in ? io.d_in : t->q_rgb.p;
     cudaEvent_t *ev_in = t->band_ev.data(), *ev_a = ev_in + nb, *ev_b = ev_a + nb, *ev_c = ev_b + nb, *ev_d = ev_c + nb;
     cudaEvent_t ev_start = t->band_ev[5 * nb], *ev_join = &t->band_ev[5 * nb + 1];
     cudaStream_t sa = t->st, sb = t->st_choose, sc = t->st_pull;
-    PT_CUDA(cudaEventRecord(ev_start, sa));
-    for (cudaStream_t s2 : {t->st_in, sb, sc, t->st_out}) PT_CUDA(cudaStreamWaitEvent(s2, ev_start, 0));
+    PT_CUDA(cudaEventRecord(ev_start, io.origin));
+    for (cudaStream_t s2 : {sa, t->st_in, sb, sc, t->st_out})
+        if (s2 != io.origin) PT_CUDA(cudaStreamWaitEvent(s2, ev_start, 0));
     QuerySetup qs;
     qs.aw = w; qs.ah = h; qs.bw = t->w; qs.bh = t->h;
     qs.prop_scale = 1.0 / (1 + p.coherence_spatial);
@@ -818,10 +836,12 @@ pt_status enqueue_bands(pt_table *t, const float *a, double *ann_out, int h, int
             const int r0 = b * B, r1 = std::min(eh, r0 + B);
             const int p0 = b == 0 ? 0 : r0 + 7, p1 = b == nb - 1 ? h : r1 + 7;
             const size_t px0 = (size_t) p0 * w * 3, npx = (size_t) (p1 - p0) * w * 3;
-            PT_CUDA(cudaMemcpyAsync(t->q_rgb.p + px0, a + px0, sizeof(float) * npx, cudaMemcpyHostToDevice, t->st_in));
-            PT_CUDA(cudaEventRecord(ev_in[b], t->st_in));
-            PT_CUDA(cudaStreamWaitEvent(sa, ev_in[b], 0));
-            PT_TRY(pt_launch_descriptor_cells(p.ndims, p.nchroma, t->q_rgb.p, h, w, pt_color_mode(p), t->q_rgba.p,
+            if (a) {
+                PT_CUDA(cudaMemcpyAsync(t->q_rgb.p + px0, a + px0, sizeof(float) * npx, cudaMemcpyHostToDevice, t->st_in));
+                PT_CUDA(cudaEventRecord(ev_in[b], t->st_in));
+                PT_CUDA(cudaStreamWaitEvent(sa, ev_in[b], 0));
+            }
+            PT_TRY(pt_launch_descriptor_cells(p.ndims, p.nchroma, rgb, h, w, pt_color_mode(p), t->q_rgba.p,
                                               t->bins, t->to_bin.p, t->table.p, t->q_tcand.p, r0 / 8, (r1 - r0 + 7) / 8, sa));
             PT_CUDA(cudaEventRecord(ev_a[b], sa));
         }
@@ -845,12 +865,14 @@ pt_status enqueue_bands(pt_table *t, const float *a, double *ann_out, int h, int
             qb.stream = sc;
             /* the pull writes the band's final field: packed position and float distance, or
                (without host widening) the float64 records */
-            if (!widen) qb.ann = t->q_ann.p;
+            if (io.d_out) qb.ann = io.d_out;
+            else if (!widen) qb.ann = t->q_ann.p;
             PT_TRY(pt_launch_pull(qb, (int) P, t->q_rgba.p, t->b_rgba.p, nullptr, nullptr, t->q_chpos.p, t->q_chd.p,
                                   t->q_pos[1].p, t->q_d[1].p, nullptr, sc));
             const size_t o = (size_t) r0 * ew;
             const size_t n = (size_t) (r1 - r0) * ew;
             PT_CUDA(cudaEventRecord(ev_c[b - 2], sc));
+            if (io.d_out) continue;
             PT_CUDA(cudaStreamWaitEvent(t->st_out, ev_c[b - 2], 0));
             if (widen) {
                 PT_CUDA(cudaMemcpyAsync(t->h_pos.p + o, t->q_pos[1].p + o, sizeof(int) * n, cudaMemcpyDeviceToHost, t->st_out));
@@ -863,12 +885,20 @@ pt_status enqueue_bands(pt_table *t, const float *a, double *ann_out, int h, int
         }
     }
     int k = 0;
-    for (cudaStream_t s2 : {t->st_in, sb, sc, t->st_out}) {
+    for (cudaStream_t s2 : {sa, t->st_in, sb, sc, t->st_out}) {
+        if (s2 == io.origin) continue;
         PT_CUDA(cudaEventRecord(ev_join[k], s2));
-        PT_CUDA(cudaStreamWaitEvent(sa, ev_join[k], 0));
+        PT_CUDA(cudaStreamWaitEvent(io.origin, ev_join[k], 0));
         k++;
     }
     return PT_OK;
+}
+
+/* Lookups that run as a band pipeline: the plain single-table query of one pass with
+   propagation, from the default field, on images of at least 64 patch rows. */
+bool banded_schedule(const pt_table *t, int h) {
+    return !t->desc_mode && !t->pca && t->subs.empty() && !t->p.init_random && pt_default_passes(t->p) == 1 &&
+           t->p.do_prop && h - 7 >= 64;
 }
 
 pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_out) {
@@ -878,7 +908,7 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     for (cudaStream_t *sp : {&t->st_in, &t->st_out, &t->st_choose, &t->st_pull})
         if (!*sp) PT_CUDA(cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking));
     const int B = band_rows(t, h, w), nb = (eh + B - 1) / B;
-    while ((int) t->band_ev.size() < 5 * nb + 5) {
+    while ((int) t->band_ev.size() < 5 * nb + 6) {
         cudaEvent_t e;
         PT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         t->band_ev.push_back(e);
@@ -890,7 +920,12 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     } else {
         PT_CUDA(t->q_ann.reserve((size_t) P * 3));
     }
-    PT_TRY(enqueue_bands(t, a, ann_out, h, w, B, nb, widen));
+    BandIO io;
+    io.a = a;
+    io.ann_out = ann_out;
+    io.widen = widen;
+    io.origin = t->st;
+    PT_TRY(enqueue_bands(t, io, h, w, B, nb));
     t->last_h2d = (long long) sizeof(float) * h * w * 3;
     t->last_d2h = (long long) (widen ? sizeof(int) + sizeof(float) : 3 * sizeof(double)) * P;
     /* widen each band as soon as it has arrived */
@@ -903,6 +938,28 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     }
     PT_CUDA(cudaStreamSynchronize(t->st));
     return PT_OK;
+}
+
+/* The device lookup of a one-pass schedule as the same band pipeline without copies: the
+   descriptor pass of band b+1, the choose of band b and the pull of band b-1 run on three streams,
+   so the issue-bound descriptor work and the memory-bound query kernels share the SMs and no
+   kernel waits for another's last wave; the pull writes the float64 NNF. */
+pt_status lookup_banded_device(pt_table *t, const float *d_a, int h, int w, double *d_ann, cudaStream_t st) {
+    const int eh = h - 7;
+    PT_TRY(ensure_query_buffers(t, h, w));
+    for (cudaStream_t *sp : {&t->st_in, &t->st_out, &t->st_choose, &t->st_pull})
+        if (!*sp) PT_CUDA(cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking));
+    const int B = band_rows(t, h, w), nb = (eh + B - 1) / B;
+    while ((int) t->band_ev.size() < 5 * nb + 6) {
+        cudaEvent_t e;
+        PT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        t->band_ev.push_back(e);
+    }
+    BandIO io;
+    io.d_in = d_a;
+    io.d_out = d_ann;
+    io.origin = st;
+    return enqueue_bands(t, io, h, w, B, nb);
 }
 
 /* lookup_device with stage events; stage_ms[nst] receives summed stage times, counters[nctr] the
@@ -1222,8 +1279,7 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int ih, int iw, double *a
         if (seconds) *seconds = now_s() - T0;
         return PT_OK;
     }
-    if (!t->desc_mode && !t->pca && t->subs.empty() && !t->p.init_random && pt_default_passes(t->p) == 1 && t->p.do_prop &&
-        h - 7 >= 64) {
+    if (banded_schedule(t, h)) {
         PT_TRY(lookup_banded(t, a, h, w, ann_out));
         if (seconds) *seconds = now_s() - T0;
         return PT_OK;
@@ -1259,6 +1315,8 @@ pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int ih, int iw, 
     if (!t || !d_a || !d_ann) return pt_fail(PT_BAD_ARG, "null argument");
     int h, w;
     PT_TRY(query_dims(t, ih, iw, h, w));
+    if (banded_schedule(t, h))
+        return lookup_banded_device(t, d_a, h, w, d_ann, (cudaStream_t) stream);
     return lookup_device(t, d_a, h, w, d_ann, (cudaStream_t) stream);
 }
 

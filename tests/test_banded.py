@@ -1,6 +1,7 @@
-"""The host lookup of one-pass schedules streams the image through bands of rows (uploads and
-downloads overlapped with the kernels).  Its NNF must equal the whole-image device lookup's bit
-for bit, for every image shape, band remainder and propagation radius."""
+"""Lookups of one-pass schedules stream the image through bands of rows: the host lookup overlaps
+uploads and downloads with the kernels, and the device lookup overlaps the bands' kernels on three
+streams.  Both NNFs must equal the whole-image launch sequence's bit for bit, for every image
+shape, band remainder and propagation radius."""
 import numpy as np
 import pytest
 
@@ -11,13 +12,20 @@ pytestmark = pytest.mark.gpu
 
 
 def _device(t, a):
+    """The whole-image launch sequence (the diagnostic entry point runs it unbanded), and the device
+    entry point, which runs one-pass schedules as a band pipeline: both must agree."""
     import torch
     h, w = a.shape[:2]
     da = torch.from_numpy(np.ascontiguousarray(a)).cuda()
     ann = torch.empty((h - 7, w - 7, 3), dtype=torch.float64, device="cuda")
-    t.lookup_device(da.data_ptr(), h, w, ann.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    st = torch.cuda.current_stream().cuda_stream
+    t.lookup_profile(da.data_ptr(), h, w, ann.data_ptr(), st)
+    whole = ann.cpu().numpy()
+    ann.fill_(-1)
+    t.lookup_device(da.data_ptr(), h, w, ann.data_ptr(), st)
     torch.cuda.synchronize()
-    return ann.cpu().numpy()
+    assert np.array_equal(ann.cpu().numpy(), whole)
+    return whole
 
 
 @pytest.mark.parametrize("h,w,sw", [
