@@ -91,11 +91,14 @@ __global__ void k_inner_box(int first, int count, int nd, float *lo, float *hi) 
 }
 
 /* Squared distance from q to a box, rounded down enough to be a lower bound of the squared distance. */
-__device__ __forceinline__ float box_lb(const float *q, const float *lo, const float *hi, int nd) {
+__device__ __forceinline__ float box_lb(const float (&q)[PT_DESC_MAX], const float *lo, const float *hi, int nd) {
     float s = 0.f;
-    for (int d = 0; d < nd; d++) {
-        float e = fmaxf(fmaxf(lo[d] - q[d], q[d] - hi[d]), 0.f);
-        s += e * e;
+#pragma unroll
+    for (int d = 0; d < PT_DESC_MAX; d++) {          /* unrolled: q stays in registers */
+        if (d < nd) {
+            float e = fmaxf(fmaxf(lo[d] - q[d], q[d] - hi[d]), 0.f);
+            s += e * e;
+        }
     }
     return s * (1.0f - 1e-5f);
 }
@@ -111,13 +114,13 @@ __device__ __forceinline__ bool before(float d, int i, float d2, int i2) { retur
 constexpr int KNN_STACK = 64;
 constexpr int PSTRIDE = PT_DESC_MAX + 1;            /* staged point stride (odd: no bank conflicts) */
 
-template<int K>
+template<int K, int NV>
 __global__ void __launch_bounds__(NT)
 k_knn_warp(const float *__restrict__ sp, const int *__restrict__ sidx, int N, int nd, int L,
            const float *__restrict__ lo, const float *__restrict__ hi, const float *__restrict__ qdesc,
            const int *__restrict__ qorder, int Q, int *out) {
     __shared__ int stk_s[NT / 32][KNN_STACK];
-    __shared__ float pts_s[NT / 32][BUCKET * PSTRIDE];
+    __shared__ float4 pts_s[NT / 32][BUCKET * NV];       /* a leaf's points, NV float4 each (zero-padded) */
     __shared__ int pid_s[NT / 32][BUCKET];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -132,7 +135,7 @@ k_knn_warp(const float *__restrict__ sp, const int *__restrict__ sidx, int N, in
 #pragma unroll
     for (int j = 0; j < K; j++) { kd[j] = __int_as_float(0x7f800000); ki[j] = 0x7fffffff; }
     int *stk = stk_s[wid];
-    float *pts = pts_s[wid];
+    float4 *pts = pts_s[wid];
     int *pid = pid_s[wid];
     if (lane == 0) stk[0] = 1;
     __syncwarp();
@@ -148,21 +151,33 @@ k_knn_warp(const float *__restrict__ sp, const int *__restrict__ sidx, int N, in
             const int cnt = min(BUCKET, N - base);
             if (lane < cnt) {
                 const float *src = sp + (size_t) (base + lane) * nd;
-                for (int d = 0; d < nd; d++) pts[lane * PSTRIDE + d] = src[d];
+                float v[4 * NV];
+#pragma unroll
+                for (int d = 0; d < 4 * NV; d++) v[d] = d < nd ? src[d] : 0.f;
+#pragma unroll
+                for (int u = 0; u < NV; u++) pts[lane * NV + u] = make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
                 pid[lane] = sidx[base + lane];
             }
             __syncwarp();
             if (want) {
                 for (int m = 0; m < cnt; m++) {
-                    const float *pv = pts + m * PSTRIDE;
+                    /* every lane reads the same point: 16-byte broadcasts; the partial sum after
+                       the first four dimensions already rejects most points (it only grows) */
                     float dsum = 0.f;
 #pragma unroll
-                    for (int d = 0; d < PT_DESC_MAX; d++) {
-                        if (d < nd) {
-                            const float e = __fsub_rn(qv[d], pv[d]);
-                            dsum = __fadd_rn(dsum, __fmul_rn(e, e));
+                    for (int u = 0; u < NV; u++) {
+                        const float4 pv = pts[m * NV + u];
+                        const float pc[4] = {pv.x, pv.y, pv.z, pv.w};
+#pragma unroll
+                        for (int c = 0; c < 4; c++) {
+                            if (4 * u + c < nd) {
+                                const float e = __fsub_rn(qv[4 * u + c], pc[c]);
+                                dsum = __fadd_rn(dsum, __fmul_rn(e, e));
+                            }
                         }
+                        if (u == 0 && dsum > kd[K - 1]) break;
                     }
+                    if (dsum > kd[K - 1]) continue;
                     const int id = pid[m];
                     if (!before(dsum, id, kd[K - 1], ki[K - 1])) continue;
 #pragma unroll
@@ -384,7 +399,8 @@ pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, i
         PT_CUDA(cudaStreamSynchronize(st));
         return PT_OK;
     }
-#define PT_KNN_K(KK) case KK: k_knn_warp<KK><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
+#define PT_KNN_K(KK) case KK: if (nd <= 8) k_knn_warp<KK, 2><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); \
+        else k_knn_warp<KK, 4><<<grid, NT, 0, st>>>(sp.p, perm.p, N, nd, L, lo.p, hi.p, qdesc, qorder.p, Q, out); break;
     switch (K) {
         PT_KNN_K(12) PT_KNN_K(16) PT_KNN_K(24) PT_KNN_K(32) PT_KNN_K(48) PT_KNN_K(64)
         default: return pt_fail(PT_UNSUPPORTED, "knn K=%d", K);
