@@ -443,6 +443,16 @@ def main():
     H, W = a.shape[:2]
     P = (H - 7) * (W - 7)
     params = ptb.PatchTableParams(WORKLOAD["switches"])
+    # the first table of a process also loads the library's kernels onto the device: time it, then
+    # time the build again as every later table of the process runs it
+    ctypes.CDLL(None).srand(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    first = ptb.PatchTable(params, b)
+    torch.cuda.synchronize()
+    first_build_s = time.perf_counter() - t0
+    first.close()
+    del first
     ctypes.CDLL(None).srand(1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -603,7 +613,7 @@ def main():
         "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded generator, patchtable_b200/synth.py)",
         "config": {"workload": WORKLOAD["name"], "patches_per_step": P, "image": [H, W], "table_image": list(b.shape[:2]),
-                   "build_s": build_s, "build_stage_ms": build_stage_ms, "mean_nnf_dist": md, "mean_nnf_dist_e2e": md_e2e,
+                   "build_s": build_s, "build_stage_ms": build_stage_ms, "first_build_s": first_build_s, "mean_nnf_dist": md, "mean_nnf_dist_e2e": md_e2e,
                    "e2e_ms": {"mean": 1000 * sum(e2e_s) / len(e2e_s), "median": 1000 * float(np.median(e2e_s)),
                               "min": 1000 * min(e2e_s), "max": 1000 * max(e2e_s), "calls": len(e2e_s)},
                    "reference_mean_nnf_dist": ref_md,

@@ -751,7 +751,9 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
    position, float32 distance: 8 bytes per patch instead of the float64 record's 24) into pinned
    staging; once a band has arrived, the host threads widen it into the caller's float64 buffer
    while later bands are still computed and copied.  The launches are enqueued directly: replaying
-   the same sequence as a recorded CUDA graph measured slower (1.45 against 1.29 ms at 1080p). */
+   the same sequence as a recorded CUDA graph measured slower (1.45 against 1.29 ms at 1080p).
+   Device-resident lookups keep the whole-image launches: the same bands on three streams without
+   copies measured 1.10 against 0.98 ms. */
 int band_rows(const pt_table *t, int h, int w) {
     const pt_params &p = t->p;
     const int eh = h - 7, ew = w - 7;
@@ -788,15 +790,12 @@ int band_rows(const pt_table *t, int h, int w) {
 
 /* Enqueues the band pipeline on the table's streams, starting after the work queued on t->st and
    joining every stream back into t->st at the end.  ev_d[b] marks band b's download. */
-/* Where a band pipeline's input comes from and its output goes: a host image uploaded band by band
-   into the table's buffer (a set) or a device image (d_in set); the packed field downloaded for
-   host widening (widen), the float64 records downloaded to ann_out, or -- d_out set -- written by
-   the pull to device memory and not downloaded. */
+/* A band pipeline's host image (uploaded band by band into the table's buffer) and its output:
+   the packed field downloaded for host widening (widen) or the float64 records downloaded to
+   ann_out. */
 struct BandIO {
     const float *a = nullptr;
-    const float *d_in = nullptr;
     double *ann_out = nullptr;
-    double *d_out = nullptr;
     bool widen = false;
     cudaStream_t origin = nullptr;    /* the pipeline starts after and joins into this stream */
 };
@@ -808,7 +807,7 @@ pt_status enqueue_bands(pt_table *t, const BandIO &io, int h, int w, int B, int 
     const float *a = io.a;
     double *ann_out = io.ann_out;
     const bool widen = io.widen;
-    const float *rgb = io.d_in ? io.d_in : t->q_rgb.p;
+    const float *rgb = t->q_rgb.p;
     cudaEvent_t *ev_in = t->band_ev.data(), *ev_a = ev_in + nb, *ev_b = ev_a + nb, *ev_c = ev_b + nb, *ev_d = ev_c + nb;
     cudaEvent_t ev_start = t->band_ev[5 * nb], *ev_join = &t->band_ev[5 * nb + 1];
     cudaStream_t sa = t->st, sb = t->st_choose, sc = t->st_pull;
@@ -836,11 +835,9 @@ pt_status enqueue_bands(pt_table *t, const BandIO &io, int h, int w, int B, int 
             const int r0 = b * B, r1 = std::min(eh, r0 + B);
             const int p0 = b == 0 ? 0 : r0 + 7, p1 = b == nb - 1 ? h : r1 + 7;
             const size_t px0 = (size_t) p0 * w * 3, npx = (size_t) (p1 - p0) * w * 3;
-            if (a) {
-                PT_CUDA(cudaMemcpyAsync(t->q_rgb.p + px0, a + px0, sizeof(float) * npx, cudaMemcpyHostToDevice, t->st_in));
-                PT_CUDA(cudaEventRecord(ev_in[b], t->st_in));
-                PT_CUDA(cudaStreamWaitEvent(sa, ev_in[b], 0));
-            }
+            PT_CUDA(cudaMemcpyAsync(t->q_rgb.p + px0, a + px0, sizeof(float) * npx, cudaMemcpyHostToDevice, t->st_in));
+            PT_CUDA(cudaEventRecord(ev_in[b], t->st_in));
+            PT_CUDA(cudaStreamWaitEvent(sa, ev_in[b], 0));
             PT_TRY(pt_launch_descriptor_cells(p.ndims, p.nchroma, rgb, h, w, pt_color_mode(p), t->q_rgba.p,
                                               t->bins, t->to_bin.p, t->table.p, t->q_tcand.p, r0 / 8, (r1 - r0 + 7) / 8, sa));
             PT_CUDA(cudaEventRecord(ev_a[b], sa));
@@ -865,14 +862,12 @@ pt_status enqueue_bands(pt_table *t, const BandIO &io, int h, int w, int B, int 
             qb.stream = sc;
             /* the pull writes the band's final field: packed position and float distance, or
                (without host widening) the float64 records */
-            if (io.d_out) qb.ann = io.d_out;
-            else if (!widen) qb.ann = t->q_ann.p;
+            if (!widen) qb.ann = t->q_ann.p;
             PT_TRY(pt_launch_pull(qb, (int) P, t->q_rgba.p, t->b_rgba.p, nullptr, nullptr, t->q_chpos.p, t->q_chd.p,
                                   t->q_pos[1].p, t->q_d[1].p, nullptr, sc));
             const size_t o = (size_t) r0 * ew;
             const size_t n = (size_t) (r1 - r0) * ew;
             PT_CUDA(cudaEventRecord(ev_c[b - 2], sc));
-            if (io.d_out) continue;
             PT_CUDA(cudaStreamWaitEvent(t->st_out, ev_c[b - 2], 0));
             if (widen) {
                 PT_CUDA(cudaMemcpyAsync(t->h_pos.p + o, t->q_pos[1].p + o, sizeof(int) * n, cudaMemcpyDeviceToHost, t->st_out));
@@ -938,28 +933,6 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     }
     PT_CUDA(cudaStreamSynchronize(t->st));
     return PT_OK;
-}
-
-/* The device lookup of a one-pass schedule as the same band pipeline without copies: the
-   descriptor pass of band b+1, the choose of band b and the pull of band b-1 run on three streams,
-   so the issue-bound descriptor work and the memory-bound query kernels share the SMs and no
-   kernel waits for another's last wave; the pull writes the float64 NNF. */
-pt_status lookup_banded_device(pt_table *t, const float *d_a, int h, int w, double *d_ann, cudaStream_t st) {
-    const int eh = h - 7;
-    PT_TRY(ensure_query_buffers(t, h, w));
-    for (cudaStream_t *sp : {&t->st_in, &t->st_out, &t->st_choose, &t->st_pull})
-        if (!*sp) PT_CUDA(cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking));
-    const int B = band_rows(t, h, w), nb = (eh + B - 1) / B;
-    while ((int) t->band_ev.size() < 5 * nb + 6) {
-        cudaEvent_t e;
-        PT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        t->band_ev.push_back(e);
-    }
-    BandIO io;
-    io.d_in = d_a;
-    io.d_out = d_ann;
-    io.origin = st;
-    return enqueue_bands(t, io, h, w, B, nb);
 }
 
 /* lookup_device with stage events; stage_ms[nst] receives summed stage times, counters[nctr] the
@@ -1315,8 +1288,6 @@ pt_status pt_table_lookup_device(pt_table *t, const float *d_a, int ih, int iw, 
     if (!t || !d_a || !d_ann) return pt_fail(PT_BAD_ARG, "null argument");
     int h, w;
     PT_TRY(query_dims(t, ih, iw, h, w));
-    if (banded_schedule(t, h))
-        return lookup_banded_device(t, d_a, h, w, d_ann, (cudaStream_t) stream);
     return lookup_device(t, d_a, h, w, d_ann, (cudaStream_t) stream);
 }
 

@@ -1,7 +1,6 @@
-"""Lookups of one-pass schedules stream the image through bands of rows: the host lookup overlaps
-uploads and downloads with the kernels, and the device lookup overlaps the bands' kernels on three
-streams.  Both NNFs must equal the whole-image launch sequence's bit for bit, for every image
-shape, band remainder and propagation radius."""
+"""The host lookup of one-pass schedules streams the image through bands of rows (uploads and
+downloads overlapped with the kernels).  Its NNF must equal the whole-image device lookup's bit
+for bit, for every image shape, band remainder and propagation radius."""
 import numpy as np
 import pytest
 
@@ -12,8 +11,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _device(t, a):
-    """The whole-image launch sequence (the diagnostic entry point runs it unbanded), and the device
-    entry point, which runs one-pass schedules as a band pipeline: both must agree."""
+    """The whole-image launch sequence, through the diagnostic and the device entry points."""
     import torch
     h, w = a.shape[:2]
     da = torch.from_numpy(np.ascontiguousarray(a)).cuda()
