@@ -20,6 +20,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "patchtable_b200.h"
@@ -110,6 +111,7 @@ struct pt_table {
     DevBuf<float> pca_mean, pca_basis;
     cudaStream_t st = nullptr;
     bool own_stream = false;
+    cudaStream_t st2 = nullptr;       /* the build's second stream (range and partition) */
     DevBuf<float4> b_rgba;
     DevBuf<float4> b_rgba1;           /* b_rgba shifted by one pixel, b_rgba1[i] = b_rgba[i + 1] */
     DevBuf<float> b_desc;
@@ -164,6 +166,7 @@ struct pt_table {
         if (st_choose) cudaStreamDestroy(st_choose);
         if (st_pull) cudaStreamDestroy(st_pull);
         if (own_stream && st) cudaStreamDestroy(st);
+        if (st2) cudaStreamDestroy(st2);
     }
 };
 
@@ -197,9 +200,9 @@ pt_status check_params(const pt_params *p, int h, int w) {
     return PT_OK;
 }
 
-pt_status upload_partition(pt_table *t);
+pt_status upload_partition(pt_table *t, cudaStream_t st);
 
-pt_status build_partition(pt_table *t) {
+pt_status build_partition(pt_table *t, cudaStream_t st) {
     const int G = t->G;
     t->part.assign(G, PtPartition());
     for (int d = 0; d < G; d++) {
@@ -214,7 +217,7 @@ pt_status build_partition(pt_table *t) {
         int N = 0;
         std::vector<float> vals;
         PT_TRY(pt_quantile_values(t->b_desc.p, t->ds, d, t->eh, t->ew, t->p.partition_step, t->allowed.p,
-                                  t->p.allowed_index, {}, vals, &N, t->st));
+                                  t->p.allowed_index, {}, vals, &N, st));
         if (N < 1) return pt_fail(PT_BAD_ARG, "no allowed patches to build a table from");
         std::vector<int> want;
         want.reserve(2 * ns);
@@ -224,7 +227,7 @@ pt_status build_partition(pt_table *t) {
         }
         int N2 = 0;
         PT_TRY(pt_quantile_values(t->b_desc.p, t->ds, d, t->eh, t->ew, t->p.partition_step, t->allowed.p,
-                                  t->p.allowed_index, want, vals, &N2, t->st));
+                                  t->p.allowed_index, want, vals, &N2, st));
         P.centers.resize(ns);
         P.lsizes.resize(ns);
         P.rsizes.resize(ns);
@@ -257,17 +260,17 @@ pt_status build_partition(pt_table *t) {
             P.to_bin[i] = (coord < mid) ? prev_c : next_c;
         }
     }
-    return upload_partition(t);
+    return upload_partition(t, st);
 }
 
 /* Device copies of the partition: the to_bin tables, the centres / sizes the proposal features
    read, and the per-dimension get_bin parameters. */
-pt_status upload_partition(pt_table *t) {
+pt_status upload_partition(pt_table *t, cudaStream_t st) {
     const int G = t->G;
     std::vector<int> flat((size_t) G * PT_NMAP);
     for (int d = 0; d < G; d++) std::copy(t->part[d].to_bin.begin(), t->part[d].to_bin.end(), flat.begin() + (size_t) d * PT_NMAP);
     PT_CUDA(t->to_bin.reserve(flat.size()));
-    PT_CUDA(cudaMemcpyAsync(t->to_bin.p, flat.data(), sizeof(int) * flat.size(), cudaMemcpyHostToDevice, t->st));
+    PT_CUDA(cudaMemcpyAsync(t->to_bin.p, flat.data(), sizeof(int) * flat.size(), cudaMemcpyHostToDevice, st));
     {
         std::vector<float> pd;
         for (int d = 0; d < G; d++) {
@@ -278,8 +281,8 @@ pt_status upload_partition(pt_table *t) {
             pd.insert(pd.end(), P.rsizes.begin(), P.rsizes.end());
         }
         PT_CUDA(t->part_dev.reserve(pd.size()));
-        PT_CUDA(cudaMemcpyAsync(t->part_dev.p, pd.data(), sizeof(float) * pd.size(), cudaMemcpyHostToDevice, t->st));
-        PT_CUDA(cudaStreamSynchronize(t->st));
+        PT_CUDA(cudaMemcpyAsync(t->part_dev.p, pd.data(), sizeof(float) * pd.size(), cudaMemcpyHostToDevice, st));
+        PT_CUDA(cudaStreamSynchronize(st));
     }
     memset(&t->bins, 0, sizeof(t->bins));
     t->bins.G = G;
@@ -442,53 +445,86 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
     }
     PT_TRY(stage_done(PT_BUILD_DESCRIPTOR));
 
-    /* k-coherence is computed before the table in the reference (patchtable.h:2653). */
-    if (p.kcoherence > 0) PT_TRY(build_kcoherence(t.get(), allowed_h));
-    PT_TRY(stage_done(PT_BUILD_KCOHERENCE));
-
-    /* set_min_max + set_nslices (patchtable.h:1758-1810, 2567-2582). */
-    t->min_val.assign(t->G, 0.f);
-    t->max_val.assign(t->G, 0.f);
-    PT_TRY(pt_launch_minmax(t->b_desc.p, t->ds, t->G, P, t->allowed.p, p.allowed_index, t->min_val.data(),
-                            t->max_val.data(), t->st));
-    t->range.resize(t->G);
-    for (int d = 0; d < t->G; d++) t->range[d] = t->max_val[d] - t->min_val[d];
-    std::vector<int> ns(t->G);
-    if (p.n_nslices == 0) {
-        float max_range = t->range[0];
-        for (int d = 1; d < t->G; d++) if (t->range[d] > max_range) max_range = t->range[d];
-        double scale = 200.0 / max_range;
-        for (int d = 0; d < t->G; d++) ns[d] = (int) (t->range[d] * scale);
-    } else {
-        if (p.n_nslices != t->G) return pt_fail(PT_BAD_ARG, "-nslices has %d entries, grid has %d dims", p.n_nslices, t->G);
-        for (int d = 0; d < t->G; d++) ns[d] = p.nslices[d];
-    }
-    t->nslices = scale_slices_to_limit(ns, p.limit);
-    t->stride.assign(t->G, 1);
-    t->ncells = 1;
-    for (int d = t->G - 1; d >= 0; d--) { t->stride[d] = t->ncells; t->ncells *= t->nslices[d]; }
-    if (t->ncells >= (1ll << 31)) return pt_fail(PT_UNSUPPORTED, "table of %lld cells exceeds 2^31", t->ncells);
-    PT_TRY(build_partition(t.get()));
-    PT_TRY(stage_done(PT_BUILD_PARTITION));
-
+    /* Three independent steps run at once, each on its own host thread: the k-coherence set on the
+       table's stream (computed before the table in the reference, patchtable.h:2653), the range and
+       partition on a second stream, and the populate order on the host.  Only the populate order
+       draws from rand(), as the reference's does at this point; nothing else draws meanwhile. */
+    auto timed = [](double &ms, auto &&fn) -> pt_status {
+        const double t0 = now_s();
+        const pt_status r = fn();
+        ms = 1000.0 * (now_s() - t0);
+        return r;
+    };
     /* Populate in std::random_shuffle order (patchtable.h:3142-3154): the permutation is drawn
        from the C library rand(), consuming it exactly as the reference does. */
     std::vector<int> order_xy, rank(P, -1);
-    order_xy.reserve(P);
-    for (int y = 0; y < t->eh; y++)
-        for (int x = 0; x < t->ew; x++)
-            if (host_allowed(allowed_h, p.allowed_index, y, x, t->ew)) order_xy.push_back(pt_xy(x + 7, y + 7));
-    if (order_xy.empty()) return pt_fail(PT_BAD_ARG, "no allowed patches");
-    if (p.populate_random)
-        for (size_t i = 1; i < order_xy.size(); i++) {
-            size_t j = (size_t) (rand() % (int) (i + 1));
-            if (i != j) std::swap(order_xy[i], order_xy[j]);
+    double shuffle_ms = 0.0;
+    std::thread shuffler([&] {
+        const double t0 = now_s();
+        order_xy.reserve(P);
+        for (int y = 0; y < t->eh; y++)
+            for (int x = 0; x < t->ew; x++)
+                if (host_allowed(allowed_h, p.allowed_index, y, x, t->ew)) order_xy.push_back(pt_xy(x + 7, y + 7));
+        if (p.populate_random)
+            for (size_t i = 1; i < order_xy.size(); i++) {
+                size_t j = (size_t) (rand() % (int) (i + 1));
+                if (i != j) std::swap(order_xy[i], order_xy[j]);
+            }
+        for (size_t i = 0; i < order_xy.size(); i++) {
+            int v = order_xy[i];
+            rank[(size_t) (pt_y(v) - 7) * t->ew + (pt_x(v) - 7)] = (int) i;
         }
-    for (size_t i = 0; i < order_xy.size(); i++) {
-        int v = order_xy[i];
-        rank[(size_t) (pt_y(v) - 7) * t->ew + (pt_x(v) - 7)] = (int) i;
+        shuffle_ms = 1000.0 * (now_s() - t0);
+    });
+    /* set_min_max + set_nslices (patchtable.h:1758-1810, 2567-2582), then the partition */
+    if (!t->st2) {
+        cudaError_t e = cudaStreamCreateWithFlags(&t->st2, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { shuffler.join(); return pt_fail(PT_CUDA_ERR, "stream: %s", cudaGetErrorString(e)); }
     }
-    PT_TRY(stage_done(PT_BUILD_SHUFFLE));
+    double part_ms = 0.0;
+    std::string part_err;
+    pt_status part_st = PT_OK;
+    std::thread partitioner([&] {
+        part_st = timed(part_ms, [&]() -> pt_status {
+            cudaStream_t s2 = t->st2;
+            t->min_val.assign(t->G, 0.f);
+            t->max_val.assign(t->G, 0.f);
+            PT_TRY(pt_launch_minmax(t->b_desc.p, t->ds, t->G, P, t->allowed.p, p.allowed_index, t->min_val.data(),
+                                    t->max_val.data(), s2));
+            t->range.resize(t->G);
+            for (int d = 0; d < t->G; d++) t->range[d] = t->max_val[d] - t->min_val[d];
+            std::vector<int> ns(t->G);
+            if (p.n_nslices == 0) {
+                float max_range = t->range[0];
+                for (int d = 1; d < t->G; d++) if (t->range[d] > max_range) max_range = t->range[d];
+                double scale = 200.0 / max_range;
+                for (int d = 0; d < t->G; d++) ns[d] = (int) (t->range[d] * scale);
+            } else {
+                if (p.n_nslices != t->G) return pt_fail(PT_BAD_ARG, "-nslices has %d entries, grid has %d dims", p.n_nslices, t->G);
+                for (int d = 0; d < t->G; d++) ns[d] = p.nslices[d];
+            }
+            t->nslices = scale_slices_to_limit(ns, p.limit);
+            t->stride.assign(t->G, 1);
+            t->ncells = 1;
+            for (int d = t->G - 1; d >= 0; d--) { t->stride[d] = t->ncells; t->ncells *= t->nslices[d]; }
+            if (t->ncells >= (1ll << 31)) return pt_fail(PT_UNSUPPORTED, "table of %lld cells exceeds 2^31", t->ncells);
+            PT_TRY(build_partition(t.get(), s2));
+            PT_CUDA(cudaStreamSynchronize(s2));
+            return PT_OK;
+        });
+        if (part_st != PT_OK) part_err = pt_last_error();
+    });
+    pt_status kc_st = PT_OK;
+    if (p.kcoherence > 0) kc_st = build_kcoherence(t.get(), allowed_h);
+    if (kc_st == PT_OK) kc_st = stage_done(PT_BUILD_KCOHERENCE);
+    partitioner.join();
+    shuffler.join();
+    t_mark = now_s();
+    if (kc_st != PT_OK) return kc_st;
+    if (part_st != PT_OK) return pt_fail(part_st, "%s", part_err.c_str());
+    t->build_ms[PT_BUILD_PARTITION] = part_ms;
+    t->build_ms[PT_BUILD_SHUFFLE] = shuffle_ms;
+    if (order_xy.empty()) return pt_fail(PT_BAD_ARG, "no allowed patches");
     {
         DevBuf<int> d_rank, d_order;
         PT_CUDA(d_rank.reserve(P));
@@ -1156,7 +1192,7 @@ pt_status load_impl(const pt_params *pin, const char *filename, pt_table **out) 
         t->max_val[d] = t->part[d].max_val;
         t->range[d] = t->part[d].range;
     }
-    PT_TRY(upload_partition(t.get()));
+    PT_TRY(upload_partition(t.get(), t->st));
     PT_CUDA(t->table.reserve(t->ncells));
     PT_CUDA(cudaMemcpyAsync(t->table.p, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice, t->st));
     PT_CUDA(cudaStreamSynchronize(t->st));
