@@ -22,6 +22,8 @@
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
+#include <vector>
+
 #include "pt_internal.h"
 #include "pt_descdist.cuh"
 #include "pt_kernels.h"
@@ -299,6 +301,60 @@ __global__ void k_kc_finish(const int *__restrict__ seg_start, int nseg, int Q, 
    (patch coords) of the train points.  Queries are train rows qrow[q] at positions qpos[q], in
    the reference's loop order, with output cell qcell[q] (index into the beh x bew grid).
    seg_start: first query of each segment.  kcoh receives beh x bew x kc (pos, dist bits). */
+namespace {
+
+/* The k-coherence index lists of a build without an allowed mask (build_kcoherence's loops):
+   train point i = patch (tx * fbs, ty * fbs) in raster order; query i = patch (qx * ks, qy * ks)
+   with its output cell; segment j starts at query row j / ncols, column cols[j % ncols]. */
+__global__ void k_kc_lists(int ew, int fbs, int ks, int ntx, int nqx, int N, int Q, int ncols, int nseg,
+                           const int *__restrict__ cols, int *trows, int *tpos, int *qrows, int *qpos, int *qcell, int *seg) {
+    const long long i = blockIdx.x * 256ll + threadIdx.x;
+    if (i < N) {
+        const int y = (int) (i / ntx) * fbs, x = (int) (i % ntx) * fbs;
+        trows[i] = y * ew + x;
+        tpos[i] = pt_xy(x, y);
+    }
+    if (i < Q) {
+        const int py = (int) (i / nqx) * ks, px = (int) (i % nqx) * ks;
+        qrows[i] = py * ew + px;
+        qpos[i] = pt_xy(px, py);
+        qcell[i] = (py / ks) * ew + px / ks;
+    }
+    if (i < nseg) seg[i] = (int) (i / ncols) * nqx + cols[i % ncols];
+}
+
+}  // namespace
+
+pt_status pt_kc_lists(int ew, int eh, int fbs, int ks, int reset, int *trows, int *tpos, int *qrows, int *qpos,
+                      int *qcell, int *seg, int *n_out, int *q_out, int *nseg_out, cudaStream_t st) {
+    const int ntx = (ew + fbs - 1) / fbs, nty = (eh + fbs - 1) / fbs;
+    const int nqx = (ew + ks - 1) / ks, nqy = (eh + ks - 1) / ks;
+    const long long N = (long long) ntx * nty, Q = (long long) nqx * nqy;
+    /* the columns where a segment starts: (x / ks) % reset == 0 with x = px + 7 in padded
+       coordinates (patchtable.h:2714); the first query always starts one */
+    std::vector<int> cols;
+    for (int qx = 0; qx < nqx; qx++)
+        if (((qx * ks + 7) / ks) % reset == 0) cols.push_back(qx);
+    if (cols.empty() || Q >= (1ll << 31) || N >= (1ll << 31))
+        return pt_fail(PT_UNSUPPORTED, "k-coherence index lists");    /* callers use the general path */
+    const bool first = cols[0] != 0;                                   /* query 0 opens a segment of its own */
+    const long long nseg = (long long) nqy * (long long) cols.size();
+    DevBuf<int> d_cols;
+    PT_CUDA(d_cols.reserve(cols.size()));
+    PT_CUDA(cudaMemcpyAsync(d_cols.p, cols.data(), sizeof(int) * cols.size(), cudaMemcpyHostToDevice, st));
+    const long long tot = std::max(std::max(N, Q), nseg);
+    k_kc_lists<<<(unsigned) ((tot + 255) / 256), 256, 0, st>>>(ew, fbs, ks, ntx, nqx, (int) N, (int) Q, (int) cols.size(),
+                                                           (int) nseg, d_cols.p, trows, tpos, qrows, qpos, qcell,
+                                                           seg + (first ? 1 : 0));
+    PT_LAUNCHED();
+    if (first) PT_CUDA(cudaMemsetAsync(seg, 0, sizeof(int), st));
+    PT_CUDA(cudaStreamSynchronize(st));           /* d_cols goes out of scope */
+    *n_out = (int) N;
+    *q_out = (int) Q;
+    *nseg_out = (int) nseg + (first ? 1 : 0);
+    return PT_OK;
+}
+
 pt_status pt_gather_rows(const float *desc, int ds, int nd, const int *rows, int n, float *out, cudaStream_t st) {
     long long tot = (long long) n * nd;
     k_gather_rows<<<(unsigned) ((tot + 255) / 256), 256, 0, st>>>(desc, ds, nd, rows, n, out);

@@ -80,6 +80,11 @@ pt_status pt_dt_brute(int *table, int G, const int *nslices, const float *part, 
 #define PT_KNN_WIDE_MAX 1024                 /* largest neighbour list of the k-coherence search */
 pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, int Q, int K, int *out, cudaStream_t st);
 pt_status pt_gather_rows(const float *desc, int ds, int nd, const int *rows, int n, float *out, cudaStream_t st);
+/* The k-coherence index lists of a build without an allowed mask, generated on the device (train
+   rows / positions, query rows / positions / cells, segment starts; buffers sized for every patch,
+   seg for every query + 1); PT_UNSUPPORTED when the general host path must be used. */
+pt_status pt_kc_lists(int ew, int eh, int fbs, int ks, int reset, int *trows, int *tpos, int *qrows, int *qpos,
+                      int *qcell, int *seg, int *n_out, int *q_out, int *nseg_out, cudaStream_t st);
 /* Exact distances from b_rgba (image mode) or, when bdesc is set, from the descriptor store
    (descriptor mode: ds floats per patch, ew patches per row). */
 pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *bdesc, int ds, int ew, const float *train, int N, int nd, const int *tpos,

@@ -301,6 +301,26 @@ bool host_allowed(const std::vector<int> &allowed, int idx, int py, int px, int 
 pt_status build_kcoherence(pt_table *t, const std::vector<int> &allowed) {
     const pt_params &p = t->p;
     const int ew = t->ew, eh = t->eh;
+    if (allowed.empty()) {
+        /* without a mask the lists are regular: generated on the device, no host loops or copies */
+        const long long P = (long long) eh * ew;
+        DevBuf<int> d_trows, d_tpos, d_qrows, d_qpos, d_qcell, d_seg;
+        PT_CUDA(d_trows.reserve(P)); PT_CUDA(d_tpos.reserve(P));
+        PT_CUDA(d_qrows.reserve(P)); PT_CUDA(d_qpos.reserve(P)); PT_CUDA(d_qcell.reserve(P)); PT_CUDA(d_seg.reserve(P + 1));
+        int N = 0, Q = 0, nseg = 0;
+        if (pt_kc_lists(ew, eh, p.flann_build_step, p.kcoherence_step, p.flann_reset_step, d_trows.p, d_tpos.p, d_qrows.p,
+                        d_qpos.p, d_qcell.p, d_seg.p, &N, &Q, &nseg, t->st) == PT_OK) {
+            PT_CUDA(t->kcoh.reserve((size_t) P * p.kcoherence));
+            PT_CUDA(cudaMemsetAsync(t->kcoh.p, 0, sizeof(int2) * (size_t) P * p.kcoherence, t->st));
+            DevBuf<float> train, qdesc;
+            PT_CUDA(train.reserve((size_t) N * t->nd)); PT_CUDA(qdesc.reserve((size_t) Q * t->nd));
+            PT_TRY(pt_gather_rows(t->b_desc.p, t->ds, t->nd, d_trows.p, N, train.p, t->st));
+            PT_TRY(pt_gather_rows(t->b_desc.p, t->ds, t->nd, d_qrows.p, Q, qdesc.p, t->st));
+            return pt_kcoherence(t->b_rgba.p, t->w, t->desc_mode ? t->b_desc.p : nullptr, t->ds, t->ew, train.p, N, t->nd,
+                                 d_tpos.p, qdesc.p, d_qpos.p, d_qcell.p, Q, d_seg.p, nseg, p.kcoherence,
+                                 p.kcoherence_min_dist, t->kcoh.p, &t->kc_list, t->st);
+        }
+    }
     /* Train set: build_flann_index_func (patchtable.h:822-861), allowed patches every
        flann_build_step pixels in raster order. */
     std::vector<int> trows, tpos;

@@ -160,6 +160,30 @@ def test_kcoherence_long_neighbour_lists(gpu, oracle, libc, args, sw, knn_min):
     check_nnf(oracle, a, b, gt.lookup(a))
 
 
+@pytest.mark.parametrize("sw,masked", [("-limit 0.5 -kcoherence 3 -kcoherence_step 2 -flann_build_step 2 -flann_reset_step 3", False),
+                                       ("-limit 0.5 -kcoherence 2 -flann_reset_step 1", False),
+                                       ("-limit 0.5 -kcoherence 2 -kcoherence_step 3 -flann_reset_step 4", True)])
+def test_kcoherence_steps_and_segments(gpu, oracle, libc, sw, masked):
+    """Sampled train sets (flann_build_step), sampled queries (kcoherence_step) and the knn reset
+    segments (flann_reset_step, patchtable.h:2705-2714), with and without an allowed mask: the
+    k-coherence set and the table equal the oracle's bit for bit."""
+    a, b = synth.pair(70, 90, 27)
+    allowed = None
+    if masked:
+        rng = np.random.default_rng(27)
+        allowed = (rng.random((63, 83)) < 0.8).astype(np.int32)
+    p = ptb.PatchTableParams(sw)
+    srand_all(libc, 1)
+    ot = oracle.build(p.as_dict(), b, allowed=allowed)
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b, wh0=ot.wh0(), allowed_patches=allowed)
+    kg, ko = gt.kcoherence(), ot.kcoherence()
+    assert np.array_equal(kg[0], ko[0])
+    assert np.array_equal(kg[1], ko[1])
+    assert np.array_equal(gt.table(), ot.table())
+    check_nnf(oracle, a, b, gt.lookup(a))
+
+
 BRUTE_CASES = [("-limit 0.002", 60, 90, 21, False), ("-limit 0.004 -ndims 8", 43, 71, 5, True),
                ("-limit 0.0005 -grid_ndims 2", 40, 60, 6, False), ("-limit 0.003 -nchroma 0 -ndims 5", 50, 50, 8, True),
                ("-limit 0.01 -grid_ndims 7 -ndims 7", 80, 100, 9, False)]
