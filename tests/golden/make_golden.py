@@ -55,6 +55,10 @@ CASES = [
          switches="-dim_algo pca -ndims 4 -pca_subtract_mean 0 -pca_samples 300 -limit 0.5"),
     dict(name="pca_nd12_rgb_110x80", h=80, w=110, seed=14, switches="-dim_algo pca -ndims 12 -colorspace rgb -limit 3"),
     dict(name="pca_lab_120x90", h=90, w=120, seed=15, switches="-dim_algo pca -colorspace lab -limit 1"),
+    # sampled k-coherence: train set every 2nd patch, queries every 2nd / 3rd pixel, knn reset segments
+    dict(name="kc_steps_90x70", h=70, w=90, seed=27,
+         switches="-limit 0.5 -kcoherence 3 -kcoherence_step 2 -flann_build_step 2 -flann_reset_step 3"),
+    dict(name="kc_reset1_90x70", h=70, w=90, seed=27, switches="-limit 0.5 -kcoherence 2 -flann_reset_step 1"),
 ]
 C2 = dict(name="c2_1920x1080_coh4", h=1080, w=1920, seed=2, switches="-speed 3 -coherence_spatial 4")
 # Descriptor mode (is_descriptor): synth.descriptor_pair inputs.  Three channels are left out: the
