@@ -403,6 +403,7 @@ def one_vs_many_measure():
     table = ptb.PatchTable(params, atlas, allowed_patches=allowed)
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
+    build_stage_ms = table.build_profile()
     H, W = query.shape[:2]
     P = (H - 7) * (W - 7)
     da = torch.from_numpy(query).cuda()
@@ -418,7 +419,7 @@ def one_vs_many_measure():
                                     "all_matches_allowed": ok}
     table.close()
     return {"query": [H, W], "atlas": list(atlas.shape[:2]), "database_images": len(boxes),
-            "allowed_patches": int(allowed.sum()), "build_s": build_s, "schedules": rows}
+            "allowed_patches": int(allowed.sum()), "build_s": build_s, "build_stage_ms": build_stage_ms, "schedules": rows}
 
 
 def main():
