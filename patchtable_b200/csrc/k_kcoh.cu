@@ -323,7 +323,96 @@ __global__ void k_kc_lists(int ew, int fbs, int ks, int ntx, int nqx, int N, int
     if (i < nseg) seg[i] = (int) (i / ncols) * nqx + cols[i % ncols];
 }
 
+/* Masked lists, step 1: which train and query grid points are allowed patches. */
+__global__ void k_kc_flags(const int *__restrict__ allowed, int idx, int ew, int fbs, int ks, int ntx, int N0, int nqx,
+                           int Q0, int *tflag, int *qflag) {
+    const long long i = blockIdx.x * 256ll + threadIdx.x;
+    if (i < N0) {
+        const int y = (int) (i / ntx) * fbs, x = (int) (i % ntx) * fbs;
+        tflag[i] = __ldg(allowed + (size_t) y * ew + x) == idx;
+    }
+    if (i < Q0) {
+        const int py = (int) (i / nqx) * ks, px = (int) (i % nqx) * ks;
+        qflag[i] = __ldg(allowed + (size_t) py * ew + px) == idx;
+    }
+}
+
+/* Step 2: an allowed query opens a segment when it is the first allowed query or its column
+   satisfies the reset rule ((x / ks) % reset == 0, x in padded coordinates). */
+__global__ void k_kc_segflags(int ks, int reset, int nqx, int Q0, const int *__restrict__ qflag,
+                              const int *__restrict__ qinc, int *gflag) {
+    const long long i = blockIdx.x * 256ll + threadIdx.x;
+    if (i >= Q0) return;
+    const int px = (int) (i % nqx) * ks;
+    gflag[i] = qflag[i] && (qinc[i] == 1 || ((px + 7) / ks) % reset == 0);
+}
+
+/* Step 3: allowed points go to their ranks among the allowed ones (inclusive scans - 1), so the
+   lists keep the raster order of the unmasked loops with the disallowed points left out. */
+__global__ void k_kc_scatter(int ew, int fbs, int ks, int ntx, int N0, int nqx, int Q0, const int *__restrict__ tflag,
+                             const int *__restrict__ tinc, const int *__restrict__ qflag, const int *__restrict__ qinc,
+                             const int *__restrict__ gflag, const int *__restrict__ ginc, int *trows, int *tpos,
+                             int *qrows, int *qpos, int *qcell, int *seg) {
+    const long long i = blockIdx.x * 256ll + threadIdx.x;
+    if (i < N0 && tflag[i]) {
+        const int y = (int) (i / ntx) * fbs, x = (int) (i % ntx) * fbs, o = tinc[i] - 1;
+        trows[o] = y * ew + x;
+        tpos[o] = pt_xy(x, y);
+    }
+    if (i < Q0 && qflag[i]) {
+        const int py = (int) (i / nqx) * ks, px = (int) (i % nqx) * ks, o = qinc[i] - 1;
+        qrows[o] = py * ew + px;
+        qpos[o] = pt_xy(px, py);
+        qcell[o] = (py / ks) * ew + px / ks;
+        if (gflag[i]) seg[ginc[i] - 1] = o;
+    }
+}
+
 }  // namespace
+
+pt_status pt_kc_lists_masked(int ew, int eh, int fbs, int ks, int reset, const int *allowed, int allowed_index,
+                             int *trows, int *tpos, int *qrows, int *qpos, int *qcell, int *seg, int *n_out, int *q_out,
+                             int *nseg_out, cudaStream_t st) {
+    const int ntx = (ew + fbs - 1) / fbs, nty = (eh + fbs - 1) / fbs;
+    const int nqx = (ew + ks - 1) / ks, nqy = (eh + ks - 1) / ks;
+    const long long N0 = (long long) ntx * nty, Q0 = (long long) nqx * nqy;
+    if (Q0 >= (1ll << 31) || N0 >= (1ll << 31) || reset < 1)
+        return pt_fail(PT_UNSUPPORTED, "k-coherence index lists");    /* callers use the general path */
+    const long long M = std::max(N0, Q0);
+    DevBuf<int> tflag, tinc, qflag, qinc, gflag, ginc, tot;
+    PT_CUDA(tflag.reserve(N0)); PT_CUDA(tinc.reserve(N0));
+    PT_CUDA(qflag.reserve(Q0)); PT_CUDA(qinc.reserve(Q0));
+    PT_CUDA(gflag.reserve(Q0)); PT_CUDA(ginc.reserve(Q0));
+    PT_CUDA(tot.reserve(3));
+    size_t tmp_bytes = 0;
+    PT_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, tflag.p, tinc.p, (int) M, st));
+    DevBuf<unsigned char> tmp;
+    PT_CUDA(tmp.reserve(tmp_bytes));
+    const unsigned blocks = (unsigned) ((M + 255) / 256);
+    k_kc_flags<<<blocks, 256, 0, st>>>(allowed, allowed_index, ew, fbs, ks, ntx, (int) N0, nqx, (int) Q0, tflag.p, qflag.p);
+    PT_LAUNCHED();
+    size_t b = tmp_bytes;
+    PT_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, b, tflag.p, tinc.p, (int) N0, st));
+    b = tmp_bytes;
+    PT_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, b, qflag.p, qinc.p, (int) Q0, st));
+    k_kc_segflags<<<(unsigned) ((Q0 + 255) / 256), 256, 0, st>>>(ks, reset, nqx, (int) Q0, qflag.p, qinc.p, gflag.p);
+    PT_LAUNCHED();
+    b = tmp_bytes;
+    PT_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, b, gflag.p, ginc.p, (int) Q0, st));
+    k_kc_scatter<<<blocks, 256, 0, st>>>(ew, fbs, ks, ntx, (int) N0, nqx, (int) Q0, tflag.p, tinc.p, qflag.p, qinc.p,
+                                         gflag.p, ginc.p, trows, tpos, qrows, qpos, qcell, seg);
+    PT_LAUNCHED();
+    PT_CUDA(cudaMemcpyAsync(tot.p, tinc.p + N0 - 1, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    PT_CUDA(cudaMemcpyAsync(tot.p + 1, qinc.p + Q0 - 1, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    PT_CUDA(cudaMemcpyAsync(tot.p + 2, ginc.p + Q0 - 1, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    int h_tot[3] = {0, 0, 0};
+    PT_CUDA(cudaMemcpyAsync(h_tot, tot.p, sizeof(h_tot), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaStreamSynchronize(st));           /* the scratch goes out of scope */
+    *n_out = h_tot[0];
+    *q_out = h_tot[1];
+    *nseg_out = h_tot[2];
+    return PT_OK;
+}
 
 pt_status pt_kc_lists(int ew, int eh, int fbs, int ks, int reset, int *trows, int *tpos, int *qrows, int *qpos,
                       int *qcell, int *seg, int *n_out, int *q_out, int *nseg_out, cudaStream_t st) {

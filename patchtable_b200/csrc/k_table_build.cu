@@ -20,8 +20,9 @@
      seed      the seeded cells, in increasing cell order, become the first frontier (label 0):
                each CTA writes its range at the prefix of the counts before it;
      levels    the reference's breadth-first fill, level-synchronously: every frontier element
-               claims the unused neighbours its label allows with atomicMin on (element, edge);
-               each CTA counts the claims its contiguous range of elements won; winners fill their
+               claims the unused neighbours its label allows with atomicMin on (element, edge) and
+               keeps a bit mask of those edges; each CTA checks, for its contiguous range of
+               elements, which of the masked claims they won (a second mask); winners fill their
                cells and append (cell, label) to the next frontier at the scanned offsets, i.e. in
                (element, edge) order, which is the order of the reference's next frontier list.
    The filled table is therefore bit-identical to the reference's.  Data written by other CTAs in
@@ -57,7 +58,7 @@ struct CellBuild {
     unsigned *claim;
     int *fidx[2];
     unsigned char *flab[2];
-    unsigned char *cnt;          /* cells each element of the level won (at most 2 * G) */
+    unsigned *emask;             /* per frontier element: edges to unused neighbours, then the edges it won */
     long long *ctot;             /* per-CTA totals */
     unsigned *bar;               /* [0] arrivals, [1] generation */
     int *status;                 /* [0] pt_status of the launch, [1] levels, [2] phase that failed */
@@ -218,35 +219,44 @@ __global__ void __launch_bounds__(NT) k_table_build(const CellBuild a) {
             }
             const int *fi = a.fidx[cur];
             const unsigned char *fl = a.flab[cur];
-            /* claim: the smallest (element, edge) key wins each unused neighbour (:2131-2156) */
+            /* claim: the smallest (element, edge) key wins each unused neighbour (:2131-2156); the
+               element remembers which of its edges led to an unused neighbour */
             for (long long i = tid; i < n; i += nthr) {
                 const long long g = __ldcg(fi + i);
                 const int lab = __ldcg(fl + i), ne = edge_count(a.G, lab);
+                unsigned open = 0;
                 for (int e = 0; e < ne; e++) {
                     int dim, dir;
                     edge_of(lab, e, dim, dir);
                     const long long gp = open_neighbour(a, g, dim, dir);
-                    if (gp >= 0) atomicMin(a.claim + gp, ((unsigned) i << 5) | (unsigned) e);
+                    if (gp >= 0) {
+                        atomicMin(a.claim + gp, ((unsigned) i << 5) | (unsigned) e);
+                        open |= 1u << e;
+                    }
                 }
+                a.emask[i] = open;
             }
             if (!grid_barrier(a, 5)) return;
-            /* count the claims each element of this CTA's range won */
+            /* count the claims each element of this CTA's range won (only its open edges) */
             const long long ech = (n + gridDim.x - 1) / gridDim.x;
             const long long e0 = min(n, (long long) blockIdx.x * ech), e1 = min(n, e0 + ech);
             {
                 long long local = 0;
                 for (long long i = e0 + threadIdx.x; i < e1; i += NT) {
-                    const long long g = __ldcg(fi + i);
-                    const int lab = __ldcg(fl + i), ne = edge_count(a.G, lab);
-                    int c = 0;
-                    for (int e = 0; e < ne; e++) {
-                        int dim, dir;
-                        edge_of(lab, e, dim, dir);
-                        const long long gp = open_neighbour(a, g, dim, dir);
-                        if (gp >= 0 && __ldcg(a.claim + gp) == (((unsigned) i << 5) | (unsigned) e)) c++;
+                    unsigned open = __ldcg(a.emask + i), won = 0;
+                    if (open) {
+                        const long long g = __ldcg(fi + i);
+                        const int lab = __ldcg(fl + i);
+                        while (open) {
+                            const int e = __ffs(open) - 1;
+                            open &= open - 1;
+                            int dim, dir;
+                            edge_of(lab, e, dim, dir);
+                            if (__ldcg(a.claim + g + dir * a.stride[dim]) == (((unsigned) i << 5) | (unsigned) e)) won |= 1u << e;
+                        }
                     }
-                    a.cnt[i] = (unsigned char) c;
-                    local += c;
+                    a.emask[i] = won;
+                    local += __popc(won);
                 }
                 const long long s = cta_sum(sh, local);
                 if (threadIdx.x == 0) a.ctot[blockIdx.x] = s;
@@ -260,26 +270,25 @@ __global__ void __launch_bounds__(NT) k_table_build(const CellBuild a) {
             long long o2 = base;
             for (long long t0 = e0; t0 < e1; t0 += NT) {
                 const long long i = t0 + threadIdx.x;
-                const int c = i < e1 ? (int) __ldcg(a.cnt + i) : 0;
+                unsigned won = i < e1 ? __ldcg(a.emask + i) : 0u;
                 int off, tot;
                 __syncthreads();
-                Scan(sh.scan).ExclusiveSum(c, off, tot);
-                if (c) {
+                Scan(sh.scan).ExclusiveSum(__popc(won), off, tot);
+                if (won) {
                     const long long g = __ldcg(fi + i);
-                    const int lab = __ldcg(fl + i), ne = edge_count(a.G, lab);
+                    const int lab = __ldcg(fl + i);
                     const int val = __ldcg(a.table + g);
                     long long w = o2 + off;
-                    for (int e = 0; e < ne; e++) {
+                    while (won) {
+                        const int e = __ffs(won) - 1;
+                        won &= won - 1;
                         int dim, dir;
                         edge_of(lab, e, dim, dir);
-                        /* only the winner writes gp in this level, so the winner still reads it unused */
-                        const long long gp = open_neighbour(a, g, dim, dir);
-                        if (gp >= 0 && __ldcg(a.claim + gp) == (((unsigned) i << 5) | (unsigned) e)) {
-                            a.table[gp] = val;
-                            nfi[w] = (int) gp;
-                            nfl[w] = (unsigned char) (2 * dim + 1 + (dir + 1) / 2);
-                            w++;
-                        }
+                        const long long gp = g + dir * a.stride[dim];
+                        a.table[gp] = val;
+                        nfi[w] = (int) gp;
+                        nfl[w] = (unsigned char) (2 * dim + 1 + (dir + 1) / 2);
+                        w++;
                     }
                 }
                 o2 += tot;
@@ -338,14 +347,15 @@ pt_status pt_build_cells(const PtBins &bins, const int *nslices, const float *de
     /* Scratch: claim keys and two frontiers of at most one element per cell. */
     DevBuf<unsigned> claim;
     DevBuf<int> fidx0, fidx1, status;
-    DevBuf<unsigned char> flab0, flab1, cnt;
+    DevBuf<unsigned char> flab0, flab1;
+    DevBuf<unsigned> emask;
     DevBuf<long long> ctot, seed_n;
     DevBuf<unsigned> bar;
     if (run_dt) {
         PT_CUDA(claim.reserve(ncells));
         PT_CUDA(fidx0.reserve(ncells)); PT_CUDA(fidx1.reserve(ncells));
         PT_CUDA(flab0.reserve(ncells)); PT_CUDA(flab1.reserve(ncells));
-        PT_CUDA(cnt.reserve(ncells));
+        PT_CUDA(emask.reserve(ncells));
     }
     PT_CUDA(ctot.reserve(grid));
     PT_CUDA(seed_n.reserve(1));
@@ -356,7 +366,7 @@ pt_status pt_build_cells(const PtBins &bins, const int *nslices, const float *de
     a.claim = claim.p;
     a.fidx[0] = fidx0.p; a.fidx[1] = fidx1.p;
     a.flab[0] = flab0.p; a.flab[1] = flab1.p;
-    a.cnt = cnt.p;
+    a.emask = emask.p;
     a.ctot = ctot.p;
     a.bar = bar.p;
     a.status = status.p;

@@ -85,6 +85,11 @@ pt_status pt_gather_rows(const float *desc, int ds, int nd, const int *rows, int
    seg for every query + 1); PT_UNSUPPORTED when the general host path must be used. */
 pt_status pt_kc_lists(int ew, int eh, int fbs, int ks, int reset, int *trows, int *tpos, int *qrows, int *qpos,
                       int *qcell, int *seg, int *n_out, int *q_out, int *nseg_out, cudaStream_t st);
+/* The same lists for a build with an allowed mask (allowed: ew x eh patches on the device):
+   only points whose entry equals allowed_index, in the same order. */
+pt_status pt_kc_lists_masked(int ew, int eh, int fbs, int ks, int reset, const int *allowed, int allowed_index,
+                             int *trows, int *tpos, int *qrows, int *qpos, int *qcell, int *seg, int *n_out, int *q_out,
+                             int *nseg_out, cudaStream_t st);
 /* Exact distances from b_rgba (image mode) or, when bdesc is set, from the descriptor store
    (descriptor mode: ds floats per patch, ew patches per row). */
 pt_status pt_kcoherence(const float4 *b_rgba, int bw, const float *bdesc, int ds, int ew, const float *train, int N, int nd, const int *tpos,

@@ -301,17 +301,25 @@ bool host_allowed(const std::vector<int> &allowed, int idx, int py, int px, int 
 pt_status build_kcoherence(pt_table *t, const std::vector<int> &allowed) {
     const pt_params &p = t->p;
     const int ew = t->ew, eh = t->eh;
-    if (allowed.empty()) {
-        /* without a mask the lists are regular: generated on the device, no host loops or copies */
+    {
+        /* The lists are generated on the device (no host loops or copies): regular grids without
+           a mask, the same grids compacted to the allowed points with one. */
         const long long P = (long long) eh * ew;
         DevBuf<int> d_trows, d_tpos, d_qrows, d_qpos, d_qcell, d_seg;
         PT_CUDA(d_trows.reserve(P)); PT_CUDA(d_tpos.reserve(P));
         PT_CUDA(d_qrows.reserve(P)); PT_CUDA(d_qpos.reserve(P)); PT_CUDA(d_qcell.reserve(P)); PT_CUDA(d_seg.reserve(P + 1));
         int N = 0, Q = 0, nseg = 0;
-        if (pt_kc_lists(ew, eh, p.flann_build_step, p.kcoherence_step, p.flann_reset_step, d_trows.p, d_tpos.p, d_qrows.p,
-                        d_qpos.p, d_qcell.p, d_seg.p, &N, &Q, &nseg, t->st) == PT_OK) {
+        const pt_status lst =
+            allowed.empty()
+                ? pt_kc_lists(ew, eh, p.flann_build_step, p.kcoherence_step, p.flann_reset_step, d_trows.p, d_tpos.p,
+                              d_qrows.p, d_qpos.p, d_qcell.p, d_seg.p, &N, &Q, &nseg, t->st)
+                : pt_kc_lists_masked(ew, eh, p.flann_build_step, p.kcoherence_step, p.flann_reset_step, t->allowed.p,
+                                     p.allowed_index, d_trows.p, d_tpos.p, d_qrows.p, d_qpos.p, d_qcell.p, d_seg.p, &N,
+                                     &Q, &nseg, t->st);
+        if (lst == PT_OK) {
             PT_CUDA(t->kcoh.reserve((size_t) P * p.kcoherence));
             PT_CUDA(cudaMemsetAsync(t->kcoh.p, 0, sizeof(int2) * (size_t) P * p.kcoherence, t->st));
+            if (Q == 0) return PT_OK;
             DevBuf<float> train, qdesc;
             PT_CUDA(train.reserve((size_t) N * t->nd)); PT_CUDA(qdesc.reserve((size_t) Q * t->nd));
             PT_TRY(pt_gather_rows(t->b_desc.p, t->ds, t->nd, d_trows.p, N, train.p, t->st));
@@ -498,7 +506,11 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
     });
     /* set_min_max + set_nslices (patchtable.h:1758-1810, 2567-2582), then the partition */
     if (!t->st2) {
-        cudaError_t e = cudaStreamCreateWithFlags(&t->st2, cudaStreamNonBlocking);
+        /* highest priority: the partition's short kernels take SMs as the k-NN search's CTAs
+           retire instead of queueing behind the whole search */
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        cudaError_t e = cudaStreamCreateWithPriority(&t->st2, cudaStreamNonBlocking, greatest);
         if (e != cudaSuccess) { shuffler.join(); return pt_fail(PT_CUDA_ERR, "stream: %s", cudaGetErrorString(e)); }
     }
     double part_ms = 0.0;

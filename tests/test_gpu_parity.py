@@ -161,17 +161,21 @@ def test_kcoherence_long_neighbour_lists(gpu, oracle, libc, args, sw, knn_min):
 
 
 @pytest.mark.parametrize("sw,masked", [("-limit 0.5 -kcoherence 3 -kcoherence_step 2 -flann_build_step 2 -flann_reset_step 3", False),
+                                       ("-limit 0.5 -kcoherence 3 -kcoherence_step 2 -flann_build_step 2 -flann_reset_step 3", True),
                                        ("-limit 0.5 -kcoherence 2 -flann_reset_step 1", False),
+                                       ("-limit 0.5 -kcoherence 2 -flann_reset_step 1", True),
                                        ("-limit 0.5 -kcoherence 2 -kcoherence_step 3 -flann_reset_step 4", True)])
 def test_kcoherence_steps_and_segments(gpu, oracle, libc, sw, masked):
     """Sampled train sets (flann_build_step), sampled queries (kcoherence_step) and the knn reset
     segments (flann_reset_step, patchtable.h:2705-2714), with and without an allowed mask: the
-    k-coherence set and the table equal the oracle's bit for bit."""
+    k-coherence set and the table equal the oracle's bit for bit.  The masks leave out the first
+    patches of the top row, so the first allowed query opens a segment off the reset columns."""
     a, b = synth.pair(70, 90, 27)
     allowed = None
     if masked:
         rng = np.random.default_rng(27)
         allowed = (rng.random((63, 83)) < 0.8).astype(np.int32)
+        allowed[0, :5] = 0
     p = ptb.PatchTableParams(sw)
     srand_all(libc, 1)
     ot = oracle.build(p.as_dict(), b, allowed=allowed)
