@@ -93,17 +93,16 @@ inline int blocks_for(long long n) { return (int) ((n + NT - 1) / NT); }
 
 }  // namespace
 
-pt_status pt_launch_minmax(const float *desc, int ds, int G, long long P, const int *allowed, int allowed_index,
-                           float *hmin, float *hmax, cudaStream_t st) {
+pt_status pt_launch_minmax(PtPartScratch &s, const float *desc, int ds, int G, long long P, const int *allowed,
+                           int allowed_index, float *hmin, float *hmax, cudaStream_t st) {
     const int NB = 296;
-    DevBuf<float> pmin, pmax;
-    PT_CUDA(pmin.reserve(NB * PT_DESC_MAX));
-    PT_CUDA(pmax.reserve(NB * PT_DESC_MAX));
-    k_minmax<<<NB, NT, 0, st>>>(desc, ds, G, P, allowed, allowed_index, pmin.p, pmax.p);
+    PT_CUDA(s.pmin.reserve(NB * PT_DESC_MAX));
+    PT_CUDA(s.pmax.reserve(NB * PT_DESC_MAX));
+    k_minmax<<<NB, NT, 0, st>>>(desc, ds, G, P, allowed, allowed_index, s.pmin.p, s.pmax.p);
     PT_LAUNCHED();
     std::vector<float> a(NB * PT_DESC_MAX), b(NB * PT_DESC_MAX);
-    PT_CUDA(cudaMemcpyAsync(a.data(), pmin.p, sizeof(float) * a.size(), cudaMemcpyDeviceToHost, st));
-    PT_CUDA(cudaMemcpyAsync(b.data(), pmax.p, sizeof(float) * b.size(), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaMemcpyAsync(a.data(), s.pmin.p, sizeof(float) * a.size(), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaMemcpyAsync(b.data(), s.pmax.p, sizeof(float) * b.size(), cudaMemcpyDeviceToHost, st));
     PT_CUDA(cudaStreamSynchronize(st));
     for (int d = 0; d < G; d++) {
         float mn = 1e20f, mx = -1e20f;
@@ -113,36 +112,38 @@ pt_status pt_launch_minmax(const float *desc, int ds, int G, long long P, const 
     return PT_OK;
 }
 
-pt_status pt_quantile_values(const float *desc, int ds, int d, int eh, int ew, int step, const int *allowed,
-                             int allowed_index, const std::vector<int> &want, std::vector<float> &vals,
-                             int *count_out, cudaStream_t st) {
-    long long P = (long long) eh * ew;
-    DevBuf<float> keys, sorted, picked;
-    DevBuf<int> cnt, idx;
-    PT_CUDA(keys.reserve(P));
-    PT_CUDA(sorted.reserve(P));
-    PT_CUDA(cnt.reserve(1));
-    PT_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int), st));
-    k_gather_dim<<<blocks_for(P), NT, 0, st>>>(desc, ds, d, eh, ew, step, allowed, allowed_index, keys.p, cnt.p);
+pt_status pt_quantile_gather(PtPartScratch &s, const float *desc, int ds, int d, int eh, int ew, int step,
+                             const int *allowed, int allowed_index, int *count_out, cudaStream_t st) {
+    const long long P = (long long) eh * ew;
+    PT_CUDA(s.keys.reserve(P));
+    PT_CUDA(s.cnt.reserve(1));
+    PT_CUDA(cudaMemsetAsync(s.cnt.p, 0, sizeof(int), st));
+    k_gather_dim<<<blocks_for(P), NT, 0, st>>>(desc, ds, d, eh, ew, step, allowed, allowed_index, s.keys.p, s.cnt.p);
     PT_LAUNCHED();
     int n = 0;
-    PT_CUDA(cudaMemcpyAsync(&n, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaMemcpyAsync(&n, s.cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     PT_CUDA(cudaStreamSynchronize(st));
     *count_out = n;
-    if (want.empty()) return PT_OK;
+    return PT_OK;
+}
+
+pt_status pt_quantile_pick(PtPartScratch &s, int n, const std::vector<int> &want, std::vector<float> &vals,
+                           cudaStream_t st) {
+    vals.clear();
+    if (want.empty() || n < 1) return PT_OK;
+    PT_CUDA(s.sorted.reserve(n));
     size_t tmp_bytes = 0;
-    PT_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, keys.p, sorted.p, n, 0, 32, st));
-    DevBuf<unsigned char> tmp;
-    PT_CUDA(tmp.reserve(tmp_bytes));
-    PT_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, tmp_bytes, keys.p, sorted.p, n, 0, 32, st));
+    PT_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, s.keys.p, s.sorted.p, n, 0, 32, st));
+    PT_CUDA(s.tmp.reserve(tmp_bytes));
+    PT_CUDA(cub::DeviceRadixSort::SortKeys(s.tmp.p, tmp_bytes, s.keys.p, s.sorted.p, n, 0, 32, st));
     pt_count_launches(4);
-    PT_CUDA(idx.reserve(want.size()));
-    PT_CUDA(picked.reserve(want.size()));
-    PT_CUDA(cudaMemcpyAsync(idx.p, want.data(), sizeof(int) * want.size(), cudaMemcpyHostToDevice, st));
-    k_pick<<<blocks_for((long long) want.size()), NT, 0, st>>>(sorted.p, idx.p, (int) want.size(), picked.p);
+    PT_CUDA(s.idx.reserve(want.size()));
+    PT_CUDA(s.picked.reserve(want.size()));
+    PT_CUDA(cudaMemcpyAsync(s.idx.p, want.data(), sizeof(int) * want.size(), cudaMemcpyHostToDevice, st));
+    k_pick<<<blocks_for((long long) want.size()), NT, 0, st>>>(s.sorted.p, s.idx.p, (int) want.size(), s.picked.p);
     PT_LAUNCHED();
     vals.resize(want.size());
-    PT_CUDA(cudaMemcpyAsync(vals.data(), picked.p, sizeof(float) * want.size(), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaMemcpyAsync(vals.data(), s.picked.p, sizeof(float) * want.size(), cudaMemcpyDeviceToHost, st));
     PT_CUDA(cudaStreamSynchronize(st));
     return PT_OK;
 }

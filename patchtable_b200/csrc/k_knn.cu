@@ -346,12 +346,18 @@ pt_status pt_launch_knn(const float *train, int N, int nd, const float *qdesc, i
     memset(&qz, 0, sizeof(qz));
     qz.nd = nd;
     qz.bits = std::min(10, 63 / nd);
+    /* One scale for every dimension (that of the widest range): the Morton order then splits the
+       dimensions in proportion to their spread, so a bucket's box is about as wide in every
+       dimension in distance units, which is what the Euclidean lower bounds prune with.  (The
+       search is exact whatever the order; only its pruning depends on the boxes.) */
+    float rmax = 0.f;
     for (int d = 0; d < nd; d++) {
         float mn = a[d], mx = b[d];
         for (int i = 1; i < NB; i++) { mn = std::min(mn, a[i * PT_DESC_MAX + d]); mx = std::max(mx, b[i * PT_DESC_MAX + d]); }
         qz.mn[d] = mn;
-        qz.scale[d] = mx > mn ? (float) ((1u << qz.bits) - 1) / (mx - mn) : 0.f;
+        rmax = std::max(rmax, mx - mn);
     }
+    for (int d = 0; d < nd; d++) qz.scale[d] = rmax > 0.f ? (float) ((1u << qz.bits) - 1) / rmax : 0.f;
     /* sort train points and queries by Morton code */
     DevBuf<unsigned long long> codes, codes2;
     DevBuf<int> idx, perm, qidx, qorder, sidx;

@@ -40,11 +40,27 @@ pt_status pt_launch_descriptor_input(const float *in, int H, int W, int nd, int 
                                      cudaStream_t st);
 
 /* k_build.cu */
-pt_status pt_launch_minmax(const float *desc, int ds, int G, long long P, const int *allowed, int allowed_index,
-                           float *hmin, float *hmax, cudaStream_t st);
-pt_status pt_quantile_values(const float *desc, int ds, int d, int eh, int ew, int step, const int *allowed,
-                             int allowed_index, const std::vector<int> &want, std::vector<float> &vals,
-                             int *count_out, cudaStream_t st);
+/* Device scratch of the range and partition stages.  The build runs them beside the k-coherence
+   search, so the scratch is owned by the caller and freed after both have finished: a cudaFree
+   inside the stages would wait for the whole device, the search included. */
+#ifdef __CUDACC__
+struct PtPartScratch {
+    DevBuf<float> pmin, pmax, keys, sorted, picked;
+    DevBuf<int> cnt, idx;
+    DevBuf<unsigned char> tmp;
+};
+#else
+struct PtPartScratch;
+#endif
+pt_status pt_launch_minmax(PtPartScratch &s, const float *desc, int ds, int G, long long P, const int *allowed,
+                           int allowed_index, float *hmin, float *hmax, cudaStream_t st);
+/* The partition sample of dimension d (every step-th allowed patch, patchtable.h:1193-1201) into
+   s.keys; *count_out = its size. */
+pt_status pt_quantile_gather(PtPartScratch &s, const float *desc, int ds, int d, int eh, int ew, int step,
+                             const int *allowed, int allowed_index, int *count_out, cudaStream_t st);
+/* vals[i] = the want[i]-th smallest of the n gathered values. */
+pt_status pt_quantile_pick(PtPartScratch &s, int n, const std::vector<int> &want, std::vector<float> &vals,
+                           cudaStream_t st);
 /* Per-dimension get_bin parameters of a built table. */
 struct PtBins {
     int G;

@@ -202,7 +202,7 @@ pt_status check_params(const pt_params *p, int h, int w) {
 
 pt_status upload_partition(pt_table *t, cudaStream_t st);
 
-pt_status build_partition(pt_table *t, cudaStream_t st) {
+pt_status build_partition(pt_table *t, PtPartScratch &scratch, cudaStream_t st) {
     const int G = t->G;
     t->part.assign(G, PtPartition());
     for (int d = 0; d < G; d++) {
@@ -216,8 +216,8 @@ pt_status build_partition(pt_table *t, cudaStream_t st) {
            (PatchPartition1D, patchtable.h:1193-1201). */
         int N = 0;
         std::vector<float> vals;
-        PT_TRY(pt_quantile_values(t->b_desc.p, t->ds, d, t->eh, t->ew, t->p.partition_step, t->allowed.p,
-                                  t->p.allowed_index, {}, vals, &N, st));
+        PT_TRY(pt_quantile_gather(scratch, t->b_desc.p, t->ds, d, t->eh, t->ew, t->p.partition_step, t->allowed.p,
+                                  t->p.allowed_index, &N, st));
         if (N < 1) return pt_fail(PT_BAD_ARG, "no allowed patches to build a table from");
         std::vector<int> want;
         want.reserve(2 * ns);
@@ -225,9 +225,7 @@ pt_status build_partition(pt_table *t, cudaStream_t st) {
             want.push_back((int) ((long long) (N - 1) * i / ns));
             want.push_back((int) ((long long) (N - 1) * (i + 1) / ns));
         }
-        int N2 = 0;
-        PT_TRY(pt_quantile_values(t->b_desc.p, t->ds, d, t->eh, t->ew, t->p.partition_step, t->allowed.p,
-                                  t->p.allowed_index, want, vals, &N2, st));
+        PT_TRY(pt_quantile_pick(scratch, N, want, vals, st));
         P.centers.resize(ns);
         P.lsizes.resize(ns);
         P.rsizes.resize(ns);
@@ -514,6 +512,7 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
         if (e != cudaSuccess) { shuffler.join(); return pt_fail(PT_CUDA_ERR, "stream: %s", cudaGetErrorString(e)); }
     }
     double part_ms = 0.0;
+    PtPartScratch part_scratch;       /* freed when the build returns, after the search has ended */
     std::string part_err;
     pt_status part_st = PT_OK;
     std::thread partitioner([&] {
@@ -521,7 +520,7 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
             cudaStream_t s2 = t->st2;
             t->min_val.assign(t->G, 0.f);
             t->max_val.assign(t->G, 0.f);
-            PT_TRY(pt_launch_minmax(t->b_desc.p, t->ds, t->G, P, t->allowed.p, p.allowed_index, t->min_val.data(),
+            PT_TRY(pt_launch_minmax(part_scratch, t->b_desc.p, t->ds, t->G, P, t->allowed.p, p.allowed_index, t->min_val.data(),
                                     t->max_val.data(), s2));
             t->range.resize(t->G);
             for (int d = 0; d < t->G; d++) t->range[d] = t->max_val[d] - t->min_val[d];
@@ -540,7 +539,7 @@ pt_status create_impl(const pt_params *pin, const float *b, int h, int w, int ch
             t->ncells = 1;
             for (int d = t->G - 1; d >= 0; d--) { t->stride[d] = t->ncells; t->ncells *= t->nslices[d]; }
             if (t->ncells >= (1ll << 31)) return pt_fail(PT_UNSUPPORTED, "table of %lld cells exceeds 2^31", t->ncells);
-            PT_TRY(build_partition(t.get(), s2));
+            PT_TRY(build_partition(t.get(), part_scratch, s2));
             PT_CUDA(cudaStreamSynchronize(s2));
             return PT_OK;
         });
