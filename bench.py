@@ -4,8 +4,8 @@
 Workload (default): the 1920x1080 synthetic match -- image a = 4 octaves of value noise + 20
 rectangles, b = a warped by a smooth random flow (max 16 px) + N(0, 0.02) noise (seed 2) -- with
 the reference's default parameters plus -speed 3 -coherence_spatial 4.  One step = one full query
-(descriptor of a, table lookup, k-coherence, propagation passes, float64 NNF) against a table of b
-built once before warm-up.
+(descriptor of a, table lookup, k-coherence unless the schedule caps it at none, propagation
+passes, float64 NNF) against a table of b built once before warm-up.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
   python bench.py --profile-case query|query-default|infer|build|build-c2  (short fixed runs for ncu)
@@ -41,8 +41,10 @@ UNIT = "patches/s"
 L2_FLUSH_BYTES = 256 << 20
 # query schedules (passes, first jump, pull candidates per patch; 0 = all); every one is timed and
 # the fastest whose mean NNF distance is within 1% of the reference's is the measured one
-SCHEDULES = [(1, 2, 1), (1, 1, 1), (1, 2, 2), (1, 2, 3), (1, 2, 0), (2, 2, 1), (2, 2, 2), (2, 2, 0), (3, 4, 0),
-             (4, 8, 0)]
+# a fourth entry caps the k-coherence neighbours tried per patch (gpu_kc_max; -1 = none, the table
+# step and the pulls alone); the table is the same in every case
+SCHEDULES = [(1, 2, 1, -1), (1, 1, 1, -1), (1, 2, 2, -1), (2, 2, 1, -1), (1, 2, 1, 1), (1, 2, 1), (1, 1, 1), (1, 2, 2),
+             (1, 2, 3), (1, 2, 0), (2, 2, 1), (2, 2, 2), (2, 2, 0), (3, 4, 0), (4, 8, 0)]
 # learned-proposal comparison: schedules tried for both forms against the plain default's quality
 LEARNED_SCHEDULES = [(1, 2, 0), (2, 2, 0), (2, 2, 2), (3, 4, 0), (4, 8, 0)]
 PROPOSAL_WEIGHTS = os.path.join(ROOT, "patchtable_b200", "data", "proposal_weights.npy")
@@ -212,7 +214,7 @@ def profile_case(name):
         p = ptb.PatchTableParams(WORKLOAD["switches"])
         t = ptb.PatchTable(p, b)
         if name == "query":
-            p.gpu_prop_passes, p.gpu_jump, p.gpu_pull_max = SCHEDULES[0]
+            p.set_schedule(SCHEDULES[0])
             p.gpu_tile = 64          # the CTA width the timed run's sweep selects on B200
         da = torch.from_numpy(a).cuda()
         dann = torch.empty((H - 7) * (W - 7) * 3, dtype=torch.float64, device="cuda")
@@ -242,7 +244,7 @@ def timed_schedule(table, sched, da, H, W, dann, sptr, flush, reps=3, net=None):
     import torch
     from patchtable_b200.metrics import get_mean_dist
     p = table.params
-    p.gpu_prop_passes, p.gpu_jump, p.gpu_pull_max = sched
+    p.set_schedule(sched)
     stream = torch.cuda.current_stream()
     best = None
     for i in range(reps + 1):
@@ -266,6 +268,7 @@ def learned_comparison(table, da, H, W, dann, sptr, flush, P):
     """The learned-proposal query against the plain one at the plain default schedule's quality."""
     if not os.path.exists(PROPOSAL_WEIGHTS):
         return {"unavailable": "no trained proposal weights at patchtable_b200/data/proposal_weights.npy"}
+    import patchtable_b200 as ptb
     from patchtable_b200.proposal import ProposalNet
     net = ProposalNet.load(PROPOSAL_WEIGHTS)
     _, target = timed_schedule(table, (0, 0, 0), da, H, W, dann, sptr, flush, reps=1)
@@ -281,11 +284,11 @@ def learned_comparison(table, da, H, W, dann, sptr, flush, P):
             else:
                 net.configure(thr, False)
                 ms, md = timed_schedule(table, sched, da, H, W, dann, sptr, flush, net=net)
-            tried["%d/%d/%d" % sched] = {"ms": ms, "mean_nnf_dist": md}
+            tried[ptb.schedule_name(sched)] = {"ms": ms, "mean_nnf_dist": md}
             if md <= bar and (best is None or ms < best[0]):
                 best = (ms, sched, md)
         rows[label] = {"patches_per_s": P / (best[0] / 1000.0) if best else None,
-                       "schedule": "%d/%d/%d" % best[1] if best else None,
+                       "schedule": ptb.schedule_name(best[1]) if best else None,
                        "mean_nnf_dist": best[2] if best else None, "tried": tried}
     out.update(rows)
     if rows["plain"]["patches_per_s"]:
@@ -338,14 +341,14 @@ def uneven_batch_measure():
             table.lookup_device(rgb.data_ptr() + 12 * int(po), q.shape[0], q.shape[1], ann.data_ptr() + 24 * int(qo), st)
 
     rows = {}
-    for passes, jump, pm in ((2, 2, 0), (4, 8, 0), (8, 8, 0), SCHEDULES[0]):
-        params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = passes, jump, pm
+    for sched in ((2, 2, 0), (4, 8, 0), (8, 8, 0), SCHEDULES[0]):
+        params.set_schedule(sched)
         best, tune = qb.autotune(rgb.data_ptr(), ann.data_ptr(), st)
         qb.capture(rgb.data_ptr(), ann.data_ptr(), st)
         g_ms = _event_ms(lambda: qb.replay(st), 3)
         md = get_mean_dist(ann.view(-1, 3).cpu().numpy()[None])
         pi_ms = _event_ms(per_image, 2)
-        rows["%d/%d/%d" % (passes, jump, pm)] = {
+        rows[ptb.schedule_name(sched)] = {
             "graph_patches_per_s": P / (g_ms / 1000.0), "per_image_patches_per_s": P / (pi_ms / 1000.0),
             "speedup": pi_ms / g_ms, "mean_nnf_dist": md, "patches_per_cta": best,
             "autotune_ms": {str(k): v for k, v in tune.items()}}
@@ -368,7 +371,7 @@ def uneven_batch_sharded(dev, world, rank):
     params = ptb.PatchTableParams(WORKLOAD["switches"])
     ctypes.CDLL(None).srand(1)
     table = ptb.PatchTable(params, table_img)
-    params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = SCHEDULES[0]
+    params.set_schedule(SCHEDULES[0])
     qs = [queries[i] for i in mine]
     qb = table.batch([q.shape[:2] for q in qs])
     rgb = torch.empty(qb.pixels * 3, dtype=torch.float32, device=dev)
@@ -411,11 +414,11 @@ def one_vs_many_measure():
     st = torch.cuda.current_stream().cuda_stream
     rows = {}
     for sched in (SCHEDULES[0], (0, 0, 0)):
-        params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = sched
+        params.set_schedule(sched)
         ms = _event_ms(lambda: table.lookup_device(da.data_ptr(), H, W, dann.data_ptr(), st), 3)
         ann = dann.cpu().numpy()
         ok = bool(np.all(allowed[ann[..., 1].astype(int), ann[..., 0].astype(int)] == 1))
-        rows["%d/%d/%d" % sched] = {"patches_per_s": P / (ms / 1000.0), "ms": ms, "mean_nnf_dist": get_mean_dist(ann),
+        rows[ptb.schedule_name(sched)] = {"patches_per_s": P / (ms / 1000.0), "ms": ms, "mean_nnf_dist": get_mean_dist(ann),
                                     "all_matches_allowed": ok}
     table.close()
     return {"query": [H, W], "atlas": list(atlas.shape[:2]), "database_images": len(boxes),
@@ -474,7 +477,7 @@ def main():
     chosen = None
     for sched in SCHEDULES:
         ms, m = timed_schedule(table, sched, da, H, W, dann, sptr, flush)
-        sched_md["%d/%d/%d" % sched] = {"ms": ms, "mean_nnf_dist": m}
+        sched_md[ptb.schedule_name(sched)] = {"ms": ms, "mean_nnf_dist": m}
         if m <= 1.01 * ref_md and (chosen is None or ms < chosen[0]):
             chosen = (ms, sched)
     chosen = chosen[1] if chosen else SCHEDULES[-1]
@@ -485,7 +488,7 @@ def main():
         params.gpu_tile = tile
         tile_ms[tile], _ = timed_schedule(table, chosen, da, H, W, dann, sptr, flush)
     params.gpu_tile = int(replicas.agree(min(tile_ms, key=tile_ms.get), dev))
-    params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = chosen
+    params.set_schedule(chosen)
     for _ in range(max(args.warmup, 3)):
         flush.zero_()
         table.lookup_device(da.data_ptr(), H, W, dann.data_ptr(), sptr)
@@ -562,7 +565,7 @@ def main():
     learned = None
     if not args.no_learned and rank == 0:
         learned = learned_comparison(table, da, H, W, dann, sptr, flush, P)
-    params.gpu_prop_passes, params.gpu_jump, params.gpu_pull_max = chosen
+    params.set_schedule(chosen)
 
     # roofline of the dominant query kernel.  Both query kernels are limited by the L1TEX data
     # pipe (wavefronts of the scattered 8x8 patch gathers) long before HBM; the HBM figure counts
@@ -574,7 +577,10 @@ def main():
     # bytes per patch averaged over the passes: the first pass reads no state (8 B), the last pull
     # writes the float64 NNF (24 B) in place of the next state (8 B)
     later = (passes - 1) / passes
-    alg_bytes = {"choose": 64 + 8 * later, "pull": 40 + 8 * later + (24 + 8 * (passes - 1)) / passes}[dom] * P
+    # choose: a 16, table entry 4, b pixels 16, chosen 12, and 8 per k-coherence entry it reads
+    kc_cap = chosen[3] if len(chosen) > 3 else 0
+    kc_n = params.kcoherence if kc_cap == 0 else (0 if kc_cap < 0 else min(kc_cap, params.kcoherence))
+    alg_bytes = {"choose": 48 + 8 * kc_n + 8 * later, "pull": 40 + 8 * later + (24 + 8 * (passes - 1)) / passes}[dom] * P
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
     # DRAM traffic and the L1 data-pipe share cannot be measured inside this run: they come from
     # the committed ncu summary of the same kernel and schedule, which names its source revision
@@ -618,7 +624,8 @@ def main():
                    "e2e_ms": {"mean": 1000 * sum(e2e_s) / len(e2e_s), "median": 1000 * float(np.median(e2e_s)),
                               "min": 1000 * min(e2e_s), "max": 1000 * max(e2e_s), "calls": len(e2e_s)},
                    "reference_mean_nnf_dist": ref_md,
-                   "schedule": {"passes": chosen[0], "first_jump": chosen[1], "pull_max": chosen[2], "tried": sched_md,
+                   "schedule": {"passes": chosen[0], "first_jump": chosen[1], "pull_max": chosen[2],
+                                "kc_max": chosen[3] if len(chosen) > 3 else 0, "tried": sched_md,
                                 "patches_per_cta": params.gpu_tile, "patches_per_cta_ms": {str(k): v for k, v in tile_ms.items()},
                                 "rule": "fastest schedule with mean NNF dist <= 1.01 x the reference's on this workload"},
                    "library_default_schedule": default_sched, "learned": learned,

@@ -75,6 +75,11 @@ typedef struct pt_params {
        band's launches fill whole waves of the GPU): uploads, kernels and downloads of consecutive
        bands overlap.  The result does not depend on it. */
     int gpu_bands;
+    /* k-coherence neighbours the query tries per patch (no reference counterpart; a GPU schedule
+       knob like gpu_pull_max): 0 = every one the set lists (the reference's behaviour), n > 0 =
+       at most the first n, negative = none (the table step and the pulls alone; the table's
+       k-coherence set is still built).  Trades NNF quality for speed; distances stay exact. */
+    int gpu_kc_max;
 } pt_params;
 
 typedef struct pt_table pt_table;

@@ -71,6 +71,7 @@ class _Params(C.Structure):
         ("gpu_tile", C.c_int),
         ("pca_samples", C.c_int), ("pca_subtract_mean", C.c_int), ("pca_mean", C.c_int),
         ("gpu_bands", C.c_int),
+        ("gpu_kc_max", C.c_int),
     ]
 
 
@@ -189,6 +190,12 @@ class PatchTableParams:
     def set_speed(self, i: int) -> None:
         _check(lib().pt_params_set_speed(C.byref(self._p), int(i)))
 
+    def set_schedule(self, sched) -> None:
+        """GPU query schedule (passes, first jump, pull candidates[, k-coherence neighbours]):
+        gpu_prop_passes, gpu_jump, gpu_pull_max and gpu_kc_max (0 when not given)."""
+        self.gpu_prop_passes, self.gpu_jump, self.gpu_pull_max = (int(v) for v in sched[:3])
+        self.gpu_kc_max = int(sched[3]) if len(sched) > 3 else 0
+
     @property
     def nslices(self):
         return [self._p.nslices[i] for i in range(self._p.n_nslices)]
@@ -212,6 +219,11 @@ class PatchTableParams:
         d = {f: getattr(self, f) for f, _ in _Params._fields_ if f not in ("nslices", "n_nslices")}
         d["nslices"] = self.nslices
         return d
+
+
+def schedule_name(sched) -> str:
+    """passes/jump/pull candidates, plus /k-coherence neighbours when set (-1 = none)."""
+    return "/".join(str(int(v)) for v in (sched if len(sched) > 3 and sched[3] else sched[:3]))
 
 
 def _img(x, channels=3):

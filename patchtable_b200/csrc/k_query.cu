@@ -33,7 +33,8 @@ struct QPlan {
     int bew, beh;            /* b patches */
     double prop_scale;
     double triangle;
-    int kc, ks;              /* kcoherence, kcoherence_step */
+    int kc, ks;              /* kcoherence (entries per cell), kcoherence_step */
+    int kc_try;              /* entries tried per patch (<= kc) */
     int radius;              /* query_step + prop_dist */
     int do_kcoh;
     int step;                /* neighbour spacing of this pull pass (jump flooding) */
@@ -339,7 +340,7 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
             const int kdx = ks > 1 ? xb % ks : 0, kdy = ks > 1 ? yb % ks : 0;
             constexpr int G = 2;             /* -speed presets list 2 to 20 neighbours; pairs keep registers low */
             bool done = false;
-            for (int k = 0; k < c_q.kc && !done; k += G) {
+            for (int k = 0; k < c_q.kc_try && !done; k += G) {
                 int cg[G];
                 float kdg[G];
                 unsigned m = 0;
@@ -347,7 +348,7 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
                 for (int j = 0; j < G; j++) {
                     cg[j] = 0;
                     kdg[j] = 0.f;
-                    if (m == (1u << j) - 1 && k + j < c_q.kc) {
+                    if (m == (1u << j) - 1 && k + j < c_q.kc_try) {
                         const int2 e = kp[k + j];
                         const float kd = __int_as_float(e.y);
                         if ((double) kd < c_q.triangle * (double) dbest) {
@@ -737,6 +738,7 @@ static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     q.prop_scale = s.prop_scale;
     q.triangle = s.triangle_factor;
     q.kc = s.kcoherence;
+    q.kc_try = (s.kc_try > 0 && s.kc_try < s.kcoherence) ? s.kc_try : s.kcoherence;
     q.ks = s.kcoherence_step;
     q.radius = s.radius;
     q.do_kcoh = s.kcoherence > 0;

@@ -62,6 +62,7 @@ pt_status run(pt_batch *B, const float *d_rgb, double *d_ann, cudaStream_t st) {
     qs.prop_scale = 1.0 / (1 + p.coherence_spatial);
     qs.triangle_factor = p.triangle_factor;
     qs.kcoherence = p.kcoherence;
+    qs.kc_try = p.gpu_kc_max;
     qs.kcoherence_step = p.kcoherence_step;
     qs.spatial = p.spatial;
     qs.do_rs = p.do_rs;

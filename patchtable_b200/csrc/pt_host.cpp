@@ -37,12 +37,13 @@ public:
     }
     int size() const { return (int) workers_.size(); }
     /* Runs fn(0) .. fn(parts - 1): parts - 1 on the workers, the last on the caller; returns when all
-       have finished. */
+       have finished.  Calls from several host threads take their turns. */
     void run(int parts, const std::function<void(int)> &fn) {
         if (parts <= 1 || workers_.empty()) {
             for (int i = 0; i < parts; i++) fn(i);
             return;
         }
+        std::lock_guard<std::mutex> turn(run_mu_);
         {
             std::lock_guard<std::mutex> g(mu_);
             job_ = &fn;
@@ -78,7 +79,7 @@ private:
     }
 
     std::vector<std::thread> workers_;
-    std::mutex mu_;
+    std::mutex mu_, run_mu_;
     std::condition_variable cv_, done_cv_;
     const std::function<void(int)> *job_ = nullptr;
     int next_ = 0, parts_ = 0, done_ = 0;

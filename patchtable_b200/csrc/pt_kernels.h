@@ -117,6 +117,7 @@ struct QuerySetup {
     int aw, ah, bw, bh;
     double prop_scale, triangle_factor;
     int kcoherence, kcoherence_step, radius;
+    int kc_try = 0;          /* k-coherence neighbours tried per patch (0 = all kcoherence) */
     int step = 1;            /* neighbour spacing of a pull pass */
     int pull_max = 0;        /* most neighbour candidates a pull scores per patch (0 = all) */
     int tile = 0;            /* query patches per CTA in choose / pull: 32, 64, 128, 256 (0 = 32) */
@@ -158,7 +159,7 @@ inline int pt_default_jump(const pt_params &p, int passes) {
    only on sweep kcoherence_iter when that is >= 0 (patchtable.h:3612); GPU pass i stands in for
    sweep floor(i * prop_iters / passes), i.e. passes 2n and 2n+1 for sweep n by default. */
 inline bool pt_pass_kcoh(const pt_params &p, int i, int passes) {
-    if (p.kcoherence <= 0) return false;
+    if (p.kcoherence <= 0 || p.gpu_kc_max < 0) return false;
     if (p.kcoherence_iter < 0) return true;
     const int iters = p.prop_iters > 0 ? p.prop_iters : 1;
     const int sweep = passes > 0 ? (int) ((long long) i * iters / passes) : 0;

@@ -98,6 +98,7 @@ extern "C" pt_status pt_table_lookup_device_noalloc(pt_table *t, const float *d_
     qs.prop_scale = 1.0 / (1 + p.coherence_spatial);
     qs.triangle_factor = p.triangle_factor;
     qs.kcoherence = p.kcoherence;
+    qs.kc_try = p.gpu_kc_max;
     qs.kcoherence_step = p.kcoherence_step;
     qs.spatial = p.spatial;
     qs.do_rs = p.do_rs;

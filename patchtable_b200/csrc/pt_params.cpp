@@ -139,7 +139,7 @@ pt_status apply_switches(pt_params *p, const std::vector<std::string> &argv) {
     INT_SW(grid_ndims) DBL_SW(table_ratio) INT_SW(prop_dist)
     BOOL_SW(is_descriptor) BOOL_SW(descriptor_padded)
     INT_SW(gpu_prop_passes) INT_SW(gpu_jump) INT_SW(gpu_pull_max) INT_SW(gpu_tile)
-    INT_SW(pca_samples) BOOL_SW(pca_mean) BOOL_SW(pca_subtract_mean) INT_SW(gpu_bands)
+    INT_SW(pca_samples) BOOL_SW(pca_mean) BOOL_SW(pca_subtract_mean) INT_SW(gpu_bands) INT_SW(gpu_kc_max)
 #undef INT_SW
 #undef BOOL_SW
 #undef DBL_SW
@@ -208,6 +208,7 @@ void pt_params_default(pt_params *p) {
     p->gpu_jump = 0;
     p->gpu_pull_max = 0;
     p->gpu_tile = 0;
+    p->gpu_kc_max = 0;
     pt_params_set_speed(p, 3);
 }
 

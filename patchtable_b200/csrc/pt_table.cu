@@ -714,6 +714,7 @@ pt_status lookup_device(pt_table *t, const float *a_rgb, int h, int w, double *d
     qs.prop_scale = 1.0 / (1 + p.coherence_spatial);
     qs.triangle_factor = p.triangle_factor;
     qs.kcoherence = p.kcoherence;
+    qs.kc_try = p.gpu_kc_max;
     qs.kcoherence_step = p.kcoherence_step;
     qs.spatial = p.spatial;
     qs.do_rs = p.do_rs;
@@ -865,6 +866,7 @@ struct BandIO {
     double *ann_out = nullptr;
     bool widen = false;
     cudaStream_t origin = nullptr;    /* the pipeline starts after and joins into this stream */
+    std::atomic<int> *recorded = nullptr;   /* bands whose download event this call has recorded */
 };
 
 pt_status enqueue_bands(pt_table *t, const BandIO &io, int h, int w, int B, int nb) {
@@ -886,6 +888,7 @@ pt_status enqueue_bands(pt_table *t, const BandIO &io, int h, int w, int B, int 
     qs.prop_scale = 1.0 / (1 + p.coherence_spatial);
     qs.triangle_factor = p.triangle_factor;
     qs.kcoherence = pt_pass_kcoh(p, 0, 1) ? p.kcoherence : 0;
+    qs.kc_try = p.gpu_kc_max;
     qs.kcoherence_step = p.kcoherence_step;
     qs.spatial = p.spatial;
     qs.do_rs = p.do_rs;
@@ -897,13 +900,18 @@ pt_status enqueue_bands(pt_table *t, const BandIO &io, int h, int w, int B, int 
     qs.allowed_index = p.allowed_index;
     QuerySetup qp = qs;
     qp.step = pt_pass_step(0, 1, pt_default_jump(p, 1));
+    /* Every band's upload is enqueued first, so the image streams in without gaps and each band's
+       kernels start as soon as its rows have arrived. */
+    for (int b = 0; b < nb; b++) {
+        const int r0 = b * B, r1 = std::min(eh, r0 + B);
+        const int p0 = b == 0 ? 0 : r0 + 7, p1 = b == nb - 1 ? h : r1 + 7;
+        const size_t px0 = (size_t) p0 * w * 3, npx = (size_t) (p1 - p0) * w * 3;
+        PT_CUDA(cudaMemcpyAsync(t->q_rgb.p + px0, a + px0, sizeof(float) * npx, cudaMemcpyHostToDevice, t->st_in));
+        PT_CUDA(cudaEventRecord(ev_in[b], t->st_in));
+    }
     for (int b = 0; b <= nb + 1; b++) {
         if (b < nb) {
             const int r0 = b * B, r1 = std::min(eh, r0 + B);
-            const int p0 = b == 0 ? 0 : r0 + 7, p1 = b == nb - 1 ? h : r1 + 7;
-            const size_t px0 = (size_t) p0 * w * 3, npx = (size_t) (p1 - p0) * w * 3;
-            PT_CUDA(cudaMemcpyAsync(t->q_rgb.p + px0, a + px0, sizeof(float) * npx, cudaMemcpyHostToDevice, t->st_in));
-            PT_CUDA(cudaEventRecord(ev_in[b], t->st_in));
             PT_CUDA(cudaStreamWaitEvent(sa, ev_in[b], 0));
             PT_TRY(pt_launch_descriptor_cells(p.ndims, p.nchroma, rgb, h, w, pt_color_mode(p), t->q_rgba.p,
                                               t->bins, t->to_bin.p, t->table.p, t->q_tcand.p, r0 / 8, (r1 - r0 + 7) / 8, sa));
@@ -944,6 +952,7 @@ pt_status enqueue_bands(pt_table *t, const BandIO &io, int h, int w, int B, int 
                                         t->st_out));
             }
             PT_CUDA(cudaEventRecord(ev_d[b - 2], t->st_out));
+            if (io.recorded) io.recorded->store(b - 1, std::memory_order_release);
         }
     }
     int k = 0;
@@ -987,17 +996,42 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     io.ann_out = ann_out;
     io.widen = widen;
     io.origin = t->st;
-    PT_TRY(enqueue_bands(t, io, h, w, B, nb));
+    /* Each band is widened as soon as it has arrived, by a second host thread (with the widening
+       pool), while this thread is still enqueueing the later bands: enqueueing a band takes about
+       as long as the GPU takes to run it, so widening only after the last enqueue would leave the
+       first bands' records waiting. */
+    std::atomic<int> recorded(0);
+    std::atomic<bool> stop(false);
+    cudaError_t widen_err = cudaSuccess;
+    cudaEvent_t *ev_d = t->band_ev.data() + 4 * nb;
+    std::thread widener;
+    if (widen) {
+        io.recorded = &recorded;
+        widener = std::thread([&] {
+            for (int b = 0; b < nb; b++) {
+                while (recorded.load(std::memory_order_acquire) <= b) {
+                    if (stop.load(std::memory_order_acquire)) return;
+                    std::this_thread::yield();
+                }
+                const cudaError_t e = cudaEventSynchronize(ev_d[b]);
+                if (e != cudaSuccess) { widen_err = e; return; }
+                const int r0 = b * B, r1 = std::min(eh, r0 + B);
+                const size_t o = (size_t) r0 * ew;
+                pt_expand_nnf(t->h_pos.p + o, t->h_d.p + o, (long long) (r1 - r0) * ew, ann_out + 3 * o);
+            }
+        });
+    }
+    const pt_status est = enqueue_bands(t, io, h, w, B, nb);
+    if (est != PT_OK) stop.store(true, std::memory_order_release);
+    if (widener.joinable()) widener.join();
+    if (est != PT_OK) {
+        for (cudaStream_t s2 : {t->st, t->st_in, t->st_choose, t->st_pull, t->st_out})
+            cudaStreamSynchronize(s2);       /* nothing of this call stays in flight */
+        return est;
+    }
     t->last_h2d = (long long) sizeof(float) * h * w * 3;
     t->last_d2h = (long long) (widen ? sizeof(int) + sizeof(float) : 3 * sizeof(double)) * P;
-    /* widen each band as soon as it has arrived */
-    cudaEvent_t *ev_d = t->band_ev.data() + 4 * nb;
-    for (int b = 0; b < nb && widen; b++) {
-        PT_CUDA(cudaEventSynchronize(ev_d[b]));
-        const int r0 = b * B, r1 = std::min(eh, r0 + B);
-        const size_t o = (size_t) r0 * ew;
-        pt_expand_nnf(t->h_pos.p + o, t->h_d.p + o, (long long) (r1 - r0) * ew, ann_out + 3 * o);
-    }
+    if (widen_err != cudaSuccess) return pt_fail(PT_CUDA_ERR, "band download: %s", cudaGetErrorString(widen_err));
     PT_CUDA(cudaStreamSynchronize(t->st));
     return PT_OK;
 }
@@ -1517,6 +1551,7 @@ pt_status pt_table_set_params(pt_table *t, const pt_params *p) {
     q.gpu_pull_max = p->gpu_pull_max;
     q.gpu_tile = p->gpu_tile;
     q.gpu_bands = p->gpu_bands;
+    q.gpu_kc_max = p->gpu_kc_max;
     q.do_rs = p->do_rs;
     q.spatial = p->spatial;
     q.init_random = p->init_random;

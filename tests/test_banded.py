@@ -31,6 +31,7 @@ def _device(t, a):
     (71, 100, "-speed 3 -coherence_spatial 4 -limit 2"),
     (333, 200, "-speed 3 -coherence_spatial 4 -limit 2 -gpu_tile 128"),
     (517, 263, "-speed 3 -coherence_spatial 4 -limit 2 -query_step 2 -gpu_jump 8"),
+    (300, 411, "-speed 3 -coherence_spatial 4 -limit 2 -gpu_kc_max -1"),
 ])
 def test_banded_host_lookup_equals_device(gpu, libc, h, w, sw):
     a, b = synth.pair(h, w, 90 + h)

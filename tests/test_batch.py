@@ -47,11 +47,11 @@ def _split(qb, imgs, ann):
     return out
 
 
-@pytest.mark.parametrize("sched", [(0, 0, 0), (1, 2, 1), (2, 2, 0)])
+@pytest.mark.parametrize("sched", [(0, 0, 0), (1, 2, 1), (2, 2, 0), (1, 2, 1, -1), (2, 2, 0, 1)])
 def test_batch_equals_per_image(gpu, libc, sched):
     import torch
     t, b = _table(libc)
-    t.params.gpu_prop_passes, t.params.gpu_jump, t.params.gpu_pull_max = sched
+    t.params.set_schedule(sched)
     imgs = _queries()
     single = [t.lookup(x) for x in imgs]
     host = t.lookup_batch(imgs)

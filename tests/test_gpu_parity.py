@@ -352,6 +352,32 @@ def test_nnf_quality_and_distances(gpu, oracle, libc, seed, sw):
     assert np.array_equal(ann, gt.lookup(a))
 
 
+@pytest.mark.parametrize("sw", ["", "-coherence_spatial 4 -kcoherence 4", "-speed 6"])
+def test_kcoherence_cap(gpu, oracle, libc, sw):
+    """gpu_kc_max: a cap at or above kcoherence changes nothing; -1 is exactly the query without
+    the k-coherence step (kcoherence_iter past every sweep); 1 tries only each list's first
+    neighbour.  Distances stay exact, the table is untouched."""
+    a, b = synth.pair(200, 260, 31)
+    p = ptb.PatchTableParams(sw + " -limit 10")
+    srand_all(libc, 1)
+    gt = ptb.PatchTable(p, b)
+    table = gt.table()
+    full = gt.lookup(a)
+    p.gpu_kc_max = p.kcoherence
+    assert np.array_equal(gt.lookup(a), full)
+    p.gpu_kc_max = -1
+    none = gt.lookup(a)
+    check_nnf(oracle, a, b, none, sample=500)
+    p.gpu_kc_max = 0
+    p.kcoherence_iter = 99
+    assert np.array_equal(gt.lookup(a), none)
+    p.kcoherence_iter = -1
+    p.gpu_kc_max = 1
+    one = gt.lookup(a)
+    check_nnf(oracle, a, b, one, sample=500)
+    assert np.array_equal(gt.table(), table)
+
+
 def test_query_of_another_size_and_reuse(gpu, oracle, libc):
     _, b = synth.pair(150, 170, 7)
     p = ptb.PatchTableParams("-limit 2")

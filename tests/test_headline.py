@@ -5,8 +5,8 @@
   reference sources compiled in place).
 * GPU: given that descriptor, the GPU build's partition, table after the DT and k-coherence set
   have the reference's digests, bit for bit.
-* GPU: every query schedule the bench may time (its SCHEDULES, at the CTA width it usually picks)
-  returns exact, in-bounds distances (NNF_DIST bit-exact with patch_dist_exact, within 1e-5 of a
+* GPU: every query schedule the bench may time (its SCHEDULES, at the CTA width it usually picks,
+  with and without the k-coherence step) returns exact, in-bounds distances (NNF_DIST bit-exact with patch_dist_exact, within 1e-5 of a
   float64 recompute), the same field through the device entry point and the host lookup, and a
   mean NNF distance at most 1% above the reference's.
 """
@@ -73,13 +73,13 @@ def c2_table(gpu, libc, c2_pair):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("sched", SCHEDULES, ids=["%d/%d/%d" % s for s in SCHEDULES])
+@pytest.mark.parametrize("sched", SCHEDULES, ids=[ptb.schedule_name(s) for s in SCHEDULES])
 def test_benchmarked_schedules(gpu, oracle, c2_pair, c2_table, sched):
     import torch
     a, b = c2_pair
     H, W = a.shape[:2]
     p = c2_table.params
-    p.gpu_prop_passes, p.gpu_jump, p.gpu_pull_max = sched
+    p.set_schedule(sched)
     p.gpu_tile = 64
     try:
         host = c2_table.lookup(a)
@@ -91,5 +91,5 @@ def test_benchmarked_schedules(gpu, oracle, c2_pair, c2_table, sched):
         check_nnf(oracle, a, b, host, sample=1500)
         assert mean_dist(host) <= MEAN_DIST_SLACK * GOLDEN["mean_dist"], (mean_dist(host), GOLDEN["mean_dist"])
     finally:
-        p.gpu_prop_passes = p.gpu_jump = p.gpu_pull_max = 0
+        p.set_schedule((0, 0, 0))
         p.gpu_tile = 0

@@ -24,7 +24,8 @@ def _fn():
 
 
 @pytest.mark.parametrize("sw", ["-limit 2", "-limit 2 -prop_iters 0", "-limit 2 -do_prop 0", "-limit 2 -gpu_tile 128",
-                                "-limit 2 -kcoherence_iter 1 -gpu_tile 64"])
+                                "-limit 2 -kcoherence_iter 1 -gpu_tile 64", "-limit 2 -gpu_kc_max -1",
+                                "-limit 2 -gpu_kc_max 1 -gpu_prop_passes 1"])
 def test_noalloc_lookup_matches_device_lookup_on_consecutive_calls(sw):
     import torch
     assert torch.cuda.is_available()
