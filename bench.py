@@ -62,7 +62,7 @@ def reference_mean_dist():
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -457,13 +457,21 @@ def main():
     first_build_s = time.perf_counter() - t0
     first.close()
     del first
-    ctypes.CDLL(None).srand(1)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    table = ptb.PatchTable(params, b)
-    torch.cuda.synchronize()
-    build_s = time.perf_counter() - t0
-    build_stage_ms = table.build_profile()
+    # warm builds: the median of three (the host's page-locking, allocation and thread start-up
+    # make single builds vary); the last table answers the queries
+    builds = []
+    table = None
+    for _ in range(3):
+        if table is not None:
+            table.close()
+        ctypes.CDLL(None).srand(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        table = ptb.PatchTable(params, b)
+        torch.cuda.synchronize()
+        builds.append((time.perf_counter() - t0, table.build_profile()))
+    build_s, build_stage_ms = sorted(builds, key=lambda x: x[0])[1]
+    build_s_all = [x[0] for x in builds]
 
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
@@ -620,7 +628,8 @@ def main():
         "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded generator, patchtable_b200/synth.py)",
         "config": {"workload": WORKLOAD["name"], "patches_per_step": P, "image": [H, W], "table_image": list(b.shape[:2]),
-                   "build_s": build_s, "build_stage_ms": build_stage_ms, "first_build_s": first_build_s, "mean_nnf_dist": md, "mean_nnf_dist_e2e": md_e2e,
+                   "build_s": build_s, "build_s_all": build_s_all, "build_stage_ms": build_stage_ms,
+                   "first_build_s": first_build_s, "mean_nnf_dist": md, "mean_nnf_dist_e2e": md_e2e,
                    "e2e_ms": {"mean": 1000 * sum(e2e_s) / len(e2e_s), "median": 1000 * float(np.median(e2e_s)),
                               "min": 1000 * min(e2e_s), "max": 1000 * max(e2e_s), "calls": len(e2e_s)},
                    "reference_mean_nnf_dist": ref_md,
