@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <condition_variable>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -90,18 +91,19 @@ private:
 std::mutex g_pool_mu;
 int g_threads = 0;                 /* 0: not chosen yet */
 bool g_widen = true;               /* false: the GPU writes float64 records and they are copied */
-Pool *g_pool = nullptr;
+std::shared_ptr<Pool> g_pool;      /* a lookup holds its own reference while it widens, so a
+                                      pt_set_host_threads meanwhile retires the old pool safely */
 
 int default_threads() {
     const unsigned hw = std::thread::hardware_concurrency();
     return (int) std::max(1u, std::min(8u, hw ? hw : 1u));
 }
 
-Pool &pool() {
+std::shared_ptr<Pool> pool() {
     std::lock_guard<std::mutex> g(g_pool_mu);
     if (!g_threads) g_threads = default_threads();
-    if (!g_pool) g_pool = new Pool(g_threads - 1);      /* the caller is the last worker */
-    return *g_pool;
+    if (!g_pool) g_pool = std::make_shared<Pool>(g_threads - 1);      /* the caller is the last worker */
+    return g_pool;
 }
 
 }  // namespace
@@ -137,7 +139,8 @@ static void widen_range(const int *pos, const float *dist, long long i0, long lo
 
 void pt_expand_nnf(const int *pos, const float *dist, long long n, double *ann) {
     if (n <= 0) return;
-    Pool &pl = pool();
+    const std::shared_ptr<Pool> keep = pool();
+    Pool &pl = *keep;
     const int parts = (int) std::min<long long>(pl.size() + 1, std::max<long long>(1, n / 4096));
     long long per = (n + parts - 1) / parts;
     per = (per + 1) & ~1ll;                 /* even: a part's pairs keep the alignment of the whole */
@@ -153,8 +156,7 @@ extern "C" int pt_set_host_threads(int n) {
     g_widen = n >= 0;
     const int want = n > 0 ? std::min(n, 256) : default_threads();
     if (want != g_threads) {
-        delete g_pool;          /* joins the old workers */
-        g_pool = nullptr;
+        g_pool.reset();         /* the old workers are joined once no lookup holds the pool */
         g_threads = want;
     }
     return old;
