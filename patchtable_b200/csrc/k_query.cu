@@ -70,6 +70,11 @@ __device__ __forceinline__ void count_work(unsigned long long *counters, unsigne
 }
 
 constexpr int TWD = 32;                   /* query patches per CTA row segment when none is chosen */
+/* Threads per SM the register caps of the lean choose and the one-candidate pull leave room for.
+   Both compile to 56 registers under these caps; tighter caps (20 x 64 or 24 x 64 threads per
+   SM: 48 or 40 registers, no spills) measured 1-3 % slower at 1080p. */
+constexpr int CHOOSE_LEAN_LANES = 12 * 64;
+constexpr int PULL_ONE_LANES = 16 * 64;
 constexpr int TWD_DESC = 64;              /* query patches per CTA in descriptor mode */
 
 /* Stages the 8 pixel rows under a CTA's row segment of TW query patches in shared memory
@@ -243,7 +248,9 @@ struct LearnedArgs {
    instantiation replaces, for patches whose proposal confidence reaches the threshold, the table
    candidate by the network's proposals (scored best-first in groups of three) and, unless
    configured otherwise, skips k-coherence for them. */
-template<int TW, bool LEARNED, bool DESC>
+/* LEAN: the table step only (no further tables, k-coherence, spatial or random search), so the
+   registers those steps need are not reserved. */
+template<int TW, bool LEARNED, bool DESC, bool LEAN = false>
 __device__ __forceinline__ void
 choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const float4 *__restrict__ b,
            const int *__restrict__ cur_pos, const float *__restrict__ cur_d, const int *__restrict__ tcand,
@@ -313,7 +320,7 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
             /* Further tables (patchtable.h:3711-3735): each entry is scored unless it equals the
                best so far or the previous table's entry. */
             const size_t np = (size_t) c_q.ew * c_q.eh;
-            for (int k = 0; k < c_q.ntc; k++) {
+            for (int k = 0; k < (LEAN ? 0 : c_q.ntc); k++) {
                 const int v1 = c_q.tcand_more[(size_t) k * np + p];
                 const int xs1 = pt_x(v1) - 7, ys1 = pt_y(v1) - 7;
                 if ((xs1 != xb || ys1 != yb) && (xs1 != xs || ys1 != ys)) {
@@ -329,7 +336,7 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
         const bool repeat = use_done && kc_done[p] == kc_src;
         bool accepted = false;
         const bool kc_here = !LEARNED || !confident || la.kcoh_confident;
-        if (c_q.do_kcoh && kc_here && !repeat && xb < c_q.bew && yb < c_q.beh) {
+        if (!LEAN && c_q.do_kcoh && kc_here && !repeat && xb < c_q.bew && yb < c_q.beh) {
             /* The reference tries the list in order and stops at the first neighbour whose stored
                distance reaches triangle * best.  Here two neighbours are scored together with the
                best known before the group as the early-exit bound, then the sequential decisions
@@ -374,9 +381,9 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
                 }
             }
         }
-        if (c_q.do_kcoh) kc_done[p] = (repeat || !accepted) ? kc_src : -1;
+        if (!LEAN && c_q.do_kcoh) kc_done[p] = (repeat || !accepted) ? kc_src : -1;
         const bool have = xb < c_q.bew && yb < c_q.beh;
-        if (c_q.spatial > 0 && have) {
+        if (!LEAN && c_q.spatial > 0 && have) {
             /* Spatial search (patchtable.h:3855-3873): every other patch of the (2s+1)^2 window
                around the best match, rows then columns, scored in pairs and replayed in order. */
             const int S = c_q.spatial, xb0 = xb, yb0 = yb;
@@ -409,7 +416,7 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
                 for (int j = 0; j < G; j++)
                     if (((m >> j) & 1) && d[j] < dbest) { dbest = d[j]; dch = d[j]; xb = pt_x(cg[j]); yb = pt_y(cg[j]); }
             }
-        } else if (c_q.do_rs && have) {
+        } else if (!LEAN && c_q.do_rs && have) {
             /* Random search (patchtable.h:3874-3903): one of the 8 neighbours of the best match.
                dx, dy + 1 for r = 0..7 are packed two bits each: {-1,0,1,-1,1,-1,0,1},
                {-1,-1,-1,0,0,1,1,1}. */
@@ -435,14 +442,14 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
 /* At least 10 x 64 threads' worth of CTAs per SM: the register budget this leaves keeps the gather
    latency hidden without the spills of tighter caps (measured at 1080p, 64 patches per CTA:
    choose 0.70 ms unrestricted, 0.611 at 10 x 64, 0.619 at 12 x 64, 0.625 at 16 x 64). */
-template<int TW, bool LEARNED, bool DESC>
-__global__ void __launch_bounds__(TW, (10 * 64) / TW)
+template<int TW, bool LEARNED, bool DESC, bool LEAN = false>
+__global__ void __launch_bounds__(TW, (LEAN ? CHOOSE_LEAN_LANES : 10 * 64) / TW)
 k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
               const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
               int *ch_pos, float *ch_d, int *kc_done, int use_done, unsigned long long *counters, const LearnedArgs la) {
     extern __shared__ float4 atile[];
-    choose_seg<TW, LEARNED, DESC>(c_q, atile, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done,
-                                  use_done, counters, la, blockIdx.x * TW, blockIdx.y + c_q.row0);
+    choose_seg<TW, LEARNED, DESC, LEAN>(c_q, atile, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done,
+                                        use_done, counters, la, blockIdx.x * TW, blockIdx.y + c_q.row0);
 }
 
 /* Step 4 as a pull: the best of the stored match and every neighbour's chosen offset applied to
@@ -452,7 +459,10 @@ k_choose_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__res
    Neighbours sit `step` patches apart; passes with decreasing steps (jump flooding) carry an
    offset across a region in a logarithmic number of passes, where the reference's sequential
    sweep carries it along a whole row in one sweep. */
-template<int TW, int R, bool DESC>
+/* ONE: a single neighbour candidate per patch (pull_max 1).  The candidate is the one the
+   general path would sort first -- among distinct candidates keyed by their first occurrence, the
+   smallest key, the earliest on ties -- found in one streaming pass, and it is scored alone. */
+template<int TW, int R, bool DESC, bool ONE = false>
 __device__ __forceinline__ void
 pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const float4 *__restrict__ b,
          const int *__restrict__ cur_pos, const float *__restrict__ cur_d, const int *__restrict__ ch_pos,
@@ -477,14 +487,52 @@ pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const fl
             if (pt_x(cp) < c_q.bew && pt_y(cp) < c_q.beh && cp != bpos && ch_d[p] < bd) { bd = ch_d[p]; bpos = cp; }
         }
         constexpr int MAXC = (2 * R + 1) * (2 * R + 1) - 1;
+        const int S = c_q.step;
+        int nc = 0;
+        if constexpr (ONE) {
+            /* the distinct candidates seen so far, newest first (fixed register slots) */
+            int seen[MAXC];
+#pragma unroll
+            for (int t = 0; t < MAXC; t++) seen[t] = -1;
+            int best = -1;
+            float bestk = finf();
+#pragma unroll
+            for (int dy = -R; dy <= R; dy++) {
+#pragma unroll
+                for (int dx = -R; dx <= R; dx++) {
+                    if (dx == 0 && dy == 0) continue;
+                    const int ny = y + S * dy, nx = x + S * dx;
+                    if (ny < 0 || ny >= c_q.eh || nx < 0 || nx >= c_q.ew) continue;
+                    const int q = ny * c_q.ew + nx;
+                    const int cp = ch_pos[q];
+                    const int xs = pt_x(cp) - S * dx, ys = pt_y(cp) - S * dy;
+                    if (xs < 0 || ys < 0 || xs >= c_q.bew || ys >= c_q.beh) continue;
+                    if (c_q.allowed && __ldg(c_q.allowed + (size_t) ys * c_q.bew + xs) != c_q.allowed_index) continue;
+                    const int c = pt_xy(xs, ys);
+                    bool dup = c == bpos;
+#pragma unroll
+                    for (int t = 0; t < MAXC; t++) dup |= seen[t] == c;
+                    if (dup) continue;
+#pragma unroll
+                    for (int t = MAXC - 1; t > 0; t--) seen[t] = seen[t - 1];
+                    seen[0] = c;
+                    const float k = ch_d[q];
+                    if (best < 0 || k < bestk) { bestk = k; best = c; }
+                    nc++;
+                }
+            }
+            if (nc > 0) {
+                nc = 1;
+                const float d = dist1<TW, DESC>(aq, c_q, b, pt_x(best), pt_y(best), bd, rows);
+                if (d < bd) { bd = d; bpos = best; }
+            }
+        } else {
         /* distinct neighbour candidates sorted by the neighbour's own distance (ties keep the
            neighbour order), kept in registers: every slot index is known at compile time */
         int cand[MAXC];
         float key[MAXC];
 #pragma unroll
         for (int t = 0; t < MAXC; t++) { cand[t] = -1; key[t] = finf(); }
-        int nc = 0;
-        const int S = c_q.step;
 #pragma unroll
         for (int dy = -R; dy <= R; dy++) {
 #pragma unroll
@@ -528,6 +576,7 @@ pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const fl
                     if (((m >> g) & 1) && d[g] < bd) { bd = d[g]; bpos = cg[g]; }
             }
         }
+        }
         ne += nc;
         if (c_q.ann) {                          /* k_output fused: x, y, dist of the final field */
             double *o = c_q.ann + 3 * (size_t) p;
@@ -545,14 +594,14 @@ pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const fl
 /* At most 14 x 64 threads' worth of CTAs per SM (73 registers, 10 bytes of spills): the pull is
    latency-bound, and the extra resident warps hide the gathers (measured at 1080p with one
    candidate per patch: 0.341 -> 0.286 ms; at 16 x 64 the spills grow to 200 bytes and it slows). */
-template<int TW, int R, bool DESC>
-__global__ void __launch_bounds__(TW, (14 * 64) / TW)
+template<int TW, int R, bool DESC, bool ONE = false>
+__global__ void __launch_bounds__(TW, (ONE ? PULL_ONE_LANES : 14 * 64) / TW)
 k_pull_tile(const QPlan c_q, const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
             const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
             int *nxt_pos, float *nxt_d, unsigned long long *counters) {
     extern __shared__ float4 atile[];
-    pull_seg<TW, R, DESC>(c_q, atile, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, counters, blockIdx.x * TW,
-                          blockIdx.y + c_q.row0);
+    pull_seg<TW, R, DESC, ONE>(c_q, atile, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, counters, blockIdx.x * TW,
+                               blockIdx.y + c_q.row0);
 }
 
 /* ---- batched queries: many images, one launch per phase over a flattened segment list ---- */
@@ -797,9 +846,11 @@ pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const fl
         return PT_OK;
     }
 #define PT_CHOOSE_T(T) { dim3 grid((q.ew + T - 1) / T, q.rows); \
-        k_choose_tile<T, false, false><<<grid, T, atile_bytes(T), st>>>(q, a, b, cur_pos, cur_d, tcand, kcoh, \
-                                                                                    do_table, ch_pos, ch_d, kc_done, use_done, \
-                                                                                    evals, none); }
+        if (lean) k_choose_tile<T, false, false, true><<<grid, T, atile_bytes(T), st>>>( \
+            q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done, use_done, evals, none); \
+        else k_choose_tile<T, false, false><<<grid, T, atile_bytes(T), st>>>( \
+            q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done, use_done, evals, none); }
+    const bool lean = !q.do_kcoh && q.ntc == 0 && q.spatial == 0 && !q.do_rs;
     switch (q.tile) {
         case 32: PT_CHOOSE_T(32) break;
         case 64: PT_CHOOSE_T(64) break;
@@ -857,8 +908,11 @@ pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const floa
         return PT_OK;
     }
 #define PT_PULL_T(T, RR) { dim3 grid((q.ew + T - 1) / T, q.rows); \
-        k_pull_tile<T, RR, false><<<grid, T, atile_bytes(T), st>>>(q, a, b, cur_pos, cur_d, ch_pos, ch_d, \
-                                                                                nxt_pos, nxt_d, evals); }
+        if (one) k_pull_tile<T, RR, false, true><<<grid, T, atile_bytes(T), st>>>( \
+            q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals); \
+        else k_pull_tile<T, RR, false><<<grid, T, atile_bytes(T), st>>>( \
+            q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals); }
+    const bool one = q.pull_max == 1;
     switch (q.tile) {
         case 32: if (r1) PT_PULL_T(32, 1) else PT_PULL_T(32, 2) break;
         case 64: if (r1) PT_PULL_T(64, 1) else PT_PULL_T(64, 2) break;
