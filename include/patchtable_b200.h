@@ -364,9 +364,16 @@ int64_t pt_device_bytes_in_use(void);
    24-byte records into the caller's buffer while later rows are still computed.  n = 0 restores
    the default, min(8, hardware threads); n < 0 turns the host widening off (the GPU writes the
    float64 records and they are copied as they are: three times the bytes over PCIe, no host
-   work).  Returns the previous count (-1 when widening was off).  Not to be called while a lookup
-   runs. */
+   work).  Returns the previous count (-1 when widening was off).  A lookup already widening
+   finishes with the threads it started with. */
 int pt_set_host_threads(int n);
+
+/* Specialised query kernels (no reference counterpart): the choose of a pass that has only the
+   table step, and the pull of a schedule with one neighbour candidate, run as variants compiled
+   without the other steps (fewer registers, more resident warps); their results are bit-identical
+   to the general kernels'.  on = 0 runs the general kernels everywhere, which the tests use to
+   compare the two; returns the previous setting (default 1).  Process-wide. */
+int pt_set_lean_kernels(int on);
 /* Bytes the last pt_table_lookup on this table copied host -> device and device -> host. */
 pt_status pt_table_last_transfer(const pt_table *t, int64_t *h2d_bytes, int64_t *d2h_bytes);
 

@@ -155,6 +155,8 @@ def lib() -> C.CDLL:
     L.pt_last_error.restype = C.c_char_p
     L.pt_version.restype = C.c_char_p
     L.pt_set_host_threads.argtypes = [C.c_int]
+    L.pt_set_lean_kernels.argtypes = [C.c_int]
+    L.pt_set_lean_kernels.restype = C.c_int
     L.pt_table_last_transfer.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.pt_set_spin_limit.argtypes = [C.c_int64]
     L.pt_set_spin_limit.restype = C.c_int64
@@ -576,6 +578,12 @@ def descriptor(params: PatchTableParams, img):
 def set_host_threads(n: int) -> int:
     """Host threads that widen downloaded NNFs to float64 (n <= 0: default).  Returns the previous count."""
     return int(lib().pt_set_host_threads(int(n)))
+
+
+def set_lean_kernels(on: bool) -> bool:
+    """Specialised choose / pull variants (bit-identical to the general kernels); False runs the
+    general kernels.  Returns the previous setting."""
+    return bool(lib().pt_set_lean_kernels(1 if on else 0))
 
 
 def set_spin_limit(polls: int) -> int:

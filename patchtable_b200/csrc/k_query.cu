@@ -16,6 +16,7 @@
    already reaches the value it must beat (the partial sum can only grow). */
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
 
 #include "pt_internal.h"
@@ -628,8 +629,8 @@ __device__ __forceinline__ long long next_segment(unsigned long long *work) {
 }
 
 /* Persistent choose over every row segment of every image, handed out by a work counter. */
-template<int TW>
-__global__ void __launch_bounds__(TW, (10 * 64) / TW)
+template<int TW, bool LEAN = false>
+__global__ void __launch_bounds__(TW, (LEAN ? CHOOSE_LEAN_LANES : 10 * 64) / TW)
 k_choose_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, long long nseg, int twi,
                const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
                const float *__restrict__ cur_d, const int *__restrict__ tcand, const int2 *__restrict__ kcoh, int do_table,
@@ -647,14 +648,14 @@ k_choose_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, l
         QPlan q = base;
         q.aw = g.w; q.ah = g.h; q.ew = g.ew; q.eh = g.eh;
         const long long o = g.patch_off;
-        choose_seg<TW, false, false>(q, atile, a + g.pix_off, b, cur_pos ? cur_pos + o : nullptr, cur_d ? cur_d + o : nullptr,
-                                     tcand + o, kcoh, do_table, ch_pos + o,
-                              ch_d + o, kc_done + o, use_done, counters, none, x0, y);
+        choose_seg<TW, false, false, LEAN>(q, atile, a + g.pix_off, b, cur_pos ? cur_pos + o : nullptr,
+                                           cur_d ? cur_d + o : nullptr, tcand + o, kcoh, do_table, ch_pos + o, ch_d + o,
+                                           kc_done + o, use_done, counters, none, x0, y);
     }
 }
 
-template<int TW, int R>
-__global__ void __launch_bounds__(TW, (14 * 64) / TW)
+template<int TW, int R, bool ONE = false>
+__global__ void __launch_bounds__(TW, (ONE ? PULL_ONE_LANES : 14 * 64) / TW)
 k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, long long nseg, int twi,
              const float4 *__restrict__ a, const float4 *__restrict__ b, const int *__restrict__ cur_pos,
              const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
@@ -670,9 +671,8 @@ k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, lon
         q.aw = g.w; q.ah = g.h; q.ew = g.ew; q.eh = g.eh;
         const long long o = g.patch_off;
         if (base.ann) q.ann = base.ann + 3 * o;        /* last pass: this image's NNF records */
-        pull_seg<TW, R, false>(q, atile, a + g.pix_off, b, cur_pos ? cur_pos + o : nullptr, cur_d ? cur_d + o : nullptr, ch_pos + o,
-                               ch_d + o, nxt_pos + o, nxt_d + o,
-                        counters, x0, y);
+        pull_seg<TW, R, false, ONE>(q, atile, a + g.pix_off, b, cur_pos ? cur_pos + o : nullptr,
+                                    cur_d ? cur_d + o : nullptr, ch_pos + o, ch_d + o, nxt_pos + o, nxt_d + o, counters, x0, y);
     }
 }
 
@@ -780,6 +780,22 @@ __global__ void k_output(int n, const int *__restrict__ pos, const float *__rest
 
 }  // namespace
 
+namespace {
+
+std::atomic<int> g_lean_kernels{1};
+
+/* The specialised variants apply: the choose of a pass with only the table step, the pull of a
+   schedule with one neighbour candidate (image mode; descriptor mode keeps the general kernels). */
+bool lean_choose(const QPlan &q) {
+    return g_lean_kernels.load(std::memory_order_relaxed) && !q.adesc && !q.do_kcoh && q.ntc == 0 && q.spatial == 0 &&
+           !q.do_rs;
+}
+bool one_pull(const QPlan &q) { return g_lean_kernels.load(std::memory_order_relaxed) && !q.adesc && q.pull_max == 1; }
+
+}  // namespace
+
+extern "C" int pt_set_lean_kernels(int on) { return g_lean_kernels.exchange(on ? 1 : 0); }
+
 static pt_status make_qplan(const QuerySetup &s, QPlan &q) {
     memset(&q, 0, sizeof(q));
     q.aw = s.aw; q.ah = s.ah; q.ew = s.aw - 7; q.eh = s.ah - 7;
@@ -850,7 +866,7 @@ pt_status pt_launch_choose(const QuerySetup &s, int n, const float4 *a, const fl
             q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done, use_done, evals, none); \
         else k_choose_tile<T, false, false><<<grid, T, atile_bytes(T), st>>>( \
             q, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, kc_done, use_done, evals, none); }
-    const bool lean = !q.do_kcoh && q.ntc == 0 && q.spatial == 0 && !q.do_rs;
+    const bool lean = lean_choose(q);
     switch (q.tile) {
         case 32: PT_CHOOSE_T(32) break;
         case 64: PT_CHOOSE_T(64) break;
@@ -912,7 +928,7 @@ pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const floa
             q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals); \
         else k_pull_tile<T, RR, false><<<grid, T, atile_bytes(T), st>>>( \
             q, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals); }
-    const bool one = q.pull_max == 1;
+    const bool one = one_pull(q);
     switch (q.tile) {
         case 32: if (r1) PT_PULL_T(32, 1) else PT_PULL_T(32, 2) break;
         case 64: if (r1) PT_PULL_T(64, 1) else PT_PULL_T(64, 2) break;
@@ -963,9 +979,13 @@ pt_status pt_launch_choose_batch(const QuerySetup &s, const PtBatchImage *imgs, 
     if (nseg <= 0) return PT_OK;
     PT_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st));
 #define PT_CHOOSE_B(T) { const size_t sm = atile_bytes(T); \
-        const int g = persistent_grid(k_choose_batch<T>, T, sm, nseg); \
-        k_choose_batch<T><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, ch_d, \
-                                            kc_done, use_done, evals, work); }
+        if (lean) { const int g = persistent_grid(k_choose_batch<T, true>, T, sm, nseg); \
+            k_choose_batch<T, true><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, tcand, kcoh, do_table, \
+                                                      ch_pos, ch_d, kc_done, use_done, evals, work); } \
+        else { const int g = persistent_grid(k_choose_batch<T>, T, sm, nseg); \
+            k_choose_batch<T><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, tcand, kcoh, do_table, ch_pos, \
+                                                ch_d, kc_done, use_done, evals, work); } }
+    const bool lean = lean_choose(q);
     switch (BATCH_TW[twi]) {
         case 32: PT_CHOOSE_B(32) break;
         case 64: PT_CHOOSE_B(64) break;
@@ -986,9 +1006,13 @@ pt_status pt_launch_pull_batch(const QuerySetup &s, const PtBatchImage *imgs, in
     if (nseg <= 0) return PT_OK;
     PT_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned long long), st));
 #define PT_PULL_B(T, RR) { const size_t sm = atile_bytes(T); \
-        const int g = persistent_grid(k_pull_batch<T, RR>, T, sm, nseg); \
-        k_pull_batch<T, RR><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, evals, \
-                                              work); }
+        if (one) { const int g = persistent_grid(k_pull_batch<T, RR, true>, T, sm, nseg); \
+            k_pull_batch<T, RR, true><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, \
+                                                        nxt_d, evals, work); } \
+        else { const int g = persistent_grid(k_pull_batch<T, RR>, T, sm, nseg); \
+            k_pull_batch<T, RR><<<g, T, sm, st>>>(q, imgs, n, nseg, twi, a, b, cur_pos, cur_d, ch_pos, ch_d, nxt_pos, nxt_d, \
+                                                  evals, work); } }
+    const bool one = one_pull(q);
     const bool r1 = q.radius <= 1;
     switch (BATCH_TW[twi]) {
         case 32: if (r1) PT_PULL_B(32, 1) else PT_PULL_B(32, 2) break;
