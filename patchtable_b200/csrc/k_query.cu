@@ -518,12 +518,12 @@ pull_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const fl
                     for (int t = MAXC - 1; t > 0; t--) seen[t] = seen[t - 1];
                     seen[0] = c;
                     const float k = ch_d[q];
-                    if (best < 0 || k < bestk) { bestk = k; best = c; }
+                    if (k < bestk) { bestk = k; best = c; }   /* the general sort's insertion rule */
                     nc++;
                 }
             }
-            if (nc > 0) {
-                nc = 1;
+            nc = best >= 0 ? 1 : 0;
+            if (nc) {
                 const float d = dist1<TW, DESC>(aq, c_q, b, pt_x(best), pt_y(best), bd, rows);
                 if (d < bd) { bd = d; bpos = best; }
             }
