@@ -244,11 +244,14 @@ k_descriptor_batch(const DescPlan c_plan, const CellPlan cp, const PtBatchImage 
                    unsigned long long *work) {
     extern __shared__ __align__(16) float smem[];
     __shared__ long long s_next;
-    for (;;) {
-        if (threadIdx.x == 0) s_next = (long long) atomicAdd(work, 1ull);   /* tiles go out one at a time */
-        __syncthreads();
-        const long long t = s_next;
-        if (t >= ntiles) break;
+    /* tiles go out one at a time; a CTA claims its next tile when it starts the current one and
+       reads the claim after it, so the counter's round trip overlaps the work */
+    if (threadIdx.x == 0) s_next = (long long) atomicAdd(work, 1ull);
+    __syncthreads();
+    long long t = s_next;
+    while (t < ntiles) {
+        long long claim = 0;
+        if (threadIdx.x == 0) claim = (long long) atomicAdd(work, 1ull);
         int lo = 0, hi = n - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
@@ -261,6 +264,9 @@ k_descriptor_batch(const DescPlan c_plan, const CellPlan cp, const PtBatchImage 
                          CELLS ? nullptr : desc + g.patch_off * ds, ds, g.eh, g.ew, (int) (lt % tpr) * TW, (int) (lt / tpr) * TH,
                          &cp, CELLS ? cp.tcand + g.patch_off : nullptr);
         __syncthreads();                                 /* the next tile reuses the shared memory and s_next */
+        if (threadIdx.x == 0) s_next = claim;
+        __syncthreads();
+        t = s_next;
     }
 }
 

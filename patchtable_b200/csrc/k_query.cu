@@ -617,15 +617,26 @@ __device__ __forceinline__ int owner(const PtBatchImage *__restrict__ imgs, int 
     return lo;
 }
 
-/* The next row segment for this CTA from the launch's work counter (zeroed before the launch):
-   segments go out in order, one at a time, to whichever CTA is free, so uneven segment costs
-   cannot leave some CTAs with a longer share. */
-__device__ __forceinline__ long long next_segment(unsigned long long *work) {
+/* Runs body(s) for the row segments this CTA takes from the launch's work counter (zeroed before
+   the launch): segments go out in order, one at a time, to whichever CTA is free, so uneven
+   segment costs cannot leave some CTAs with a longer share.  A CTA claims its next segment when it
+   starts the current one and reads the claim only after it, so the counter's round trip overlaps
+   the work. */
+template<class Body>
+__device__ __forceinline__ void for_each_segment(unsigned long long *work, long long nseg, Body &&body) {
     __shared__ long long s_next;
-    __syncthreads();                           /* the previous segment is done with s_next and atile */
     if (threadIdx.x == 0) s_next = (long long) atomicAdd(work, 1ull);
     __syncthreads();
-    return s_next;
+    long long s = s_next;
+    while (s < nseg) {
+        long long claim = 0;
+        if (threadIdx.x == 0) claim = (long long) atomicAdd(work, 1ull);
+        body(s);
+        __syncthreads();                       /* every thread is done with s_next and the staged tile */
+        if (threadIdx.x == 0) s_next = claim;
+        __syncthreads();
+        s = s_next;
+    }
 }
 
 /* Persistent choose over every row segment of every image, handed out by a work counter. */
@@ -639,7 +650,7 @@ k_choose_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, l
     extern __shared__ float4 atile[];
     LearnedArgs none;
     none.cand = nullptr; none.conf = nullptr; none.threshold = 0.f; none.kcoh_confident = 0; none.counters = nullptr;
-    for (long long s = next_segment(work); s < nseg; s = next_segment(work)) {
+    for_each_segment(work, nseg, [&](long long s) {
         const int i = owner(imgs, n, s, twi);
         const PtBatchImage &g = imgs[i];
         const long long ls = s - g.seg_off[twi];
@@ -651,7 +662,7 @@ k_choose_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, l
         choose_seg<TW, false, false, LEAN>(q, atile, a + g.pix_off, b, cur_pos ? cur_pos + o : nullptr,
                                            cur_d ? cur_d + o : nullptr, tcand + o, kcoh, do_table, ch_pos + o, ch_d + o,
                                            kc_done + o, use_done, counters, none, x0, y);
-    }
+    });
 }
 
 template<int TW, int R, bool ONE = false>
@@ -661,7 +672,7 @@ k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, lon
              const float *__restrict__ cur_d, const int *__restrict__ ch_pos, const float *__restrict__ ch_d,
              int *nxt_pos, float *nxt_d, unsigned long long *counters, unsigned long long *work) {
     extern __shared__ float4 atile[];
-    for (long long s = next_segment(work); s < nseg; s = next_segment(work)) {
+    for_each_segment(work, nseg, [&](long long s) {
         const int i = owner(imgs, n, s, twi);
         const PtBatchImage &g = imgs[i];
         const long long ls = s - g.seg_off[twi];
@@ -673,7 +684,7 @@ k_pull_batch(const QPlan base, const PtBatchImage *__restrict__ imgs, int n, lon
         if (base.ann) q.ann = base.ann + 3 * o;        /* last pass: this image's NNF records */
         pull_seg<TW, R, false, ONE>(q, atile, a + g.pix_off, b, cur_pos ? cur_pos + o : nullptr,
                                     cur_d ? cur_d + o : nullptr, ch_pos + o, ch_d + o, nxt_pos + o, nxt_d + o, counters, x0, y);
-    }
+    });
 }
 
 /* patch_dist_exact of a patch of a (RGBA rows in global memory) and a patch of b, in the
