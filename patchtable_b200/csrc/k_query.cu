@@ -288,8 +288,10 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
             const int own = pt_xy(xb, yb);
 #pragma unroll
             for (int j = 0; j < PT_PROP_TOPK; j++) {
-                cand[j] = raw[j] < 0 ? -1 : pt_xy(pt_x(raw[j]) - 7, pt_y(raw[j]) - 7);
-                bool dup = raw[j] < 0 || cand[j] == own;
+                const int px = pt_x(raw[j]) - 7, py = pt_y(raw[j]) - 7;
+                const bool in_b = raw[j] >= 0 && px >= 0 && py >= 0 && px < c_q.bew && py < c_q.beh;
+                cand[j] = in_b ? pt_xy(px, py) : -1;
+                bool dup = !in_b || cand[j] == own;
 #pragma unroll
                 for (int t = 0; t < j; t++) dup |= ((keep >> t) & 1) && cand[t] == cand[j];
                 if (!dup) keep |= 1u << j;
@@ -313,7 +315,10 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
         } else if (do_table) {
             int v = tcand[p];
             int xs = pt_x(v) - 7, ys = pt_y(v) - 7;
-            if (xs != xb || ys != yb) {
+            /* a table built here only holds patches of b; the range test guards against a corrupt
+               table file or entry array, which must not make the kernel read outside b */
+            const bool in_b = xs >= 0 && ys >= 0 && xs < c_q.bew && ys < c_q.beh;
+            if (in_b && (xs != xb || ys != yb)) {
                 float dc = dist1<TW, DESC>(aq, c_q, b, xs, ys, dbest, rows);
                 ne++;
                 if (dc < dbest) { dbest = dc; dch = dc; xb = xs; yb = ys; }
@@ -324,7 +329,8 @@ choose_seg(const QPlan &c_q, float4 *atile, const float4 *__restrict__ a, const 
             for (int k = 0; k < (LEAN ? 0 : c_q.ntc); k++) {
                 const int v1 = c_q.tcand_more[(size_t) k * np + p];
                 const int xs1 = pt_x(v1) - 7, ys1 = pt_y(v1) - 7;
-                if ((xs1 != xb || ys1 != yb) && (xs1 != xs || ys1 != ys)) {
+                const bool in_b1 = xs1 >= 0 && ys1 >= 0 && xs1 < c_q.bew && ys1 < c_q.beh;
+                if (in_b1 && (xs1 != xb || ys1 != yb) && (xs1 != xs || ys1 != ys)) {
                     float dc = dist1<TW, DESC>(aq, c_q, b, xs1, ys1, dbest, rows);
                     ne++;
                     if (dc < dbest) { dbest = dc; dch = dc; xb = xs1; yb = ys1; }
