@@ -110,7 +110,7 @@ class Clocks:
         nv = self.nv
         while not self.stop_ev.is_set():
             try:
-                self.samples.append((nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM),
+                self.samples.append((time.perf_counter(), nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM),
                                      nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
             except Exception:
                 pass
@@ -121,16 +121,23 @@ class Clocks:
             self.th = threading.Thread(target=self._loop, daemon=True)
             self.th.start()
 
-    def stop(self):
+    def stop(self, window=None):
+        """Clock record of the samples inside `window` (perf_counter start, end) -- the timed
+        region; when an NVML call is slow and fewer than 3 land there, the samples of the whole
+        sampled stretch (warm-up lookups and timed region, the same load) are used and said so."""
         if self.nv is None or self.th is None:
             return None
         self.stop_ev.set()
         self.th.join(timeout=5)
         if not self.samples:
             return None
-        reasons = sorted({n for _, r in self.samples for bit, n in self.NAMES.items() if r & bit})
-        return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
-                "reasons": reasons, "samples": len(self.samples), "source": "nvml, every 1 ms"}
+        inside = [x for x in self.samples if window is None or window[0] <= x[0] <= window[1]]
+        used, span = ((inside, "timed region") if len(inside) >= 3 else
+                      (self.samples, "timed region and the 0.25 s of warm-up lookups just before it"))
+        reasons = sorted({n for _, _, r in used for bit, n in self.NAMES.items() if r & bit})
+        return {"sm_mhz": statistics.median(m for _, m, _ in used), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(inside), "samples_used": len(used), "window": span,
+                "source": "nvml, every 1 ms"}
 
 
 def make_inputs():
@@ -497,17 +504,23 @@ def main():
         tile_ms[tile], _ = timed_schedule(table, chosen, da, H, W, dann, sptr, flush)
     params.gpu_tile = int(replicas.agree(min(tile_ms, key=tile_ms.get), dev))
     params.set_schedule(chosen)
-    for _ in range(max(args.warmup, 3)):
+    # warm-up: at least W lookups and at least 0.25 s of them, with the clocks sampled from here on
+    # (an NVML query can take longer than a millisecond, and the timed region is short)
+    clocks = Clocks(local)
+    clocks.start()
+    tw_start = time.perf_counter()
+    n_warm = 0
+    while n_warm < max(args.warmup, 3) or time.perf_counter() - tw_start < 0.25:
         flush.zero_()
         table.lookup_device(da.data_ptr(), H, W, dann.data_ptr(), sptr)
+        n_warm += 1
+        if n_warm % 16 == 0:
+            torch.cuda.synchronize()
     torch.cuda.synchronize()
-    md = mean_dist(dann.cpu().numpy())
 
     # the timed region: one CUDA event pair around each production call (pt_table_lookup_device)
-    clocks = Clocks(local)
     replicas.barrier()
     torch.cuda.synchronize()
-    clocks.start()
     ptb.reset_launch_count()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     tw0 = time.perf_counter()
@@ -519,12 +532,13 @@ def main():
     torch.cuda.synchronize()
     wall = time.perf_counter() - tw0
     launches = ptb.launch_count()
+    clk = clocks.stop((tw0, tw0 + wall))
     replicas.barrier()
-    clk = clocks.stop()
     step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
     tot_ms = replicas.max_over_ranks(sum(step_ms), dev)
     value = replicas.whole_job_rate(P * args.steps, tot_ms / 1000.0, world)
     md_timed = mean_dist(dann.cpu().numpy())
+    md = md_timed                           # every step returns the same field
 
     # per-kernel breakdown for the roofline: the same steps again through the diagnostic entry
     # point, which records a CUDA event after every kernel on the launching stream
