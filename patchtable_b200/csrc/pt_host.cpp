@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <condition_variable>
 #include <functional>
 #include <memory>
@@ -147,6 +148,18 @@ void pt_expand_nnf(const int *pos, const float *dist, long long n, double *ann) 
     pl.run(parts, [&](int k) {
         const long long i0 = std::min(n, k * per), i1 = std::min(n, i0 + per);
         widen_range(pos, dist, i0, i1, ann);
+    });
+}
+
+void pt_host_copy(float *dst, const float *src, size_t n) {
+    if (n == 0) return;
+    const std::shared_ptr<Pool> keep = pool();
+    Pool &pl = *keep;
+    const int parts = (int) std::min<size_t>((size_t) pl.size() + 1, std::max<size_t>(1, n / 65536));
+    const size_t per = (n + parts - 1) / parts;
+    pl.run(parts, [&](int k) {
+        const size_t i0 = std::min(n, (size_t) k * per), i1 = std::min(n, i0 + per);
+        if (i1 > i0) memcpy(dst + i0, src + i0, sizeof(float) * (i1 - i0));
     });
 }
 

@@ -109,3 +109,6 @@ template<class T> struct PinnedBuf {
 void pt_expand_nnf(const int *pos, const float *dist, long long n, double *ann);
 /* false when pt_set_host_threads(n < 0) asked for float64 records written on the GPU instead. */
 bool pt_host_widen();
+/* dst[0 .. n) = src[0 .. n), split across the same host threads (staging a pageable query image
+   in page-locked memory). */
+void pt_host_copy(float *dst, const float *src, size_t n);

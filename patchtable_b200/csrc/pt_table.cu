@@ -155,6 +155,7 @@ struct pt_table {
     cudaStream_t st_choose = nullptr, st_pull = nullptr; /* banded host lookups: later phases */
     std::vector<cudaEvent_t> band_ev;
     PinnedBuf<int> h_pos;             /* banded host lookups: packed field downloaded per band */
+    PinnedBuf<float> h_in;            /* banded host lookups: a pageable query image, staged per band */
     PinnedBuf<float> h_d;
     long long last_h2d = 0, last_d2h = 0;   /* bytes copied by the last host lookup */
 
@@ -867,6 +868,7 @@ struct BandIO {
     bool widen = false;
     cudaStream_t origin = nullptr;    /* the pipeline starts after and joins into this stream */
     std::atomic<int> *recorded = nullptr;   /* bands whose download event this call has recorded */
+    float *stage = nullptr;           /* page-locked copy of a pageable query image, or NULL */
 };
 
 /* Row boundaries of the bands: B rows each (a multiple of 8: the descriptor pass works on 8-row
@@ -915,7 +917,14 @@ pt_status enqueue_bands(pt_table *t, const BandIO &io, int h, int w, const std::
         const int r0 = edge[b], r1 = edge[b + 1];
         const int p0 = b == 0 ? 0 : r0 + 7, p1 = b == nb - 1 ? h : r1 + 7;
         const size_t px0 = (size_t) p0 * w * 3, npx = (size_t) (p1 - p0) * w * 3;
-        PT_CUDA(cudaMemcpyAsync(t->q_rgb.p + px0, a + px0, sizeof(float) * npx, cudaMemcpyHostToDevice, t->st_in));
+        const float *src = a + px0;
+        if (io.stage) {
+            /* a pageable image: host threads copy the band into page-locked memory, and its upload
+               runs while the next band is copied */
+            pt_host_copy(io.stage + px0, a + px0, npx);
+            src = io.stage + px0;
+        }
+        PT_CUDA(cudaMemcpyAsync(t->q_rgb.p + px0, src, sizeof(float) * npx, cudaMemcpyHostToDevice, t->st_in));
         PT_CUDA(cudaEventRecord(ev_in[b], t->st_in));
     }
     for (int b = 0; b <= nb + 1; b++) {
@@ -1007,6 +1016,16 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     BandIO io;
     io.a = a;
     io.ann_out = ann_out;
+    {
+        cudaPointerAttributes at;
+        bool pinned = false;
+        if (cudaPointerGetAttributes(&at, a) == cudaSuccess) pinned = at.type == cudaMemoryTypeHost;
+        else cudaGetLastError();
+        if (!pinned) {
+            PT_CUDA(t->h_in.reserve((size_t) h * w * 3));
+            io.stage = t->h_in.p;
+        }
+    }
     io.widen = widen;
     io.origin = t->st;
     /* Each band is widened as soon as it has arrived, by a second host thread (with the widening
