@@ -786,6 +786,15 @@ __global__ void k_init(int n, int pos, float d, int *cur_pos, float *cur_d) {
     if (p < n) { cur_pos[p] = pos; cur_d[p] = d; }
 }
 
+/* The packed form of a float64 NNF whose distances are float values (every lookup but the
+   temporal one): position x | y << 16 and the float distance, both exact. */
+__global__ void k_pack_nnf(long long n, const double *__restrict__ ann, int *pos, float *d) {
+    const long long p = blockIdx.x * (long long) NT + threadIdx.x;
+    if (p >= n) return;
+    pos[p] = pt_xy((int) ann[3 * p], (int) ann[3 * p + 1]);
+    d[p] = (float) ann[3 * p + 2];
+}
+
 __global__ void k_output(int n, const int *__restrict__ pos, const float *__restrict__ d, double *ann) {
     int p = blockIdx.x * NT + threadIdx.x;
     if (p >= n) return;
@@ -953,6 +962,13 @@ pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const floa
         default: if (r1) PT_PULL_T(256, 1) else PT_PULL_T(256, 2) break;
     }
 #undef PT_PULL_T
+    PT_LAUNCHED();
+    return PT_OK;
+}
+
+pt_status pt_launch_pack_nnf(long long n, const double *ann, int *pos, float *d, cudaStream_t st) {
+    if (n <= 0) return PT_OK;
+    k_pack_nnf<<<(unsigned) ((n + NT - 1) / NT), NT, 0, st>>>(n, ann, pos, d);
     PT_LAUNCHED();
     return PT_OK;
 }

@@ -187,6 +187,8 @@ pt_status pt_launch_choose_learned(const QuerySetup &s, const float4 *a, const f
 pt_status pt_launch_pull(const QuerySetup &s, int n, const float4 *a, const float4 *b, const int *cur_pos, const float *cur_d,
                          const int *ch_pos, const float *ch_d, int *nxt_pos, float *nxt_d,
                          unsigned long long *evals, cudaStream_t st);
+/* Packed positions and float distances of a float64 NNF whose distances are float values. */
+pt_status pt_launch_pack_nnf(long long n, const double *ann, int *pos, float *d, cudaStream_t st);
 pt_status pt_launch_output(int n, const int *pos, const float *d, double *ann, cudaStream_t st);
 /* Temporal lookups (ann_prev): initial field from the previous NNF and the final restore of the
    unscaled distance (patchtable.h:3548-3585, 4178-4193); *bad becomes 1 when a previous match lies

@@ -293,6 +293,14 @@ pt_status upload_partition(pt_table *t, cudaStream_t st) {
     return PT_OK;
 }
 
+/* Whether a host pointer is page-locked (cudaHostAlloc / cudaHostRegister / pinned tensors). */
+bool host_pinned(const void *p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) == cudaSuccess) return at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    return false;
+}
+
 bool host_allowed(const std::vector<int> &allowed, int idx, int py, int px, int ew) {
     return allowed.empty() || allowed[(size_t) py * ew + px] == idx;
 }
@@ -1016,15 +1024,9 @@ pt_status lookup_banded(pt_table *t, const float *a, int h, int w, double *ann_o
     BandIO io;
     io.a = a;
     io.ann_out = ann_out;
-    {
-        cudaPointerAttributes at;
-        bool pinned = false;
-        if (cudaPointerGetAttributes(&at, a) == cudaSuccess) pinned = at.type == cudaMemoryTypeHost;
-        else cudaGetLastError();
-        if (!pinned) {
-            PT_CUDA(t->h_in.reserve((size_t) h * w * 3));
-            io.stage = t->h_in.p;
-        }
+    if (!host_pinned(a)) {
+        PT_CUDA(t->h_in.reserve((size_t) h * w * 3));
+        io.stage = t->h_in.p;
     }
     io.widen = widen;
     io.origin = t->st;
@@ -1392,12 +1394,31 @@ pt_status pt_table_lookup(pt_table *t, const float *a, int ih, int iw, double *a
     }
     PT_TRY(ensure_query_buffers(t, h, w));
     PT_CUDA(t->q_ann.reserve((size_t) P * 3));
-    PT_CUDA(cudaMemcpyAsync(t->q_rgb.p, a, sizeof(float) * in_floats, cudaMemcpyHostToDevice, t->st));
+    /* a pageable image is copied into page-locked memory by the host threads first */
+    const float *src = a;
+    if (!host_pinned(a)) {
+        PT_CUDA(t->h_in.reserve(in_floats));
+        pt_host_copy(t->h_in.p, a, in_floats);
+        src = t->h_in.p;
+    }
+    PT_CUDA(cudaMemcpyAsync(t->q_rgb.p, src, sizeof(float) * in_floats, cudaMemcpyHostToDevice, t->st));
     PT_TRY(lookup_device(t, t->q_rgb.p, h, w, t->q_ann.p, t->st));
-    PT_CUDA(cudaMemcpyAsync(ann_out, t->q_ann.p, sizeof(double) * (size_t) P * 3, cudaMemcpyDeviceToHost, t->st));
-    PT_CUDA(cudaStreamSynchronize(t->st));
     t->last_h2d = (long long) (sizeof(float) * in_floats);
-    t->last_d2h = (long long) sizeof(double) * 3 * P;
+    if (pt_host_widen()) {
+        /* 8 bytes per patch over PCIe, widened to the float64 records by the host threads */
+        PT_CUDA(t->h_pos.reserve(P));
+        PT_CUDA(t->h_d.reserve(P));
+        PT_TRY(pt_launch_pack_nnf(P, t->q_ann.p, t->q_pos[1].p, t->q_d[1].p, t->st));
+        PT_CUDA(cudaMemcpyAsync(t->h_pos.p, t->q_pos[1].p, sizeof(int) * P, cudaMemcpyDeviceToHost, t->st));
+        PT_CUDA(cudaMemcpyAsync(t->h_d.p, t->q_d[1].p, sizeof(float) * P, cudaMemcpyDeviceToHost, t->st));
+        PT_CUDA(cudaStreamSynchronize(t->st));
+        pt_expand_nnf(t->h_pos.p, t->h_d.p, P, ann_out);
+        t->last_d2h = (long long) (sizeof(int) + sizeof(float)) * P;
+    } else {
+        PT_CUDA(cudaMemcpyAsync(ann_out, t->q_ann.p, sizeof(double) * (size_t) P * 3, cudaMemcpyDeviceToHost, t->st));
+        PT_CUDA(cudaStreamSynchronize(t->st));
+        t->last_d2h = (long long) sizeof(double) * 3 * P;
+    }
     if (seconds) *seconds = now_s() - T0;
     return PT_OK;
 }
